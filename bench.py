@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""HOLD step throughput on B200: top-level HOLD steps/s and pair interactions/s.
+
+Workload (one GPU): a seeded Plummer sphere, N = 16384 equal masses, Henon units,
+eta = 0.03, top-level step dt = 2^-6, mixed precision (FP32 pair terms, FP64 state).
+A "step" is one top-level hold_step (timesteps recomputed at the top). Inputs are
+resident in HBM when the timed region starts; L2 is flushed between timed steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: a single system does not shard (replicas only): each rank integrates its
+own independently seeded sphere; value = all ranks' steps / max-over-ranks time.
+--impl reference times the CPU FP64 restatement of the reference HOLD step (the
+reference has no CPU HOLD of its own) on the host cores, on rank 0 only.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "parallel-hhs_b200"))
+
+METRIC = "pair interactions/s & HOLD steps/s at |dE/E|<=1e-6 vs plain FP64 GPU path"
+KICK_FLOPS_PER_PAIR = 20.0   # conventional direct-sum count (Nyland, Harris & Prins 2007)
+TS_FLOPS_PER_PAIR = 50.0     # FP operations of the reference pair-timestep expression
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=16384)
+    p.add_argument("--eta", type=float, default=0.03)
+    p.add_argument("--dt", type=float, default=2.0 ** -6)
+    p.add_argument("--seed", type=int, default=2024)
+    p.add_argument("--prec", default="mixed", choices=["mixed", "fp64"])
+    p.add_argument("--schedule", default="auto", choices=["auto", "host"])
+    p.add_argument("--no-baselines", action="store_true",
+                   help="skip the FP64 GPU and CPU baselines (quick runs)")
+    return p.parse_args()
+
+
+def workload_name(a):
+    return (f"Plummer N={a.n} equal-mass Henon units, eta={a.eta}, dt_top=2^{int(round(__import__('math').log2(a.dt)))}, "
+            f"{a.prec} precision, one top-level HOLD step per step")
+
+
+# ------------------------------------------------------------------------ clocks
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200",
+                                       "-i", str(self.dev)], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------ reference arm
+def run_reference(a, rank, world):
+    """CPU FP64 restatement of the reference HOLD step on the host cores (rank 0)."""
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import hhs
+    import oracle
+    oracle.build()
+    s = hhs.plummer(a.n, a.seed)
+    budget_s = 150.0
+    t0 = time.perf_counter()
+    oracle.hold_step(s, a.dt, True, a.eta)           # one warm-up step
+    one = time.perf_counter() - t0
+    steps = max(1, min(a.steps, int(budget_s / max(one, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        oracle.hold_step(s, a.dt, True, a.eta)
+    el = time.perf_counter() - t0
+    v = steps / el
+    cores = oracle.threads()
+    return {"metric": METRIC, "value": v, "unit": "HOLD steps/s", "impl": "reference",
+            "n_gpus": world, "steps": steps, "warmup": 1, "ms_per_step": el / steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": workload_name(a).replace(a.prec, "fp64")},
+            "cpu_baseline": {"value": v, "unit": "HOLD steps/s", "cores": cores, "kind": "port",
+                             "sample": f"{steps} top-level HOLD step(s) of the same N={a.n} "
+                                       f"Plummer sphere, FP64 CPU restatement, OpenMP "
+                                       f"{cores} threads (the reference has no CPU HOLD)"},
+            "e2e": {"value": v, "unit": "HOLD steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+# ------------------------------------------------------------------------ our arm
+def run_ours(a, rank, world, torch, dist):
+    import numpy as np
+    import hhs
+
+    dev = torch.cuda.current_device()
+    stream = torch.cuda.Stream()
+    sh = ctypes.c_void_p(stream.cuda_stream)
+    prec = hhs.PREC_MIXED if a.prec == "mixed" else hhs.PREC_FP64
+    seed = a.seed + 7919 * rank
+    ics = hhs.plummer(a.n, seed)
+    e0 = hhs.energy_host(ics)
+    ctx = hhs.Context(a.n, 64, eta=a.eta)
+    sys_ = hhs.ParticleSystem(a.n)
+    sys_.upload(ics, stream=sh)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def step(p=prec):
+        if a.schedule == "host":
+            hhs.hold_step_host(ctx, sys_, a.n, a.dt, True, p, stream=sh)
+        else:
+            hhs.hold_step(ctx, sys_, a.n, 0.0, a.dt, True, p, stream=sh)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    with torch.cuda.stream(stream):
+        for _ in range(a.warmup):
+            step()
+        ctx.check(sh)
+        ctx.reset_stats(sh)
+        ctx.set_profiling(True)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(a.steps)]
+        clocks = ClockSampler(dev)
+        barrier()
+        torch.cuda.synchronize()
+        clocks.start()
+        l0 = hhs.launch_count()
+        for k in range(a.steps):
+            flush.zero_()
+            evs[k][0].record(stream)
+            step()
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        l1 = hhs.launch_count()
+        barrier()
+        clk = clocks.stop()
+        ctx.check(sh)
+        t_ms = sum(e0_.elapsed_time(e1_) for e0_, e1_ in evs)
+        prof = ctx.profile()
+        ctx.set_profiling(False)
+        stats = ctx.stats(sh)
+        out = sys_.download(stream=sh)
+        torch.cuda.synchronize()
+    e1 = hhs.energy_host(out)
+
+    t_max = t_ms
+    if dist is not None:
+        t = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    steps_total = a.steps * world
+    value = steps_total / (t_max * 1e-3)
+    pairs_step = (stats["kick_pairs"] + stats["ts_pairs"]) / a.steps
+    res = {"value": value, "t_ms": t_max, "pairs_per_step": pairs_step, "stats": stats,
+           "prof": prof, "clocks": clk, "launches": (l1 - l0), "dE_over_E": (e1 - e0) / e0}
+
+    # ---- end to end through the public API: host buffers, copies inside the timed region
+    pin = {k: torch.from_numpy(np.ascontiguousarray(out[k])).pin_memory().numpy()
+           for k in ("x", "y", "z", "vx", "vy", "vz", "m", "ts")}
+    pin["id"] = torch.from_numpy(out["id"].copy()).pin_memory().numpy()
+    res_pin = {k: torch.empty(a.n, dtype=torch.float64).pin_memory().numpy()
+               for k in ("x", "y", "z", "vx", "vy", "vz", "ts")}
+    h2d = a.n * (8 * 8 + 4)
+    d2h = a.n * 7 * 8
+    L = hhs.lib()
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int32)
+
+    def pp(arr, t=dp):
+        return None if arr is None else arr.ctypes.data_as(t)
+
+    with torch.cuda.stream(stream):
+        e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(a.steps)]
+        barrier()
+        torch.cuda.synchronize()
+        for k in range(a.steps):
+            flush.zero_()
+            e2e_ev[k][0].record(stream)
+            assert L.hhs_particle_system_upload(sys_.ref, a.n, *[pp(pin[f]) for f in
+                                                                 ("x", "y", "z", "vx", "vy", "vz",
+                                                                  "m", "ts")],
+                                                pp(pin["id"], ip), sh) == 0
+            step()
+            assert L.hhs_particle_system_download(sys_.ref, a.n, *[pp(res_pin.get(f)) for f in
+                                                                   ("x", "y", "z", "vx", "vy",
+                                                                    "vz", "m", "ts")],
+                                                  None, sh) == 0
+            e2e_ev[k][1].record(stream)
+            stream.synchronize()
+            for f in res_pin:
+                pin[f][:] = res_pin[f]
+        torch.cuda.synchronize()
+        barrier()
+    t_e2e = sum(x.elapsed_time(y) for x, y in e2e_ev)
+    if dist is not None:
+        t = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    res["e2e"] = {"value": steps_total / (t_e2e * 1e-3), "unit": "HOLD steps/s",
+                  "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+
+    # ---- plain FP64 GPU HOLD (host-driven schedule): the denominator of the target
+    if not a.no_baselines:
+        k64 = max(2, a.steps // 5)
+        sys64 = hhs.ParticleSystem(a.n)
+        sys64.upload(ics, stream=sh)
+        with torch.cuda.stream(stream):
+            hhs.hold_step_host(ctx, sys64, a.n, a.dt, True, hhs.PREC_FP64, stream=sh)
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in range(k64)]
+            torch.cuda.synchronize()
+            for k in range(k64):
+                flush.zero_()
+                evs[k][0].record(stream)
+                hhs.hold_step_host(ctx, sys64, a.n, a.dt, True, hhs.PREC_FP64, stream=sh)
+                evs[k][1].record(stream)
+            torch.cuda.synchronize()
+        t64 = sum(x.elapsed_time(y) for x, y in evs)
+        res["fp64_plain_steps_per_s"] = k64 / (t64 * 1e-3)
+        res["fp64_plain_steps"] = k64
+    res["fma_peaks"] = hhs.measure_fma_peaks(sh)
+    return res
+
+
+def roofline(res, a, peaks_tflops):
+    prof = res["prof"]
+    if not prof:
+        return None
+    kind = max(("kick", "timesteps"), key=lambda k: prof.get(k, {}).get("ms", 0.0))
+    p = prof[kind]
+    fpp = KICK_FLOPS_PER_PAIR if kind == "kick" else TS_FLOPS_PER_PAIR
+    avg_ms = p["ms"] / p["launches"]
+    flops_per_launch = p["pairs"] * fpp / p["launches"]
+    achieved = flops_per_launch / (avg_ms * 1e-3) / 1e12
+    peak = peaks_tflops[0] if a.prec == "mixed" else peaks_tflops[1]
+    return {"bound": "fp32-fma" if a.prec == "mixed" else "fp64-fma", "kernel": kind,
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "peak_source": "measured FMA-chain peak of this B200 (hhs_measure_fma_peaks)",
+            "flops_per_pair": fpp, "avg_launch_ms": avg_ms, "launches": p["launches"],
+            "share_of_step": p["ms"] / res["t_ms"], "traffic": None}
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        out = run_reference(a, rank, world)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as d
+        d.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                             device_id=torch.device("cuda", local))
+        dist = d
+    res = run_ours(a, rank, world, torch, dist)
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_baselines:
+        ref = run_reference(argparse.Namespace(**{**vars(a), "steps": 1}), 0, 1)
+        cpu = ref["cpu_baseline"]
+    if rank == 0:
+        step_ms = res["t_ms"] / a.steps
+        line = {
+            "metric": METRIC, "value": res["value"], "unit": "HOLD steps/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32-pair/f64-state" if a.prec == "mixed" else "f64",
+            "data": "synthetic (seeded Plummer sphere; no dataset)",
+            "config": {"workload": workload_name(a), "n": a.n, "eta": a.eta, "dt_top": a.dt,
+                       "precision": a.prec, "schedule": a.schedule,
+                       "l2": "flushed between timed steps (256 MiB memset)",
+                       "parallelism": f"replicas x{world}"},
+            "pair_interactions_per_s": res["pairs_per_step"] * res["value"],
+            "pairs_per_step": res["pairs_per_step"],
+            "hierarchy": {"nodes_per_step": res["stats"]["nodes"] / a.steps,
+                          "max_level": res["stats"]["max_level"]},
+            "dE_over_E_bench_run": res["dE_over_E"],
+            "e2e": res["e2e"],
+            "gpu_launches": res["launches"],
+            "clocks": res["clocks"],
+            "roofline": roofline(res, a, res["fma_peaks"]),
+            "kernel_profile": res["prof"],
+            "fma_peaks_tflops": {"fp32": res["fma_peaks"][0], "fp64": res["fma_peaks"][1]},
+            "cpu_baseline": cpu,
+        }
+        if "fp64_plain_steps_per_s" in res:
+            line["fp64_plain_gpu"] = {"value": res["fp64_plain_steps_per_s"],
+                                      "unit": "HOLD steps/s", "steps": res["fp64_plain_steps"],
+                                      "schedule": "host-driven, one-thread-per-sink FP64"}
+            line["speedup_vs_fp64_plain"] = res["value"] / res["fp64_plain_steps_per_s"]
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

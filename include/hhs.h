@@ -1,0 +1,217 @@
+/*
+ * hhs.h -- C ABI of the B200-native HOLD (Hierarchical Hamiltonian Splitting) step.
+ *
+ * Drop-in boundary for the header-only C++ templates of parallel-hhs
+ * (paths relative to that project's root). Every function returns an hhs_status,
+ * never calls exit(), and runs stream-ordered on the caller's cudaStream_t
+ * (passed as void*; NULL = legacy default stream). No function allocates device
+ * memory while a step runs: particle systems and contexts are allocated up front.
+ *
+ * Floating point: FP64 state (positions, velocities, masses, timesteps).
+ * HHS_PREC_FP64 evaluates every pair term in FP64 with the reference's operation
+ * order and no fused multiply-add, so it reproduces the CPU FP64 restatement bit
+ * for bit. HHS_PREC_MIXED evaluates pair terms in FP32 from FP64 relative
+ * coordinates and accumulates with compensated FP32 sums applied in FP64.
+ */
+#ifndef HHS_H
+#define HHS_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Replaces gpuErrchk -> exit(code) (src/utils.cuh:4-12) and the exit(1) store checks
+ * (src/particle_system.cuh:138-141,164-167,181-184,198-201,214-217,232-235). */
+typedef enum {
+    HHS_OK = 0,
+    HHS_ERR_INVALID_ARG = 1,
+    HHS_ERR_CUDA = 2,
+    HHS_ERR_OOM = 3,
+    HHS_ERR_TIMEOUT = 4,             /* a bounded device wait gave up */
+    HHS_ERR_DEVICE_FAULT_FLAG = 5,   /* a device-side check recorded an error word */
+    HHS_ERR_DEPTH = 6,               /* hierarchy deeper than the context's level capacity */
+    HHS_ERR_CAPACITY = 7             /* n larger than the object was created for */
+} hhs_status;
+
+typedef enum { HHS_PREC_FP64 = 0, HHS_PREC_MIXED = 1 } hhs_precision;
+
+typedef enum {
+    HHS_MASS_EQUAL = 0,
+    HHS_MASS_SALPETER = 1,       /* dN/dm ~ m^-2.35 on [0.1, 100] */
+    HHS_MASS_TWO_COMPONENT = 2   /* 90% m = 1, 10% m = 10 */
+} hhs_mass_spectrum;
+
+/* {N_slow, N_fast} -- struct partition, src/particle_system.cuh:8-11 */
+typedef struct {
+    int32_t n_slow;
+    int32_t n_fast;
+} hhs_partition;
+
+/* nbody_params<T>, src/particle_system.cuh:13-17 (eps is stored, unused as in the
+ * reference: src/hold.cuh:136,141,157) */
+typedef struct {
+    double eta;
+    double eps;
+} hhs_params;
+
+/* particle_system<T>, src/particle_system.cuh:20-54, as true SoA FP64 device arrays.
+ * The caller owns the struct; hhs_particle_system_alloc fills the pointers from one
+ * device allocation (256-byte aligned arrays). */
+typedef struct {
+    int32_t n;                /* capacity */
+    double *x, *y, *z;        /* pos */
+    double *vx, *vy, *vz;     /* vel */
+    double *ax, *ay, *az;     /* acc (written by the standalone kicks) */
+    double *ts;               /* timestep */
+    double *m;
+    int32_t *id, *parent_id;
+    void* _base;              /* owning allocation */
+} hhs_particle_system;
+
+/* gpu_alloc / gpu_free: src/particle_system.cuh:135-177 */
+hhs_status hhs_particle_system_alloc(hhs_particle_system* sys, int32_t n);
+hhs_status hhs_particle_system_free(hhs_particle_system* sys);
+
+/* host_to_gpu / gpu_to_host: src/particle_system.cuh:212-247. Host arrays are SoA;
+ * any pointer may be NULL to skip that field. Copies are async on `stream`
+ * (pinned host memory makes them truly asynchronous). */
+hhs_status hhs_particle_system_upload(hhs_particle_system* sys, int32_t n,
+                                      const double* x, const double* y, const double* z,
+                                      const double* vx, const double* vy, const double* vz,
+                                      const double* m, const double* ts, const int32_t* id,
+                                      void* stream);
+hhs_status hhs_particle_system_download(const hhs_particle_system* sys, int32_t n,
+                                        double* x, double* y, double* z,
+                                        double* vx, double* vy, double* vz,
+                                        double* m, double* ts, int32_t* id, void* stream);
+/* Interleaved (vec3<double>, AoS) host layout of the reference: pos/vel as 3n doubles. */
+hhs_status hhs_particle_system_upload_aos(hhs_particle_system* sys, int32_t n,
+                                          const double* pos3, const double* vel3,
+                                          const double* m, const double* ts,
+                                          const int32_t* id, void* stream);
+hhs_status hhs_particle_system_download_aos(const hhs_particle_system* sys, int32_t n,
+                                            double* pos3, double* vel3, double* m,
+                                            double* ts, int32_t* id, void* stream);
+
+/* Library context: nbodysystem_globals<T> (src/particle_system.cuh:65-104) plus the
+ * per-level arena that replaces the per-call nbodysystem_buffers<T> allocations of
+ * src/hold.cuh:56 (and the per-call scan cudaMalloc of src/split.cuh:512-514).
+ * One context per stream; distinct contexts are independent. */
+typedef struct hhs_ctx hhs_ctx;
+
+size_t hhs_workspace_size(int32_t n_max, int32_t max_levels);
+hhs_status hhs_ctx_create(int32_t n_max, int32_t max_levels, hhs_params params,
+                          hhs_ctx** out);
+hhs_status hhs_ctx_destroy(hhs_ctx* ctx);
+hhs_status hhs_ctx_set_params(hhs_ctx* ctx, hhs_params params);
+/* globals->simtime (sum of leaf dt, src/hold.cuh:106-114) -- synchronises the stream */
+hhs_status hhs_ctx_get_simtime(hhs_ctx* ctx, double* simtime, void* stream);
+hhs_status hhs_ctx_flush_simtime(hhs_ctx* ctx, void* stream);
+/* Synchronises the stream and converts the device error words (bounded waits that
+ * gave up, depth or capacity overflow) into a status. */
+hhs_status hhs_ctx_check(hhs_ctx* ctx, void* stream);
+hhs_status hhs_ctx_clear_errors(hhs_ctx* ctx, void* stream);
+
+/* timesteps<T,BS>(sys, globals, N): src/timestep.cuh:103-118 (kernel :65-99) */
+hhs_status hhs_timesteps(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n,
+                         hhs_precision prec, void* stream);
+
+/* split<T,BS,U>(total, slow, fast, pred, scan, pivot, N, part): src/split.cuh:573-610.
+ * Predicate ts <= pivot, exact exclusive scan, stable scatter of pos, vel, m, ts, id
+ * with parent_id = source index, N_fast == 1 folded into slow (lone particle last).
+ * `part` is a device (or managed) pointer written on the stream; `predicate` and
+ * `scanned_predicate` are optional device int32[n] outputs (NULL = not written). */
+hhs_status hhs_split(hhs_ctx* ctx, const hhs_particle_system* total,
+                     hhs_particle_system* slow, hhs_particle_system* fast,
+                     int32_t* predicate, int32_t* scanned_predicate, double pivot,
+                     int32_t n, hhs_partition* part, void* stream);
+
+/* kick_slow<T,BS>(sys, dt, fac, N): src/kick.cuh:158-168. acc = sum over the set;
+ * vel += acc * (fac*dt). Attractive gravity, as the reference's CPU force test has it
+ * (tests/test_nbforce.cu:14-18); the reference GPU kernel adds the opposite sign
+ * (src/kick.cuh:23,28). */
+hhs_status hhs_kick_slow(hhs_particle_system* sys, double dt, double fac, int32_t n,
+                         hhs_precision prec, void* stream);
+/* kick_sf<T,BS>(so_sys, si_sys, dt, fac, N_sink, M_src): src/kick.cuh:170-181 */
+hhs_status hhs_kick_sf(const hhs_particle_system* so_sys, hhs_particle_system* si_sys,
+                       double dt, double fac, int32_t n_sink, int32_t m_src,
+                       hhs_precision prec, void* stream);
+/* drift<T,BS>(sys, dt, fac, N): src/drift.cuh:30-43 */
+hhs_status hhs_drift(hhs_particle_system* sys, double dt, double fac, int32_t n,
+                     void* stream);
+/* update_system<T,BS>(prev, cur, N): src/update_system.cuh:29-43 */
+hhs_status hhs_update_system(hhs_particle_system* prev, const hhs_particle_system* cur,
+                             int32_t n, void* stream);
+
+/* hold_step<T,BS>(clevel, globals, sys, N, stime, etime, dt, calc_timestep):
+ * src/hold.cuh:51-181. The whole recursive step on the first n particles of sys,
+ * stream-ordered; partition counts stay on the device. clevel only labels the trace. */
+hhs_status hhs_hold_step(hhs_ctx* ctx, int32_t clevel, hhs_particle_system* sys,
+                         int32_t n, double stime, double etime, double dt,
+                         int32_t calc_timestep, hhs_precision prec, void* stream);
+
+/* The same step driven from the host: the partition counts are read back after every
+ * split (the reference synchronises at the same point, src/split.cuh:430) and the
+ * recursion runs on the CPU. Synchronous; the plain baseline schedule. */
+hhs_status hhs_hold_step_host(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n, double dt,
+                              int32_t calc_timestep, hhs_precision prec, void* stream);
+
+/* Exact exclusive prefix sum of int32 values (the contract of
+ * scan_predicate_small/large, src/split.cuh:438-565) in one decoupled-lookback pass.
+ * d_workspace: hhs_scan_workspace_size(n) bytes of device memory (need not be zeroed;
+ * the call clears what it uses). */
+size_t hhs_scan_workspace_size(int64_t n);
+hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out, int64_t n,
+                                  void* d_workspace, size_t workspace_bytes, void* stream);
+/* Synchronises the stream; HHS_ERR_TIMEOUT if a look-back wait of the last scan on this
+ * workspace gave up. */
+hhs_status hhs_scan_workspace_status(const void* d_workspace, void* stream);
+
+/* ---- diagnostics ---------------------------------------------------------------- */
+/* Work recorded by the HOLD schedule since the last reset (device counters). */
+typedef struct {
+    uint64_t nodes;          /* hold_step calls (split nodes) */
+    int32_t max_level;
+    int32_t _pad;
+    double kick_pairs;       /* sum over nodes of N_s(N_s-1) + 2 N_s N_f */
+    double ts_pairs;         /* sum over timestep evaluations of N(N-1) */
+} hhs_stats;
+hhs_status hhs_ctx_get_stats(hhs_ctx* ctx, hhs_stats* out, void* stream);
+hhs_status hhs_ctx_reset_stats(hhs_ctx* ctx, void* stream);
+
+/* Per-kernel timing of the pair kernels (CUDA events on the launching stream) while
+ * profiling is on; kinds: 0 timesteps, 1 kick, 2 split, 3 drift, 4 whole-step engine. */
+typedef struct {
+    uint64_t launches[8];
+    double ms[8];
+    double pairs[8];
+} hhs_profile;
+hhs_status hhs_ctx_set_profiling(hhs_ctx* ctx, int32_t on);
+hhs_status hhs_ctx_get_profile(hhs_ctx* ctx, hhs_profile* out);
+
+/* Kernel launches issued by this library since it was loaded (all contexts). */
+uint64_t hhs_kernel_launch_count(void);
+
+/* Measured arithmetic peaks of the current device: a register-resident chain of FP32
+ * (and FP64) fused multiply-adds on every SM, timed with CUDA events. TFLOP/s. */
+hhs_status hhs_measure_fma_peaks(double* fp32_tflops, double* fp64_tflops, void* stream);
+
+/* Host-side utilities (no GPU): seeded Plummer initial conditions in Henon units,
+ * and FP64 energies with compensated sums. */
+hhs_status hhs_ic_plummer(int32_t n, uint64_t seed, int32_t mass_spectrum, double* x,
+                          double* y, double* z, double* vx, double* vy, double* vz,
+                          double* m);
+double hhs_host_potential_energy(int32_t n, const double* x, const double* y,
+                                 const double* z, const double* m);
+double hhs_host_kinetic_energy(int32_t n, const double* vx, const double* vy,
+                               const double* vz, const double* m);
+
+/* Human-readable name of a status code. */
+const char* hhs_status_string(hhs_status s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HHS_H */

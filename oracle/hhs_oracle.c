@@ -1,0 +1,303 @@
+/*
+ * hhs_oracle.c -- CPU FP64 restatement of the HOLD step of parallel-hhs.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker). Only the tests, the smoke check and the
+ * benchmark's CPU-baseline leg load this file's library; the product never does.
+ * Compiled with -O2 -ffp-contract=off -fopenmp; see hhs_oracle.h for the map from
+ * each function to the reference lines it restates.
+ */
+#include "hhs_oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define ORACLE_HUGE 1.e30 /* src/timestep.cuh:4 */
+
+int oracle_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/* Pair timestep of sink i against every source j != i.
+ * Restates src/timestep.cuh:17-60 expression by expression:
+ *   dr = x_i - x_j, dv = v_i - v_j, r = sqrt(dr.dr), vdotdr2 = (dr.dv)/dr2
+ *   free-fall: tau = eta/M_SQRT2 * r * sqrt(r/(m_j+m_i)); dtau = 3*tau*vdotdr2/2
+ *   fly-by:    tau = eta*r/sqrt(dv2); dtau = tau*vdotdr2*(1+(m_i+m_j)/(dv2*r))
+ *   each: dtau = (dtau < 1) ? dtau : 1; tau /= (1 - dtau/2); min. */
+void oracle_timesteps(int n, const double* x, const double* y, const double* z,
+                      const double* vx, const double* vy, const double* vz,
+                      const double* m, double eta, double* ts) {
+    const double eta_s2 = eta / M_SQRT2;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int i = 0; i < n; i++) {
+        const double xi = x[i], yi = y[i], zi = z[i];
+        const double vxi = vx[i], vyi = vy[i], vzi = vz[i];
+        const double mi = m[i];
+        double minval = ORACLE_HUGE;
+        for (int j = 0; j < n; j++) {
+            if (j == i) continue;
+            const double drx = xi - x[j], dry = yi - y[j], drz = zi - z[j];
+            const double dvx = vxi - vx[j], dvy = vyi - vy[j], dvz = vzi - vz[j];
+            const double dr2 = drx * drx + dry * dry + drz * drz;
+            const double dv2 = dvx * dvx + dvy * dvy + dvz * dvz;
+            const double r = sqrt(dr2);
+            const double vdotdr2 = (dvx * drx + dvy * dry + dvz * drz) / dr2;
+            double tau = eta_s2 * r * sqrt(r / (m[j] + mi));
+            double dtau = 3 * tau * vdotdr2 / 2;
+            dtau = (dtau < 1) ? dtau : 1;
+            tau /= (1 - dtau / 2);
+            if (tau < minval) minval = tau;
+            tau = eta * r / sqrt(dv2);
+            dtau = tau * vdotdr2 * (1 + (mi + m[j]) / (dv2 * r));
+            dtau = (dtau < 1) ? dtau : 1;
+            tau /= (1 - dtau / 2);
+            if (tau < minval) minval = tau;
+        }
+        ts[i] = minval;
+    }
+}
+
+/* Exact exclusive prefix sum (the contract of the reference's multi-level Blelloch
+ * scan, src/split.cuh:131-302 and its host recursion :438-565). */
+void oracle_scan_exclusive_i32(int64_t n, const int32_t* in, int32_t* out) {
+    int32_t acc = 0;
+    for (int64_t i = 0; i < n; i++) {
+        out[i] = acc;
+        acc += in[i];
+    }
+}
+
+/* Predicate ts <= pivot (src/split.cuh:114-116), exclusive scan, stable scatter
+ * (src/split.cuh:335-357): fast particle i goes to scan[i], slow particle i goes to
+ * i - scan[i]. N_fast = pred[N-1] + scan[N-1] (:312). If N_fast == 1 the lone fast
+ * particle is folded into the slow set at slot N-1 and N_fast becomes 0 (intended
+ * semantics of :321-324,361-368). order[] holds parent indices. */
+int oracle_split(int n, const double* ts, double pivot, int32_t* order) {
+    if (n <= 0) return 0;
+    int32_t* pred = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+    int32_t* scan = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+    for (int i = 0; i < n; i++) pred[i] = ts[i] <= pivot;
+    oracle_scan_exclusive_i32(n, pred, scan);
+    int n_fast = pred[n - 1] + scan[n - 1];
+    if (n_fast == 1) {
+        int lone = -1;
+        for (int i = 0; i < n; i++) {
+            if (pred[i]) lone = i;
+            else order[i - scan[i]] = i;
+        }
+        order[n - 1] = lone;
+        n_fast = 0;
+    } else {
+        for (int i = 0; i < n; i++) {
+            if (pred[i]) order[scan[i]] = i;
+            else order[n_fast + (i - scan[i])] = i;
+        }
+    }
+    free(pred);
+    free(scan);
+    return n_fast;
+}
+
+/* Direct-sum kick, restating src/kick.cuh:19-30 and :82-105 per sink:
+ *   dx = x_j - x_i; d2 = dx.dx; skip d2 == 0; d = sqrt(d2); inv = 1.0/(d2*d);
+ *   a += dx * (m_j * inv)           (attractive; the reference GPU kernel has the
+ *                                    opposite sign, see tests/test_nbforce.cu:14-18)
+ *   v += a * dtfac                  (dtfac = fac*dt of the reference call)
+ * Sources are summed in index order. */
+void oracle_kick(int n_sink, const double* sx, const double* sy, const double* sz,
+                 double* svx, double* svy, double* svz,
+                 double* ax, double* ay, double* az,
+                 int n_src, const double* px, const double* py, const double* pz,
+                 const double* pm, double dtfac) {
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int i = 0; i < n_sink; i++) {
+        const double xi = sx[i], yi = sy[i], zi = sz[i];
+        double accx = 0.0, accy = 0.0, accz = 0.0;
+        for (int j = 0; j < n_src; j++) {
+            const double dxx = px[j] - xi, dxy = py[j] - yi, dxz = pz[j] - zi;
+            const double d2 = dxx * dxx + dxy * dxy + dxz * dxz;
+            if (d2 == 0.0) continue;
+            const double d = sqrt(d2);
+            const double inv = 1.0 / (d2 * d);
+            const double s = pm[j] * inv;
+            accx = accx + dxx * s;
+            accy = accy + dxy * s;
+            accz = accz + dxz * s;
+        }
+        if (ax) { ax[i] = accx; ay[i] = accy; az[i] = accz; }
+        svx[i] = svx[i] + accx * dtfac;
+        svy[i] = svy[i] + accy * dtfac;
+        svz[i] = svz[i] + accz * dtfac;
+    }
+}
+
+/* pos += vel * (dt*fac)   (src/drift.cuh:24-26) */
+void oracle_drift(int n, double* x, double* y, double* z,
+                  const double* vx, const double* vy, const double* vz, double dtfac) {
+    for (int i = 0; i < n; i++) {
+        x[i] = x[i] + vx[i] * dtfac;
+        y[i] = y[i] + vy[i] * dtfac;
+        z[i] = z[i] + vz[i] * dtfac;
+    }
+}
+
+/* ---------------------------------------------------------------------------- */
+/* Recursive HOLD on per-level copies (src/hold.cuh:51-181)                      */
+
+typedef struct {
+    int n;
+    double *x, *y, *z, *vx, *vy, *vz, *m, *ts;
+    int32_t *id, *parent;
+} osys;
+
+static void osys_alloc(osys* s, int n) {
+    size_t nn = (size_t)(n > 0 ? n : 1);
+    s->n = n;
+    double* d = (double*)malloc(sizeof(double) * nn * 8);
+    s->x = d; s->y = d + nn; s->z = d + 2 * nn;
+    s->vx = d + 3 * nn; s->vy = d + 4 * nn; s->vz = d + 5 * nn;
+    s->m = d + 6 * nn; s->ts = d + 7 * nn;
+    s->id = (int32_t*)malloc(sizeof(int32_t) * nn * 2);
+    s->parent = s->id + nn;
+}
+
+static void osys_free(osys* s) {
+    free(s->x);
+    free(s->id);
+}
+
+/* copy parent particle order[k] into child slot k (src/split.cuh:341-356) */
+static void osys_gather(osys* child, const osys* parent, const int32_t* order, int cnt) {
+    for (int k = 0; k < cnt; k++) {
+        int i = order[k];
+        child->x[k] = parent->x[i]; child->y[k] = parent->y[i]; child->z[k] = parent->z[i];
+        child->vx[k] = parent->vx[i]; child->vy[k] = parent->vy[i]; child->vz[k] = parent->vz[i];
+        child->m[k] = parent->m[i]; child->ts[k] = parent->ts[i];
+        child->id[k] = parent->id[i];
+        child->parent[k] = i;
+    }
+    child->n = cnt;
+}
+
+/* prev[parent_id[k]] <- cur[k] for pos, vel, m, timestep (src/update_system.cuh:14-23) */
+static void osys_update(osys* prev, const osys* cur) {
+    for (int k = 0; k < cur->n; k++) {
+        int p = cur->parent[k];
+        prev->x[p] = cur->x[k]; prev->y[p] = cur->y[k]; prev->z[p] = cur->z[k];
+        prev->vx[p] = cur->vx[k]; prev->vy[p] = cur->vy[k]; prev->vz[p] = cur->vz[k];
+        prev->m[p] = cur->m[k];
+        prev->ts[p] = cur->ts[k];
+    }
+}
+
+static void trace_node(oracle_trace* tr, int level, int n, int nf, int calc) {
+    if (!tr) return;
+    if (tr->nodes && tr->count < tr->capacity) {
+        oracle_node* e = &tr->nodes[tr->count];
+        e->level = level; e->n = n; e->n_fast = nf; e->calc_ts = calc;
+    }
+    tr->count++;
+    if (level > tr->max_level) tr->max_level = level;
+    double ns = (double)(n - nf), nfd = (double)nf;
+    tr->kick_pairs += ns * (ns - 1.0) + 2.0 * ns * nfd;
+    if (calc) tr->ts_pairs += (double)n * (double)(n - 1);
+}
+
+static void hold_rec(int level, osys* total, double dt, int calc_ts, double eta,
+                     oracle_trace* tr) {
+    const int n = total->n;
+    if (calc_ts)
+        oracle_timesteps(n, total->x, total->y, total->z, total->vx, total->vy,
+                         total->vz, total->m, eta, total->ts);
+    int32_t* order = (int32_t*)malloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+    int nf = oracle_split(n, total->ts, dt, order);
+    int ns = n - nf;
+    trace_node(tr, level, n, nf, calc_ts);
+
+    osys fast, slow;
+    osys_alloc(&fast, nf);
+    osys_alloc(&slow, ns);
+    osys_gather(&fast, total, order, nf);
+    osys_gather(&slow, total, order + nf, ns);
+    free(order);
+
+    if (nf == 0 && tr) tr->leaf_time += dt; /* src/hold.cuh:106-114 */
+
+    if (nf > 0) hold_rec(level + 1, &fast, dt / 2, 0, eta, tr);
+    if (ns > 0)
+        oracle_drift(ns, slow.x, slow.y, slow.z, slow.vx, slow.vy, slow.vz, dt * 0.5);
+    if (ns > 0) {
+        /* kick_slow(slow, dt, 1.0): v += a * (1.0*dt)  (src/hold.cuh:138) */
+        oracle_kick(ns, slow.x, slow.y, slow.z, slow.vx, slow.vy, slow.vz, NULL, NULL, NULL,
+                    ns, slow.x, slow.y, slow.z, slow.m, 1.0 * dt);
+        if (nf > 0) {
+            /* kick_sf(src=fast, sink=slow, 1.0, dt): v += a * (dt*1.0)  (:142) */
+            oracle_kick(ns, slow.x, slow.y, slow.z, slow.vx, slow.vy, slow.vz, NULL, NULL,
+                        NULL, nf, fast.x, fast.y, fast.z, fast.m, dt * 1.0);
+            /* kick_sf(src=slow, sink=fast, 1.0, dt)  (:143) */
+            oracle_kick(nf, fast.x, fast.y, fast.z, fast.vx, fast.vy, fast.vz, NULL, NULL,
+                        NULL, ns, slow.x, slow.y, slow.z, slow.m, dt * 1.0);
+        }
+    }
+    if (ns > 0)
+        oracle_drift(ns, slow.x, slow.y, slow.z, slow.vx, slow.vy, slow.vz, dt * 0.5);
+    if (nf > 0) hold_rec(level + 1, &fast, dt / 2, 1, eta, tr);
+
+    osys_update(total, &fast);
+    osys_update(total, &slow);
+    osys_free(&fast);
+    osys_free(&slow);
+}
+
+void oracle_hold_step(int n, double* x, double* y, double* z,
+                      double* vx, double* vy, double* vz, double* m, double* ts,
+                      int32_t* id, double dt, int calc_ts, double eta,
+                      oracle_trace* trace) {
+    if (n <= 0) return;
+    osys top;
+    top.n = n; top.x = x; top.y = y; top.z = z; top.vx = vx; top.vy = vy; top.vz = vz;
+    top.m = m; top.ts = ts; top.id = id; top.parent = NULL;
+    hold_rec(0, &top, dt, calc_ts, eta, trace);
+}
+
+/* Neumaier compensated accumulation */
+typedef struct { double s, c; } nsum;
+static inline void nsum_add(nsum* a, double v) {
+    double t = a->s + v;
+    if (fabs(a->s) >= fabs(v)) a->c += (a->s - t) + v;
+    else a->c += (v - t) + a->s;
+    a->s = t;
+}
+
+void oracle_energy(int n, const double* x, const double* y, const double* z,
+                   const double* vx, const double* vy, const double* vz,
+                   const double* m, double* out) {
+    nsum ke = {0, 0};
+    for (int i = 0; i < n; i++)
+        nsum_add(&ke, 0.5 * m[i] * (vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i]));
+    /* per-row compensated sums, then a sequential compensated sum over rows, so the
+     * result does not depend on the thread count */
+    double* rows = (double*)malloc(sizeof(double) * (size_t)(2 * (n > 0 ? n : 1)));
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int i = 0; i < n; i++) {
+        nsum row = {0, 0};
+        for (int j = i + 1; j < n; j++) {
+            double dx = x[i] - x[j], dy = y[i] - y[j], dz = z[i] - z[j];
+            double r = sqrt(dx * dx + dy * dy + dz * dz);
+            if (r > 0.0) nsum_add(&row, -m[i] * m[j] / r);
+        }
+        rows[2 * i] = row.s;
+        rows[2 * i + 1] = row.c;
+    }
+    nsum pot = {0, 0};
+    for (int i = 0; i < 2 * n; i++) nsum_add(&pot, rows[i]);
+    free(rows);
+    out[0] = ke.s + ke.c;
+    out[1] = pot.s + pot.c;
+}

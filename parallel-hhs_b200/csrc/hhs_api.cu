@@ -1,0 +1,526 @@
+// hhs_api.cu -- C ABI: particle systems, the context, the reference-shaped entry
+// points (timesteps / split / kick_slow / kick_sf / drift / update_system) and the
+// host-driven HOLD schedule.
+#include <atomic>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "hhs_ctx.h"
+#include "hhs_kernels.h"
+
+namespace {
+
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t v) { return (v + kAlign - 1) & ~(kAlign - 1); }
+
+SoA soa_of(const hhs_particle_system* s) {
+    SoA r;
+    r.x = s->x; r.y = s->y; r.z = s->z;
+    r.vx = s->vx; r.vy = s->vy; r.vz = s->vz;
+    r.m = s->m; r.ts = s->ts; r.id = s->id;
+    return r;
+}
+
+bool sys_ok(const hhs_particle_system* s) { return s && s->_base && s->n > 0; }
+
+// (de)interleave vec3<double> arrays through the acc region (3n contiguous doubles)
+__global__ void k_deinterleave(const double* __restrict__ v3, double* __restrict__ x,
+                               double* __restrict__ y, double* __restrict__ z, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        x[i] = v3[3 * (size_t)i];
+        y[i] = v3[3 * (size_t)i + 1];
+        z[i] = v3[3 * (size_t)i + 2];
+    }
+}
+
+__global__ void k_interleave(double* __restrict__ v3, const double* __restrict__ x,
+                             const double* __restrict__ y, const double* __restrict__ z,
+                             int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        v3[3 * (size_t)i] = x[i];
+        v3[3 * (size_t)i + 1] = y[i];
+        v3[3 * (size_t)i + 2] = z[i];
+    }
+}
+
+inline int small_grid(int n) {
+    int g = (n + 255) / 256;
+    return g < 1 ? 1 : (g > 1184 ? 1184 : g);
+}
+
+}  // namespace
+
+static std::atomic<unsigned long long> g_launches{0};
+void hhs_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+extern "C" uint64_t hhs_kernel_launch_count(void) { return g_launches.load(); }
+
+// Event profiler of the host-driven schedule: an event pair around each timed launch,
+// resolved when the profile is read.
+struct Profiler {
+    struct Rec {
+        int kind;
+        cudaEvent_t a, b;
+        double pairs;
+    };
+    bool on = false;
+    std::vector<Rec> pending;
+    std::vector<cudaEvent_t> pool;
+    hhs_profile acc{};
+    cudaEvent_t get() {
+        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void begin(Rec& r, int kind, double pairs, cudaStream_t s) {
+        r.kind = kind; r.pairs = pairs; r.a = get(); r.b = get();
+        cudaEventRecord(r.a, s);
+    }
+    void end(Rec& r, cudaStream_t s) {
+        cudaEventRecord(r.b, s);
+        pending.push_back(r);
+    }
+    void resolve() {
+        for (auto& r : pending) {
+            float ms = 0.f;
+            cudaEventSynchronize(r.b);
+            cudaEventElapsedTime(&ms, r.a, r.b);
+            acc.launches[r.kind] += 1;
+            acc.ms[r.kind] += ms;
+            acc.pairs[r.kind] += r.pairs;
+            pool.push_back(r.a);
+            pool.push_back(r.b);
+        }
+        pending.clear();
+    }
+    ~Profiler() {
+        resolve();
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
+extern "C" const char* hhs_status_string(hhs_status s) {
+    switch (s) {
+        case HHS_OK: return "HHS_OK";
+        case HHS_ERR_INVALID_ARG: return "HHS_ERR_INVALID_ARG";
+        case HHS_ERR_CUDA: return "HHS_ERR_CUDA";
+        case HHS_ERR_OOM: return "HHS_ERR_OOM";
+        case HHS_ERR_TIMEOUT: return "HHS_ERR_TIMEOUT";
+        case HHS_ERR_DEVICE_FAULT_FLAG: return "HHS_ERR_DEVICE_FAULT_FLAG";
+        case HHS_ERR_DEPTH: return "HHS_ERR_DEPTH";
+        case HHS_ERR_CAPACITY: return "HHS_ERR_CAPACITY";
+    }
+    return "HHS_ERR_UNKNOWN";
+}
+
+// ------------------------------------------------------------------ particle systems
+extern "C" hhs_status hhs_particle_system_alloc(hhs_particle_system* sys, int32_t n) {
+    if (!sys || n <= 0) return HHS_ERR_INVALID_ARG;
+    std::memset(sys, 0, sizeof(*sys));
+    const size_t dbl = align_up(sizeof(double) * (size_t)n);
+    const size_t acc3 = align_up(sizeof(double) * 3 * (size_t)n);
+    const size_t i32 = align_up(sizeof(int32_t) * (size_t)n);
+    const size_t total = 8 * dbl + acc3 + 2 * i32;
+    void* base = nullptr;
+    cudaError_t e = cudaMalloc(&base, total);
+    if (e != cudaSuccess) return hhs_from_cuda(e);
+    char* p = static_cast<char*>(base);
+    double** f[8] = {&sys->x, &sys->y, &sys->z, &sys->vx, &sys->vy, &sys->vz, &sys->ts, &sys->m};
+    for (int k = 0; k < 8; k++) { *f[k] = reinterpret_cast<double*>(p); p += dbl; }
+    sys->ax = reinterpret_cast<double*>(p);  // ax, ay, az contiguous: 3n doubles
+    sys->ay = sys->ax + n;
+    sys->az = sys->ax + 2 * (size_t)n;
+    p += acc3;
+    sys->id = reinterpret_cast<int32_t*>(p); p += i32;
+    sys->parent_id = reinterpret_cast<int32_t*>(p);
+    sys->n = n;
+    sys->_base = base;
+    e = cudaMemset(base, 0, total);
+    if (e != cudaSuccess) { cudaFree(base); std::memset(sys, 0, sizeof(*sys)); return hhs_from_cuda(e); }
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_particle_system_free(hhs_particle_system* sys) {
+    if (!sys) return HHS_ERR_INVALID_ARG;
+    if (sys->_base) {
+        cudaError_t e = cudaFree(sys->_base);
+        std::memset(sys, 0, sizeof(*sys));
+        if (e != cudaSuccess) return hhs_from_cuda(e);
+    }
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_particle_system_upload(hhs_particle_system* sys, int32_t n,
+                                                 const double* x, const double* y,
+                                                 const double* z, const double* vx,
+                                                 const double* vy, const double* vz,
+                                                 const double* m, const double* ts,
+                                                 const int32_t* id, void* stream) {
+    if (!sys_ok(sys) || n < 0) return HHS_ERR_INVALID_ARG;
+    if (n > sys->n) return HHS_ERR_CAPACITY;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t b = sizeof(double) * (size_t)n;
+    const double* src[8] = {x, y, z, vx, vy, vz, m, ts};
+    double* dst[8] = {sys->x, sys->y, sys->z, sys->vx, sys->vy, sys->vz, sys->m, sys->ts};
+    for (int k = 0; k < 8; k++)
+        if (src[k]) HHS_CUDA_TRY(cudaMemcpyAsync(dst[k], src[k], b, cudaMemcpyHostToDevice, s));
+    if (id) HHS_CUDA_TRY(cudaMemcpyAsync(sys->id, id, sizeof(int32_t) * (size_t)n,
+                                         cudaMemcpyHostToDevice, s));
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_particle_system_download(const hhs_particle_system* sys, int32_t n,
+                                                   double* x, double* y, double* z,
+                                                   double* vx, double* vy, double* vz,
+                                                   double* m, double* ts, int32_t* id,
+                                                   void* stream) {
+    if (!sys_ok(sys) || n < 0) return HHS_ERR_INVALID_ARG;
+    if (n > sys->n) return HHS_ERR_CAPACITY;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t b = sizeof(double) * (size_t)n;
+    double* dst[8] = {x, y, z, vx, vy, vz, m, ts};
+    const double* src[8] = {sys->x, sys->y, sys->z, sys->vx, sys->vy, sys->vz, sys->m, sys->ts};
+    for (int k = 0; k < 8; k++)
+        if (dst[k]) HHS_CUDA_TRY(cudaMemcpyAsync(dst[k], src[k], b, cudaMemcpyDeviceToHost, s));
+    if (id) HHS_CUDA_TRY(cudaMemcpyAsync(id, sys->id, sizeof(int32_t) * (size_t)n,
+                                         cudaMemcpyDeviceToHost, s));
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_particle_system_upload_aos(hhs_particle_system* sys, int32_t n,
+                                                     const double* pos3, const double* vel3,
+                                                     const double* m, const double* ts,
+                                                     const int32_t* id, void* stream) {
+    if (!sys_ok(sys) || n < 0) return HHS_ERR_INVALID_ARG;
+    if (n > sys->n) return HHS_ERR_CAPACITY;
+    if (n == 0) return HHS_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t b3 = sizeof(double) * 3 * (size_t)n;
+    if (pos3) {
+        HHS_CUDA_TRY(cudaMemcpyAsync(sys->ax, pos3, b3, cudaMemcpyHostToDevice, s));
+        k_deinterleave<<<small_grid(n), 256, 0, s>>>(sys->ax, sys->x, sys->y, sys->z, n);
+        HHS_LAUNCH_CHECK();
+    }
+    if (vel3) {
+        HHS_CUDA_TRY(cudaMemcpyAsync(sys->ax, vel3, b3, cudaMemcpyHostToDevice, s));
+        k_deinterleave<<<small_grid(n), 256, 0, s>>>(sys->ax, sys->vx, sys->vy, sys->vz, n);
+        HHS_LAUNCH_CHECK();
+    }
+    return hhs_particle_system_upload(sys, n, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                      nullptr, m, ts, id, stream);
+}
+
+extern "C" hhs_status hhs_particle_system_download_aos(const hhs_particle_system* sys,
+                                                       int32_t n, double* pos3, double* vel3,
+                                                       double* m, double* ts, int32_t* id,
+                                                       void* stream) {
+    if (!sys_ok(sys) || n < 0) return HHS_ERR_INVALID_ARG;
+    if (n > sys->n) return HHS_ERR_CAPACITY;
+    if (n == 0) return HHS_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t b3 = sizeof(double) * 3 * (size_t)n;
+    if (pos3) {
+        k_interleave<<<small_grid(n), 256, 0, s>>>(sys->ax, sys->x, sys->y, sys->z, n);
+        HHS_LAUNCH_CHECK();
+        HHS_CUDA_TRY(cudaMemcpyAsync(pos3, sys->ax, b3, cudaMemcpyDeviceToHost, s));
+    }
+    if (vel3) {
+        // a second staging round trip: the first copy must finish before reuse
+        HHS_CUDA_TRY(cudaStreamSynchronize(s));
+        k_interleave<<<small_grid(n), 256, 0, s>>>(sys->ax, sys->vx, sys->vy, sys->vz, n);
+        HHS_LAUNCH_CHECK();
+        HHS_CUDA_TRY(cudaMemcpyAsync(vel3, sys->ax, b3, cudaMemcpyDeviceToHost, s));
+    }
+    return hhs_particle_system_download(sys, n, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                        nullptr, m, ts, id, stream);
+}
+
+// ------------------------------------------------------------------ context
+namespace {
+struct CtxLayout {
+    size_t lists, counts, ws, leaf, err, stats, engine, total;
+};
+CtxLayout ctx_layout(int n_max, int max_levels) {
+    CtxLayout L;
+    L.lists = align_up(sizeof(int32_t) * (size_t)n_max * (size_t)max_levels);
+    L.counts = align_up(sizeof(hhs_partition) * (size_t)max_levels);
+    L.ws = align_up(split_workspace_bytes(n_max));
+    L.leaf = align_up(sizeof(double));
+    L.err = align_up(sizeof(unsigned));
+    L.stats = align_up(sizeof(hhs_stats));
+    L.engine = align_up(engine_workspace_bytes(n_max, max_levels));
+    L.total = 2 * L.lists + L.counts + L.ws + L.leaf + L.err + L.stats + L.engine;
+    return L;
+}
+}  // namespace
+
+extern "C" size_t hhs_workspace_size(int32_t n_max, int32_t max_levels) {
+    if (n_max <= 0 || max_levels <= 0) return 0;
+    return ctx_layout(n_max, max_levels).total;
+}
+
+extern "C" hhs_status hhs_ctx_create(int32_t n_max, int32_t max_levels, hhs_params params,
+                                     hhs_ctx** out) {
+    if (!out || n_max <= 0 || max_levels <= 0 || max_levels > 1024) return HHS_ERR_INVALID_ARG;
+    if (!(params.eta > 0.0)) return HHS_ERR_INVALID_ARG;
+    *out = nullptr;
+    hhs_ctx* c = new (std::nothrow) hhs_ctx();
+    if (!c) return HHS_ERR_OOM;
+    c->n_max = n_max;
+    c->max_levels = max_levels;
+    c->params = params;
+    cudaGetDevice(&c->device);
+    const CtxLayout L = ctx_layout(n_max, max_levels);
+    cudaError_t e = cudaMalloc(&c->arena, L.total);
+    if (e != cudaSuccess) { delete c; return hhs_from_cuda(e); }
+    c->arena_bytes = L.total;
+    e = cudaMemset(c->arena, 0, L.total);
+    if (e != cudaSuccess) { cudaFree(c->arena); delete c; return hhs_from_cuda(e); }
+    char* p = static_cast<char*>(c->arena);
+    c->fast_lists = reinterpret_cast<int32_t*>(p); p += L.lists;
+    c->slow_lists = reinterpret_cast<int32_t*>(p); p += L.lists;
+    c->counts = reinterpret_cast<hhs_partition*>(p); p += L.counts;
+    c->split_ws = p; p += L.ws;
+    c->leaf_time = reinterpret_cast<double*>(p); p += L.leaf;
+    c->err = reinterpret_cast<unsigned*>(p); p += L.err;
+    c->stats = reinterpret_cast<hhs_stats*>(p); p += L.stats;
+    c->engine = p;
+    c->engine_bytes = L.engine;
+    e = cudaMallocHost(&c->host_counts, sizeof(hhs_partition) * (size_t)max_levels);
+    if (e != cudaSuccess) { cudaFree(c->arena); delete c; return hhs_from_cuda(e); }
+    hhs_status st = engine_init(c, c->engine);
+    if (st != HHS_OK) { cudaFreeHost(c->host_counts); cudaFree(c->arena); delete c; return st; }
+    c->prof = new (std::nothrow) Profiler();
+    *out = c;
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_ctx_destroy(hhs_ctx* c) {
+    if (!c) return HHS_ERR_INVALID_ARG;
+    delete static_cast<Profiler*>(c->prof);
+    cudaError_t e1 = cudaFreeHost(c->host_counts);
+    cudaError_t e2 = cudaFree(c->arena);
+    delete c;
+    if (e1 != cudaSuccess) return hhs_from_cuda(e1);
+    return hhs_from_cuda(e2);
+}
+
+extern "C" hhs_status hhs_ctx_set_params(hhs_ctx* c, hhs_params params) {
+    if (!c || !(params.eta > 0.0)) return HHS_ERR_INVALID_ARG;
+    c->params = params;
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_ctx_get_simtime(hhs_ctx* c, double* simtime, void* stream) {
+    if (!c || !simtime) return HHS_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    HHS_CUDA_TRY(cudaMemcpyAsync(simtime, c->leaf_time, sizeof(double), cudaMemcpyDeviceToHost, s));
+    HHS_CUDA_TRY(cudaStreamSynchronize(s));
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_ctx_flush_simtime(hhs_ctx* c, void* stream) {
+    if (!c) return HHS_ERR_INVALID_ARG;
+    HHS_CUDA_TRY(cudaMemsetAsync(c->leaf_time, 0, sizeof(double), static_cast<cudaStream_t>(stream)));
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_ctx_check(hhs_ctx* c, void* stream) {
+    if (!c) return HHS_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    HHS_CUDA_TRY(cudaStreamSynchronize(s));
+    unsigned e1 = 0, e2 = 0;
+    HHS_CUDA_TRY(cudaMemcpy(&e1, c->err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    HHS_CUDA_TRY(cudaMemcpy(&e2, scan_workspace_error_word(c->split_ws), sizeof(unsigned),
+                            cudaMemcpyDeviceToHost));
+    const unsigned e = e1 | e2;
+    if (e & (HHS_ERRBIT_LOOKBACK_TIMEOUT | HHS_ERRBIT_BARRIER_TIMEOUT)) return HHS_ERR_TIMEOUT;
+    if (e & HHS_ERRBIT_DEPTH) return HHS_ERR_DEPTH;
+    if (e & HHS_ERRBIT_CAPACITY) return HHS_ERR_CAPACITY;
+    if (e) return HHS_ERR_DEVICE_FAULT_FLAG;
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_ctx_clear_errors(hhs_ctx* c, void* stream) {
+    if (!c) return HHS_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    HHS_CUDA_TRY(cudaMemsetAsync(c->err, 0, sizeof(unsigned), s));
+    HHS_CUDA_TRY(cudaMemsetAsync(scan_workspace_error_word(c->split_ws), 0, sizeof(unsigned), s));
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_ctx_get_stats(hhs_ctx* c, hhs_stats* out, void* stream) {
+    if (!c || !out) return HHS_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    HHS_CUDA_TRY(cudaMemcpyAsync(out, c->stats, sizeof(hhs_stats), cudaMemcpyDeviceToHost, s));
+    HHS_CUDA_TRY(cudaStreamSynchronize(s));
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_ctx_reset_stats(hhs_ctx* c, void* stream) {
+    if (!c) return HHS_ERR_INVALID_ARG;
+    HHS_CUDA_TRY(cudaMemsetAsync(c->stats, 0, sizeof(hhs_stats), static_cast<cudaStream_t>(stream)));
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_ctx_set_profiling(hhs_ctx* c, int32_t on) {
+    if (!c || !c->prof) return HHS_ERR_INVALID_ARG;
+    auto* p = static_cast<Profiler*>(c->prof);
+    p->resolve();
+    p->on = on != 0;
+    p->acc = hhs_profile{};
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_ctx_get_profile(hhs_ctx* c, hhs_profile* out) {
+    if (!c || !c->prof || !out) return HHS_ERR_INVALID_ARG;
+    auto* p = static_cast<Profiler*>(c->prof);
+    p->resolve();
+    *out = p->acc;
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_measure_fma_peaks(double* fp32_tflops, double* fp64_tflops,
+                                            void* stream) {
+    if (!fp32_tflops || !fp64_tflops) return HHS_ERR_INVALID_ARG;
+    return measure_fma_peaks(fp32_tflops, fp64_tflops, static_cast<cudaStream_t>(stream));
+}
+
+// ------------------------------------------------------------------ reference-shaped ops
+extern "C" hhs_status hhs_timesteps(hhs_ctx* c, hhs_particle_system* sys, int32_t n,
+                                    hhs_precision prec, void* stream) {
+    if (!c || !sys_ok(sys) || n < 0) return HHS_ERR_INVALID_ARG;
+    if (n > sys->n) return HHS_ERR_CAPACITY;
+    return launch_timesteps(soa_of(sys), nullptr, n, c->params.eta, prec,
+                            static_cast<cudaStream_t>(stream));
+}
+
+extern "C" hhs_status hhs_split(hhs_ctx* c, const hhs_particle_system* total,
+                                hhs_particle_system* slow, hhs_particle_system* fast,
+                                int32_t* predicate, int32_t* scanned_predicate, double pivot,
+                                int32_t n, hhs_partition* part, void* stream) {
+    if (!c || !sys_ok(total) || !sys_ok(slow) || !sys_ok(fast) || !part || n <= 0)
+        return HHS_ERR_INVALID_ARG;
+    if (n > total->n || n > slow->n || n > fast->n || n > c->n_max) return HHS_ERR_CAPACITY;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    hhs_status st = launch_split_list(nullptr, n, total->ts, pivot, c->fast(0), c->slow(0),
+                                      predicate, scanned_predicate, part, nullptr, 0.0, nullptr,
+                                      0, 0, c->split_ws, s);
+    if (st != HHS_OK) return st;
+    return launch_gather_split(soa_of(total), soa_of(slow), slow->parent_id, soa_of(fast),
+                               fast->parent_id, c->slow(0), c->fast(0), part, n, s);
+}
+
+extern "C" hhs_status hhs_kick_slow(hhs_particle_system* sys, double dt, double fac, int32_t n,
+                                    hhs_precision prec, void* stream) {
+    if (!sys_ok(sys) || n < 0) return HHS_ERR_INVALID_ARG;
+    if (n > sys->n) return HHS_ERR_CAPACITY;
+    const SoA P = soa_of(sys);
+    return launch_kick_pair(P, sys->ax, sys->ay, sys->az, P, n, n, fac * dt, prec,
+                            static_cast<cudaStream_t>(stream));
+}
+
+extern "C" hhs_status hhs_kick_sf(const hhs_particle_system* so_sys,
+                                  hhs_particle_system* si_sys, double dt, double fac,
+                                  int32_t n_sink, int32_t m_src, hhs_precision prec,
+                                  void* stream) {
+    if (!sys_ok(so_sys) || !sys_ok(si_sys) || n_sink < 0 || m_src < 0) return HHS_ERR_INVALID_ARG;
+    if (n_sink > si_sys->n || m_src > so_sys->n) return HHS_ERR_CAPACITY;
+    return launch_kick_pair(soa_of(si_sys), si_sys->ax, si_sys->ay, si_sys->az, soa_of(so_sys),
+                            n_sink, m_src, fac * dt, prec, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" hhs_status hhs_drift(hhs_particle_system* sys, double dt, double fac, int32_t n,
+                                void* stream) {
+    if (!sys_ok(sys) || n < 0) return HHS_ERR_INVALID_ARG;
+    if (n > sys->n) return HHS_ERR_CAPACITY;
+    return launch_drift(soa_of(sys), n, dt * fac, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" hhs_status hhs_update_system(hhs_particle_system* prev,
+                                        const hhs_particle_system* cur, int32_t n,
+                                        void* stream) {
+    if (!sys_ok(prev) || !sys_ok(cur) || n < 0) return HHS_ERR_INVALID_ARG;
+    if (n > cur->n) return HHS_ERR_CAPACITY;
+    return launch_update_system(soa_of(prev), soa_of(cur), cur->parent_id, n,
+                                static_cast<cudaStream_t>(stream));
+}
+
+// ------------------------------------------------------------------ host-driven HOLD
+// The schedule of src/hold.cuh:51-181 driven from the host: after each split the
+// partition counts are read back (the reference synchronises the device at the same
+// point, src/split.cuh:430) to decide the recursion. Level k's subsystem is the fast
+// list of level k-1 (the whole system at level 0).
+namespace {
+hhs_status hold_host(hhs_ctx* c, const SoA& P, const int32_t* S, int n, int level, double dt,
+                     bool calc, hhs_precision prec, cudaStream_t s) {
+    if (level >= c->max_levels) return HHS_ERR_DEPTH;
+    auto* prof = static_cast<Profiler*>(c->prof);
+    const bool timed = prof && prof->on;
+    Profiler::Rec rec{};
+    hhs_status st;
+    if (calc) {
+        if (timed) prof->begin(rec, 0, (double)n * (double)(n - 1), s);
+        st = launch_timesteps(P, S, n, c->params.eta, prec, s);
+        if (st != HHS_OK) return st;
+        if (timed) prof->end(rec, s);
+    }
+    int32_t* F = c->fast(level);
+    int32_t* L = c->slow(level);
+    hhs_partition* cnt = c->counts + level;
+    if (timed) prof->begin(rec, 2, 0.0, s);
+    st = launch_split_list(S, n, P.ts, dt, F, L, nullptr, nullptr, cnt, c->leaf_time, dt,
+                           c->stats, level, calc ? 1 : 0, c->split_ws, s);
+    if (st != HHS_OK) return st;
+    if (timed) prof->end(rec, s);
+    HHS_CUDA_TRY(cudaMemcpyAsync(&c->host_counts[level], cnt, sizeof(hhs_partition),
+                                 cudaMemcpyDeviceToHost, s));
+    HHS_CUDA_TRY(cudaStreamSynchronize(s));
+    const int nf = c->host_counts[level].n_fast, ns = c->host_counts[level].n_slow;
+    if (nf < 0 || ns < 0 || nf + ns != n) return HHS_ERR_DEVICE_FAULT_FLAG;
+    if (nf > 0) {
+        st = hold_host(c, P, F, nf, level + 1, dt / 2, false, prec, s);
+        if (st != HHS_OK) return st;
+    }
+    if (ns > 0) {
+        st = launch_drift_slow(P, L, cnt, ns, dt * 0.5, s);
+        if (st != HHS_OK) return st;
+        const double pairs = (double)ns * (ns - 1.0) + 2.0 * (double)ns * (double)nf;
+        if (timed) prof->begin(rec, 1, pairs, s);
+        st = launch_kick_level(P, F, L, cnt, n, dt, prec, s);
+        if (st != HHS_OK) return st;
+        if (timed) prof->end(rec, s);
+        st = launch_drift_slow(P, L, cnt, ns, dt * 0.5, s);
+        if (st != HHS_OK) return st;
+    }
+    if (nf > 0) {
+        st = hold_host(c, P, F, nf, level + 1, dt / 2, true, prec, s);
+        if (st != HHS_OK) return st;
+    }
+    return HHS_OK;
+}
+}  // namespace
+
+extern "C" hhs_status hhs_hold_step_host(hhs_ctx* c, hhs_particle_system* sys, int32_t n,
+                                         double dt, int32_t calc_timestep, hhs_precision prec,
+                                         void* stream) {
+    if (!c || !sys_ok(sys) || n <= 0 || !(dt > 0.0)) return HHS_ERR_INVALID_ARG;
+    if (n > sys->n || n > c->n_max) return HHS_ERR_CAPACITY;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    hhs_status st = hold_host(c, soa_of(sys), nullptr, n, 0, dt, calc_timestep != 0, prec, s);
+    if (st != HHS_OK) return st;
+    return hhs_ctx_check(c, stream);
+}
+
+extern "C" hhs_status hhs_hold_step(hhs_ctx* c, int32_t clevel, hhs_particle_system* sys,
+                                    int32_t n, double stime, double etime, double dt,
+                                    int32_t calc_timestep, hhs_precision prec, void* stream) {
+    (void)clevel; (void)stime; (void)etime;
+    if (!c || !sys_ok(sys) || n <= 0 || !(dt > 0.0)) return HHS_ERR_INVALID_ARG;
+    if (n > sys->n || n > c->n_max) return HHS_ERR_CAPACITY;
+    if (c->engine_bytes == 0)
+        return hhs_hold_step_host(c, sys, n, dt, calc_timestep, prec, stream);
+    return engine_hold_step(c, soa_of(sys), n, dt, calc_timestep != 0, prec,
+                            static_cast<cudaStream_t>(stream));
+}

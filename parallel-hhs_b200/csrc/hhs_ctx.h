@@ -1,0 +1,40 @@
+// hhs_ctx.h -- the library context (definition shared by the host translation units).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "hhs_common.cuh"
+
+// nbodysystem_globals<T> (src/particle_system.cuh:65-104) plus a preallocated
+// per-level arena replacing the per-call nbodysystem_buffers<T> of src/hold.cuh:56.
+// Level k holds the split of the level-k subsystem into a fast and a slow index list
+// (global particle indices, stable order); the level-(k+1) subsystem is the fast
+// list of level k, so no particle data is copied between levels.
+struct hhs_ctx {
+    int n_max = 0;
+    int max_levels = 0;
+    hhs_params params{0.03, 0.0};
+    int device = 0;
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
+    int32_t* fast_lists = nullptr;  // [max_levels][n_max]
+    int32_t* slow_lists = nullptr;  // [max_levels][n_max]
+    hhs_partition* counts = nullptr;  // [max_levels] device
+    void* split_ws = nullptr;         // self-resetting scan workspace
+    double* leaf_time = nullptr;      // device: sum of leaf dt (globals->simtime)
+    unsigned* err = nullptr;          // device error word (HHS_ERRBIT_*)
+    hhs_partition* host_counts = nullptr;  // pinned mirror for the host-driven schedule
+    hhs_stats* stats = nullptr;            // device work counters
+    void* prof = nullptr;                  // host-side event profiler (hhs_api.cu)
+    // device-resident engine state (hhs_engine.cu)
+    void* engine = nullptr;
+    size_t engine_bytes = 0;
+
+    int32_t* fast(int level) const { return fast_lists + (size_t)level * n_max; }
+    int32_t* slow(int level) const { return slow_lists + (size_t)level * n_max; }
+};
+
+// Engine entry points (hhs_engine.cu)
+size_t engine_workspace_bytes(int n_max, int max_levels);
+hhs_status engine_init(hhs_ctx* c, void* base);
+hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool calc_ts,
+                            hhs_precision prec, cudaStream_t stream);

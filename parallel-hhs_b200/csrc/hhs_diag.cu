@@ -1,0 +1,64 @@
+// hhs_diag.cu -- measured arithmetic peaks of the device (the denominators of the
+// pair kernels' roofline): a register-resident chain of fused multiply-adds on every
+// SM, 8 independent accumulators per thread to cover the pipeline latency.
+#include "hhs_common.cuh"
+#include "hhs_kernels.h"
+
+namespace {
+
+constexpr int kIters = 4096;
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_fma_chain(T* out, T a, T b) {
+    T acc[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc[k] = (T)(threadIdx.x + k);
+#pragma unroll 4
+    for (int i = 0; i < kIters; i++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) acc[k] = fma(acc[k], a, b);
+    }
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += acc[k];
+    if (s == (T)-1.2345) out[0] = s;  // keeps the chain live; never true in practice
+}
+
+template <typename T>
+hhs_status time_chain(double* tflops, T* scratch, cudaStream_t s, int sms) {
+    const int blocks = sms * 8, threads = 256;
+    cudaEvent_t e0, e1;
+    HHS_CUDA_TRY(cudaEventCreate(&e0));
+    HHS_CUDA_TRY(cudaEventCreate(&e1));
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; rep++) {
+        cudaEventRecord(e0, s);
+        k_fma_chain<T><<<blocks, threads, 0, s>>>(scratch, (T)0.999999, (T)1e-7);
+        HHS_LAUNCH_CHECK();
+        cudaEventRecord(e1, s);
+        HHS_CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0 && ms < best) best = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const double flops = 2.0 * 8.0 * kIters * (double)blocks * threads;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return HHS_OK;
+}
+
+}  // namespace
+
+hhs_status measure_fma_peaks(double* fp32_tflops, double* fp64_tflops, cudaStream_t stream) {
+    int dev = 0, sms = 0;
+    HHS_CUDA_TRY(cudaGetDevice(&dev));
+    HHS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    void* scratch = nullptr;
+    HHS_CUDA_TRY(cudaMalloc(&scratch, 64));
+    hhs_status st = time_chain<float>(fp32_tflops, static_cast<float*>(scratch), stream, sms);
+    if (st == HHS_OK)
+        st = time_chain<double>(fp64_tflops, static_cast<double*>(scratch), stream, sms);
+    cudaFree(scratch);
+    return st;
+}

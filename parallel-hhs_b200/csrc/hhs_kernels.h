@@ -1,0 +1,45 @@
+// hhs_kernels.h -- host-side launchers shared between the library's .cu files.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "hhs_internal.h"
+
+struct SoA;
+
+// ---- scan / split (hhs_scan.cu)
+size_t scan_workspace_bytes(long long n, int tile);
+size_t split_workspace_bytes(int n);
+unsigned* scan_workspace_error_word(void* ws);
+hhs_status launch_split_list(const int32_t* list_in, int n, const double* ts, double pivot,
+                             int32_t* fast_out, int32_t* slow_out, int32_t* pred_out,
+                             int32_t* scan_out, hhs_partition* counts, double* leaf_time,
+                             double dt, hhs_stats* stats, int level, int calc_ts, void* ws,
+                             cudaStream_t stream);
+
+// ---- pair kernels, drift, gathers (hhs_pairs.cu)
+// Timesteps of the subsystem given by list (identity when nullptr), min over j != i.
+hhs_status launch_timesteps(const SoA& P, const int32_t* list, int n, double eta,
+                            hhs_precision prec, cudaStream_t stream);
+// One HOLD kick of a split level: slow sinks get slow then fast sources, fast sinks get
+// slow sources; v += a*dt. Counts are read from the device (n_max bounds the grid).
+hhs_status launch_kick_level(const SoA& P, const int32_t* fast_list,
+                             const int32_t* slow_list, const hhs_partition* counts,
+                             int n_max, double dt, hhs_precision prec, cudaStream_t stream);
+// Standalone kick: sinks = sink[0..n_sink), sources = src[0..n_src); acc written.
+hhs_status launch_kick_pair(const SoA& sink, double* ax, double* ay, double* az,
+                            const SoA& src, int n_sink, int n_src, double dtfac,
+                            hhs_precision prec, cudaStream_t stream);
+// pos += vel*h for the slow part of a split level (count read from the device).
+hhs_status launch_drift_slow(const SoA& P, const int32_t* slow_list,
+                             const hhs_partition* counts, int n_max, double h,
+                             cudaStream_t stream);
+hhs_status launch_drift(const SoA& P, int n, double h, cudaStream_t stream);
+hhs_status launch_update_system(const SoA& prev, const SoA& cur, const int32_t* parent_id,
+                                int n, cudaStream_t stream);
+hhs_status launch_gather_split(const SoA& total, const SoA& slow, int32_t* slow_parent,
+                               const SoA& fast, int32_t* fast_parent,
+                               const int32_t* slow_list, const int32_t* fast_list,
+                               const hhs_partition* counts, int n_max, cudaStream_t stream);
+
+// ---- diagnostics (hhs_diag.cu)
+hhs_status measure_fma_peaks(double* fp32_tflops, double* fp64_tflops, cudaStream_t stream);

@@ -1,0 +1,120 @@
+// hhs_pairmath.cuh -- per-pair arithmetic of the timestep and kick, in two precisions.
+//
+// FP64 ("exact") forms follow the reference expressions operation by operation
+// (src/timestep.cuh:27-57, src/kick.cuh:19-30) with explicit round-to-nearest
+// intrinsics, so no multiply-add is ever contracted and results are bit-identical
+// to an IEEE binary64 evaluation on the host.
+//
+// Mixed forms take FP64 relative coordinates through a double-single split
+// (x = hi + lo, both FP32; dx = (hi_j - hi_i) + (lo_j - lo_i), where the hi
+// difference is exact for nearby particles by Sterbenz's lemma) and evaluate the
+// pair terms in FP32 with rsqrt refined by one Newton-Raphson step
+// y1 = y0 * (3 - x*y0^2) / 2.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace hhs {
+
+__device__ __forceinline__ double f64_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double f64_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double f64_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double f64_div(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double f64_sqrt(double a) { return __dsqrt_rn(a); }
+
+// Pair timestep (src/timestep.cuh:27-57), dr = x_i - x_j, dv = v_i - v_j.
+// eta_s2 = eta / M_SQRT2. Updates minval with both candidate timescales.
+__device__ __forceinline__ void ts_pair_fp64(double drx, double dry, double drz, double dvx,
+                                             double dvy, double dvz, double mi, double mj,
+                                             double eta, double eta_s2, double& minval) {
+    const double dr2 = f64_add(f64_add(f64_mul(drx, drx), f64_mul(dry, dry)), f64_mul(drz, drz));
+    const double dv2 = f64_add(f64_add(f64_mul(dvx, dvx), f64_mul(dvy, dvy)), f64_mul(dvz, dvz));
+    const double r = f64_sqrt(dr2);
+    const double vdotdr2 =
+        f64_div(f64_add(f64_add(f64_mul(dvx, drx), f64_mul(dvy, dry)), f64_mul(dvz, drz)), dr2);
+    double tau = f64_mul(f64_mul(eta_s2, r), f64_sqrt(f64_div(r, f64_add(mj, mi))));
+    double dtau = f64_mul(f64_mul(f64_mul(3.0, tau), vdotdr2), 0.5);
+    dtau = (dtau < 1.0) ? dtau : 1.0;
+    tau = f64_div(tau, f64_sub(1.0, f64_mul(dtau, 0.5)));
+    if (tau < minval) minval = tau;
+    tau = f64_div(f64_mul(eta, r), f64_sqrt(dv2));
+    dtau = f64_mul(f64_mul(tau, vdotdr2), f64_add(1.0, f64_div(f64_add(mi, mj), f64_mul(dv2, r))));
+    dtau = (dtau < 1.0) ? dtau : 1.0;
+    tau = f64_div(tau, f64_sub(1.0, f64_mul(dtau, 0.5)));
+    if (tau < minval) minval = tau;
+}
+
+// Pair acceleration (src/kick.cuh:19-30 with the attractive sign of
+// tests/test_nbforce.cu:14-18): dx = x_j - x_i, skip d2 == 0, a += dx * (m_j/(d2*d)).
+__device__ __forceinline__ void kick_pair_fp64(double dx, double dy, double dz, double mj,
+                                               double& ax, double& ay, double& az) {
+    const double d2 = f64_add(f64_add(f64_mul(dx, dx), f64_mul(dy, dy)), f64_mul(dz, dz));
+    if (d2 == 0.0) return;
+    const double d = f64_sqrt(d2);
+    const double s = f64_mul(mj, f64_div(1.0, f64_mul(d2, d)));
+    ax = f64_add(ax, f64_mul(dx, s));
+    ay = f64_add(ay, f64_mul(dy, s));
+    az = f64_add(az, f64_mul(dz, s));
+}
+
+// ---- mixed precision -------------------------------------------------------------
+
+struct DS {  // double-single: value = hi + lo
+    float hi, lo;
+};
+
+__device__ __forceinline__ DS ds_split(double v) {
+    DS r;
+    r.hi = __double2float_rn(v);
+    r.lo = __double2float_rn(v - (double)r.hi);
+    return r;
+}
+
+// (a - b) of two double-single numbers, rounded to FP32
+__device__ __forceinline__ float ds_diff(float ahi, float alo, float bhi, float blo) {
+    return __fadd_rn(__fsub_rn(ahi, bhi), __fsub_rn(alo, blo));
+}
+
+__device__ __forceinline__ float rsqrt_nr(float x) {
+    const float y = rsqrtf(x);
+    return y * fmaf(-0.5f * x, y * y, 1.5f);
+}
+
+// Kahan-compensated accumulation s += t (c holds the running compensation).
+__device__ __forceinline__ void kahan_add(float& s, float& c, float t) {
+    const float y = __fsub_rn(t, c);
+    const float u = __fadd_rn(s, y);
+    c = __fsub_rn(__fsub_rn(u, s), y);
+    s = u;
+}
+
+// Pair timestep as a rate (1/tau) in FP32; min over tau == max over rates.
+// Free-fall: rate0 = sqrt(M/r^3)/eta_s2; the reference's correction
+// tau/(1 - dtau/2) with dtau = 1.5*tau0*vdotdr2 clamped at 1 becomes
+// rate0 - 0.75*vdotdr2 (or rate0/2 when clamped). Fly-by: rate0 = |dv|/(eta*r),
+// dtau = vdotdr2*(1 + M/(dv2*r))/rate0, likewise. dr2 == 0 gives +inf (tau = 0 in
+// the reference); dv2 == 0 gives a fly-by rate of 0 (tau = inf).
+__device__ __forceinline__ float ts_pair_rate_mixed(float drx, float dry, float drz, float dvx,
+                                                    float dvy, float dvz, float msum,
+                                                    float inv_eta_s2, float inv_eta) {
+    const float dr2 = fmaf(drx, drx, fmaf(dry, dry, drz * drz));
+    const float dv2 = fmaf(dvx, dvx, fmaf(dvy, dvy, dvz * dvz));
+    const float rdv = fmaf(drx, dvx, fmaf(dry, dvy, drz * dvz));
+    if (dr2 == 0.0f) return __int_as_float(0x7f800000);
+    const float rinv = rsqrt_nr(dr2);
+    const float rinv2 = rinv * rinv;
+    const float vdr = rdv * rinv2;
+    const float u = msum * rinv2 * rinv;
+    const float r0 = u * rsqrt_nr(u) * inv_eta_s2;
+    const float b0 = 1.5f * vdr;
+    const float rate_ff = (b0 < r0) ? fmaf(-0.5f, b0, r0) : 0.5f * r0;
+    float rate_fb = 0.0f;
+    if (dv2 > 0.0f) {
+        const float q = rsqrt_nr(dv2);
+        const float r1 = dv2 * q * rinv * inv_eta;
+        const float b1 = vdr * fmaf(msum * rinv, q * q, 1.0f);
+        rate_fb = (b1 < r1) ? fmaf(-0.5f, b1, r1) : 0.5f * r1;
+    }
+    return fmaxf(rate_ff, rate_fb);
+}
+
+}  // namespace hhs

@@ -1,0 +1,210 @@
+// hhs_scan.cu -- standalone exact exclusive scan and the fast/slow index split.
+#include "hhs_scan.cuh"
+#include "hhs_kernels.h"
+
+namespace {
+
+constexpr int kScanBlock = 256;
+constexpr int kScanItems = 16;  // 4096 values (16 KiB) per tile
+using ScanT = TileScan<kScanBlock, kScanItems>;
+
+// Exclusive scan of int32 values. VEC: 16-byte aligned input/output, so full chunks
+// move with one 128-bit streaming load/store per lane.
+template <bool VEC>
+__global__ void __launch_bounds__(kScanBlock)
+    k_scan_exclusive_i32(const int32_t* __restrict__ in, int32_t* __restrict__ out,
+                         long long n, ScanHeader* hdr, unsigned long long* status,
+                         int num_tiles) {
+    __shared__ int s_tile;
+    __shared__ unsigned s_epoch, s_prefix;
+    __shared__ unsigned s_warp[ScanT::WARPS];
+    __shared__ int s_last;
+    scan_begin(hdr, &s_tile, &s_epoch);
+    const int tile = s_tile;
+    const unsigned epoch = s_epoch;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long tbase = (long long)tile * ScanT::TILE;
+
+    unsigned v[kScanItems], ex[kScanItems];
+#pragma unroll
+    for (int c = 0; c < ScanT::CHUNKS; c++) {
+        const long long e = tbase + ScanT::offset(warp, c, lane);
+        if (VEC && e + 4 <= n) {
+            const int4 q = __ldcs(reinterpret_cast<const int4*>(in + e));
+            v[4 * c] = q.x; v[4 * c + 1] = q.y; v[4 * c + 2] = q.z; v[4 * c + 3] = q.w;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) v[4 * c + k] = (e + k < n) ? (unsigned)in[e + k] : 0u;
+        }
+    }
+    ScanT::scan(v, ex, status, tile, epoch, &hdr->error, s_warp, &s_prefix);
+#pragma unroll
+    for (int c = 0; c < ScanT::CHUNKS; c++) {
+        const long long e = tbase + ScanT::offset(warp, c, lane);
+        if (VEC && e + 4 <= n) {
+            __stcs(reinterpret_cast<int4*>(out + e),
+                   make_int4((int)ex[4 * c], (int)ex[4 * c + 1], (int)ex[4 * c + 2],
+                             (int)ex[4 * c + 3]));
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (e + k < n) out[e + k] = (int)ex[4 * c + k];
+        }
+    }
+    if (scan_finish_is_last(hdr, num_tiles, &s_last)) scan_reset(hdr, epoch);
+}
+
+constexpr int kSplitBlock = 256;
+constexpr int kSplitItems = 8;  // 2048 particles per tile
+using SplitT = TileScan<kSplitBlock, kSplitItems>;
+
+// Fast/slow split of a list of particle indices (identity when list_in == nullptr):
+// pred = ts[g] <= pivot (src/split.cuh:114-116); fast g -> fast_out[scan],
+// slow g -> slow_out[i - scan] (src/split.cuh:335-357). The last CTA applies the
+// N_fast == 1 fold (lone fast particle appended as slow_out[n-1]) and writes the
+// partition counts; with leaf_time set it also adds dt there when N_fast == 0
+// (globals->simtime, src/hold.cuh:106-114).
+__global__ void __launch_bounds__(kSplitBlock)
+    k_split_list(const int32_t* __restrict__ list_in, int n, const double* __restrict__ ts,
+                 double pivot, int32_t* __restrict__ fast_out, int32_t* __restrict__ slow_out,
+                 int32_t* __restrict__ pred_out, int32_t* __restrict__ scan_out,
+                 hhs_partition* counts, double* leaf_time, double dt, hhs_stats* stats,
+                 int level, int calc_ts, ScanHeader* hdr, unsigned long long* status,
+                 int num_tiles) {
+    __shared__ int s_tile;
+    __shared__ unsigned s_epoch, s_prefix;
+    __shared__ unsigned s_warp[SplitT::WARPS];
+    __shared__ int s_last;
+    scan_begin(hdr, &s_tile, &s_epoch);
+    const int tile = s_tile;
+    const unsigned epoch = s_epoch;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long tbase = (long long)tile * SplitT::TILE;
+
+    unsigned v[kSplitItems], ex[kSplitItems];
+    int g[kSplitItems];
+#pragma unroll
+    for (int c = 0; c < SplitT::CHUNKS; c++) {
+        const long long e = tbase + SplitT::offset(warp, c, lane);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const long long i = e + k;
+            if (i < n) {
+                const int gi = list_in ? list_in[i] : (int)i;
+                g[4 * c + k] = gi;
+                v[4 * c + k] = ts[gi] <= pivot ? 1u : 0u;
+            } else {
+                g[4 * c + k] = -1;
+                v[4 * c + k] = 0u;
+            }
+        }
+    }
+    SplitT::scan(v, ex, status, tile, epoch, &hdr->error, s_warp, &s_prefix);
+#pragma unroll
+    for (int c = 0; c < SplitT::CHUNKS; c++) {
+        const long long e = tbase + SplitT::offset(warp, c, lane);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const long long i = e + k;
+            if (i < n) {
+                const unsigned p = ex[4 * c + k];
+                if (v[4 * c + k]) fast_out[p] = g[4 * c + k];
+                else slow_out[i - p] = g[4 * c + k];
+                if (pred_out) pred_out[i] = (int)v[4 * c + k];
+                if (scan_out) scan_out[i] = (int)p;
+            }
+        }
+    }
+    if (scan_finish_is_last(hdr, num_tiles, &s_last)) {
+        if (threadIdx.x == 0) {
+            const unsigned long long s =
+                ld_relaxed_u64(&status[num_tiles - 1]);  // inclusive total of the last tile
+            int nf = (int)(unsigned)s;
+            if (nf == 1) {
+                slow_out[n - 1] = fast_out[0];
+                nf = 0;
+            }
+            counts->n_fast = nf;
+            counts->n_slow = n - nf;
+            if (leaf_time && nf == 0) *leaf_time += dt;
+            if (stats) {
+                const double ns = (double)(n - nf), nfd = (double)nf;
+                stats->nodes += 1;
+                if (level > stats->max_level) stats->max_level = level;
+                stats->kick_pairs += ns * (ns - 1.0) + 2.0 * ns * nfd;
+                if (calc_ts) stats->ts_pairs += (double)n * (double)(n - 1);
+            }
+        }
+        scan_reset(hdr, epoch);
+    }
+}
+
+}  // namespace
+
+size_t scan_workspace_bytes(long long n, int tile) {
+    const long long tiles = (n + tile - 1) / tile;
+    return sizeof(ScanHeader) + (size_t)(tiles > 0 ? tiles : 1) * sizeof(unsigned long long);
+}
+
+size_t split_workspace_bytes(int n) { return scan_workspace_bytes(n, SplitT::TILE); }
+
+hhs_status launch_split_list(const int32_t* list_in, int n, const double* ts, double pivot,
+                             int32_t* fast_out, int32_t* slow_out, int32_t* pred_out,
+                             int32_t* scan_out, hhs_partition* counts, double* leaf_time,
+                             double dt, hhs_stats* stats, int level, int calc_ts, void* ws,
+                             cudaStream_t stream) {
+    if (n <= 0) return HHS_ERR_INVALID_ARG;
+    const int tiles = (n + SplitT::TILE - 1) / SplitT::TILE;
+    auto* hdr = static_cast<ScanHeader*>(ws);
+    auto* status = reinterpret_cast<unsigned long long*>(static_cast<char*>(ws) +
+                                                         sizeof(ScanHeader));
+    k_split_list<<<tiles, kSplitBlock, 0, stream>>>(list_in, n, ts, pivot, fast_out, slow_out,
+                                                    pred_out, scan_out, counts, leaf_time, dt,
+                                                    stats, level, calc_ts, hdr, status, tiles);
+    HHS_LAUNCH_CHECK();
+    return HHS_OK;
+}
+
+unsigned* scan_workspace_error_word(void* ws) { return &static_cast<ScanHeader*>(ws)->error; }
+
+extern "C" size_t hhs_scan_workspace_size(int64_t n) {
+    return scan_workspace_bytes(n, ScanT::TILE);
+}
+
+extern "C" hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out, int64_t n,
+                                             void* d_workspace, size_t workspace_bytes,
+                                             void* stream) {
+    if (n < 0 || (n > 0 && (!d_in || !d_out || !d_workspace))) return HHS_ERR_INVALID_ARG;
+    if (n == 0) return HHS_OK;
+    if (n > (int64_t)0x7fffffff) return HHS_ERR_INVALID_ARG;
+    if (workspace_bytes < hhs_scan_workspace_size(n)) return HHS_ERR_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(d_workspace) & 7u) != 0) return HHS_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int tiles = (int)((n + ScanT::TILE - 1) / ScanT::TILE);
+    const size_t used = scan_workspace_bytes(n, ScanT::TILE);
+    HHS_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, used, s));
+    auto* hdr = static_cast<ScanHeader*>(d_workspace);
+    auto* status = reinterpret_cast<unsigned long long*>(static_cast<char*>(d_workspace) +
+                                                         sizeof(ScanHeader));
+    const bool vec = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) &
+                      15u) == 0;
+    if (vec)
+        k_scan_exclusive_i32<true><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n, hdr, status,
+                                                                tiles);
+    else
+        k_scan_exclusive_i32<false><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n, hdr, status,
+                                                                 tiles);
+    HHS_LAUNCH_CHECK();
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_scan_workspace_status(const void* d_workspace, void* stream) {
+    if (!d_workspace) return HHS_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    HHS_CUDA_TRY(cudaStreamSynchronize(s));
+    unsigned err = 0;
+    HHS_CUDA_TRY(cudaMemcpy(&err, &static_cast<const ScanHeader*>(d_workspace)->error,
+                            sizeof(err), cudaMemcpyDeviceToHost));
+    if (err & HHS_ERRBIT_LOOKBACK_TIMEOUT) return HHS_ERR_TIMEOUT;
+    return err ? HHS_ERR_DEVICE_FAULT_FLAG : HHS_OK;
+}

@@ -1,0 +1,172 @@
+// hhs_scan.cuh -- single-pass exclusive scan (decoupled look-back) used by the
+// standalone int32 scan and by the fast/slow split.
+//
+// The reference computes the same exact exclusive prefix sum with a multi-level
+// Blelloch tree scan: per-block up/down-sweep in shared memory, block sums scanned
+// recursively, and "add" kernels that fix up block offsets and the remainder
+// (src/split.cuh:64-102,131-302,372-394,438-565; 3-6 launches and two cudaMalloc /
+// cudaFree pairs per call). Here one launch does it: each CTA scans its tile in
+// registers with warp shuffles, then obtains its exclusive prefix by the
+// decoupled look-back of Merrill & Garland (2016, "Single-pass Parallel Prefix Scan
+// with Decoupled Look-back"), and the last CTA to finish resets the workspace so
+// the next call needs no memset.
+#pragma once
+#include "hhs_common.cuh"
+
+// Workspace: a 256-byte header followed by one 64-bit status word per tile.
+struct ScanHeader {
+    unsigned tile_counter;  // dynamic tile index (tiles start in index order)
+    unsigned done_counter;  // CTAs that finished; the last one resets the header
+    unsigned epoch;         // status words of other epochs read as "not ready"
+    unsigned error;         // HHS_ERRBIT_* set by timed-out waits
+    unsigned pad[60];
+};
+static_assert(sizeof(ScanHeader) == 256, "scan header must stay 256 bytes");
+
+// status word: [63:34] epoch, [33:32] flag (0 none, 1 aggregate, 2 inclusive), [31:0] value
+__device__ __forceinline__ unsigned long long scan_pack(unsigned epoch, unsigned flag,
+                                                        unsigned value) {
+    return ((unsigned long long)epoch << 34) | ((unsigned long long)flag << 32) | value;
+}
+
+__device__ __forceinline__ unsigned scan_next_epoch(const ScanHeader* h) {
+    unsigned e = (*(volatile const unsigned*)&h->epoch + 1u) & 0x3fffffffu;
+    return e ? e : 1u;
+}
+
+// Called by one full warp. Publishes this tile's aggregate, walks predecessors in
+// windows of 32, and publishes the inclusive prefix. Returns the exclusive prefix.
+__device__ __forceinline__ unsigned scan_lookback(unsigned long long* status, int tile,
+                                                  unsigned aggregate, unsigned epoch,
+                                                  unsigned* err) {
+    const int lane = threadIdx.x & 31;
+    if (tile == 0) {
+        if (lane == 0) st_relaxed_u64(&status[0], scan_pack(epoch, 2u, aggregate));
+        return 0u;
+    }
+    if (lane == 0) st_relaxed_u64(&status[tile], scan_pack(epoch, 1u, aggregate));
+    unsigned excl = 0u;
+    int pred = tile - 1;
+    unsigned spins = 0;
+    while (true) {
+        const int idx = pred - lane;
+        unsigned long long s = 0ull;
+        unsigned flag;
+        while (true) {
+            if (idx >= 0) {
+                s = ld_relaxed_u64(&status[idx]);
+                flag = ((unsigned)(s >> 34) == epoch) ? (unsigned)(s >> 32) & 3u : 0u;
+            } else {
+                flag = 2u;  // virtual tile -1: inclusive prefix 0
+                s = 0ull;
+            }
+            if (__all_sync(HHS_FULL_MASK, flag != 0u)) break;
+            if (++spins > HHS_SPIN_LIMIT) {
+                if (lane == 0) atomicOr(err, HHS_ERRBIT_LOOKBACK_TIMEOUT);
+                if (flag == 0u) { flag = 2u; s = 0ull; }
+                break;
+            }
+            __nanosleep(64);
+        }
+        unsigned val = (idx >= 0) ? (unsigned)s : 0u;
+        const unsigned pm = __ballot_sync(HHS_FULL_MASK, flag == 2u);
+        if (pm) {
+            const int first = __ffs(pm) - 1;
+            excl += (unsigned)warp_sum((int)(lane <= first ? val : 0u));
+            break;
+        }
+        excl += (unsigned)warp_sum((int)val);
+        pred -= 32;
+    }
+    if (lane == 0) st_relaxed_u64(&status[tile], scan_pack(epoch, 2u, excl + aggregate));
+    return excl;
+}
+
+// Tile layout shared by the scan kernels: BLOCK threads x ITEMS values; value k of
+// chunk c of lane l in warp w sits at tile offset w*32*ITEMS + c*128 + l*4 + k, so a
+// warp's chunk is 128 consecutive values (one 16-byte load per lane).
+template <int BLOCK, int ITEMS>
+struct TileScan {
+    static constexpr int TILE = BLOCK * ITEMS;
+    static constexpr int CHUNKS = ITEMS / 4;
+    static constexpr int WARPS = BLOCK / 32;
+    static_assert(ITEMS % 4 == 0, "ITEMS must be a multiple of 4");
+
+    __device__ static __forceinline__ long long offset(int warp, int c, int lane) {
+        return (long long)warp * (32 * ITEMS) + c * 128 + lane * 4;
+    }
+
+    // v: this thread's values. On return excl[k] holds each value's exclusive prefix
+    // within the whole input (tile prefix from the look-back included).
+    __device__ static __forceinline__ void scan(const unsigned (&v)[ITEMS],
+                                                unsigned (&excl)[ITEMS],
+                                                unsigned long long* status, int tile,
+                                                unsigned epoch, unsigned* err,
+                                                unsigned* s_warp, unsigned* s_prefix) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        unsigned cx[CHUNKS];
+        unsigned run = 0u;
+#pragma unroll
+        for (int c = 0; c < CHUNKS; c++) {
+            const unsigned s = v[4 * c] + v[4 * c + 1] + v[4 * c + 2] + v[4 * c + 3];
+            const unsigned inc = (unsigned)warp_incl_scan((int)s, lane);
+            cx[c] = run + inc - s;
+            run += (unsigned)__shfl_sync(HHS_FULL_MASK, (int)inc, 31);
+        }
+        if (lane == 0) s_warp[warp] = run;
+        __syncthreads();
+        if (warp == 0) {
+            const unsigned wt = (lane < WARPS) ? s_warp[lane] : 0u;
+            const unsigned wi = (unsigned)warp_incl_scan((int)wt, lane);
+            const unsigned total = (unsigned)__shfl_sync(HHS_FULL_MASK, (int)wi, 31);
+            const unsigned prefix = scan_lookback(status, tile, total, epoch, err);
+            if (lane < WARPS) s_warp[lane] = wi - wt;
+            if (lane == 0) *s_prefix = prefix;
+        }
+        __syncthreads();
+        const unsigned base = *s_prefix + s_warp[warp];
+#pragma unroll
+        for (int c = 0; c < CHUNKS; c++) {
+            unsigned p = base + cx[c];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                excl[4 * c + k] = p;
+                p += v[4 * c + k];
+            }
+        }
+    }
+};
+
+// Fetches this CTA's tile index and the call's epoch (thread 0), broadcast to all.
+__device__ __forceinline__ void scan_begin(ScanHeader* hdr, int* s_tile, unsigned* s_epoch) {
+    if (threadIdx.x == 0) {
+        *s_tile = (int)atomicAdd(&hdr->tile_counter, 1u);
+        *s_epoch = scan_next_epoch(hdr);
+    }
+    __syncthreads();
+}
+
+// Marks this CTA done; returns true (in every thread) for the last CTA to finish,
+// whose view of all other CTAs' global writes is then complete.
+__device__ __forceinline__ bool scan_finish_is_last(ScanHeader* hdr, int num_tiles,
+                                                    int* s_flag) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned prev = atomicAdd(&hdr->done_counter, 1u);
+        *s_flag = (prev == (unsigned)num_tiles - 1u);
+    }
+    __syncthreads();
+    const bool last = *s_flag != 0;
+    if (last) __threadfence();
+    return last;
+}
+
+// Resets the header for the next call (last CTA only, after its final reads).
+__device__ __forceinline__ void scan_reset(ScanHeader* hdr, unsigned epoch) {
+    if (threadIdx.x == 0) {
+        hdr->tile_counter = 0u;
+        hdr->done_counter = 0u;
+        hdr->epoch = epoch;
+    }
+}

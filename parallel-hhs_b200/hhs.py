@@ -1,0 +1,327 @@
+"""Python host binding of libhhs_b200.so (the C ABI declared in include/hhs.h).
+
+Mirrors the reference's host-side operator interface (src/hold.cuh, src/timestep.cuh,
+src/split.cuh, src/kick.cuh, src/drift.cuh, src/update_system.cuh): a device
+ParticleSystem, a Context (the reference's nbodysystem_globals plus a per-level arena)
+and the timesteps / split / kick_slow / kick_sf / drift / update_system / hold_step
+entry points. Errors raise HHSError carrying the library status instead of exiting.
+
+The CUDA library is required: importing this module fails loudly if it is missing.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhhs_b200.so")
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+MASS_EQUAL, MASS_SALPETER, MASS_TWO_COMPONENT = 0, 1, 2
+
+STATUS = {0: "HHS_OK", 1: "HHS_ERR_INVALID_ARG", 2: "HHS_ERR_CUDA", 3: "HHS_ERR_OOM",
+          4: "HHS_ERR_TIMEOUT", 5: "HHS_ERR_DEVICE_FAULT_FLAG", 6: "HHS_ERR_DEPTH",
+          7: "HHS_ERR_CAPACITY"}
+
+
+class HHSError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        super().__init__(f"{what}: {STATUS.get(status, status)}")
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+_vp = ctypes.c_void_p
+
+
+class Partition(ctypes.Structure):
+    _fields_ = [("n_slow", ctypes.c_int32), ("n_fast", ctypes.c_int32)]
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("eta", ctypes.c_double), ("eps", ctypes.c_double)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.c_uint64), ("max_level", ctypes.c_int32),
+                ("_pad", ctypes.c_int32), ("kick_pairs", ctypes.c_double),
+                ("ts_pairs", ctypes.c_double)]
+
+
+class Profile(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_uint64 * 8), ("ms", ctypes.c_double * 8),
+                ("pairs", ctypes.c_double * 8)]
+
+
+PROFILE_KINDS = ("timesteps", "kick", "split", "drift", "engine", "k5", "k6", "k7")
+
+
+class CParticleSystem(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32)] + \
+        [(k, _dp) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "ts", "m")] + \
+        [("id", _ip), ("parent_id", _ip), ("_base", _vp)]
+
+
+# every symbol of include/hhs.h, with its ctypes signature (restype, argtypes)
+SIGNATURES = {
+    "hhs_particle_system_alloc": (ctypes.c_int, [ctypes.POINTER(CParticleSystem), ctypes.c_int32]),
+    "hhs_particle_system_free": (ctypes.c_int, [ctypes.POINTER(CParticleSystem)]),
+    "hhs_particle_system_upload": (ctypes.c_int, [ctypes.POINTER(CParticleSystem), ctypes.c_int32]
+                                   + [_dp] * 8 + [_ip, _vp]),
+    "hhs_particle_system_download": (ctypes.c_int, [ctypes.POINTER(CParticleSystem),
+                                                    ctypes.c_int32] + [_dp] * 8 + [_ip, _vp]),
+    "hhs_particle_system_upload_aos": (ctypes.c_int, [ctypes.POINTER(CParticleSystem),
+                                                      ctypes.c_int32] + [_dp] * 4 + [_ip, _vp]),
+    "hhs_particle_system_download_aos": (ctypes.c_int, [ctypes.POINTER(CParticleSystem),
+                                                        ctypes.c_int32] + [_dp] * 4 + [_ip, _vp]),
+    "hhs_workspace_size": (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
+    "hhs_ctx_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, Params,
+                                      ctypes.POINTER(_vp)]),
+    "hhs_ctx_destroy": (ctypes.c_int, [_vp]),
+    "hhs_ctx_set_params": (ctypes.c_int, [_vp, Params]),
+    "hhs_ctx_get_simtime": (ctypes.c_int, [_vp, _dp, _vp]),
+    "hhs_ctx_flush_simtime": (ctypes.c_int, [_vp, _vp]),
+    "hhs_ctx_check": (ctypes.c_int, [_vp, _vp]),
+    "hhs_ctx_clear_errors": (ctypes.c_int, [_vp, _vp]),
+    "hhs_timesteps": (ctypes.c_int, [_vp, ctypes.POINTER(CParticleSystem), ctypes.c_int32,
+                                     ctypes.c_int, _vp]),
+    "hhs_split": (ctypes.c_int, [_vp, ctypes.POINTER(CParticleSystem),
+                                 ctypes.POINTER(CParticleSystem), ctypes.POINTER(CParticleSystem),
+                                 _vp, _vp, ctypes.c_double, ctypes.c_int32, _vp, _vp]),
+    "hhs_kick_slow": (ctypes.c_int, [ctypes.POINTER(CParticleSystem), ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_int32, ctypes.c_int, _vp]),
+    "hhs_kick_sf": (ctypes.c_int, [ctypes.POINTER(CParticleSystem),
+                                   ctypes.POINTER(CParticleSystem), ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_int32, ctypes.c_int32,
+                                   ctypes.c_int, _vp]),
+    "hhs_drift": (ctypes.c_int, [ctypes.POINTER(CParticleSystem), ctypes.c_double,
+                                 ctypes.c_double, ctypes.c_int32, _vp]),
+    "hhs_update_system": (ctypes.c_int, [ctypes.POINTER(CParticleSystem),
+                                         ctypes.POINTER(CParticleSystem), ctypes.c_int32, _vp]),
+    "hhs_hold_step": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.POINTER(CParticleSystem),
+                                     ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_int32, ctypes.c_int, _vp]),
+    "hhs_hold_step_host": (ctypes.c_int, [_vp, ctypes.POINTER(CParticleSystem), ctypes.c_int32,
+                                          ctypes.c_double, ctypes.c_int32, ctypes.c_int, _vp]),
+    "hhs_scan_workspace_size": (ctypes.c_size_t, [ctypes.c_int64]),
+    "hhs_scan_exclusive_i32": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp, ctypes.c_size_t,
+                                              _vp]),
+    "hhs_scan_workspace_status": (ctypes.c_int, [_vp, _vp]),
+    "hhs_ic_plummer": (ctypes.c_int, [ctypes.c_int32, ctypes.c_uint64, ctypes.c_int32]
+                       + [_dp] * 7),
+    "hhs_host_potential_energy": (ctypes.c_double, [ctypes.c_int32] + [_dp] * 4),
+    "hhs_host_kinetic_energy": (ctypes.c_double, [ctypes.c_int32] + [_dp] * 4),
+    "hhs_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "hhs_ctx_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(Stats), _vp]),
+    "hhs_ctx_reset_stats": (ctypes.c_int, [_vp, _vp]),
+    "hhs_ctx_set_profiling": (ctypes.c_int, [_vp, ctypes.c_int32]),
+    "hhs_ctx_get_profile": (ctypes.c_int, [_vp, ctypes.POINTER(Profile)]),
+    "hhs_kernel_launch_count": (ctypes.c_uint64, []),
+    "hhs_measure_fma_peaks": (ctypes.c_int, [_dp, _dp, _vp]),
+}
+
+_lib = None
+
+
+def lib():
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run __graft_entry__.build() first")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(status, what):
+    if status != 0:
+        raise HHSError(status, what)
+
+
+def _d(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    if a is None:
+        return None
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_ip)
+
+
+FIELDS = ("x", "y", "z", "vx", "vy", "vz", "m", "ts")
+
+
+def plummer(n, seed, mass_spectrum=MASS_EQUAL):
+    """Seeded Plummer sphere in Henon units (host arrays, dict of float64)."""
+    s = {k: np.empty(n) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    _check(lib().hhs_ic_plummer(n, seed, mass_spectrum,
+                                *[_d(s[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")]),
+           "hhs_ic_plummer")
+    s["ts"] = np.zeros(n)
+    s["id"] = np.arange(n, dtype=np.int32)
+    return s
+
+
+def energy_host(s):
+    n = len(s["x"])
+    k = lib().hhs_host_kinetic_energy(n, _d(s["vx"]), _d(s["vy"]), _d(s["vz"]), _d(s["m"]))
+    p = lib().hhs_host_potential_energy(n, _d(s["x"]), _d(s["y"]), _d(s["z"]), _d(s["m"]))
+    return k + p
+
+
+class ParticleSystem:
+    """particle_system<double> on the device (src/particle_system.cuh:20-54), SoA."""
+
+    def __init__(self, n):
+        self.c = CParticleSystem()
+        _check(lib().hhs_particle_system_alloc(ctypes.byref(self.c), n), "alloc")
+        self.n = n
+
+    @property
+    def ref(self):
+        return ctypes.byref(self.c)
+
+    def upload(self, s, n=None, stream=None):
+        n = len(s["x"]) if n is None else n
+        _check(lib().hhs_particle_system_upload(self.ref, n, *[_d(s.get(k)) for k in FIELDS],
+                                                _i(s.get("id")), stream), "upload")
+
+    def download(self, n=None, stream=None, fields=FIELDS + ("id",)):
+        n = self.n if n is None else n
+        out = {k: np.empty(n) for k in FIELDS if k in fields}
+        if "id" in fields:
+            out["id"] = np.empty(n, dtype=np.int32)
+        _check(lib().hhs_particle_system_download(self.ref, n, *[_d(out.get(k)) for k in FIELDS],
+                                                  _i(out.get("id")), stream), "download")
+        return out
+
+    def free(self):
+        if self.c._base:
+            _check(lib().hhs_particle_system_free(self.ref), "free")
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Context:
+    """nbodysystem_globals<double> plus the per-level arena (src/particle_system.cuh:65-104)."""
+
+    def __init__(self, n_max, max_levels=64, eta=0.03, eps=0.0):
+        self.h = _vp()
+        _check(lib().hhs_ctx_create(n_max, max_levels, Params(eta, eps), ctypes.byref(self.h)),
+               "hhs_ctx_create")
+
+    def check(self, stream=None):
+        _check(lib().hhs_ctx_check(self.h, stream), "hhs_ctx_check")
+
+    def simtime(self, stream=None):
+        t = ctypes.c_double(0)
+        _check(lib().hhs_ctx_get_simtime(self.h, ctypes.byref(t), stream), "simtime")
+        return t.value
+
+    def flush_simtime(self, stream=None):
+        _check(lib().hhs_ctx_flush_simtime(self.h, stream), "flush_simtime")
+
+    def stats(self, stream=None):
+        st = Stats()
+        _check(lib().hhs_ctx_get_stats(self.h, ctypes.byref(st), stream), "stats")
+        return {"nodes": st.nodes, "max_level": st.max_level, "kick_pairs": st.kick_pairs,
+                "ts_pairs": st.ts_pairs}
+
+    def reset_stats(self, stream=None):
+        _check(lib().hhs_ctx_reset_stats(self.h, stream), "reset_stats")
+
+    def set_profiling(self, on):
+        _check(lib().hhs_ctx_set_profiling(self.h, int(on)), "set_profiling")
+
+    def profile(self):
+        p = Profile()
+        _check(lib().hhs_ctx_get_profile(self.h, ctypes.byref(p)), "profile")
+        return {PROFILE_KINDS[k]: {"launches": p.launches[k], "ms": p.ms[k], "pairs": p.pairs[k]}
+                for k in range(8) if p.launches[k]}
+
+    def destroy(self):
+        if self.h:
+            _check(lib().hhs_ctx_destroy(self.h), "hhs_ctx_destroy")
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def timesteps(ctx, sys, n, prec=PREC_FP64, stream=None):
+    _check(lib().hhs_timesteps(ctx.h, sys.ref, n, prec, stream), "hhs_timesteps")
+
+
+def split(ctx, total, slow, fast, pivot, n, part_ptr, pred_ptr=None, scan_ptr=None, stream=None):
+    _check(lib().hhs_split(ctx.h, total.ref, slow.ref, fast.ref, pred_ptr, scan_ptr, pivot, n,
+                           part_ptr, stream), "hhs_split")
+
+
+def kick_slow(sys, dt, fac, n, prec=PREC_FP64, stream=None):
+    _check(lib().hhs_kick_slow(sys.ref, dt, fac, n, prec, stream), "hhs_kick_slow")
+
+
+def kick_sf(so_sys, si_sys, dt, fac, n_sink, m_src, prec=PREC_FP64, stream=None):
+    _check(lib().hhs_kick_sf(so_sys.ref, si_sys.ref, dt, fac, n_sink, m_src, prec, stream),
+           "hhs_kick_sf")
+
+
+def drift(sys, dt, fac, n, stream=None):
+    _check(lib().hhs_drift(sys.ref, dt, fac, n, stream), "hhs_drift")
+
+
+def update_system(prev, cur, n, stream=None):
+    _check(lib().hhs_update_system(prev.ref, cur.ref, n, stream), "hhs_update_system")
+
+
+def hold_step(ctx, sys, n, stime, dt, calc_timestep=True, prec=PREC_MIXED, clevel=0,
+              stream=None):
+    """hold_step<double,BS>(clevel, globals, sys, N, stime, stime+dt, dt, calc_timestep)."""
+    _check(lib().hhs_hold_step(ctx.h, clevel, sys.ref, n, stime, stime + dt, dt,
+                               int(calc_timestep), prec, stream), "hhs_hold_step")
+
+
+def hold_step_host(ctx, sys, n, dt, calc_timestep=True, prec=PREC_FP64, stream=None):
+    _check(lib().hhs_hold_step_host(ctx.h, sys.ref, n, dt, int(calc_timestep), prec, stream),
+           "hhs_hold_step_host")
+
+
+def launch_count():
+    return lib().hhs_kernel_launch_count()
+
+
+def measure_fma_peaks(stream=None):
+    a, b = ctypes.c_double(), ctypes.c_double()
+    _check(lib().hhs_measure_fma_peaks(ctypes.byref(a), ctypes.byref(b), stream), "fma_peaks")
+    return a.value, b.value
+
+
+def scan_workspace_size(n):
+    return lib().hhs_scan_workspace_size(n)
+
+
+def scan_exclusive_i32(d_in, d_out, n, d_ws, ws_bytes, stream=None):
+    _check(lib().hhs_scan_exclusive_i32(d_in, d_out, n, d_ws, ws_bytes, stream),
+           "hhs_scan_exclusive_i32")
+
+
+def scan_workspace_status(d_ws, stream=None):
+    return lib().hhs_scan_workspace_status(d_ws, stream)

@@ -1,0 +1,362 @@
+"""GPU parity tests: the CUDA path through the C ABI against the FP64 oracle, the golden
+fixtures from the reference's own test inputs, and the reference's own GPU kernels
+(compiled under oracle/_ref) where they were built."""
+import ctypes
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, REF_GPU
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("x", "y", "z", "vx", "vy", "vz", "m", "ts")
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a, dtype="<i4").tobytes()).hexdigest()
+
+
+def _scan_gpu(hhs, torch, a_dev, n, offset=0):
+    out = torch.empty(n + offset, dtype=torch.int32, device="cuda")
+    ws_bytes = hhs.scan_workspace_size(n)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+    src = a_dev[offset:offset + n]
+    dst = out[offset:offset + n]
+    hhs.scan_exclusive_i32(_ptr(src), _ptr(dst), n, _ptr(ws), ws_bytes,
+                           ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert hhs.scan_workspace_status(_ptr(ws), ctypes.c_void_p(
+        torch.cuda.current_stream().cuda_stream)) == 0
+    return dst
+
+
+def _ref_gpu():
+    if not os.path.exists(REF_GPU):
+        return None
+    L = ctypes.CDLL(REF_GPU)
+    vp, d, i = ctypes.c_void_p, ctypes.c_double, ctypes.c_int
+    L.ref_scan_predicate.argtypes = [vp, vp, i, i]
+    L.ref_timesteps.argtypes = [vp, vp, vp, vp, d, i]
+    L.ref_kick_slow.argtypes = [vp, vp, vp, vp, d, d, i]
+    L.ref_kick_sf.argtypes = [vp, vp, vp, vp, vp, d, d, i, i]
+    L.ref_drift.argtypes = [vp, vp, d, d, i]
+    return L
+
+
+def ref_scan_small_sizes(n, bs, unroll=4):
+    """Sizes passed to scan_predicate_small by the reference's host recursion
+    (src/split.cuh:438-565, 588-599) for an n-element scan with block size bs."""
+    e = bs * unroll
+    calls = []
+
+    def large(m):
+        rem = m % e
+        large_ev(m - rem)
+        if rem:
+            calls.append(rem)
+
+    def large_ev(m):
+        nb = (m + e - 1) // e
+        if nb > e:
+            large(nb)
+        else:
+            calls.append(nb)
+
+    if n > e:
+        large(n)
+    else:
+        calls.append(n)
+    return calls
+
+
+def ref_scan_in_bounds(n, bs):
+    """scan_predicate_small(m) writes indices up to max(v, 4) + v - 1 of a 2v-int dynamic
+    shared buffer (v = next power of two >= m, src/split.cuh:150-159,445-457), past its
+    end for m < 3. Such sizes are never run."""
+    return all(m >= 3 for m in ref_scan_small_sizes(n, bs))
+
+
+# ------------------------------------------------------------------------------ scan
+def test_ref_scan_size_filter():
+    assert ref_scan_small_sizes(1023, 128) == [1, 511]
+    assert not ref_scan_in_bounds(1023, 128)
+    assert ref_scan_in_bounds(1023, 256) and ref_scan_in_bounds(2048, 128)
+
+
+def test_scan_matches_golden_reference_test_inputs(cuda, hhs):
+    torch = cuda
+    from make_golden import PROGRAMS, reference_test_inputs
+    cases = json.load(open(os.path.join(GOLDEN, "scan_reference_tests.json")))["cases"]
+    ref = _ref_gpu()
+    k = 0
+    for prog, sizes in PROGRAMS.items():
+        for total in reference_test_inputs(sizes):
+            c = cases[k]
+            k += 1
+            pred = torch.from_numpy((total <= np.float32(5.0)).astype(np.int32)).cuda()
+            out = _scan_gpu(hhs, torch, pred, len(total)).cpu().numpy()
+            assert _digest(out) == c["sha256_exclusive_scan"], (prog, c["n"])
+            if ref is not None:
+                for bs in (128, 256):
+                    if not ref_scan_in_bounds(len(total), bs):
+                        continue
+                    rout = torch.empty_like(pred)
+                    assert ref.ref_scan_predicate(_ptr(pred), _ptr(rout), len(total), bs) == 0
+                    assert np.array_equal(rout.cpu().numpy(), out), (prog, c["n"], bs)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 127, 4095, 4096, 4097, 8191, 65536 + 3,
+                               (1 << 20) + 7])
+@pytest.mark.parametrize("offset", [0, 1])
+def test_scan_random_values_sizes_alignment(cuda, hhs, oracle, n, offset):
+    torch = cuda
+    rng = np.random.default_rng(n + offset)
+    a = rng.integers(-1000, 1000, n + offset).astype(np.int32)
+    dev = torch.from_numpy(a).cuda()
+    out = _scan_gpu(hhs, torch, dev, n, offset).cpu().numpy()
+    assert np.array_equal(out, oracle.scan_exclusive(a[offset:]))
+
+
+def test_scan_repeated_calls_reuse_workspace(cuda, hhs, oracle):
+    torch = cuda
+    n = 300001
+    ws_bytes = hhs.scan_workspace_size(n)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for seed in range(3):
+        a = np.random.default_rng(seed).integers(0, 2, n).astype(np.int32)
+        dev = torch.from_numpy(a).cuda()
+        out = torch.empty_like(dev)
+        hhs.scan_exclusive_i32(_ptr(dev), _ptr(out), n, _ptr(ws), ws_bytes, st)
+        assert np.array_equal(out.cpu().numpy(), oracle.scan_exclusive(a))
+
+
+@pytest.mark.parametrize("log2n", [26, 28])
+def test_scan_full_size_properties(cuda, hhs, log2n):
+    """2^26 and 2^28 Bernoulli flags: checked through size-independent properties on the
+    device (differences reproduce the input, first is 0, last + input = total)."""
+    torch = cuda
+    n = 1 << log2n
+    g = torch.Generator(device="cuda").manual_seed(log2n)
+    flags = (torch.rand(n, device="cuda", generator=g) < 0.1).to(torch.int32)
+    out = _scan_gpu(hhs, torch, flags, n)
+    assert int(out[0]) == 0
+    assert torch.equal(out[1:] - out[:-1], flags[:-1])
+    assert int(out[-1]) + int(flags[-1]) == int(flags.sum())
+    del out, flags
+    torch.cuda.empty_cache()
+
+
+# ------------------------------------------------------------------------------ split
+def _device_partition(torch):
+    return torch.zeros(2, dtype=torch.int32, device="cuda")
+
+
+@pytest.mark.parametrize("n,frac", [(2, 0.5), (3, 0.0), (64, 1.0), (1000, 0.3), (4097, 0.05),
+                                    (20000, 0.6), (20000, "one")])
+def test_split_matches_oracle(cuda, hhs, oracle, n, frac):
+    torch = cuda
+    rng = np.random.default_rng(n)
+    s = {k: rng.standard_normal(n) for k in FIELDS}
+    s["ts"] = rng.random(n)
+    s["id"] = rng.permutation(n).astype(np.int32)
+    if frac == "one":
+        pivot = float(np.sort(s["ts"])[0])  # exactly one fast particle -> fold
+    else:
+        pivot = float(np.quantile(s["ts"], frac)) if frac > 0 else -1.0
+    ctx = hhs.Context(n, 4)
+    tot, slow, fast = hhs.ParticleSystem(n), hhs.ParticleSystem(n), hhs.ParticleSystem(n)
+    tot.upload(s)
+    part = _device_partition(torch)
+    pred = torch.empty(n, dtype=torch.int32, device="cuda")
+    scan = torch.empty(n, dtype=torch.int32, device="cuda")
+    hhs.split(ctx, tot, slow, fast, pivot, n, _ptr(part), _ptr(pred), _ptr(scan))
+    torch.cuda.synchronize()
+    ctx.check()
+    n_slow, n_fast = part.cpu().numpy().tolist()
+    order, nf = oracle.split(s["ts"], pivot)
+    assert (n_fast, n_slow) == (nf, n - nf)
+    p_ref = (s["ts"] <= pivot).astype(np.int32)
+    assert np.array_equal(pred.cpu().numpy(), p_ref)
+    assert np.array_equal(scan.cpu().numpy(), oracle.scan_exclusive(p_ref))
+    F = fast.download(nf) if nf else None
+    Ls = slow.download(n - nf)
+    for k in FIELDS:
+        assert np.array_equal(Ls[k], s[k][order[nf:]]), k
+        if nf:
+            assert np.array_equal(F[k], s[k][order[:nf]]), k
+    assert np.array_equal(Ls["id"], s["id"][order[nf:]])
+    # parent_id: update_system scatters both halves back onto an empty parent
+    back = hhs.ParticleSystem(n)
+    hhs.update_system(back, slow, n - nf)
+    if nf:
+        hhs.update_system(back, fast, nf)
+    b = back.download()
+    for k in FIELDS:
+        assert np.array_equal(b[k], s[k]), k
+
+
+# ------------------------------------------------------------------------------ physics
+def _plummer(hhs, n, seed, spectrum=0):
+    return hhs.plummer(n, seed, spectrum)
+
+
+@pytest.mark.parametrize("n", [2, 3, 129, 1000])
+def test_timesteps_fp64_bit_exact(cuda, hhs, oracle, n):
+    s = _plummer(hhs, max(n, 2), 3)
+    ctx = hhs.Context(n, 4, eta=0.03)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    hhs.timesteps(ctx, d, n, hhs.PREC_FP64)
+    out = d.download()
+    assert np.array_equal(out["ts"], oracle.timesteps(s, 0.03))
+
+
+@pytest.mark.parametrize("n", [2, 1000, 5000])
+def test_timesteps_mixed_close(cuda, hhs, oracle, n):
+    s = _plummer(hhs, n, 4)
+    ctx = hhs.Context(n, 4, eta=0.02)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    hhs.timesteps(ctx, d, n, hhs.PREC_MIXED)
+    out = d.download()["ts"]
+    ref = oracle.timesteps(s, 0.02)
+    rel = np.abs(out - ref) / ref
+    assert rel.max() < 2e-6, rel.max()
+
+
+@pytest.mark.parametrize("n", [1, 7, 1000])
+def test_kick_slow_and_sf_fp64_bit_exact(cuda, hhs, oracle, n):
+    s = _plummer(hhs, max(n, 2), 5)
+    s = {k: v[:n].copy() for k, v in s.items()}
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    hhs.kick_slow(d, 0.01, 0.5, n, hhs.PREC_FP64)
+    out = d.download()
+    ref = {k: v.copy() for k, v in s.items()}
+    oracle.kick(ref, s, 0.5 * 0.01)
+    for k in ("vx", "vy", "vz", "x"):
+        assert np.array_equal(out[k], ref[k]), k
+    # kick_sf: sinks in one system, sources in another
+    src = _plummer(hhs, 333, 6)
+    so = hhs.ParticleSystem(333)
+    so.upload(src)
+    hhs.kick_sf(so, d, 1.0, 0.02, n, 333, hhs.PREC_FP64)
+    out2 = d.download()
+    oracle.kick(ref, src, 0.02 * 1.0)
+    for k in ("vx", "vy", "vz"):
+        assert np.array_equal(out2[k], ref[k]), k
+
+
+def test_kick_mixed_close(cuda, hhs, oracle):
+    n = 4000
+    s = _plummer(hhs, n, 8)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    hhs.kick_slow(d, 1.0, 1.0, n, hhs.PREC_MIXED)
+    out = d.download()
+    ref = {k: v.copy() for k, v in s.items()}
+    acc = oracle.kick(ref, s, 1.0)
+    amag = np.sqrt((acc ** 2).sum(0))
+    for c, k in enumerate(("vx", "vy", "vz")):
+        err = np.abs((out[k] - s[k]) - acc[c]) / amag
+        assert err.max() < 1e-6, (k, err.max())
+
+
+def test_drift_update_and_aos_roundtrip(cuda, hhs):
+    n = 777
+    s = _plummer(hhs, n, 9)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    hhs.drift(d, 0.125, 0.5, n)
+    out = d.download()
+    for a, v in (("x", "vx"), ("y", "vy"), ("z", "vz")):
+        assert np.array_equal(out[a], s[a] + s[v] * (0.125 * 0.5))
+    # AoS (vec3) upload / download
+    L = hhs.lib()
+    pos3 = np.ascontiguousarray(np.stack([s["x"], s["y"], s["z"]], 1))
+    vel3 = np.ascontiguousarray(np.stack([s["vx"], s["vy"], s["vz"]], 1))
+    dp = ctypes.POINTER(ctypes.c_double)
+    assert L.hhs_particle_system_upload_aos(d.ref, n, pos3.ctypes.data_as(dp),
+                                            vel3.ctypes.data_as(dp), None, None, None,
+                                            None) == 0
+    back = d.download()
+    assert np.array_equal(back["x"], s["x"]) and np.array_equal(back["vz"], s["vz"])
+    p2, v2 = np.zeros_like(pos3), np.zeros_like(vel3)
+    assert L.hhs_particle_system_download_aos(d.ref, n, p2.ctypes.data_as(dp),
+                                              v2.ctypes.data_as(dp), None, None, None,
+                                              None) == 0
+    assert np.array_equal(p2, pos3) and np.array_equal(v2, vel3)
+
+
+# ------------------------------------------------------------------------------ HOLD
+@pytest.mark.parametrize("n,steps,spectrum", [(64, 3, 0), (300, 3, 0), (1024, 2, 1)])
+def test_hold_step_host_fp64_bit_exact(cuda, hhs, oracle, n, steps, spectrum):
+    s = _plummer(hhs, n, 10 + n, spectrum)
+    ref = {k: v.copy() for k, v in s.items()}
+    ctx = hhs.Context(n, 64, eta=0.03)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    dt = 1.0 / 64
+    leaf = 0.0
+    for _ in range(steps):
+        hhs.hold_step_host(ctx, d, n, dt, True, hhs.PREC_FP64)
+        tr, _ = oracle.hold_step(ref, dt, True, 0.03)
+        leaf += tr.leaf_time
+    out = d.download()
+    for k in FIELDS:
+        assert np.array_equal(out[k], ref[k]), k
+    assert ctx.simtime() == pytest.approx(leaf, rel=1e-15)
+
+
+def test_hold_step_mixed_close(cuda, hhs, oracle):
+    n = 1024
+    s = _plummer(hhs, n, 77)
+    ref = {k: v.copy() for k, v in s.items()}
+    ctx = hhs.Context(n, 64, eta=0.03)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    dt = 1.0 / 64
+    e0 = hhs.energy_host(s)
+    hhs.hold_step(ctx, d, n, 0.0, dt, True, hhs.PREC_MIXED)
+    ctx.check()
+    out = d.download()
+    oracle.hold_step(ref, dt, True, 0.03)
+    dx = max(np.abs(out[k] - ref[k]).max() for k in ("x", "y", "z"))
+    assert dx < 1e-8, dx
+    e1 = hhs.energy_host(out)
+    assert abs((e1 - e0) / e0) < 1e-7
+
+
+# ------------------------------------------------------------------------------ reference
+@pytest.mark.skipif(not os.path.exists(REF_GPU), reason="reference GPU shims not built")
+def test_reference_gpu_kernels_pin_the_oracle(cuda, hhs, oracle):
+    """The reference's own timestep / kick / drift kernels (compiled with -fmad=false)
+    agree bit for bit with the oracle (kick: up to the reference's repulsive sign)."""
+    torch = cuda
+    ref = _ref_gpu()
+    n = 512  # a multiple of 256: the timestep kernel's tail-tile read stays out of play
+    s = _plummer(hhs, n, 12)
+    pos = torch.from_numpy(np.stack([s["x"], s["y"], s["z"]], 1).copy()).cuda()
+    vel = torch.from_numpy(np.stack([s["vx"], s["vy"], s["vz"]], 1).copy()).cuda()
+    acc = torch.zeros_like(pos)
+    m = torch.from_numpy(s["m"].copy()).cuda()
+    ts = torch.zeros(n, dtype=torch.float64, device="cuda")
+    assert ref.ref_timesteps(_ptr(pos), _ptr(vel), _ptr(m), _ptr(ts), 0.03, n) == 0
+    assert np.array_equal(ts.cpu().numpy(), oracle.timesteps(s, 0.03))
+    assert ref.ref_kick_slow(_ptr(pos), _ptr(vel), _ptr(acc), _ptr(m), 0.01, 1.0, n) == 0
+    o = {k: v.copy() for k, v in s.items()}
+    a = oracle.kick(o, s, -0.01)  # repulsive reference sign == attractive with -dt
+    assert np.array_equal(acc.cpu().numpy(), -a.T)
+    v = vel.cpu().numpy()
+    assert np.array_equal(v[:, 0], o["vx"]) and np.array_equal(v[:, 2], o["vz"])
+    assert ref.ref_drift(_ptr(pos), _ptr(vel), 0.5, 0.5, n) == 0
+    p = pos.cpu().numpy()
+    assert np.array_equal(p[:, 1], s["y"] + v[:, 1] * (0.5 * 0.5))
