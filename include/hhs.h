@@ -113,6 +113,9 @@ hhs_status hhs_ctx_flush_simtime(hhs_ctx* ctx, void* stream);
  * gave up, depth or capacity overflow) into a status. */
 hhs_status hhs_ctx_check(hhs_ctx* ctx, void* stream);
 hhs_status hhs_ctx_clear_errors(hhs_ctx* ctx, void* stream);
+/* Device-schedule tuning: nodes with at most small_n particles are solved, with their
+ * whole subtree, by a single CTA of the persistent HOLD kernel (0 = never). */
+hhs_status hhs_ctx_set_tuning(hhs_ctx* ctx, int32_t small_n);
 
 /* timesteps<T,BS>(sys, globals, N): src/timestep.cuh:103-118 (kernel :65-99) */
 hhs_status hhs_timesteps(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n,
@@ -146,8 +149,11 @@ hhs_status hhs_update_system(hhs_particle_system* prev, const hhs_particle_syste
                              int32_t n, void* stream);
 
 /* hold_step<T,BS>(clevel, globals, sys, N, stime, etime, dt, calc_timestep):
- * src/hold.cuh:51-181. The whole recursive step on the first n particles of sys,
- * stream-ordered; partition counts stay on the device. clevel only labels the trace. */
+ * src/hold.cuh:51-181. The whole recursive step on the first n particles of sys as one
+ * persistent cooperative kernel, stream-ordered and asynchronous: partition counts stay
+ * on the device and no host synchronisation happens inside the step (errors surface
+ * through hhs_ctx_check). clevel, stime and etime are accepted for the reference's
+ * signature; the top level is always 0. */
 hhs_status hhs_hold_step(hhs_ctx* ctx, int32_t clevel, hhs_particle_system* sys,
                          int32_t n, double stime, double etime, double dt,
                          int32_t calc_timestep, hhs_precision prec, void* stream);

@@ -55,5 +55,24 @@ def build(verbose=False, ptxas_info=False):
     return LIB
 
 
+def build_compat_test(verbose=False):
+    """Compiles tests/cpp/test_compat.cpp (a reference-style caller of include/hhs.hpp)."""
+    src = os.path.join(ROOT, "tests", "cpp", "test_compat.cpp")
+    out_dir = os.path.join(ROOT, "tests", "cpp", "_build")
+    exe = os.path.join(out_dir, "test_compat")
+    if not os.path.exists(src):
+        return None
+    os.makedirs(out_dir, exist_ok=True)
+    if _newer(exe, [src, LIB] + _headers() + [os.path.join(ROOT, "include", "hhs.hpp")]):
+        cmd = [NVCC] + ARCH + ["-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), src,
+                               "-o", exe, "-L" + HERE, "-lhhs_b200", "-Xlinker",
+                               "-rpath=$ORIGIN/../../../parallel-hhs_b200"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.check_call(cmd)
+    return exe
+
+
 if __name__ == "__main__":
     build(verbose=True, ptxas_info="--ptxas-info" in sys.argv)
+    build_compat_test(verbose=True)

@@ -299,6 +299,7 @@ extern "C" hhs_status hhs_ctx_create(int32_t n_max, int32_t max_levels, hhs_para
 extern "C" hhs_status hhs_ctx_destroy(hhs_ctx* c) {
     if (!c) return HHS_ERR_INVALID_ARG;
     delete static_cast<Profiler*>(c->prof);
+    engine_destroy(c);
     cudaError_t e1 = cudaFreeHost(c->host_counts);
     cudaError_t e2 = cudaFree(c->arena);
     delete c;
@@ -347,7 +348,12 @@ extern "C" hhs_status hhs_ctx_clear_errors(hhs_ctx* c, void* stream) {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     HHS_CUDA_TRY(cudaMemsetAsync(c->err, 0, sizeof(unsigned), s));
     HHS_CUDA_TRY(cudaMemsetAsync(scan_workspace_error_word(c->split_ws), 0, sizeof(unsigned), s));
-    return HHS_OK;
+    return engine_reset_barrier(c, s);
+}
+
+extern "C" hhs_status hhs_ctx_set_tuning(hhs_ctx* c, int32_t small_n) {
+    if (!c) return HHS_ERR_INVALID_ARG;
+    return engine_set_small_n(c, small_n);
 }
 
 extern "C" hhs_status hhs_ctx_get_stats(hhs_ctx* c, hhs_stats* out, void* stream) {
@@ -370,7 +376,8 @@ extern "C" hhs_status hhs_ctx_set_profiling(hhs_ctx* c, int32_t on) {
     p->resolve();
     p->on = on != 0;
     p->acc = hhs_profile{};
-    return HHS_OK;
+    hhs_profile scratch{};
+    return engine_get_profile(c, &scratch, true);
 }
 
 extern "C" hhs_status hhs_ctx_get_profile(hhs_ctx* c, hhs_profile* out) {
@@ -378,7 +385,7 @@ extern "C" hhs_status hhs_ctx_get_profile(hhs_ctx* c, hhs_profile* out) {
     auto* p = static_cast<Profiler*>(c->prof);
     p->resolve();
     *out = p->acc;
-    return HHS_OK;
+    return engine_get_profile(c, out, false);
 }
 
 extern "C" hhs_status hhs_measure_fma_peaks(double* fp32_tflops, double* fp64_tflops,
@@ -519,8 +526,14 @@ extern "C" hhs_status hhs_hold_step(hhs_ctx* c, int32_t clevel, hhs_particle_sys
     (void)clevel; (void)stime; (void)etime;
     if (!c || !sys_ok(sys) || n <= 0 || !(dt > 0.0)) return HHS_ERR_INVALID_ARG;
     if (n > sys->n || n > c->n_max) return HHS_ERR_CAPACITY;
-    if (c->engine_bytes == 0)
+    if (c->engine_bytes == 0 || !c->engine_host)
         return hhs_hold_step_host(c, sys, n, dt, calc_timestep, prec, stream);
-    return engine_hold_step(c, soa_of(sys), n, dt, calc_timestep != 0, prec,
-                            static_cast<cudaStream_t>(stream));
+    auto* prof = static_cast<Profiler*>(c->prof);
+    const bool on = prof && prof->on;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Profiler::Rec rec{};
+    if (on) prof->begin(rec, 4, 0.0, s);
+    hhs_status st = engine_hold_step(c, soa_of(sys), n, dt, calc_timestep != 0, prec, on, s);
+    if (st == HHS_OK && on) prof->end(rec, s);
+    return st;
 }

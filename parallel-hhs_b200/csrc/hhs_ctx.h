@@ -28,6 +28,7 @@ struct hhs_ctx {
     // device-resident engine state (hhs_engine.cu)
     void* engine = nullptr;
     size_t engine_bytes = 0;
+    void* engine_host = nullptr;
 
     int32_t* fast(int level) const { return fast_lists + (size_t)level * n_max; }
     int32_t* slow(int level) const { return slow_lists + (size_t)level * n_max; }
@@ -36,5 +37,9 @@ struct hhs_ctx {
 // Engine entry points (hhs_engine.cu)
 size_t engine_workspace_bytes(int n_max, int max_levels);
 hhs_status engine_init(hhs_ctx* c, void* base);
+void engine_destroy(hhs_ctx* c);
+hhs_status engine_set_small_n(hhs_ctx* c, int small_n);
+hhs_status engine_get_profile(hhs_ctx* c, hhs_profile* out, bool reset);
+hhs_status engine_reset_barrier(hhs_ctx* c, cudaStream_t stream);
 hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool calc_ts,
-                            hhs_precision prec, cudaStream_t stream);
+                            hhs_precision prec, bool profile, cudaStream_t stream);

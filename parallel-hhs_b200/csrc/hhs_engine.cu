@@ -1,10 +1,745 @@
-// hhs_engine.cu -- device-resident HOLD schedule (placeholder until the persistent
-// engine lands; the host-driven schedule is used while engine_workspace_bytes is 0).
-#include "hhs_ctx.h"
+// hhs_engine.cu -- device-resident HOLD schedule.
+//
+// The reference walks the recursion of src/hold.cuh:51-181 on the host, with a
+// device synchronisation and a host read of N_fast after every split
+// (src/split.cuh:430, src/hold.cuh:106-173) and 10-15 launches per node. Here the
+// whole top-level step is ONE persistent cooperative kernel: every CTA walks the
+// same recursion (explicit per-level state kept in registers; decisions are read
+// from device counts after grid barriers, so control flow is uniform), big nodes run
+// as grid-wide phases separated by bounded grid barriers, and small nodes (n at or
+// below a threshold) are solved with their whole subtree by one CTA while the others
+// wait at the next barrier.
+//
+// Phases of a big node at level k (S = fast list of level k-1, or all particles):
+//   [calc]  TS-units   : (sink block, source chunk) units, partial min/max per chunk
+//           TS-reduce  : per-sink reduction -> timestep, predicate, per-tile counts
+//   [!calc] COUNT      : predicate ts <= dt, per-tile counts
+//           SCATTER    : tile prefix, stable scatter into F_k / L_k, N_fast == 1 fold,
+//                        counts, leaf time (globals->simtime), work counters
+//   child (F_k, dt/2, calc = false)
+//           KICK-units : (sink block, source chunk) units; slow sources drifted by dt/2
+//                        on the fly (the first drift of src/hold.cuh:123-124)
+//           KICK-reduce: per-sink sum of partial accelerations, v += a*dt, and for
+//                        slow sinks both half drifts (src/hold.cuh:124,159)
+//   child (F_k, dt/2, calc = true)
+// Index lists replace the per-level copies and update_system of the reference
+// (src/split.cuh:341-356, src/update_system.cuh:14-23): particle data stays in the
+// caller's SoA arrays and every level works on global indices.
+#include <cstddef>
+#include <cstdint>
+#include <new>
 
-size_t engine_workspace_bytes(int, int) { return 0; }
-hhs_status engine_init(hhs_ctx*, void*) { return HHS_OK; }
-hhs_status engine_hold_step(hhs_ctx*, const SoA&, int, double, bool, hhs_precision,
-                            cudaStream_t) {
-    return HHS_ERR_INVALID_ARG;
+#include "hhs_ctx.h"
+#include "hhs_kernels.h"
+#include "hhs_pairmath.cuh"
+
+using namespace hhs;
+
+namespace {
+
+constexpr int kEB = 256;          // engine block size (one sink per thread per unit)
+constexpr int kMaxChunks = 32;    // source chunks per node (partial-sum slots)
+constexpr int kMaxLevels = 64;    // per-level state is kept in 64-bit masks
+constexpr unsigned long long kBarrierTimeoutNs = 60ull * 1000000000ull;
+
+enum ProfKind { kProfTs = 0, kProfKick = 1, kProfSplit = 2, kProfUpdate = 3, kProfSubtree = 5 };
+
+struct EngineState {
+    unsigned bar_count;
+    unsigned bar_gen;
+    unsigned pad[2];
+    unsigned long long prof_ns[8];
+    unsigned long long prof_cnt[8];
+    double prof_pairs[8];
+};
+
+struct EParams {
+    SoA P;
+    int n_top, n_max, max_levels, small_n, calc_top, profile;
+    double dt_top, eta, eta_s2;
+    float inv_eta_s2, inv_eta;
+    int32_t* fast_lists;
+    int32_t* slow_lists;
+    hhs_partition* counts;
+    double* leaf_time;
+    hhs_stats* stats;
+    double* ts_part;   // [kMaxChunks][n_max] (float view for mixed)
+    double* k_part;    // [kMaxChunks*3][n_max] (mixed) or [6][n_max] (FP64)
+    int* tile_counts;  // [n_max/kEB + 1]
+    EngineState* st;
+    unsigned* err;
+};
+
+struct __align__(16) Smem {
+    union {
+        struct { float4 A[kEB], B[kEB], V[kEB]; } tsm;         // mixed timestep tiles
+        struct { double x[kEB], y[kEB], z[kEB], vx[kEB], vy[kEB], vz[kEB], m[kEB]; } tsd;
+        struct { float4 A[kEB], B[kEB]; } km;                   // mixed kick tiles
+        struct { double x[kEB], y[kEB], z[kEB], m[kEB]; } kd;   // FP64 kick tiles
+    } u;
+    int warp_tot[kEB / 32];
+    int red[kEB / 32];
+    int ok;
+    int bcast;
+};
+
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ int ld_volatile_i32(const int32_t* p) {
+    return *reinterpret_cast<const volatile int32_t*>(p);
+}
+
+// ---------------------------------------------------------------- grid barrier
+// Sense-reversing barrier over all CTAs of the cooperative grid. Thread 0 of each CTA
+// arrives with one atomic; the last arrival resets the counter and advances the
+// generation; the others poll the generation, give up after kBarrierTimeoutNs (or as
+// soon as another CTA recorded an error) and report failure instead of hanging.
+__device__ bool grid_barrier(const EParams& E, Smem& sm) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        EngineState* st = E.st;
+        const unsigned gen = *reinterpret_cast<volatile unsigned*>(&st->bar_gen);
+        __threadfence();
+        const unsigned arrived = atomicAdd(&st->bar_count, 1u);
+        if (arrived == gridDim.x - 1) {
+            *reinterpret_cast<volatile unsigned*>(&st->bar_count) = 0u;
+            __threadfence();
+            atomicAdd(&st->bar_gen, 1u);
+        } else {
+            const unsigned long long t0 = gtimer();
+            while (ld_acquire_u32(&st->bar_gen) == gen) {
+                if (*reinterpret_cast<volatile unsigned*>(E.err) != 0u) { ok = 0; break; }
+                __nanosleep(40);
+                if (gtimer() - t0 > kBarrierTimeoutNs) {
+                    atomicOr(E.err, HHS_ERRBIT_BARRIER_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        sm.ok = ok;
+    }
+    __syncthreads();
+    return sm.ok != 0;
+}
+
+// Workers: the grid (worker = CTA) for big nodes, or one CTA alone for a subtree.
+struct Workers {
+    int id, count;
+    bool grid;
+};
+
+__device__ __forceinline__ bool phase_barrier(const EParams& E, Smem& sm, const Workers& W) {
+    if (W.grid) return grid_barrier(E, sm);
+    __syncthreads();
+    return true;
+}
+
+__device__ __forceinline__ void prof_mark(const EParams& E, const Workers& W,
+                                          unsigned long long& t_last, int kind, double pairs) {
+    if (!E.profile || threadIdx.x != 0 || W.id != 0) return;
+    const unsigned long long t = gtimer();
+    if (kind >= 0) {
+        E.st->prof_ns[kind] += t - t_last;
+        E.st->prof_cnt[kind] += 1;
+        E.st->prof_pairs[kind] += pairs;
+    }
+    t_last = t;
+}
+
+// number of source chunks for a node of n sinks
+__device__ __forceinline__ int chunks_for(int n, const Workers& W, bool split_ok) {
+    if (!W.grid || !split_ok) return 1;
+    const int nsb = (n + kEB - 1) / kEB;
+    int c = (8 * W.count + nsb - 1) / nsb;
+    c = c < 1 ? 1 : (c > kMaxChunks ? kMaxChunks : c);
+    const int maxc = (n + 63) / 64;  // at least 64 sources per chunk
+    return c < maxc ? c : (maxc < 1 ? 1 : maxc);
+}
+
+__device__ __forceinline__ int list_at(const int32_t* S, int i) { return S ? S[i] : i; }
+
+// ---------------------------------------------------------------- block scan helpers
+// exclusive prefix of a 0/1 flag over the CTA (one flag per thread) and the CTA total
+__device__ __forceinline__ int block_excl_flag(int flag, Smem& sm, int& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned b = __ballot_sync(HHS_FULL_MASK, flag);
+    const int within = __popc(b & ((1u << lane) - 1u));
+    __syncthreads();
+    if (lane == 0) sm.warp_tot[warp] = __popc(b);
+    __syncthreads();
+    int before = 0, tot = 0;
+#pragma unroll
+    for (int w = 0; w < kEB / 32; w++) {
+        const int t = sm.warp_tot[w];
+        before += (w < warp) ? t : 0;
+        tot += t;
+    }
+    total = tot;
+    return before + within;
+}
+
+__device__ __forceinline__ int block_sum(int v, Smem& sm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) sm.red[warp] = v;
+    __syncthreads();
+    int t = 0;
+#pragma unroll
+    for (int w = 0; w < kEB / 32; w++) t += sm.red[w];
+    return t;
+}
+
+// ---------------------------------------------------------------- timestep units
+template <int PREC>
+__device__ void ts_unit(const EParams& E, const int32_t* S, int n, int ib, int j0, int j1,
+                        double* out64, float* out32, Smem& sm) {
+    const int i = ib * kEB + threadIdx.x;
+    const bool act = i < n;
+    const int gi = act ? list_at(S, i) : 0;
+    const SoA& P = E.P;
+    if (PREC == HHS_PREC_FP64) {
+        double xi = 0, yi = 0, zi = 0, vxi = 0, vyi = 0, vzi = 0, mi = 0;
+        if (act) {
+            xi = P.x[gi]; yi = P.y[gi]; zi = P.z[gi];
+            vxi = P.vx[gi]; vyi = P.vy[gi]; vzi = P.vz[gi]; mi = P.m[gi];
+        }
+        double minval = 1.e30;
+        for (int t0 = j0; t0 < j1; t0 += kEB) {
+            const int tl = min(kEB, j1 - t0);
+            __syncthreads();
+            if ((int)threadIdx.x < tl) {
+                const int gj = list_at(S, t0 + threadIdx.x);
+                sm.u.tsd.x[threadIdx.x] = P.x[gj]; sm.u.tsd.y[threadIdx.x] = P.y[gj];
+                sm.u.tsd.z[threadIdx.x] = P.z[gj]; sm.u.tsd.vx[threadIdx.x] = P.vx[gj];
+                sm.u.tsd.vy[threadIdx.x] = P.vy[gj]; sm.u.tsd.vz[threadIdx.x] = P.vz[gj];
+                sm.u.tsd.m[threadIdx.x] = P.m[gj];
+            }
+            __syncthreads();
+            if (act) {
+                for (int jl = 0; jl < tl; jl++) {
+                    if (t0 + jl == i) continue;
+                    ts_pair_fp64(f64_sub(xi, sm.u.tsd.x[jl]), f64_sub(yi, sm.u.tsd.y[jl]),
+                                 f64_sub(zi, sm.u.tsd.z[jl]), f64_sub(vxi, sm.u.tsd.vx[jl]),
+                                 f64_sub(vyi, sm.u.tsd.vy[jl]), f64_sub(vzi, sm.u.tsd.vz[jl]),
+                                 mi, sm.u.tsd.m[jl], E.eta, E.eta_s2, minval);
+                }
+            }
+        }
+        if (act) out64[i] = minval;
+    } else {
+        DS xi{0, 0}, yi{0, 0}, zi{0, 0};
+        float vxi = 0, vyi = 0, vzi = 0, mi = 0;
+        if (act) {
+            xi = ds_split(P.x[gi]); yi = ds_split(P.y[gi]); zi = ds_split(P.z[gi]);
+            vxi = (float)P.vx[gi]; vyi = (float)P.vy[gi]; vzi = (float)P.vz[gi];
+            mi = (float)P.m[gi];
+        }
+        float maxrate = 0.0f;
+        for (int t0 = j0; t0 < j1; t0 += kEB) {
+            const int tl = min(kEB, j1 - t0);
+            __syncthreads();
+            if ((int)threadIdx.x < tl) {
+                const int gj = list_at(S, t0 + threadIdx.x);
+                const DS a = ds_split(P.x[gj]), b = ds_split(P.y[gj]), c = ds_split(P.z[gj]);
+                sm.u.tsm.A[threadIdx.x] = make_float4(a.hi, b.hi, c.hi, (float)P.m[gj]);
+                sm.u.tsm.B[threadIdx.x] = make_float4(a.lo, b.lo, c.lo, 0.0f);
+                sm.u.tsm.V[threadIdx.x] =
+                    make_float4((float)P.vx[gj], (float)P.vy[gj], (float)P.vz[gj], 0.0f);
+            }
+            __syncthreads();
+            if (act) {
+                for (int jl = 0; jl < tl; jl++) {
+                    if (t0 + jl == i) continue;
+                    const float4 A = sm.u.tsm.A[jl], B = sm.u.tsm.B[jl], V = sm.u.tsm.V[jl];
+                    const float r = ts_pair_rate_mixed(
+                        ds_diff(xi.hi, xi.lo, A.x, B.x), ds_diff(yi.hi, yi.lo, A.y, B.y),
+                        ds_diff(zi.hi, zi.lo, A.z, B.z), vxi - V.x, vyi - V.y, vzi - V.z,
+                        mi + A.w, E.inv_eta_s2, E.inv_eta);
+                    maxrate = fmaxf(maxrate, r);
+                }
+            }
+        }
+        if (act) out32[i] = maxrate;
+    }
+}
+
+// ---------------------------------------------------------------- kick units
+// Sinks s in [0, nf + ns): s < nf -> F[s] (fast), else L[s - nf] (slow). Sources j in
+// [0, ns + nf): j < ns -> L[j] (drifted by h on the fly), else F[j - ns]. Fast sinks
+// see slow sources only.
+template <int PREC>
+__device__ void kick_unit(const EParams& E, const int32_t* F, const int32_t* L, int nf, int ns,
+                          double h, int ib, int jc, int j0, int j1, Smem& sm) {
+    const int n = nf + ns;
+    const int s = ib * kEB + threadIdx.x;
+    const bool act = s < n;
+    const bool slow = s >= nf;
+    const int g = act ? (slow ? L[s - nf] : F[s]) : 0;
+    const int jend = slow ? j1 : min(j1, ns);
+    const SoA& P = E.P;
+    const int n_max = E.n_max;
+    if (PREC == HHS_PREC_FP64) {
+        double xi = 0, yi = 0, zi = 0;
+        if (act) {
+            xi = P.x[g]; yi = P.y[g]; zi = P.z[g];
+            if (slow) {
+                xi = f64_add(xi, f64_mul(P.vx[g], h));
+                yi = f64_add(yi, f64_mul(P.vy[g], h));
+                zi = f64_add(zi, f64_mul(P.vz[g], h));
+            }
+        }
+        double aL[3] = {0, 0, 0}, aF[3] = {0, 0, 0};
+        for (int t0 = j0; t0 < j1; t0 += kEB) {
+            const int tl = min(kEB, j1 - t0);
+            __syncthreads();
+            if ((int)threadIdx.x < tl) {
+                const int j = t0 + threadIdx.x;
+                const bool js = j < ns;
+                const int gj = js ? L[j] : F[j - ns];
+                double x = P.x[gj], y = P.y[gj], z = P.z[gj];
+                if (js) {
+                    x = f64_add(x, f64_mul(P.vx[gj], h));
+                    y = f64_add(y, f64_mul(P.vy[gj], h));
+                    z = f64_add(z, f64_mul(P.vz[gj], h));
+                }
+                sm.u.kd.x[threadIdx.x] = x; sm.u.kd.y[threadIdx.x] = y;
+                sm.u.kd.z[threadIdx.x] = z; sm.u.kd.m[threadIdx.x] = P.m[gj];
+            }
+            __syncthreads();
+            if (act) {
+                const int je = min(tl, jend - t0);
+                for (int jl = 0; jl < je; jl++) {
+                    double* a = (t0 + jl < ns) ? aL : aF;
+                    kick_pair_fp64(f64_sub(sm.u.kd.x[jl], xi), f64_sub(sm.u.kd.y[jl], yi),
+                                   f64_sub(sm.u.kd.z[jl], zi), sm.u.kd.m[jl], a[0], a[1], a[2]);
+                }
+            }
+        }
+        if (act) {
+            double* part = E.k_part;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                part[(size_t)k * n_max + s] = aL[k];
+                part[(size_t)(3 + k) * n_max + s] = aF[k];
+            }
+        }
+    } else {
+        DS xi{0, 0}, yi{0, 0}, zi{0, 0};
+        if (act) {
+            double x = P.x[g], y = P.y[g], z = P.z[g];
+            if (slow) { x = fma(P.vx[g], h, x); y = fma(P.vy[g], h, y); z = fma(P.vz[g], h, z); }
+            xi = ds_split(x); yi = ds_split(y); zi = ds_split(z);
+        }
+        float acc[3] = {0, 0, 0}, cmp[3] = {0, 0, 0};
+        for (int t0 = j0; t0 < j1; t0 += kEB) {
+            const int tl = min(kEB, j1 - t0);
+            __syncthreads();
+            if ((int)threadIdx.x < tl) {
+                const int j = t0 + threadIdx.x;
+                const bool js = j < ns;
+                const int gj = js ? L[j] : F[j - ns];
+                double x = P.x[gj], y = P.y[gj], z = P.z[gj];
+                if (js) { x = fma(P.vx[gj], h, x); y = fma(P.vy[gj], h, y); z = fma(P.vz[gj], h, z); }
+                const DS a = ds_split(x), b = ds_split(y), c = ds_split(z);
+                sm.u.km.A[threadIdx.x] = make_float4(a.hi, b.hi, c.hi, (float)P.m[gj]);
+                sm.u.km.B[threadIdx.x] = make_float4(a.lo, b.lo, c.lo, 0.0f);
+            }
+            __syncthreads();
+            if (act) {
+                const int je = min(tl, jend - t0);
+                for (int jl = 0; jl < je; jl++) {
+                    const float4 A = sm.u.km.A[jl], B = sm.u.km.B[jl];
+                    const float dx = ds_diff(A.x, B.x, xi.hi, xi.lo);
+                    const float dy = ds_diff(A.y, B.y, yi.hi, yi.lo);
+                    const float dz = ds_diff(A.z, B.z, zi.hi, zi.lo);
+                    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    if (d2 == 0.0f) continue;
+                    const float ri = rsqrt_nr(d2);
+                    const float mr3 = A.w * ri * ri * ri;
+                    kahan_add(acc[0], cmp[0], dx * mr3);
+                    kahan_add(acc[1], cmp[1], dy * mr3);
+                    kahan_add(acc[2], cmp[2], dz * mr3);
+                }
+            }
+        }
+        if (act) {
+            double* part = E.k_part;
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                part[(size_t)(jc * 3 + k) * n_max + s] = (double)acc[k] - (double)cmp[k];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- node phases
+// Per-sink reduction of the timestep partials (calc) or plain predicate (no calc),
+// writing per-tile predicate counts.
+template <int PREC>
+__device__ void count_phase(const EParams& E, const int32_t* S, int n, double dt, bool calc,
+                            int nch, const Workers& W, Smem& sm) {
+    const int ntiles = (n + kEB - 1) / kEB;
+    for (int t = W.id; t < ntiles; t += W.count) {
+        const int i = t * kEB + threadIdx.x;
+        int flag = 0;
+        if (i < n) {
+            const int gi = list_at(S, i);
+            double ts;
+            if (calc) {
+                if (PREC == HHS_PREC_FP64) {
+                    double mv = 1.e30;
+                    for (int c = 0; c < nch; c++) {
+                        const double v = E.ts_part[(size_t)c * E.n_max + i];
+                        if (v < mv) mv = v;
+                    }
+                    ts = mv;
+                } else {
+                    const float* p32 = reinterpret_cast<const float*>(E.ts_part);
+                    float mr = 0.0f;
+                    for (int c = 0; c < nch; c++) mr = fmaxf(mr, p32[(size_t)c * E.n_max + i]);
+                    const double tv = 1.0 / (double)mr;
+                    ts = tv < 1.e30 ? tv : 1.e30;
+                }
+                E.P.ts[gi] = ts;
+            } else {
+                ts = E.P.ts[gi];
+            }
+            flag = ts <= dt;
+        }
+        const int c = block_sum(flag, sm);
+        if (threadIdx.x == 0) E.tile_counts[t] = c;
+    }
+}
+
+// Stable scatter into F_k / L_k with the N_fast == 1 fold (src/split.cuh:304-370).
+__device__ void scatter_phase(const EParams& E, const int32_t* S, int n, double dt, int level,
+                              bool calc, const Workers& W, Smem& sm) {
+    const int ntiles = (n + kEB - 1) / kEB;
+    int32_t* F = E.fast_lists + (size_t)level * E.n_max;
+    int32_t* L = E.slow_lists + (size_t)level * E.n_max;
+    // grand total (every worker computes it; identical everywhere)
+    int part = 0;
+    for (int t = threadIdx.x; t < ntiles; t += kEB) part += E.tile_counts[t];
+    const int nf_raw = block_sum(part, sm);
+    const bool fold = nf_raw == 1;
+    for (int t = W.id; t < ntiles; t += W.count) {
+        int pre = 0;
+        for (int u = threadIdx.x; u < t; u += kEB) pre += E.tile_counts[u];
+        const int prefix = block_sum(pre, sm);
+        const int i = t * kEB + threadIdx.x;
+        int flag = 0, gi = 0;
+        if (i < n) {
+            gi = list_at(S, i);
+            flag = E.P.ts[gi] <= dt;
+        }
+        int tot;
+        const int ex = block_excl_flag(flag, sm, tot);
+        if (i < n) {
+            const int p = prefix + ex;
+            if (flag) {
+                if (fold) L[n - 1] = gi;
+                else F[p] = gi;
+            } else {
+                L[i - p] = gi;
+            }
+        }
+    }
+    if (W.id == 0 && threadIdx.x == 0) {
+        const int nf = fold ? 0 : nf_raw;
+        E.counts[level].n_fast = nf;
+        E.counts[level].n_slow = n - nf;
+        if (nf == 0) *E.leaf_time += dt;
+        const double ns = (double)(n - nf), nfd = (double)nf;
+        E.stats->nodes += 1;
+        if (level > E.stats->max_level) E.stats->max_level = level;
+        E.stats->kick_pairs += ns * (ns - 1.0) + 2.0 * ns * nfd;
+        if (calc) E.stats->ts_pairs += (double)n * (double)(n - 1);
+    }
+}
+
+template <int PREC>
+__device__ void kick_reduce_phase(const EParams& E, const int32_t* F, const int32_t* L, int nf,
+                                  int ns, double dt, int nch, int C, const Workers& W,
+                                  Smem& sm) {
+    const int n = nf + ns;
+    const double h = dt * 0.5;
+    const int ntiles = (n + kEB - 1) / kEB;
+    const SoA& P = E.P;
+    for (int t = W.id; t < ntiles; t += W.count) {
+        const int s = t * kEB + threadIdx.x;
+        if (s >= n) continue;
+        const bool slow = s >= nf;
+        const int g = slow ? L[s - nf] : F[s];
+        const double v0[3] = {P.vx[g], P.vy[g], P.vz[g]};
+        double v1[3];
+        if (PREC == HHS_PREC_FP64) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                double v = f64_add(v0[k], f64_mul(E.k_part[(size_t)k * E.n_max + s], dt));
+                if (slow && nf > 0)
+                    v = f64_add(v, f64_mul(E.k_part[(size_t)(3 + k) * E.n_max + s], dt));
+                v1[k] = v;
+            }
+        } else {
+            const int last = slow ? nch : min(nch, (ns + C - 1) / C);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                double a = 0.0;
+                for (int c = 0; c < last; c++) a += E.k_part[(size_t)(c * 3 + k) * E.n_max + s];
+                v1[k] = fma(a, dt, v0[k]);
+            }
+        }
+        P.vx[g] = v1[0]; P.vy[g] = v1[1]; P.vz[g] = v1[2];
+        if (slow) {
+            if (PREC == HHS_PREC_FP64) {
+                P.x[g] = f64_add(f64_add(P.x[g], f64_mul(v0[0], h)), f64_mul(v1[0], h));
+                P.y[g] = f64_add(f64_add(P.y[g], f64_mul(v0[1], h)), f64_mul(v1[1], h));
+                P.z[g] = f64_add(f64_add(P.z[g], f64_mul(v0[2], h)), f64_mul(v1[2], h));
+            } else {
+                P.x[g] = fma(v1[0], h, fma(v0[0], h, P.x[g]));
+                P.y[g] = fma(v1[1], h, fma(v0[1], h, P.y[g]));
+                P.z[g] = fma(v1[2], h, fma(v0[2], h, P.z[g]));
+            }
+        }
+    }
+    (void)sm;
+}
+
+// ---------------------------------------------------------------- the recursion
+// Walks the HOLD recursion from `top` (whose subsystem is already defined by the
+// counts/lists above it). Grid mode delegates nodes with n <= small_n to CTA 0.
+template <int PREC, bool GRID>
+__device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers& W, Smem& sm,
+                         unsigned long long& t_last) {
+    unsigned long long after1 = 0, after2 = 0, calcm = 0;  // per-level state bits
+    if (top_calc) calcm |= 1ull << top;
+    int lvl = top;
+    while (lvl >= top) {
+        const unsigned long long bit = 1ull << lvl;
+        const int n = (lvl == 0) ? E.n_top : ld_volatile_i32(&E.counts[lvl - 1].n_fast);
+        const int32_t* S = (lvl == 0) ? nullptr : E.fast_lists + (size_t)(lvl - 1) * E.n_max;
+        const double dt = ldexp(E.dt_top, -lvl);
+        const bool calc = (calcm & bit) != 0;
+        int32_t* F = E.fast_lists + (size_t)lvl * E.n_max;
+        int32_t* L = E.slow_lists + (size_t)lvl * E.n_max;
+        if (!(after1 & bit)) {
+            if (lvl >= E.max_levels || lvl >= kMaxLevels - 1) {
+                if (threadIdx.x == 0) atomicOr(E.err, HHS_ERRBIT_DEPTH);
+                return false;
+            }
+            if (GRID && n <= E.small_n) {
+                if (W.id == 0) {
+                    const Workers one{0, 1, false};
+                    unsigned long long t_sub = 0;
+                    run_hold<PREC, false>(E, lvl, calc, one, sm, t_sub);
+                }
+                if (!grid_barrier(E, sm)) return false;
+                prof_mark(E, W, t_last, kProfSubtree, 0.0);
+                calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
+                lvl--;
+                continue;
+            }
+            if (calc) {
+                const int nch = chunks_for(n, W, true);
+                const int C = (n + nch - 1) / nch;
+                const int nsb = (n + kEB - 1) / kEB;
+                for (int u = W.id; u < nsb * nch; u += W.count) {
+                    const int ib = u / nch, jc = u % nch;
+                    const int j0 = jc * C, j1 = min(n, j0 + C);
+                    ts_unit<PREC>(E, S, n, ib, j0, j1, E.ts_part + (size_t)jc * E.n_max,
+                                  reinterpret_cast<float*>(E.ts_part) + (size_t)jc * E.n_max, sm);
+                }
+                if (!phase_barrier(E, sm, W)) return false;
+                prof_mark(E, W, t_last, kProfTs, (double)n * (double)(n - 1));
+                count_phase<PREC>(E, S, n, dt, true, nch, W, sm);
+            } else {
+                count_phase<PREC>(E, S, n, dt, false, 1, W, sm);
+            }
+            if (!phase_barrier(E, sm, W)) return false;
+            scatter_phase(E, S, n, dt, lvl, calc, W, sm);
+            if (!phase_barrier(E, sm, W)) return false;
+            prof_mark(E, W, t_last, kProfSplit, 0.0);
+            after1 |= bit;
+            const int nf = ld_volatile_i32(&E.counts[lvl].n_fast);
+            if (nf > 0) {
+                lvl++;
+                const unsigned long long cb = 1ull << lvl;
+                calcm &= ~cb; after1 &= ~cb; after2 &= ~cb;
+                continue;
+            }
+        }
+        if (!(after2 & bit)) {
+            const int nf = ld_volatile_i32(&E.counts[lvl].n_fast);
+            const int ns = ld_volatile_i32(&E.counts[lvl].n_slow);
+            if (ns > 0) {
+                const int ntot = nf + ns;
+                const int nch = chunks_for(ntot, W, PREC != HHS_PREC_FP64);
+                const int C = (ntot + nch - 1) / nch;
+                const int nsb = (ntot + kEB - 1) / kEB;
+                const double h = dt * 0.5;
+                for (int u = W.id; u < nsb * nch; u += W.count) {
+                    const int ib = u / nch, jc = u % nch;
+                    const int j0 = jc * C, j1 = min(ntot, j0 + C);
+                    // blocks of fast sinks only need slow-source chunks
+                    if ((ib + 1) * kEB <= nf && j0 >= ns) continue;
+                    kick_unit<PREC>(E, F, L, nf, ns, h, ib, jc, j0, j1, sm);
+                }
+                if (!phase_barrier(E, sm, W)) return false;
+                const double ns_d = ns, nf_d = nf;
+                prof_mark(E, W, t_last, kProfKick, ns_d * (ns_d - 1.0) + 2.0 * ns_d * nf_d);
+                kick_reduce_phase<PREC>(E, F, L, nf, ns, dt, nch, C, W, sm);
+                if (!phase_barrier(E, sm, W)) return false;
+                prof_mark(E, W, t_last, kProfUpdate, 0.0);
+            }
+            after2 |= bit;
+            if (nf > 0) {
+                lvl++;
+                const unsigned long long cb = 1ull << lvl;
+                calcm = (calcm & ~cb) | cb;
+                after1 &= ~cb; after2 &= ~cb;
+                continue;
+            }
+        }
+        calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
+        lvl--;
+    }
+    return true;
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(kEB, 2) k_engine(EParams E) {
+    __shared__ Smem sm;
+    const Workers W{(int)blockIdx.x, (int)gridDim.x, true};
+    unsigned long long t_last = 0;
+    prof_mark(E, W, t_last, -1, 0.0);
+    run_hold<PREC, true>(E, 0, E.calc_top != 0, W, sm, t_last);
+}
+
+struct EngineHost {
+    int grid[2] = {0, 0};
+    int small_n = 256;
+    EngineState* st = nullptr;
+    double* ts_part = nullptr;
+    double* k_part = nullptr;
+    int* tile_counts = nullptr;
+};
+
+constexpr size_t kAl = 256;
+inline size_t al(size_t v) { return (v + kAl - 1) & ~(kAl - 1); }
+
+}  // namespace
+
+size_t engine_workspace_bytes(int n_max, int max_levels) {
+    (void)max_levels;
+    const size_t n = (size_t)n_max;
+    return al(sizeof(EngineState)) + al(sizeof(double) * kMaxChunks * n) +
+           al(sizeof(double) * kMaxChunks * 3 * n) + al(sizeof(int) * (n / kEB + 2));
+}
+
+hhs_status engine_init(hhs_ctx* c, void* base) {
+    auto* eh = new (std::nothrow) EngineHost();
+    if (!eh) return HHS_ERR_OOM;
+    char* p = static_cast<char*>(base);
+    const size_t n = (size_t)c->n_max;
+    eh->st = reinterpret_cast<EngineState*>(p); p += al(sizeof(EngineState));
+    eh->ts_part = reinterpret_cast<double*>(p); p += al(sizeof(double) * kMaxChunks * n);
+    eh->k_part = reinterpret_cast<double*>(p); p += al(sizeof(double) * kMaxChunks * 3 * n);
+    eh->tile_counts = reinterpret_cast<int*>(p);
+    int dev = 0, sms = 0, coop = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    if (!coop) { delete eh; return HHS_ERR_CUDA; }
+    int b0 = 0, b1 = 0;
+    HHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_engine<HHS_PREC_FP64>, kEB, 0));
+    HHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_engine<HHS_PREC_MIXED>, kEB, 0));
+    eh->grid[0] = sms * (b0 < 2 ? b0 : 2);
+    eh->grid[1] = sms * (b1 < 2 ? b1 : 2);
+    if (eh->grid[0] <= 0 || eh->grid[1] <= 0) { delete eh; return HHS_ERR_CUDA; }
+    c->engine_host = eh;
+    return HHS_OK;
+}
+
+void engine_destroy(hhs_ctx* c) {
+    delete static_cast<EngineHost*>(c->engine_host);
+    c->engine_host = nullptr;
+}
+
+hhs_status engine_set_small_n(hhs_ctx* c, int small_n) {
+    auto* eh = static_cast<EngineHost*>(c->engine_host);
+    if (!eh || small_n < 0) return HHS_ERR_INVALID_ARG;
+    eh->small_n = small_n;
+    return HHS_OK;
+}
+
+hhs_status engine_get_profile(hhs_ctx* c, hhs_profile* out, bool reset) {
+    auto* eh = static_cast<EngineHost*>(c->engine_host);
+    if (!eh) return HHS_ERR_INVALID_ARG;
+    EngineState h;
+    HHS_CUDA_TRY(cudaMemcpy(&h, eh->st, sizeof(h), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 8; k++) {
+        out->launches[k] += h.prof_cnt[k];
+        out->ms[k] += (double)h.prof_ns[k] * 1e-6;
+        out->pairs[k] += h.prof_pairs[k];
+    }
+    if (reset) {
+        HHS_CUDA_TRY(cudaMemset(reinterpret_cast<char*>(eh->st) + offsetof(EngineState, prof_ns),
+                                0, sizeof(EngineState) - offsetof(EngineState, prof_ns)));
+    }
+    return HHS_OK;
+}
+
+hhs_status engine_reset_barrier(hhs_ctx* c, cudaStream_t stream) {
+    auto* eh = static_cast<EngineHost*>(c->engine_host);
+    if (!eh) return HHS_ERR_INVALID_ARG;
+    HHS_CUDA_TRY(cudaMemsetAsync(eh->st, 0, 2 * sizeof(unsigned), stream));
+    return HHS_OK;
+}
+
+hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool calc_ts,
+                            hhs_precision prec, bool profile, cudaStream_t stream) {
+    auto* eh = static_cast<EngineHost*>(c->engine_host);
+    if (!eh) return HHS_ERR_INVALID_ARG;
+    EParams E;
+    E.P = P;
+    E.n_top = n;
+    E.n_max = c->n_max;
+    E.max_levels = c->max_levels < kMaxLevels - 1 ? c->max_levels : kMaxLevels - 1;
+    E.small_n = eh->small_n;
+    E.calc_top = calc_ts ? 1 : 0;
+    E.profile = profile ? 1 : 0;
+    E.dt_top = dt;
+    E.eta = c->params.eta;
+    E.eta_s2 = c->params.eta / 1.41421356237309504880;
+    E.inv_eta_s2 = (float)(1.0 / E.eta_s2);
+    E.inv_eta = (float)(1.0 / E.eta);
+    E.fast_lists = c->fast_lists;
+    E.slow_lists = c->slow_lists;
+    E.counts = c->counts;
+    E.leaf_time = c->leaf_time;
+    E.stats = c->stats;
+    E.ts_part = eh->ts_part;
+    E.k_part = eh->k_part;
+    E.tile_counts = eh->tile_counts;
+    E.st = eh->st;
+    E.err = c->err;
+    void* args[] = {&E};
+    const int pi = prec == HHS_PREC_FP64 ? 0 : 1;
+    cudaError_t e;
+    if (pi == 0)
+        e = cudaLaunchCooperativeKernel((const void*)k_engine<HHS_PREC_FP64>, eh->grid[0], kEB,
+                                        args, 0, stream);
+    else
+        e = cudaLaunchCooperativeKernel((const void*)k_engine<HHS_PREC_MIXED>, eh->grid[1], kEB,
+                                        args, 0, stream);
+    hhs_count_launch();
+    if (e != cudaSuccess) return hhs_from_cuda(e);
+    return HHS_OK;
 }

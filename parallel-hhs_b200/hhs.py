@@ -120,6 +120,7 @@ SIGNATURES = {
     "hhs_ctx_get_profile": (ctypes.c_int, [_vp, ctypes.POINTER(Profile)]),
     "hhs_kernel_launch_count": (ctypes.c_uint64, []),
     "hhs_measure_fma_peaks": (ctypes.c_int, [_dp, _dp, _vp]),
+    "hhs_ctx_set_tuning": (ctypes.c_int, [_vp, ctypes.c_int32]),
 }
 
 _lib = None
@@ -244,6 +245,9 @@ class Context:
 
     def reset_stats(self, stream=None):
         _check(lib().hhs_ctx_reset_stats(self.h, stream), "reset_stats")
+
+    def set_tuning(self, small_n):
+        _check(lib().hhs_ctx_set_tuning(self.h, small_n), "set_tuning")
 
     def set_profiling(self, on):
         _check(lib().hhs_ctx_set_profiling(self.h, int(on)), "set_profiling")

@@ -360,3 +360,85 @@ def test_reference_gpu_kernels_pin_the_oracle(cuda, hhs, oracle):
     assert ref.ref_drift(_ptr(pos), _ptr(vel), 0.5, 0.5, n) == 0
     p = pos.cpu().numpy()
     assert np.array_equal(p[:, 1], s["y"] + v[:, 1] * (0.5 * 0.5))
+
+
+# ------------------------------------------------------------------------------ engine
+@pytest.mark.parametrize("n,small_n,spectrum", [(64, 0, 0), (300, 0, 0), (300, 64, 0),
+                                                (300, 100000, 0), (2048, 256, 1),
+                                                (5000, 512, 0)])
+def test_hold_step_engine_fp64_bit_exact(cuda, hhs, oracle, n, small_n, spectrum):
+    """The persistent device schedule in FP64 reproduces the oracle bit for bit, with every
+    node on the grid (small_n = 0), every node in one CTA (huge small_n) or mixed."""
+    s = _plummer(hhs, n, 20 + n, spectrum)
+    ref = {k: v.copy() for k, v in s.items()}
+    ctx = hhs.Context(n, 64, eta=0.03)
+    ctx.set_tuning(small_n)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    dt = 1.0 / 64
+    leaf, nodes, kp, tp = 0.0, 0, 0.0, 0.0
+    for _ in range(2):
+        hhs.hold_step(ctx, d, n, 0.0, dt, True, hhs.PREC_FP64)
+        tr, _ = oracle.hold_step(ref, dt, True, 0.03)
+        leaf += tr.leaf_time
+        nodes += tr.count
+        kp += tr.kick_pairs
+        tp += tr.ts_pairs
+    ctx.check()
+    out = d.download()
+    for k in FIELDS:
+        assert np.array_equal(out[k], ref[k]), k
+    st = ctx.stats()
+    assert st["nodes"] == nodes and st["kick_pairs"] == kp and st["ts_pairs"] == tp
+    assert ctx.simtime() == pytest.approx(leaf, rel=1e-15)
+
+
+@pytest.mark.parametrize("n,small_n", [(1024, 0), (4096, 256), (16384, 512)])
+def test_hold_step_engine_mixed_close(cuda, hhs, oracle, n, small_n):
+    s = _plummer(hhs, n, 30 + n)
+    ref = {k: v.copy() for k, v in s.items()}
+    ctx = hhs.Context(n, 64, eta=0.03)
+    ctx.set_tuning(small_n)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    e0 = hhs.energy_host(s)
+    dt = 1.0 / 64
+    hhs.hold_step(ctx, d, n, 0.0, dt, True, hhs.PREC_MIXED)
+    ctx.check()
+    out = d.download()
+    oracle.hold_step(ref, dt, True, 0.03)
+    dx = max(np.abs(out[k] - ref[k]).max() for k in ("x", "y", "z"))
+    assert dx < 1e-7, dx
+    assert abs((hhs.energy_host(out) - e0) / e0) < 1e-7
+
+
+# ------------------------------------------------------------------------------ C++ API
+def test_reference_style_cpp_caller(cuda, hhs):
+    """tests/cpp/test_compat.cpp uses the reference's template API through include/hhs.hpp;
+    its result equals the same FP64 steps driven through the C ABI from Python."""
+    import subprocess
+    from conftest import ROOT
+    exe = os.path.join(ROOT, "tests", "cpp", "_build", "test_compat")
+    if not os.path.exists(exe):
+        pytest.skip("compat test binary not built")
+    n, steps = 1024, 2
+    out = subprocess.run([exe, str(n), str(steps)], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    assert "[FAIL]" not in out.stdout, out.stdout
+    res = json.loads(out.stdout.strip().splitlines()[-1])
+    s = hhs.plummer(n, 99)
+    ctx = hhs.Context(n, 64, eta=0.03)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    for _ in range(steps):
+        hhs.hold_step(ctx, d, n, 0.0, 1.0 / 64, True, hhs.PREC_FP64)
+    o = d.download()
+    h = 1469598103934665603
+    pos = np.stack([o["x"], o["y"], o["z"]], 1).tobytes()
+    vel = np.stack([o["vx"], o["vy"], o["vz"]], 1).tobytes()
+    for blob in (pos, vel, o["ts"].tobytes()):
+        for b in blob:
+            h = ((h ^ b) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    assert res["fnv"] == f"{h:016x}"
+    assert res["x0"] == o["x"][0]
+    assert res["simtime"] == pytest.approx(ctx.simtime(), rel=1e-15)
