@@ -42,6 +42,14 @@ def parse():
     p.add_argument("--seed", type=int, default=2024)
     p.add_argument("--prec", default="mixed", choices=["mixed", "fp64"])
     p.add_argument("--schedule", default="auto", choices=["auto", "host"])
+    p.add_argument("--small-n", type=int, default=256,
+                   help="device schedule: nodes with n <= this are solved by one CTA")
+    p.add_argument("--ctas-per-sm", type=int, default=2)
+    p.add_argument("--units-per-cta", type=int, default=8)
+    p.add_argument("--autotune", action="store_true",
+                   help="pick the device-schedule tuning with the library's autotuner")
+    p.add_argument("--profile-out", default=None,
+                   help="write the per-level phase profile (JSON) to this path")
     p.add_argument("--no-baselines", action="store_true",
                    help="skip the FP64 GPU and CPU baselines (quick runs)")
     return p.parse_args()
@@ -147,8 +155,12 @@ def run_ours(a, rank, world, torch, dist):
     ics = hhs.plummer(a.n, seed)
     e0 = hhs.energy_host(ics)
     ctx = hhs.Context(a.n, 64, eta=a.eta)
+    ctx.set_tuning(a.small_n, a.units_per_cta, a.ctas_per_sm)
     sys_ = hhs.ParticleSystem(a.n)
     sys_.upload(ics, stream=sh)
+    tuned = None
+    if a.autotune and a.schedule == "auto":
+        tuned = ctx.autotune(sys_, a.n, a.dt, prec, stream=sh)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
     def step(p=prec):
@@ -186,6 +198,14 @@ def run_ours(a, rank, world, torch, dist):
         ctx.check(sh)
         t_ms = sum(e0_.elapsed_time(e1_) for e0_, e1_ in evs)
         prof = ctx.profile()
+        if a.profile_out and a.schedule == "auto":
+            lms, lcnt = ctx.level_profile()
+            kinds = ["timesteps", "kick", "split", "update", "engine", "subtree", "k6", "k7"]
+            lp = {kinds[k]: {str(l): [round(float(lms[k, l]) / a.steps, 4), int(lcnt[k, l]) // a.steps]
+                             for l in range(64) if lcnt[k, l]} for k in range(8)}
+            with open(a.profile_out, "w") as f:
+                json.dump({"per_step_ms_and_phases_by_level": lp, "tuning": ctx.tuning()}, f,
+                          indent=1)
         ctx.set_profiling(False)
         stats = ctx.stats(sh)
         out = sys_.download(stream=sh)
@@ -201,6 +221,7 @@ def run_ours(a, rank, world, torch, dist):
     value = steps_total / (t_max * 1e-3)
     pairs_step = (stats["kick_pairs"] + stats["ts_pairs"]) / a.steps
     res = {"value": value, "t_ms": t_max, "pairs_per_step": pairs_step, "stats": stats,
+           "tuning": ctx.tuning(), "autotune": tuned,
            "prof": prof, "clocks": clk, "launches": (l1 - l0), "dE_over_E": (e1 - e0) / e0}
 
     # ---- end to end through the public API: host buffers, copies inside the timed region
@@ -268,6 +289,19 @@ def run_ours(a, rank, world, torch, dist):
         t64 = sum(x.elapsed_time(y) for x, y in evs)
         res["fp64_plain_steps_per_s"] = k64 / (t64 * 1e-3)
         res["fp64_plain_steps"] = k64
+        # the same FP64 kernels' arithmetic on the device-resident schedule (information)
+        if a.schedule == "auto":
+            with torch.cuda.stream(stream):
+                hhs.hold_step(ctx, sys64, a.n, 0.0, a.dt, True, hhs.PREC_FP64, stream=sh)
+                torch.cuda.synchronize()
+                for k in range(k64):
+                    flush.zero_()
+                    evs[k][0].record(stream)
+                    hhs.hold_step(ctx, sys64, a.n, 0.0, a.dt, True, hhs.PREC_FP64, stream=sh)
+                    evs[k][1].record(stream)
+                torch.cuda.synchronize()
+                ctx.check(sh)
+            res["fp64_engine_steps_per_s"] = k64 / (sum(x.elapsed_time(y) for x, y in evs) * 1e-3)
     res["fma_peaks"] = hhs.measure_fma_peaks(sh)
     return res
 
@@ -324,6 +358,7 @@ def main():
             "data": "synthetic (seeded Plummer sphere; no dataset)",
             "config": {"workload": workload_name(a), "n": a.n, "eta": a.eta, "dt_top": a.dt,
                        "precision": a.prec, "schedule": a.schedule,
+                       "tuning": res["tuning"], "autotuned": res["autotune"] is not None,
                        "l2": "flushed between timed steps (256 MiB memset)",
                        "parallelism": f"replicas x{world}"},
             "pair_interactions_per_s": res["pairs_per_step"] * res["value"],
@@ -344,6 +379,9 @@ def main():
                                       "unit": "HOLD steps/s", "steps": res["fp64_plain_steps"],
                                       "schedule": "host-driven, one-thread-per-sink FP64"}
             line["speedup_vs_fp64_plain"] = res["value"] / res["fp64_plain_steps_per_s"]
+        if "fp64_engine_steps_per_s" in res:
+            line["fp64_device_schedule"] = {"value": res["fp64_engine_steps_per_s"],
+                                            "unit": "HOLD steps/s"}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -113,9 +113,25 @@ hhs_status hhs_ctx_flush_simtime(hhs_ctx* ctx, void* stream);
  * gave up, depth or capacity overflow) into a status. */
 hhs_status hhs_ctx_check(hhs_ctx* ctx, void* stream);
 hhs_status hhs_ctx_clear_errors(hhs_ctx* ctx, void* stream);
-/* Device-schedule tuning: nodes with at most small_n particles are solved, with their
- * whole subtree, by a single CTA of the persistent HOLD kernel (0 = never). */
-hhs_status hhs_ctx_set_tuning(hhs_ctx* ctx, int32_t small_n);
+/* Device-schedule tuning. small_n: nodes with at most small_n particles are solved, with
+ * their whole subtree, by a single CTA of the persistent HOLD kernel (0 = never).
+ * units_per_cta: target number of (sink block, source chunk) work units per CTA when a
+ * node's pair work is cut into source chunks (1..64). ctas_per_sm: 1 or 2 (fewer CTAs make
+ * the grid barrier cheaper, more CTAs hide latency better). */
+typedef struct {
+    int32_t small_n;
+    int32_t units_per_cta;
+    int32_t ctas_per_sm;     /* CTAs of the persistent kernel per SM (1 or 2) */
+    int32_t _pad;
+    double ms_per_step;      /* filled by hhs_ctx_autotune: time of the chosen setting */
+} hhs_tuning;
+hhs_status hhs_ctx_set_tuning(hhs_ctx* ctx, const hhs_tuning* t);
+hhs_status hhs_ctx_get_tuning(hhs_ctx* ctx, hhs_tuning* t);
+/* Autotuner: times hold_step on the caller's system for a grid of tuning candidates,
+ * restoring the particle state before every trial and at the end, and keeps the fastest.
+ * Allocates a snapshot of the system (call it outside any timed or captured region). */
+hhs_status hhs_ctx_autotune(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n, double dt,
+                            hhs_precision prec, hhs_tuning* out, void* stream);
 
 /* timesteps<T,BS>(sys, globals, N): src/timestep.cuh:103-118 (kernel :65-99) */
 hhs_status hhs_timesteps(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n,
@@ -196,6 +212,9 @@ typedef struct {
 } hhs_profile;
 hhs_status hhs_ctx_set_profiling(hhs_ctx* ctx, int32_t on);
 hhs_status hhs_ctx_get_profile(hhs_ctx* ctx, hhs_profile* out);
+/* The device schedule's phase times per kind and level since profiling was switched on:
+ * ms[kind*64 + level] milliseconds and counts[kind*64 + level] phases (either may be NULL). */
+hhs_status hhs_ctx_get_level_profile(hhs_ctx* ctx, double* ms, uint64_t* counts);
 
 /* Kernel launches issued by this library since it was loaded (all contexts). */
 uint64_t hhs_kernel_launch_count(void);

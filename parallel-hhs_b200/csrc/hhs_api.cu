@@ -351,9 +351,14 @@ extern "C" hhs_status hhs_ctx_clear_errors(hhs_ctx* c, void* stream) {
     return engine_reset_barrier(c, s);
 }
 
-extern "C" hhs_status hhs_ctx_set_tuning(hhs_ctx* c, int32_t small_n) {
-    if (!c) return HHS_ERR_INVALID_ARG;
-    return engine_set_small_n(c, small_n);
+extern "C" hhs_status hhs_ctx_set_tuning(hhs_ctx* c, const hhs_tuning* t) {
+    if (!c || !t) return HHS_ERR_INVALID_ARG;
+    return engine_set_tuning(c, *t);
+}
+
+extern "C" hhs_status hhs_ctx_get_tuning(hhs_ctx* c, hhs_tuning* t) {
+    if (!c || !t) return HHS_ERR_INVALID_ARG;
+    return engine_get_tuning(c, t);
 }
 
 extern "C" hhs_status hhs_ctx_get_stats(hhs_ctx* c, hhs_stats* out, void* stream) {
@@ -386,6 +391,11 @@ extern "C" hhs_status hhs_ctx_get_profile(hhs_ctx* c, hhs_profile* out) {
     p->resolve();
     *out = p->acc;
     return engine_get_profile(c, out, false);
+}
+
+extern "C" hhs_status hhs_ctx_get_level_profile(hhs_ctx* c, double* ms, uint64_t* counts) {
+    if (!c) return HHS_ERR_INVALID_ARG;
+    return engine_get_level_profile(c, ms, counts);
 }
 
 extern "C" hhs_status hhs_measure_fma_peaks(double* fp32_tflops, double* fp64_tflops,
@@ -536,4 +546,82 @@ extern "C" hhs_status hhs_hold_step(hhs_ctx* c, int32_t clevel, hhs_particle_sys
     hhs_status st = engine_hold_step(c, soa_of(sys), n, dt, calc_timestep != 0, prec, on, s);
     if (st == HHS_OK && on) prof->end(rec, s);
     return st;
+}
+
+// ------------------------------------------------------------------ autotuner
+// Times the device-resident step for a grid of (small_n, units_per_cta) candidates on the
+// caller's own system: the state is snapshotted once, restored before every trial (one
+// untimed warm-up step, then two timed steps) and restored at the end; the fastest
+// candidate is kept. Pair throughput depends on how the hierarchy is cut between
+// grid-wide phases and single-CTA subtrees, which is a property of the system, so the
+// tuning is done on it rather than on a synthetic proxy.
+extern "C" hhs_status hhs_ctx_autotune(hhs_ctx* c, hhs_particle_system* sys, int32_t n,
+                                       double dt, hhs_precision prec, hhs_tuning* out,
+                                       void* stream) {
+    if (!c || !sys_ok(sys) || n <= 0 || n > sys->n || n > c->n_max || !(dt > 0.0))
+        return HHS_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    hhs_particle_system snap;
+    hhs_status st = hhs_particle_system_alloc(&snap, n);
+    if (st != HHS_OK) return st;
+    const size_t b = sizeof(double) * (size_t)n;
+    double* src[8] = {sys->x, sys->y, sys->z, sys->vx, sys->vy, sys->vz, sys->ts, sys->m};
+    double* dst[8] = {snap.x, snap.y, snap.z, snap.vx, snap.vy, snap.vz, snap.ts, snap.m};
+    auto copy_all = [&](bool save) -> hhs_status {
+        for (int k = 0; k < 8; k++)
+            HHS_CUDA_TRY(cudaMemcpyAsync(save ? dst[k] : src[k], save ? src[k] : dst[k], b,
+                                         cudaMemcpyDeviceToDevice, s));
+        return HHS_OK;
+    };
+    hhs_tuning best{}, cur{};
+    engine_get_tuning(c, &cur);
+    best = cur;
+    best.ms_per_step = 1e300;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double leaf = 0.0;
+    cudaMemcpy(&leaf, c->leaf_time, sizeof(double), cudaMemcpyDeviceToHost);
+    hhs_stats stats_saved{};
+    cudaMemcpy(&stats_saved, c->stats, sizeof(hhs_stats), cudaMemcpyDeviceToHost);
+    st = copy_all(true);
+    const int small_cands[] = {0, 32, 64, 128, 256, 512, 1024};
+    const int upc_cands[] = {4, 8, 16};
+    for (int cps = 1; cps <= 2; cps++)
+    for (int sn : small_cands) {
+        for (int upc : upc_cands) {
+            if (st != HHS_OK) break;
+            hhs_tuning t{sn, upc, cps, 0, 0.0};
+            st = engine_set_tuning(c, t);
+            if (st == HHS_OK) st = copy_all(false);
+            if (st == HHS_OK) st = engine_hold_step(c, soa_of(sys), n, dt, true, prec, false, s);
+            if (st == HHS_OK) st = copy_all(false);
+            if (st != HHS_OK) break;
+            cudaEventRecord(e0, s);
+            for (int r = 0; r < 2 && st == HHS_OK; r++)
+                st = engine_hold_step(c, soa_of(sys), n, dt, true, prec, false, s);
+            cudaEventRecord(e1, s);
+            if (st == HHS_OK) st = hhs_ctx_check(c, stream);
+            if (st != HHS_OK) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            t.ms_per_step = ms / 2.0;
+            if (t.ms_per_step < best.ms_per_step) best = t;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    hhs_status st2 = copy_all(false);
+    cudaMemcpyAsync(c->leaf_time, &leaf, sizeof(double), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(c->stats, &stats_saved, sizeof(hhs_stats), cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
+    hhs_particle_system_free(&snap);
+    if (st == HHS_OK) st = st2;
+    if (st != HHS_OK) {
+        engine_set_tuning(c, cur);
+        return st;
+    }
+    engine_set_tuning(c, best);
+    if (out) *out = best;
+    return HHS_OK;
 }

@@ -38,8 +38,10 @@ struct hhs_ctx {
 size_t engine_workspace_bytes(int n_max, int max_levels);
 hhs_status engine_init(hhs_ctx* c, void* base);
 void engine_destroy(hhs_ctx* c);
-hhs_status engine_set_small_n(hhs_ctx* c, int small_n);
+hhs_status engine_set_tuning(hhs_ctx* c, const hhs_tuning& t);
+hhs_status engine_get_tuning(hhs_ctx* c, hhs_tuning* t);
 hhs_status engine_get_profile(hhs_ctx* c, hhs_profile* out, bool reset);
+hhs_status engine_get_level_profile(hhs_ctx* c, double* ms, uint64_t* counts);
 hhs_status engine_reset_barrier(hhs_ctx* c, cudaStream_t stream);
 hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool calc_ts,
                             hhs_precision prec, bool profile, cudaStream_t stream);

@@ -51,11 +51,13 @@ struct EngineState {
     unsigned long long prof_ns[8];
     unsigned long long prof_cnt[8];
     double prof_pairs[8];
+    unsigned long long lvl_ns[8][kMaxLevels];   // per phase kind and level
+    unsigned long long lvl_cnt[8][kMaxLevels];
 };
 
 struct EParams {
     SoA P;
-    int n_top, n_max, max_levels, small_n, calc_top, profile;
+    int n_top, n_max, max_levels, small_n, calc_top, profile, units_per_cta;
     double dt_top, eta, eta_s2;
     float inv_eta_s2, inv_eta;
     int32_t* fast_lists;
@@ -66,6 +68,7 @@ struct EParams {
     double* ts_part;   // [kMaxChunks][n_max] (float view for mixed)
     double* k_part;    // [kMaxChunks*3][n_max] (mixed) or [6][n_max] (FP64)
     int* tile_counts;  // [n_max/kEB + 1]
+    unsigned* rate_acc;  // [n_max] max pair rate per list position (FP32 bits), kept at 0
     EngineState* st;
     unsigned* err;
 };
@@ -77,6 +80,7 @@ struct __align__(16) Smem {
         struct { float4 A[kEB], B[kEB]; } km;                   // mixed kick tiles
         struct { double x[kEB], y[kEB], z[kEB], m[kEB]; } kd;   // FP64 kick tiles
     } u;
+    float colred[kEB / 32][64];
     int warp_tot[kEB / 32];
     int red[kEB / 32];
     int ok;
@@ -141,23 +145,29 @@ __device__ __forceinline__ bool phase_barrier(const EParams& E, Smem& sm, const 
     return true;
 }
 
+// Phase timing by CTA 0 of the grid: the time from the previous mark to the release of
+// the barrier that ends the phase (the phase's makespan over all CTAs), per kind and level.
 __device__ __forceinline__ void prof_mark(const EParams& E, const Workers& W,
-                                          unsigned long long& t_last, int kind, double pairs) {
-    if (!E.profile || threadIdx.x != 0 || W.id != 0) return;
+                                          unsigned long long& t_last, int kind, double pairs,
+                                          int level = 0) {
+    if (!E.profile || !W.grid || threadIdx.x != 0 || W.id != 0) return;
     const unsigned long long t = gtimer();
     if (kind >= 0) {
         E.st->prof_ns[kind] += t - t_last;
         E.st->prof_cnt[kind] += 1;
         E.st->prof_pairs[kind] += pairs;
+        const int l = level < kMaxLevels ? level : kMaxLevels - 1;
+        E.st->lvl_ns[kind][l] += t - t_last;
+        E.st->lvl_cnt[kind][l] += 1;
     }
     t_last = t;
 }
 
 // number of source chunks for a node of n sinks
-__device__ __forceinline__ int chunks_for(int n, const Workers& W, bool split_ok) {
+__device__ __forceinline__ int chunks_for(int n, const Workers& W, bool split_ok, int upc) {
     if (!W.grid || !split_ok) return 1;
     const int nsb = (n + kEB - 1) / kEB;
-    int c = (8 * W.count + nsb - 1) / nsb;
+    int c = (upc * W.count + nsb - 1) / nsb;
     c = c < 1 ? 1 : (c > kMaxChunks ? kMaxChunks : c);
     const int maxc = (n + 63) / 64;  // at least 64 sources per chunk
     return c < maxc ? c : (maxc < 1 ? 1 : maxc);
@@ -271,6 +281,86 @@ __device__ void ts_unit(const EParams& E, const int32_t* S, int n, int ib, int j
     }
 }
 
+
+// ---------------------------------------------------------------- symmetric timestep
+// The pair timestep is exactly symmetric under i <-> j (dr, dv negate exactly, squares,
+// products of two negated values and the mass sum are unchanged), so each unordered pair
+// is evaluated once, in the unit (row block of kEB list positions, column block of 64)
+// that holds it with i < j. Rows keep their running max rate in a register; the column
+// maxima of a warp's 32 rows come from a butterfly transpose-reduce (31 shuffles for 32
+// columns). Both are merged into rate_acc with an integer atomicMax on the FP32 bit
+// pattern (rates are >= 0, so integer order is float order). Max is exact and
+// order-independent: the result equals the all-pairs evaluation bit for bit.
+constexpr int kCB = 64;
+
+__device__ __forceinline__ void butterfly_max32(float (&r)[32], int lane) {
+#pragma unroll
+    for (int k = 16; k >= 1; k >>= 1) {
+        const bool upper = (lane & k) != 0;
+#pragma unroll
+        for (int c = 0; c < k; c++) {
+            const float send = upper ? r[c] : r[c + k];
+            const float keep = upper ? r[c + k] : r[c];
+            r[c] = fmaxf(keep, __shfl_xor_sync(HHS_FULL_MASK, send, k));
+        }
+    }
+}
+
+__device__ void ts_sym_unit(const EParams& E, const int32_t* S, int n, int rb, int cb,
+                            Smem& sm) {
+    const SoA& P = E.P;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int i = rb * kEB + threadIdx.x;
+    const int c0 = cb * kCB;
+    const int ncol = min(kCB, n - c0);
+    __syncthreads();
+    if ((int)threadIdx.x < ncol) {
+        const int gj = list_at(S, c0 + threadIdx.x);
+        const DS a = ds_split(P.x[gj]), b = ds_split(P.y[gj]), c = ds_split(P.z[gj]);
+        sm.u.tsm.A[threadIdx.x] = make_float4(a.hi, b.hi, c.hi, (float)P.m[gj]);
+        sm.u.tsm.B[threadIdx.x] = make_float4(a.lo, b.lo, c.lo, 0.0f);
+        sm.u.tsm.V[threadIdx.x] =
+            make_float4((float)P.vx[gj], (float)P.vy[gj], (float)P.vz[gj], 0.0f);
+    }
+    const bool act = i < n;
+    DS xi{0, 0}, yi{0, 0}, zi{0, 0};
+    float vxi = 0, vyi = 0, vzi = 0, mi = 0;
+    if (act) {
+        const int gi = list_at(S, i);
+        xi = ds_split(P.x[gi]); yi = ds_split(P.y[gi]); zi = ds_split(P.z[gi]);
+        vxi = (float)P.vx[gi]; vyi = (float)P.vy[gi]; vzi = (float)P.vz[gi];
+        mi = (float)P.m[gi];
+    }
+    __syncthreads();
+    float rowmax = 0.0f;
+#pragma unroll 1
+    for (int g = 0; g < kCB / 32; g++) {
+        float r[32];
+#pragma unroll
+        for (int c = 0; c < 32; c++) {
+            const int jl = g * 32 + c;
+            const float4 A = sm.u.tsm.A[jl], B = sm.u.tsm.B[jl], V = sm.u.tsm.V[jl];
+            const float rate = ts_pair_rate_mixed(
+                ds_diff(xi.hi, xi.lo, A.x, B.x), ds_diff(yi.hi, yi.lo, A.y, B.y),
+                ds_diff(zi.hi, zi.lo, A.z, B.z), vxi - V.x, vyi - V.y, vzi - V.z, mi + A.w,
+                E.inv_eta_s2, E.inv_eta);
+            const bool ok = act && (jl < ncol) && (c0 + jl > i);
+            r[c] = ok ? rate : 0.0f;
+            rowmax = fmaxf(rowmax, r[c]);
+        }
+        butterfly_max32(r, lane);
+        sm.colred[warp][g * 32 + lane] = r[0];
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < ncol) {
+        float cm = 0.0f;
+#pragma unroll
+        for (int w = 0; w < kEB / 32; w++) cm = fmaxf(cm, sm.colred[w][threadIdx.x]);
+        if (cm > 0.0f) atomicMax(&E.rate_acc[c0 + threadIdx.x], __float_as_uint(cm));
+    }
+    if (act && rowmax > 0.0f) atomicMax(&E.rate_acc[i], __float_as_uint(rowmax));
+}
+
 // ---------------------------------------------------------------- kick units
 // Sinks s in [0, nf + ns): s < nf -> F[s] (fast), else L[s - nf] (slow). Sources j in
 // [0, ns + nf): j < ns -> L[j] (drifted by h on the fly), else F[j - ns]. Fast sinks
@@ -355,18 +445,26 @@ __device__ void kick_unit(const EParams& E, const int32_t* F, const int32_t* L, 
             __syncthreads();
             if (act) {
                 const int je = min(tl, jend - t0);
-                for (int jl = 0; jl < je; jl++) {
-                    const float4 A = sm.u.km.A[jl], B = sm.u.km.B[jl];
-                    const float dx = ds_diff(A.x, B.x, xi.hi, xi.lo);
-                    const float dy = ds_diff(A.y, B.y, yi.hi, yi.lo);
-                    const float dz = ds_diff(A.z, B.z, zi.hi, zi.lo);
-                    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                    if (d2 == 0.0f) continue;
-                    const float ri = rsqrt_nr(d2);
-                    const float mr3 = A.w * ri * ri * ri;
-                    kahan_add(acc[0], cmp[0], dx * mr3);
-                    kahan_add(acc[1], cmp[1], dy * mr3);
-                    kahan_add(acc[2], cmp[2], dz * mr3);
+                // blocked compensated summation: 32-pair FP32 blocks, Kahan across blocks
+                for (int jb = 0; jb < je; jb += 32) {
+                    const int jn = min(32, je - jb);
+                    float bx = 0.0f, by = 0.0f, bz = 0.0f;
+                    for (int jl = jb; jl < jb + jn; jl++) {
+                        const float4 A = sm.u.km.A[jl], B = sm.u.km.B[jl];
+                        const float dx = ds_diff(A.x, B.x, xi.hi, xi.lo);
+                        const float dy = ds_diff(A.y, B.y, yi.hi, yi.lo);
+                        const float dz = ds_diff(A.z, B.z, zi.hi, zi.lo);
+                        const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        const float ri = rsqrt_nr(d2);
+                        const float ri2 = ri * ri;
+                        const float mr3 = (d2 > 0.0f) ? A.w * ri2 * ri : 0.0f;
+                        bx = fmaf(dx, mr3, bx);
+                        by = fmaf(dy, mr3, by);
+                        bz = fmaf(dz, mr3, bz);
+                    }
+                    kahan_add(acc[0], cmp[0], bx);
+                    kahan_add(acc[1], cmp[1], by);
+                    kahan_add(acc[2], cmp[2], bz);
                 }
             }
         }
@@ -401,9 +499,8 @@ __device__ void count_phase(const EParams& E, const int32_t* S, int n, double dt
                     }
                     ts = mv;
                 } else {
-                    const float* p32 = reinterpret_cast<const float*>(E.ts_part);
-                    float mr = 0.0f;
-                    for (int c = 0; c < nch; c++) mr = fmaxf(mr, p32[(size_t)c * E.n_max + i]);
+                    const float mr = __uint_as_float(E.rate_acc[i]);
+                    E.rate_acc[i] = 0u;
                     const double tv = 1.0 / (double)mr;
                     ts = tv < 1.e30 ? tv : 1.e30;
                 }
@@ -541,23 +638,33 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                     run_hold<PREC, false>(E, lvl, calc, one, sm, t_sub);
                 }
                 if (!grid_barrier(E, sm)) return false;
-                prof_mark(E, W, t_last, kProfSubtree, 0.0);
+                prof_mark(E, W, t_last, kProfSubtree, 0.0, lvl);
                 calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
                 lvl--;
                 continue;
             }
             if (calc) {
-                const int nch = chunks_for(n, W, true);
-                const int C = (n + nch - 1) / nch;
-                const int nsb = (n + kEB - 1) / kEB;
-                for (int u = W.id; u < nsb * nch; u += W.count) {
-                    const int ib = u / nch, jc = u % nch;
-                    const int j0 = jc * C, j1 = min(n, j0 + C);
-                    ts_unit<PREC>(E, S, n, ib, j0, j1, E.ts_part + (size_t)jc * E.n_max,
-                                  reinterpret_cast<float*>(E.ts_part) + (size_t)jc * E.n_max, sm);
+                int nch = 1;
+                if (PREC == HHS_PREC_FP64) {
+                    nch = chunks_for(n, W, true, E.units_per_cta);
+                    const int C = (n + nch - 1) / nch;
+                    const int nsb = (n + kEB - 1) / kEB;
+                    for (int u = W.id; u < nsb * nch; u += W.count) {
+                        const int ib = u / nch, jc = u % nch;
+                        const int j0 = jc * C, j1 = min(n, j0 + C);
+                        ts_unit<PREC>(E, S, n, ib, j0, j1, E.ts_part + (size_t)jc * E.n_max,
+                                      nullptr, sm);
+                    }
+                } else {
+                    const int nrb = (n + kEB - 1) / kEB, ncb = (n + kCB - 1) / kCB;
+                    for (int u = W.id; u < nrb * ncb; u += W.count) {
+                        const int rb = u / ncb, cb = u % ncb;
+                        if ((cb + 1) * kCB <= rb * kEB + 1) continue;  // no pair with j > i
+                        ts_sym_unit(E, S, n, rb, cb, sm);
+                    }
                 }
                 if (!phase_barrier(E, sm, W)) return false;
-                prof_mark(E, W, t_last, kProfTs, (double)n * (double)(n - 1));
+                prof_mark(E, W, t_last, kProfTs, (double)n * (double)(n - 1), lvl);
                 count_phase<PREC>(E, S, n, dt, true, nch, W, sm);
             } else {
                 count_phase<PREC>(E, S, n, dt, false, 1, W, sm);
@@ -565,7 +672,7 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
             if (!phase_barrier(E, sm, W)) return false;
             scatter_phase(E, S, n, dt, lvl, calc, W, sm);
             if (!phase_barrier(E, sm, W)) return false;
-            prof_mark(E, W, t_last, kProfSplit, 0.0);
+            prof_mark(E, W, t_last, kProfSplit, 0.0, lvl);
             after1 |= bit;
             const int nf = ld_volatile_i32(&E.counts[lvl].n_fast);
             if (nf > 0) {
@@ -580,7 +687,7 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
             const int ns = ld_volatile_i32(&E.counts[lvl].n_slow);
             if (ns > 0) {
                 const int ntot = nf + ns;
-                const int nch = chunks_for(ntot, W, PREC != HHS_PREC_FP64);
+                const int nch = chunks_for(ntot, W, PREC != HHS_PREC_FP64, E.units_per_cta);
                 const int C = (ntot + nch - 1) / nch;
                 const int nsb = (ntot + kEB - 1) / kEB;
                 const double h = dt * 0.5;
@@ -593,10 +700,10 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                 }
                 if (!phase_barrier(E, sm, W)) return false;
                 const double ns_d = ns, nf_d = nf;
-                prof_mark(E, W, t_last, kProfKick, ns_d * (ns_d - 1.0) + 2.0 * ns_d * nf_d);
+                prof_mark(E, W, t_last, kProfKick, ns_d * (ns_d - 1.0) + 2.0 * ns_d * nf_d, lvl);
                 kick_reduce_phase<PREC>(E, F, L, nf, ns, dt, nch, C, W, sm);
                 if (!phase_barrier(E, sm, W)) return false;
-                prof_mark(E, W, t_last, kProfUpdate, 0.0);
+                prof_mark(E, W, t_last, kProfUpdate, 0.0, lvl);
             }
             after2 |= bit;
             if (nf > 0) {
@@ -624,11 +731,16 @@ __global__ void __launch_bounds__(kEB, 2) k_engine(EParams E) {
 
 struct EngineHost {
     int grid[2] = {0, 0};
+    int sms = 0, occ[2] = {0, 0};
+    int ctas_per_sm = 2;
     int small_n = 256;
+    int units_per_cta = 8;
     EngineState* st = nullptr;
     double* ts_part = nullptr;
     double* k_part = nullptr;
     int* tile_counts = nullptr;
+    unsigned* rate_acc = nullptr;
+    int n_max = 0;
 };
 
 constexpr size_t kAl = 256;
@@ -640,7 +752,8 @@ size_t engine_workspace_bytes(int n_max, int max_levels) {
     (void)max_levels;
     const size_t n = (size_t)n_max;
     return al(sizeof(EngineState)) + al(sizeof(double) * kMaxChunks * n) +
-           al(sizeof(double) * kMaxChunks * 3 * n) + al(sizeof(int) * (n / kEB + 2));
+           al(sizeof(double) * kMaxChunks * 3 * n) + al(sizeof(int) * (n / kEB + 2)) +
+           al(sizeof(unsigned) * n);
 }
 
 hhs_status engine_init(hhs_ctx* c, void* base) {
@@ -651,7 +764,9 @@ hhs_status engine_init(hhs_ctx* c, void* base) {
     eh->st = reinterpret_cast<EngineState*>(p); p += al(sizeof(EngineState));
     eh->ts_part = reinterpret_cast<double*>(p); p += al(sizeof(double) * kMaxChunks * n);
     eh->k_part = reinterpret_cast<double*>(p); p += al(sizeof(double) * kMaxChunks * 3 * n);
-    eh->tile_counts = reinterpret_cast<int*>(p);
+    eh->tile_counts = reinterpret_cast<int*>(p); p += al(sizeof(int) * (n / kEB + 2));
+    eh->rate_acc = reinterpret_cast<unsigned*>(p);
+    eh->n_max = c->n_max;
     int dev = 0, sms = 0, coop = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -660,6 +775,9 @@ hhs_status engine_init(hhs_ctx* c, void* base) {
     int b0 = 0, b1 = 0;
     HHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_engine<HHS_PREC_FP64>, kEB, 0));
     HHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_engine<HHS_PREC_MIXED>, kEB, 0));
+    eh->sms = sms;
+    eh->occ[0] = b0;
+    eh->occ[1] = b1;
     eh->grid[0] = sms * (b0 < 2 ? b0 : 2);
     eh->grid[1] = sms * (b1 < 2 ? b1 : 2);
     if (eh->grid[0] <= 0 || eh->grid[1] <= 0) { delete eh; return HHS_ERR_CUDA; }
@@ -672,10 +790,38 @@ void engine_destroy(hhs_ctx* c) {
     c->engine_host = nullptr;
 }
 
-hhs_status engine_set_small_n(hhs_ctx* c, int small_n) {
+hhs_status engine_set_tuning(hhs_ctx* c, const hhs_tuning& t) {
     auto* eh = static_cast<EngineHost*>(c->engine_host);
-    if (!eh || small_n < 0) return HHS_ERR_INVALID_ARG;
-    eh->small_n = small_n;
+    if (!eh || t.small_n < 0 || t.units_per_cta < 1 || t.units_per_cta > 64 ||
+        t.ctas_per_sm < 1 || t.ctas_per_sm > 2)
+        return HHS_ERR_INVALID_ARG;
+    eh->small_n = t.small_n;
+    eh->units_per_cta = t.units_per_cta;
+    eh->ctas_per_sm = t.ctas_per_sm;
+    for (int k = 0; k < 2; k++)
+        eh->grid[k] = eh->sms * (eh->occ[k] < t.ctas_per_sm ? eh->occ[k] : t.ctas_per_sm);
+    return HHS_OK;
+}
+
+hhs_status engine_get_tuning(hhs_ctx* c, hhs_tuning* t) {
+    auto* eh = static_cast<EngineHost*>(c->engine_host);
+    if (!eh || !t) return HHS_ERR_INVALID_ARG;
+    t->small_n = eh->small_n;
+    t->units_per_cta = eh->units_per_cta;
+    t->ctas_per_sm = eh->ctas_per_sm;
+    return HHS_OK;
+}
+
+hhs_status engine_get_level_profile(hhs_ctx* c, double* ms, uint64_t* counts) {
+    auto* eh = static_cast<EngineHost*>(c->engine_host);
+    if (!eh) return HHS_ERR_INVALID_ARG;
+    EngineState h;
+    HHS_CUDA_TRY(cudaMemcpy(&h, eh->st, sizeof(h), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 8; k++)
+        for (int l = 0; l < kMaxLevels; l++) {
+            if (ms) ms[k * kMaxLevels + l] = (double)h.lvl_ns[k][l] * 1e-6;
+            if (counts) counts[k * kMaxLevels + l] = h.lvl_cnt[k][l];
+        }
     return HHS_OK;
 }
 
@@ -700,6 +846,7 @@ hhs_status engine_reset_barrier(hhs_ctx* c, cudaStream_t stream) {
     auto* eh = static_cast<EngineHost*>(c->engine_host);
     if (!eh) return HHS_ERR_INVALID_ARG;
     HHS_CUDA_TRY(cudaMemsetAsync(eh->st, 0, 2 * sizeof(unsigned), stream));
+    HHS_CUDA_TRY(cudaMemsetAsync(eh->rate_acc, 0, sizeof(unsigned) * (size_t)eh->n_max, stream));
     return HHS_OK;
 }
 
@@ -713,6 +860,7 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
     E.n_max = c->n_max;
     E.max_levels = c->max_levels < kMaxLevels - 1 ? c->max_levels : kMaxLevels - 1;
     E.small_n = eh->small_n;
+    E.units_per_cta = eh->units_per_cta;
     E.calc_top = calc_ts ? 1 : 0;
     E.profile = profile ? 1 : 0;
     E.dt_top = dt;
@@ -728,6 +876,7 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
     E.ts_part = eh->ts_part;
     E.k_part = eh->k_part;
     E.tile_counts = eh->tile_counts;
+    E.rate_acc = eh->rate_acc;
     E.st = eh->st;
     E.err = c->err;
     void* args[] = {&E};

@@ -137,10 +137,11 @@ extern "C" hhs_status hhs_ic_plummer(int n, uint64_t seed, int mass_spectrum, do
         x[i] -= c[0]; y[i] -= c[1]; z[i] -= c[2];
         vx[i] -= c[3]; vy[i] -= c[4]; vz[i] -= c[5];
     }
-    // Henon units: E = -1/4 with the sampled virial ratio kept
+    // Henon units: E = -1/4 with the sampled virial ratio kept. A handful of particles
+    // can sample an unbound system (E >= 0); it is returned in structural units.
     double e = hhs_host_kinetic_energy(n, vx, vy, vz, m) +
                hhs_host_potential_energy(n, x, y, z, m);
-    if (!(e < 0.0)) return HHS_ERR_INVALID_ARG;
+    if (!(e < 0.0)) return HHS_OK;
     double beta = -4.0 * e, vs = 1.0 / std::sqrt(beta);
     for (int i = 0; i < n; i++) {
         x[i] *= beta; y[i] *= beta; z[i] *= beta;

@@ -58,6 +58,12 @@ class Profile(ctypes.Structure):
 PROFILE_KINDS = ("timesteps", "kick", "split", "drift", "engine", "k5", "k6", "k7")
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("small_n", ctypes.c_int32), ("units_per_cta", ctypes.c_int32),
+                ("ctas_per_sm", ctypes.c_int32), ("_pad", ctypes.c_int32),
+                ("ms_per_step", ctypes.c_double)]
+
+
 class CParticleSystem(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int32)] + \
         [(k, _dp) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "ts", "m")] + \
@@ -118,9 +124,14 @@ SIGNATURES = {
     "hhs_ctx_reset_stats": (ctypes.c_int, [_vp, _vp]),
     "hhs_ctx_set_profiling": (ctypes.c_int, [_vp, ctypes.c_int32]),
     "hhs_ctx_get_profile": (ctypes.c_int, [_vp, ctypes.POINTER(Profile)]),
+    "hhs_ctx_get_level_profile": (ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_uint64)]),
     "hhs_kernel_launch_count": (ctypes.c_uint64, []),
     "hhs_measure_fma_peaks": (ctypes.c_int, [_dp, _dp, _vp]),
-    "hhs_ctx_set_tuning": (ctypes.c_int, [_vp, ctypes.c_int32]),
+    "hhs_ctx_set_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(Tuning)]),
+    "hhs_ctx_get_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(Tuning)]),
+    "hhs_ctx_autotune": (ctypes.c_int, [_vp, ctypes.POINTER(CParticleSystem), ctypes.c_int32,
+                                        ctypes.c_double, ctypes.c_int, ctypes.POINTER(Tuning),
+                                        _vp]),
 }
 
 _lib = None
@@ -246,8 +257,29 @@ class Context:
     def reset_stats(self, stream=None):
         _check(lib().hhs_ctx_reset_stats(self.h, stream), "reset_stats")
 
-    def set_tuning(self, small_n):
-        _check(lib().hhs_ctx_set_tuning(self.h, small_n), "set_tuning")
+    def set_tuning(self, small_n=None, units_per_cta=None, ctas_per_sm=None):
+        t = Tuning()
+        _check(lib().hhs_ctx_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
+        if small_n is not None:
+            t.small_n = small_n
+        if units_per_cta is not None:
+            t.units_per_cta = units_per_cta
+        if ctas_per_sm is not None:
+            t.ctas_per_sm = ctas_per_sm
+        _check(lib().hhs_ctx_set_tuning(self.h, ctypes.byref(t)), "set_tuning")
+
+    def tuning(self):
+        t = Tuning()
+        _check(lib().hhs_ctx_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
+        return {"small_n": t.small_n, "units_per_cta": t.units_per_cta,
+                "ctas_per_sm": t.ctas_per_sm}
+
+    def autotune(self, sys, n, dt, prec=1, stream=None):
+        t = Tuning()
+        _check(lib().hhs_ctx_autotune(self.h, sys.ref, n, dt, prec, ctypes.byref(t), stream),
+               "autotune")
+        return {"small_n": t.small_n, "units_per_cta": t.units_per_cta,
+                "ctas_per_sm": t.ctas_per_sm, "ms_per_step": t.ms_per_step}
 
     def set_profiling(self, on):
         _check(lib().hhs_ctx_set_profiling(self.h, int(on)), "set_profiling")
@@ -257,6 +289,14 @@ class Context:
         _check(lib().hhs_ctx_get_profile(self.h, ctypes.byref(p)), "profile")
         return {PROFILE_KINDS[k]: {"launches": p.launches[k], "ms": p.ms[k], "pairs": p.pairs[k]}
                 for k in range(8) if p.launches[k]}
+
+    def level_profile(self):
+        ms = np.zeros(8 * 64)
+        cnt = np.zeros(8 * 64, dtype=np.uint64)
+        _check(lib().hhs_ctx_get_level_profile(self.h, _d(ms),
+                                               cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))),
+               "level_profile")
+        return ms.reshape(8, 64), cnt.reshape(8, 64)
 
     def destroy(self):
         if self.h:
