@@ -122,7 +122,7 @@ typedef struct {
     int32_t small_n;
     int32_t units_per_cta;
     int32_t ctas_per_sm;     /* CTAs of the persistent kernel per SM (1 or 2) */
-    int32_t _pad;
+    int32_t warp_n;          /* nodes with at most warp_n (<= 32) particles run on one warp */
     double ms_per_step;      /* filled by hhs_ctx_autotune: time of the chosen setting */
 } hhs_tuning;
 hhs_status hhs_ctx_set_tuning(hhs_ctx* ctx, const hhs_tuning* t);
@@ -187,6 +187,13 @@ hhs_status hhs_hold_step_host(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n,
 size_t hhs_scan_workspace_size(int64_t n);
 hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out, int64_t n,
                                   void* d_workspace, size_t workspace_bytes, void* stream);
+/* Stream compaction (the split of a flag array, src/split.cuh:573-610 on int32 data):
+ * d_idx[k] = index of the k-th nonzero flag, *d_count = number of nonzero flags, and
+ * d_scan (optional, NULL = not written) = exclusive scan of (flag != 0). One pass;
+ * workspace as for hhs_scan_exclusive_i32. */
+hhs_status hhs_compact_flags_i32(const int32_t* d_flags, int32_t* d_scan, int32_t* d_idx,
+                                 int32_t* d_count, int64_t n, void* d_workspace,
+                                 size_t workspace_bytes, void* stream);
 /* Synchronises the stream; HHS_ERR_TIMEOUT if a look-back wait of the last scan on this
  * workspace gave up. */
 hhs_status hhs_scan_workspace_status(const void* d_workspace, void* stream);
@@ -222,6 +229,28 @@ uint64_t hhs_kernel_launch_count(void);
 /* Measured arithmetic peaks of the current device: a register-resident chain of FP32
  * (and FP64) fused multiply-adds on every SM, timed with CUDA events. TFLOP/s. */
 hhs_status hhs_measure_fma_peaks(double* fp32_tflops, double* fp64_tflops, void* stream);
+
+/* ---- batched systems ------------------------------------------------------------ */
+/* Many independent systems packed back to back in one particle system: system k holds
+ * particles [offsets[k], offsets[k+1]) (host array, offsets[0] = 0). hhs_hold_batched
+ * advances every system by one top-level HOLD step in ONE launch: hardware thread-block
+ * clusters take the large systems (largest first, one cluster per system, cluster
+ * barriers between phases), then single CTAs take the rest, each split being a
+ * per-system (segmented) scan and compaction. Per-system leaf times are kept. */
+typedef struct hhs_batch hhs_batch;
+hhs_status hhs_batch_create(int32_t n_sys, const int32_t* offsets, int32_t max_levels,
+                            hhs_params params, hhs_batch** out);
+hhs_status hhs_batch_destroy(hhs_batch* b);
+/* big_n: systems with more particles run on a thread-block cluster; small_n: inside a
+ * system, nodes with at most small_n particles run on one CTA; units_per_cta as above. */
+hhs_status hhs_batch_set_tuning(hhs_batch* b, int32_t big_n, int32_t small_n,
+                                int32_t units_per_cta);
+hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, double dt,
+                            int32_t calc_timestep, hhs_precision prec, void* stream);
+hhs_status hhs_batch_get_simtime(hhs_batch* b, double* per_system, void* stream);
+hhs_status hhs_batch_get_stats(hhs_batch* b, hhs_stats* out, void* stream);
+hhs_status hhs_batch_reset_stats(hhs_batch* b, void* stream);
+hhs_status hhs_batch_check(hhs_batch* b, void* stream);
 
 /* Host-side utilities (no GPU): seeded Plummer initial conditions in Henon units,
  * and FP64 energies with compensated sums. */

@@ -591,7 +591,7 @@ extern "C" hhs_status hhs_ctx_autotune(hhs_ctx* c, hhs_particle_system* sys, int
     for (int sn : small_cands) {
         for (int upc : upc_cands) {
             if (st != HHS_OK) break;
-            hhs_tuning t{sn, upc, cps, 0, 0.0};
+            hhs_tuning t{sn, upc, cps, cur.warp_n, 0.0};
             st = engine_set_tuning(c, t);
             if (st == HHS_OK) st = copy_all(false);
             if (st == HHS_OK) st = engine_hold_step(c, soa_of(sys), n, dt, true, prec, false, s);

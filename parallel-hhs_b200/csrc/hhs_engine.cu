@@ -25,9 +25,14 @@
 // Index lists replace the per-level copies and update_system of the reference
 // (src/split.cuh:341-356, src/update_system.cuh:14-23): particle data stays in the
 // caller's SoA arrays and every level works on global indices.
+#include <cooperative_groups.h>
+
+#include <algorithm>
 #include <cstddef>
 #include <cstdint>
 #include <new>
+#include <numeric>
+#include <vector>
 
 #include "hhs_ctx.h"
 #include "hhs_kernels.h"
@@ -57,7 +62,7 @@ struct EngineState {
 
 struct EParams {
     SoA P;
-    int n_top, n_max, max_levels, small_n, calc_top, profile, units_per_cta;
+    int n_top, n_max, max_levels, small_n, calc_top, profile, units_per_cta, warp_n;
     double dt_top, eta, eta_s2;
     float inv_eta_s2, inv_eta;
     int32_t* fast_lists;
@@ -81,6 +86,8 @@ struct __align__(16) Smem {
         struct { double x[kEB], y[kEB], z[kEB], m[kEB]; } kd;   // FP64 kick tiles
     } u;
     float colred[kEB / 32][64];
+    unsigned wfast[kMaxLevels];   // warp solver: fast-lane mask per depth
+    int wlone[kMaxLevels];        // warp solver: lane folded into the slow set, or -1
     int warp_tot[kEB / 32];
     int red[kEB / 32];
     int ok;
@@ -133,14 +140,19 @@ __device__ bool grid_barrier(const EParams& E, Smem& sm) {
     return sm.ok != 0;
 }
 
-// Workers: the grid (worker = CTA) for big nodes, or one CTA alone for a subtree.
+// Workers: the whole cooperative grid (one worker per CTA), a hardware thread-block
+// cluster (one worker per CTA of the cluster; batched systems), or one CTA alone.
+enum { kModeBlock = 0, kModeGrid = 1, kModeCluster = 2 };
 struct Workers {
-    int id, count;
-    bool grid;
+    int id, count, mode;
 };
 
 __device__ __forceinline__ bool phase_barrier(const EParams& E, Smem& sm, const Workers& W) {
-    if (W.grid) return grid_barrier(E, sm);
+    if (W.mode == kModeGrid) return grid_barrier(E, sm);
+    if (W.mode == kModeCluster) {
+        cooperative_groups::this_cluster().sync();
+        return true;
+    }
     __syncthreads();
     return true;
 }
@@ -150,7 +162,7 @@ __device__ __forceinline__ bool phase_barrier(const EParams& E, Smem& sm, const 
 __device__ __forceinline__ void prof_mark(const EParams& E, const Workers& W,
                                           unsigned long long& t_last, int kind, double pairs,
                                           int level = 0) {
-    if (!E.profile || !W.grid || threadIdx.x != 0 || W.id != 0) return;
+    if (!E.profile || W.mode != kModeGrid || threadIdx.x != 0 || W.id != 0) return;
     const unsigned long long t = gtimer();
     if (kind >= 0) {
         E.st->prof_ns[kind] += t - t_last;
@@ -165,7 +177,7 @@ __device__ __forceinline__ void prof_mark(const EParams& E, const Workers& W,
 
 // number of source chunks for a node of n sinks
 __device__ __forceinline__ int chunks_for(int n, const Workers& W, bool split_ok, int upc) {
-    if (!W.grid || !split_ok) return 1;
+    if (W.mode == kModeBlock || !split_ok) return 1;
     const int nsb = (n + kEB - 1) / kEB;
     int c = (upc * W.count + nsb - 1) / nsb;
     c = c < 1 ? 1 : (c > kMaxChunks ? kMaxChunks : c);
@@ -554,10 +566,10 @@ __device__ void scatter_phase(const EParams& E, const int32_t* S, int n, double 
         E.counts[level].n_slow = n - nf;
         if (nf == 0) *E.leaf_time += dt;
         const double ns = (double)(n - nf), nfd = (double)nf;
-        E.stats->nodes += 1;
-        if (level > E.stats->max_level) E.stats->max_level = level;
-        E.stats->kick_pairs += ns * (ns - 1.0) + 2.0 * ns * nfd;
-        if (calc) E.stats->ts_pairs += (double)n * (double)(n - 1);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&E.stats->nodes), 1ull);
+        atomicMax(&E.stats->max_level, level);
+        atomicAdd(&E.stats->kick_pairs, ns * (ns - 1.0) + 2.0 * ns * nfd);
+        if (calc) atomicAdd(&E.stats->ts_pairs, (double)n * (double)(n - 1));
     }
 }
 
@@ -609,10 +621,218 @@ __device__ void kick_reduce_phase(const EParams& E, const int32_t* F, const int3
     (void)sm;
 }
 
+
+// ---------------------------------------------------------------- warp subtree solver
+// A subsystem of at most 32 particles, with its whole subtree, on one warp: one particle
+// per lane in registers (FP64 state), each level's subset a 32-bit lane mask, the split a
+// ballot (stable order = lane order; the N_fast == 1 fold keeps the lone lane and visits
+// it last among the slow sources), pair loops over set bits with the sources staged in
+// shared memory. No list, count or partial-sum traffic; state is written back once.
+// The FP64 form keeps the reference's summation order, so it stays bit-exact.
+__device__ __forceinline__ void warp_stage(Smem& sm, int lane, double x, double y, double z,
+                                           double vx, double vy, double vz, double m) {
+    sm.u.tsd.x[lane] = x; sm.u.tsd.y[lane] = y; sm.u.tsd.z[lane] = z;
+    sm.u.tsd.vx[lane] = vx; sm.u.tsd.vy[lane] = vy; sm.u.tsd.vz[lane] = vz;
+    sm.u.tsd.m[lane] = m;
+    __syncwarp();
+}
+
+template <int PREC>
+__device__ void warp_hold(const EParams& E, const int32_t* S, int n, int level0, bool calc0,
+                          Smem& sm) {
+    const int lane = threadIdx.x & 31;
+    const bool act = lane < n;
+    const int g = act ? list_at(S, lane) : 0;
+    const SoA& P = E.P;
+    double x = 0, y = 0, z = 0, vx = 0, vy = 0, vz = 0, m = 0, ts = 1.e30;
+    if (act) {
+        x = P.x[g]; y = P.y[g]; z = P.z[g];
+        vx = P.vx[g]; vy = P.vy[g]; vz = P.vz[g];
+        m = P.m[g]; ts = P.ts[g];
+    }
+    const unsigned top_mask = n >= 32 ? 0xffffffffu : ((1u << n) - 1u);
+    unsigned long long after1 = 0, after2 = 0, calcm = calc0 ? 1ull : 0ull;
+    bool ok = true;
+    int d = 0;
+    while (d >= 0) {
+        const int lvl = level0 + d;
+        const unsigned long long bit = 1ull << d;
+        const unsigned mask = d == 0 ? top_mask : sm.wfast[d - 1];
+        const bool in = (mask >> lane) & 1u;
+        const double dt = ldexp(E.dt_top, -lvl);
+        if (!(after1 & bit)) {
+            if (lvl >= E.max_levels || lvl >= kMaxLevels - 1) {
+                if (lane == 0) atomicOr(E.err, HHS_ERRBIT_DEPTH);
+                ok = false;
+                break;
+            }
+            const int cnt = __popc(mask);
+            if (calcm & bit) {
+                warp_stage(sm, lane, x, y, z, vx, vy, vz, m);
+                if (PREC == HHS_PREC_FP64) {
+                    double minval = 1.e30;
+                    for (unsigned mm = mask; mm; mm &= mm - 1u) {
+                        const int j = __ffs(mm) - 1;
+                        if (j == lane) continue;
+                        ts_pair_fp64(f64_sub(x, sm.u.tsd.x[j]), f64_sub(y, sm.u.tsd.y[j]),
+                                     f64_sub(z, sm.u.tsd.z[j]), f64_sub(vx, sm.u.tsd.vx[j]),
+                                     f64_sub(vy, sm.u.tsd.vy[j]), f64_sub(vz, sm.u.tsd.vz[j]), m,
+                                     sm.u.tsd.m[j], E.eta, E.eta_s2, minval);
+                    }
+                    if (in) ts = minval;
+                } else {
+                    const DS xi = ds_split(x), yi = ds_split(y), zi = ds_split(z);
+                    float maxrate = 0.0f;
+                    for (unsigned mm = mask; mm; mm &= mm - 1u) {
+                        const int j = __ffs(mm) - 1;
+                        if (j == lane) continue;
+                        const DS xj = ds_split(sm.u.tsd.x[j]), yj = ds_split(sm.u.tsd.y[j]),
+                                 zj = ds_split(sm.u.tsd.z[j]);
+                        const float r = ts_pair_rate_mixed(
+                            ds_diff(xi.hi, xi.lo, xj.hi, xj.lo), ds_diff(yi.hi, yi.lo, yj.hi, yj.lo),
+                            ds_diff(zi.hi, zi.lo, zj.hi, zj.lo), (float)vx - (float)sm.u.tsd.vx[j],
+                            (float)vy - (float)sm.u.tsd.vy[j], (float)vz - (float)sm.u.tsd.vz[j],
+                            (float)m + (float)sm.u.tsd.m[j], E.inv_eta_s2, E.inv_eta);
+                        maxrate = fmaxf(maxrate, r);
+                    }
+                    if (in) {
+                        const double tv = 1.0 / (double)maxrate;
+                        ts = tv < 1.e30 ? tv : 1.e30;
+                    }
+                }
+                __syncwarp();
+            }
+            unsigned F = __ballot_sync(HHS_FULL_MASK, in && ts <= dt);
+            int lone = -1;
+            if (__popc(F) == 1) { lone = __ffs(F) - 1; F = 0u; }
+            if (lane == 0) {
+                sm.wfast[d] = F;
+                sm.wlone[d] = lone;
+                const int nf = __popc(F);
+                const double ns = (double)(cnt - nf), nfd = (double)nf;
+                if (nf == 0) *E.leaf_time += dt;
+                atomicAdd(reinterpret_cast<unsigned long long*>(&E.stats->nodes), 1ull);
+                atomicMax(&E.stats->max_level, lvl);
+                atomicAdd(&E.stats->kick_pairs, ns * (ns - 1.0) + 2.0 * ns * nfd);
+                if (calcm & bit) atomicAdd(&E.stats->ts_pairs, (double)cnt * (double)(cnt - 1));
+            }
+            __syncwarp();
+            after1 |= bit;
+            if (F) {
+                d++;
+                const unsigned long long cb = 1ull << d;
+                calcm &= ~cb; after1 &= ~cb; after2 &= ~cb;
+                continue;
+            }
+        }
+        if (!(after2 & bit)) {
+            const unsigned F = sm.wfast[d];
+            const int lone = sm.wlone[d];
+            const unsigned L = mask & ~F;
+            const bool is_slow = (L >> lane) & 1u, is_fast = (F >> lane) & 1u;
+            const double h = dt * 0.5;
+            if (L) {
+                // first half drift of the slow lanes (src/hold.cuh:123-124)
+                if (is_slow) {
+                    if (PREC == HHS_PREC_FP64) {
+                        x = f64_add(x, f64_mul(vx, h)); y = f64_add(y, f64_mul(vy, h));
+                        z = f64_add(z, f64_mul(vz, h));
+                    } else {
+                        x = fma(vx, h, x); y = fma(vy, h, y); z = fma(vz, h, z);
+                    }
+                }
+                warp_stage(sm, lane, x, y, z, vx, vy, vz, m);
+                const unsigned Lord = lone >= 0 ? (L & ~(1u << lone)) : L;
+                if (PREC == HHS_PREC_FP64) {
+                    double aL[3] = {0, 0, 0}, aF[3] = {0, 0, 0};
+                    if (is_slow || is_fast) {
+                        for (unsigned mm = Lord; mm; mm &= mm - 1u) {
+                            const int j = __ffs(mm) - 1;
+                            kick_pair_fp64(f64_sub(sm.u.tsd.x[j], x), f64_sub(sm.u.tsd.y[j], y),
+                                           f64_sub(sm.u.tsd.z[j], z), sm.u.tsd.m[j], aL[0], aL[1],
+                                           aL[2]);
+                        }
+                        if (lone >= 0)
+                            kick_pair_fp64(f64_sub(sm.u.tsd.x[lone], x), f64_sub(sm.u.tsd.y[lone], y),
+                                           f64_sub(sm.u.tsd.z[lone], z), sm.u.tsd.m[lone], aL[0],
+                                           aL[1], aL[2]);
+                    }
+                    if (is_slow) {
+                        for (unsigned mm = F; mm; mm &= mm - 1u) {
+                            const int j = __ffs(mm) - 1;
+                            kick_pair_fp64(f64_sub(sm.u.tsd.x[j], x), f64_sub(sm.u.tsd.y[j], y),
+                                           f64_sub(sm.u.tsd.z[j], z), sm.u.tsd.m[j], aF[0], aF[1],
+                                           aF[2]);
+                        }
+                    }
+                    if (is_slow || is_fast) {
+                        const double v0x = vx, v0y = vy, v0z = vz;
+                        vx = f64_add(vx, f64_mul(aL[0], dt));
+                        vy = f64_add(vy, f64_mul(aL[1], dt));
+                        vz = f64_add(vz, f64_mul(aL[2], dt));
+                        if (is_slow && F) {
+                            vx = f64_add(vx, f64_mul(aF[0], dt));
+                            vy = f64_add(vy, f64_mul(aF[1], dt));
+                            vz = f64_add(vz, f64_mul(aF[2], dt));
+                        }
+                        (void)v0x; (void)v0y; (void)v0z;
+                    }
+                    if (is_slow) {
+                        x = f64_add(x, f64_mul(vx, h)); y = f64_add(y, f64_mul(vy, h));
+                        z = f64_add(z, f64_mul(vz, h));
+                    }
+                } else {
+                    const DS xi = ds_split(x), yi = ds_split(y), zi = ds_split(z);
+                    float a[3] = {0, 0, 0}, c[3] = {0, 0, 0};
+                    const unsigned srcs = is_slow ? (L | F) : (is_fast ? L : 0u);
+                    for (unsigned mm = srcs; mm; mm &= mm - 1u) {
+                        const int j = __ffs(mm) - 1;
+                        const DS xj = ds_split(sm.u.tsd.x[j]), yj = ds_split(sm.u.tsd.y[j]),
+                                 zj = ds_split(sm.u.tsd.z[j]);
+                        const float dx = ds_diff(xj.hi, xj.lo, xi.hi, xi.lo);
+                        const float dy = ds_diff(yj.hi, yj.lo, yi.hi, yi.lo);
+                        const float dz = ds_diff(zj.hi, zj.lo, zi.hi, zi.lo);
+                        const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        const float ri = rsqrt_nr(d2);
+                        const float mr3 = (d2 > 0.0f) ? (float)sm.u.tsd.m[j] * ri * ri * ri : 0.0f;
+                        kahan_add(a[0], c[0], dx * mr3);
+                        kahan_add(a[1], c[1], dy * mr3);
+                        kahan_add(a[2], c[2], dz * mr3);
+                    }
+                    if (is_slow || is_fast) {
+                        vx = fma((double)a[0] - (double)c[0], dt, vx);
+                        vy = fma((double)a[1] - (double)c[1], dt, vy);
+                        vz = fma((double)a[2] - (double)c[2], dt, vz);
+                    }
+                    if (is_slow) { x = fma(vx, h, x); y = fma(vy, h, y); z = fma(vz, h, z); }
+                }
+                __syncwarp();
+            }
+            after2 |= bit;
+            if (F) {
+                d++;
+                const unsigned long long cb = 1ull << d;
+                calcm = (calcm & ~cb) | cb;
+                after1 &= ~cb; after2 &= ~cb;
+                continue;
+            }
+        }
+        calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
+        d--;
+    }
+    (void)ok;
+    if (act) {
+        P.x[g] = x; P.y[g] = y; P.z[g] = z;
+        P.vx[g] = vx; P.vy[g] = vy; P.vz[g] = vz;
+        P.ts[g] = ts;
+    }
+}
+
 // ---------------------------------------------------------------- the recursion
 // Walks the HOLD recursion from `top` (whose subsystem is already defined by the
-// counts/lists above it). Grid mode delegates nodes with n <= small_n to CTA 0.
-template <int PREC, bool GRID>
+// counts/lists above it). Grid and cluster modes delegate nodes with n <= small_n,
+// with their whole subtree, to worker 0 alone.
+template <int PREC, int MODE>
 __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers& W, Smem& sm,
                          unsigned long long& t_last) {
     unsigned long long after1 = 0, after2 = 0, calcm = 0;  // per-level state bits
@@ -631,13 +851,21 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                 if (threadIdx.x == 0) atomicOr(E.err, HHS_ERRBIT_DEPTH);
                 return false;
             }
-            if (GRID && n <= E.small_n) {
+            if (n <= E.warp_n) {
+                if (W.id == 0 && (threadIdx.x >> 5) == 0) warp_hold<PREC>(E, S, n, lvl, calc, sm);
+                if (!phase_barrier(E, sm, W)) return false;
+                prof_mark(E, W, t_last, kProfSubtree, 0.0, lvl);
+                calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
+                lvl--;
+                continue;
+            }
+            if (MODE != kModeBlock && n <= E.small_n) {
                 if (W.id == 0) {
-                    const Workers one{0, 1, false};
+                    const Workers one{0, 1, kModeBlock};
                     unsigned long long t_sub = 0;
-                    run_hold<PREC, false>(E, lvl, calc, one, sm, t_sub);
+                    run_hold<PREC, kModeBlock>(E, lvl, calc, one, sm, t_sub);
                 }
-                if (!grid_barrier(E, sm)) return false;
+                if (!phase_barrier(E, sm, W)) return false;
                 prof_mark(E, W, t_last, kProfSubtree, 0.0, lvl);
                 calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
                 lvl--;
@@ -723,10 +951,95 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
 template <int PREC>
 __global__ void __launch_bounds__(kEB, 2) k_engine(EParams E) {
     __shared__ Smem sm;
-    const Workers W{(int)blockIdx.x, (int)gridDim.x, true};
+    const Workers W{(int)blockIdx.x, (int)gridDim.x, kModeGrid};
     unsigned long long t_last = 0;
     prof_mark(E, W, t_last, -1, 0.0);
-    run_hold<PREC, true>(E, 0, E.calc_top != 0, W, sm, t_last);
+    run_hold<PREC, kModeGrid>(E, 0, E.calc_top != 0, W, sm, t_last);
+}
+
+// ---------------------------------------------------------------- batched systems
+// Many independent systems packed back to back: the hardware clusters of the launch
+// first take the large systems from a queue ordered by decreasing size (each cluster
+// runs one system at a time with cluster barriers between phases), then every CTA takes
+// the remaining small systems one by one and solves each alone. Each worker group owns
+// a scratch slot (level lists, counts, partial sums) for the system it is running.
+struct Slot {
+    int32_t* fast_lists;
+    int32_t* slow_lists;
+    hhs_partition* counts;
+    double* ts_part;
+    double* k_part;
+    int* tile_counts;
+    unsigned* rate_acc;
+};
+
+struct BParams {
+    EParams E;               // common fields; per-system fields are filled in per system
+    const int32_t* offsets;  // [n_sys + 1]
+    const int32_t* order;    // systems by decreasing size
+    int n_sys, n_big;
+    unsigned* queues;        // [0] big-system queue, [1] small-system queue, [2 + c] broadcast
+    char* cluster_slots;
+    char* cta_slots;
+    size_t cluster_slot_bytes, cta_slot_bytes;
+    size_t off_lists, off_counts, off_ts, off_k, off_tiles, off_rate;
+    double* leaf_times;      // [n_sys]
+};
+
+__device__ __forceinline__ EParams system_params(const BParams& B, int sys, const char* slot) {
+    EParams E = B.E;
+    const int o = B.offsets[sys];
+    E.P.x += o; E.P.y += o; E.P.z += o;
+    E.P.vx += o; E.P.vy += o; E.P.vz += o;
+    E.P.m += o; E.P.ts += o; E.P.id += o;
+    E.n_top = B.offsets[sys + 1] - o;
+    char* p = const_cast<char*>(slot);
+    const size_t lists = (size_t)E.max_levels * E.n_max;
+    E.fast_lists = reinterpret_cast<int32_t*>(p + B.off_lists);
+    E.slow_lists = E.fast_lists + lists;
+    E.counts = reinterpret_cast<hhs_partition*>(p + B.off_counts);
+    E.ts_part = reinterpret_cast<double*>(p + B.off_ts);
+    E.k_part = reinterpret_cast<double*>(p + B.off_k);
+    E.tile_counts = reinterpret_cast<int*>(p + B.off_tiles);
+    E.rate_acc = reinterpret_cast<unsigned*>(p + B.off_rate);
+    E.leaf_time = B.leaf_times + sys;
+    return E;
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(kEB, 2) k_batched(BParams B) {
+    __shared__ Smem sm;
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int cs = (int)cluster.num_blocks();
+    const int rank = (int)cluster.block_rank();
+    const int cid = (int)(blockIdx.x / cs);
+    unsigned long long t = 0;
+    // large systems: one hardware cluster per system
+    while (true) {
+        if (rank == 0 && threadIdx.x == 0)
+            *reinterpret_cast<volatile unsigned*>(&B.queues[2 + cid]) = atomicAdd(&B.queues[0], 1u);
+        cluster.sync();
+        const int idx = (int)*reinterpret_cast<volatile unsigned*>(&B.queues[2 + cid]);
+        cluster.sync();
+        if (idx >= B.n_big) break;
+        const int sys = B.order[idx];
+        const EParams E = system_params(B, sys, B.cluster_slots + (size_t)cid * B.cluster_slot_bytes);
+        const Workers W{rank, cs, kModeCluster};
+        run_hold<PREC, kModeCluster>(E, 0, E.calc_top != 0, W, sm, t);
+    }
+    // small systems: one CTA per system
+    while (true) {
+        if (threadIdx.x == 0) sm.bcast = (int)atomicAdd(&B.queues[1], 1u);
+        __syncthreads();
+        const int idx = sm.bcast;
+        __syncthreads();
+        if (idx >= B.n_sys - B.n_big) break;
+        const int sys = B.order[B.n_big + idx];
+        const EParams E = system_params(B, sys, B.cta_slots + (size_t)blockIdx.x * B.cta_slot_bytes);
+        const Workers W{0, 1, kModeBlock};
+        run_hold<PREC, kModeBlock>(E, 0, E.calc_top != 0, W, sm, t);
+    }
 }
 
 struct EngineHost {
@@ -735,6 +1048,7 @@ struct EngineHost {
     int ctas_per_sm = 2;
     int small_n = 256;
     int units_per_cta = 8;
+    int warp_n = 32;
     EngineState* st = nullptr;
     double* ts_part = nullptr;
     double* k_part = nullptr;
@@ -793,8 +1107,9 @@ void engine_destroy(hhs_ctx* c) {
 hhs_status engine_set_tuning(hhs_ctx* c, const hhs_tuning& t) {
     auto* eh = static_cast<EngineHost*>(c->engine_host);
     if (!eh || t.small_n < 0 || t.units_per_cta < 1 || t.units_per_cta > 64 ||
-        t.ctas_per_sm < 1 || t.ctas_per_sm > 2)
+        t.ctas_per_sm < 1 || t.ctas_per_sm > 2 || t.warp_n < 0 || t.warp_n > 32)
         return HHS_ERR_INVALID_ARG;
+    eh->warp_n = t.warp_n;
     eh->small_n = t.small_n;
     eh->units_per_cta = t.units_per_cta;
     eh->ctas_per_sm = t.ctas_per_sm;
@@ -809,6 +1124,7 @@ hhs_status engine_get_tuning(hhs_ctx* c, hhs_tuning* t) {
     t->small_n = eh->small_n;
     t->units_per_cta = eh->units_per_cta;
     t->ctas_per_sm = eh->ctas_per_sm;
+    t->warp_n = eh->warp_n;
     return HHS_OK;
 }
 
@@ -861,6 +1177,7 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
     E.max_levels = c->max_levels < kMaxLevels - 1 ? c->max_levels : kMaxLevels - 1;
     E.small_n = eh->small_n;
     E.units_per_cta = eh->units_per_cta;
+    E.warp_n = eh->warp_n;
     E.calc_top = calc_ts ? 1 : 0;
     E.profile = profile ? 1 : 0;
     E.dt_top = dt;
@@ -890,5 +1207,246 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
                                         args, 0, stream);
     hhs_count_launch();
     if (e != cudaSuccess) return hhs_from_cuda(e);
+    return HHS_OK;
+}
+
+// ------------------------------------------------------------------ batched host side
+struct hhs_batch {
+    int n_sys = 0, n_total = 0, n_max_sys = 0, max_levels = 0;
+    hhs_params params{0.03, 0.0};
+    int big_n = 1024, cluster_size = 8, small_n = 64, units_per_cta = 8, warp_n = 32;
+    int n_big = 0, n_clusters[2] = {0, 0};
+    void* arena = nullptr;
+    int32_t* d_offsets = nullptr;
+    int32_t* d_order = nullptr;
+    unsigned* d_queues = nullptr;
+    double* d_leaf = nullptr;
+    hhs_stats* d_stats = nullptr;
+    unsigned* d_err = nullptr;
+    char* cluster_slots = nullptr;
+    char* cta_slots = nullptr;
+    size_t cluster_slot_bytes = 0, cta_slot_bytes = 0;
+    size_t off_lists = 0, off_counts = 0, off_ts = 0, off_k = 0, off_tiles = 0, off_rate = 0;
+    int max_clusters = 0, max_ctas = 0;
+    std::vector<int> sizes, order;
+};
+
+namespace {
+template <int PREC>
+cudaError_t batched_occupancy(int cs, int* clusters) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs, 1, 1);
+    cfg.blockDim = dim3(kEB, 1, 1);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaOccupancyMaxActiveClusters(clusters, (void*)k_batched<PREC>, &cfg);
+}
+
+size_t slot_layout(int n, int levels, int chunks, size_t* off) {
+    size_t p = 0;
+    off[0] = p; p += al(sizeof(int32_t) * 2 * (size_t)levels * n);          // lists
+    off[1] = p; p += al(sizeof(hhs_partition) * (size_t)levels);            // counts
+    off[2] = p; p += al(sizeof(double) * (size_t)chunks * n);               // ts partials
+    off[3] = p; p += al(sizeof(double) * (size_t)(chunks * 3 > 6 ? chunks * 3 : 6) * n);
+    off[4] = p; p += al(sizeof(int) * (size_t)(n / kEB + 2));               // tile counts
+    off[5] = p; p += al(sizeof(unsigned) * (size_t)n);                      // rate_acc
+    return p;
+}
+}  // namespace
+
+extern "C" hhs_status hhs_batch_create(int32_t n_sys, const int32_t* offsets, int32_t max_levels,
+                                       hhs_params params, hhs_batch** out) {
+    if (!out || n_sys <= 0 || !offsets || max_levels <= 0 || !(params.eta > 0.0))
+        return HHS_ERR_INVALID_ARG;
+    *out = nullptr;
+    auto* b = new (std::nothrow) hhs_batch();
+    if (!b) return HHS_ERR_OOM;
+    b->n_sys = n_sys;
+    b->max_levels = max_levels < kMaxLevels - 1 ? max_levels : kMaxLevels - 1;
+    b->params = params;
+    b->sizes.resize(n_sys);
+    if (offsets[0] != 0) { delete b; return HHS_ERR_INVALID_ARG; }
+    for (int k = 0; k < n_sys; k++) {
+        const int sz = offsets[k + 1] - offsets[k];
+        if (sz <= 0) { delete b; return HHS_ERR_INVALID_ARG; }
+        b->sizes[k] = sz;
+        b->n_max_sys = sz > b->n_max_sys ? sz : b->n_max_sys;
+    }
+    b->n_total = offsets[n_sys];
+    b->order.resize(n_sys);
+    std::iota(b->order.begin(), b->order.end(), 0);
+    std::stable_sort(b->order.begin(), b->order.end(),
+                     [&](int a, int c) { return b->sizes[a] > b->sizes[c]; });
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int c0 = 0, c1 = 0;
+    if (batched_occupancy<HHS_PREC_FP64>(b->cluster_size, &c0) != cudaSuccess ||
+        batched_occupancy<HHS_PREC_MIXED>(b->cluster_size, &c1) != cudaSuccess || c0 <= 0 ||
+        c1 <= 0) {
+        delete b;
+        return HHS_ERR_CUDA;
+    }
+    b->n_clusters[0] = c0;
+    b->n_clusters[1] = c1;
+    b->max_clusters = c0 > c1 ? c0 : c1;
+    b->max_ctas = b->max_clusters * b->cluster_size;
+    size_t offc[6], offs[6];
+    b->cluster_slot_bytes = slot_layout(b->n_max_sys, b->max_levels, kMaxChunks, offc);
+    b->cta_slot_bytes = slot_layout(b->n_max_sys, b->max_levels, 1, offs);
+    // both slot kinds use the same offsets up to their own sizes: lists and counts first
+    b->off_lists = offc[0]; b->off_counts = offc[1];
+    // offsets beyond counts differ; keep the larger (cluster) layout for both
+    b->cta_slot_bytes = b->cluster_slot_bytes;
+    b->off_ts = offc[2]; b->off_k = offc[3]; b->off_tiles = offc[4]; b->off_rate = offc[5];
+    (void)offs;
+    const size_t head = al(sizeof(int32_t) * (n_sys + 1)) + al(sizeof(int32_t) * n_sys) +
+                        al(sizeof(unsigned) * (2 + b->max_clusters)) + al(sizeof(double) * n_sys) +
+                        al(sizeof(hhs_stats)) + al(sizeof(unsigned));
+    const size_t total = head + b->cluster_slot_bytes * (size_t)b->max_clusters +
+                         b->cta_slot_bytes * (size_t)b->max_ctas;
+    cudaError_t e = cudaMalloc(&b->arena, total);
+    if (e != cudaSuccess) { delete b; return hhs_from_cuda(e); }
+    e = cudaMemset(b->arena, 0, total);
+    char* p = static_cast<char*>(b->arena);
+    b->d_offsets = reinterpret_cast<int32_t*>(p); p += al(sizeof(int32_t) * (n_sys + 1));
+    b->d_order = reinterpret_cast<int32_t*>(p); p += al(sizeof(int32_t) * n_sys);
+    b->d_queues = reinterpret_cast<unsigned*>(p); p += al(sizeof(unsigned) * (2 + b->max_clusters));
+    b->d_leaf = reinterpret_cast<double*>(p); p += al(sizeof(double) * n_sys);
+    b->d_stats = reinterpret_cast<hhs_stats*>(p); p += al(sizeof(hhs_stats));
+    b->d_err = reinterpret_cast<unsigned*>(p); p += al(sizeof(unsigned));
+    b->cluster_slots = p; p += b->cluster_slot_bytes * (size_t)b->max_clusters;
+    b->cta_slots = p;
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_offsets, offsets, sizeof(int32_t) * (n_sys + 1), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_order, b->order.data(), sizeof(int32_t) * n_sys, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { cudaFree(b->arena); delete b; return hhs_from_cuda(e); }
+    for (int k = 0; k < n_sys; k++)
+        if (b->sizes[b->order[k]] > b->big_n) b->n_big = k + 1;
+    *out = b;
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_batch_destroy(hhs_batch* b) {
+    if (!b) return HHS_ERR_INVALID_ARG;
+    cudaError_t e = cudaFree(b->arena);
+    delete b;
+    return hhs_from_cuda(e);
+}
+
+extern "C" hhs_status hhs_batch_set_tuning(hhs_batch* b, int32_t big_n, int32_t small_n,
+                                           int32_t units_per_cta) {
+    if (!b || big_n < 0 || small_n < 0 || units_per_cta < 1 || units_per_cta > 64)
+        return HHS_ERR_INVALID_ARG;
+    b->big_n = big_n;
+    b->small_n = small_n;
+    b->units_per_cta = units_per_cta;
+    b->n_big = 0;
+    for (int k = 0; k < b->n_sys; k++)
+        if (b->sizes[b->order[k]] > b->big_n) b->n_big = k + 1;
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, double dt,
+                                       int32_t calc_timestep, hhs_precision prec, void* stream) {
+    if (!b || !sys || !sys->_base || !(dt > 0.0)) return HHS_ERR_INVALID_ARG;
+    if (b->n_total > sys->n) return HHS_ERR_CAPACITY;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int pi = prec == HHS_PREC_FP64 ? 0 : 1;
+    const int nclu = b->n_clusters[pi];
+    HHS_CUDA_TRY(cudaMemsetAsync(b->d_queues, 0, sizeof(unsigned) * (2 + nclu), s));
+    BParams B;
+    EParams& E = B.E;
+    E.P.x = sys->x; E.P.y = sys->y; E.P.z = sys->z;
+    E.P.vx = sys->vx; E.P.vy = sys->vy; E.P.vz = sys->vz;
+    E.P.m = sys->m; E.P.ts = sys->ts; E.P.id = sys->id;
+    E.n_top = 0;
+    E.n_max = b->n_max_sys;
+    E.max_levels = b->max_levels;
+    E.small_n = b->small_n;
+    E.calc_top = calc_timestep ? 1 : 0;
+    E.profile = 0;
+    E.units_per_cta = b->units_per_cta;
+    E.warp_n = b->warp_n;
+    E.dt_top = dt;
+    E.eta = b->params.eta;
+    E.eta_s2 = b->params.eta / 1.41421356237309504880;
+    E.inv_eta_s2 = (float)(1.0 / E.eta_s2);
+    E.inv_eta = (float)(1.0 / E.eta);
+    E.fast_lists = E.slow_lists = nullptr;
+    E.counts = nullptr;
+    E.leaf_time = nullptr;
+    E.stats = b->d_stats;
+    E.ts_part = E.k_part = nullptr;
+    E.tile_counts = nullptr;
+    E.rate_acc = nullptr;
+    E.st = nullptr;
+    E.err = b->d_err;
+    B.offsets = b->d_offsets;
+    B.order = b->d_order;
+    B.n_sys = b->n_sys;
+    B.n_big = b->n_big;
+    B.queues = b->d_queues;
+    B.cluster_slots = b->cluster_slots;
+    B.cta_slots = b->cta_slots;
+    B.cluster_slot_bytes = b->cluster_slot_bytes;
+    B.cta_slot_bytes = b->cta_slot_bytes;
+    B.off_lists = b->off_lists; B.off_counts = b->off_counts; B.off_ts = b->off_ts;
+    B.off_k = b->off_k; B.off_tiles = b->off_tiles; B.off_rate = b->off_rate;
+    B.leaf_times = b->d_leaf;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nclu * b->cluster_size, 1, 1);
+    cfg.blockDim = dim3(kEB, 1, 1);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = b->cluster_size;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaError_t e = pi == 0 ? cudaLaunchKernelEx(&cfg, k_batched<HHS_PREC_FP64>, B)
+                            : cudaLaunchKernelEx(&cfg, k_batched<HHS_PREC_MIXED>, B);
+    hhs_count_launch();
+    return hhs_from_cuda(e);
+}
+
+extern "C" hhs_status hhs_batch_get_simtime(hhs_batch* b, double* out, void* stream) {
+    if (!b || !out) return HHS_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    HHS_CUDA_TRY(cudaMemcpyAsync(out, b->d_leaf, sizeof(double) * b->n_sys, cudaMemcpyDeviceToHost, s));
+    HHS_CUDA_TRY(cudaStreamSynchronize(s));
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_batch_get_stats(hhs_batch* b, hhs_stats* out, void* stream) {
+    if (!b || !out) return HHS_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    HHS_CUDA_TRY(cudaMemcpyAsync(out, b->d_stats, sizeof(hhs_stats), cudaMemcpyDeviceToHost, s));
+    HHS_CUDA_TRY(cudaStreamSynchronize(s));
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_batch_reset_stats(hhs_batch* b, void* stream) {
+    if (!b) return HHS_ERR_INVALID_ARG;
+    HHS_CUDA_TRY(cudaMemsetAsync(b->d_stats, 0, sizeof(hhs_stats), static_cast<cudaStream_t>(stream)));
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_batch_check(hhs_batch* b, void* stream) {
+    if (!b) return HHS_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    HHS_CUDA_TRY(cudaStreamSynchronize(s));
+    unsigned e = 0;
+    HHS_CUDA_TRY(cudaMemcpy(&e, b->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (e & (HHS_ERRBIT_LOOKBACK_TIMEOUT | HHS_ERRBIT_BARRIER_TIMEOUT)) return HHS_ERR_TIMEOUT;
+    if (e & HHS_ERRBIT_DEPTH) return HHS_ERR_DEPTH;
+    if (e) return HHS_ERR_DEVICE_FAULT_FLAG;
     return HHS_OK;
 }

@@ -54,6 +54,61 @@ __global__ void __launch_bounds__(kScanBlock)
     if (scan_finish_is_last(hdr, num_tiles, &s_last)) scan_reset(hdr, epoch);
 }
 
+// Stream compaction of int32 flags: the indices of the nonzero flags, in order, go to
+// idx_out[scan]; the exclusive scan of (flag != 0) optionally goes to scan_out; the last
+// CTA writes the number of selected elements to *count.
+template <bool VEC>
+__global__ void __launch_bounds__(kScanBlock)
+    k_compact_flags(const int32_t* __restrict__ flags, int32_t* __restrict__ scan_out,
+                    int32_t* __restrict__ idx_out, int32_t* __restrict__ count, long long n,
+                    ScanHeader* hdr, unsigned long long* status, int num_tiles) {
+    __shared__ int s_tile;
+    __shared__ unsigned s_epoch, s_prefix;
+    __shared__ unsigned s_warp[ScanT::WARPS];
+    __shared__ int s_last;
+    scan_begin(hdr, &s_tile, &s_epoch);
+    const int tile = s_tile;
+    const unsigned epoch = s_epoch;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long tbase = (long long)tile * ScanT::TILE;
+    unsigned v[kScanItems], ex[kScanItems];
+#pragma unroll
+    for (int c = 0; c < ScanT::CHUNKS; c++) {
+        const long long e = tbase + ScanT::offset(warp, c, lane);
+        if (VEC && e + 4 <= n) {
+            const int4 q = __ldcs(reinterpret_cast<const int4*>(flags + e));
+            v[4 * c] = q.x != 0; v[4 * c + 1] = q.y != 0;
+            v[4 * c + 2] = q.z != 0; v[4 * c + 3] = q.w != 0;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) v[4 * c + k] = (e + k < n) ? (flags[e + k] != 0) : 0u;
+        }
+    }
+    ScanT::scan(v, ex, status, tile, epoch, &hdr->error, s_warp, &s_prefix);
+#pragma unroll
+    for (int c = 0; c < ScanT::CHUNKS; c++) {
+        const long long e = tbase + ScanT::offset(warp, c, lane);
+        if (scan_out) {
+            if (VEC && e + 4 <= n) {
+                __stcs(reinterpret_cast<int4*>(scan_out + e),
+                       make_int4((int)ex[4 * c], (int)ex[4 * c + 1], (int)ex[4 * c + 2],
+                                 (int)ex[4 * c + 3]));
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (e + k < n) scan_out[e + k] = (int)ex[4 * c + k];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (v[4 * c + k]) idx_out[ex[4 * c + k]] = (int)(e + k);
+    }
+    if (scan_finish_is_last(hdr, num_tiles, &s_last)) {
+        if (threadIdx.x == 0) *count = (int)(unsigned)ld_relaxed_u64(&status[num_tiles - 1]);
+        scan_reset(hdr, epoch);
+    }
+}
+
 constexpr int kSplitBlock = 256;
 constexpr int kSplitItems = 8;  // 2048 particles per tile
 using SplitT = TileScan<kSplitBlock, kSplitItems>;
@@ -194,6 +249,37 @@ extern "C" hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out
     else
         k_scan_exclusive_i32<false><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n, hdr, status,
                                                                  tiles);
+    HHS_LAUNCH_CHECK();
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_compact_flags_i32(const int32_t* d_flags, int32_t* d_scan,
+                                            int32_t* d_idx, int32_t* d_count, int64_t n,
+                                            void* d_workspace, size_t workspace_bytes,
+                                            void* stream) {
+    if (n < 0 || (n > 0 && (!d_flags || !d_idx || !d_count || !d_workspace)))
+        return HHS_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (n == 0) {
+        HHS_CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(int32_t), s));
+        return HHS_OK;
+    }
+    if (n > (int64_t)0x7fffffff) return HHS_ERR_INVALID_ARG;
+    if (workspace_bytes < hhs_scan_workspace_size(n)) return HHS_ERR_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(d_workspace) & 7u) != 0) return HHS_ERR_INVALID_ARG;
+    const int tiles = (int)((n + ScanT::TILE - 1) / ScanT::TILE);
+    HHS_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, scan_workspace_bytes(n, ScanT::TILE), s));
+    auto* hdr = static_cast<ScanHeader*>(d_workspace);
+    auto* status = reinterpret_cast<unsigned long long*>(static_cast<char*>(d_workspace) +
+                                                         sizeof(ScanHeader));
+    const bool vec = ((reinterpret_cast<uintptr_t>(d_flags) |
+                       reinterpret_cast<uintptr_t>(d_scan)) & 15u) == 0;
+    if (vec)
+        k_compact_flags<true><<<tiles, kScanBlock, 0, s>>>(d_flags, d_scan, d_idx, d_count, n,
+                                                           hdr, status, tiles);
+    else
+        k_compact_flags<false><<<tiles, kScanBlock, 0, s>>>(d_flags, d_scan, d_idx, d_count, n,
+                                                            hdr, status, tiles);
     HHS_LAUNCH_CHECK();
     return HHS_OK;
 }

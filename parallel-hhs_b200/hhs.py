@@ -60,7 +60,7 @@ PROFILE_KINDS = ("timesteps", "kick", "split", "drift", "engine", "k5", "k6", "k
 
 class Tuning(ctypes.Structure):
     _fields_ = [("small_n", ctypes.c_int32), ("units_per_cta", ctypes.c_int32),
-                ("ctas_per_sm", ctypes.c_int32), ("_pad", ctypes.c_int32),
+                ("ctas_per_sm", ctypes.c_int32), ("warp_n", ctypes.c_int32),
                 ("ms_per_step", ctypes.c_double)]
 
 
@@ -115,6 +115,8 @@ SIGNATURES = {
     "hhs_scan_exclusive_i32": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp, ctypes.c_size_t,
                                               _vp]),
     "hhs_scan_workspace_status": (ctypes.c_int, [_vp, _vp]),
+    "hhs_compact_flags_i32": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int64, _vp,
+                                             ctypes.c_size_t, _vp]),
     "hhs_ic_plummer": (ctypes.c_int, [ctypes.c_int32, ctypes.c_uint64, ctypes.c_int32]
                        + [_dp] * 7),
     "hhs_host_potential_energy": (ctypes.c_double, [ctypes.c_int32] + [_dp] * 4),
@@ -127,6 +129,16 @@ SIGNATURES = {
     "hhs_ctx_get_level_profile": (ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_uint64)]),
     "hhs_kernel_launch_count": (ctypes.c_uint64, []),
     "hhs_measure_fma_peaks": (ctypes.c_int, [_dp, _dp, _vp]),
+    "hhs_batch_create": (ctypes.c_int, [ctypes.c_int32, _ip, ctypes.c_int32, Params,
+                                        ctypes.POINTER(_vp)]),
+    "hhs_batch_destroy": (ctypes.c_int, [_vp]),
+    "hhs_batch_set_tuning": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    "hhs_hold_batched": (ctypes.c_int, [_vp, ctypes.POINTER(CParticleSystem), ctypes.c_double,
+                                        ctypes.c_int32, ctypes.c_int, _vp]),
+    "hhs_batch_get_simtime": (ctypes.c_int, [_vp, _dp, _vp]),
+    "hhs_batch_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(Stats), _vp]),
+    "hhs_batch_reset_stats": (ctypes.c_int, [_vp, _vp]),
+    "hhs_batch_check": (ctypes.c_int, [_vp, _vp]),
     "hhs_ctx_set_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(Tuning)]),
     "hhs_ctx_get_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(Tuning)]),
     "hhs_ctx_autotune": (ctypes.c_int, [_vp, ctypes.POINTER(CParticleSystem), ctypes.c_int32,
@@ -257,7 +269,7 @@ class Context:
     def reset_stats(self, stream=None):
         _check(lib().hhs_ctx_reset_stats(self.h, stream), "reset_stats")
 
-    def set_tuning(self, small_n=None, units_per_cta=None, ctas_per_sm=None):
+    def set_tuning(self, small_n=None, units_per_cta=None, ctas_per_sm=None, warp_n=None):
         t = Tuning()
         _check(lib().hhs_ctx_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
         if small_n is not None:
@@ -266,20 +278,22 @@ class Context:
             t.units_per_cta = units_per_cta
         if ctas_per_sm is not None:
             t.ctas_per_sm = ctas_per_sm
+        if warp_n is not None:
+            t.warp_n = warp_n
         _check(lib().hhs_ctx_set_tuning(self.h, ctypes.byref(t)), "set_tuning")
 
     def tuning(self):
         t = Tuning()
         _check(lib().hhs_ctx_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
         return {"small_n": t.small_n, "units_per_cta": t.units_per_cta,
-                "ctas_per_sm": t.ctas_per_sm}
+                "ctas_per_sm": t.ctas_per_sm, "warp_n": t.warp_n}
 
     def autotune(self, sys, n, dt, prec=1, stream=None):
         t = Tuning()
         _check(lib().hhs_ctx_autotune(self.h, sys.ref, n, dt, prec, ctypes.byref(t), stream),
                "autotune")
         return {"small_n": t.small_n, "units_per_cta": t.units_per_cta,
-                "ctas_per_sm": t.ctas_per_sm, "ms_per_step": t.ms_per_step}
+                "ctas_per_sm": t.ctas_per_sm, "warp_n": t.warp_n, "ms_per_step": t.ms_per_step}
 
     def set_profiling(self, on):
         _check(lib().hhs_ctx_set_profiling(self.h, int(on)), "set_profiling")
@@ -301,6 +315,53 @@ class Context:
     def destroy(self):
         if self.h:
             _check(lib().hhs_ctx_destroy(self.h), "hhs_ctx_destroy")
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many independent systems in one particle system (hhs_batch)."""
+
+    def __init__(self, offsets, max_levels=64, eta=0.03, eps=0.0):
+        off = np.ascontiguousarray(offsets, dtype=np.int32)
+        self.n_sys = len(off) - 1
+        self.offsets = off
+        self.h = _vp()
+        _check(lib().hhs_batch_create(self.n_sys, _i(off), max_levels, Params(eta, eps),
+                                      ctypes.byref(self.h)), "hhs_batch_create")
+
+    def set_tuning(self, big_n=1024, small_n=64, units_per_cta=8):
+        _check(lib().hhs_batch_set_tuning(self.h, big_n, small_n, units_per_cta), "batch tuning")
+
+    def step(self, sys, dt, calc_timestep=True, prec=PREC_MIXED, stream=None):
+        _check(lib().hhs_hold_batched(self.h, sys.ref, dt, int(calc_timestep), prec, stream),
+               "hhs_hold_batched")
+
+    def check(self, stream=None):
+        _check(lib().hhs_batch_check(self.h, stream), "hhs_batch_check")
+
+    def simtime(self, stream=None):
+        out = np.zeros(self.n_sys)
+        _check(lib().hhs_batch_get_simtime(self.h, _d(out), stream), "batch simtime")
+        return out
+
+    def stats(self, stream=None):
+        st = Stats()
+        _check(lib().hhs_batch_get_stats(self.h, ctypes.byref(st), stream), "batch stats")
+        return {"nodes": st.nodes, "max_level": st.max_level, "kick_pairs": st.kick_pairs,
+                "ts_pairs": st.ts_pairs}
+
+    def reset_stats(self, stream=None):
+        _check(lib().hhs_batch_reset_stats(self.h, stream), "batch reset_stats")
+
+    def destroy(self):
+        if self.h:
+            _check(lib().hhs_batch_destroy(self.h), "hhs_batch_destroy")
             self.h = _vp()
 
     def __del__(self):
@@ -365,6 +426,11 @@ def scan_workspace_size(n):
 def scan_exclusive_i32(d_in, d_out, n, d_ws, ws_bytes, stream=None):
     _check(lib().hhs_scan_exclusive_i32(d_in, d_out, n, d_ws, ws_bytes, stream),
            "hhs_scan_exclusive_i32")
+
+
+def compact_flags_i32(d_flags, d_scan, d_idx, d_count, n, d_ws, ws_bytes, stream=None):
+    _check(lib().hhs_compact_flags_i32(d_flags, d_scan, d_idx, d_count, n, d_ws, ws_bytes,
+                                       stream), "hhs_compact_flags_i32")
 
 
 def scan_workspace_status(d_ws, stream=None):

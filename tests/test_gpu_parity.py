@@ -466,3 +466,88 @@ def test_autotune_restores_state_and_keeps_results(cuda, hhs, oracle):
     out = d.download()
     for k in FIELDS:
         assert np.array_equal(out[k], ref[k]), k
+
+
+@pytest.mark.parametrize("n,p", [(1, 1.0), (5, 0.5), (4097, 0.01), (100003, 0.5),
+                                 ((1 << 20) + 5, 0.1)])
+def test_compact_flags_matches_oracle(cuda, hhs, oracle, n, p):
+    torch = cuda
+    rng = np.random.default_rng(n)
+    flags = (rng.random(n) < p).astype(np.int32) * rng.integers(1, 5, n).astype(np.int32)
+    dev = torch.from_numpy(flags).cuda()
+    scan = torch.empty_like(dev)
+    idx = torch.full_like(dev, -1)
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ws_bytes = hhs.scan_workspace_size(n)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+    hhs.compact_flags_i32(_ptr(dev), _ptr(scan), _ptr(idx), _ptr(cnt), n, _ptr(ws), ws_bytes,
+                          ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    pred = (flags != 0).astype(np.int32)
+    k = int(cnt.item())
+    assert k == pred.sum()
+    assert np.array_equal(scan.cpu().numpy(), oracle.scan_exclusive(pred))
+    order, _ = oracle.split(np.where(pred == 1, 0.0, 1.0), 0.5)
+    if k != 1:
+        assert np.array_equal(idx.cpu().numpy()[:k], order[:k])
+    else:
+        assert idx.cpu().numpy()[0] == np.nonzero(pred)[0][0]
+
+
+@pytest.mark.parametrize("warp_n,small_n", [(32, 0), (0, 0), (32, 256), (16, 100000)])
+def test_engine_warp_solver_fp64_bit_exact(cuda, hhs, oracle, warp_n, small_n):
+    n = 700
+    s = _plummer(hhs, n, 55)
+    ref = {k: v.copy() for k, v in s.items()}
+    ctx = hhs.Context(n, 64, eta=0.03)
+    ctx.set_tuning(small_n=small_n, warp_n=warp_n)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    nodes = 0
+    for _ in range(2):
+        hhs.hold_step(ctx, d, n, 0.0, 1.0 / 64, True, hhs.PREC_FP64)
+        tr, _ = oracle.hold_step(ref, 1.0 / 64, True, 0.03)
+        nodes += tr.count
+    ctx.check()
+    out = d.download()
+    for k in FIELDS:
+        assert np.array_equal(out[k], ref[k]), k
+    assert ctx.stats()["nodes"] == nodes
+
+
+def _packed(hhs, sizes, seed0):
+    parts = [hhs.plummer(nk, seed0 + k) for k, nk in enumerate(sizes)]
+    packed = {f: np.concatenate([p[f] for p in parts]) for f in FIELDS}
+    packed["id"] = np.arange(sum(sizes), dtype=np.int32)
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    return parts, packed, offsets
+
+
+@pytest.mark.parametrize("sizes,big_n,prec", [
+    ([64, 100, 33, 2, 500, 1500, 3000, 7, 260], 1024, 0),
+    ([300] * 12 + [2000] * 3, 128, 0),
+    ([64, 100, 33, 2, 500, 1500, 3000, 7, 260], 1024, 1)])
+def test_hold_batched_matches_per_system_oracle(cuda, hhs, oracle, sizes, big_n, prec):
+    parts, packed, offsets = _packed(hhs, sizes, 300)
+    n = int(offsets[-1])
+    d = hhs.ParticleSystem(n)
+    d.upload(packed)
+    b = hhs.Batch(offsets, 64, eta=0.03)
+    b.set_tuning(big_n, 64, 8)
+    dt = 1.0 / 64
+    leaf = np.zeros(len(sizes))
+    for _ in range(2):
+        b.step(d, dt, True, prec)
+        for k, p in enumerate(parts):
+            tr, _ = oracle.hold_step(p, dt, True, 0.03)
+            leaf[k] += tr.leaf_time
+    b.check()
+    out = d.download()
+    for k, p in enumerate(parts):
+        sl = slice(offsets[k], offsets[k + 1])
+        for f in FIELDS:
+            if prec == 0:
+                assert np.array_equal(out[f][sl], p[f]), (k, f)
+            elif f in ("x", "y", "z"):
+                assert np.max(np.abs(out[f][sl] - p[f])) < 1e-7, (k, f)
+    assert np.allclose(b.simtime(), leaf, rtol=1e-15, atol=0)
