@@ -50,6 +50,13 @@ def parse():
                    help="pick the device-schedule tuning with the library's autotuner")
     p.add_argument("--profile-out", default=None,
                    help="write the per-level phase profile (JSON) to this path")
+    p.add_argument("--workload", default="plummer16k",
+                   choices=["plummer16k", "batched", "scan", "large", "deep"],
+                   help="plummer16k (default headline), batched (512 clusters), scan (flag "
+                        "compaction sweep), large (N=262144, 90/10 masses), deep (N=65536 "
+                        "Salpeter)")
+    p.add_argument("--scan-log2n", type=int, default=None,
+                   help="scan workload: run this one size instead of the 2^20..2^28 sweep")
     p.add_argument("--no-baselines", action="store_true",
                    help="skip the FP64 GPU and CPU baselines (quick runs)")
     return p.parse_args()
@@ -152,7 +159,7 @@ def run_ours(a, rank, world, torch, dist):
     sh = ctypes.c_void_p(stream.cuda_stream)
     prec = hhs.PREC_MIXED if a.prec == "mixed" else hhs.PREC_FP64
     seed = a.seed + 7919 * rank
-    ics = hhs.plummer(a.n, seed)
+    ics = hhs.plummer(a.n, seed, getattr(a, "mass", 0))
     e0 = hhs.energy_host(ics)
     ctx = hhs.Context(a.n, 64, eta=a.eta)
     ctx.set_tuning(a.small_n, a.units_per_cta, a.ctas_per_sm)
@@ -200,7 +207,7 @@ def run_ours(a, rank, world, torch, dist):
         prof = ctx.profile()
         if a.profile_out and a.schedule == "auto":
             lms, lcnt = ctx.level_profile()
-            kinds = ["timesteps", "kick", "split", "update", "engine", "subtree", "k6", "k7"]
+            kinds = ["timesteps", "kick", "split", "update", "engine", "subtree", "cluster_node", "k7"]
             lp = {kinds[k]: {str(l): [round(float(lms[k, l]) / a.steps, 4), int(lcnt[k, l]) // a.steps]
                              for l in range(64) if lcnt[k, l]} for k in range(8)}
             with open(a.profile_out, "w") as f:
@@ -324,6 +331,157 @@ def roofline(res, a, peaks_tflops):
             "share_of_step": p["ms"] / res["t_ms"], "traffic": None}
 
 
+# ------------------------------------------------------------------------ other workloads
+def run_batched(a, torch):
+    """512 independent Plummer clusters, N log-uniform in [64, 4096], one launch per step."""
+    import numpy as np
+    import hhs
+    rng = np.random.default_rng(a.seed)
+    sizes = np.round(np.exp(rng.uniform(np.log(64), np.log(4096), 512))).astype(np.int64)
+    parts = [hhs.plummer(int(nk), a.seed * 1000 + k) for k, nk in enumerate(sizes)]
+    e0 = np.array([hhs.energy_host(p) for p in parts])
+    packed = {f: np.concatenate([p[f] for p in parts]) for f in hhs.FIELDS}
+    packed["id"] = np.arange(int(sizes.sum()), dtype=np.int32)
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    n = int(off[-1])
+    stream = torch.cuda.Stream()
+    sh = ctypes.c_void_p(stream.cuda_stream)
+    prec = hhs.PREC_MIXED if a.prec == "mixed" else hhs.PREC_FP64
+    d = hhs.ParticleSystem(n)
+    d.upload(packed, stream=sh)
+    b = hhs.Batch(off, 64, eta=a.eta)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    with torch.cuda.stream(stream):
+        for _ in range(a.warmup):
+            b.step(d, a.dt, True, prec, stream=sh)
+        b.check(sh)
+        b.reset_stats(sh)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(a.steps)]
+        torch.cuda.synchronize()
+        for k in range(a.steps):
+            flush.zero_()
+            evs[k][0].record(stream)
+            b.step(d, a.dt, True, prec, stream=sh)
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        b.check(sh)
+    t_ms = sum(x.elapsed_time(y) for x, y in evs)
+    st = b.stats(sh)
+    out = d.download()
+    de = []
+    for k in range(len(sizes)):
+        sl = slice(off[k], off[k + 1])
+        e1 = hhs.energy_host({f: np.ascontiguousarray(out[f][sl]) for f in ("x", "y", "z", "vx",
+                                                                            "vy", "vz", "m")})
+        de.append(abs((e1 - e0[k]) / e0[k]))
+    de = np.array(de)
+    steps_all = a.steps + a.warmup
+    return {"metric": "aggregate HOLD steps/s over 512 independent clusters",
+            "value": len(sizes) * a.steps / (t_ms * 1e-3), "unit": "cluster HOLD steps/s",
+            "launches_per_s": a.steps / (t_ms * 1e-3), "ms_per_step": t_ms / a.steps,
+            "steps": a.steps, "warmup": a.warmup, "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32-pair/f64-state" if a.prec == "mixed" else "f64",
+            "data": "synthetic (seeded Plummer clusters)",
+            "config": {"workload": f"512 Plummer clusters, N log-uniform [64,4096] (total {n}), "
+                                   f"eta={a.eta}, dt_top={a.dt}, one launch per top step",
+                       "n_total": n, "l2": "flushed between timed steps"},
+            "pair_interactions_per_s": (st["kick_pairs"] + st["ts_pairs"]) / (t_ms * 1e-3),
+            "dE_over_E_after_steps": {"steps": steps_all, "median": float(np.median(de)),
+                                      "p90": float(np.percentile(de, 90)),
+                                      "max": float(de.max())}}
+
+
+def ref_scan_in_bounds(n, bs, unroll=4):
+    """True when the reference's scan recursion (src/split.cuh:438-565) never calls
+    scan_predicate_small with fewer than 3 elements, which writes past its dynamic
+    shared buffer; only such sizes are run."""
+    e = bs * unroll
+    calls = []
+
+    def large(m):
+        rem = m % e
+        large_ev(m - rem)
+        if rem:
+            calls.append(rem)
+
+    def large_ev(m):
+        nb = (m + e - 1) // e
+        (large if nb > e else calls.append)(nb)
+
+    (large if n > e else calls.append)(n)
+    return all(m >= 3 for m in calls)
+
+
+def run_scan(a, torch):
+    """Exclusive scan and stream compaction of Bernoulli(p) int32 flags, 2^20 .. 2^28."""
+    import hhs
+    ref = None
+    ref_path = os.path.join(ROOT, "oracle", "_ref", "libref_gpu_nofma.so")
+    if os.path.exists(ref_path):
+        ref = ctypes.CDLL(ref_path)
+        ref.ref_scan_predicate.argtypes = [ctypes.c_void_p] * 2 + [ctypes.c_int] * 2
+    stream = torch.cuda.current_stream()
+    sh = ctypes.c_void_p(stream.cuda_stream)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    rows = []
+
+    def ptr(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    def timed(fn, reps):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(reps)]
+        fn()
+        torch.cuda.synchronize()
+        for k in range(reps):
+            flush.zero_()
+            ev[k][0].record()
+            fn()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        return sum(x.elapsed_time(y) for x, y in ev) / reps
+
+    sizes = [a.scan_log2n] if a.scan_log2n else list(range(20, 29, 2))
+    for lg in sizes:
+        n = 1 << lg
+        ws_b = hhs.scan_workspace_size(n)
+        ws = torch.empty(ws_b, dtype=torch.uint8, device="cuda")
+        out = torch.empty(n, dtype=torch.int32, device="cuda")
+        idx = torch.empty(n, dtype=torch.int32, device="cuda")
+        cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+        for p in (0.01, 0.1, 0.5):
+            g = torch.Generator(device="cuda").manual_seed(lg * 10 + int(p * 100))
+            flags = (torch.rand(n, device="cuda", generator=g) < p).to(torch.int32)
+            ms_scan = timed(lambda: hhs.scan_exclusive_i32(ptr(flags), ptr(out), n, ptr(ws), ws_b,
+                                                           sh), a.steps)
+            ok = bool(torch.equal(out[1:] - out[:-1], flags[:-1])) and int(out[0]) == 0
+            ms_comp = timed(lambda: hhs.compact_flags_i32(ptr(flags), None, ptr(idx), ptr(cnt), n,
+                                                          ptr(ws), ws_b, sh), a.steps)
+            k = int(cnt.item())
+            row = {"log2n": lg, "p": p, "scan_ms": ms_scan, "scan_GBps": 8 * n / ms_scan / 1e6,
+                   "compact_ms": ms_comp, "compact_GBps": (4 * n + 4 * k) / ms_comp / 1e6,
+                   "scan_properties_ok": ok, "selected": k}
+            bs = next((b for b in (256, 128) if ref_scan_in_bounds(n, b)), None)
+            if ref is not None and bs is not None:
+                rout = torch.empty_like(flags)
+                ms_ref = timed(lambda: ref.ref_scan_predicate(ptr(flags), ptr(rout), n, bs), 3)
+                row["reference_scan_ms"] = ms_ref
+                row["reference_scan_GBps"] = 8 * n / ms_ref / 1e6
+                row["bit_exact_vs_reference"] = bool(torch.equal(rout, out))
+            rows.append(row)
+        del ws, out, idx, flags
+        torch.cuda.empty_cache()
+    top = [r for r in rows if r["log2n"] == sizes[-1] and r["p"] == 0.5][0]
+    return {"metric": f"exclusive scan HBM GB/s (8 B/element), 2^{sizes[-1]} int32 flags, p=0.5",
+            "value": top["scan_GBps"], "unit": "GB/s", "n_gpus": 1, "steps": a.steps,
+            "higher_is_better": True, "dtype": "i32", "data": "synthetic Bernoulli flags",
+            "config": {"workload": "scan/compaction sweep 2^20..2^28, p in {0.01,0.1,0.5}",
+                       "l2": "flushed between timed calls"},
+            "roofline": {"bound": "hbm", "achieved": top["scan_GBps"],
+                         "unit": "GB/s", "traffic": None}, "sweep": rows}
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -343,6 +501,23 @@ def main():
         d.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                              device_id=torch.device("cuda", local))
         dist = d
+    if a.workload in ("batched", "scan"):
+        if rank == 0:
+            out = run_batched(a, torch) if a.workload == "batched" else run_scan(a, torch)
+            peaks = None
+            try:
+                peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+            except (OSError, ValueError):
+                pass
+            if a.workload == "scan" and peaks:
+                out["roofline"]["peak"] = peaks["hbm_gbs"]
+                out["roofline"]["frac"] = out["value"] / peaks["hbm_gbs"]
+            print(json.dumps(out), flush=True)
+        return
+    if a.workload == "large":
+        a.n, a.eta, a.mass = 262144, 0.02, 2
+    elif a.workload == "deep":
+        a.n, a.eta, a.mass = 65536, 0.02, 1
     res = run_ours(a, rank, world, torch, dist)
     cpu = None
     if rank == 0 and world == 1 and not a.no_baselines:

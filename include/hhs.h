@@ -123,6 +123,8 @@ typedef struct {
     int32_t units_per_cta;
     int32_t ctas_per_sm;     /* CTAs of the persistent kernel per SM (1 or 2) */
     int32_t warp_n;          /* nodes with at most warp_n (<= 32) particles run on one warp */
+    int32_t cluster_size;    /* launch the persistent kernel in thread-block clusters (1,2,4,8) */
+    int32_t mid_n;           /* with clusters: nodes with small_n < n <= mid_n run on one cluster */
     double ms_per_step;      /* filled by hhs_ctx_autotune: time of the chosen setting */
 } hhs_tuning;
 hhs_status hhs_ctx_set_tuning(hhs_ctx* ctx, const hhs_tuning* t);
@@ -173,6 +175,13 @@ hhs_status hhs_update_system(hhs_particle_system* prev, const hhs_particle_syste
 hhs_status hhs_hold_step(hhs_ctx* ctx, int32_t clevel, hhs_particle_system* sys,
                          int32_t n, double stime, double etime, double dt,
                          int32_t calc_timestep, hhs_precision prec, void* stream);
+
+/* `steps` consecutive top-level steps (calc_timestep = 1 each), captured once into a CUDA
+ * graph and replayed on later calls with the same system, n, dt, steps, precision and
+ * tuning (one graph launch per call). Falls back to direct launches when the stream
+ * cannot be captured. Not for use inside another stream capture. */
+hhs_status hhs_hold_integrate(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n, double dt,
+                              int32_t steps, hhs_precision prec, void* stream);
 
 /* The same step driven from the host: the partition counts are read back after every
  * split (the reference synchronises at the same point, src/split.cuh:430) and the

@@ -299,6 +299,7 @@ extern "C" hhs_status hhs_ctx_create(int32_t n_max, int32_t max_levels, hhs_para
 extern "C" hhs_status hhs_ctx_destroy(hhs_ctx* c) {
     if (!c) return HHS_ERR_INVALID_ARG;
     delete static_cast<Profiler*>(c->prof);
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     engine_destroy(c);
     cudaError_t e1 = cudaFreeHost(c->host_counts);
     cudaError_t e2 = cudaFree(c->arena);
@@ -585,15 +586,19 @@ extern "C" hhs_status hhs_ctx_autotune(hhs_ctx* c, hhs_particle_system* sys, int
     hhs_stats stats_saved{};
     cudaMemcpy(&stats_saved, c->stats, sizeof(hhs_stats), cudaMemcpyDeviceToHost);
     st = copy_all(true);
-    const int small_cands[] = {0, 32, 64, 128, 256, 512, 1024};
+    // (small_n, mid_n, cluster_size) tiers, then units per CTA and CTAs per SM
+    struct Tier { int sn, mid, cs; };
+    const Tier tiers[] = {{32, 0, 1},    {64, 0, 1},     {128, 0, 1},   {256, 0, 1},
+                          {32, 512, 8},  {64, 1024, 8},  {64, 2048, 8}, {128, 2048, 8},
+                          {32, 1024, 4}, {64, 2048, 4}};
     const int upc_cands[] = {4, 8, 16};
     for (int cps = 1; cps <= 2; cps++)
-    for (int sn : small_cands) {
+    for (const Tier& tr : tiers) {
         for (int upc : upc_cands) {
             if (st != HHS_OK) break;
-            hhs_tuning t{sn, upc, cps, cur.warp_n, 0.0};
-            st = engine_set_tuning(c, t);
-            if (st == HHS_OK) st = copy_all(false);
+            hhs_tuning t{tr.sn, upc, cps, cur.warp_n, tr.cs, tr.mid, 0.0};
+            if (engine_set_tuning(c, t) != HHS_OK) continue;  // e.g. no cluster occupancy
+            st = copy_all(false);
             if (st == HHS_OK) st = engine_hold_step(c, soa_of(sys), n, dt, true, prec, false, s);
             if (st == HHS_OK) st = copy_all(false);
             if (st != HHS_OK) break;
@@ -623,5 +628,58 @@ extern "C" hhs_status hhs_ctx_autotune(hhs_ctx* c, hhs_particle_system* sys, int
     }
     engine_set_tuning(c, best);
     if (out) *out = best;
+    return HHS_OK;
+}
+
+// ------------------------------------------------------------------ graph-captured steps
+// `steps` consecutive top-level HOLD steps captured once into a CUDA graph (one node per
+// persistent-kernel launch) and replayed on later calls with the same system, size, step,
+// precision and tuning. Replays cost one graph launch instead of `steps` kernel launches.
+// If the stream cannot be captured, the steps are launched directly.
+extern "C" hhs_status hhs_hold_integrate(hhs_ctx* c, hhs_particle_system* sys, int32_t n,
+                                         double dt, int32_t steps, hhs_precision prec,
+                                         void* stream) {
+    if (!c || !sys_ok(sys) || n <= 0 || steps <= 0 || !(dt > 0.0)) return HHS_ERR_INVALID_ARG;
+    if (n > sys->n || n > c->n_max) return HHS_ERR_CAPACITY;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    hhs_tuning t{};
+    engine_get_tuning(c, &t);
+    unsigned long long dtbits;
+    std::memcpy(&dtbits, &dt, sizeof(dtbits));
+    const unsigned long long key[6] = {
+        reinterpret_cast<uintptr_t>(sys->x), (unsigned long long)n, dtbits,
+        ((unsigned long long)steps << 8) | (unsigned long long)prec,
+        ((unsigned long long)t.small_n << 32) | (unsigned)t.mid_n,
+        ((unsigned long long)t.units_per_cta << 32) |
+            (unsigned)(t.ctas_per_sm | (t.warp_n << 8) | (t.cluster_size << 16))};
+    const bool hit = c->graph_exec && std::memcmp(key, c->graph_key, sizeof(key)) == 0;
+    if (!hit) {
+        if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }
+        cudaGraph_t g = nullptr;
+        bool captured = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        hhs_status st = HHS_OK;
+        if (captured) {
+            for (int k = 0; k < steps && st == HHS_OK; k++)
+                st = engine_hold_step(c, soa_of(sys), n, dt, true, prec, false, s);
+            const cudaError_t e = cudaStreamEndCapture(s, &g);
+            captured = (st == HHS_OK && e == cudaSuccess && g != nullptr);
+            if (captured && cudaGraphInstantiate(&c->graph_exec, g, 0) != cudaSuccess) {
+                c->graph_exec = nullptr;
+                captured = false;
+            }
+            if (g) cudaGraphDestroy(g);
+        }
+        cudaGetLastError();
+        if (!captured) {
+            for (int k = 0; k < steps; k++) {
+                hhs_status st2 = engine_hold_step(c, soa_of(sys), n, dt, true, prec, false, s);
+                if (st2 != HHS_OK) return st2;
+            }
+            return HHS_OK;
+        }
+        std::memcpy(c->graph_key, key, sizeof(key));
+    }
+    HHS_CUDA_TRY(cudaGraphLaunch(c->graph_exec, s));
+    hhs_count_launch();
     return HHS_OK;
 }

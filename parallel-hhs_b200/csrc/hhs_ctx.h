@@ -29,6 +29,9 @@ struct hhs_ctx {
     void* engine = nullptr;
     size_t engine_bytes = 0;
     void* engine_host = nullptr;
+    // CUDA graph of a captured multi-step integration (hhs_hold_integrate)
+    cudaGraphExec_t graph_exec = nullptr;
+    unsigned long long graph_key[6] = {0, 0, 0, 0, 0, 0};
 
     int32_t* fast(int level) const { return fast_lists + (size_t)level * n_max; }
     int32_t* slow(int level) const { return slow_lists + (size_t)level * n_max; }

@@ -47,7 +47,9 @@ constexpr int kMaxChunks = 32;    // source chunks per node (partial-sum slots)
 constexpr int kMaxLevels = 64;    // per-level state is kept in 64-bit masks
 constexpr unsigned long long kBarrierTimeoutNs = 60ull * 1000000000ull;
 
-enum ProfKind { kProfTs = 0, kProfKick = 1, kProfSplit = 2, kProfUpdate = 3, kProfSubtree = 5 };
+enum ProfKind {
+    kProfTs = 0, kProfKick = 1, kProfSplit = 2, kProfUpdate = 3, kProfSubtree = 5, kProfCluster = 6
+};
 
 struct EngineState {
     unsigned bar_count;
@@ -62,7 +64,7 @@ struct EngineState {
 
 struct EParams {
     SoA P;
-    int n_top, n_max, max_levels, small_n, calc_top, profile, units_per_cta, warp_n;
+    int n_top, n_max, max_levels, small_n, calc_top, profile, units_per_cta, warp_n, mid_n;
     double dt_top, eta, eta_s2;
     float inv_eta_s2, inv_eta;
     int32_t* fast_lists;
@@ -105,19 +107,27 @@ __device__ __forceinline__ int ld_volatile_i32(const int32_t* p) {
 }
 
 // ---------------------------------------------------------------- grid barrier
-// Sense-reversing barrier over all CTAs of the cooperative grid. Thread 0 of each CTA
-// arrives with one atomic; the last arrival resets the counter and advances the
-// generation; the others poll the generation, give up after kBarrierTimeoutNs (or as
-// soon as another CTA recorded an error) and report failure instead of hanging.
+// Sense-reversing barrier over all CTAs of the cooperative grid. When the grid is
+// launched in thread-block clusters, the CTAs of a cluster first meet at the hardware
+// cluster barrier and only the cluster's first CTA arrives at the global counter, so
+// the serialised atomics drop by the cluster size. The last arrival resets the counter
+// and advances the generation; the others poll the generation, give up after
+// kBarrierTimeoutNs (or as soon as another CTA recorded an error) and report failure
+// instead of hanging.
 __device__ bool grid_barrier(const EParams& E, Smem& sm) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    namespace cg = cooperative_groups;
+    const unsigned cs = cg::this_cluster().num_blocks();
+    const bool leader = cs == 1 || cg::this_cluster().block_rank() == 0;
+    if (cs > 1) cg::this_cluster().sync();
+    else __syncthreads();
+    if (leader && threadIdx.x == 0) {
         int ok = 1;
         EngineState* st = E.st;
+        const unsigned parties = gridDim.x / cs;
         const unsigned gen = *reinterpret_cast<volatile unsigned*>(&st->bar_gen);
         __threadfence();
         const unsigned arrived = atomicAdd(&st->bar_count, 1u);
-        if (arrived == gridDim.x - 1) {
+        if (arrived == parties - 1) {
             *reinterpret_cast<volatile unsigned*>(&st->bar_count) = 0u;
             __threadfence();
             atomicAdd(&st->bar_gen, 1u);
@@ -125,7 +135,7 @@ __device__ bool grid_barrier(const EParams& E, Smem& sm) {
             const unsigned long long t0 = gtimer();
             while (ld_acquire_u32(&st->bar_gen) == gen) {
                 if (*reinterpret_cast<volatile unsigned*>(E.err) != 0u) { ok = 0; break; }
-                __nanosleep(40);
+                __nanosleep(32);
                 if (gtimer() - t0 > kBarrierTimeoutNs) {
                     atomicOr(E.err, HHS_ERRBIT_BARRIER_TIMEOUT);
                     ok = 0;
@@ -135,6 +145,10 @@ __device__ bool grid_barrier(const EParams& E, Smem& sm) {
         }
         __threadfence();
         sm.ok = ok;
+    }
+    if (cs > 1) {
+        cg::this_cluster().sync();
+        return *reinterpret_cast<volatile unsigned*>(E.err) == 0u;
     }
     __syncthreads();
     return sm.ok != 0;
@@ -859,6 +873,22 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                 lvl--;
                 continue;
             }
+            if (MODE == kModeGrid && n <= E.mid_n && n > E.small_n) {
+                namespace cg = cooperative_groups;
+                const int cs = (int)cg::this_cluster().num_blocks();
+                if (cs > 1) {
+                    if ((int)blockIdx.x < cs) {
+                        const Workers cw{(int)cg::this_cluster().block_rank(), cs, kModeCluster};
+                        unsigned long long t_sub = 0;
+                        run_hold<PREC, kModeCluster>(E, lvl, calc, cw, sm, t_sub);
+                    }
+                    if (!phase_barrier(E, sm, W)) return false;
+                    prof_mark(E, W, t_last, kProfCluster, 0.0, lvl);
+                    calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
+                    lvl--;
+                    continue;
+                }
+            }
             if (MODE != kModeBlock && n <= E.small_n) {
                 if (W.id == 0) {
                     const Workers one{0, 1, kModeBlock};
@@ -1049,6 +1079,8 @@ struct EngineHost {
     int small_n = 256;
     int units_per_cta = 8;
     int warp_n = 32;
+    int cluster_size = 1;
+    int mid_n = 0;
     EngineState* st = nullptr;
     double* ts_part = nullptr;
     double* k_part = nullptr;
@@ -1107,14 +1139,39 @@ void engine_destroy(hhs_ctx* c) {
 hhs_status engine_set_tuning(hhs_ctx* c, const hhs_tuning& t) {
     auto* eh = static_cast<EngineHost*>(c->engine_host);
     if (!eh || t.small_n < 0 || t.units_per_cta < 1 || t.units_per_cta > 64 ||
-        t.ctas_per_sm < 1 || t.ctas_per_sm > 2 || t.warp_n < 0 || t.warp_n > 32)
+        t.ctas_per_sm < 1 || t.ctas_per_sm > 2 || t.warp_n < 0 || t.warp_n > 32 ||
+        !(t.cluster_size == 1 || t.cluster_size == 2 || t.cluster_size == 4 ||
+          t.cluster_size == 8) || t.mid_n < 0)
         return HHS_ERR_INVALID_ARG;
     eh->warp_n = t.warp_n;
+    eh->cluster_size = t.cluster_size;
+    eh->mid_n = t.mid_n;
     eh->small_n = t.small_n;
     eh->units_per_cta = t.units_per_cta;
     eh->ctas_per_sm = t.ctas_per_sm;
-    for (int k = 0; k < 2; k++)
-        eh->grid[k] = eh->sms * (eh->occ[k] < t.ctas_per_sm ? eh->occ[k] : t.ctas_per_sm);
+    for (int k = 0; k < 2; k++) {
+        int g = eh->sms * (eh->occ[k] < t.ctas_per_sm ? eh->occ[k] : t.ctas_per_sm);
+        if (t.cluster_size > 1) {
+            int nc = 0;
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(t.cluster_size, 1, 1);
+            cfg.blockDim = dim3(kEB, 1, 1);
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = t.cluster_size;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            const cudaError_t e =
+                k == 0 ? cudaOccupancyMaxActiveClusters(&nc, (void*)k_engine<HHS_PREC_FP64>, &cfg)
+                       : cudaOccupancyMaxActiveClusters(&nc, (void*)k_engine<HHS_PREC_MIXED>, &cfg);
+            if (e != cudaSuccess || nc <= 0) return HHS_ERR_CUDA;
+            const int gc = nc * t.cluster_size;
+            g = (g < gc ? g : gc) / t.cluster_size * t.cluster_size;
+        }
+        eh->grid[k] = g;
+    }
     return HHS_OK;
 }
 
@@ -1125,6 +1182,8 @@ hhs_status engine_get_tuning(hhs_ctx* c, hhs_tuning* t) {
     t->units_per_cta = eh->units_per_cta;
     t->ctas_per_sm = eh->ctas_per_sm;
     t->warp_n = eh->warp_n;
+    t->cluster_size = eh->cluster_size;
+    t->mid_n = eh->mid_n;
     return HHS_OK;
 }
 
@@ -1178,6 +1237,7 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
     E.small_n = eh->small_n;
     E.units_per_cta = eh->units_per_cta;
     E.warp_n = eh->warp_n;
+    E.mid_n = eh->mid_n;
     E.calc_top = calc_ts ? 1 : 0;
     E.profile = profile ? 1 : 0;
     E.dt_top = dt;
@@ -1196,15 +1256,25 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
     E.rate_acc = eh->rate_acc;
     E.st = eh->st;
     E.err = c->err;
-    void* args[] = {&E};
     const int pi = prec == HHS_PREC_FP64 ? 0 : 1;
-    cudaError_t e;
-    if (pi == 0)
-        e = cudaLaunchCooperativeKernel((const void*)k_engine<HHS_PREC_FP64>, eh->grid[0], kEB,
-                                        args, 0, stream);
-    else
-        e = cudaLaunchCooperativeKernel((const void*)k_engine<HHS_PREC_MIXED>, eh->grid[1], kEB,
-                                        args, 0, stream);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(eh->grid[pi], 1, 1);
+    cfg.blockDim = dim3(kEB, 1, 1);
+    cfg.stream = stream;
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    if (eh->cluster_size > 1) {
+        at[1].id = cudaLaunchAttributeClusterDimension;
+        at[1].val.clusterDim.x = eh->cluster_size;
+        at[1].val.clusterDim.y = 1;
+        at[1].val.clusterDim.z = 1;
+        cfg.numAttrs = 2;
+    }
+    cudaError_t e = pi == 0 ? cudaLaunchKernelEx(&cfg, k_engine<HHS_PREC_FP64>, E)
+                            : cudaLaunchKernelEx(&cfg, k_engine<HHS_PREC_MIXED>, E);
     hhs_count_launch();
     if (e != cudaSuccess) return hhs_from_cuda(e);
     return HHS_OK;
@@ -1374,6 +1444,7 @@ extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, d
     E.profile = 0;
     E.units_per_cta = b->units_per_cta;
     E.warp_n = b->warp_n;
+    E.mid_n = 0;
     E.dt_top = dt;
     E.eta = b->params.eta;
     E.eta_s2 = b->params.eta / 1.41421356237309504880;

@@ -92,14 +92,15 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float t) {
 // tau/(1 - dtau/2) with dtau = 1.5*tau0*vdotdr2 clamped at 1 becomes
 // rate0 - 0.75*vdotdr2 (or rate0/2 when clamped). Fly-by: rate0 = |dv|/(eta*r),
 // dtau = vdotdr2*(1 + M/(dv2*r))/rate0, likewise. dr2 == 0 gives +inf (tau = 0 in
-// the reference); dv2 == 0 gives a fly-by rate of 0 (tau = inf).
+// the reference). dv2 == 0 makes the fly-by rate NaN (rsqrt(0) = inf times 0), which
+// fmaxf discards: the pair's rate is then the free-fall one, as tau = inf for the
+// fly-by term in the reference.
 __device__ __forceinline__ float ts_pair_rate_mixed(float drx, float dry, float drz, float dvx,
                                                     float dvy, float dvz, float msum,
                                                     float inv_eta_s2, float inv_eta) {
     const float dr2 = fmaf(drx, drx, fmaf(dry, dry, drz * drz));
     const float dv2 = fmaf(dvx, dvx, fmaf(dvy, dvy, dvz * dvz));
     const float rdv = fmaf(drx, dvx, fmaf(dry, dvy, drz * dvz));
-    if (dr2 == 0.0f) return __int_as_float(0x7f800000);
     const float rinv = rsqrt_nr(dr2);
     const float rinv2 = rinv * rinv;
     const float vdr = rdv * rinv2;
@@ -107,14 +108,12 @@ __device__ __forceinline__ float ts_pair_rate_mixed(float drx, float dry, float 
     const float r0 = u * rsqrt_nr(u) * inv_eta_s2;
     const float b0 = 1.5f * vdr;
     const float rate_ff = (b0 < r0) ? fmaf(-0.5f, b0, r0) : 0.5f * r0;
-    float rate_fb = 0.0f;
-    if (dv2 > 0.0f) {
-        const float q = rsqrt_nr(dv2);
-        const float r1 = dv2 * q * rinv * inv_eta;
-        const float b1 = vdr * fmaf(msum * rinv, q * q, 1.0f);
-        rate_fb = (b1 < r1) ? fmaf(-0.5f, b1, r1) : 0.5f * r1;
-    }
-    return fmaxf(rate_ff, rate_fb);
+    const float q = rsqrt_nr(dv2);
+    const float r1 = dv2 * q * rinv * inv_eta;
+    const float b1 = vdr * fmaf(msum * rinv, q * q, 1.0f);
+    const float rate_fb = (b1 < r1) ? fmaf(-0.5f, b1, r1) : 0.5f * r1;
+    const float rate = fmaxf(rate_ff, rate_fb);
+    return dr2 == 0.0f ? __int_as_float(0x7f800000) : rate;
 }
 
 }  // namespace hhs

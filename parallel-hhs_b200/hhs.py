@@ -55,12 +55,14 @@ class Profile(ctypes.Structure):
                 ("pairs", ctypes.c_double * 8)]
 
 
-PROFILE_KINDS = ("timesteps", "kick", "split", "drift", "engine", "k5", "k6", "k7")
+PROFILE_KINDS = ("timesteps", "kick", "split", "update", "engine", "subtree", "cluster_node",
+                 "k7")
 
 
 class Tuning(ctypes.Structure):
     _fields_ = [("small_n", ctypes.c_int32), ("units_per_cta", ctypes.c_int32),
                 ("ctas_per_sm", ctypes.c_int32), ("warp_n", ctypes.c_int32),
+                ("cluster_size", ctypes.c_int32), ("mid_n", ctypes.c_int32),
                 ("ms_per_step", ctypes.c_double)]
 
 
@@ -109,6 +111,8 @@ SIGNATURES = {
     "hhs_hold_step": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.POINTER(CParticleSystem),
                                      ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_double, ctypes.c_int32, ctypes.c_int, _vp]),
+    "hhs_hold_integrate": (ctypes.c_int, [_vp, ctypes.POINTER(CParticleSystem), ctypes.c_int32,
+                                          ctypes.c_double, ctypes.c_int32, ctypes.c_int, _vp]),
     "hhs_hold_step_host": (ctypes.c_int, [_vp, ctypes.POINTER(CParticleSystem), ctypes.c_int32,
                                           ctypes.c_double, ctypes.c_int32, ctypes.c_int, _vp]),
     "hhs_scan_workspace_size": (ctypes.c_size_t, [ctypes.c_int64]),
@@ -269,7 +273,8 @@ class Context:
     def reset_stats(self, stream=None):
         _check(lib().hhs_ctx_reset_stats(self.h, stream), "reset_stats")
 
-    def set_tuning(self, small_n=None, units_per_cta=None, ctas_per_sm=None, warp_n=None):
+    def set_tuning(self, small_n=None, units_per_cta=None, ctas_per_sm=None, warp_n=None,
+                   cluster_size=None, mid_n=None):
         t = Tuning()
         _check(lib().hhs_ctx_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
         if small_n is not None:
@@ -280,20 +285,26 @@ class Context:
             t.ctas_per_sm = ctas_per_sm
         if warp_n is not None:
             t.warp_n = warp_n
+        if cluster_size is not None:
+            t.cluster_size = cluster_size
+        if mid_n is not None:
+            t.mid_n = mid_n
         _check(lib().hhs_ctx_set_tuning(self.h, ctypes.byref(t)), "set_tuning")
 
     def tuning(self):
         t = Tuning()
         _check(lib().hhs_ctx_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
         return {"small_n": t.small_n, "units_per_cta": t.units_per_cta,
-                "ctas_per_sm": t.ctas_per_sm, "warp_n": t.warp_n}
+                "ctas_per_sm": t.ctas_per_sm, "warp_n": t.warp_n,
+                "cluster_size": t.cluster_size, "mid_n": t.mid_n}
 
     def autotune(self, sys, n, dt, prec=1, stream=None):
         t = Tuning()
         _check(lib().hhs_ctx_autotune(self.h, sys.ref, n, dt, prec, ctypes.byref(t), stream),
                "autotune")
         return {"small_n": t.small_n, "units_per_cta": t.units_per_cta,
-                "ctas_per_sm": t.ctas_per_sm, "warp_n": t.warp_n, "ms_per_step": t.ms_per_step}
+                "ctas_per_sm": t.ctas_per_sm, "warp_n": t.warp_n,
+                "cluster_size": t.cluster_size, "mid_n": t.mid_n, "ms_per_step": t.ms_per_step}
 
     def set_profiling(self, on):
         _check(lib().hhs_ctx_set_profiling(self.h, int(on)), "set_profiling")
@@ -402,6 +413,12 @@ def hold_step(ctx, sys, n, stime, dt, calc_timestep=True, prec=PREC_MIXED, cleve
     """hold_step<double,BS>(clevel, globals, sys, N, stime, stime+dt, dt, calc_timestep)."""
     _check(lib().hhs_hold_step(ctx.h, clevel, sys.ref, n, stime, stime + dt, dt,
                                int(calc_timestep), prec, stream), "hhs_hold_step")
+
+
+def hold_integrate(ctx, sys, n, dt, steps, prec=PREC_MIXED, stream=None):
+    """`steps` top-level steps as one replayed CUDA graph (hhs_hold_integrate)."""
+    _check(lib().hhs_hold_integrate(ctx.h, sys.ref, n, dt, steps, prec, stream),
+           "hhs_hold_integrate")
 
 
 def hold_step_host(ctx, sys, n, dt, calc_timestep=True, prec=PREC_FP64, stream=None):

@@ -551,3 +551,20 @@ def test_hold_batched_matches_per_system_oracle(cuda, hhs, oracle, sizes, big_n,
             elif f in ("x", "y", "z"):
                 assert np.max(np.abs(out[f][sl] - p[f])) < 1e-7, (k, f)
     assert np.allclose(b.simtime(), leaf, rtol=1e-15, atol=0)
+
+
+def test_hold_integrate_graph_matches_steps(cuda, hhs, oracle):
+    n = 800
+    s = _plummer(hhs, n, 61)
+    ref = {k: v.copy() for k, v in s.items()}
+    ctx = hhs.Context(n, 64, eta=0.03)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    for _ in range(2):  # capture, then replay
+        hhs.hold_integrate(ctx, d, n, 1.0 / 64, 2, hhs.PREC_FP64)
+    ctx.check()
+    for _ in range(4):
+        oracle.hold_step(ref, 1.0 / 64, True, 0.03)
+    out = d.download()
+    for k in FIELDS:
+        assert np.array_equal(out[k], ref[k]), k
