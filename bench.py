@@ -45,6 +45,8 @@ def parse():
     p.add_argument("--small-n", type=int, default=256,
                    help="device schedule: nodes with n <= this are solved by one CTA")
     p.add_argument("--ctas-per-sm", type=int, default=2)
+    p.add_argument("--cluster-size", type=int, default=1)
+    p.add_argument("--mid-n", type=int, default=0)
     p.add_argument("--units-per-cta", type=int, default=8)
     p.add_argument("--autotune", action="store_true",
                    help="pick the device-schedule tuning with the library's autotuner")
@@ -162,7 +164,8 @@ def run_ours(a, rank, world, torch, dist):
     ics = hhs.plummer(a.n, seed, getattr(a, "mass", 0))
     e0 = hhs.energy_host(ics)
     ctx = hhs.Context(a.n, 64, eta=a.eta)
-    ctx.set_tuning(a.small_n, a.units_per_cta, a.ctas_per_sm)
+    ctx.set_tuning(a.small_n, a.units_per_cta, a.ctas_per_sm, cluster_size=a.cluster_size,
+                   mid_n=a.mid_n)
     sys_ = hhs.ParticleSystem(a.n)
     sys_.upload(ics, stream=sh)
     tuned = None

@@ -86,8 +86,19 @@ struct __align__(16) Smem {
         struct { double x[kEB], y[kEB], z[kEB], vx[kEB], vy[kEB], vz[kEB], m[kEB]; } tsd;
         struct { float4 A[kEB], B[kEB]; } km;                   // mixed kick tiles
         struct { double x[kEB], y[kEB], z[kEB], m[kEB]; } kd;   // FP64 kick tiles
+        struct {                                                  // tiny-subtree state
+            double x[32], y[32], z[32], vx[32], vy[32], vz[32], m[32], ts[32];
+            float4 A[32], B[32], V[32];
+            double pmin[kEB / 32][32];
+            float pmax[kEB / 32][32];
+            float part[kEB / 32][3][32];
+            int g[32];
+        } tiny;
     } u;
     float colred[kEB / 32][64];
+    unsigned long long prof_ns[8][kMaxLevels];  // phase times of this launch (CTA 0)
+    unsigned prof_cnt[8][kMaxLevels];
+    double prof_pairs[8];
     unsigned wfast[kMaxLevels];   // warp solver: fast-lane mask per depth
     int wlone[kMaxLevels];        // warp solver: lane folded into the slow set, or -1
     int warp_tot[kEB / 32];
@@ -172,21 +183,57 @@ __device__ __forceinline__ bool phase_barrier(const EParams& E, Smem& sm, const 
 }
 
 // Phase timing by CTA 0 of the grid: the time from the previous mark to the release of
-// the barrier that ends the phase (the phase's makespan over all CTAs), per kind and level.
+// the barrier that ends the phase (the phase's makespan over all CTAs), per kind and
+// level, accumulated in shared memory and added to the context's counters at the end of
+// the launch.
 __device__ __forceinline__ void prof_mark(const EParams& E, const Workers& W,
                                           unsigned long long& t_last, int kind, double pairs,
-                                          int level = 0) {
+                                          Smem& sm, int level = 0) {
     if (!E.profile || W.mode != kModeGrid || threadIdx.x != 0 || W.id != 0) return;
     const unsigned long long t = gtimer();
     if (kind >= 0) {
-        E.st->prof_ns[kind] += t - t_last;
-        E.st->prof_cnt[kind] += 1;
-        E.st->prof_pairs[kind] += pairs;
         const int l = level < kMaxLevels ? level : kMaxLevels - 1;
-        E.st->lvl_ns[kind][l] += t - t_last;
-        E.st->lvl_cnt[kind][l] += 1;
+        sm.prof_ns[kind][l] += t - t_last;
+        sm.prof_cnt[kind][l] += 1;
+        sm.prof_pairs[kind] += pairs;
     }
     t_last = t;
+}
+
+__device__ void prof_begin(const EParams& E, Smem& sm) {
+    if (!E.profile || blockIdx.x != 0) return;
+    for (int i = threadIdx.x; i < 8 * kMaxLevels; i += blockDim.x) {
+        (&sm.prof_ns[0][0])[i] = 0ull;
+        (&sm.prof_cnt[0][0])[i] = 0u;
+    }
+    if (threadIdx.x < 8) sm.prof_pairs[threadIdx.x] = 0.0;
+    __syncthreads();
+}
+
+__device__ void prof_end(const EParams& E, Smem& sm) {
+    if (!E.profile || blockIdx.x != 0) return;
+    __syncthreads();
+    EngineState* st = E.st;
+    for (int i = threadIdx.x; i < 8 * kMaxLevels; i += blockDim.x) {
+        const int k = i / kMaxLevels, l = i % kMaxLevels;
+        const unsigned long long ns = sm.prof_ns[k][l];
+        const unsigned c = sm.prof_cnt[k][l];
+        if (c) {
+            st->lvl_ns[k][l] += ns;
+            st->lvl_cnt[k][l] += c;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        unsigned long long ns = 0, c = 0;
+        for (int l = 0; l < kMaxLevels; l++) {
+            ns += sm.prof_ns[threadIdx.x][l];
+            c += sm.prof_cnt[threadIdx.x][l];
+        }
+        st->prof_ns[threadIdx.x] += ns;
+        st->prof_cnt[threadIdx.x] += c;
+        st->prof_pairs[threadIdx.x] += sm.prof_pairs[threadIdx.x];
+    }
 }
 
 // number of source chunks for a node of n sinks
@@ -313,15 +360,20 @@ __device__ void ts_unit(const EParams& E, const int32_t* S, int n, int ib, int j
 // products of two negated values and the mass sum are unchanged), so each unordered pair
 // is evaluated once, in the unit (row block of kEB list positions, column block of 64)
 // that holds it with i < j. Rows keep their running max rate in a register; the column
-// maxima of a warp's 32 rows come from a butterfly transpose-reduce (31 shuffles for 32
+// maxima of a warp's 32 rows come from a butterfly transpose-reduce (31 shuffles per 16
 // columns). Both are merged into rate_acc with an integer atomicMax on the FP32 bit
 // pattern (rates are >= 0, so integer order is float order). Max is exact and
 // order-independent: the result equals the all-pairs evaluation bit for bit.
 constexpr int kCB = 64;
 
-__device__ __forceinline__ void butterfly_max32(float (&r)[32], int lane) {
+// Column maxima of a 32-row x 16-column block held one row per lane: after the first
+// exchange both half-warps hold the pairwise maxima of the same 16 columns, then a
+// transpose-reduce over the 16 lanes of each half leaves column (lane & 15) in r[0].
+__device__ __forceinline__ void butterfly_max16(float (&r)[16], int lane) {
 #pragma unroll
-    for (int k = 16; k >= 1; k >>= 1) {
+    for (int c = 0; c < 16; c++) r[c] = fmaxf(r[c], __shfl_xor_sync(HHS_FULL_MASK, r[c], 16));
+#pragma unroll
+    for (int k = 8; k >= 1; k >>= 1) {
         const bool upper = (lane & k) != 0;
 #pragma unroll
         for (int c = 0; c < k; c++) {
@@ -360,11 +412,11 @@ __device__ void ts_sym_unit(const EParams& E, const int32_t* S, int n, int rb, i
     __syncthreads();
     float rowmax = 0.0f;
 #pragma unroll 1
-    for (int g = 0; g < kCB / 32; g++) {
-        float r[32];
+    for (int g = 0; g < kCB / 16; g++) {
+        float r[16];
 #pragma unroll
-        for (int c = 0; c < 32; c++) {
-            const int jl = g * 32 + c;
+        for (int c = 0; c < 16; c++) {
+            const int jl = g * 16 + c;
             const float4 A = sm.u.tsm.A[jl], B = sm.u.tsm.B[jl], V = sm.u.tsm.V[jl];
             const float rate = ts_pair_rate_mixed(
                 ds_diff(xi.hi, xi.lo, A.x, B.x), ds_diff(yi.hi, yi.lo, A.y, B.y),
@@ -374,8 +426,8 @@ __device__ void ts_sym_unit(const EParams& E, const int32_t* S, int n, int rb, i
             r[c] = ok ? rate : 0.0f;
             rowmax = fmaxf(rowmax, r[c]);
         }
-        butterfly_max32(r, lane);
-        sm.colred[warp][g * 32 + lane] = r[0];
+        butterfly_max16(r, lane);
+        if (lane < 16) sm.colred[warp][g * 16 + lane] = r[0];
     }
     __syncthreads();
     if ((int)threadIdx.x < ncol) {
@@ -636,37 +688,33 @@ __device__ void kick_reduce_phase(const EParams& E, const int32_t* F, const int3
 }
 
 
-// ---------------------------------------------------------------- warp subtree solver
-// A subsystem of at most 32 particles, with its whole subtree, on one warp: one particle
-// per lane in registers (FP64 state), each level's subset a 32-bit lane mask, the split a
-// ballot (stable order = lane order; the N_fast == 1 fold keeps the lone lane and visits
-// it last among the slow sources), pair loops over set bits with the sources staged in
-// shared memory. No list, count or partial-sum traffic; state is written back once.
-// The FP64 form keeps the reference's summation order, so it stays bit-exact.
-__device__ __forceinline__ void warp_stage(Smem& sm, int lane, double x, double y, double z,
-                                           double vx, double vy, double vz, double m) {
-    sm.u.tsd.x[lane] = x; sm.u.tsd.y[lane] = y; sm.u.tsd.z[lane] = z;
-    sm.u.tsd.vx[lane] = vx; sm.u.tsd.vy[lane] = vy; sm.u.tsd.vz[lane] = vz;
-    sm.u.tsd.m[lane] = m;
-    __syncwarp();
-}
-
+// ---------------------------------------------------------------- tiny subtree solver
+// A subsystem of at most 32 particles, with its whole subtree, on one CTA: the state
+// lives in shared memory (FP64), each level's subset is a 32-bit slot mask, the split is
+// a ballot (stable order = slot order; the N_fast == 1 fold keeps the lone slot and
+// visits it last among the slow sources). Pair work is spread over the CTA's 8 warps:
+// lane = sink slot, warp = source group (slots w, w+8, w+16, w+24), partial results
+// reduced by warp 0. The FP64 kick sums stay sequential per sink (warp 0) so the FP64
+// form keeps the reference's summation order and stays bit-exact. No list, count or
+// partial-sum traffic to global memory; the state is written back once.
 template <int PREC>
-__device__ void warp_hold(const EParams& E, const int32_t* S, int n, int level0, bool calc0,
+__device__ void tiny_hold(const EParams& E, const int32_t* S, int n, int level0, bool calc0,
                           Smem& sm) {
-    const int lane = threadIdx.x & 31;
-    const bool act = lane < n;
-    const int g = act ? list_at(S, lane) : 0;
+    auto& T = sm.u.tiny;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const SoA& P = E.P;
-    double x = 0, y = 0, z = 0, vx = 0, vy = 0, vz = 0, m = 0, ts = 1.e30;
-    if (act) {
-        x = P.x[g]; y = P.y[g]; z = P.z[g];
-        vx = P.vx[g]; vy = P.vy[g]; vz = P.vz[g];
-        m = P.m[g]; ts = P.ts[g];
+    if (warp == 0) {
+        const bool act = lane < n;
+        const int g = act ? list_at(S, lane) : 0;
+        T.g[lane] = g;
+        T.x[lane] = act ? P.x[g] : 0.0; T.y[lane] = act ? P.y[g] : 0.0;
+        T.z[lane] = act ? P.z[g] : 0.0; T.vx[lane] = act ? P.vx[g] : 0.0;
+        T.vy[lane] = act ? P.vy[g] : 0.0; T.vz[lane] = act ? P.vz[g] : 0.0;
+        T.m[lane] = act ? P.m[g] : 0.0; T.ts[lane] = act ? P.ts[g] : 1.e30;
     }
+    __syncthreads();
     const unsigned top_mask = n >= 32 ? 0xffffffffu : ((1u << n) - 1u);
     unsigned long long after1 = 0, after2 = 0, calcm = calc0 ? 1ull : 0ull;
-    bool ok = true;
     int d = 0;
     while (d >= 0) {
         const int lvl = level0 + d;
@@ -676,63 +724,85 @@ __device__ void warp_hold(const EParams& E, const int32_t* S, int n, int level0,
         const double dt = ldexp(E.dt_top, -lvl);
         if (!(after1 & bit)) {
             if (lvl >= E.max_levels || lvl >= kMaxLevels - 1) {
-                if (lane == 0) atomicOr(E.err, HHS_ERRBIT_DEPTH);
-                ok = false;
+                if (threadIdx.x == 0) atomicOr(E.err, HHS_ERRBIT_DEPTH);
                 break;
             }
             const int cnt = __popc(mask);
             if (calcm & bit) {
-                warp_stage(sm, lane, x, y, z, vx, vy, vz, m);
                 if (PREC == HHS_PREC_FP64) {
-                    double minval = 1.e30;
-                    for (unsigned mm = mask; mm; mm &= mm - 1u) {
-                        const int j = __ffs(mm) - 1;
-                        if (j == lane) continue;
-                        ts_pair_fp64(f64_sub(x, sm.u.tsd.x[j]), f64_sub(y, sm.u.tsd.y[j]),
-                                     f64_sub(z, sm.u.tsd.z[j]), f64_sub(vx, sm.u.tsd.vx[j]),
-                                     f64_sub(vy, sm.u.tsd.vy[j]), f64_sub(vz, sm.u.tsd.vz[j]), m,
-                                     sm.u.tsd.m[j], E.eta, E.eta_s2, minval);
-                    }
-                    if (in) ts = minval;
-                } else {
-                    const DS xi = ds_split(x), yi = ds_split(y), zi = ds_split(z);
-                    float maxrate = 0.0f;
-                    for (unsigned mm = mask; mm; mm &= mm - 1u) {
-                        const int j = __ffs(mm) - 1;
-                        if (j == lane) continue;
-                        const DS xj = ds_split(sm.u.tsd.x[j]), yj = ds_split(sm.u.tsd.y[j]),
-                                 zj = ds_split(sm.u.tsd.z[j]);
-                        const float r = ts_pair_rate_mixed(
-                            ds_diff(xi.hi, xi.lo, xj.hi, xj.lo), ds_diff(yi.hi, yi.lo, yj.hi, yj.lo),
-                            ds_diff(zi.hi, zi.lo, zj.hi, zj.lo), (float)vx - (float)sm.u.tsd.vx[j],
-                            (float)vy - (float)sm.u.tsd.vy[j], (float)vz - (float)sm.u.tsd.vz[j],
-                            (float)m + (float)sm.u.tsd.m[j], E.inv_eta_s2, E.inv_eta);
-                        maxrate = fmaxf(maxrate, r);
-                    }
+                    double mv = 1.e30;
                     if (in) {
-                        const double tv = 1.0 / (double)maxrate;
-                        ts = tv < 1.e30 ? tv : 1.e30;
+#pragma unroll 1
+                        for (int j = warp; j < 32; j += kEB / 32) {
+                            if (!((mask >> j) & 1u) || j == lane) continue;
+                            ts_pair_fp64(f64_sub(T.x[lane], T.x[j]), f64_sub(T.y[lane], T.y[j]),
+                                         f64_sub(T.z[lane], T.z[j]), f64_sub(T.vx[lane], T.vx[j]),
+                                         f64_sub(T.vy[lane], T.vy[j]), f64_sub(T.vz[lane], T.vz[j]),
+                                         T.m[lane], T.m[j], E.eta, E.eta_s2, mv);
+                        }
+                    }
+                    T.pmin[warp][lane] = mv;
+                    __syncthreads();
+                    if (warp == 0 && in) {
+                        double m = 1.e30;
+#pragma unroll
+                        for (int w = 0; w < kEB / 32; w++) m = T.pmin[w][lane] < m ? T.pmin[w][lane] : m;
+                        T.ts[lane] = m;
+                    }
+                } else {
+                    if (warp == 0) {
+                        const DS a = ds_split(T.x[lane]), b = ds_split(T.y[lane]),
+                                 c = ds_split(T.z[lane]);
+                        T.A[lane] = make_float4(a.hi, b.hi, c.hi, (float)T.m[lane]);
+                        T.B[lane] = make_float4(a.lo, b.lo, c.lo, 0.0f);
+                        T.V[lane] = make_float4((float)T.vx[lane], (float)T.vy[lane],
+                                                (float)T.vz[lane], 0.0f);
+                    }
+                    __syncthreads();
+                    float mr = 0.0f;
+                    if (in) {
+                        const float4 Ai = T.A[lane], Bi = T.B[lane], Vi = T.V[lane];
+#pragma unroll 1
+                        for (int j = warp; j < 32; j += kEB / 32) {
+                            if (!((mask >> j) & 1u) || j == lane) continue;
+                            const float4 A = T.A[j], B = T.B[j], V = T.V[j];
+                            mr = fmaxf(mr, ts_pair_rate_mixed(
+                                               ds_diff(Ai.x, Bi.x, A.x, B.x), ds_diff(Ai.y, Bi.y, A.y, B.y),
+                                               ds_diff(Ai.z, Bi.z, A.z, B.z), Vi.x - V.x, Vi.y - V.y,
+                                               Vi.z - V.z, Ai.w + A.w, E.inv_eta_s2, E.inv_eta));
+                        }
+                    }
+                    T.pmax[warp][lane] = mr;
+                    __syncthreads();
+                    if (warp == 0 && in) {
+                        float m = 0.0f;
+#pragma unroll
+                        for (int w = 0; w < kEB / 32; w++) m = fmaxf(m, T.pmax[w][lane]);
+                        const double tv = 1.0 / (double)m;
+                        T.ts[lane] = tv < 1.e30 ? tv : 1.e30;
                     }
                 }
-                __syncwarp();
+                __syncthreads();
             }
-            unsigned F = __ballot_sync(HHS_FULL_MASK, in && ts <= dt);
-            int lone = -1;
-            if (__popc(F) == 1) { lone = __ffs(F) - 1; F = 0u; }
-            if (lane == 0) {
-                sm.wfast[d] = F;
-                sm.wlone[d] = lone;
-                const int nf = __popc(F);
-                const double ns = (double)(cnt - nf), nfd = (double)nf;
-                if (nf == 0) *E.leaf_time += dt;
-                atomicAdd(reinterpret_cast<unsigned long long*>(&E.stats->nodes), 1ull);
-                atomicMax(&E.stats->max_level, lvl);
-                atomicAdd(&E.stats->kick_pairs, ns * (ns - 1.0) + 2.0 * ns * nfd);
-                if (calcm & bit) atomicAdd(&E.stats->ts_pairs, (double)cnt * (double)(cnt - 1));
+            if (warp == 0) {
+                unsigned F = __ballot_sync(HHS_FULL_MASK, in && T.ts[lane] <= dt);
+                int lone = -1;
+                if (__popc(F) == 1) { lone = __ffs(F) - 1; F = 0u; }
+                if (lane == 0) {
+                    sm.wfast[d] = F;
+                    sm.wlone[d] = lone;
+                    const int nf = __popc(F);
+                    const double ns = (double)(cnt - nf), nfd = (double)nf;
+                    if (nf == 0) *E.leaf_time += dt;
+                    atomicAdd(reinterpret_cast<unsigned long long*>(&E.stats->nodes), 1ull);
+                    atomicMax(&E.stats->max_level, lvl);
+                    atomicAdd(&E.stats->kick_pairs, ns * (ns - 1.0) + 2.0 * ns * nfd);
+                    if (calcm & bit) atomicAdd(&E.stats->ts_pairs, (double)cnt * (double)(cnt - 1));
+                }
             }
-            __syncwarp();
+            __syncthreads();
             after1 |= bit;
-            if (F) {
+            if (sm.wfast[d]) {
                 d++;
                 const unsigned long long cb = 1ull << d;
                 calcm &= ~cb; after1 &= ~cb; after2 &= ~cb;
@@ -746,81 +816,108 @@ __device__ void warp_hold(const EParams& E, const int32_t* S, int n, int level0,
             const bool is_slow = (L >> lane) & 1u, is_fast = (F >> lane) & 1u;
             const double h = dt * 0.5;
             if (L) {
-                // first half drift of the slow lanes (src/hold.cuh:123-124)
-                if (is_slow) {
-                    if (PREC == HHS_PREC_FP64) {
-                        x = f64_add(x, f64_mul(vx, h)); y = f64_add(y, f64_mul(vy, h));
-                        z = f64_add(z, f64_mul(vz, h));
-                    } else {
-                        x = fma(vx, h, x); y = fma(vy, h, y); z = fma(vz, h, z);
+                if (warp == 0) {
+                    // first half drift of the slow slots (src/hold.cuh:123-124)
+                    if (is_slow) {
+                        if (PREC == HHS_PREC_FP64) {
+                            T.x[lane] = f64_add(T.x[lane], f64_mul(T.vx[lane], h));
+                            T.y[lane] = f64_add(T.y[lane], f64_mul(T.vy[lane], h));
+                            T.z[lane] = f64_add(T.z[lane], f64_mul(T.vz[lane], h));
+                        } else {
+                            T.x[lane] = fma(T.vx[lane], h, T.x[lane]);
+                            T.y[lane] = fma(T.vy[lane], h, T.y[lane]);
+                            T.z[lane] = fma(T.vz[lane], h, T.z[lane]);
+                        }
+                    }
+                    if (PREC != HHS_PREC_FP64) {
+                        __syncwarp();
+                        const DS a = ds_split(T.x[lane]), b = ds_split(T.y[lane]),
+                                 c = ds_split(T.z[lane]);
+                        T.A[lane] = make_float4(a.hi, b.hi, c.hi, (float)T.m[lane]);
+                        T.B[lane] = make_float4(a.lo, b.lo, c.lo, 0.0f);
                     }
                 }
-                warp_stage(sm, lane, x, y, z, vx, vy, vz, m);
-                const unsigned Lord = lone >= 0 ? (L & ~(1u << lone)) : L;
+                __syncthreads();
                 if (PREC == HHS_PREC_FP64) {
-                    double aL[3] = {0, 0, 0}, aF[3] = {0, 0, 0};
-                    if (is_slow || is_fast) {
+                    if (warp == 0 && (is_slow || is_fast)) {
+                        const double xi = T.x[lane], yi = T.y[lane], zi = T.z[lane];
+                        const unsigned Lord = lone >= 0 ? (L & ~(1u << lone)) : L;
+                        double aL[3] = {0, 0, 0}, aF[3] = {0, 0, 0};
+#pragma unroll 1
                         for (unsigned mm = Lord; mm; mm &= mm - 1u) {
                             const int j = __ffs(mm) - 1;
-                            kick_pair_fp64(f64_sub(sm.u.tsd.x[j], x), f64_sub(sm.u.tsd.y[j], y),
-                                           f64_sub(sm.u.tsd.z[j], z), sm.u.tsd.m[j], aL[0], aL[1],
-                                           aL[2]);
+                            kick_pair_fp64(f64_sub(T.x[j], xi), f64_sub(T.y[j], yi),
+                                           f64_sub(T.z[j], zi), T.m[j], aL[0], aL[1], aL[2]);
                         }
                         if (lone >= 0)
-                            kick_pair_fp64(f64_sub(sm.u.tsd.x[lone], x), f64_sub(sm.u.tsd.y[lone], y),
-                                           f64_sub(sm.u.tsd.z[lone], z), sm.u.tsd.m[lone], aL[0],
-                                           aL[1], aL[2]);
-                    }
-                    if (is_slow) {
-                        for (unsigned mm = F; mm; mm &= mm - 1u) {
-                            const int j = __ffs(mm) - 1;
-                            kick_pair_fp64(f64_sub(sm.u.tsd.x[j], x), f64_sub(sm.u.tsd.y[j], y),
-                                           f64_sub(sm.u.tsd.z[j], z), sm.u.tsd.m[j], aF[0], aF[1],
-                                           aF[2]);
+                            kick_pair_fp64(f64_sub(T.x[lone], xi), f64_sub(T.y[lone], yi),
+                                           f64_sub(T.z[lone], zi), T.m[lone], aL[0], aL[1], aL[2]);
+                        if (is_slow) {
+#pragma unroll 1
+                            for (unsigned mm = F; mm; mm &= mm - 1u) {
+                                const int j = __ffs(mm) - 1;
+                                kick_pair_fp64(f64_sub(T.x[j], xi), f64_sub(T.y[j], yi),
+                                               f64_sub(T.z[j], zi), T.m[j], aF[0], aF[1], aF[2]);
+                            }
                         }
-                    }
-                    if (is_slow || is_fast) {
-                        const double v0x = vx, v0y = vy, v0z = vz;
-                        vx = f64_add(vx, f64_mul(aL[0], dt));
-                        vy = f64_add(vy, f64_mul(aL[1], dt));
-                        vz = f64_add(vz, f64_mul(aL[2], dt));
+                        double vx = f64_add(T.vx[lane], f64_mul(aL[0], dt));
+                        double vy = f64_add(T.vy[lane], f64_mul(aL[1], dt));
+                        double vz = f64_add(T.vz[lane], f64_mul(aL[2], dt));
                         if (is_slow && F) {
                             vx = f64_add(vx, f64_mul(aF[0], dt));
                             vy = f64_add(vy, f64_mul(aF[1], dt));
                             vz = f64_add(vz, f64_mul(aF[2], dt));
                         }
-                        (void)v0x; (void)v0y; (void)v0z;
-                    }
-                    if (is_slow) {
-                        x = f64_add(x, f64_mul(vx, h)); y = f64_add(y, f64_mul(vy, h));
-                        z = f64_add(z, f64_mul(vz, h));
+                        __syncwarp(__activemask());
+                        T.vx[lane] = vx; T.vy[lane] = vy; T.vz[lane] = vz;
+                        if (is_slow) {
+                            T.x[lane] = f64_add(xi, f64_mul(vx, h));
+                            T.y[lane] = f64_add(yi, f64_mul(vy, h));
+                            T.z[lane] = f64_add(zi, f64_mul(vz, h));
+                        }
                     }
                 } else {
-                    const DS xi = ds_split(x), yi = ds_split(y), zi = ds_split(z);
-                    float a[3] = {0, 0, 0}, c[3] = {0, 0, 0};
+                    float a[3] = {0, 0, 0};
                     const unsigned srcs = is_slow ? (L | F) : (is_fast ? L : 0u);
-                    for (unsigned mm = srcs; mm; mm &= mm - 1u) {
-                        const int j = __ffs(mm) - 1;
-                        const DS xj = ds_split(sm.u.tsd.x[j]), yj = ds_split(sm.u.tsd.y[j]),
-                                 zj = ds_split(sm.u.tsd.z[j]);
-                        const float dx = ds_diff(xj.hi, xj.lo, xi.hi, xi.lo);
-                        const float dy = ds_diff(yj.hi, yj.lo, yi.hi, yi.lo);
-                        const float dz = ds_diff(zj.hi, zj.lo, zi.hi, zi.lo);
-                        const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        const float ri = rsqrt_nr(d2);
-                        const float mr3 = (d2 > 0.0f) ? (float)sm.u.tsd.m[j] * ri * ri * ri : 0.0f;
-                        kahan_add(a[0], c[0], dx * mr3);
-                        kahan_add(a[1], c[1], dy * mr3);
-                        kahan_add(a[2], c[2], dz * mr3);
+                    if (srcs) {
+                        const float4 Ai = T.A[lane], Bi = T.B[lane];
+#pragma unroll 1
+                        for (int j = warp; j < 32; j += kEB / 32) {
+                            if (!((srcs >> j) & 1u)) continue;
+                            const float4 A = T.A[j], B = T.B[j];
+                            const float dx = ds_diff(A.x, B.x, Ai.x, Bi.x);
+                            const float dy = ds_diff(A.y, B.y, Ai.y, Bi.y);
+                            const float dz = ds_diff(A.z, B.z, Ai.z, Bi.z);
+                            const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                            const float ri = rsqrt_nr(d2);
+                            const float mr3 = (d2 > 0.0f) ? A.w * ri * ri * ri : 0.0f;
+                            a[0] = fmaf(dx, mr3, a[0]);
+                            a[1] = fmaf(dy, mr3, a[1]);
+                            a[2] = fmaf(dz, mr3, a[2]);
+                        }
                     }
-                    if (is_slow || is_fast) {
-                        vx = fma((double)a[0] - (double)c[0], dt, vx);
-                        vy = fma((double)a[1] - (double)c[1], dt, vy);
-                        vz = fma((double)a[2] - (double)c[2], dt, vz);
+                    T.part[warp][0][lane] = a[0];
+                    T.part[warp][1][lane] = a[1];
+                    T.part[warp][2][lane] = a[2];
+                    __syncthreads();
+                    if (warp == 0 && (is_slow || is_fast)) {
+                        double acc[3] = {0, 0, 0};
+#pragma unroll
+                        for (int w = 0; w < kEB / 32; w++)
+#pragma unroll
+                            for (int k = 0; k < 3; k++) acc[k] += (double)T.part[w][k][lane];
+                        const double vx = fma(acc[0], dt, T.vx[lane]);
+                        const double vy = fma(acc[1], dt, T.vy[lane]);
+                        const double vz = fma(acc[2], dt, T.vz[lane]);
+                        T.vx[lane] = vx; T.vy[lane] = vy; T.vz[lane] = vz;
+                        if (is_slow) {
+                            T.x[lane] = fma(vx, h, T.x[lane]);
+                            T.y[lane] = fma(vy, h, T.y[lane]);
+                            T.z[lane] = fma(vz, h, T.z[lane]);
+                        }
                     }
-                    if (is_slow) { x = fma(vx, h, x); y = fma(vy, h, y); z = fma(vz, h, z); }
                 }
-                __syncwarp();
+                __syncthreads();
             }
             after2 |= bit;
             if (F) {
@@ -834,12 +931,14 @@ __device__ void warp_hold(const EParams& E, const int32_t* S, int n, int level0,
         calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
         d--;
     }
-    (void)ok;
-    if (act) {
-        P.x[g] = x; P.y[g] = y; P.z[g] = z;
-        P.vx[g] = vx; P.vy[g] = vy; P.vz[g] = vz;
-        P.ts[g] = ts;
+    __syncthreads();
+    if ((int)threadIdx.x < n) {
+        const int g = T.g[threadIdx.x];
+        P.x[g] = T.x[threadIdx.x]; P.y[g] = T.y[threadIdx.x]; P.z[g] = T.z[threadIdx.x];
+        P.vx[g] = T.vx[threadIdx.x]; P.vy[g] = T.vy[threadIdx.x]; P.vz[g] = T.vz[threadIdx.x];
+        P.ts[g] = T.ts[threadIdx.x];
     }
+    __syncthreads();
 }
 
 // ---------------------------------------------------------------- the recursion
@@ -866,9 +965,9 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                 return false;
             }
             if (n <= E.warp_n) {
-                if (W.id == 0 && (threadIdx.x >> 5) == 0) warp_hold<PREC>(E, S, n, lvl, calc, sm);
+                if (W.id == 0) tiny_hold<PREC>(E, S, n, lvl, calc, sm);
                 if (!phase_barrier(E, sm, W)) return false;
-                prof_mark(E, W, t_last, kProfSubtree, 0.0, lvl);
+                prof_mark(E, W, t_last, kProfSubtree, 0.0, sm, lvl);
                 calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
                 lvl--;
                 continue;
@@ -883,7 +982,7 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                         run_hold<PREC, kModeCluster>(E, lvl, calc, cw, sm, t_sub);
                     }
                     if (!phase_barrier(E, sm, W)) return false;
-                    prof_mark(E, W, t_last, kProfCluster, 0.0, lvl);
+                    prof_mark(E, W, t_last, kProfCluster, 0.0, sm, lvl);
                     calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
                     lvl--;
                     continue;
@@ -896,7 +995,7 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                     run_hold<PREC, kModeBlock>(E, lvl, calc, one, sm, t_sub);
                 }
                 if (!phase_barrier(E, sm, W)) return false;
-                prof_mark(E, W, t_last, kProfSubtree, 0.0, lvl);
+                prof_mark(E, W, t_last, kProfSubtree, 0.0, sm, lvl);
                 calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
                 lvl--;
                 continue;
@@ -922,7 +1021,7 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                     }
                 }
                 if (!phase_barrier(E, sm, W)) return false;
-                prof_mark(E, W, t_last, kProfTs, (double)n * (double)(n - 1), lvl);
+                prof_mark(E, W, t_last, kProfTs, (double)n * (double)(n - 1), sm, lvl);
                 count_phase<PREC>(E, S, n, dt, true, nch, W, sm);
             } else {
                 count_phase<PREC>(E, S, n, dt, false, 1, W, sm);
@@ -930,7 +1029,7 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
             if (!phase_barrier(E, sm, W)) return false;
             scatter_phase(E, S, n, dt, lvl, calc, W, sm);
             if (!phase_barrier(E, sm, W)) return false;
-            prof_mark(E, W, t_last, kProfSplit, 0.0, lvl);
+            prof_mark(E, W, t_last, kProfSplit, 0.0, sm, lvl);
             after1 |= bit;
             const int nf = ld_volatile_i32(&E.counts[lvl].n_fast);
             if (nf > 0) {
@@ -958,10 +1057,10 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                 }
                 if (!phase_barrier(E, sm, W)) return false;
                 const double ns_d = ns, nf_d = nf;
-                prof_mark(E, W, t_last, kProfKick, ns_d * (ns_d - 1.0) + 2.0 * ns_d * nf_d, lvl);
+                prof_mark(E, W, t_last, kProfKick, ns_d * (ns_d - 1.0) + 2.0 * ns_d * nf_d, sm, lvl);
                 kick_reduce_phase<PREC>(E, F, L, nf, ns, dt, nch, C, W, sm);
                 if (!phase_barrier(E, sm, W)) return false;
-                prof_mark(E, W, t_last, kProfUpdate, 0.0, lvl);
+                prof_mark(E, W, t_last, kProfUpdate, 0.0, sm, lvl);
             }
             after2 |= bit;
             if (nf > 0) {
@@ -983,8 +1082,10 @@ __global__ void __launch_bounds__(kEB, 2) k_engine(EParams E) {
     __shared__ Smem sm;
     const Workers W{(int)blockIdx.x, (int)gridDim.x, kModeGrid};
     unsigned long long t_last = 0;
-    prof_mark(E, W, t_last, -1, 0.0);
+    prof_begin(E, sm);
+    prof_mark(E, W, t_last, -1, 0.0, sm);
     run_hold<PREC, kModeGrid>(E, 0, E.calc_top != 0, W, sm, t_last);
+    prof_end(E, sm);
 }
 
 // ---------------------------------------------------------------- batched systems

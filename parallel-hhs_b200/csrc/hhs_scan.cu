@@ -10,7 +10,9 @@ using ScanT = TileScan<kScanBlock, kScanItems>;
 
 // Exclusive scan of int32 values. VEC: 16-byte aligned input/output, so full chunks
 // move with one 128-bit streaming load/store per lane.
-template <bool VEC>
+// SELF_RESET: the last CTA resets the workspace header for the next call (used where the
+// workspace is reused without a memset); the standalone calls memset it instead.
+template <bool VEC, bool SELF_RESET>
 __global__ void __launch_bounds__(kScanBlock)
     k_scan_exclusive_i32(const int32_t* __restrict__ in, int32_t* __restrict__ out,
                          long long n, ScanHeader* hdr, unsigned long long* status,
@@ -25,7 +27,7 @@ __global__ void __launch_bounds__(kScanBlock)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long tbase = (long long)tile * ScanT::TILE;
 
-    unsigned v[kScanItems], ex[kScanItems];
+    unsigned v[kScanItems], cb[ScanT::CHUNKS];
 #pragma unroll
     for (int c = 0; c < ScanT::CHUNKS; c++) {
         const long long e = tbase + ScanT::offset(warp, c, lane);
@@ -37,27 +39,28 @@ __global__ void __launch_bounds__(kScanBlock)
             for (int k = 0; k < 4; k++) v[4 * c + k] = (e + k < n) ? (unsigned)in[e + k] : 0u;
         }
     }
-    ScanT::scan(v, ex, status, tile, epoch, &hdr->error, s_warp, &s_prefix);
+    ScanT::scan(v, cb, status, tile, epoch, &hdr->error, s_warp, &s_prefix);
 #pragma unroll
     for (int c = 0; c < ScanT::CHUNKS; c++) {
         const long long e = tbase + ScanT::offset(warp, c, lane);
+        const unsigned p0 = cb[c], p1 = p0 + v[4 * c], p2 = p1 + v[4 * c + 1],
+                       p3 = p2 + v[4 * c + 2];
         if (VEC && e + 4 <= n) {
-            __stcs(reinterpret_cast<int4*>(out + e),
-                   make_int4((int)ex[4 * c], (int)ex[4 * c + 1], (int)ex[4 * c + 2],
-                             (int)ex[4 * c + 3]));
+            __stcs(reinterpret_cast<int4*>(out + e), make_int4((int)p0, (int)p1, (int)p2, (int)p3));
         } else {
+            const unsigned pp[4] = {p0, p1, p2, p3};
 #pragma unroll
             for (int k = 0; k < 4; k++)
-                if (e + k < n) out[e + k] = (int)ex[4 * c + k];
+                if (e + k < n) out[e + k] = (int)pp[k];
         }
     }
-    if (scan_finish_is_last(hdr, num_tiles, &s_last)) scan_reset(hdr, epoch);
+    if (SELF_RESET && scan_finish_is_last(hdr, num_tiles, &s_last)) scan_reset(hdr, epoch);
 }
 
 // Stream compaction of int32 flags: the indices of the nonzero flags, in order, go to
 // idx_out[scan]; the exclusive scan of (flag != 0) optionally goes to scan_out; the last
 // CTA writes the number of selected elements to *count.
-template <bool VEC>
+template <bool VEC, bool SELF_RESET>
 __global__ void __launch_bounds__(kScanBlock)
     k_compact_flags(const int32_t* __restrict__ flags, int32_t* __restrict__ scan_out,
                     int32_t* __restrict__ idx_out, int32_t* __restrict__ count, long long n,
@@ -71,7 +74,7 @@ __global__ void __launch_bounds__(kScanBlock)
     const unsigned epoch = s_epoch;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long tbase = (long long)tile * ScanT::TILE;
-    unsigned v[kScanItems], ex[kScanItems];
+    unsigned v[kScanItems], cb[ScanT::CHUNKS];
 #pragma unroll
     for (int c = 0; c < ScanT::CHUNKS; c++) {
         const long long e = tbase + ScanT::offset(warp, c, lane);
@@ -84,29 +87,32 @@ __global__ void __launch_bounds__(kScanBlock)
             for (int k = 0; k < 4; k++) v[4 * c + k] = (e + k < n) ? (flags[e + k] != 0) : 0u;
         }
     }
-    ScanT::scan(v, ex, status, tile, epoch, &hdr->error, s_warp, &s_prefix);
+    ScanT::scan(v, cb, status, tile, epoch, &hdr->error, s_warp, &s_prefix);
 #pragma unroll
     for (int c = 0; c < ScanT::CHUNKS; c++) {
         const long long e = tbase + ScanT::offset(warp, c, lane);
+        unsigned pp[4];
+        pp[0] = cb[c];
+#pragma unroll
+        for (int k = 1; k < 4; k++) pp[k] = pp[k - 1] + v[4 * c + k - 1];
         if (scan_out) {
             if (VEC && e + 4 <= n) {
                 __stcs(reinterpret_cast<int4*>(scan_out + e),
-                       make_int4((int)ex[4 * c], (int)ex[4 * c + 1], (int)ex[4 * c + 2],
-                                 (int)ex[4 * c + 3]));
+                       make_int4((int)pp[0], (int)pp[1], (int)pp[2], (int)pp[3]));
             } else {
 #pragma unroll
                 for (int k = 0; k < 4; k++)
-                    if (e + k < n) scan_out[e + k] = (int)ex[4 * c + k];
+                    if (e + k < n) scan_out[e + k] = (int)pp[k];
             }
         }
 #pragma unroll
         for (int k = 0; k < 4; k++)
-            if (v[4 * c + k]) idx_out[ex[4 * c + k]] = (int)(e + k);
+            if (v[4 * c + k]) idx_out[pp[k]] = (int)(e + k);
     }
-    if (scan_finish_is_last(hdr, num_tiles, &s_last)) {
-        if (threadIdx.x == 0) *count = (int)(unsigned)ld_relaxed_u64(&status[num_tiles - 1]);
-        scan_reset(hdr, epoch);
-    }
+    // the tile holding the last element knows the total
+    if (tile == num_tiles - 1 && threadIdx.x == 0)
+        *count = (int)(unsigned)(ld_relaxed_u64(&status[num_tiles - 1]) & 0xffffffffull);
+    if (SELF_RESET && scan_finish_is_last(hdr, num_tiles, &s_last)) scan_reset(hdr, epoch);
 }
 
 constexpr int kSplitBlock = 256;
@@ -136,7 +142,7 @@ __global__ void __launch_bounds__(kSplitBlock)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long tbase = (long long)tile * SplitT::TILE;
 
-    unsigned v[kSplitItems], ex[kSplitItems];
+    unsigned v[kSplitItems], cb[SplitT::CHUNKS];
     int g[kSplitItems];
 #pragma unroll
     for (int c = 0; c < SplitT::CHUNKS; c++) {
@@ -154,15 +160,15 @@ __global__ void __launch_bounds__(kSplitBlock)
             }
         }
     }
-    SplitT::scan(v, ex, status, tile, epoch, &hdr->error, s_warp, &s_prefix);
+    SplitT::scan(v, cb, status, tile, epoch, &hdr->error, s_warp, &s_prefix);
 #pragma unroll
     for (int c = 0; c < SplitT::CHUNKS; c++) {
         const long long e = tbase + SplitT::offset(warp, c, lane);
+        unsigned p = cb[c];
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
+        for (int k = 0; k < 4; k++, p += v[4 * c + k - 1]) {
             const long long i = e + k;
             if (i < n) {
-                const unsigned p = ex[4 * c + k];
                 if (v[4 * c + k]) fast_out[p] = g[4 * c + k];
                 else slow_out[i - p] = g[4 * c + k];
                 if (pred_out) pred_out[i] = (int)v[4 * c + k];
@@ -244,11 +250,11 @@ extern "C" hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out
     const bool vec = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) &
                       15u) == 0;
     if (vec)
-        k_scan_exclusive_i32<true><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n, hdr, status,
-                                                                tiles);
+        k_scan_exclusive_i32<true, false><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n, hdr,
+                                                                       status, tiles);
     else
-        k_scan_exclusive_i32<false><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n, hdr, status,
-                                                                 tiles);
+        k_scan_exclusive_i32<false, false><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n, hdr,
+                                                                        status, tiles);
     HHS_LAUNCH_CHECK();
     return HHS_OK;
 }
@@ -275,11 +281,11 @@ extern "C" hhs_status hhs_compact_flags_i32(const int32_t* d_flags, int32_t* d_s
     const bool vec = ((reinterpret_cast<uintptr_t>(d_flags) |
                        reinterpret_cast<uintptr_t>(d_scan)) & 15u) == 0;
     if (vec)
-        k_compact_flags<true><<<tiles, kScanBlock, 0, s>>>(d_flags, d_scan, d_idx, d_count, n,
-                                                           hdr, status, tiles);
+        k_compact_flags<true, false><<<tiles, kScanBlock, 0, s>>>(d_flags, d_scan, d_idx,
+                                                                  d_count, n, hdr, status, tiles);
     else
-        k_compact_flags<false><<<tiles, kScanBlock, 0, s>>>(d_flags, d_scan, d_idx, d_count, n,
-                                                            hdr, status, tiles);
+        k_compact_flags<false, false><<<tiles, kScanBlock, 0, s>>>(d_flags, d_scan, d_idx,
+                                                                   d_count, n, hdr, status, tiles);
     HHS_LAUNCH_CHECK();
     return HHS_OK;
 }

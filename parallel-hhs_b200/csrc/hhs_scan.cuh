@@ -66,7 +66,7 @@ __device__ __forceinline__ unsigned scan_lookback(unsigned long long* status, in
                 if (flag == 0u) { flag = 2u; s = 0ull; }
                 break;
             }
-            __nanosleep(64);
+            if (spins > 64) __nanosleep(64);  // poll tightly first, then back off
         }
         unsigned val = (idx >= 0) ? (unsigned)s : 0u;
         const unsigned pm = __ballot_sync(HHS_FULL_MASK, flag == 2u);
@@ -96,21 +96,21 @@ struct TileScan {
         return (long long)warp * (32 * ITEMS) + c * 128 + lane * 4;
     }
 
-    // v: this thread's values. On return excl[k] holds each value's exclusive prefix
-    // within the whole input (tile prefix from the look-back included).
+    // v: this thread's values. On return cbase[c] holds the exclusive prefix (within the
+    // whole input, tile prefix from the look-back included) of the first value of chunk c;
+    // the prefixes of the other values follow by adding v in order.
     __device__ static __forceinline__ void scan(const unsigned (&v)[ITEMS],
-                                                unsigned (&excl)[ITEMS],
+                                                unsigned (&cbase)[CHUNKS],
                                                 unsigned long long* status, int tile,
                                                 unsigned epoch, unsigned* err,
                                                 unsigned* s_warp, unsigned* s_prefix) {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        unsigned cx[CHUNKS];
         unsigned run = 0u;
 #pragma unroll
         for (int c = 0; c < CHUNKS; c++) {
             const unsigned s = v[4 * c] + v[4 * c + 1] + v[4 * c + 2] + v[4 * c + 3];
             const unsigned inc = (unsigned)warp_incl_scan((int)s, lane);
-            cx[c] = run + inc - s;
+            cbase[c] = run + inc - s;
             run += (unsigned)__shfl_sync(HHS_FULL_MASK, (int)inc, 31);
         }
         if (lane == 0) s_warp[warp] = run;
@@ -126,14 +126,7 @@ struct TileScan {
         __syncthreads();
         const unsigned base = *s_prefix + s_warp[warp];
 #pragma unroll
-        for (int c = 0; c < CHUNKS; c++) {
-            unsigned p = base + cx[c];
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                excl[4 * c + k] = p;
-                p += v[4 * c + k];
-            }
-        }
+        for (int c = 0; c < CHUNKS; c++) cbase[c] += base;
     }
 };
 
