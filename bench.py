@@ -53,10 +53,12 @@ def parse():
     p.add_argument("--profile-out", default=None,
                    help="write the per-level phase profile (JSON) to this path")
     p.add_argument("--workload", default="plummer16k",
-                   choices=["plummer16k", "batched", "scan", "large", "deep"],
+                   choices=["plummer16k", "batched", "scan", "large", "deep", "validate"],
                    help="plummer16k (default headline), batched (512 clusters), scan (flag "
                         "compaction sweep), large (N=262144, 90/10 masses), deep (N=65536 "
-                        "Salpeter)")
+                        "Salpeter), validate (integrate to --t-end in mixed and FP64 precision "
+                        "and compare)")
+    p.add_argument("--t-end", type=float, default=1.0)
     p.add_argument("--scan-log2n", type=int, default=None,
                    help="scan workload: run this one size instead of the 2^20..2^28 sweep")
     p.add_argument("--no-baselines", action="store_true",
@@ -67,6 +69,26 @@ def parse():
 def workload_name(a):
     return (f"Plummer N={a.n} equal-mass Henon units, eta={a.eta}, dt_top=2^{int(round(__import__('math').log2(a.dt)))}, "
             f"{a.prec} precision, one top-level HOLD step per step")
+
+
+# ------------------------------------------------------------------------ ranks
+def replica_seed(seed, rank):
+    """Each rank integrates its own independently seeded system (replicas only)."""
+    return seed + 7919 * rank
+
+
+def max_over_ranks(value, dist, torch, device="cuda"):
+    """Max over all ranks of a per-rank time (the job's time is its slowest rank)."""
+    if dist is None:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_value(steps, world, t_max_ms):
+    """Whole-job throughput: all ranks' steps over the max-over-ranks time."""
+    return steps * world / (t_max_ms * 1e-3)
 
 
 # ------------------------------------------------------------------------ clocks
@@ -160,7 +182,7 @@ def run_ours(a, rank, world, torch, dist):
     stream = torch.cuda.Stream()
     sh = ctypes.c_void_p(stream.cuda_stream)
     prec = hhs.PREC_MIXED if a.prec == "mixed" else hhs.PREC_FP64
-    seed = a.seed + 7919 * rank
+    seed = replica_seed(a.seed, rank)
     ics = hhs.plummer(a.n, seed, getattr(a, "mass", 0))
     e0 = hhs.energy_host(ics)
     ctx = hhs.Context(a.n, 64, eta=a.eta)
@@ -222,13 +244,9 @@ def run_ours(a, rank, world, torch, dist):
         torch.cuda.synchronize()
     e1 = hhs.energy_host(out)
 
-    t_max = t_ms
-    if dist is not None:
-        t = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
+    t_max = max_over_ranks(t_ms, dist, torch)
     steps_total = a.steps * world
-    value = steps_total / (t_max * 1e-3)
+    value = aggregate_value(a.steps, world, t_max)
     pairs_step = (stats["kick_pairs"] + stats["ts_pairs"]) / a.steps
     res = {"value": value, "t_ms": t_max, "pairs_per_step": pairs_step, "stats": stats,
            "tuning": ctx.tuning(), "autotune": tuned,
@@ -272,11 +290,7 @@ def run_ours(a, rank, world, torch, dist):
                 pin[f][:] = res_pin[f]
         torch.cuda.synchronize()
         barrier()
-    t_e2e = sum(x.elapsed_time(y) for x, y in e2e_ev)
-    if dist is not None:
-        t = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    t_e2e = max_over_ranks(sum(x.elapsed_time(y) for x, y in e2e_ev), dist, torch)
     res["e2e"] = {"value": steps_total / (t_e2e * 1e-3), "unit": "HOLD steps/s",
                   "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
@@ -313,6 +327,7 @@ def run_ours(a, rank, world, torch, dist):
                 ctx.check(sh)
             res["fp64_engine_steps_per_s"] = k64 / (sum(x.elapsed_time(y) for x, y in evs) * 1e-3)
     res["fma_peaks"] = hhs.measure_fma_peaks(sh)
+    res["fma2_peak"] = hhs.measure_fma2_peak(sh)
     return res
 
 
@@ -485,6 +500,46 @@ def run_scan(a, torch):
                          "unit": "GB/s", "traffic": None}, "sweep": rows}
 
 
+def run_validate(a, torch):
+    """Integrates the workload to t_end in mixed precision and in FP64 (the FP64 device
+    schedule reproduces the CPU oracle bit for bit) and reports both energy errors, the
+    position deviation and the split agreement of the final state."""
+    import numpy as np
+    import hhs
+    steps = int(round(a.t_end / a.dt))
+    ics = hhs.plummer(a.n, a.seed, getattr(a, "mass", 0))
+    e0 = hhs.energy_host(ics)
+    out = {}
+    res = {}
+    for name, prec in (("mixed", hhs.PREC_MIXED), ("fp64", hhs.PREC_FP64)):
+        ctx = hhs.Context(a.n, 64, eta=a.eta)
+        d = hhs.ParticleSystem(a.n)
+        d.upload(ics)
+        ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        torch.cuda.synchronize()
+        ev[0].record()
+        for _ in range(steps):
+            hhs.hold_step(ctx, d, a.n, 0.0, a.dt, True, prec)
+        ev[1].record()
+        ctx.check()
+        res[name] = d.download()
+        e1 = hhs.energy_host(res[name])
+        st = ctx.stats()
+        out[name] = {"dE_over_E": (e1 - e0) / e0, "seconds": ev[0].elapsed_time(ev[1]) * 1e-3,
+                     "steps_per_s": steps / (ev[0].elapsed_time(ev[1]) * 1e-3),
+                     "nodes_per_step": st["nodes"] / steps, "max_level": st["max_level"],
+                     "simtime": ctx.simtime()}
+    m, f = res["mixed"], res["fp64"]
+    dx = max(float(np.max(np.abs(m[k] - f[k]))) for k in ("x", "y", "z"))
+    rel_ts = np.abs(m["ts"] - f["ts"]) / f["ts"]
+    return {"metric": "accuracy of the mixed-precision HOLD against FP64 after t_end",
+            "value": abs(out["mixed"]["dE_over_E"]), "unit": "|dE/E| (mixed)",
+            "n": a.n, "eta": a.eta, "dt_top": a.dt, "t_end": a.t_end, "steps": steps,
+            "results": out, "max_abs_dx_mixed_vs_fp64": dx,
+            "median_rel_ts_diff": float(np.median(rel_ts)),
+            "speedup_mixed_vs_fp64_device": out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"]}
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -504,23 +559,24 @@ def main():
         d.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                              device_id=torch.device("cuda", local))
         dist = d
-    if a.workload in ("batched", "scan"):
+    if a.workload == "large":
+        a.n, a.eta, a.mass = 262144, 0.02, 2
+    elif a.workload == "deep":
+        a.n, a.eta, a.mass = 65536, 0.02, 1
+    if a.workload in ("batched", "scan", "validate"):
         if rank == 0:
-            out = run_batched(a, torch) if a.workload == "batched" else run_scan(a, torch)
+            fn = {"batched": run_batched, "scan": run_scan, "validate": run_validate}[a.workload]
+            out = fn(a, torch)
             peaks = None
             try:
                 peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
             except (OSError, ValueError):
                 pass
-            if a.workload == "scan" and peaks:
+            if a.workload == "scan" and peaks and "roofline" in out:
                 out["roofline"]["peak"] = peaks["hbm_gbs"]
                 out["roofline"]["frac"] = out["value"] / peaks["hbm_gbs"]
             print(json.dumps(out), flush=True)
         return
-    if a.workload == "large":
-        a.n, a.eta, a.mass = 262144, 0.02, 2
-    elif a.workload == "deep":
-        a.n, a.eta, a.mass = 65536, 0.02, 1
     res = run_ours(a, rank, world, torch, dist)
     cpu = None
     if rank == 0 and world == 1 and not a.no_baselines:
@@ -549,7 +605,8 @@ def main():
             "clocks": res["clocks"],
             "roofline": roofline(res, a, res["fma_peaks"]),
             "kernel_profile": res["prof"],
-            "fma_peaks_tflops": {"fp32": res["fma_peaks"][0], "fp64": res["fma_peaks"][1]},
+            "fma_peaks_tflops": {"fp32": res["fma_peaks"][0], "fp64": res["fma_peaks"][1],
+                                 "fp32x2_packed": res["fma2_peak"]},
             "cpu_baseline": cpu,
         }
         if "fp64_plain_steps_per_s" in res:

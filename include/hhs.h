@@ -238,6 +238,8 @@ uint64_t hhs_kernel_launch_count(void);
 /* Measured arithmetic peaks of the current device: a register-resident chain of FP32
  * (and FP64) fused multiply-adds on every SM, timed with CUDA events. TFLOP/s. */
 hhs_status hhs_measure_fma_peaks(double* fp32_tflops, double* fp64_tflops, void* stream);
+/* The same chain with packed FP32 pairs (sm_100 fma.rn.f32x2). TFLOP/s. */
+hhs_status hhs_measure_fma2_peak(double* fp32x2_tflops, void* stream);
 
 /* ---- batched systems ------------------------------------------------------------ */
 /* Many independent systems packed back to back in one particle system: system k holds

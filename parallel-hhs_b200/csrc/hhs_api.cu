@@ -405,6 +405,11 @@ extern "C" hhs_status hhs_measure_fma_peaks(double* fp32_tflops, double* fp64_tf
     return measure_fma_peaks(fp32_tflops, fp64_tflops, static_cast<cudaStream_t>(stream));
 }
 
+extern "C" hhs_status hhs_measure_fma2_peak(double* fp32x2_tflops, void* stream) {
+    if (!fp32x2_tflops) return HHS_ERR_INVALID_ARG;
+    return measure_fma2_peak(fp32x2_tflops, static_cast<cudaStream_t>(stream));
+}
+
 // ------------------------------------------------------------------ reference-shaped ops
 extern "C" hhs_status hhs_timesteps(hhs_ctx* c, hhs_particle_system* sys, int32_t n,
                                     hhs_precision prec, void* stream) {

@@ -43,3 +43,4 @@ hhs_status launch_gather_split(const SoA& total, const SoA& slow, int32_t* slow_
 
 // ---- diagnostics (hhs_diag.cu)
 hhs_status measure_fma_peaks(double* fp32_tflops, double* fp64_tflops, cudaStream_t stream);
+hhs_status measure_fma2_peak(double* tflops, cudaStream_t stream);

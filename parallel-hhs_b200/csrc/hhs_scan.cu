@@ -4,9 +4,9 @@
 
 namespace {
 
-constexpr int kScanBlock = 256;
-constexpr int kScanItems = 16;  // 4096 values (16 KiB) per tile
-using ScanT = TileScan<kScanBlock, kScanItems>;
+constexpr int kScanBlock = 512;
+constexpr int kScanItems = 16;  // 8192 values (32 KiB) per tile
+using ScanT = TileScan<kScanBlock, kScanItems, 4>;  // 128-tile look-back windows
 
 // Exclusive scan of int32 values. VEC: 16-byte aligned input/output, so full chunks
 // move with one 128-bit streaming load/store per lane.

@@ -35,10 +35,13 @@ __device__ __forceinline__ unsigned scan_next_epoch(const ScanHeader* h) {
 }
 
 // Called by one full warp. Publishes this tile's aggregate, walks predecessors in
-// windows of 32, and publishes the inclusive prefix. Returns the exclusive prefix.
-__device__ __forceinline__ unsigned scan_lookback(unsigned long long* status, int tile,
-                                                  unsigned aggregate, unsigned epoch,
-                                                  unsigned* err) {
+// windows of 32*PER_LANE (each lane reads PER_LANE consecutive predecessors), and
+// publishes the inclusive prefix. Returns the exclusive prefix. Wider windows let the
+// inclusive prefixes propagate further per round trip to L2.
+template <int PER_LANE>
+__device__ __forceinline__ unsigned scan_lookback_w(unsigned long long* status, int tile,
+                                                    unsigned aggregate, unsigned epoch,
+                                                    unsigned* err) {
     const int lane = threadIdx.x & 31;
     if (tile == 0) {
         if (lane == 0) st_relaxed_u64(&status[0], scan_pack(epoch, 2u, aggregate));
@@ -49,43 +52,64 @@ __device__ __forceinline__ unsigned scan_lookback(unsigned long long* status, in
     int pred = tile - 1;
     unsigned spins = 0;
     while (true) {
-        const int idx = pred - lane;
-        unsigned long long s = 0ull;
-        unsigned flag;
+        unsigned val[PER_LANE], flag[PER_LANE];
         while (true) {
-            if (idx >= 0) {
-                s = ld_relaxed_u64(&status[idx]);
-                flag = ((unsigned)(s >> 34) == epoch) ? (unsigned)(s >> 32) & 3u : 0u;
-            } else {
-                flag = 2u;  // virtual tile -1: inclusive prefix 0
-                s = 0ull;
+            bool ready = true;
+#pragma unroll
+            for (int k = 0; k < PER_LANE; k++) {
+                const int idx = pred - (lane * PER_LANE + k);
+                if (idx >= 0) {
+                    const unsigned long long s = ld_relaxed_u64(&status[idx]);
+                    flag[k] = ((unsigned)(s >> 34) == epoch) ? (unsigned)(s >> 32) & 3u : 0u;
+                    val[k] = (unsigned)s;
+                } else {
+                    flag[k] = 2u;  // virtual tile -1: inclusive prefix 0
+                    val[k] = 0u;
+                }
+                ready = ready && flag[k] != 0u;
             }
-            if (__all_sync(HHS_FULL_MASK, flag != 0u)) break;
+            if (__all_sync(HHS_FULL_MASK, ready)) break;
             if (++spins > HHS_SPIN_LIMIT) {
                 if (lane == 0) atomicOr(err, HHS_ERRBIT_LOOKBACK_TIMEOUT);
-                if (flag == 0u) { flag = 2u; s = 0ull; }
+#pragma unroll
+                for (int k = 0; k < PER_LANE; k++)
+                    if (flag[k] == 0u) { flag[k] = 2u; val[k] = 0u; }
                 break;
             }
             if (spins > 64) __nanosleep(64);  // poll tightly first, then back off
         }
-        unsigned val = (idx >= 0) ? (unsigned)s : 0u;
-        const unsigned pm = __ballot_sync(HHS_FULL_MASK, flag == 2u);
+        // within this lane: values up to and including its first inclusive prefix
+        int firstp = PER_LANE;
+#pragma unroll
+        for (int k = PER_LANE - 1; k >= 0; k--)
+            if (flag[k] == 2u) firstp = k;
+        unsigned mine = 0u;
+#pragma unroll
+        for (int k = 0; k < PER_LANE; k++)
+            if (k <= firstp) mine += val[k];
+        const unsigned pm = __ballot_sync(HHS_FULL_MASK, firstp < PER_LANE);
         if (pm) {
             const int first = __ffs(pm) - 1;
-            excl += (unsigned)warp_sum((int)(lane <= first ? val : 0u));
+            excl += (unsigned)warp_sum((int)(lane <= first ? mine : 0u));
             break;
         }
-        excl += (unsigned)warp_sum((int)val);
-        pred -= 32;
+        excl += (unsigned)warp_sum((int)mine);
+        pred -= 32 * PER_LANE;
     }
     if (lane == 0) st_relaxed_u64(&status[tile], scan_pack(epoch, 2u, excl + aggregate));
     return excl;
 }
 
+__device__ __forceinline__ unsigned scan_lookback(unsigned long long* status, int tile,
+                                                  unsigned aggregate, unsigned epoch,
+                                                  unsigned* err) {
+    return scan_lookback_w<1>(status, tile, aggregate, epoch, err);
+}
+
 // Tile layout shared by the scan kernels: BLOCK threads x ITEMS values; value k of
 // chunk c of lane l in warp w sits at tile offset w*32*ITEMS + c*128 + l*4 + k, so a
 // warp's chunk is 128 consecutive values (one 16-byte load per lane).
-template <int BLOCK, int ITEMS>
+template <int BLOCK, int ITEMS, int LOOKBACK = 1>
 struct TileScan {
     static constexpr int TILE = BLOCK * ITEMS;
     static constexpr int CHUNKS = ITEMS / 4;
@@ -119,7 +143,7 @@ struct TileScan {
             const unsigned wt = (lane < WARPS) ? s_warp[lane] : 0u;
             const unsigned wi = (unsigned)warp_incl_scan((int)wt, lane);
             const unsigned total = (unsigned)__shfl_sync(HHS_FULL_MASK, (int)wi, 31);
-            const unsigned prefix = scan_lookback(status, tile, total, epoch, err);
+            const unsigned prefix = scan_lookback_w<LOOKBACK>(status, tile, total, epoch, err);
             if (lane < WARPS) s_warp[lane] = wi - wt;
             if (lane == 0) *s_prefix = prefix;
         }

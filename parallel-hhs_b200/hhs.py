@@ -133,6 +133,7 @@ SIGNATURES = {
     "hhs_ctx_get_level_profile": (ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_uint64)]),
     "hhs_kernel_launch_count": (ctypes.c_uint64, []),
     "hhs_measure_fma_peaks": (ctypes.c_int, [_dp, _dp, _vp]),
+    "hhs_measure_fma2_peak": (ctypes.c_int, [_dp, _vp]),
     "hhs_batch_create": (ctypes.c_int, [ctypes.c_int32, _ip, ctypes.c_int32, Params,
                                         ctypes.POINTER(_vp)]),
     "hhs_batch_destroy": (ctypes.c_int, [_vp]),
@@ -434,6 +435,12 @@ def measure_fma_peaks(stream=None):
     a, b = ctypes.c_double(), ctypes.c_double()
     _check(lib().hhs_measure_fma_peaks(ctypes.byref(a), ctypes.byref(b), stream), "fma_peaks")
     return a.value, b.value
+
+
+def measure_fma2_peak(stream=None):
+    a = ctypes.c_double()
+    _check(lib().hhs_measure_fma2_peak(ctypes.byref(a), stream), "fma2_peak")
+    return a.value
 
 
 def scan_workspace_size(n):
