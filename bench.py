@@ -47,6 +47,7 @@ def parse():
     p.add_argument("--ctas-per-sm", type=int, default=2)
     p.add_argument("--cluster-size", type=int, default=1)
     p.add_argument("--mid-n", type=int, default=0)
+    p.add_argument("--packed", type=int, default=0)
     p.add_argument("--units-per-cta", type=int, default=8)
     p.add_argument("--autotune", action="store_true",
                    help="pick the device-schedule tuning with the library's autotuner")
@@ -187,7 +188,7 @@ def run_ours(a, rank, world, torch, dist):
     e0 = hhs.energy_host(ics)
     ctx = hhs.Context(a.n, 64, eta=a.eta)
     ctx.set_tuning(a.small_n, a.units_per_cta, a.ctas_per_sm, cluster_size=a.cluster_size,
-                   mid_n=a.mid_n)
+                   mid_n=a.mid_n, packed=a.packed)
     sys_ = hhs.ParticleSystem(a.n)
     sys_.upload(ics, stream=sh)
     tuned = None

@@ -125,6 +125,8 @@ typedef struct {
     int32_t warp_n;          /* nodes with at most warp_n (<= 32) particles run on one warp */
     int32_t cluster_size;    /* launch the persistent kernel in thread-block clusters (1,2,4,8) */
     int32_t mid_n;           /* with clusters: nodes with small_n < n <= mid_n run on one cluster */
+    int32_t packed;          /* mixed kick: two sinks per thread in packed FP32x2 arithmetic */
+    int32_t _reserved;
     double ms_per_step;      /* filled by hhs_ctx_autotune: time of the chosen setting */
 } hhs_tuning;
 hhs_status hhs_ctx_set_tuning(hhs_ctx* ctx, const hhs_tuning* t);

@@ -601,7 +601,7 @@ extern "C" hhs_status hhs_ctx_autotune(hhs_ctx* c, hhs_particle_system* sys, int
     for (const Tier& tr : tiers) {
         for (int upc : upc_cands) {
             if (st != HHS_OK) break;
-            hhs_tuning t{tr.sn, upc, cps, cur.warp_n, tr.cs, tr.mid, 0.0};
+            hhs_tuning t{tr.sn, upc, cps, cur.warp_n, tr.cs, tr.mid, cur.packed, 0, 0.0};
             if (engine_set_tuning(c, t) != HHS_OK) continue;  // e.g. no cluster occupancy
             st = copy_all(false);
             if (st == HHS_OK) st = engine_hold_step(c, soa_of(sys), n, dt, true, prec, false, s);
@@ -656,7 +656,7 @@ extern "C" hhs_status hhs_hold_integrate(hhs_ctx* c, hhs_particle_system* sys, i
         ((unsigned long long)steps << 8) | (unsigned long long)prec,
         ((unsigned long long)t.small_n << 32) | (unsigned)t.mid_n,
         ((unsigned long long)t.units_per_cta << 32) |
-            (unsigned)(t.ctas_per_sm | (t.warp_n << 8) | (t.cluster_size << 16))};
+            (unsigned)(t.ctas_per_sm | (t.warp_n << 8) | (t.cluster_size << 16) | (t.packed << 24))};
     const bool hit = c->graph_exec && std::memcmp(key, c->graph_key, sizeof(key)) == 0;
     if (!hit) {
         if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }

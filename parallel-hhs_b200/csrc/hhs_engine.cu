@@ -65,6 +65,7 @@ struct EngineState {
 struct EParams {
     SoA P;
     int n_top, n_max, max_levels, small_n, calc_top, profile, units_per_cta, warp_n, mid_n;
+    int packed;  // mixed kick: two sinks per thread in packed FP32x2 arithmetic
     double dt_top, eta, eta_s2;
     float inv_eta_s2, inv_eta;
     int32_t* fast_lists;
@@ -85,6 +86,7 @@ struct __align__(16) Smem {
         struct { float4 A[kEB], B[kEB], V[kEB]; } tsm;         // mixed timestep tiles
         struct { double x[kEB], y[kEB], z[kEB], vx[kEB], vy[kEB], vz[kEB], m[kEB]; } tsd;
         struct { float4 A[kEB], B[kEB]; } km;                   // mixed kick tiles
+        struct { float4 P0[kEB], P1[kEB], P2[kEB]; float2 M[kEB]; } kx;  // packed kick tiles
         struct { double x[kEB], y[kEB], z[kEB], m[kEB]; } kd;   // FP64 kick tiles
         struct {                                                  // tiny-subtree state
             double x[32], y[32], z[32], vx[32], vy[32], vz[32], m[32], ts[32];
@@ -237,9 +239,10 @@ __device__ void prof_end(const EParams& E, Smem& sm) {
 }
 
 // number of source chunks for a node of n sinks
-__device__ __forceinline__ int chunks_for(int n, const Workers& W, bool split_ok, int upc) {
+__device__ __forceinline__ int chunks_for(int n, const Workers& W, bool split_ok, int upc,
+                                          int block = kEB) {
     if (W.mode == kModeBlock || !split_ok) return 1;
-    const int nsb = (n + kEB - 1) / kEB;
+    const int nsb = (n + block - 1) / block;
     int c = (upc * W.count + nsb - 1) / nsb;
     c = c < 1 ? 1 : (c > kMaxChunks ? kMaxChunks : c);
     const int maxc = (n + 63) / 64;  // at least 64 sources per chunk
@@ -439,6 +442,7 @@ __device__ void ts_sym_unit(const EParams& E, const int32_t* S, int n, int rb, i
     if (act && rowmax > 0.0f) atomicMax(&E.rate_acc[i], __float_as_uint(rowmax));
 }
 
+
 // ---------------------------------------------------------------- kick units
 // Sinks s in [0, nf + ns): s < nf -> F[s] (fast), else L[s - nf] (slow). Sources j in
 // [0, ns + nf): j < ns -> L[j] (drifted by h on the fly), else F[j - ns]. Fast sinks
@@ -553,6 +557,116 @@ __device__ void kick_unit(const EParams& E, const int32_t* F, const int32_t* L, 
                 part[(size_t)(jc * 3 + k) * n_max + s] = (double)acc[k] - (double)cmp[k];
         }
     }
+}
+
+
+// ---------------------------------------------------------------- packed kick units
+// The mixed kick with two sinks per thread (s and s + kEB) evaluated together in packed
+// FP32 pairs (fma/add/mul.rn.f32x2 of sm_100): one instruction advances both sinks'
+// pair terms, so the per-pair instruction count halves. Sources are staged once per
+// tile with each coordinate duplicated, so a 128-bit shared load fills two packed
+// operands. Self pairs (d2 == 0) contribute exactly 0 through a 1e-20 floor on d2
+// (finite rsqrt, zero numerator); for d2 >= 1e-20 the floor never changes d2.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+// lim0: sources at or beyond lim0 do not act on the first sink (a fast sink sharing the
+// thread with a slow one sees slow sources only)
+__device__ __forceinline__ void kick_x2_pairs(const Smem& sm, int jbeg, int jend, float2 nxh,
+                                              float2 nyh, float2 nzh, float2 nxl, float2 nyl,
+                                              float2 nzl, int lim0, float2& ax, float2& ay,
+                                              float2& az) {
+    const float2 half = f2(-0.5f, -0.5f), three_half = f2(1.5f, 1.5f);
+#pragma unroll 4
+    for (int jl = jbeg; jl < jend; jl++) {
+        const float4 P0 = sm.u.kx.P0[jl], P1 = sm.u.kx.P1[jl], P2 = sm.u.kx.P2[jl];
+        float2 M = sm.u.kx.M[jl];
+        if (jl >= lim0) M.x = 0.0f;
+        const float2 dx = __fadd2_rn(__fadd2_rn(f2(P0.x, P0.y), nxh), __fadd2_rn(f2(P1.z, P1.w), nxl));
+        const float2 dy = __fadd2_rn(__fadd2_rn(f2(P0.z, P0.w), nyh), __fadd2_rn(f2(P2.x, P2.y), nyl));
+        const float2 dz = __fadd2_rn(__fadd2_rn(f2(P1.x, P1.y), nzh), __fadd2_rn(f2(P2.z, P2.w), nzl));
+        float2 d2 = __fmul2_rn(dz, dz);
+        d2 = __ffma2_rn(dy, dy, d2);
+        d2 = __ffma2_rn(dx, dx, d2);
+        d2.x = fmaxf(d2.x, 1e-20f);
+        d2.y = fmaxf(d2.y, 1e-20f);
+        const float2 y = f2(rsqrtf(d2.x), rsqrtf(d2.y));
+        const float2 ri = __fmul2_rn(y, __ffma2_rn(__fmul2_rn(d2, half), __fmul2_rn(y, y), three_half));
+        const float2 ri2 = __fmul2_rn(ri, ri);
+        const float2 mr3 = __fmul2_rn(__fmul2_rn(M, ri2), ri);
+        ax = __ffma2_rn(dx, mr3, ax);
+        ay = __ffma2_rn(dy, mr3, ay);
+        az = __ffma2_rn(dz, mr3, az);
+    }
+}
+
+__device__ void kick_unit_x2(const EParams& E, const int32_t* F, const int32_t* L, int nf,
+                             int ns, double h, int ib, int jc, int j0, int j1, Smem& sm) {
+    const int n = nf + ns;
+    const SoA& P = E.P;
+    const int n_max = E.n_max;
+    int s[2];
+    s[0] = ib * (2 * kEB) + threadIdx.x;
+    s[1] = s[0] + kEB;
+    DS sx[2], sy[2], sz[2];
+    int jend[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const bool act = s[q] < n;
+        const bool slow = s[q] >= nf;
+        jend[q] = act ? (slow ? j1 : min(j1, ns)) : j0;
+        double x = 0, y = 0, z = 0;
+        if (act) {
+            const int g = slow ? L[s[q] - nf] : F[s[q]];
+            x = P.x[g]; y = P.y[g]; z = P.z[g];
+            if (slow) { x = fma(P.vx[g], h, x); y = fma(P.vy[g], h, y); z = fma(P.vz[g], h, z); }
+        }
+        sx[q] = ds_split(x); sy[q] = ds_split(y); sz[q] = ds_split(z);
+    }
+    const float2 nxh = f2(-sx[0].hi, -sx[1].hi), nyh = f2(-sy[0].hi, -sy[1].hi),
+                 nzh = f2(-sz[0].hi, -sz[1].hi), nxl = f2(-sx[0].lo, -sx[1].lo),
+                 nyl = f2(-sy[0].lo, -sy[1].lo), nzl = f2(-sz[0].lo, -sz[1].lo);
+    float acc[2][3] = {{0, 0, 0}, {0, 0, 0}}, cmp[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    for (int t0 = j0; t0 < j1; t0 += kEB) {
+        const int tl = min(kEB, j1 - t0);
+        __syncthreads();
+        if ((int)threadIdx.x < tl) {
+            const int j = t0 + threadIdx.x;
+            const bool js = j < ns;
+            const int gj = js ? L[j] : F[j - ns];
+            double x = P.x[gj], y = P.y[gj], z = P.z[gj];
+            if (js) { x = fma(P.vx[gj], h, x); y = fma(P.vy[gj], h, y); z = fma(P.vz[gj], h, z); }
+            const DS a = ds_split(x), b = ds_split(y), c = ds_split(z);
+            sm.u.kx.P0[threadIdx.x] = make_float4(a.hi, a.hi, b.hi, b.hi);
+            sm.u.kx.P1[threadIdx.x] = make_float4(c.hi, c.hi, a.lo, a.lo);
+            sm.u.kx.P2[threadIdx.x] = make_float4(b.lo, b.lo, c.lo, c.lo);
+            const float m = (float)P.m[gj];
+            sm.u.kx.M[threadIdx.x] = make_float2(m, m);
+        }
+        __syncthreads();
+        // fast sinks come first in a block, so when the two sinks' source limits differ
+        // the first sink is the fast one (smaller limit); an inactive second sink's
+        // results are never written
+        const int e0 = min(tl, jend[0] - t0), e1 = min(tl, jend[1] - t0);
+        const int emax = max(e0, e1);
+        for (int jb = 0; jb < emax; jb += 32) {
+            float2 bx = f2(0.f, 0.f), by = f2(0.f, 0.f), bz = f2(0.f, 0.f);
+            kick_x2_pairs(sm, jb, min(jb + 32, emax), nxh, nyh, nzh, nxl, nyl, nzl, e0, bx, by,
+                          bz);
+            kahan_add(acc[0][0], cmp[0][0], bx.x);
+            kahan_add(acc[0][1], cmp[0][1], by.x);
+            kahan_add(acc[0][2], cmp[0][2], bz.x);
+            kahan_add(acc[1][0], cmp[1][0], bx.y);
+            kahan_add(acc[1][1], cmp[1][1], by.y);
+            kahan_add(acc[1][2], cmp[1][2], bz.y);
+        }
+    }
+    double* part = E.k_part;
+#pragma unroll
+    for (int q = 0; q < 2; q++)
+        if (s[q] < n)
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                part[(size_t)(jc * 3 + k) * n_max + s[q]] = (double)acc[q][k] - (double)cmp[q][k];
 }
 
 // ---------------------------------------------------------------- node phases
@@ -1044,16 +1158,19 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
             const int ns = ld_volatile_i32(&E.counts[lvl].n_slow);
             if (ns > 0) {
                 const int ntot = nf + ns;
-                const int nch = chunks_for(ntot, W, PREC != HHS_PREC_FP64, E.units_per_cta);
+                const bool x2 = PREC != HHS_PREC_FP64 && E.packed;
+                const int blk = x2 ? 2 * kEB : kEB;
+                const int nch = chunks_for(ntot, W, PREC != HHS_PREC_FP64, E.units_per_cta, blk);
                 const int C = (ntot + nch - 1) / nch;
-                const int nsb = (ntot + kEB - 1) / kEB;
+                const int nsb = (ntot + blk - 1) / blk;
                 const double h = dt * 0.5;
                 for (int u = W.id; u < nsb * nch; u += W.count) {
                     const int ib = u / nch, jc = u % nch;
                     const int j0 = jc * C, j1 = min(ntot, j0 + C);
                     // blocks of fast sinks only need slow-source chunks
-                    if ((ib + 1) * kEB <= nf && j0 >= ns) continue;
-                    kick_unit<PREC>(E, F, L, nf, ns, h, ib, jc, j0, j1, sm);
+                    if ((ib + 1) * blk <= nf && j0 >= ns) continue;
+                    if (x2) kick_unit_x2(E, F, L, nf, ns, h, ib, jc, j0, j1, sm);
+                    else kick_unit<PREC>(E, F, L, nf, ns, h, ib, jc, j0, j1, sm);
                 }
                 if (!phase_barrier(E, sm, W)) return false;
                 const double ns_d = ns, nf_d = nf;
@@ -1182,6 +1299,7 @@ struct EngineHost {
     int warp_n = 32;
     int cluster_size = 1;
     int mid_n = 0;
+    int packed = 0;
     EngineState* st = nullptr;
     double* ts_part = nullptr;
     double* k_part = nullptr;
@@ -1247,6 +1365,7 @@ hhs_status engine_set_tuning(hhs_ctx* c, const hhs_tuning& t) {
     eh->warp_n = t.warp_n;
     eh->cluster_size = t.cluster_size;
     eh->mid_n = t.mid_n;
+    eh->packed = t.packed != 0;
     eh->small_n = t.small_n;
     eh->units_per_cta = t.units_per_cta;
     eh->ctas_per_sm = t.ctas_per_sm;
@@ -1285,6 +1404,7 @@ hhs_status engine_get_tuning(hhs_ctx* c, hhs_tuning* t) {
     t->warp_n = eh->warp_n;
     t->cluster_size = eh->cluster_size;
     t->mid_n = eh->mid_n;
+    t->packed = eh->packed;
     return HHS_OK;
 }
 
@@ -1339,6 +1459,7 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
     E.units_per_cta = eh->units_per_cta;
     E.warp_n = eh->warp_n;
     E.mid_n = eh->mid_n;
+    E.packed = eh->packed;
     E.calc_top = calc_ts ? 1 : 0;
     E.profile = profile ? 1 : 0;
     E.dt_top = dt;
@@ -1385,7 +1506,7 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
 struct hhs_batch {
     int n_sys = 0, n_total = 0, n_max_sys = 0, max_levels = 0;
     hhs_params params{0.03, 0.0};
-    int big_n = 1024, cluster_size = 8, small_n = 64, units_per_cta = 8, warp_n = 32;
+    int big_n = 1024, cluster_size = 8, small_n = 64, units_per_cta = 8, warp_n = 32, packed = 0;
     int n_big = 0, n_clusters[2] = {0, 0};
     void* arena = nullptr;
     int32_t* d_offsets = nullptr;
@@ -1546,6 +1667,7 @@ extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, d
     E.units_per_cta = b->units_per_cta;
     E.warp_n = b->warp_n;
     E.mid_n = 0;
+    E.packed = b->packed;
     E.dt_top = dt;
     E.eta = b->params.eta;
     E.eta_s2 = b->params.eta / 1.41421356237309504880;

@@ -116,4 +116,11 @@ __device__ __forceinline__ float ts_pair_rate_mixed(float drx, float dry, float 
     return dr2 == 0.0f ? __int_as_float(0x7f800000) : rate;
 }
 
+// ---- packed FP32 pairs (sm_100 f32x2) ----------------------------------------------
+__device__ __forceinline__ float2 rsqrt_nr2(float2 x) {
+    const float2 y = make_float2(rsqrtf(x.x), rsqrtf(x.y));
+    return __fmul2_rn(y, __ffma2_rn(__fmul2_rn(x, make_float2(-0.5f, -0.5f)), __fmul2_rn(y, y),
+                                    make_float2(1.5f, 1.5f)));
+}
+
 }  // namespace hhs

@@ -4,8 +4,8 @@
 
 namespace {
 
-constexpr int kScanBlock = 512;
-constexpr int kScanItems = 16;  // 8192 values (32 KiB) per tile
+constexpr int kScanBlock = 256;
+constexpr int kScanItems = 16;  // 4096 values (16 KiB) per tile
 using ScanT = TileScan<kScanBlock, kScanItems, 4>;  // 128-tile look-back windows
 
 // Exclusive scan of int32 values. VEC: 16-byte aligned input/output, so full chunks

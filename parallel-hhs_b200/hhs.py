@@ -63,6 +63,7 @@ class Tuning(ctypes.Structure):
     _fields_ = [("small_n", ctypes.c_int32), ("units_per_cta", ctypes.c_int32),
                 ("ctas_per_sm", ctypes.c_int32), ("warp_n", ctypes.c_int32),
                 ("cluster_size", ctypes.c_int32), ("mid_n", ctypes.c_int32),
+                ("packed", ctypes.c_int32), ("_reserved", ctypes.c_int32),
                 ("ms_per_step", ctypes.c_double)]
 
 
@@ -275,7 +276,7 @@ class Context:
         _check(lib().hhs_ctx_reset_stats(self.h, stream), "reset_stats")
 
     def set_tuning(self, small_n=None, units_per_cta=None, ctas_per_sm=None, warp_n=None,
-                   cluster_size=None, mid_n=None):
+                   cluster_size=None, mid_n=None, packed=None):
         t = Tuning()
         _check(lib().hhs_ctx_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
         if small_n is not None:
@@ -290,6 +291,8 @@ class Context:
             t.cluster_size = cluster_size
         if mid_n is not None:
             t.mid_n = mid_n
+        if packed is not None:
+            t.packed = int(packed)
         _check(lib().hhs_ctx_set_tuning(self.h, ctypes.byref(t)), "set_tuning")
 
     def tuning(self):
@@ -297,7 +300,7 @@ class Context:
         _check(lib().hhs_ctx_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
         return {"small_n": t.small_n, "units_per_cta": t.units_per_cta,
                 "ctas_per_sm": t.ctas_per_sm, "warp_n": t.warp_n,
-                "cluster_size": t.cluster_size, "mid_n": t.mid_n}
+                "cluster_size": t.cluster_size, "mid_n": t.mid_n, "packed": t.packed}
 
     def autotune(self, sys, n, dt, prec=1, stream=None):
         t = Tuning()
@@ -305,7 +308,8 @@ class Context:
                "autotune")
         return {"small_n": t.small_n, "units_per_cta": t.units_per_cta,
                 "ctas_per_sm": t.ctas_per_sm, "warp_n": t.warp_n,
-                "cluster_size": t.cluster_size, "mid_n": t.mid_n, "ms_per_step": t.ms_per_step}
+                "cluster_size": t.cluster_size, "mid_n": t.mid_n, "packed": t.packed,
+                "ms_per_step": t.ms_per_step}
 
     def set_profiling(self, on):
         _check(lib().hhs_ctx_set_profiling(self.h, int(on)), "set_profiling")

@@ -395,12 +395,13 @@ def test_hold_step_engine_fp64_bit_exact(cuda, hhs, oracle, n, small_n, spectrum
     assert ctx.simtime() == pytest.approx(leaf, rel=1e-15)
 
 
-@pytest.mark.parametrize("n,small_n", [(1024, 0), (4096, 256), (16384, 512)])
-def test_hold_step_engine_mixed_close(cuda, hhs, oracle, n, small_n):
+@pytest.mark.parametrize("n,small_n,packed", [(1024, 0, 0), (4096, 256, 0), (16384, 512, 0),
+                                              (1024, 0, 1), (5000, 64, 1)])
+def test_hold_step_engine_mixed_close(cuda, hhs, oracle, n, small_n, packed):
     s = _plummer(hhs, n, 30 + n)
     ref = {k: v.copy() for k, v in s.items()}
     ctx = hhs.Context(n, 64, eta=0.03)
-    ctx.set_tuning(small_n)
+    ctx.set_tuning(small_n, packed=packed)
     d = hhs.ParticleSystem(n)
     d.upload(s)
     e0 = hhs.energy_host(s)
