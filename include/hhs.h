@@ -198,6 +198,22 @@ hhs_status hhs_hold_step_host(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n,
 size_t hhs_scan_workspace_size(int64_t n);
 hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out, int64_t n,
                                   void* d_workspace, size_t workspace_bytes, void* stream);
+/* Allocation-free exclusive scan. No counterpart in the reference: it is an addition for
+ * callers that must not allocate device memory -- an application that has handed the
+ * device to its own memory pool, or a step loop that must run under a fixed device-memory
+ * budget -- and so cannot provide the workspace hhs_scan_exclusive_i32 needs. The same
+ * kernel runs with its workspace in a fixed 128.3 KiB array inside the library's own
+ * device memory, present on every device that loads the library until the process
+ * exits. Limit: n <= HHS_SCAN_NOALLOC_MAX_N (2^26 values); larger n returns
+ * HHS_ERR_CAPACITY. The call allocates nothing; it clears the part of the array it uses
+ * with cudaMemsetAsync before the launch. Every call shares the one array, so calls
+ * that overlap on the GPU (different streams, or several host threads at once) race:
+ * serialise them. The first call on each device looks up the array's device address;
+ * make that first call before any stream capture. */
+#define HHS_SCAN_NOALLOC_MAX_N (1LL << 26)
+hhs_status hhs_scan_exclusive_i32_noalloc(const int32_t* d_in, int32_t* d_out, int64_t n,
+                                          void* stream);
+
 /* Stream compaction (the split of a flag array, src/split.cuh:573-610 on int32 data):
  * d_idx[k] = index of the k-th nonzero flag, *d_count = number of nonzero flags, and
  * d_scan (optional, NULL = not written) = exclusive scan of (flag != 0). One pass;

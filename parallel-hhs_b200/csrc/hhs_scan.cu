@@ -1,4 +1,6 @@
 // hhs_scan.cu -- standalone exact exclusive scan and the fast/slow index split.
+#include <atomic>
+
 #include "hhs_scan.cuh"
 #include "hhs_kernels.h"
 
@@ -286,6 +288,67 @@ extern "C" hhs_status hhs_compact_flags_i32(const int32_t* d_flags, int32_t* d_s
     else
         k_compact_flags<false, false><<<tiles, kScanBlock, 0, s>>>(d_flags, d_scan, d_idx,
                                                                    d_count, n, hdr, status, tiles);
+    HHS_LAUNCH_CHECK();
+    return HHS_OK;
+}
+
+// ------------------------------------------------------------------ allocation-free scan
+// The same single-pass scan for callers that may not allocate device memory: its
+// workspace is this file-scope device array (128.3 KiB, present on every device that
+// loads the library until the process exits), so inputs are limited to
+// kStaticScanTiles tiles of ScanT::TILE values (2^26 = 67,108,864 values).
+constexpr int kStaticScanTiles = 16384;
+constexpr size_t kStaticScanBytes =
+    sizeof(ScanHeader) + sizeof(unsigned long long) * (size_t)kStaticScanTiles;
+constexpr long long kStaticScanMaxN = (long long)kStaticScanTiles * ScanT::TILE;
+static_assert(kStaticScanMaxN == HHS_SCAN_NOALLOC_MAX_N, "limit stated in hhs.h");
+static __device__ __align__(256) unsigned char g_static_scan_ws[kStaticScanBytes];
+
+namespace {
+// Device address of g_static_scan_ws per device, looked up once with that device current
+// (in host code the array's name is only a host-side stand-in, not a device address).
+constexpr int kMaxDevices = 64;
+std::atomic<void*> g_static_ws_addr[kMaxDevices];
+
+hhs_status static_scan_workspace(void** out) {
+    int dev = 0;
+    HHS_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return HHS_ERR_CUDA;
+    void* p = g_static_ws_addr[dev].load(std::memory_order_acquire);
+    if (!p) {
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scan_ws);
+        if (e != cudaSuccess || !p) return hhs_from_cuda(e == cudaSuccess ? cudaErrorUnknown : e);
+        g_static_ws_addr[dev].store(p, std::memory_order_release);
+    }
+    *out = p;
+    return HHS_OK;
+}
+}  // namespace
+
+extern "C" hhs_status hhs_scan_exclusive_i32_noalloc(const int32_t* d_in, int32_t* d_out,
+                                                     int64_t n, void* stream) {
+    if (n < 0 || (n > 0 && (!d_in || !d_out))) return HHS_ERR_INVALID_ARG;
+    if (n == 0) return HHS_OK;
+    if (n > kStaticScanMaxN) return HHS_ERR_CAPACITY;
+    void* ws = nullptr;
+    hhs_status st = static_scan_workspace(&ws);
+    if (st != HHS_OK) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int tiles = (int)((n + ScanT::TILE - 1) / ScanT::TILE);
+    // the array keeps the previous call's contents: clear the header and the status words
+    // this call uses
+    HHS_CUDA_TRY(cudaMemsetAsync(ws, 0, scan_workspace_bytes(n, ScanT::TILE), s));
+    auto* hdr = static_cast<ScanHeader*>(ws);
+    auto* status = reinterpret_cast<unsigned long long*>(static_cast<char*>(ws) +
+                                                         sizeof(ScanHeader));
+    const bool vec = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) &
+                      15u) == 0;
+    if (vec)
+        k_scan_exclusive_i32<true, false><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n, hdr,
+                                                                       status, tiles);
+    else
+        k_scan_exclusive_i32<false, false><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n, hdr,
+                                                                        status, tiles);
     HHS_LAUNCH_CHECK();
     return HHS_OK;
 }

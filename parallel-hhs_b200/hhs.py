@@ -120,6 +120,7 @@ SIGNATURES = {
     "hhs_scan_exclusive_i32": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp, ctypes.c_size_t,
                                               _vp]),
     "hhs_scan_workspace_status": (ctypes.c_int, [_vp, _vp]),
+    "hhs_scan_exclusive_i32_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp]),
     "hhs_compact_flags_i32": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int64, _vp,
                                              ctypes.c_size_t, _vp]),
     "hhs_ic_plummer": (ctypes.c_int, [ctypes.c_int32, ctypes.c_uint64, ctypes.c_int32]
