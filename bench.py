@@ -462,6 +462,7 @@ def run_scan(a, torch):
         return sum(x.elapsed_time(y) for x, y in ev) / reps
 
     sizes = [a.scan_log2n] if a.scan_log2n else list(range(20, 29, 2))
+    probs = (0.5,) if a.scan_log2n else (0.01, 0.1, 0.5)
     for lg in sizes:
         n = 1 << lg
         ws_b = hhs.scan_workspace_size(n)
@@ -469,7 +470,7 @@ def run_scan(a, torch):
         out = torch.empty(n, dtype=torch.int32, device="cuda")
         idx = torch.empty(n, dtype=torch.int32, device="cuda")
         cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
-        for p in (0.01, 0.1, 0.5):
+        for p in probs:
             g = torch.Generator(device="cuda").manual_seed(lg * 10 + int(p * 100))
             flags = (torch.rand(n, device="cuda", generator=g) < p).to(torch.int32)
             ms_scan = timed(lambda: hhs.scan_exclusive_i32(ptr(flags), ptr(out), n, ptr(ws), ws_b,

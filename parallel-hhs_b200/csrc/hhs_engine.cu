@@ -134,19 +134,24 @@ __device__ bool grid_barrier(const EParams& E, Smem& sm) {
     if (cs > 1) cg::this_cluster().sync();
     else __syncthreads();
     if (leader && threadIdx.x == 0) {
+        // The CTA barrier above orders every thread's writes before this thread's
+        // release; arrival is an acquire-release add (the last arrival acquires all the
+        // others' releases), the generation is advanced with a release add and polled
+        // with acquire loads, so no separate fences are needed.
         int ok = 1;
         EngineState* st = E.st;
         const unsigned parties = gridDim.x / cs;
-        const unsigned gen = *reinterpret_cast<volatile unsigned*>(&st->bar_gen);
-        __threadfence();
-        const unsigned arrived = atomicAdd(&st->bar_count, 1u);
+        const unsigned gen = ld_acquire_u32(&st->bar_gen);
+        const unsigned arrived = atom_add_acq_rel_u32(&st->bar_count, 1u);
         if (arrived == parties - 1) {
             *reinterpret_cast<volatile unsigned*>(&st->bar_count) = 0u;
-            __threadfence();
-            atomicAdd(&st->bar_gen, 1u);
+            red_add_release_u32(&st->bar_gen, 1u);
         } else {
-            const unsigned long long t0 = gtimer();
+            unsigned polls = 0;
+            unsigned long long t0 = 0;
             while (ld_acquire_u32(&st->bar_gen) == gen) {
+                if (++polls < 256) continue;  // tight polling first
+                if (t0 == 0) t0 = gtimer();
                 if (*reinterpret_cast<volatile unsigned*>(E.err) != 0u) { ok = 0; break; }
                 __nanosleep(32);
                 if (gtimer() - t0 > kBarrierTimeoutNs) {
@@ -156,7 +161,6 @@ __device__ bool grid_barrier(const EParams& E, Smem& sm) {
                 }
             }
         }
-        __threadfence();
         sm.ok = ok;
     }
     if (cs > 1) {

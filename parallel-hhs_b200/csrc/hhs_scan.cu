@@ -1,5 +1,6 @@
 // hhs_scan.cu -- standalone exact exclusive scan and the fast/slow index split.
 #include <atomic>
+#include <cstdlib>
 
 #include "hhs_scan.cuh"
 #include "hhs_kernels.h"
@@ -8,7 +9,9 @@ namespace {
 
 constexpr int kScanBlock = 256;
 constexpr int kScanItems = 16;  // 4096 values (16 KiB) per tile
-using ScanT = TileScan<kScanBlock, kScanItems, 4>;  // 128-tile look-back windows
+using ScanT = TileScan<kScanBlock, kScanItems, 1>;
+// workspace sizes are quoted for the smallest tile any scan launch shape uses
+constexpr int kScanMinTile = 2048;
 
 // Exclusive scan of int32 values. VEC: 16-byte aligned input/output, so full chunks
 // move with one 128-bit streaming load/store per lane.
@@ -57,6 +60,71 @@ __global__ void __launch_bounds__(kScanBlock)
         }
     }
     if (SELF_RESET && scan_finish_is_last(hdr, num_tiles, &s_last)) scan_reset(hdr, epoch);
+}
+
+// Launch-shape variants of the standalone scan (tile = BLOCK x ITEMS values, look-back
+// windows of 32 x LB tiles, at least MINB resident CTAs per SM), selected by
+// scan_variant(); the default shape is variant 0.
+template <int BLOCK, int ITEMS, int LB, int MINB, bool VEC>
+__global__ void __launch_bounds__(BLOCK, MINB)
+    k_scan_v(const int32_t* __restrict__ in, int32_t* __restrict__ out, long long n,
+             ScanHeader* hdr, unsigned long long* status, int num_tiles) {
+    using T = TileScan<BLOCK, ITEMS, LB>;
+    __shared__ int s_tile;
+    __shared__ unsigned s_epoch, s_prefix;
+    __shared__ unsigned s_warp[T::WARPS];
+    scan_begin(hdr, &s_tile, &s_epoch);
+    const int tile = s_tile;
+    const unsigned epoch = s_epoch;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long tbase = (long long)tile * T::TILE;
+    unsigned v[ITEMS], cb[T::CHUNKS];
+#pragma unroll
+    for (int c = 0; c < T::CHUNKS; c++) {
+        const long long e = tbase + T::offset(warp, c, lane);
+        if (VEC && e + 4 <= n) {
+            const int4 q = __ldcs(reinterpret_cast<const int4*>(in + e));
+            v[4 * c] = q.x; v[4 * c + 1] = q.y; v[4 * c + 2] = q.z; v[4 * c + 3] = q.w;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) v[4 * c + k] = (e + k < n) ? (unsigned)in[e + k] : 0u;
+        }
+    }
+    T::scan(v, cb, status, tile, epoch, &hdr->error, s_warp, &s_prefix);
+#pragma unroll
+    for (int c = 0; c < T::CHUNKS; c++) {
+        const long long e = tbase + T::offset(warp, c, lane);
+        const unsigned p0 = cb[c], p1 = p0 + v[4 * c], p2 = p1 + v[4 * c + 1],
+                       p3 = p2 + v[4 * c + 2];
+        if (VEC && e + 4 <= n) {
+            __stcs(reinterpret_cast<int4*>(out + e), make_int4((int)p0, (int)p1, (int)p2, (int)p3));
+        } else {
+            const unsigned pp[4] = {p0, p1, p2, p3};
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (e + k < n) out[e + k] = (int)pp[k];
+        }
+    }
+}
+
+template <int BLOCK, int ITEMS, int LB, int MINB>
+void launch_scan_v(const int32_t* in, int32_t* out, long long n, void* ws, bool vec,
+                   cudaStream_t s) {
+    constexpr int TILE = BLOCK * ITEMS;
+    const int tiles = (int)((n + TILE - 1) / TILE);
+    auto* hdr = static_cast<ScanHeader*>(ws);
+    auto* status = reinterpret_cast<unsigned long long*>(static_cast<char*>(ws) +
+                                                         sizeof(ScanHeader));
+    if (vec) k_scan_v<BLOCK, ITEMS, LB, MINB, true><<<tiles, BLOCK, 0, s>>>(in, out, n, hdr, status, tiles);
+    else k_scan_v<BLOCK, ITEMS, LB, MINB, false><<<tiles, BLOCK, 0, s>>>(in, out, n, hdr, status, tiles);
+}
+
+int scan_variant() {
+    static int v = [] {
+        const char* e = std::getenv("HHS_SCAN_VARIANT");
+        return e ? std::atoi(e) : 0;
+    }();
+    return v;
 }
 
 // Stream compaction of int32 flags: the indices of the nonzero flags, in order, go to
@@ -231,7 +299,7 @@ hhs_status launch_split_list(const int32_t* list_in, int n, const double* ts, do
 unsigned* scan_workspace_error_word(void* ws) { return &static_cast<ScanHeader*>(ws)->error; }
 
 extern "C" size_t hhs_scan_workspace_size(int64_t n) {
-    return scan_workspace_bytes(n, ScanT::TILE);
+    return scan_workspace_bytes(n, kScanMinTile);
 }
 
 extern "C" hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out, int64_t n,
@@ -244,19 +312,28 @@ extern "C" hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out
     if ((reinterpret_cast<uintptr_t>(d_workspace) & 7u) != 0) return HHS_ERR_INVALID_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int tiles = (int)((n + ScanT::TILE - 1) / ScanT::TILE);
-    const size_t used = scan_workspace_bytes(n, ScanT::TILE);
+    const size_t used = scan_workspace_bytes(n, kScanMinTile);
     HHS_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, used, s));
     auto* hdr = static_cast<ScanHeader*>(d_workspace);
     auto* status = reinterpret_cast<unsigned long long*>(static_cast<char*>(d_workspace) +
                                                          sizeof(ScanHeader));
     const bool vec = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) &
                       15u) == 0;
-    if (vec)
-        k_scan_exclusive_i32<true, false><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n, hdr,
-                                                                       status, tiles);
-    else
-        k_scan_exclusive_i32<false, false><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n, hdr,
-                                                                        status, tiles);
+    switch (scan_variant()) {
+        case 1: launch_scan_v<256, 8, 1, 1>(d_in, d_out, n, d_workspace, vec, s); break;
+        case 2: launch_scan_v<128, 16, 1, 1>(d_in, d_out, n, d_workspace, vec, s); break;
+        case 3: launch_scan_v<256, 16, 1, 6>(d_in, d_out, n, d_workspace, vec, s); break;
+        case 4: launch_scan_v<512, 16, 1, 1>(d_in, d_out, n, d_workspace, vec, s); break;
+        case 5: launch_scan_v<256, 32, 1, 1>(d_in, d_out, n, d_workspace, vec, s); break;
+        case 6: launch_scan_v<256, 8, 1, 8>(d_in, d_out, n, d_workspace, vec, s); break;
+        default:
+            if (vec)
+                k_scan_exclusive_i32<true, false><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n,
+                                                                               hdr, status, tiles);
+            else
+                k_scan_exclusive_i32<false, false><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n,
+                                                                                hdr, status, tiles);
+    }
     HHS_LAUNCH_CHECK();
     return HHS_OK;
 }

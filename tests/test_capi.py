@@ -42,7 +42,7 @@ def test_invalid_arguments_return_status_without_device(hhs):
     assert L.hhs_hold_step(None, 0, None, 16, 0.0, 1.0, 1.0, 1, 1, None) == 1
     assert L.hhs_workspace_size(0, 4) == 0
     assert L.hhs_workspace_size(1024, 64) > 2 * 64 * 1024 * 4
-    assert L.hhs_scan_workspace_size(1 << 20) >= 256 + 8 * ((1 << 20) // 4096)
+    assert L.hhs_scan_workspace_size(1 << 20) >= 256 + 8 * ((1 << 20) // 2048)
 
 
 def test_plummer_ic_deterministic_henon_units(hhs):
