@@ -42,13 +42,13 @@ def parse():
     p.add_argument("--seed", type=int, default=2024)
     p.add_argument("--prec", default="mixed", choices=["mixed", "fp64"])
     p.add_argument("--schedule", default="auto", choices=["auto", "host"])
-    p.add_argument("--small-n", type=int, default=256,
+    p.add_argument("--small-n", type=int, default=64,
                    help="device schedule: nodes with n <= this are solved by one CTA")
     p.add_argument("--ctas-per-sm", type=int, default=2)
     p.add_argument("--cluster-size", type=int, default=1)
     p.add_argument("--mid-n", type=int, default=0)
     p.add_argument("--packed", type=int, default=0)
-    p.add_argument("--units-per-cta", type=int, default=8)
+    p.add_argument("--units-per-cta", type=int, default=16)
     p.add_argument("--autotune", action="store_true",
                    help="pick the device-schedule tuning with the library's autotuner")
     p.add_argument("--profile-out", default=None,
@@ -85,6 +85,29 @@ def max_over_ranks(value, dist, torch, device="cuda"):
     t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def cluster_sizes(seed, count=512, lo=64, hi=4096):
+    """Cluster sizes of the batched workload: log-uniform in [lo, hi] from the seed."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return np.round(np.exp(rng.uniform(np.log(lo), np.log(hi), count))).astype(np.int64)
+
+
+def gather_by_index(local_idx, local_vals, n_total, dist):
+    """Reassembles per-cluster values computed on the ranks (each rank holds the values of
+    the clusters local_idx) into one array in cluster order; the batched workload's only
+    collective, taken once after the timed region."""
+    import numpy as np
+    out = np.full(n_total, np.nan)
+    if dist is None:
+        out[np.asarray(local_idx)] = local_vals
+        return out
+    parts = [None] * dist.get_world_size()
+    dist.all_gather_object(parts, (list(map(int, local_idx)), list(map(float, local_vals))))
+    for idx, vals in parts:
+        out[np.asarray(idx, dtype=np.int64)] = vals
+    return out
 
 
 def aggregate_value(steps, world, t_max_ms):
@@ -351,18 +374,20 @@ def roofline(res, a, peaks_tflops):
 
 
 # ------------------------------------------------------------------------ other workloads
-def run_batched(a, torch):
-    """512 independent Plummer clusters, N log-uniform in [64, 4096], one launch per step."""
+def run_batched(a, torch, rank=0, world=1, dist=None):
+    """512 independent Plummer clusters, N log-uniform in [64, 4096], one launch per step.
+    With several ranks the clusters are sharded by hhs_batch_partition (balanced sum of
+    N^2, no data exchange); value = all clusters' steps over the max-over-ranks time."""
     import numpy as np
     import hhs
-    rng = np.random.default_rng(a.seed)
-    sizes = np.round(np.exp(rng.uniform(np.log(64), np.log(4096), 512))).astype(np.int64)
-    parts = [hhs.plummer(int(nk), a.seed * 1000 + k) for k, nk in enumerate(sizes)]
+    sizes = cluster_sizes(a.seed)
+    mine = hhs.batch_shard(sizes, world, rank) if world > 1 else np.arange(len(sizes))
+    parts = [hhs.plummer(int(sizes[k]), a.seed * 1000 + int(k)) for k in mine]
     e0 = np.array([hhs.energy_host(p) for p in parts])
     packed = {f: np.concatenate([p[f] for p in parts]) for f in hhs.FIELDS}
-    packed["id"] = np.arange(int(sizes.sum()), dtype=np.int32)
-    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
-    n = int(off[-1])
+    n = int(sum(len(p["x"]) for p in parts))
+    packed["id"] = np.arange(n, dtype=np.int32)
+    off = np.concatenate([[0], np.cumsum([len(p["x"]) for p in parts])]).astype(np.int32)
     stream = torch.cuda.Stream()
     sh = ctypes.c_void_p(stream.cuda_stream)
     prec = hhs.PREC_MIXED if a.prec == "mixed" else hhs.PREC_FP64
@@ -377,6 +402,8 @@ def run_batched(a, torch):
         b.reset_stats(sh)
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                for _ in range(a.steps)]
+        if dist is not None:
+            dist.barrier()
         torch.cuda.synchronize()
         for k in range(a.steps):
             flush.zero_()
@@ -384,28 +411,39 @@ def run_batched(a, torch):
             b.step(d, a.dt, True, prec, stream=sh)
             evs[k][1].record(stream)
         torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
         b.check(sh)
-    t_ms = sum(x.elapsed_time(y) for x, y in evs)
+    t_ms = max_over_ranks(sum(x.elapsed_time(y) for x, y in evs), dist, torch)
     st = b.stats(sh)
+    pairs = st["kick_pairs"] + st["ts_pairs"]
+    if dist is not None:
+        tp = torch.tensor([pairs], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tp)
+        pairs = float(tp.item())
     out = d.download()
     de = []
-    for k in range(len(sizes)):
+    for k in range(len(parts)):
         sl = slice(off[k], off[k + 1])
         e1 = hhs.energy_host({f: np.ascontiguousarray(out[f][sl]) for f in ("x", "y", "z", "vx",
                                                                             "vy", "vz", "m")})
         de.append(abs((e1 - e0[k]) / e0[k]))
-    de = np.array(de)
+    de = gather_by_index(mine, de, len(sizes), dist)
     steps_all = a.steps + a.warmup
+    n_total = int(sizes.sum())
     return {"metric": "aggregate HOLD steps/s over 512 independent clusters",
             "value": len(sizes) * a.steps / (t_ms * 1e-3), "unit": "cluster HOLD steps/s",
             "launches_per_s": a.steps / (t_ms * 1e-3), "ms_per_step": t_ms / a.steps,
-            "steps": a.steps, "warmup": a.warmup, "n_gpus": 1, "higher_is_better": True,
+            "steps": a.steps, "warmup": a.warmup, "n_gpus": world, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None,
             "dtype": "f32-pair/f64-state" if a.prec == "mixed" else "f64",
             "data": "synthetic (seeded Plummer clusters)",
-            "config": {"workload": f"512 Plummer clusters, N log-uniform [64,4096] (total {n}), "
-                                   f"eta={a.eta}, dt_top={a.dt}, one launch per top step",
-                       "n_total": n, "l2": "flushed between timed steps"},
-            "pair_interactions_per_s": (st["kick_pairs"] + st["ts_pairs"]) / (t_ms * 1e-3),
+            "config": {"workload": f"512 Plummer clusters, N log-uniform [64,4096] "
+                                   f"(total {n_total}), eta={a.eta}, dt_top={a.dt}, one launch "
+                                   f"per top step per rank",
+                       "n_total": n_total, "l2": "flushed between timed steps",
+                       "parallelism": f"clusters sharded x{world} (balanced sum N^2)"},
+            "pair_interactions_per_s": pairs / (t_ms * 1e-3),
             "dE_over_E_after_steps": {"steps": steps_all, "median": float(np.median(de)),
                                       "p90": float(np.percentile(de, 90)),
                                       "max": float(de.max())}}
@@ -565,9 +603,16 @@ def main():
         a.n, a.eta, a.mass = 262144, 0.02, 2
     elif a.workload == "deep":
         a.n, a.eta, a.mass = 65536, 0.02, 1
-    if a.workload in ("batched", "scan", "validate"):
+    if a.workload == "batched":
+        out = run_batched(a, torch, rank, world, dist)
         if rank == 0:
-            fn = {"batched": run_batched, "scan": run_scan, "validate": run_validate}[a.workload]
+            print(json.dumps(out), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    if a.workload in ("scan", "validate"):
+        if rank == 0:
+            fn = {"scan": run_scan, "validate": run_validate}[a.workload]
             out = fn(a, torch)
             peaks = None
             try:
@@ -578,6 +623,9 @@ def main():
                 out["roofline"]["peak"] = peaks["hbm_gbs"]
                 out["roofline"]["frac"] = out["value"] / peaks["hbm_gbs"]
             print(json.dumps(out), flush=True)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
         return
     res = run_ours(a, rank, world, torch, dist)
     cpu = None

@@ -281,6 +281,43 @@ hhs_status hhs_batch_get_stats(hhs_batch* b, hhs_stats* out, void* stream);
 hhs_status hhs_batch_reset_stats(hhs_batch* b, void* stream);
 hhs_status hhs_batch_check(hhs_batch* b, void* stream);
 
+/* Multi-GPU sharding of a batch (host only, no device work): assigns each of the n_sys
+ * independent systems (sizes[k] particles) to one of n_ranks ranks so that the per-rank
+ * sums of sizes[k]^2 (the O(N^2) pair work) are balanced: longest-processing-time greedy,
+ * systems taken by decreasing size (ties by index), each to the least-loaded rank (ties by
+ * rank). Deterministic, so every rank computes the same rank_of[n_sys] without an
+ * exchange. load (optional, n_ranks entries) receives each rank's sum of sizes^2. */
+hhs_status hhs_batch_partition(int32_t n_sys, const int32_t* sizes, int32_t n_ranks,
+                               int32_t* rank_of, double* load);
+
+/* ---- driver: hold(), energy diagnostic, snapshots ------------------------------ */
+/* FP64 total energy of the first n particles (kinetic and potential, compensated sums,
+ * pair potential with softening length eps). Uses the system's acceleration arrays as
+ * scratch; synchronises the stream. */
+hhs_status hhs_energy(hhs_particle_system* sys, int32_t n, double eps, double* kinetic,
+                      double* potential, void* stream);
+/* Binary snapshot (checkpoint): an 80-byte header ("HHSSNAP1", n, time, eta, eps, dt,
+ * step) followed by the FP64 SoA arrays x y z vx vy vz m ts and the int32 ids. */
+hhs_status hhs_snapshot_write(const hhs_particle_system* sys, int32_t n, double time,
+                              const hhs_params* params, double dt, int32_t step,
+                              const char* path, void* stream);
+hhs_status hhs_snapshot_read(hhs_particle_system* sys, const char* path, int32_t* n_out,
+                             double* time, int32_t* step, void* stream);
+/* Energy log filled by hhs_hold: one (time, energy) entry per diagnostic. */
+typedef struct {
+    double* time;
+    double* energy;
+    int32_t capacity;
+    int32_t n_entries;
+} hhs_run_log;
+/* hold(...) of the reference (declared at src/hold.cuh:20-23, sketched at :26-35, never
+ * defined): integrate from stime to etime in top-level steps of dt. Every
+ * snapshot_every steps and at the end the energy is logged and, with a non-empty
+ * prefix, "<prefix>_<step>.hhs" is written. Segments run as graph-captured steps. */
+hhs_status hhs_hold(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n, double stime,
+                    double etime, double dt, hhs_precision prec, int32_t snapshot_every,
+                    const char* snapshot_prefix, hhs_run_log* log, void* stream);
+
 /* Host-side utilities (no GPU): seeded Plummer initial conditions in Henon units,
  * and FP64 energies with compensated sums. */
 hhs_status hhs_ic_plummer(int32_t n, uint64_t seed, int32_t mass_spectrum, double* x,

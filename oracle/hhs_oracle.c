@@ -105,23 +105,25 @@ int oracle_split(int n, const double* ts, double pivot, int32_t* order) {
 }
 
 /* Direct-sum kick, restating src/kick.cuh:19-30 and :82-105 per sink:
- *   dx = x_j - x_i; d2 = dx.dx; skip d2 == 0; d = sqrt(d2); inv = 1.0/(d2*d);
+ *   dx = x_j - x_i; d2 = dx.dx + eps2; skip d2 == 0; d = sqrt(d2); inv = 1.0/(d2*d);
  *   a += dx * (m_j * inv)           (attractive; the reference GPU kernel has the
  *                                    opposite sign, see tests/test_nbforce.cu:14-18)
  *   v += a * dtfac                  (dtfac = fac*dt of the reference call)
- * Sources are summed in index order. */
-void oracle_kick(int n_sink, const double* sx, const double* sy, const double* sz,
-                 double* svx, double* svy, double* svz,
-                 double* ax, double* ay, double* az,
-                 int n_src, const double* px, const double* py, const double* pz,
-                 const double* pm, double dtfac) {
+ * Sources are summed in index order. eps2 is the squared softening length the
+ * reference keeps in nbodysystem_globals (src/particle_system.cuh:16) but never
+ * applies; eps2 = 0 gives the reference expression exactly (d2 + 0 == d2). */
+void oracle_kick_soft(int n_sink, const double* sx, const double* sy, const double* sz,
+                      double* svx, double* svy, double* svz,
+                      double* ax, double* ay, double* az,
+                      int n_src, const double* px, const double* py, const double* pz,
+                      const double* pm, double dtfac, double eps2) {
 #pragma omp parallel for schedule(dynamic, 16)
     for (int i = 0; i < n_sink; i++) {
         const double xi = sx[i], yi = sy[i], zi = sz[i];
         double accx = 0.0, accy = 0.0, accz = 0.0;
         for (int j = 0; j < n_src; j++) {
             const double dxx = px[j] - xi, dxy = py[j] - yi, dxz = pz[j] - zi;
-            const double d2 = dxx * dxx + dxy * dxy + dxz * dxz;
+            const double d2 = dxx * dxx + dxy * dxy + dxz * dxz + eps2;
             if (d2 == 0.0) continue;
             const double d = sqrt(d2);
             const double inv = 1.0 / (d2 * d);
@@ -135,6 +137,15 @@ void oracle_kick(int n_sink, const double* sx, const double* sy, const double* s
         svy[i] = svy[i] + accy * dtfac;
         svz[i] = svz[i] + accz * dtfac;
     }
+}
+
+void oracle_kick(int n_sink, const double* sx, const double* sy, const double* sz,
+                 double* svx, double* svy, double* svz,
+                 double* ax, double* ay, double* az,
+                 int n_src, const double* px, const double* py, const double* pz,
+                 const double* pm, double dtfac) {
+    oracle_kick_soft(n_sink, sx, sy, sz, svx, svy, svz, ax, ay, az, n_src, px, py, pz, pm,
+                     dtfac, 0.0);
 }
 
 /* pos += vel * (dt*fac)   (src/drift.cuh:24-26) */
@@ -210,7 +221,7 @@ static void trace_node(oracle_trace* tr, int level, int n, int nf, int calc) {
 }
 
 static void hold_rec(int level, osys* total, double dt, int calc_ts, double eta,
-                     oracle_trace* tr) {
+                     double eps2, oracle_trace* tr) {
     const int n = total->n;
     if (calc_ts)
         oracle_timesteps(n, total->x, total->y, total->z, total->vx, total->vy,
@@ -229,25 +240,25 @@ static void hold_rec(int level, osys* total, double dt, int calc_ts, double eta,
 
     if (nf == 0 && tr) tr->leaf_time += dt; /* src/hold.cuh:106-114 */
 
-    if (nf > 0) hold_rec(level + 1, &fast, dt / 2, 0, eta, tr);
+    if (nf > 0) hold_rec(level + 1, &fast, dt / 2, 0, eta, eps2, tr);
     if (ns > 0)
         oracle_drift(ns, slow.x, slow.y, slow.z, slow.vx, slow.vy, slow.vz, dt * 0.5);
     if (ns > 0) {
         /* kick_slow(slow, dt, 1.0): v += a * (1.0*dt)  (src/hold.cuh:138) */
-        oracle_kick(ns, slow.x, slow.y, slow.z, slow.vx, slow.vy, slow.vz, NULL, NULL, NULL,
-                    ns, slow.x, slow.y, slow.z, slow.m, 1.0 * dt);
+        oracle_kick_soft(ns, slow.x, slow.y, slow.z, slow.vx, slow.vy, slow.vz, NULL, NULL,
+                         NULL, ns, slow.x, slow.y, slow.z, slow.m, 1.0 * dt, eps2);
         if (nf > 0) {
             /* kick_sf(src=fast, sink=slow, 1.0, dt): v += a * (dt*1.0)  (:142) */
-            oracle_kick(ns, slow.x, slow.y, slow.z, slow.vx, slow.vy, slow.vz, NULL, NULL,
-                        NULL, nf, fast.x, fast.y, fast.z, fast.m, dt * 1.0);
+            oracle_kick_soft(ns, slow.x, slow.y, slow.z, slow.vx, slow.vy, slow.vz, NULL, NULL,
+                             NULL, nf, fast.x, fast.y, fast.z, fast.m, dt * 1.0, eps2);
             /* kick_sf(src=slow, sink=fast, 1.0, dt)  (:143) */
-            oracle_kick(nf, fast.x, fast.y, fast.z, fast.vx, fast.vy, fast.vz, NULL, NULL,
-                        NULL, ns, slow.x, slow.y, slow.z, slow.m, dt * 1.0);
+            oracle_kick_soft(nf, fast.x, fast.y, fast.z, fast.vx, fast.vy, fast.vz, NULL, NULL,
+                             NULL, ns, slow.x, slow.y, slow.z, slow.m, dt * 1.0, eps2);
         }
     }
     if (ns > 0)
         oracle_drift(ns, slow.x, slow.y, slow.z, slow.vx, slow.vy, slow.vz, dt * 0.5);
-    if (nf > 0) hold_rec(level + 1, &fast, dt / 2, 1, eta, tr);
+    if (nf > 0) hold_rec(level + 1, &fast, dt / 2, 1, eta, eps2, tr);
 
     osys_update(total, &fast);
     osys_update(total, &slow);
@@ -255,15 +266,22 @@ static void hold_rec(int level, osys* total, double dt, int calc_ts, double eta,
     osys_free(&slow);
 }
 
-void oracle_hold_step(int n, double* x, double* y, double* z,
-                      double* vx, double* vy, double* vz, double* m, double* ts,
-                      int32_t* id, double dt, int calc_ts, double eta,
-                      oracle_trace* trace) {
+void oracle_hold_step_soft(int n, double* x, double* y, double* z,
+                           double* vx, double* vy, double* vz, double* m, double* ts,
+                           int32_t* id, double dt, int calc_ts, double eta, double eps2,
+                           oracle_trace* trace) {
     if (n <= 0) return;
     osys top;
     top.n = n; top.x = x; top.y = y; top.z = z; top.vx = vx; top.vy = vy; top.vz = vz;
     top.m = m; top.ts = ts; top.id = id; top.parent = NULL;
-    hold_rec(0, &top, dt, calc_ts, eta, trace);
+    hold_rec(0, &top, dt, calc_ts, eta, eps2, trace);
+}
+
+void oracle_hold_step(int n, double* x, double* y, double* z,
+                      double* vx, double* vy, double* vz, double* m, double* ts,
+                      int32_t* id, double dt, int calc_ts, double eta,
+                      oracle_trace* trace) {
+    oracle_hold_step_soft(n, x, y, z, vx, vy, vz, m, ts, id, dt, calc_ts, eta, 0.0, trace);
 }
 
 /* Neumaier compensated accumulation */

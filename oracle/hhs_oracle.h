@@ -69,6 +69,13 @@ void oracle_kick(int n_sink, const double* sx, const double* sy, const double* s
                  int n_src, const double* px, const double* py, const double* pz,
                  const double* pm, double dtfac);
 
+/* oracle_kick with a softening length: d2 = dx.dx + eps2 (eps2 = eps^2). */
+void oracle_kick_soft(int n_sink, const double* sx, const double* sy, const double* sz,
+                      double* svx, double* svy, double* svz,
+                      double* ax, double* ay, double* az,
+                      int n_src, const double* px, const double* py, const double* pz,
+                      const double* pm, double dtfac, double eps2);
+
 void oracle_drift(int n, double* x, double* y, double* z,
                   const double* vx, const double* vy, const double* vz, double dtfac);
 
@@ -77,6 +84,12 @@ void oracle_hold_step(int n, double* x, double* y, double* z,
                       double* vx, double* vy, double* vz, double* m, double* ts,
                       int32_t* id, double dt, int calc_ts, double eta,
                       oracle_trace* trace);
+
+/* oracle_hold_step with every kick softened by eps2 = eps^2. */
+void oracle_hold_step_soft(int n, double* x, double* y, double* z,
+                           double* vx, double* vy, double* vz, double* m, double* ts,
+                           int32_t* id, double dt, int calc_ts, double eta, double eps2,
+                           oracle_trace* trace);
 
 /* Total energy with Neumaier-compensated sums: out[0]=kinetic, out[1]=potential. */
 void oracle_energy(int n, const double* x, const double* y, const double* z,

@@ -55,6 +55,11 @@ def lib():
         L.oracle_split.restype = ctypes.c_int
         L.oracle_kick.argtypes = [ctypes.c_int] + [_dp] * 9 + [ctypes.c_int] + [_dp] * 4 + \
             [ctypes.c_double]
+        L.oracle_kick_soft.argtypes = [ctypes.c_int] + [_dp] * 9 + [ctypes.c_int] + \
+            [_dp] * 4 + [ctypes.c_double, ctypes.c_double]
+        L.oracle_hold_step_soft.argtypes = [ctypes.c_int] + [_dp] * 8 + [
+            _ip, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+            ctypes.POINTER(Trace)]
         L.oracle_drift.argtypes = [ctypes.c_int] + [_dp] * 6 + [ctypes.c_double]
         L.oracle_hold_step.argtypes = [ctypes.c_int] + [_dp] * 8 + [_ip, ctypes.c_double,
                                                                      ctypes.c_int, ctypes.c_double,
@@ -97,15 +102,15 @@ def split(ts, pivot):
     return order, nf
 
 
-def kick(sink, src, dtfac):
+def kick(sink, src, dtfac, eps=0.0):
     """Updates sink['vx'..'vz'] in place; returns acc (3, n_sink)."""
     n = len(sink["x"])
     acc = np.zeros((3, n))
     ax, ay, az = acc[0], acc[1], acc[2]
-    lib().oracle_kick(n, _d(sink["x"]), _d(sink["y"]), _d(sink["z"]), _d(sink["vx"]),
-                      _d(sink["vy"]), _d(sink["vz"]), _d(ax), _d(ay), _d(az),
-                      len(src["x"]), _d(src["x"]), _d(src["y"]), _d(src["z"]), _d(src["m"]),
-                      dtfac)
+    lib().oracle_kick_soft(n, _d(sink["x"]), _d(sink["y"]), _d(sink["z"]), _d(sink["vx"]),
+                           _d(sink["vy"]), _d(sink["vz"]), _d(ax), _d(ay), _d(az),
+                           len(src["x"]), _d(src["x"]), _d(src["y"]), _d(src["z"]),
+                           _d(src["m"]), dtfac, eps * eps)
     return acc
 
 
@@ -114,13 +119,14 @@ def drift(s, dtfac):
                        _d(s["vy"]), _d(s["vz"]), dtfac)
 
 
-def hold_step(s, dt, calc_ts, eta, capacity=0):
+def hold_step(s, dt, calc_ts, eta, capacity=0, eps=0.0):
     """One recursive HOLD step in place on dict-of-arrays s. Returns (trace, nodes)."""
     nodes = (Node * capacity)() if capacity > 0 else None
     tr = Trace(nodes if nodes is not None else None, capacity, 0, 0, 0.0, 0.0, 0.0)
-    lib().oracle_hold_step(len(s["x"]), _d(s["x"]), _d(s["y"]), _d(s["z"]), _d(s["vx"]),
-                           _d(s["vy"]), _d(s["vz"]), _d(s["m"]), _d(s["ts"]), _i(s["id"]),
-                           dt, int(calc_ts), eta, ctypes.byref(tr))
+    lib().oracle_hold_step_soft(len(s["x"]), _d(s["x"]), _d(s["y"]), _d(s["z"]),
+                                _d(s["vx"]), _d(s["vy"]), _d(s["vz"]), _d(s["m"]),
+                                _d(s["ts"]), _i(s["id"]), dt, int(calc_ts), eta, eps * eps,
+                                ctypes.byref(tr))
     out = None
     if nodes is not None:
         k = min(tr.count, capacity)

@@ -511,7 +511,7 @@ hhs_status hold_host(hhs_ctx* c, const SoA& P, const int32_t* S, int n, int leve
         if (st != HHS_OK) return st;
         const double pairs = (double)ns * (ns - 1.0) + 2.0 * (double)ns * (double)nf;
         if (timed) prof->begin(rec, 1, pairs, s);
-        st = launch_kick_level(P, F, L, cnt, n, dt, prec, s);
+        st = launch_kick_level(P, F, L, cnt, n, dt, c->params.eps * c->params.eps, prec, s);
         if (st != HHS_OK) return st;
         if (timed) prof->end(rec, s);
         st = launch_drift_slow(P, L, cnt, ns, dt * 0.5, s);

@@ -66,8 +66,8 @@ struct EParams {
     SoA P;
     int n_top, n_max, max_levels, small_n, calc_top, profile, units_per_cta, warp_n, mid_n;
     int packed;  // mixed kick: two sinks per thread in packed FP32x2 arithmetic
-    double dt_top, eta, eta_s2;
-    float inv_eta_s2, inv_eta;
+    double dt_top, eta, eta_s2, eps2;
+    float inv_eta_s2, inv_eta, eps2f;
     int32_t* fast_lists;
     int32_t* slow_lists;
     hhs_partition* counts;
@@ -495,7 +495,8 @@ __device__ void kick_unit(const EParams& E, const int32_t* F, const int32_t* L, 
                 for (int jl = 0; jl < je; jl++) {
                     double* a = (t0 + jl < ns) ? aL : aF;
                     kick_pair_fp64(f64_sub(sm.u.kd.x[jl], xi), f64_sub(sm.u.kd.y[jl], yi),
-                                   f64_sub(sm.u.kd.z[jl], zi), sm.u.kd.m[jl], a[0], a[1], a[2]);
+                                   f64_sub(sm.u.kd.z[jl], zi), sm.u.kd.m[jl], a[0], a[1], a[2],
+                                   E.eps2);
                 }
             }
         }
@@ -540,7 +541,7 @@ __device__ void kick_unit(const EParams& E, const int32_t* F, const int32_t* L, 
                         const float dx = ds_diff(A.x, B.x, xi.hi, xi.lo);
                         const float dy = ds_diff(A.y, B.y, yi.hi, yi.lo);
                         const float dz = ds_diff(A.z, B.z, zi.hi, zi.lo);
-                        const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, E.eps2f)));
                         const float ri = rsqrt_nr(d2);
                         const float ri2 = ri * ri;
                         const float mr3 = (d2 > 0.0f) ? A.w * ri2 * ri : 0.0f;
@@ -577,8 +578,8 @@ __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b
 // thread with a slow one sees slow sources only)
 __device__ __forceinline__ void kick_x2_pairs(const Smem& sm, int jbeg, int jend, float2 nxh,
                                               float2 nyh, float2 nzh, float2 nxl, float2 nyl,
-                                              float2 nzl, int lim0, float2& ax, float2& ay,
-                                              float2& az) {
+                                              float2 nzl, int lim0, float2 eps2, float2& ax,
+                                              float2& ay, float2& az) {
     const float2 half = f2(-0.5f, -0.5f), three_half = f2(1.5f, 1.5f);
 #pragma unroll 4
     for (int jl = jbeg; jl < jend; jl++) {
@@ -588,7 +589,7 @@ __device__ __forceinline__ void kick_x2_pairs(const Smem& sm, int jbeg, int jend
         const float2 dx = __fadd2_rn(__fadd2_rn(f2(P0.x, P0.y), nxh), __fadd2_rn(f2(P1.z, P1.w), nxl));
         const float2 dy = __fadd2_rn(__fadd2_rn(f2(P0.z, P0.w), nyh), __fadd2_rn(f2(P2.x, P2.y), nyl));
         const float2 dz = __fadd2_rn(__fadd2_rn(f2(P1.x, P1.y), nzh), __fadd2_rn(f2(P2.z, P2.w), nzl));
-        float2 d2 = __fmul2_rn(dz, dz);
+        float2 d2 = __ffma2_rn(dz, dz, eps2);
         d2 = __ffma2_rn(dy, dy, d2);
         d2 = __ffma2_rn(dx, dx, d2);
         d2.x = fmaxf(d2.x, 1e-20f);
@@ -654,8 +655,8 @@ __device__ void kick_unit_x2(const EParams& E, const int32_t* F, const int32_t* 
         const int emax = max(e0, e1);
         for (int jb = 0; jb < emax; jb += 32) {
             float2 bx = f2(0.f, 0.f), by = f2(0.f, 0.f), bz = f2(0.f, 0.f);
-            kick_x2_pairs(sm, jb, min(jb + 32, emax), nxh, nyh, nzh, nxl, nyl, nzl, e0, bx, by,
-                          bz);
+            kick_x2_pairs(sm, jb, min(jb + 32, emax), nxh, nyh, nzh, nxl, nyl, nzl, e0,
+                          make_float2(E.eps2f, E.eps2f), bx, by, bz);
             kahan_add(acc[0][0], cmp[0][0], bx.x);
             kahan_add(acc[0][1], cmp[0][1], by.x);
             kahan_add(acc[0][2], cmp[0][2], bz.x);
@@ -965,17 +966,20 @@ __device__ void tiny_hold(const EParams& E, const int32_t* S, int n, int level0,
                         for (unsigned mm = Lord; mm; mm &= mm - 1u) {
                             const int j = __ffs(mm) - 1;
                             kick_pair_fp64(f64_sub(T.x[j], xi), f64_sub(T.y[j], yi),
-                                           f64_sub(T.z[j], zi), T.m[j], aL[0], aL[1], aL[2]);
+                                           f64_sub(T.z[j], zi), T.m[j], aL[0], aL[1], aL[2],
+                                           E.eps2);
                         }
                         if (lone >= 0)
                             kick_pair_fp64(f64_sub(T.x[lone], xi), f64_sub(T.y[lone], yi),
-                                           f64_sub(T.z[lone], zi), T.m[lone], aL[0], aL[1], aL[2]);
+                                           f64_sub(T.z[lone], zi), T.m[lone], aL[0], aL[1], aL[2],
+                                           E.eps2);
                         if (is_slow) {
 #pragma unroll 1
                             for (unsigned mm = F; mm; mm &= mm - 1u) {
                                 const int j = __ffs(mm) - 1;
                                 kick_pair_fp64(f64_sub(T.x[j], xi), f64_sub(T.y[j], yi),
-                                               f64_sub(T.z[j], zi), T.m[j], aF[0], aF[1], aF[2]);
+                                               f64_sub(T.z[j], zi), T.m[j], aF[0], aF[1], aF[2],
+                                               E.eps2);
                             }
                         }
                         double vx = f64_add(T.vx[lane], f64_mul(aL[0], dt));
@@ -1006,7 +1010,7 @@ __device__ void tiny_hold(const EParams& E, const int32_t* S, int n, int level0,
                             const float dx = ds_diff(A.x, B.x, Ai.x, Bi.x);
                             const float dy = ds_diff(A.y, B.y, Ai.y, Bi.y);
                             const float dz = ds_diff(A.z, B.z, Ai.z, Bi.z);
-                            const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                            const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, E.eps2f)));
                             const float ri = rsqrt_nr(d2);
                             const float mr3 = (d2 > 0.0f) ? A.w * ri * ri * ri : 0.0f;
                             a[0] = fmaf(dx, mr3, a[0]);
@@ -1298,8 +1302,8 @@ struct EngineHost {
     int grid[2] = {0, 0};
     int sms = 0, occ[2] = {0, 0};
     int ctas_per_sm = 2;
-    int small_n = 256;
-    int units_per_cta = 8;
+    int small_n = 64;
+    int units_per_cta = 16;
     int warp_n = 32;
     int cluster_size = 1;
     int mid_n = 0;
@@ -1468,6 +1472,8 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
     E.profile = profile ? 1 : 0;
     E.dt_top = dt;
     E.eta = c->params.eta;
+    E.eps2 = c->params.eps * c->params.eps;
+    E.eps2f = (float)E.eps2;
     E.eta_s2 = c->params.eta / 1.41421356237309504880;
     E.inv_eta_s2 = (float)(1.0 / E.eta_s2);
     E.inv_eta = (float)(1.0 / E.eta);
@@ -1674,6 +1680,8 @@ extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, d
     E.packed = b->packed;
     E.dt_top = dt;
     E.eta = b->params.eta;
+    E.eps2 = b->params.eps * b->params.eps;
+    E.eps2f = (float)E.eps2;
     E.eta_s2 = b->params.eta / 1.41421356237309504880;
     E.inv_eta_s2 = (float)(1.0 / E.eta_s2);
     E.inv_eta = (float)(1.0 / E.eta);

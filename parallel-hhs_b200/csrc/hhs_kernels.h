@@ -24,7 +24,8 @@ hhs_status launch_timesteps(const SoA& P, const int32_t* list, int n, double eta
 // slow sources; v += a*dt. Counts are read from the device (n_max bounds the grid).
 hhs_status launch_kick_level(const SoA& P, const int32_t* fast_list,
                              const int32_t* slow_list, const hhs_partition* counts,
-                             int n_max, double dt, hhs_precision prec, cudaStream_t stream);
+                             int n_max, double dt, double eps2, hhs_precision prec,
+                             cudaStream_t stream);
 // Standalone kick: sinks = sink[0..n_sink), sources = src[0..n_src); acc written.
 hhs_status launch_kick_pair(const SoA& sink, double* ax, double* ay, double* az,
                             const SoA& src, int n_sink, int n_src, double dtfac,

@@ -45,9 +45,14 @@ __device__ __forceinline__ void ts_pair_fp64(double drx, double dry, double drz,
 
 // Pair acceleration (src/kick.cuh:19-30 with the attractive sign of
 // tests/test_nbforce.cu:14-18): dx = x_j - x_i, skip d2 == 0, a += dx * (m_j/(d2*d)).
+// eps2 is the squared softening length the reference stores but never applies
+// (src/particle_system.cuh:16, TODOs at src/hold.cuh:136,141,157); with eps2 = 0 the
+// result is unchanged bit for bit (d2 + 0 == d2).
 __device__ __forceinline__ void kick_pair_fp64(double dx, double dy, double dz, double mj,
-                                               double& ax, double& ay, double& az) {
-    const double d2 = f64_add(f64_add(f64_mul(dx, dx), f64_mul(dy, dy)), f64_mul(dz, dz));
+                                               double& ax, double& ay, double& az,
+                                               double eps2 = 0.0) {
+    const double d2 = f64_add(
+        f64_add(f64_add(f64_mul(dx, dx), f64_mul(dy, dy)), f64_mul(dz, dz)), eps2);
     if (d2 == 0.0) return;
     const double d = f64_sqrt(d2);
     const double s = f64_mul(mj, f64_div(1.0, f64_mul(d2, d)));

@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(kTsBlock)
 // src/hold.cuh:138,142); fast sinks apply v += aFL*dt (kick_sf(slow->fast), :143).
 __global__ void __launch_bounds__(kKickBlock)
     k_kick_level_fp64(SoA P, const int32_t* __restrict__ F, const int32_t* __restrict__ L,
-                      const hhs_partition* __restrict__ counts, double dt) {
+                      const hhs_partition* __restrict__ counts, double dt, double eps2) {
     __shared__ double sx[kKickBlock], sy[kKickBlock], sz[kKickBlock], sm[kKickBlock];
     const int nf = counts->n_fast, ns = counts->n_slow, n = nf + ns;
     if (ns == 0) return;
@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(kKickBlock)
             const int jn = min(kKickBlock, ns - jt);
             for (int jl = 0; jl < jn; jl++)
                 kick_pair_fp64(f64_sub(sx[jl], xi), f64_sub(sy[jl], yi), f64_sub(sz[jl], zi), sm[jl],
-                               aLx, aLy, aLz);
+                               aLx, aLy, aLz, eps2);
         }
         __syncthreads();
     }
@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(kKickBlock)
             const int jn = min(kKickBlock, nf - jt);
             for (int jl = 0; jl < jn; jl++)
                 kick_pair_fp64(f64_sub(sx[jl], xi), f64_sub(sy[jl], yi), f64_sub(sz[jl], zi), sm[jl],
-                               aFx, aFy, aFz);
+                               aFx, aFy, aFz, eps2);
         }
         __syncthreads();
     }
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kKickBlock)
 // and fast source sums are kept apart so the update order matches the FP64 form.
 __global__ void __launch_bounds__(kKickBlock)
     k_kick_level_mixed(SoA P, const int32_t* __restrict__ F, const int32_t* __restrict__ L,
-                       const hhs_partition* __restrict__ counts, double dt) {
+                       const hhs_partition* __restrict__ counts, double dt, float eps2) {
     __shared__ float4 sA[kKickBlock];  // xh, yh, zh, m
     __shared__ float4 sB[kKickBlock];  // xl, yl, zl, -
     const int nf = counts->n_fast, ns = counts->n_slow, n = nf + ns;
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(kKickBlock)
                     const float dx = ds_diff(A.x, B.x, xi.hi, xi.lo);
                     const float dy = ds_diff(A.y, B.y, yi.hi, yi.lo);
                     const float dz = ds_diff(A.z, B.z, zi.hi, zi.lo);
-                    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
                     if (d2 == 0.0f) continue;
                     const float ri = rsqrt_nr(d2);
                     const float mr3 = A.w * ri * ri * ri;
@@ -387,14 +387,15 @@ hhs_status launch_timesteps(const SoA& P, const int32_t* list, int n, double eta
 
 hhs_status launch_kick_level(const SoA& P, const int32_t* fast_list,
                              const int32_t* slow_list, const hhs_partition* counts,
-                             int n_max, double dt, hhs_precision prec, cudaStream_t stream) {
+                             int n_max, double dt, double eps2, hhs_precision prec,
+                             cudaStream_t stream) {
     if (n_max <= 0) return HHS_OK;
     if (prec == HHS_PREC_FP64)
         k_kick_level_fp64<<<grid_for(n_max, kKickBlock), kKickBlock, 0, stream>>>(
-            P, fast_list, slow_list, counts, dt);
+            P, fast_list, slow_list, counts, dt, eps2);
     else
         k_kick_level_mixed<<<grid_for(n_max, kKickBlock), kKickBlock, 0, stream>>>(
-            P, fast_list, slow_list, counts, dt);
+            P, fast_list, slow_list, counts, dt, (float)eps2);
     HHS_LAUNCH_CHECK();
     return HHS_OK;
 }

@@ -18,7 +18,7 @@ constexpr int kScanMinTile = 2048;
 // SELF_RESET: the last CTA resets the workspace header for the next call (used where the
 // workspace is reused without a memset); the standalone calls memset it instead.
 template <bool VEC, bool SELF_RESET>
-__global__ void __launch_bounds__(kScanBlock)
+__global__ void __launch_bounds__(kScanBlock, 6)
     k_scan_exclusive_i32(const int32_t* __restrict__ in, int32_t* __restrict__ out,
                          long long n, ScanHeader* hdr, unsigned long long* status,
                          int num_tiles) {
@@ -131,7 +131,7 @@ int scan_variant() {
 // idx_out[scan]; the exclusive scan of (flag != 0) optionally goes to scan_out; the last
 // CTA writes the number of selected elements to *count.
 template <bool VEC, bool SELF_RESET>
-__global__ void __launch_bounds__(kScanBlock)
+__global__ void __launch_bounds__(kScanBlock, 6)
     k_compact_flags(const int32_t* __restrict__ flags, int32_t* __restrict__ scan_out,
                     int32_t* __restrict__ idx_out, int32_t* __restrict__ count, long long n,
                     ScanHeader* hdr, unsigned long long* status, int num_tiles) {

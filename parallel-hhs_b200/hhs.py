@@ -67,6 +67,11 @@ class Tuning(ctypes.Structure):
                 ("ms_per_step", ctypes.c_double)]
 
 
+class RunLog(ctypes.Structure):
+    _fields_ = [("time", _dp), ("energy", _dp), ("capacity", ctypes.c_int32),
+                ("n_entries", ctypes.c_int32)]
+
+
 class CParticleSystem(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int32)] + \
         [(k, _dp) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "ts", "m")] + \
@@ -146,6 +151,17 @@ SIGNATURES = {
     "hhs_batch_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(Stats), _vp]),
     "hhs_batch_reset_stats": (ctypes.c_int, [_vp, _vp]),
     "hhs_batch_check": (ctypes.c_int, [_vp, _vp]),
+    "hhs_batch_partition": (ctypes.c_int, [ctypes.c_int32, _ip, ctypes.c_int32, _ip, _dp]),
+    "hhs_energy": (ctypes.c_int, [ctypes.POINTER(CParticleSystem), ctypes.c_int32, ctypes.c_double,
+                                  _dp, _dp, _vp]),
+    "hhs_snapshot_write": (ctypes.c_int, [ctypes.POINTER(CParticleSystem), ctypes.c_int32,
+                                          ctypes.c_double, ctypes.POINTER(Params), ctypes.c_double,
+                                          ctypes.c_int32, ctypes.c_char_p, _vp]),
+    "hhs_snapshot_read": (ctypes.c_int, [ctypes.POINTER(CParticleSystem), ctypes.c_char_p, _ip,
+                                         _dp, _ip, _vp]),
+    "hhs_hold": (ctypes.c_int, [_vp, ctypes.POINTER(CParticleSystem), ctypes.c_int32,
+                                ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                ctypes.c_int32, ctypes.c_char_p, ctypes.POINTER(RunLog), _vp]),
     "hhs_ctx_set_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(Tuning)]),
     "hhs_ctx_get_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(Tuning)]),
     "hhs_ctx_autotune": (ctypes.c_int, [_vp, ctypes.POINTER(CParticleSystem), ctypes.c_int32,
@@ -341,6 +357,23 @@ class Context:
             pass
 
 
+def batch_partition(sizes, n_ranks):
+    """Rank of each independent system, balancing the per-rank sum of N^2
+    (hhs_batch_partition); returns (rank_of, load)."""
+    sz = np.ascontiguousarray(sizes, dtype=np.int32)
+    rank_of = np.zeros(len(sz), dtype=np.int32)
+    load = np.zeros(n_ranks)
+    _check(lib().hhs_batch_partition(len(sz), _i(sz), n_ranks, _i(rank_of), _d(load)),
+           "hhs_batch_partition")
+    return rank_of, load
+
+
+def batch_shard(sizes, n_ranks, rank):
+    """Indices (ascending) of the systems this rank integrates."""
+    rank_of, _ = batch_partition(sizes, n_ranks)
+    return np.nonzero(rank_of == rank)[0]
+
+
 class Batch:
     """Many independent systems in one particle system (hhs_batch)."""
 
@@ -425,6 +458,39 @@ def hold_integrate(ctx, sys, n, dt, steps, prec=PREC_MIXED, stream=None):
     """`steps` top-level steps as one replayed CUDA graph (hhs_hold_integrate)."""
     _check(lib().hhs_hold_integrate(ctx.h, sys.ref, n, dt, steps, prec, stream),
            "hhs_hold_integrate")
+
+
+def energy(sys, n, eps=0.0, stream=None):
+    """FP64 (kinetic, potential) of the first n particles, computed on the device."""
+    k, p = ctypes.c_double(), ctypes.c_double()
+    _check(lib().hhs_energy(sys.ref, n, eps, ctypes.byref(k), ctypes.byref(p), stream),
+           "hhs_energy")
+    return k.value, p.value
+
+
+def snapshot_write(sys, n, time, path, eta=0.03, eps=0.0, dt=0.0, step=0, stream=None):
+    prm = Params(eta, eps)
+    _check(lib().hhs_snapshot_write(sys.ref, n, time, ctypes.byref(prm), dt, step,
+                                    path.encode(), stream), "hhs_snapshot_write")
+
+
+def snapshot_read(sys, path, stream=None):
+    n, t, st = ctypes.c_int32(), ctypes.c_double(), ctypes.c_int32()
+    _check(lib().hhs_snapshot_read(sys.ref, path.encode(), ctypes.byref(n), ctypes.byref(t),
+                                   ctypes.byref(st), stream), "hhs_snapshot_read")
+    return n.value, t.value, st.value
+
+
+def hold(ctx, sys, n, stime, etime, dt, prec=PREC_MIXED, snapshot_every=0, prefix=None,
+         max_log=1024, stream=None):
+    """hold(): integrate stime..etime; returns [(time, energy)] diagnostics."""
+    t = np.zeros(max_log)
+    e = np.zeros(max_log)
+    log = RunLog(_d(t), _d(e), max_log, 0)
+    _check(lib().hhs_hold(ctx.h, sys.ref, n, stime, etime, dt, prec, snapshot_every,
+                          prefix.encode() if prefix else None, ctypes.byref(log), stream),
+           "hhs_hold")
+    return list(zip(t[:log.n_entries].tolist(), e[:log.n_entries].tolist()))
 
 
 def hold_step_host(ctx, sys, n, dt, calc_timestep=True, prec=PREC_FP64, stream=None):

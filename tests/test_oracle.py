@@ -153,6 +153,29 @@ def test_kick_matches_numpy(oracle):
     assert np.allclose(sink["vx"], s["vx"] + acc[0] * 0.25, rtol=0, atol=0)
 
 
+def test_softened_kick_matches_numpy_and_eps0_is_plain(oracle):
+    s = _rand_system(200, 3)
+    plain = {k: v.copy() for k, v in s.items()}
+    zero = {k: v.copy() for k, v in s.items()}
+    a0 = oracle.kick(plain, s, 0.1)
+    lib = oracle.lib()
+    ax, ay, az = np.zeros(200), np.zeros(200), np.zeros(200)
+    d = oracle._d
+    lib.oracle_kick(200, d(zero["x"]), d(zero["y"]), d(zero["z"]), d(zero["vx"]), d(zero["vy"]),
+                    d(zero["vz"]), d(ax), d(ay), d(az), 200, d(s["x"]), d(s["y"]), d(s["z"]),
+                    d(s["m"]), 0.1)
+    assert np.array_equal(a0[0], ax) and np.array_equal(zero["vz"], plain["vz"])
+    eps = 0.3
+    soft = {k: v.copy() for k, v in s.items()}
+    a = oracle.kick(soft, s, 0.1, eps=eps)
+    for i in (0, 99, 199):
+        dx, dy, dz = s["x"] - s["x"][i], s["y"] - s["y"][i], s["z"] - s["z"][i]
+        d2 = dx * dx + dy * dy + dz * dz + eps * eps
+        w = s["m"] / (d2 * np.sqrt(d2))
+        assert np.allclose(a[:, i], [np.sum(dx * w), np.sum(dy * w), np.sum(dz * w)],
+                           rtol=1e-12, atol=0)
+
+
 def test_hold_step_conserves_energy_and_tracks_leaf_time(oracle, hhs):
     s = hhs.plummer(512, 11)
     e0, _ = oracle.energy(s)
