@@ -45,8 +45,13 @@ def parse():
     p.add_argument("--small-n", type=int, default=64,
                    help="device schedule: nodes with n <= this are solved by one CTA")
     p.add_argument("--ctas-per-sm", type=int, default=2)
-    p.add_argument("--cluster-size", type=int, default=1)
-    p.add_argument("--mid-n", type=int, default=0)
+    p.add_argument("--cluster-size", type=int, default=2,
+                   help="launch the HOLD kernel in thread-block clusters of this size")
+    p.add_argument("--mid-n", type=int, default=640,
+                   help="subtrees of at most this many particles run from shared memory on "
+                        "one cluster (0 = off)")
+    p.add_argument("--mid-dist-n", type=int, default=96,
+                   help="inside such a subtree, nodes above this size spread over the cluster")
     p.add_argument("--packed", type=int, default=0)
     p.add_argument("--units-per-cta", type=int, default=16)
     p.add_argument("--autotune", action="store_true",
@@ -117,6 +122,8 @@ def aggregate_value(steps, world, t_max_ms):
 
 # ------------------------------------------------------------------------ clocks
 class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples every 50 ms on a reader thread; only
+    the samples taken between mark_start() and mark_stop() (the timed region) count."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -124,28 +131,55 @@ class ClockSampler:
     def __init__(self, dev):
         self.dev = dev
         self.p = None
+        self.lines = []
+        self.t0 = self.t1 = None
+        self.th = None
 
     def start(self):
+        import threading
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200",
+                                       "--format=csv,noheader,nounits", "-lms", "50",
                                        "-i", str(self.dev)], stdout=subprocess.PIPE,
                                       stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.p = None
+            return
+
+        def reader():
+            for line in self.p.stdout:
+                self.lines.append((time.monotonic(), line))
+
+        self.th = threading.Thread(target=reader, daemon=True)
+        self.th.start()
+        deadline = time.monotonic() + 5.0
+        while not self.lines and time.monotonic() < deadline:
+            time.sleep(0.01)
+
+    def mark_start(self):
+        self.t0 = time.monotonic()
+
+    def mark_stop(self):
+        self.t1 = time.monotonic()
+        # let the sampler take at least one more sample past the region's end
+        time.sleep(0.06)
 
     def stop(self):
         if self.p is None:
             return None
         self.p.terminate()
         try:
-            out, _ = self.p.communicate(timeout=5)
+            self.p.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.p.kill()
-            out, _ = self.p.communicate()
+        if self.th is not None:
+            self.th.join(timeout=5)
+        inside = [l for t, l in self.lines
+                  if self.t0 is not None and self.t1 is not None and self.t0 <= t <= self.t1 + 0.06]
+        use = inside if inside else [l for _, l in self.lines]
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.splitlines():
+        for line in use:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -161,7 +195,7 @@ class ClockSampler:
             return None
         sm.sort()
         return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "in_timed_region": bool(inside)}
 
 
 # ------------------------------------------------------------------------ reference arm
@@ -211,7 +245,7 @@ def run_ours(a, rank, world, torch, dist):
     e0 = hhs.energy_host(ics)
     ctx = hhs.Context(a.n, 64, eta=a.eta)
     ctx.set_tuning(a.small_n, a.units_per_cta, a.ctas_per_sm, cluster_size=a.cluster_size,
-                   mid_n=a.mid_n, packed=a.packed)
+                   mid_n=a.mid_n, packed=a.packed, mid_dist_n=a.mid_dist_n)
     sys_ = hhs.ParticleSystem(a.n)
     sys_.upload(ics, stream=sh)
     tuned = None
@@ -241,6 +275,7 @@ def run_ours(a, rank, world, torch, dist):
         barrier()
         torch.cuda.synchronize()
         clocks.start()
+        clocks.mark_start()
         l0 = hhs.launch_count()
         for k in range(a.steps):
             flush.zero_()
@@ -249,6 +284,7 @@ def run_ours(a, rank, world, torch, dist):
             evs[k][1].record(stream)
         torch.cuda.synchronize()
         l1 = hhs.launch_count()
+        clocks.mark_stop()
         barrier()
         clk = clocks.stop()
         ctx.check(sh)

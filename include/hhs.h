@@ -49,8 +49,10 @@ typedef struct {
     int32_t n_fast;
 } hhs_partition;
 
-/* nbody_params<T>, src/particle_system.cuh:13-17 (eps is stored, unused as in the
- * reference: src/hold.cuh:136,141,157) */
+/* nbody_params<T>, src/particle_system.cuh:13-17. The reference stores eps but never
+ * applies it (TODOs at src/hold.cuh:136,141,157); here every kick of the HOLD step
+ * (hhs_hold_step, hhs_hold_step_host, hhs_hold_batched) uses d^2 + eps^2, and eps = 0
+ * reproduces the unsoftened reference bit for bit. */
 typedef struct {
     double eta;
     double eps;
@@ -124,13 +126,20 @@ typedef struct {
     int32_t ctas_per_sm;     /* CTAs of the persistent kernel per SM (1 or 2) */
     int32_t warp_n;          /* nodes with at most warp_n (<= 32) particles run on one warp */
     int32_t cluster_size;    /* launch the persistent kernel in thread-block clusters (1,2,4,8) */
-    int32_t mid_n;           /* with clusters: nodes with small_n < n <= mid_n run on one cluster */
+    int32_t mid_n;           /* nodes with n <= mid_n (at most 640) run, with their whole subtree,
+                                from shared memory on the first cluster (on CTA 0 when
+                                cluster_size is 1); 0 = never */
     int32_t packed;          /* mixed kick: two sinks per thread in packed FP32x2 arithmetic */
-    int32_t _reserved;
+    int32_t mid_dist_n;      /* in such a subtree, nodes with more than mid_dist_n particles spread
+                                their pair work over the cluster's CTAs */
     double ms_per_step;      /* filled by hhs_ctx_autotune: time of the chosen setting */
 } hhs_tuning;
 hhs_status hhs_ctx_set_tuning(hhs_ctx* ctx, const hhs_tuning* t);
 hhs_status hhs_ctx_get_tuning(hhs_ctx* ctx, hhs_tuning* t);
+/* Launch shape of the persistent HOLD kernel under the current tuning: grid_ctas[0] for
+ * HHS_PREC_FP64 and grid_ctas[1] for HHS_PREC_MIXED (CTAs of 256 threads), and its
+ * dynamic shared memory per CTA. Either pointer may be NULL. */
+hhs_status hhs_ctx_get_launch(hhs_ctx* ctx, int32_t* grid_ctas, int32_t* smem_bytes);
 /* Autotuner: times hold_step on the caller's system for a grid of tuning candidates,
  * restoring the particle state before every trial and at the end, and keeps the fastest.
  * Allocates a snapshot of the system (call it outside any timed or captured region). */

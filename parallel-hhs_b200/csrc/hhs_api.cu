@@ -362,6 +362,11 @@ extern "C" hhs_status hhs_ctx_get_tuning(hhs_ctx* c, hhs_tuning* t) {
     return engine_get_tuning(c, t);
 }
 
+extern "C" hhs_status hhs_ctx_get_launch(hhs_ctx* c, int32_t* grid_ctas, int32_t* smem_bytes) {
+    if (!c) return HHS_ERR_INVALID_ARG;
+    return engine_get_launch(c, grid_ctas, smem_bytes);
+}
+
 extern "C" hhs_status hhs_ctx_get_stats(hhs_ctx* c, hhs_stats* out, void* stream) {
     if (!c || !out) return HHS_ERR_INVALID_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -593,15 +598,14 @@ extern "C" hhs_status hhs_ctx_autotune(hhs_ctx* c, hhs_particle_system* sys, int
     st = copy_all(true);
     // (small_n, mid_n, cluster_size) tiers, then units per CTA and CTAs per SM
     struct Tier { int sn, mid, cs; };
-    const Tier tiers[] = {{32, 0, 1},    {64, 0, 1},     {128, 0, 1},   {256, 0, 1},
-                          {32, 512, 8},  {64, 1024, 8},  {64, 2048, 8}, {128, 2048, 8},
-                          {32, 1024, 4}, {64, 2048, 4}};
-    const int upc_cands[] = {4, 8, 16};
+    const Tier tiers[] = {{64, 0, 1},   {128, 0, 1},  {64, 0, 2},   {64, 640, 1},
+                          {64, 640, 2}, {64, 256, 2}, {64, 640, 4}, {64, 640, 8}};
+    const int upc_cands[] = {8, 16};
     for (int cps = 1; cps <= 2; cps++)
     for (const Tier& tr : tiers) {
         for (int upc : upc_cands) {
             if (st != HHS_OK) break;
-            hhs_tuning t{tr.sn, upc, cps, cur.warp_n, tr.cs, tr.mid, cur.packed, 0, 0.0};
+            hhs_tuning t{tr.sn, upc, cps, cur.warp_n, tr.cs, tr.mid, cur.packed, cur.mid_dist_n, 0.0};
             if (engine_set_tuning(c, t) != HHS_OK) continue;  // e.g. no cluster occupancy
             st = copy_all(false);
             if (st == HHS_OK) st = engine_hold_step(c, soa_of(sys), n, dt, true, prec, false, s);
@@ -653,7 +657,8 @@ extern "C" hhs_status hhs_hold_integrate(hhs_ctx* c, hhs_particle_system* sys, i
     std::memcpy(&dtbits, &dt, sizeof(dtbits));
     const unsigned long long key[6] = {
         reinterpret_cast<uintptr_t>(sys->x), (unsigned long long)n, dtbits,
-        ((unsigned long long)steps << 8) | (unsigned long long)prec,
+        ((unsigned long long)steps << 32) | ((unsigned long long)t.mid_dist_n << 8) |
+            (unsigned long long)prec,
         ((unsigned long long)t.small_n << 32) | (unsigned)t.mid_n,
         ((unsigned long long)t.units_per_cta << 32) |
             (unsigned)(t.ctas_per_sm | (t.warp_n << 8) | (t.cluster_size << 16) | (t.packed << 24))};

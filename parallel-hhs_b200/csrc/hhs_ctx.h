@@ -43,6 +43,7 @@ hhs_status engine_init(hhs_ctx* c, void* base);
 void engine_destroy(hhs_ctx* c);
 hhs_status engine_set_tuning(hhs_ctx* c, const hhs_tuning& t);
 hhs_status engine_get_tuning(hhs_ctx* c, hhs_tuning* t);
+hhs_status engine_get_launch(hhs_ctx* c, int32_t* grid, int32_t* smem_bytes);
 hhs_status engine_get_profile(hhs_ctx* c, hhs_profile* out, bool reset);
 hhs_status engine_get_level_profile(hhs_ctx* c, double* ms, uint64_t* counts);
 hhs_status engine_reset_barrier(hhs_ctx* c, cudaStream_t stream);

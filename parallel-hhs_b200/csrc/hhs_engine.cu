@@ -65,6 +65,7 @@ struct EngineState {
 struct EParams {
     SoA P;
     int n_top, n_max, max_levels, small_n, calc_top, profile, units_per_cta, warp_n, mid_n;
+    int mid_dist_n;  // cluster subtree solver: nodes above this size are spread over the cluster
     int packed;  // mixed kick: two sinks per thread in packed FP32x2 arithmetic
     double dt_top, eta, eta_s2, eps2;
     float inv_eta_s2, inv_eta, eps2f;
@@ -81,7 +82,45 @@ struct EParams {
     unsigned* err;
 };
 
+// Cluster subtree solver state (one replica per CTA of the cluster): a subsystem of at
+// most kMid particles with its whole subtree lives in shared memory.
+constexpr int kMid = 640;
+constexpr int kMidW = kMid / 32;
+struct __align__(16) MidState {
+    double x[kMid], y[kMid], z[kMid], vx[kMid], vy[kMid], vz[kMid], m[kMid], ts[kMid];
+    float4 A[kMid], B[kMid], V[kMid];     // mixed: position hi + mass, position lo, velocity
+    int g[kMid];                          // global index of each slot
+    unsigned fmask[kMaxLevels][kMidW];    // fast set (slot bitmask) chosen at each depth
+    int lone[kMaxLevels];                 // slot folded into the slow set, or -1
+    int nmem[kMaxLevels];                 // member count of the node at each depth
+    short mem[kMid];                      // member slots of the current node, increasing
+    short kl[kMid];                       // kick order: slow slots (lone last), then fast
+    union {
+        double pmin[8][32];               // partial timesteps (FP64)
+        float pmax[8][32];                // partial pair rates (mixed)
+        float part[8][3][32];             // partial accelerations (mixed)
+    } red;
+    unsigned allw[kMidW];                 // members of the subtree's root (every slot)
+    short wslot[32];                      // warp solver: slot of each lane's particle
+    unsigned wf[kMaxLevels];              // warp solver: fast-lane mask per depth
+    int wl[kMaxLevels];                   // warp solver: lane folded into the slow set, or -1
+    int wbase[kMidW], wbase2[kMidW];
+    int wcnt[kEB / 32];
+    int total, total2;
+};
+
 struct __align__(16) Smem {
+    float colred[kEB / 32][64];
+    unsigned long long prof_ns[8][kMaxLevels];  // phase times of this launch (CTA 0)
+    unsigned prof_cnt[8][kMaxLevels];
+    double prof_pairs[8];
+    unsigned wfast[kMaxLevels];   // warp solver: fast-lane mask per depth
+    int wlone[kMaxLevels];        // warp solver: lane folded into the slow set, or -1
+    int warp_tot[kEB / 32];
+    int red[kEB / 32];
+    int ok;
+    int bcast;
+    // last, so that the persistent kernel's dynamic allocation can extend it to a MidState
     union {
         struct { float4 A[kEB], B[kEB], V[kEB]; } tsm;         // mixed timestep tiles
         struct { double x[kEB], y[kEB], z[kEB], vx[kEB], vy[kEB], vz[kEB], m[kEB]; } tsd;
@@ -97,17 +136,12 @@ struct __align__(16) Smem {
             int g[32];
         } tiny;
     } u;
-    float colred[kEB / 32][64];
-    unsigned long long prof_ns[8][kMaxLevels];  // phase times of this launch (CTA 0)
-    unsigned prof_cnt[8][kMaxLevels];
-    double prof_pairs[8];
-    unsigned wfast[kMaxLevels];   // warp solver: fast-lane mask per depth
-    int wlone[kMaxLevels];        // warp solver: lane folded into the slow set, or -1
-    int warp_tot[kEB / 32];
-    int red[kEB / 32];
-    int ok;
-    int bcast;
 };
+
+// dynamic shared memory of the persistent kernel: Smem with its last member grown to
+// hold a MidState
+constexpr size_t kEngineSmem =
+    offsetof(Smem, u) + (sizeof(MidState) > sizeof(Smem::u) ? sizeof(MidState) : sizeof(Smem::u));
 
 __device__ __forceinline__ unsigned long long gtimer() {
     unsigned long long t;
@@ -120,27 +154,21 @@ __device__ __forceinline__ int ld_volatile_i32(const int32_t* p) {
 }
 
 // ---------------------------------------------------------------- grid barrier
-// Sense-reversing barrier over all CTAs of the cooperative grid. When the grid is
-// launched in thread-block clusters, the CTAs of a cluster first meet at the hardware
-// cluster barrier and only the cluster's first CTA arrives at the global counter, so
-// the serialised atomics drop by the cluster size. The last arrival resets the counter
-// and advances the generation; the others poll the generation, give up after
-// kBarrierTimeoutNs (or as soon as another CTA recorded an error) and report failure
-// instead of hanging.
+// Sense-reversing barrier over all CTAs of the cooperative grid (also when the grid is
+// launched in thread-block clusters: a cluster-level first stage measured slower). The
+// last arrival resets the counter and advances the generation; the others poll the
+// generation, give up after kBarrierTimeoutNs (or as soon as another CTA recorded an
+// error) and report failure instead of hanging.
 __device__ bool grid_barrier(const EParams& E, Smem& sm) {
-    namespace cg = cooperative_groups;
-    const unsigned cs = cg::this_cluster().num_blocks();
-    const bool leader = cs == 1 || cg::this_cluster().block_rank() == 0;
-    if (cs > 1) cg::this_cluster().sync();
-    else __syncthreads();
-    if (leader && threadIdx.x == 0) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
         // The CTA barrier above orders every thread's writes before this thread's
         // release; arrival is an acquire-release add (the last arrival acquires all the
         // others' releases), the generation is advanced with a release add and polled
         // with acquire loads, so no separate fences are needed.
         int ok = 1;
         EngineState* st = E.st;
-        const unsigned parties = gridDim.x / cs;
+        const unsigned parties = gridDim.x;
         const unsigned gen = ld_acquire_u32(&st->bar_gen);
         const unsigned arrived = atom_add_acq_rel_u32(&st->bar_count, 1u);
         if (arrived == parties - 1) {
@@ -162,10 +190,6 @@ __device__ bool grid_barrier(const EParams& E, Smem& sm) {
             }
         }
         sm.ok = ok;
-    }
-    if (cs > 1) {
-        cg::this_cluster().sync();
-        return *reinterpret_cast<volatile unsigned*>(E.err) == 0u;
     }
     __syncthreads();
     return sm.ok != 0;
@@ -1063,6 +1087,727 @@ __device__ void tiny_hold(const EParams& E, const int32_t* S, int n, int level0,
     __syncthreads();
 }
 
+// ---------------------------------------------------------------- cluster subtree solver
+// A subsystem of at most kMid particles, with its whole subtree, on one thread-block
+// cluster (or one CTA). Every CTA of the cluster holds a replica of the subsystem in
+// shared memory and walks the same recursion; the members of each level are slot
+// bitmasks (stable order = slot order, the N_fast == 1 fold visits the lone slot last
+// among the slow ones). Splits and drifts are computed redundantly in every CTA (the
+// same arithmetic in the same order keeps the replicas identical). The pair work of a
+// node with more than `dist_n` members is divided among the cluster's CTAs: each CTA
+// computes its share of the sinks and stores the results (timesteps or velocities)
+// into every replica through distributed shared memory, between two cluster barriers
+// (the first one makes sure no CTA is still reading what the stores overwrite). Nodes
+// of up to 32 members run with their subtree on one warp of every CTA (warp_subtree);
+// the others are computed whole by every CTA with CTA barriers only. Global memory is
+// read once at entry and written once at exit.
+namespace mid {
+
+// slots of the set bits of words[0..nw) in increasing order -> out; returns the count
+__device__ __forceinline__ int compact(const unsigned* words, int nw, short* out,
+                                       MidState& M) {
+    const int tid = threadIdx.x, lane = tid & 31;
+    if (tid < 32) {
+        const int c = lane < nw ? __popc(words[lane]) : 0;
+        const int inc = warp_incl_scan(c, lane);
+        if (lane < nw) M.wbase[lane] = inc - c;
+        if (lane == 31) M.total = inc;
+    }
+    __syncthreads();
+    for (int s = tid; s < nw * 32; s += kEB) {
+        const unsigned w = words[s >> 5];
+        const int b = s & 31;
+        if ((w >> b) & 1u) out[M.wbase[s >> 5] + __popc(w & ((1u << b) - 1u))] = (short)s;
+    }
+    const int total = M.total;
+    __syncthreads();
+    return total;
+}
+
+// kick order of a node in one pass: the slow members (stable; the lone slot, if any,
+// last) then the fast ones. Returns the number of slow slots; *nf_out the fast count.
+__device__ __forceinline__ int kick_order(const unsigned* memw, const unsigned* fastw, int lone,
+                                          int nw, short* out, MidState& M, int* nf_out) {
+    const int tid = threadIdx.x, lane = tid & 31;
+    const unsigned lone_word = lone >= 0 ? (unsigned)(lone >> 5) : 0xffffffffu;
+    const unsigned lone_keep = lone >= 0 ? ~(1u << (lone & 31)) : ~0u;
+    if (tid < 32) {
+        unsigned sw = 0u, fw = 0u;
+        if (lane < nw) {
+            fw = fastw[lane];
+            sw = memw[lane] & ~fw;
+            if ((unsigned)lane == lone_word) sw &= lone_keep;
+        }
+        const int cs_ = __popc(sw), cf = __popc(fw);
+        const int is = warp_incl_scan(cs_, lane), iff = warp_incl_scan(cf, lane);
+        if (lane < nw) {
+            M.wbase[lane] = is - cs_;
+            M.wbase2[lane] = iff - cf;
+        }
+        if (lane == 31) {
+            M.total = is + (lone >= 0 ? 1 : 0);
+            M.total2 = iff;
+        }
+    }
+    __syncthreads();
+    const int ns = M.total, nf = M.total2;
+    for (int s = tid; s < nw * 32; s += kEB) {
+        const int w = s >> 5, b = s & 31;
+        const unsigned fw = fastw[w];
+        unsigned sw = memw[w] & ~fw;
+        if ((unsigned)w == lone_word) sw &= lone_keep;
+        const unsigned below = (1u << b) - 1u;
+        if ((sw >> b) & 1u) out[M.wbase[w] + __popc(sw & below)] = (short)s;
+        else if ((fw >> b) & 1u) out[ns + M.wbase2[w] + __popc(fw & below)] = (short)s;
+    }
+    if (tid == 0 && lone >= 0) out[ns - 1] = (short)lone;
+    __syncthreads();
+    *nf_out = nf;
+    return ns;
+}
+
+// mixed-precision views of slot k (double-single position, FP32 velocity)
+__device__ __forceinline__ void refresh_pos(MidState& M, int k) {
+    const DS a = ds_split(M.x[k]), b = ds_split(M.y[k]), c = ds_split(M.z[k]);
+    M.A[k] = make_float4(a.hi, b.hi, c.hi, (float)M.m[k]);
+    M.B[k] = make_float4(a.lo, b.lo, c.lo, 0.0f);
+}
+__device__ __forceinline__ void refresh_vel(MidState& M, int k) {
+    M.V[k] = make_float4((float)M.vx[k], (float)M.vy[k], (float)M.vz[k], 0.0f);
+}
+
+// a result for slot p: into this replica only, or into every replica of the cluster
+template <class T>
+__device__ __forceinline__ void put(T* p, T v, bool dist, int cs) {
+    if (!dist) {
+        *p = v;
+        return;
+    }
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    for (int r = 0; r < cs; r++) *cl.map_shared_rank(p, (unsigned)r) = v;
+}
+
+// the CTA's share [s0, s1) of n sinks and the (sink group, source part) work layout
+struct Share {
+    int s0, s1, ng, wpg;
+};
+__device__ __forceinline__ Share share_of(int n, bool dist, int cs, int rank) {
+    Share sh;
+    const int parts = dist ? cs : 1;
+    const int r = dist ? rank : 0;
+    const int q = (n + parts - 1) / parts;
+    sh.s0 = min(n, r * q);
+    sh.s1 = min(n, sh.s0 + q);
+    sh.ng = (sh.s1 - sh.s0 + 31) / 32;
+    sh.wpg = sh.ng >= kEB / 32 ? 1 : (sh.ng > 0 ? (kEB / 32) / sh.ng : 1);
+    return sh;
+}
+
+// max pair rate of sink i over the sources list[q], q = q0, q0 + step, ... < qn (the sink
+// itself excluded); four independent pairs per iteration
+__device__ __forceinline__ float rate_over(const EParams& E, const MidState& M, const short* list,
+                                           int q0, int qn, int step, int i) {
+    const float4 Ai = M.A[i], Bi = M.B[i], Vi = M.V[i];
+    float mr = 0.0f;
+    int q = q0;
+    auto one = [&](int j) {
+        const float4 A = M.A[j], B = M.B[j], V = M.V[j];
+        const float r = ts_pair_rate_mixed(ds_diff(Ai.x, Bi.x, A.x, B.x), ds_diff(Ai.y, Bi.y, A.y, B.y),
+                                           ds_diff(Ai.z, Bi.z, A.z, B.z), Vi.x - V.x, Vi.y - V.y,
+                                           Vi.z - V.z, Ai.w + A.w, E.inv_eta_s2, E.inv_eta);
+        return j == i ? 0.0f : r;
+    };
+#pragma unroll 1
+    for (; q + 3 * step < qn; q += 4 * step) {
+        const int j0 = list[q], j1 = list[q + step], j2 = list[q + 2 * step], j3 = list[q + 3 * step];
+        const float r0 = one(j0), r1 = one(j1), r2 = one(j2), r3 = one(j3);
+        mr = fmaxf(mr, fmaxf(fmaxf(r0, r1), fmaxf(r2, r3)));
+    }
+#pragma unroll 1
+    for (; q < qn; q += step) mr = fmaxf(mr, one(list[q]));
+    return mr;
+}
+
+// mixed acceleration of sink i from the sources list[q], q = q0, q0 + step, ... < qn
+__device__ __forceinline__ void acc_over(const EParams& E, const MidState& M, const short* list,
+                                         int q0, int qn, int step, int i, float (&a)[3]) {
+    const float4 Ai = M.A[i], Bi = M.B[i];
+    auto one = [&](int j) {
+        const float4 A = M.A[j], B = M.B[j];
+        const float dx = ds_diff(A.x, B.x, Ai.x, Bi.x);
+        const float dy = ds_diff(A.y, B.y, Ai.y, Bi.y);
+        const float dz = ds_diff(A.z, B.z, Ai.z, Bi.z);
+        const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, E.eps2f)));
+        const float ri = rsqrt_nr(d2);
+        const float mr3 = (d2 > 0.0f) ? A.w * ri * ri * ri : 0.0f;
+        a[0] = fmaf(dx, mr3, a[0]);
+        a[1] = fmaf(dy, mr3, a[1]);
+        a[2] = fmaf(dz, mr3, a[2]);
+    };
+    int q = q0;
+#pragma unroll 1
+    for (; q + 3 * step < qn; q += 4 * step) {
+        const int j0 = list[q], j1 = list[q + step], j2 = list[q + 2 * step], j3 = list[q + 3 * step];
+        one(j0); one(j1); one(j2); one(j3);
+    }
+#pragma unroll 1
+    for (; q < qn; q += step) one(list[q]);
+}
+
+}  // namespace mid
+
+// Warp solver for a node of at most 32 members with its whole subtree (every node below
+// it is smaller): warp 0 of the CTA, one member per lane, warp barriers only. Lanes are
+// members in increasing slot order (the stable order); the state stays in the MidState
+// arrays, read and written by slot. Work counters go to lane 0's accumulators.
+template <int PREC>
+__device__ void warp_subtree(const EParams& E, MidState& M, const unsigned* memw, int nw,
+                             int cnt, int level0, bool calc0, unsigned long long& nodes,
+                             int& maxl, double& kpairs, double& tpairs, double& leaf,
+                             bool& ok) {
+    const int lane = threadIdx.x & 31;
+    // lane l takes the l-th member
+    {
+        const int c = lane < nw ? __popc(memw[lane]) : 0;
+        const int base = warp_incl_scan(c, lane) - c;
+        for (int w = 0; w < nw; w++) {
+            const int bw = __shfl_sync(HHS_FULL_MASK, base, w);
+            const int cw = __shfl_sync(HHS_FULL_MASK, c, w);
+            if (lane >= bw && lane < bw + cw)
+                M.wslot[lane] = (short)(w * 32 + (int)__fns(memw[w], 0, lane - bw + 1));
+        }
+        __syncwarp();
+    }
+    const int me = lane < cnt ? M.wslot[lane] : 0;
+    const unsigned top = cnt >= 32 ? 0xffffffffu : ((1u << cnt) - 1u);
+    unsigned long long after1 = 0, after2 = 0, calcm = calc0 ? 1ull : 0ull;
+    int dd = 0;
+    while (dd >= 0) {
+        const int lvl = level0 + dd;
+        const unsigned long long bit = 1ull << dd;
+        const double dt = ldexp(E.dt_top, -lvl);
+        const unsigned mk = dd == 0 ? top : M.wf[dd - 1];
+        const bool in = (mk >> lane) & 1u;
+        if (!(after1 & bit)) {
+            if (lvl >= E.max_levels || lvl >= kMaxLevels - 1) {
+                if (lane == 0) atomicOr(E.err, HHS_ERRBIT_DEPTH);
+                ok = false;
+                return;
+            }
+            const int n_here = __popc(mk);
+            if (calcm & bit) {
+                if (in) {
+                    const unsigned srcs = mk & ~(1u << lane);
+                    if (PREC == HHS_PREC_FP64) {
+                        const double xi = M.x[me], yi = M.y[me], zi = M.z[me];
+                        const double vxi = M.vx[me], vyi = M.vy[me], vzi = M.vz[me], mi = M.m[me];
+                        double mv = 1.e30;
+#pragma unroll 1
+                        for (unsigned m = srcs; m; m &= m - 1u) {
+                            const int j = M.wslot[__ffs(m) - 1];
+                            ts_pair_fp64(f64_sub(xi, M.x[j]), f64_sub(yi, M.y[j]),
+                                         f64_sub(zi, M.z[j]), f64_sub(vxi, M.vx[j]),
+                                         f64_sub(vyi, M.vy[j]), f64_sub(vzi, M.vz[j]), mi, M.m[j],
+                                         E.eta, E.eta_s2, mv);
+                        }
+                        M.ts[me] = mv;
+                    } else {
+                        const float4 Ai = M.A[me], Bi = M.B[me], Vi = M.V[me];
+                        auto rate = [&](int j) {
+                            const float4 A = M.A[j], B = M.B[j], V = M.V[j];
+                            return ts_pair_rate_mixed(
+                                ds_diff(Ai.x, Bi.x, A.x, B.x), ds_diff(Ai.y, Bi.y, A.y, B.y),
+                                ds_diff(Ai.z, Bi.z, A.z, B.z), Vi.x - V.x, Vi.y - V.y, Vi.z - V.z,
+                                Ai.w + A.w, E.inv_eta_s2, E.inv_eta);
+                        };
+                        float mr = 0.0f;
+                        unsigned m = srcs;
+#pragma unroll 1
+                        while (__popc(m) >= 4) {  // four independent pairs per iteration
+                            const int l0 = __ffs(m) - 1;
+                            m &= m - 1u;
+                            const int l1 = __ffs(m) - 1;
+                            m &= m - 1u;
+                            const int l2 = __ffs(m) - 1;
+                            m &= m - 1u;
+                            const int l3 = __ffs(m) - 1;
+                            m &= m - 1u;
+                            const float r0 = rate(M.wslot[l0]), r1 = rate(M.wslot[l1]);
+                            const float r2 = rate(M.wslot[l2]), r3 = rate(M.wslot[l3]);
+                            mr = fmaxf(mr, fmaxf(fmaxf(r0, r1), fmaxf(r2, r3)));
+                        }
+#pragma unroll 1
+                        for (; m; m &= m - 1u) mr = fmaxf(mr, rate(M.wslot[__ffs(m) - 1]));
+                        const double tv = 1.0 / (double)mr;
+                        M.ts[me] = tv < 1.e30 ? tv : 1.e30;
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) tpairs += (double)n_here * (double)(n_here - 1);
+            }
+            unsigned F = __ballot_sync(HHS_FULL_MASK, in && M.ts[me] <= dt);
+            int lone = -1;
+            if (__popc(F) == 1) {
+                lone = __ffs(F) - 1;
+                F = 0u;
+            }
+            if (lane == 0) {
+                M.wf[dd] = F;
+                M.wl[dd] = lone;
+                const int nf = __popc(F);
+                const double ns = (double)(n_here - nf), nfd = (double)nf;
+                nodes++;
+                maxl = max(maxl, lvl);
+                kpairs += ns * (ns - 1.0) + 2.0 * ns * nfd;
+                if (nf == 0) leaf += dt;
+            }
+            __syncwarp();
+            after1 |= bit;
+            if (F) {
+                dd++;
+                const unsigned long long cb = 1ull << dd;
+                calcm &= ~cb; after1 &= ~cb; after2 &= ~cb;
+                continue;
+            }
+        }
+        if (!(after2 & bit)) {
+            const unsigned F = M.wf[dd];
+            const int lone = M.wl[dd];
+            const unsigned L = mk & ~F;
+            const bool is_slow = (L >> lane) & 1u, is_fast = (F >> lane) & 1u;
+            const double h = dt * 0.5;
+            if (L) {
+                // first half drift of the slow lanes (src/hold.cuh:123-124)
+                if (is_slow) {
+                    if (PREC == HHS_PREC_FP64) {
+                        M.x[me] = f64_add(M.x[me], f64_mul(M.vx[me], h));
+                        M.y[me] = f64_add(M.y[me], f64_mul(M.vy[me], h));
+                        M.z[me] = f64_add(M.z[me], f64_mul(M.vz[me], h));
+                    } else {
+                        M.x[me] = fma(M.vx[me], h, M.x[me]);
+                        M.y[me] = fma(M.vy[me], h, M.y[me]);
+                        M.z[me] = fma(M.vz[me], h, M.z[me]);
+                        mid::refresh_pos(M, me);
+                    }
+                }
+                __syncwarp();
+                double vx = 0.0, vy = 0.0, vz = 0.0;
+                if (is_slow || is_fast) {
+                    if (PREC == HHS_PREC_FP64) {
+                        const double xi = M.x[me], yi = M.y[me], zi = M.z[me];
+                        const unsigned Lord = lone >= 0 ? (L & ~(1u << lone)) : L;
+                        double aL[3] = {0, 0, 0}, aF[3] = {0, 0, 0};
+#pragma unroll 1
+                        for (unsigned m = Lord; m; m &= m - 1u) {
+                            const int j = M.wslot[__ffs(m) - 1];
+                            kick_pair_fp64(f64_sub(M.x[j], xi), f64_sub(M.y[j], yi),
+                                           f64_sub(M.z[j], zi), M.m[j], aL[0], aL[1], aL[2],
+                                           E.eps2);
+                        }
+                        if (lone >= 0) {
+                            const int j = M.wslot[lone];
+                            kick_pair_fp64(f64_sub(M.x[j], xi), f64_sub(M.y[j], yi),
+                                           f64_sub(M.z[j], zi), M.m[j], aL[0], aL[1], aL[2],
+                                           E.eps2);
+                        }
+                        if (is_slow) {
+#pragma unroll 1
+                            for (unsigned m = F; m; m &= m - 1u) {
+                                const int j = M.wslot[__ffs(m) - 1];
+                                kick_pair_fp64(f64_sub(M.x[j], xi), f64_sub(M.y[j], yi),
+                                               f64_sub(M.z[j], zi), M.m[j], aF[0], aF[1], aF[2],
+                                               E.eps2);
+                            }
+                        }
+                        vx = f64_add(M.vx[me], f64_mul(aL[0], dt));
+                        vy = f64_add(M.vy[me], f64_mul(aL[1], dt));
+                        vz = f64_add(M.vz[me], f64_mul(aL[2], dt));
+                        if (is_slow && F) {
+                            vx = f64_add(vx, f64_mul(aF[0], dt));
+                            vy = f64_add(vy, f64_mul(aF[1], dt));
+                            vz = f64_add(vz, f64_mul(aF[2], dt));
+                        }
+                    } else {
+                        const float4 Ai = M.A[me], Bi = M.B[me];
+                        float a[3] = {0, 0, 0};
+                        auto acc = [&](int j) {
+                            const float4 A = M.A[j], B = M.B[j];
+                            const float dx = ds_diff(A.x, B.x, Ai.x, Bi.x);
+                            const float dy = ds_diff(A.y, B.y, Ai.y, Bi.y);
+                            const float dz = ds_diff(A.z, B.z, Ai.z, Bi.z);
+                            const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, E.eps2f)));
+                            const float ri = rsqrt_nr(d2);
+                            const float mr3 = (d2 > 0.0f) ? A.w * ri * ri * ri : 0.0f;
+                            a[0] = fmaf(dx, mr3, a[0]);
+                            a[1] = fmaf(dy, mr3, a[1]);
+                            a[2] = fmaf(dz, mr3, a[2]);
+                        };
+                        unsigned m = is_slow ? (L | F) : L;
+#pragma unroll 1
+                        while (__popc(m) >= 4) {
+                            const int l0 = __ffs(m) - 1;
+                            m &= m - 1u;
+                            const int l1 = __ffs(m) - 1;
+                            m &= m - 1u;
+                            const int l2 = __ffs(m) - 1;
+                            m &= m - 1u;
+                            const int l3 = __ffs(m) - 1;
+                            m &= m - 1u;
+                            acc(M.wslot[l0]);
+                            acc(M.wslot[l1]);
+                            acc(M.wslot[l2]);
+                            acc(M.wslot[l3]);
+                        }
+#pragma unroll 1
+                        for (; m; m &= m - 1u) acc(M.wslot[__ffs(m) - 1]);
+                        vx = fma((double)a[0], dt, M.vx[me]);
+                        vy = fma((double)a[1], dt, M.vy[me]);
+                        vz = fma((double)a[2], dt, M.vz[me]);
+                    }
+                }
+                __syncwarp();  // every lane's reads of the positions precede the drifts
+                if (is_slow || is_fast) {
+                    M.vx[me] = vx; M.vy[me] = vy; M.vz[me] = vz;
+                    if (PREC != HHS_PREC_FP64) mid::refresh_vel(M, me);
+                }
+                if (is_slow) {
+                    // second half drift (src/hold.cuh:158-159)
+                    if (PREC == HHS_PREC_FP64) {
+                        M.x[me] = f64_add(M.x[me], f64_mul(vx, h));
+                        M.y[me] = f64_add(M.y[me], f64_mul(vy, h));
+                        M.z[me] = f64_add(M.z[me], f64_mul(vz, h));
+                    } else {
+                        M.x[me] = fma(vx, h, M.x[me]);
+                        M.y[me] = fma(vy, h, M.y[me]);
+                        M.z[me] = fma(vz, h, M.z[me]);
+                        mid::refresh_pos(M, me);
+                    }
+                }
+                __syncwarp();
+            }
+            after2 |= bit;
+            if (F) {
+                dd++;
+                const unsigned long long cb = 1ull << dd;
+                calcm = (calcm & ~cb) | cb;
+                after1 &= ~cb; after2 &= ~cb;
+                continue;
+            }
+        }
+        calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
+        dd--;
+    }
+}
+
+template <int PREC>
+__device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, bool calc0,
+                         int dist_n, Smem& sm) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int cs = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    MidState& M = *reinterpret_cast<MidState*>(&sm.u);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const SoA& P = E.P;
+    const int nw = (n + 31) >> 5;
+    for (int k = tid; k < n; k += kEB) {
+        const int g = list_at(S, k);
+        M.g[k] = g;
+        M.x[k] = P.x[g]; M.y[k] = P.y[g]; M.z[k] = P.z[g];
+        M.vx[k] = P.vx[g]; M.vy[k] = P.vy[g]; M.vz[k] = P.vz[g];
+        M.m[k] = P.m[g]; M.ts[k] = P.ts[g];
+        if (PREC != HHS_PREC_FP64) { mid::refresh_pos(M, k); mid::refresh_vel(M, k); }
+    }
+    if (tid < kMidW)
+        M.allw[tid] = tid < nw ? (tid == nw - 1 && (n & 31) ? (1u << (n & 31)) - 1u : ~0u) : 0u;
+    if (tid == 0) M.nmem[0] = n;
+    __syncthreads();
+    // work counters of this subtree (thread 0; added to the context once, by CTA 0)
+    unsigned long long nodes = 0;
+    int maxl = 0;
+    double kpairs = 0.0, tpairs = 0.0, leaf = 0.0;
+    unsigned long long after1 = 0, after2 = 0, calcm = calc0 ? 1ull : 0ull;
+    int d = 0;
+    bool ok = true;
+    while (d >= 0) {
+        const int lvl = level0 + d;
+        const unsigned long long bit = 1ull << d;
+        const double dt = ldexp(E.dt_top, -lvl);
+        const unsigned* memw = d == 0 ? M.allw : M.fmask[d - 1];
+        if (!(after1 & bit)) {
+            if (lvl >= E.max_levels || lvl >= kMaxLevels - 1) {
+                if (tid == 0) atomicOr(E.err, HHS_ERRBIT_DEPTH);
+                ok = false;
+                break;
+            }
+            if (M.nmem[d] <= 32) {
+                // at most 32 members: the whole subtree on warp 0 of every CTA
+                if (warp == 0)
+                    warp_subtree<PREC>(E, M, memw, nw, M.nmem[d], lvl, (calcm & bit) != 0,
+                                       nodes, maxl, kpairs, tpairs, leaf, ok);
+                __syncthreads();
+                calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
+                d--;
+                continue;
+            }
+            if (calcm & bit) {
+                // ---- timesteps of the members (min over all other members)
+                const int nm = mid::compact(memw, nw, M.mem, M);
+                const bool dist = cs > 1 && nm > dist_n;
+                if (dist) cl.sync();
+                const mid::Share sh = mid::share_of(nm, dist, cs, rank);
+                const int items = sh.ng * sh.wpg;
+                for (int it = warp; it < items; it += kEB / 32) {
+                    const int grp = it / sh.wpg, part = it % sh.wpg;
+                    const int p = sh.s0 + grp * 32 + lane;
+                    const bool act = p < sh.s1;
+                    const int i = act ? M.mem[p] : 0;
+                    if (PREC == HHS_PREC_FP64) {
+                        double mv = 1.e30;
+                        if (act) {
+                            const double xi = M.x[i], yi = M.y[i], zi = M.z[i];
+                            const double vxi = M.vx[i], vyi = M.vy[i], vzi = M.vz[i], mi = M.m[i];
+#pragma unroll 1
+                            for (int q = part; q < nm; q += sh.wpg) {
+                                const int j = M.mem[q];
+                                if (j == i) continue;
+                                ts_pair_fp64(f64_sub(xi, M.x[j]), f64_sub(yi, M.y[j]),
+                                             f64_sub(zi, M.z[j]), f64_sub(vxi, M.vx[j]),
+                                             f64_sub(vyi, M.vy[j]), f64_sub(vzi, M.vz[j]), mi,
+                                             M.m[j], E.eta, E.eta_s2, mv);
+                            }
+                        }
+                        if (sh.wpg > 1) M.red.pmin[it][lane] = mv;
+                        else if (act) mid::put(&M.ts[i], mv, dist, cs);
+                    } else {
+                        const float mr = act ? mid::rate_over(E, M, M.mem, part, nm, sh.wpg, i) : 0.0f;
+                        if (sh.wpg > 1) {
+                            M.red.pmax[it][lane] = mr;
+                        } else if (act) {
+                            const double tv = 1.0 / (double)mr;
+                            mid::put(&M.ts[i], tv < 1.e30 ? tv : 1.e30, dist, cs);
+                        }
+                    }
+                }
+                if (sh.wpg > 1) {
+                    __syncthreads();
+                    const int t = tid;
+                    if (t < sh.s1 - sh.s0) {
+                        const int grp = t >> 5, l = t & 31;
+                        const int i = M.mem[sh.s0 + t];
+                        if (PREC == HHS_PREC_FP64) {
+                            double mv = 1.e30;
+                            for (int q = 0; q < sh.wpg; q++) {
+                                const double v = M.red.pmin[grp * sh.wpg + q][l];
+                                mv = v < mv ? v : mv;
+                            }
+                            mid::put(&M.ts[i], mv, dist, cs);
+                        } else {
+                            float mr = 0.0f;
+                            for (int q = 0; q < sh.wpg; q++) mr = fmaxf(mr, M.red.pmax[grp * sh.wpg + q][l]);
+                            const double tv = 1.0 / (double)mr;
+                            mid::put(&M.ts[i], tv < 1.e30 ? tv : 1.e30, dist, cs);
+                        }
+                    }
+                }
+                if (dist) cl.sync();
+                else __syncthreads();
+                if (tid == 0) tpairs += (double)nm * (double)(nm - 1);
+            }
+            // ---- split: fast = members with ts <= dt, N_fast == 1 folded into the slow set
+            int cnt = 0, mcnt = 0;
+            for (int w = warp; w < nw; w += kEB / 32) {
+                const unsigned mw = memw[w];
+                const bool in = (mw >> lane) & 1u;
+                const unsigned f = __ballot_sync(HHS_FULL_MASK, in && M.ts[w * 32 + lane] <= dt);
+                if (lane == 0) M.fmask[d][w] = f;
+                cnt += __popc(f);
+                mcnt += __popc(mw);
+            }
+            if (tid >= nw && tid < kMidW) M.fmask[d][tid] = 0u;
+            if (lane == 0) M.wcnt[warp] = cnt | (mcnt << 16);
+            __syncthreads();
+            int nf = 0, nm = 0;
+#pragma unroll
+            for (int w = 0; w < kEB / 32; w++) {
+                nf += M.wcnt[w] & 0xffff;
+                nm += M.wcnt[w] >> 16;
+            }
+            int lone = -1;
+            if (nf == 1) {
+                for (int w = 0; w < nw; w++)
+                    if (M.fmask[d][w]) lone = w * 32 + __ffs(M.fmask[d][w]) - 1;
+                nf = 0;
+            }
+            if (tid == 0) {
+                M.lone[d] = lone;
+                if (nf > 0) M.nmem[d + 1] = nf;
+                const double ns = (double)(nm - nf), nfd = (double)nf;
+                nodes++;
+                maxl = max(maxl, lvl);
+                kpairs += ns * (ns - 1.0) + 2.0 * nfd * ns;
+                if (nf == 0) leaf += dt;
+            }
+            __syncthreads();  // everyone has read fmask[d] before the fold clears it
+            if (lone >= 0 && tid == 0) M.fmask[d][lone >> 5] = 0u;
+            after1 |= bit;
+            if (nf > 0) {
+                d++;
+                const unsigned long long cb = 1ull << d;
+                calcm &= ~cb; after1 &= ~cb; after2 &= ~cb;
+                continue;
+            }
+            __syncthreads();
+        }
+        if (!(after2 & bit)) {
+            // ---- kick order: slow slots (stable, lone last), then fast slots
+            int nf = 0;
+            const int ns = mid::kick_order(memw, M.fmask[d], M.lone[d], nw, M.kl, M, &nf);
+            const int nk = ns + nf;
+            const double h = dt * 0.5;
+            if (ns > 0) {
+                // first half drift of the slow slots (src/hold.cuh:123-124), every replica
+                for (int p = tid; p < ns; p += kEB) {
+                    const int k = M.kl[p];
+                    if (PREC == HHS_PREC_FP64) {
+                        M.x[k] = f64_add(M.x[k], f64_mul(M.vx[k], h));
+                        M.y[k] = f64_add(M.y[k], f64_mul(M.vy[k], h));
+                        M.z[k] = f64_add(M.z[k], f64_mul(M.vz[k], h));
+                    } else {
+                        M.x[k] = fma(M.vx[k], h, M.x[k]);
+                        M.y[k] = fma(M.vy[k], h, M.y[k]);
+                        M.z[k] = fma(M.vz[k], h, M.z[k]);
+                        mid::refresh_pos(M, k);
+                    }
+                }
+                // ---- kicks (src/hold.cuh:138-143): slow sinks from slow + fast sources,
+                // fast sinks from slow sources
+                const bool dist = cs > 1 && nk > dist_n;
+                if (dist) cl.sync();
+                else __syncthreads();
+                const mid::Share sh = mid::share_of(nk, dist, cs, rank);
+                if (PREC == HHS_PREC_FP64) {
+                    // one thread per sink, sources in the reference's order
+                    for (int p = sh.s0 + tid; p < sh.s1; p += kEB) {
+                        const int i = M.kl[p];
+                        const bool slow = p < ns;
+                        const double xi = M.x[i], yi = M.y[i], zi = M.z[i];
+                        double aL[3] = {0, 0, 0}, aF[3] = {0, 0, 0};
+#pragma unroll 1
+                        for (int q = 0; q < ns; q++) {
+                            const int j = M.kl[q];
+                            kick_pair_fp64(f64_sub(M.x[j], xi), f64_sub(M.y[j], yi),
+                                           f64_sub(M.z[j], zi), M.m[j], aL[0], aL[1], aL[2],
+                                           E.eps2);
+                        }
+                        if (slow) {
+#pragma unroll 1
+                            for (int q = ns; q < nk; q++) {
+                                const int j = M.kl[q];
+                                kick_pair_fp64(f64_sub(M.x[j], xi), f64_sub(M.y[j], yi),
+                                               f64_sub(M.z[j], zi), M.m[j], aF[0], aF[1],
+                                               aF[2], E.eps2);
+                            }
+                        }
+                        double vx = f64_add(M.vx[i], f64_mul(aL[0], dt));
+                        double vy = f64_add(M.vy[i], f64_mul(aL[1], dt));
+                        double vz = f64_add(M.vz[i], f64_mul(aL[2], dt));
+                        if (slow && nf > 0) {
+                            vx = f64_add(vx, f64_mul(aF[0], dt));
+                            vy = f64_add(vy, f64_mul(aF[1], dt));
+                            vz = f64_add(vz, f64_mul(aF[2], dt));
+                        }
+                        mid::put(&M.vx[i], vx, dist, cs);
+                        mid::put(&M.vy[i], vy, dist, cs);
+                        mid::put(&M.vz[i], vz, dist, cs);
+                    }
+                } else {
+                    const int items = sh.ng * sh.wpg;
+                    for (int it = warp; it < items; it += kEB / 32) {
+                        const int grp = it / sh.wpg, part = it % sh.wpg;
+                        const int p = sh.s0 + grp * 32 + lane;
+                        const bool act = p < sh.s1;
+                        const int i = act ? M.kl[p] : 0;
+                        float a[3] = {0, 0, 0};
+                        if (act) mid::acc_over(E, M, M.kl, part, p < ns ? nk : ns, sh.wpg, i, a);
+                        if (sh.wpg > 1) {
+                            M.red.part[it][0][lane] = a[0];
+                            M.red.part[it][1][lane] = a[1];
+                            M.red.part[it][2][lane] = a[2];
+                        } else if (act) {
+                            mid::put(&M.vx[i], fma((double)a[0], dt, M.vx[i]), dist, cs);
+                            mid::put(&M.vy[i], fma((double)a[1], dt, M.vy[i]), dist, cs);
+                            mid::put(&M.vz[i], fma((double)a[2], dt, M.vz[i]), dist, cs);
+                        }
+                    }
+                    if (sh.wpg > 1) {
+                        __syncthreads();
+                        const int t = tid;
+                        if (t < sh.s1 - sh.s0) {
+                            const int grp = t >> 5, l = t & 31;
+                            const int i = M.kl[sh.s0 + t];
+                            double acc[3] = {0, 0, 0};
+                            for (int q = 0; q < sh.wpg; q++)
+#pragma unroll
+                                for (int c = 0; c < 3; c++)
+                                    acc[c] += (double)M.red.part[grp * sh.wpg + q][c][l];
+                            mid::put(&M.vx[i], fma(acc[0], dt, M.vx[i]), dist, cs);
+                            mid::put(&M.vy[i], fma(acc[1], dt, M.vy[i]), dist, cs);
+                            mid::put(&M.vz[i], fma(acc[2], dt, M.vz[i]), dist, cs);
+                        }
+                    }
+                }
+                if (dist) cl.sync();
+                else __syncthreads();
+                // second half drift of the slow slots (src/hold.cuh:158-159), every replica
+                for (int p = tid; p < nk; p += kEB) {
+                    const int k = M.kl[p];
+                    if (p < ns) {
+                        if (PREC == HHS_PREC_FP64) {
+                            M.x[k] = f64_add(M.x[k], f64_mul(M.vx[k], h));
+                            M.y[k] = f64_add(M.y[k], f64_mul(M.vy[k], h));
+                            M.z[k] = f64_add(M.z[k], f64_mul(M.vz[k], h));
+                        } else {
+                            M.x[k] = fma(M.vx[k], h, M.x[k]);
+                            M.y[k] = fma(M.vy[k], h, M.y[k]);
+                            M.z[k] = fma(M.vz[k], h, M.z[k]);
+                            mid::refresh_pos(M, k);
+                        }
+                    }
+                    if (PREC != HHS_PREC_FP64) mid::refresh_vel(M, k);
+                }
+                __syncthreads();
+            }
+            after2 |= bit;
+            if (nf > 0) {
+                d++;
+                const unsigned long long cb = 1ull << d;
+                calcm = (calcm & ~cb) | cb;
+                after1 &= ~cb; after2 &= ~cb;
+                continue;
+            }
+        }
+        calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
+        d--;
+    }
+    // write back this CTA's share of the slots; work counters once per subtree
+    for (int k = rank + cs * tid; k < n; k += cs * kEB) {
+        const int g = M.g[k];
+        P.x[g] = M.x[k]; P.y[g] = M.y[k]; P.z[g] = M.z[k];
+        P.vx[g] = M.vx[k]; P.vy[g] = M.vy[k]; P.vz[g] = M.vz[k];
+        P.ts[g] = M.ts[k];
+    }
+    if (ok && rank == 0 && tid == 0 && nodes) {
+        *E.leaf_time += leaf;
+        atomicAdd(reinterpret_cast<unsigned long long*>(&E.stats->nodes), nodes);
+        atomicMax(&E.stats->max_level, maxl);
+        atomicAdd(&E.stats->kick_pairs, kpairs);
+        atomicAdd(&E.stats->ts_pairs, tpairs);
+    }
+    if (cs > 1) cl.sync();
+    else __syncthreads();
+}
+
 // ---------------------------------------------------------------- the recursion
 // Walks the HOLD recursion from `top` (whose subsystem is already defined by the
 // counts/lists above it). Grid and cluster modes delegate nodes with n <= small_n,
@@ -1086,6 +1831,18 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                 if (threadIdx.x == 0) atomicOr(E.err, HHS_ERRBIT_DEPTH);
                 return false;
             }
+            if constexpr (MODE == kModeGrid) {
+                if (n <= E.mid_n && n <= kMid) {
+                    // the whole subtree on the first cluster (or CTA 0), from shared memory
+                    const int cs = (int)cooperative_groups::this_cluster().num_blocks();
+                    if ((int)blockIdx.x < cs) mid_hold<PREC>(E, S, n, lvl, calc, E.mid_dist_n, sm);
+                    if (!phase_barrier(E, sm, W)) return false;
+                    prof_mark(E, W, t_last, kProfCluster, 0.0, sm, lvl);
+                    calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
+                    lvl--;
+                    continue;
+                }
+            }
             if (n <= E.warp_n) {
                 if (W.id == 0) tiny_hold<PREC>(E, S, n, lvl, calc, sm);
                 if (!phase_barrier(E, sm, W)) return false;
@@ -1093,22 +1850,6 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                 calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
                 lvl--;
                 continue;
-            }
-            if (MODE == kModeGrid && n <= E.mid_n && n > E.small_n) {
-                namespace cg = cooperative_groups;
-                const int cs = (int)cg::this_cluster().num_blocks();
-                if (cs > 1) {
-                    if ((int)blockIdx.x < cs) {
-                        const Workers cw{(int)cg::this_cluster().block_rank(), cs, kModeCluster};
-                        unsigned long long t_sub = 0;
-                        run_hold<PREC, kModeCluster>(E, lvl, calc, cw, sm, t_sub);
-                    }
-                    if (!phase_barrier(E, sm, W)) return false;
-                    prof_mark(E, W, t_last, kProfCluster, 0.0, sm, lvl);
-                    calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
-                    lvl--;
-                    continue;
-                }
             }
             if (MODE != kModeBlock && n <= E.small_n) {
                 if (W.id == 0) {
@@ -1204,7 +1945,8 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
 
 template <int PREC>
 __global__ void __launch_bounds__(kEB, 2) k_engine(EParams E) {
-    __shared__ Smem sm;
+    extern __shared__ __align__(16) unsigned char engine_smem[];
+    Smem& sm = *reinterpret_cast<Smem*>(engine_smem);
     const Workers W{(int)blockIdx.x, (int)gridDim.x, kModeGrid};
     unsigned long long t_last = 0;
     prof_begin(E, sm);
@@ -1305,8 +2047,9 @@ struct EngineHost {
     int small_n = 64;
     int units_per_cta = 16;
     int warp_n = 32;
-    int cluster_size = 1;
-    int mid_n = 0;
+    int cluster_size = 2;
+    int mid_n = 640;
+    int mid_dist_n = 96;
     int packed = 0;
     EngineState* st = nullptr;
     double* ts_part = nullptr;
@@ -1346,8 +2089,14 @@ hhs_status engine_init(hhs_ctx* c, void* base) {
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
     if (!coop) { delete eh; return HHS_ERR_CUDA; }
     int b0 = 0, b1 = 0;
-    HHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_engine<HHS_PREC_FP64>, kEB, 0));
-    HHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_engine<HHS_PREC_MIXED>, kEB, 0));
+    HHS_CUDA_TRY(cudaFuncSetAttribute(k_engine<HHS_PREC_FP64>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEngineSmem));
+    HHS_CUDA_TRY(cudaFuncSetAttribute(k_engine<HHS_PREC_MIXED>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEngineSmem));
+    HHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_engine<HHS_PREC_FP64>, kEB,
+                                                               kEngineSmem));
+    HHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_engine<HHS_PREC_MIXED>, kEB,
+                                                               kEngineSmem));
     eh->sms = sms;
     eh->occ[0] = b0;
     eh->occ[1] = b1;
@@ -1355,6 +2104,14 @@ hhs_status engine_init(hhs_ctx* c, void* base) {
     eh->grid[1] = sms * (b1 < 2 ? b1 : 2);
     if (eh->grid[0] <= 0 || eh->grid[1] <= 0) { delete eh; return HHS_ERR_CUDA; }
     c->engine_host = eh;
+    // size the grid for the default tuning (thread-block clusters included); without
+    // cluster occupancy fall back to plain CTAs
+    hhs_tuning t{};
+    engine_get_tuning(c, &t);
+    if (engine_set_tuning(c, t) != HHS_OK) {
+        t.cluster_size = 1;
+        if (engine_set_tuning(c, t) != HHS_OK) { engine_destroy(c); return HHS_ERR_CUDA; }
+    }
     return HHS_OK;
 }
 
@@ -1368,11 +2125,12 @@ hhs_status engine_set_tuning(hhs_ctx* c, const hhs_tuning& t) {
     if (!eh || t.small_n < 0 || t.units_per_cta < 1 || t.units_per_cta > 64 ||
         t.ctas_per_sm < 1 || t.ctas_per_sm > 2 || t.warp_n < 0 || t.warp_n > 32 ||
         !(t.cluster_size == 1 || t.cluster_size == 2 || t.cluster_size == 4 ||
-          t.cluster_size == 8) || t.mid_n < 0)
+          t.cluster_size == 8) || t.mid_n < 0 || t.mid_dist_n < 0)
         return HHS_ERR_INVALID_ARG;
     eh->warp_n = t.warp_n;
     eh->cluster_size = t.cluster_size;
     eh->mid_n = t.mid_n;
+    eh->mid_dist_n = t.mid_dist_n;
     eh->packed = t.packed != 0;
     eh->small_n = t.small_n;
     eh->units_per_cta = t.units_per_cta;
@@ -1384,6 +2142,7 @@ hhs_status engine_set_tuning(hhs_ctx* c, const hhs_tuning& t) {
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(t.cluster_size, 1, 1);
             cfg.blockDim = dim3(kEB, 1, 1);
+            cfg.dynamicSmemBytes = kEngineSmem;
             cudaLaunchAttribute at[1];
             at[0].id = cudaLaunchAttributeClusterDimension;
             at[0].val.clusterDim.x = t.cluster_size;
@@ -1403,6 +2162,14 @@ hhs_status engine_set_tuning(hhs_ctx* c, const hhs_tuning& t) {
     return HHS_OK;
 }
 
+hhs_status engine_get_launch(hhs_ctx* c, int32_t* grid, int32_t* smem_bytes) {
+    auto* eh = static_cast<EngineHost*>(c->engine_host);
+    if (!eh) return HHS_ERR_INVALID_ARG;
+    if (grid) { grid[0] = eh->grid[0]; grid[1] = eh->grid[1]; }
+    if (smem_bytes) *smem_bytes = (int32_t)kEngineSmem;
+    return HHS_OK;
+}
+
 hhs_status engine_get_tuning(hhs_ctx* c, hhs_tuning* t) {
     auto* eh = static_cast<EngineHost*>(c->engine_host);
     if (!eh || !t) return HHS_ERR_INVALID_ARG;
@@ -1412,6 +2179,7 @@ hhs_status engine_get_tuning(hhs_ctx* c, hhs_tuning* t) {
     t->warp_n = eh->warp_n;
     t->cluster_size = eh->cluster_size;
     t->mid_n = eh->mid_n;
+    t->mid_dist_n = eh->mid_dist_n;
     t->packed = eh->packed;
     return HHS_OK;
 }
@@ -1467,6 +2235,7 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
     E.units_per_cta = eh->units_per_cta;
     E.warp_n = eh->warp_n;
     E.mid_n = eh->mid_n;
+    E.mid_dist_n = eh->mid_dist_n;
     E.packed = eh->packed;
     E.calc_top = calc_ts ? 1 : 0;
     E.profile = profile ? 1 : 0;
@@ -1492,6 +2261,7 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(eh->grid[pi], 1, 1);
     cfg.blockDim = dim3(kEB, 1, 1);
+    cfg.dynamicSmemBytes = kEngineSmem;
     cfg.stream = stream;
     cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeCooperative;
@@ -1677,6 +2447,7 @@ extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, d
     E.units_per_cta = b->units_per_cta;
     E.warp_n = b->warp_n;
     E.mid_n = 0;
+    E.mid_dist_n = 0;
     E.packed = b->packed;
     E.dt_top = dt;
     E.eta = b->params.eta;

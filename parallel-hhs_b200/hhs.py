@@ -63,7 +63,7 @@ class Tuning(ctypes.Structure):
     _fields_ = [("small_n", ctypes.c_int32), ("units_per_cta", ctypes.c_int32),
                 ("ctas_per_sm", ctypes.c_int32), ("warp_n", ctypes.c_int32),
                 ("cluster_size", ctypes.c_int32), ("mid_n", ctypes.c_int32),
-                ("packed", ctypes.c_int32), ("_reserved", ctypes.c_int32),
+                ("packed", ctypes.c_int32), ("mid_dist_n", ctypes.c_int32),
                 ("ms_per_step", ctypes.c_double)]
 
 
@@ -164,6 +164,7 @@ SIGNATURES = {
                                 ctypes.c_int32, ctypes.c_char_p, ctypes.POINTER(RunLog), _vp]),
     "hhs_ctx_set_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(Tuning)]),
     "hhs_ctx_get_tuning": (ctypes.c_int, [_vp, ctypes.POINTER(Tuning)]),
+    "hhs_ctx_get_launch": (ctypes.c_int, [_vp, _ip, _ip]),
     "hhs_ctx_autotune": (ctypes.c_int, [_vp, ctypes.POINTER(CParticleSystem), ctypes.c_int32,
                                         ctypes.c_double, ctypes.c_int, ctypes.POINTER(Tuning),
                                         _vp]),
@@ -293,7 +294,7 @@ class Context:
         _check(lib().hhs_ctx_reset_stats(self.h, stream), "reset_stats")
 
     def set_tuning(self, small_n=None, units_per_cta=None, ctas_per_sm=None, warp_n=None,
-                   cluster_size=None, mid_n=None, packed=None):
+                   cluster_size=None, mid_n=None, packed=None, mid_dist_n=None):
         t = Tuning()
         _check(lib().hhs_ctx_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
         if small_n is not None:
@@ -310,6 +311,8 @@ class Context:
             t.mid_n = mid_n
         if packed is not None:
             t.packed = int(packed)
+        if mid_dist_n is not None:
+            t.mid_dist_n = mid_dist_n
         _check(lib().hhs_ctx_set_tuning(self.h, ctypes.byref(t)), "set_tuning")
 
     def tuning(self):
@@ -317,7 +320,15 @@ class Context:
         _check(lib().hhs_ctx_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
         return {"small_n": t.small_n, "units_per_cta": t.units_per_cta,
                 "ctas_per_sm": t.ctas_per_sm, "warp_n": t.warp_n,
-                "cluster_size": t.cluster_size, "mid_n": t.mid_n, "packed": t.packed}
+                "cluster_size": t.cluster_size, "mid_n": t.mid_n, "packed": t.packed,
+                "mid_dist_n": t.mid_dist_n}
+
+    def launch(self):
+        """(grid CTAs for FP64, grid CTAs for mixed, dynamic shared memory bytes per CTA)."""
+        g = np.zeros(2, dtype=np.int32)
+        sm = ctypes.c_int32()
+        _check(lib().hhs_ctx_get_launch(self.h, _i(g), ctypes.byref(sm)), "get_launch")
+        return int(g[0]), int(g[1]), sm.value
 
     def autotune(self, sys, n, dt, prec=1, stream=None):
         t = Tuning()
@@ -326,7 +337,7 @@ class Context:
         return {"small_n": t.small_n, "units_per_cta": t.units_per_cta,
                 "ctas_per_sm": t.ctas_per_sm, "warp_n": t.warp_n,
                 "cluster_size": t.cluster_size, "mid_n": t.mid_n, "packed": t.packed,
-                "ms_per_step": t.ms_per_step}
+                "mid_dist_n": t.mid_dist_n, "ms_per_step": t.ms_per_step}
 
     def set_profiling(self, on):
         _check(lib().hhs_ctx_set_profiling(self.h, int(on)), "set_profiling")

@@ -17,15 +17,16 @@ def _copy(s):
 
 
 # ------------------------------------------------------------------------------ softening
-@pytest.mark.parametrize("schedule,n,small_n", [("host", 300, 0), ("engine", 300, 0),
-                                                ("engine", 2048, 256),
-                                                ("engine", 300, 100000)])
-def test_softened_hold_fp64_bit_exact(cuda, hhs, oracle, schedule, n, small_n):
+@pytest.mark.parametrize("schedule,n,small_n,mid_n", [("host", 300, 0, 0), ("engine", 300, 0, 0),
+                                                      ("engine", 2048, 256, 0),
+                                                      ("engine", 300, 100000, 0),
+                                                      ("engine", 2048, 64, 640)])
+def test_softened_hold_fp64_bit_exact(cuda, hhs, oracle, schedule, n, small_n, mid_n):
     """With eps > 0 every kick uses d2 + eps^2; both schedules stay bit-exact."""
     s = hhs.plummer(n, 90 + n)
     ref = _copy(s)
     ctx = hhs.Context(n, 64, eta=0.03, eps=EPS)
-    ctx.set_tuning(small_n)
+    ctx.set_tuning(small_n, mid_n=mid_n)
     d = hhs.ParticleSystem(n)
     d.upload(s)
     dt = 1.0 / 64

@@ -374,7 +374,7 @@ def test_hold_step_engine_fp64_bit_exact(cuda, hhs, oracle, n, small_n, spectrum
     s = _plummer(hhs, n, 20 + n, spectrum)
     ref = {k: v.copy() for k, v in s.items()}
     ctx = hhs.Context(n, 64, eta=0.03)
-    ctx.set_tuning(small_n)
+    ctx.set_tuning(small_n, cluster_size=1, mid_n=0)  # grid, block and tiny paths only
     d = hhs.ParticleSystem(n)
     d.upload(s)
     dt = 1.0 / 64
@@ -401,7 +401,7 @@ def test_hold_step_engine_mixed_close(cuda, hhs, oracle, n, small_n, packed):
     s = _plummer(hhs, n, 30 + n)
     ref = {k: v.copy() for k, v in s.items()}
     ctx = hhs.Context(n, 64, eta=0.03)
-    ctx.set_tuning(small_n, packed=packed)
+    ctx.set_tuning(small_n, packed=packed, cluster_size=1, mid_n=0)
     d = hhs.ParticleSystem(n)
     d.upload(s)
     e0 = hhs.energy_host(s)
@@ -501,7 +501,7 @@ def test_engine_warp_solver_fp64_bit_exact(cuda, hhs, oracle, warp_n, small_n):
     s = _plummer(hhs, n, 55)
     ref = {k: v.copy() for k, v in s.items()}
     ctx = hhs.Context(n, 64, eta=0.03)
-    ctx.set_tuning(small_n=small_n, warp_n=warp_n)
+    ctx.set_tuning(small_n=small_n, warp_n=warp_n, cluster_size=1, mid_n=0)
     d = hhs.ParticleSystem(n)
     d.upload(s)
     nodes = 0
@@ -569,3 +569,56 @@ def test_hold_integrate_graph_matches_steps(cuda, hhs, oracle):
     out = d.download()
     for k in FIELDS:
         assert np.array_equal(out[k], ref[k]), k
+
+
+# ------------------------------------------------------------------------------ cluster solver
+@pytest.mark.parametrize("n,cs,mid_n,dist_n,spectrum", [
+    (2, 1, 640, 96, 0), (24, 8, 640, 96, 0), (33, 2, 640, 0, 0),
+    (300, 1, 640, 96, 0), (300, 2, 640, 16, 0), (300, 8, 640, 16, 0), (640, 4, 640, 0, 1),
+    (2048, 8, 640, 96, 0), (2048, 8, 256, 32, 1), (5000, 4, 640, 64, 0)])
+def test_hold_step_cluster_solver_fp64_bit_exact(cuda, hhs, oracle, n, cs, mid_n, dist_n,
+                                                 spectrum):
+    """Subtrees of at most mid_n particles solved from shared memory on one thread-block
+    cluster (cs CTAs; pair work spread over the cluster above dist_n members, nodes of up
+    to 32 members on one warp) reproduce the oracle bit for bit, with its work counters."""
+    s = _plummer(hhs, n, 40 + n, spectrum)
+    ref = {k: v.copy() for k, v in s.items()}
+    ctx = hhs.Context(n, 64, eta=0.03)
+    ctx.set_tuning(64, cluster_size=cs, mid_n=mid_n, mid_dist_n=dist_n)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    dt = 1.0 / 64
+    leaf, nodes, kp, tp = 0.0, 0, 0.0, 0.0
+    for _ in range(2):
+        hhs.hold_step(ctx, d, n, 0.0, dt, True, hhs.PREC_FP64)
+        tr, _ = oracle.hold_step(ref, dt, True, 0.03)
+        leaf += tr.leaf_time
+        nodes += tr.count
+        kp += tr.kick_pairs
+        tp += tr.ts_pairs
+    ctx.check()
+    out = d.download()
+    for k in FIELDS:
+        assert np.array_equal(out[k], ref[k]), k
+    st = ctx.stats()
+    assert st["nodes"] == nodes and st["kick_pairs"] == kp and st["ts_pairs"] == tp
+    assert ctx.simtime() == pytest.approx(leaf, rel=1e-15)
+
+
+@pytest.mark.parametrize("cs,dist_n", [(1, 96), (8, 32), (8, 96)])
+def test_hold_step_cluster_solver_mixed_close(cuda, hhs, oracle, cs, dist_n):
+    n = 4096
+    s = _plummer(hhs, n, 44)
+    ref = {k: v.copy() for k, v in s.items()}
+    ctx = hhs.Context(n, 64, eta=0.03, eps=0.001)
+    ctx.set_tuning(64, cluster_size=cs, mid_n=640, mid_dist_n=dist_n)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    e0 = hhs.energy_host(s)
+    hhs.hold_step(ctx, d, n, 0.0, 1.0 / 64, True, hhs.PREC_MIXED)
+    ctx.check()
+    out = d.download()
+    oracle.hold_step(ref, 1.0 / 64, True, 0.03, eps=0.001)
+    dx = max(np.abs(out[k] - ref[k]).max() for k in ("x", "y", "z"))
+    assert dx < 1e-7, dx
+    assert abs((hhs.energy_host(out) - hhs.energy_host(ref)) / e0) < 1e-8
