@@ -1876,11 +1876,22 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                                       nullptr, sm);
                     }
                 } else {
+                    // only units with a pair j > i: row block rb takes column blocks
+                    // cb >= rb * kEB / kCB; the workers stride through that triangle
                     const int nrb = (n + kEB - 1) / kEB, ncb = (n + kCB - 1) / kCB;
-                    for (int u = W.id; u < nrb * ncb; u += W.count) {
-                        const int rb = u / ncb, cb = u % ncb;
-                        if ((cb + 1) * kCB <= rb * kEB + 1) continue;  // no pair with j > i
-                        ts_sym_unit(E, S, n, rb, cb, sm);
+                    constexpr int kRowStep = kEB / kCB;
+                    int rb = 0, off = W.id;  // unit = (rb, rb * kRowStep + off)
+                    while (rb < nrb && off >= ncb - rb * kRowStep) {
+                        off -= ncb - rb * kRowStep;
+                        rb++;
+                    }
+                    while (rb < nrb) {
+                        ts_sym_unit(E, S, n, rb, rb * kRowStep + off, sm);
+                        off += W.count;
+                        while (rb < nrb && off >= ncb - rb * kRowStep) {
+                            off -= ncb - rb * kRowStep;
+                            rb++;
+                        }
                     }
                 }
                 if (!phase_barrier(E, sm, W)) return false;
@@ -1913,11 +1924,22 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                 const int C = (ntot + nch - 1) / nch;
                 const int nsb = (ntot + blk - 1) / blk;
                 const double h = dt * 0.5;
-                for (int u = W.id; u < nsb * nch; u += W.count) {
-                    const int ib = u / nch, jc = u % nch;
+                // blocks of fast sinks only need the slow-source chunks: the work units
+                // are the first nfb blocks x jcs chunks, then the other blocks x nch
+                const int nfb = nf / blk;
+                const int jcs = min(nch, (ns + C - 1) / C);
+                const int uf = nfb * jcs;
+                const int units = uf + (nsb - nfb) * nch;
+                for (int u = W.id; u < units; u += W.count) {
+                    int ib, jc;
+                    if (u < uf) {
+                        ib = u / jcs;
+                        jc = u % jcs;
+                    } else {
+                        ib = nfb + (u - uf) / nch;
+                        jc = (u - uf) % nch;
+                    }
                     const int j0 = jc * C, j1 = min(ntot, j0 + C);
-                    // blocks of fast sinks only need slow-source chunks
-                    if ((ib + 1) * blk <= nf && j0 >= ns) continue;
                     if (x2) kick_unit_x2(E, F, L, nf, ns, h, ib, jc, j0, j1, sm);
                     else kick_unit<PREC>(E, F, L, nf, ns, h, ib, jc, j0, j1, sm);
                 }
