@@ -283,6 +283,10 @@ hhs_status hhs_batch_destroy(hhs_batch* b);
  * system, nodes with at most small_n particles run on one CTA; units_per_cta as above. */
 hhs_status hhs_batch_set_tuning(hhs_batch* b, int32_t big_n, int32_t small_n,
                                 int32_t units_per_cta);
+/* Subtrees of at most mid_n (<= 640) particles run from shared memory: on the system's
+ * cluster for large systems (nodes above mid_dist_n spread over its CTAs), on one CTA for
+ * the others (default 640 and 96; mid_n = 0 turns it off). */
+hhs_status hhs_batch_set_mid(hhs_batch* b, int32_t mid_n, int32_t mid_dist_n);
 hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, double dt,
                             int32_t calc_timestep, hhs_precision prec, void* stream);
 hhs_status hhs_batch_get_simtime(hhs_batch* b, double* per_system, void* stream);

@@ -1500,12 +1500,13 @@ __device__ void warp_subtree(const EParams& E, MidState& M, const unsigned* memw
     }
 }
 
+// cs, rank: the hardware cluster that runs the subtree (every CTA of it calls mid_hold),
+// or cs = 1 for one CTA alone whatever cluster it belongs to.
 template <int PREC>
 __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, bool calc0,
-                         int dist_n, Smem& sm) {
+                         int dist_n, int cs, int rank, Smem& sm) {
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
-    const int cs = (int)cl.num_blocks(), rank = (int)cl.block_rank();
     MidState& M = *reinterpret_cast<MidState*>(&sm.u);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const SoA& P = E.P;
@@ -1831,17 +1832,23 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                 if (threadIdx.x == 0) atomicOr(E.err, HHS_ERRBIT_DEPTH);
                 return false;
             }
-            if constexpr (MODE == kModeGrid) {
-                if (n <= E.mid_n && n <= kMid) {
-                    // the whole subtree on the first cluster (or CTA 0), from shared memory
-                    const int cs = (int)cooperative_groups::this_cluster().num_blocks();
-                    if ((int)blockIdx.x < cs) mid_hold<PREC>(E, S, n, lvl, calc, E.mid_dist_n, sm);
-                    if (!phase_barrier(E, sm, W)) return false;
-                    prof_mark(E, W, t_last, kProfCluster, 0.0, sm, lvl);
-                    calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
-                    lvl--;
-                    continue;
+            if (n <= E.mid_n && n <= kMid) {
+                // the whole subtree from shared memory: on the grid's first cluster (or
+                // CTA 0), on this hardware cluster, or on this CTA alone
+                if constexpr (MODE == kModeGrid) {
+                    namespace cg = cooperative_groups;
+                    const int cs = (int)cg::this_cluster().num_blocks();
+                    if ((int)blockIdx.x < cs)
+                        mid_hold<PREC>(E, S, n, lvl, calc, E.mid_dist_n, cs,
+                                       (int)cg::this_cluster().block_rank(), sm);
+                } else {
+                    mid_hold<PREC>(E, S, n, lvl, calc, E.mid_dist_n, W.count, W.id, sm);
                 }
+                if (!phase_barrier(E, sm, W)) return false;
+                prof_mark(E, W, t_last, kProfCluster, 0.0, sm, lvl);
+                calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
+                lvl--;
+                continue;
             }
             if (n <= E.warp_n) {
                 if (W.id == 0) tiny_hold<PREC>(E, S, n, lvl, calc, sm);
@@ -2028,7 +2035,8 @@ __device__ __forceinline__ EParams system_params(const BParams& B, int sys, cons
 
 template <int PREC>
 __global__ void __launch_bounds__(kEB, 2) k_batched(BParams B) {
-    __shared__ Smem sm;
+    extern __shared__ __align__(16) unsigned char batched_smem[];
+    Smem& sm = *reinterpret_cast<Smem*>(batched_smem);
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
     const int cs = (int)cluster.num_blocks();
@@ -2309,6 +2317,7 @@ struct hhs_batch {
     int n_sys = 0, n_total = 0, n_max_sys = 0, max_levels = 0;
     hhs_params params{0.03, 0.0};
     int big_n = 1024, cluster_size = 8, small_n = 64, units_per_cta = 8, warp_n = 32, packed = 0;
+    int mid_n = kMid, mid_dist_n = 96;
     int n_big = 0, n_clusters[2] = {0, 0};
     void* arena = nullptr;
     int32_t* d_offsets = nullptr;
@@ -2328,9 +2337,13 @@ struct hhs_batch {
 namespace {
 template <int PREC>
 cudaError_t batched_occupancy(int cs, int* clusters) {
+    cudaError_t e = cudaFuncSetAttribute(k_batched<PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kEngineSmem);
+    if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(cs, 1, 1);
     cfg.blockDim = dim3(kEB, 1, 1);
+    cfg.dynamicSmemBytes = kEngineSmem;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = cs;
@@ -2447,6 +2460,13 @@ extern "C" hhs_status hhs_batch_set_tuning(hhs_batch* b, int32_t big_n, int32_t 
     return HHS_OK;
 }
 
+extern "C" hhs_status hhs_batch_set_mid(hhs_batch* b, int32_t mid_n, int32_t mid_dist_n) {
+    if (!b || mid_n < 0 || mid_dist_n < 0) return HHS_ERR_INVALID_ARG;
+    b->mid_n = mid_n;
+    b->mid_dist_n = mid_dist_n;
+    return HHS_OK;
+}
+
 extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, double dt,
                                        int32_t calc_timestep, hhs_precision prec, void* stream) {
     if (!b || !sys || !sys->_base || !(dt > 0.0)) return HHS_ERR_INVALID_ARG;
@@ -2468,8 +2488,8 @@ extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, d
     E.profile = 0;
     E.units_per_cta = b->units_per_cta;
     E.warp_n = b->warp_n;
-    E.mid_n = 0;
-    E.mid_dist_n = 0;
+    E.mid_n = b->mid_n;
+    E.mid_dist_n = b->mid_dist_n;
     E.packed = b->packed;
     E.dt_top = dt;
     E.eta = b->params.eta;
@@ -2502,6 +2522,7 @@ extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, d
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(nclu * b->cluster_size, 1, 1);
     cfg.blockDim = dim3(kEB, 1, 1);
+    cfg.dynamicSmemBytes = kEngineSmem;
     cfg.stream = s;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeClusterDimension;

@@ -151,6 +151,7 @@ SIGNATURES = {
     "hhs_batch_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(Stats), _vp]),
     "hhs_batch_reset_stats": (ctypes.c_int, [_vp, _vp]),
     "hhs_batch_check": (ctypes.c_int, [_vp, _vp]),
+    "hhs_batch_set_mid": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32]),
     "hhs_batch_partition": (ctypes.c_int, [ctypes.c_int32, _ip, ctypes.c_int32, _ip, _dp]),
     "hhs_energy": (ctypes.c_int, [ctypes.POINTER(CParticleSystem), ctypes.c_int32, ctypes.c_double,
                                   _dp, _dp, _vp]),
@@ -398,6 +399,9 @@ class Batch:
 
     def set_tuning(self, big_n=1024, small_n=64, units_per_cta=8):
         _check(lib().hhs_batch_set_tuning(self.h, big_n, small_n, units_per_cta), "batch tuning")
+
+    def set_mid(self, mid_n=640, mid_dist_n=96):
+        _check(lib().hhs_batch_set_mid(self.h, mid_n, mid_dist_n), "batch set_mid")
 
     def step(self, sys, dt, calc_timestep=True, prec=PREC_MIXED, stream=None):
         _check(lib().hhs_hold_batched(self.h, sys.ref, dt, int(calc_timestep), prec, stream),

@@ -524,17 +524,22 @@ def _packed(hhs, sizes, seed0):
     return parts, packed, offsets
 
 
-@pytest.mark.parametrize("sizes,big_n,prec", [
-    ([64, 100, 33, 2, 500, 1500, 3000, 7, 260], 1024, 0),
-    ([300] * 12 + [2000] * 3, 128, 0),
-    ([64, 100, 33, 2, 500, 1500, 3000, 7, 260], 1024, 1)])
-def test_hold_batched_matches_per_system_oracle(cuda, hhs, oracle, sizes, big_n, prec):
+@pytest.mark.parametrize("sizes,big_n,prec,mid_n", [
+    ([64, 100, 33, 2, 500, 1500, 3000, 7, 260], 1024, 0, 640),
+    ([64, 100, 33, 2, 500, 1500, 3000, 7, 260], 1024, 0, 0),
+    ([300] * 12 + [2000] * 3, 128, 0, 640),
+    ([300] * 12 + [2000] * 3, 128, 0, 0),
+    ([64, 100, 33, 2, 500, 1500, 3000, 7, 260], 1024, 1, 640)])
+def test_hold_batched_matches_per_system_oracle(cuda, hhs, oracle, sizes, big_n, prec, mid_n):
+    """Independent systems in one launch: large ones on a thread-block cluster, small ones
+    on one CTA, with (mid_n = 640) or without the shared-memory subtree solver."""
     parts, packed, offsets = _packed(hhs, sizes, 300)
     n = int(offsets[-1])
     d = hhs.ParticleSystem(n)
     d.upload(packed)
     b = hhs.Batch(offsets, 64, eta=0.03)
     b.set_tuning(big_n, 64, 8)
+    b.set_mid(mid_n, 96)
     dt = 1.0 / 64
     leaf = np.zeros(len(sizes))
     for _ in range(2):
