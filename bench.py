@@ -59,12 +59,16 @@ def parse():
     p.add_argument("--profile-out", default=None,
                    help="write the per-level phase profile (JSON) to this path")
     p.add_argument("--workload", default="plummer16k",
-                   choices=["plummer16k", "batched", "scan", "large", "deep", "validate"],
+                   choices=["plummer16k", "batched", "scan", "large", "deep", "validate",
+                            "plain1k"],
                    help="plummer16k (default headline), batched (512 clusters), scan (flag "
                         "compaction sweep), large (N=262144, 90/10 masses), deep (N=65536 "
-                        "Salpeter), validate (integrate to --t-end in mixed and FP64 precision "
-                        "and compare)")
+                        "Salpeter), validate (integrate --n/--eta/--mass to --t-end in mixed "
+                        "and FP64 precision and compare), plain1k (N=1024 FP64 to t=1 on the "
+                        "GPU and on the CPU oracle, compared bit for bit)")
     p.add_argument("--t-end", type=float, default=1.0)
+    p.add_argument("--mass", type=int, default=0, choices=[0, 1, 2],
+                   help="mass spectrum: 0 equal, 1 Salpeter on [0.1, 100], 2 90%%/10%% two-component")
     p.add_argument("--scan-log2n", type=int, default=None,
                    help="scan workload: run this one size instead of the 2^20..2^28 sweep")
     p.add_argument("--no-baselines", action="store_true",
@@ -72,8 +76,13 @@ def parse():
     return p.parse_args()
 
 
+MASS_NAMES = {0: "equal-mass", 1: "Salpeter dN/dm ~ m^-2.35 on [0.1,100]",
+              2: "two-component (90% m=1, 10% m=10)"}
+
+
 def workload_name(a):
-    return (f"Plummer N={a.n} equal-mass Henon units, eta={a.eta}, dt_top=2^{int(round(__import__('math').log2(a.dt)))}, "
+    return (f"Plummer N={a.n} {MASS_NAMES[getattr(a, 'mass', 0)]}, Henon units, eta={a.eta}, "
+            f"dt_top=2^{int(round(__import__('math').log2(a.dt)))}, "
             f"{a.prec} precision, one top-level HOLD step per step")
 
 
@@ -391,22 +400,38 @@ def run_ours(a, rank, world, torch, dist):
     return res
 
 
+# DRAM bytes of one k_engine launch of the default workload (dram__bytes_read.sum +
+# dram__bytes_write.sum of an ncu capture of one launch after three warm-up launches)
+ENGINE_16K_DRAM_BYTES = 1.195264e6 + 1.224960e6
+
+
 def roofline(res, a, peaks_tflops):
+    """Roofline of the dominant kernel, the persistent HOLD kernel (one launch per step):
+    algorithmic flops per launch (timestep pairs x 50 + kick pairs x 20, from the run's own
+    work counters) over the launch's CUDA-event duration, against the measured FMA-chain
+    peak; the timestep and kick phases are reported beside it from the phase profile."""
     prof = res["prof"]
-    if not prof:
-        return None
-    kind = max(("kick", "timesteps"), key=lambda k: prof.get(k, {}).get("ms", 0.0))
-    p = prof[kind]
-    fpp = KICK_FLOPS_PER_PAIR if kind == "kick" else TS_FLOPS_PER_PAIR
-    avg_ms = p["ms"] / p["launches"]
-    flops_per_launch = p["pairs"] * fpp / p["launches"]
-    achieved = flops_per_launch / (avg_ms * 1e-3) / 1e12
+    st = res["stats"]
+    launch_ms = res["t_ms"] / a.steps
+    flops = (st["ts_pairs"] * TS_FLOPS_PER_PAIR + st["kick_pairs"] * KICK_FLOPS_PER_PAIR) / a.steps
+    achieved = flops / (launch_ms * 1e-3) / 1e12
     peak = peaks_tflops[0] if a.prec == "mixed" else peaks_tflops[1]
-    return {"bound": "fp32-fma" if a.prec == "mixed" else "fp64-fma", "kernel": kind,
+    phases = {}
+    for kind, fpp in (("timesteps", TS_FLOPS_PER_PAIR), ("kick", KICK_FLOPS_PER_PAIR)):
+        p = (prof or {}).get(kind)
+        if p and p["ms"] > 0:
+            tf = p["pairs"] * fpp / (p["ms"] * 1e-3) / 1e12
+            phases[kind] = {"achieved": tf, "frac": tf / peak, "flops_per_pair": fpp,
+                            "share_of_step": p["ms"] / res["t_ms"]}
+    default = (a.n == 16384 and a.prec == "mixed" and a.workload == "plummer16k")
+    return {"bound": "fp32-fma" if a.prec == "mixed" else "fp64-fma", "kernel": "k_engine",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "peak_source": "measured FMA-chain peak of this B200 (hhs_measure_fma_peaks)",
-            "flops_per_pair": fpp, "avg_launch_ms": avg_ms, "launches": p["launches"],
-            "share_of_step": p["ms"] / res["t_ms"], "traffic": None}
+            "peak_source": "measured FMA-chain peak of this B200 (hhs_measure_fma_peaks); "
+                           "the pair kernels use neither tensor cores nor HBM bandwidth",
+            "flops_per_launch": flops, "launch_ms": launch_ms, "phases": phases,
+            "traffic": ENGINE_16K_DRAM_BYTES if default else None,
+            "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                            "of this workload" if default else None}
 
 
 # ------------------------------------------------------------------------ other workloads
@@ -576,6 +601,44 @@ def run_scan(a, torch):
                          "unit": "GB/s", "traffic": None}, "sweep": rows}
 
 
+def run_plain1k(a, torch):
+    """Plain FP64 HOLD of a Plummer N=1024 sphere to t=1 on the GPU (device schedule) and on
+    the CPU oracle (OpenMP, host cores): the final states must agree bit for bit."""
+    import numpy as np
+    import hhs
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.build()
+    n, eta, dt = 1024, 0.03, a.dt
+    steps = int(round(1.0 / dt))
+    ics = hhs.plummer(n, a.seed)
+    e0 = hhs.energy_host(ics)
+    ctx = hhs.Context(n, 64, eta=eta)
+    d = hhs.ParticleSystem(n)
+    d.upload(ics)
+    ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    torch.cuda.synchronize()
+    ev[0].record()
+    for _ in range(steps):
+        hhs.hold_step(ctx, d, n, 0.0, dt, True, hhs.PREC_FP64)
+    ev[1].record()
+    ctx.check()
+    gpu = d.download()
+    t_gpu = ev[0].elapsed_time(ev[1]) * 1e-3
+    ref = {k: v.copy() for k, v in ics.items()}
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        oracle.hold_step(ref, dt, True, eta)
+    t_cpu = time.perf_counter() - t0
+    same = all(np.array_equal(gpu[k], ref[k]) for k in hhs.FIELDS)
+    return {"metric": "plain FP64 HOLD, Plummer N=1024 to t=1: GPU vs CPU oracle",
+            "value": steps / t_gpu, "unit": "HOLD steps/s", "n": n, "eta": eta, "dt_top": dt,
+            "steps": steps, "gpu_steps_per_s": steps / t_gpu,
+            "cpu_oracle_steps_per_s": steps / t_cpu, "cpu_threads": oracle.threads(),
+            "bit_exact_gpu_vs_oracle": bool(same),
+            "dE_over_E": (hhs.energy_host(gpu) - e0) / e0}
+
+
 def run_validate(a, torch):
     """Integrates the workload to t_end in mixed precision and in FP64 (the FP64 device
     schedule reproduces the CPU oracle bit for bit) and reports both energy errors, the
@@ -646,9 +709,9 @@ def main():
         if dist is not None:
             dist.destroy_process_group()
         return
-    if a.workload in ("scan", "validate"):
+    if a.workload in ("scan", "validate", "plain1k"):
         if rank == 0:
-            fn = {"scan": run_scan, "validate": run_validate}[a.workload]
+            fn = {"scan": run_scan, "validate": run_validate, "plain1k": run_plain1k}[a.workload]
             out = fn(a, torch)
             peaks = None
             try:
