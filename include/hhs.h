@@ -233,6 +233,14 @@ hhs_status hhs_compact_flags_i32(const int32_t* d_flags, int32_t* d_scan, int32_
 /* Synchronises the stream; HHS_ERR_TIMEOUT if a look-back wait of the last scan on this
  * workspace gave up. */
 hhs_status hhs_scan_workspace_status(const void* d_workspace, void* stream);
+/* Failure-detection self-test of the bounded look-back wait (no counterpart in the
+ * reference, whose waits are unbounded): runs the scan with its first tile left out, so
+ * every look-back waits for a predecessor that never publishes; each wait gives up after
+ * max_polls (1..2^22) polls, records the timeout in the workspace and returns. Synchronises
+ * the stream; returns HHS_ERR_TIMEOUT when the waits ran out as designed. n >= 8192. */
+hhs_status hhs_scan_selftest_stalled_predecessor(const int32_t* d_in, int32_t* d_out, int64_t n,
+                                                 void* d_workspace, size_t workspace_bytes,
+                                                 uint32_t max_polls, void* stream);
 
 /* ---- diagnostics ---------------------------------------------------------------- */
 /* Work recorded by the HOLD schedule since the last reset (device counters). */

@@ -1,6 +1,7 @@
 // hhs_scan.cu -- standalone exact exclusive scan and the fast/slow index split.
 #include <atomic>
 #include <cstdlib>
+#include <cstring>
 
 #include "hhs_scan.cuh"
 #include "hhs_kernels.h"
@@ -23,10 +24,10 @@ __global__ void __launch_bounds__(kScanBlock, 6)
                          long long n, ScanHeader* hdr, unsigned long long* status,
                          int num_tiles) {
     __shared__ int s_tile;
-    __shared__ unsigned s_epoch, s_prefix;
+    __shared__ unsigned s_epoch, s_prefix, s_limit;
     __shared__ unsigned s_warp[ScanT::WARPS];
     __shared__ int s_last;
-    scan_begin(hdr, &s_tile, &s_epoch);
+    scan_begin(hdr, &s_tile, &s_epoch, &s_limit);
     const int tile = s_tile;
     const unsigned epoch = s_epoch;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -44,7 +45,7 @@ __global__ void __launch_bounds__(kScanBlock, 6)
             for (int k = 0; k < 4; k++) v[4 * c + k] = (e + k < n) ? (unsigned)in[e + k] : 0u;
         }
     }
-    ScanT::scan(v, cb, status, tile, epoch, &hdr->error, s_warp, &s_prefix);
+    ScanT::scan(v, cb, status, tile, epoch, &hdr->error, s_warp, &s_prefix, s_limit);
 #pragma unroll
     for (int c = 0; c < ScanT::CHUNKS; c++) {
         const long long e = tbase + ScanT::offset(warp, c, lane);
@@ -71,9 +72,9 @@ __global__ void __launch_bounds__(BLOCK, MINB)
              ScanHeader* hdr, unsigned long long* status, int num_tiles) {
     using T = TileScan<BLOCK, ITEMS, LB>;
     __shared__ int s_tile;
-    __shared__ unsigned s_epoch, s_prefix;
+    __shared__ unsigned s_epoch, s_prefix, s_limit;
     __shared__ unsigned s_warp[T::WARPS];
-    scan_begin(hdr, &s_tile, &s_epoch);
+    scan_begin(hdr, &s_tile, &s_epoch, &s_limit);
     const int tile = s_tile;
     const unsigned epoch = s_epoch;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -90,7 +91,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
             for (int k = 0; k < 4; k++) v[4 * c + k] = (e + k < n) ? (unsigned)in[e + k] : 0u;
         }
     }
-    T::scan(v, cb, status, tile, epoch, &hdr->error, s_warp, &s_prefix);
+    T::scan(v, cb, status, tile, epoch, &hdr->error, s_warp, &s_prefix, s_limit);
 #pragma unroll
     for (int c = 0; c < T::CHUNKS; c++) {
         const long long e = tbase + T::offset(warp, c, lane);
@@ -136,10 +137,10 @@ __global__ void __launch_bounds__(kScanBlock, 6)
                     int32_t* __restrict__ idx_out, int32_t* __restrict__ count, long long n,
                     ScanHeader* hdr, unsigned long long* status, int num_tiles) {
     __shared__ int s_tile;
-    __shared__ unsigned s_epoch, s_prefix;
+    __shared__ unsigned s_epoch, s_prefix, s_limit;
     __shared__ unsigned s_warp[ScanT::WARPS];
     __shared__ int s_last;
-    scan_begin(hdr, &s_tile, &s_epoch);
+    scan_begin(hdr, &s_tile, &s_epoch, &s_limit);
     const int tile = s_tile;
     const unsigned epoch = s_epoch;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -157,7 +158,7 @@ __global__ void __launch_bounds__(kScanBlock, 6)
             for (int k = 0; k < 4; k++) v[4 * c + k] = (e + k < n) ? (flags[e + k] != 0) : 0u;
         }
     }
-    ScanT::scan(v, cb, status, tile, epoch, &hdr->error, s_warp, &s_prefix);
+    ScanT::scan(v, cb, status, tile, epoch, &hdr->error, s_warp, &s_prefix, s_limit);
 #pragma unroll
     for (int c = 0; c < ScanT::CHUNKS; c++) {
         const long long e = tbase + ScanT::offset(warp, c, lane);
@@ -203,10 +204,10 @@ __global__ void __launch_bounds__(kSplitBlock)
                  int level, int calc_ts, ScanHeader* hdr, unsigned long long* status,
                  int num_tiles) {
     __shared__ int s_tile;
-    __shared__ unsigned s_epoch, s_prefix;
+    __shared__ unsigned s_epoch, s_prefix, s_limit;
     __shared__ unsigned s_warp[SplitT::WARPS];
     __shared__ int s_last;
-    scan_begin(hdr, &s_tile, &s_epoch);
+    scan_begin(hdr, &s_tile, &s_epoch, &s_limit);
     const int tile = s_tile;
     const unsigned epoch = s_epoch;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -230,7 +231,7 @@ __global__ void __launch_bounds__(kSplitBlock)
             }
         }
     }
-    SplitT::scan(v, cb, status, tile, epoch, &hdr->error, s_warp, &s_prefix);
+    SplitT::scan(v, cb, status, tile, epoch, &hdr->error, s_warp, &s_prefix, s_limit);
 #pragma unroll
     for (int c = 0; c < SplitT::CHUNKS; c++) {
         const long long e = tbase + SplitT::offset(warp, c, lane);
@@ -439,4 +440,36 @@ extern "C" hhs_status hhs_scan_workspace_status(const void* d_workspace, void* s
                             sizeof(err), cudaMemcpyDeviceToHost));
     if (err & HHS_ERRBIT_LOOKBACK_TIMEOUT) return HHS_ERR_TIMEOUT;
     return err ? HHS_ERR_DEVICE_FAULT_FLAG : HHS_OK;
+}
+
+// ------------------------------------------------------------------ bounded-wait self-test
+// Runs the scan of hhs_scan_exclusive_i32 with tile 0 left out (the tile counter starts at
+// 1), so every look-back waits on a predecessor that never publishes. Each wait gives up
+// after max_polls polls, records HHS_ERRBIT_LOOKBACK_TIMEOUT in the workspace header and
+// lets its CTA finish; the call synchronises the stream and returns the workspace status,
+// HHS_ERR_TIMEOUT when the waits ran out as designed. The output is not a valid scan.
+extern "C" hhs_status hhs_scan_selftest_stalled_predecessor(const int32_t* d_in, int32_t* d_out,
+                                                             int64_t n, void* d_workspace,
+                                                             size_t workspace_bytes,
+                                                             uint32_t max_polls, void* stream) {
+    if (n < 2 * (int64_t)ScanT::TILE || n > (int64_t)0x7fffffff || !d_in || !d_out ||
+        !d_workspace || max_polls == 0 || max_polls > HHS_SPIN_LIMIT)
+        return HHS_ERR_INVALID_ARG;
+    if (workspace_bytes < hhs_scan_workspace_size(n)) return HHS_ERR_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(d_workspace) & 7u) != 0) return HHS_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int tiles = (int)((n + ScanT::TILE - 1) / ScanT::TILE);
+    HHS_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, scan_workspace_bytes(n, kScanMinTile), s));
+    ScanHeader h;
+    std::memset(&h, 0, sizeof(h));
+    h.tile_counter = 1u;
+    h.spin_limit = max_polls;
+    HHS_CUDA_TRY(cudaMemcpyAsync(d_workspace, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+    auto* hdr = static_cast<ScanHeader*>(d_workspace);
+    auto* status = reinterpret_cast<unsigned long long*>(static_cast<char*>(d_workspace) +
+                                                         sizeof(ScanHeader));
+    k_scan_exclusive_i32<false, false><<<tiles - 1, kScanBlock, 0, s>>>(d_in, d_out, n, hdr,
+                                                                       status, tiles);
+    HHS_LAUNCH_CHECK();
+    return hhs_scan_workspace_status(d_workspace, stream);
 }

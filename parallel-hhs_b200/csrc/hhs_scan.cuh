@@ -19,7 +19,8 @@ struct ScanHeader {
     unsigned done_counter;  // CTAs that finished; the last one resets the header
     unsigned epoch;         // status words of other epochs read as "not ready"
     unsigned error;         // HHS_ERRBIT_* set by timed-out waits
-    unsigned pad[60];
+    unsigned spin_limit;    // look-back polls before giving up (0: HHS_SPIN_LIMIT)
+    unsigned pad[59];
 };
 static_assert(sizeof(ScanHeader) == 256, "scan header must stay 256 bytes");
 
@@ -41,7 +42,7 @@ __device__ __forceinline__ unsigned scan_next_epoch(const ScanHeader* h) {
 template <int PER_LANE>
 __device__ __forceinline__ unsigned scan_lookback_w(unsigned long long* status, int tile,
                                                     unsigned aggregate, unsigned epoch,
-                                                    unsigned* err) {
+                                                    unsigned* err, unsigned limit) {
     const int lane = threadIdx.x & 31;
     if (tile == 0) {
         if (lane == 0) st_relaxed_u64(&status[0], scan_pack(epoch, 2u, aggregate));
@@ -69,7 +70,7 @@ __device__ __forceinline__ unsigned scan_lookback_w(unsigned long long* status, 
                 ready = ready && flag[k] != 0u;
             }
             if (__all_sync(HHS_FULL_MASK, ready)) break;
-            if (++spins > HHS_SPIN_LIMIT) {
+            if (++spins > limit) {
                 if (lane == 0) atomicOr(err, HHS_ERRBIT_LOOKBACK_TIMEOUT);
 #pragma unroll
                 for (int k = 0; k < PER_LANE; k++)
@@ -100,11 +101,6 @@ __device__ __forceinline__ unsigned scan_lookback_w(unsigned long long* status, 
     return excl;
 }
 
-__device__ __forceinline__ unsigned scan_lookback(unsigned long long* status, int tile,
-                                                  unsigned aggregate, unsigned epoch,
-                                                  unsigned* err) {
-    return scan_lookback_w<1>(status, tile, aggregate, epoch, err);
-}
 
 // Tile layout shared by the scan kernels: BLOCK threads x ITEMS values; value k of
 // chunk c of lane l in warp w sits at tile offset w*32*ITEMS + c*128 + l*4 + k, so a
@@ -127,7 +123,8 @@ struct TileScan {
                                                 unsigned (&cbase)[CHUNKS],
                                                 unsigned long long* status, int tile,
                                                 unsigned epoch, unsigned* err,
-                                                unsigned* s_warp, unsigned* s_prefix) {
+                                                unsigned* s_warp, unsigned* s_prefix,
+                                                unsigned limit) {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         unsigned run = 0u;
 #pragma unroll
@@ -143,7 +140,8 @@ struct TileScan {
             const unsigned wt = (lane < WARPS) ? s_warp[lane] : 0u;
             const unsigned wi = (unsigned)warp_incl_scan((int)wt, lane);
             const unsigned total = (unsigned)__shfl_sync(HHS_FULL_MASK, (int)wi, 31);
-            const unsigned prefix = scan_lookback_w<LOOKBACK>(status, tile, total, epoch, err);
+            const unsigned prefix =
+                scan_lookback_w<LOOKBACK>(status, tile, total, epoch, err, limit);
             if (lane < WARPS) s_warp[lane] = wi - wt;
             if (lane == 0) *s_prefix = prefix;
         }
@@ -154,11 +152,15 @@ struct TileScan {
     }
 };
 
-// Fetches this CTA's tile index and the call's epoch (thread 0), broadcast to all.
-__device__ __forceinline__ void scan_begin(ScanHeader* hdr, int* s_tile, unsigned* s_epoch) {
+// Fetches this CTA's tile index, the call's epoch and the look-back poll limit
+// (thread 0), broadcast to all.
+__device__ __forceinline__ void scan_begin(ScanHeader* hdr, int* s_tile, unsigned* s_epoch,
+                                           unsigned* s_limit) {
     if (threadIdx.x == 0) {
         *s_tile = (int)atomicAdd(&hdr->tile_counter, 1u);
         *s_epoch = scan_next_epoch(hdr);
+        const unsigned lim = *reinterpret_cast<volatile const unsigned*>(&hdr->spin_limit);
+        *s_limit = lim ? lim : HHS_SPIN_LIMIT;
     }
     __syncthreads();
 }

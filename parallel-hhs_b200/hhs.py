@@ -125,6 +125,9 @@ SIGNATURES = {
     "hhs_scan_exclusive_i32": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp, ctypes.c_size_t,
                                               _vp]),
     "hhs_scan_workspace_status": (ctypes.c_int, [_vp, _vp]),
+    "hhs_scan_selftest_stalled_predecessor": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp,
+                                                              ctypes.c_size_t, ctypes.c_uint32,
+                                                              _vp]),
     "hhs_scan_exclusive_i32_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp]),
     "hhs_compact_flags_i32": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int64, _vp,
                                              ctypes.c_size_t, _vp]),
@@ -541,6 +544,12 @@ def scan_exclusive_i32(d_in, d_out, n, d_ws, ws_bytes, stream=None):
 def compact_flags_i32(d_flags, d_scan, d_idx, d_count, n, d_ws, ws_bytes, stream=None):
     _check(lib().hhs_compact_flags_i32(d_flags, d_scan, d_idx, d_count, n, d_ws, ws_bytes,
                                        stream), "hhs_compact_flags_i32")
+
+
+def scan_selftest_stalled_predecessor(d_in, d_out, n, d_ws, ws_bytes, max_polls, stream=None):
+    """Status of a scan whose first tile never publishes (HHS_ERR_TIMEOUT expected)."""
+    return lib().hhs_scan_selftest_stalled_predecessor(d_in, d_out, n, d_ws, ws_bytes,
+                                                       max_polls, stream)
 
 
 def scan_workspace_status(d_ws, stream=None):

@@ -124,6 +124,28 @@ def test_scan_random_values_sizes_alignment(cuda, hhs, oracle, n, offset):
     assert np.array_equal(out, oracle.scan_exclusive(a[offset:]))
 
 
+def test_scan_lookback_wait_gives_up_and_reports_timeout(cuda, hhs, oracle):
+    """Failure detection without a GPU fault: with the first tile left out, every look-back
+    waits for a predecessor that never publishes; the bounded waits give up, the call
+    returns HHS_ERR_TIMEOUT, and the context stays usable for a correct scan after it."""
+    torch = cuda
+    n = 1 << 16
+    ws_bytes = hhs.scan_workspace_size(n)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    a = np.random.default_rng(5).integers(0, 2, n).astype(np.int32)
+    dev = torch.from_numpy(a).cuda()
+    out = torch.empty_like(dev)
+    status = hhs.scan_selftest_stalled_predecessor(_ptr(dev), _ptr(out), n, _ptr(ws), ws_bytes,
+                                                   2048, st)
+    assert hhs.STATUS[status] == "HHS_ERR_TIMEOUT"
+    hhs.scan_exclusive_i32(_ptr(dev), _ptr(out), n, _ptr(ws), ws_bytes, st)
+    assert hhs.scan_workspace_status(_ptr(ws), st) == 0
+    assert np.array_equal(out.cpu().numpy(), oracle.scan_exclusive(a))
+    assert hhs.scan_selftest_stalled_predecessor(_ptr(dev), _ptr(out), 100, _ptr(ws), ws_bytes,
+                                                 2048, st) != 0  # fewer than two tiles
+
+
 def test_scan_repeated_calls_reuse_workspace(cuda, hhs, oracle):
     torch = cuda
     n = 300001
