@@ -233,6 +233,15 @@ hhs_status hhs_compact_flags_i32(const int32_t* d_flags, int32_t* d_scan, int32_
 /* Synchronises the stream; HHS_ERR_TIMEOUT if a look-back wait of the last scan on this
  * workspace gave up. */
 hhs_status hhs_scan_workspace_status(const void* d_workspace, void* stream);
+/* The split in the (unstable) particle order of the HHS CPU integrators: the permutation
+ * left by cpu_split's in-place two-pointer partition (src/cpu_scan.h:20-50) of d_ts
+ * against pivot. d_order[0..n_fast) = fast (ts <= pivot), d_order[n_fast..n) = slow;
+ * *d_counts on the device. No N_fast == 1 fold (cpu_split has none). Workspace: 256-byte
+ * aligned, hhs_split_cpu_order_workspace_size(n) bytes. */
+size_t hhs_split_cpu_order_workspace_size(int64_t n);
+hhs_status hhs_split_cpu_order(const double* d_ts, int32_t n, double pivot, int32_t* d_order,
+                               hhs_partition* d_counts, void* d_workspace,
+                               size_t workspace_bytes, void* stream);
 /* Failure-detection self-test of the bounded look-back wait (no counterpart in the
  * reference, whose waits are unbounded): runs the scan with its first tile left out, so
  * every look-back waits for a predecessor that never publishes; each wait gives up after

@@ -104,6 +104,30 @@ int oracle_split(int n, const double* ts, double pivot, int32_t* order) {
     return n_fast;
 }
 
+/* In-place two-pointer partition of the HHS CPU integrators, restating
+ * cpu_split (src/cpu_scan.h:20-50) on particle indices: a left cursor skips entries with
+ * ts <= pivot, a right cursor skips entries with ts > pivot, the two are exchanged while
+ * the cursors have not met. order[0..n_fast) ends as the fast set and order[n_fast..n)
+ * as the slow set, both in that routine's (unstable) order. Returns n_fast. */
+int oracle_split_cpu_order(int n, const double* ts, double pivot, int32_t* order) {
+    for (int i = 0; i < n; i++) order[i] = i;
+    if (n <= 0) return 0;
+    int left = 0, right = n - 1;
+    for (;;) {
+        while (ts[order[left]] <= pivot && left < right) left++;
+        while (ts[order[right]] > pivot && left < right) right--;
+        if (left < right) {
+            int32_t t = order[left];
+            order[left] = order[right];
+            order[right] = t;
+        } else {
+            break;
+        }
+    }
+    if (ts[order[left]] <= pivot) left++;
+    return left;
+}
+
 /* Direct-sum kick, restating src/kick.cuh:19-30 and :82-105 per sink:
  *   dx = x_j - x_i; d2 = dx.dx + eps2; skip d2 == 0; d = sqrt(d2); inv = 1.0/(d2*d);
  *   a += dx * (m_j * inv)           (attractive; the reference GPU kernel has the

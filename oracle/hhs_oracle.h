@@ -61,6 +61,10 @@ void oracle_scan_exclusive_i32(int64_t n, const int32_t* in, int32_t* out);
  * order[n_fast..n) = slow set, and returns n_fast (after the fold). */
 int oracle_split(int n, const double* ts, double pivot, int32_t* order);
 
+/* cpu_split (src/cpu_scan.h:20-50) on indices: the unstable in-place partition of the
+ * HHS CPU integrators. order receives fast then slow indices; returns n_fast. */
+int oracle_split_cpu_order(int n, const double* ts, double pivot, int32_t* order);
+
 /* sinks: positions (read) and velocities (updated by acc*dtfac); sources: positions
  * and masses. acc (3 arrays, may be NULL) receives this call's acceleration. */
 void oracle_kick(int n_sink, const double* sx, const double* sy, const double* sz,

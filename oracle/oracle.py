@@ -53,6 +53,8 @@ def lib():
         L.oracle_scan_exclusive_i32.argtypes = [ctypes.c_int64, _ip, _ip]
         L.oracle_split.argtypes = [ctypes.c_int, _dp, ctypes.c_double, _ip]
         L.oracle_split.restype = ctypes.c_int
+        L.oracle_split_cpu_order.argtypes = [ctypes.c_int, _dp, ctypes.c_double, _ip]
+        L.oracle_split_cpu_order.restype = ctypes.c_int
         L.oracle_kick.argtypes = [ctypes.c_int] + [_dp] * 9 + [ctypes.c_int] + [_dp] * 4 + \
             [ctypes.c_double]
         L.oracle_kick_soft.argtypes = [ctypes.c_int] + [_dp] * 9 + [ctypes.c_int] + \
@@ -99,6 +101,14 @@ def split(ts, pivot):
     ts = np.ascontiguousarray(ts, dtype=np.float64)
     order = np.empty(len(ts), dtype=np.int32)
     nf = lib().oracle_split(len(ts), _d(ts), pivot, _i(order))
+    return order, nf
+
+
+def split_cpu_order(ts, pivot):
+    """Permutation of cpu_split (fast first, unstable order) and n_fast."""
+    ts = np.ascontiguousarray(ts, dtype=np.float64)
+    order = np.empty(len(ts), dtype=np.int32)
+    nf = lib().oracle_split_cpu_order(len(ts), _d(ts), pivot, _i(order))
     return order, nf
 
 

@@ -473,3 +473,99 @@ extern "C" hhs_status hhs_scan_selftest_stalled_predecessor(const int32_t* d_in,
     HHS_LAUNCH_CHECK();
     return hhs_scan_workspace_status(d_workspace, stream);
 }
+
+// ------------------------------------------------------------------ CPU-order split
+// The permutation left behind by the in-place two-pointer partition of the HHS CPU
+// integrators (cpu_split, src/cpu_scan.h:20-50), computed in closed form from one exclusive
+// scan of the fast flags (ts <= pivot). With n_fast fast particles, the k-th slow entry of
+// [0, n_fast) counted from the left is exchanged with the k-th fast entry of [n_fast, n)
+// counted from the right, and every other entry stays in place: exactly the exchanges the
+// two cursors make before they meet.
+namespace {
+
+constexpr int kOrderBlock = 256;
+
+__global__ void k_cpu_order_flags(const double* __restrict__ ts, int n, double pivot,
+                                  int32_t* __restrict__ flags) {
+    const int i = blockIdx.x * kOrderBlock + threadIdx.x;
+    if (i < n) flags[i] = ts[i] <= pivot ? 1 : 0;
+}
+
+__device__ __forceinline__ int cpu_order_nfast(const int32_t* flags, const int32_t* excl, int n) {
+    return excl[n - 1] + flags[n - 1];
+}
+
+// identity order; rank of each misplaced entry; the counts
+__global__ void k_cpu_order_ranks(const int32_t* __restrict__ flags,
+                                  const int32_t* __restrict__ excl, int n,
+                                  int32_t* __restrict__ order, int32_t* __restrict__ pos_slow,
+                                  int32_t* __restrict__ pos_fast, hhs_partition* counts) {
+    const int nf = cpu_order_nfast(flags, excl, n);
+    const int i = blockIdx.x * kOrderBlock + threadIdx.x;
+    if (i == 0) {
+        counts->n_fast = nf;
+        counts->n_slow = n - nf;
+    }
+    if (i >= n) return;
+    order[i] = i;
+    const int f = flags[i], e = excl[i];
+    if (i < nf && !f) pos_slow[i - e] = i;          // slow entries before it: i - e
+    if (i >= nf && f) pos_fast[nf - e - 1] = i;     // fast entries after it
+}
+
+__global__ void k_cpu_order_swap(const int32_t* __restrict__ flags,
+                                 const int32_t* __restrict__ excl, int n,
+                                 const int32_t* __restrict__ pos_slow,
+                                 const int32_t* __restrict__ pos_fast,
+                                 int32_t* __restrict__ order) {
+    const int nf = cpu_order_nfast(flags, excl, n);
+    const int m = nf < n ? nf - excl[nf] : 0;  // slow entries inside [0, n_fast)
+    const int k = blockIdx.x * kOrderBlock + threadIdx.x;
+    if (k >= m) return;
+    const int a = pos_slow[k], b = pos_fast[k];
+    order[a] = b;
+    order[b] = a;
+}
+
+size_t cpu_order_offset(long long n, int part) {
+    const size_t arr = ((size_t)n * sizeof(int32_t) + 255) & ~(size_t)255;
+    return ((scan_workspace_bytes(n, kScanMinTile) + 255) & ~(size_t)255) + arr * (size_t)part;
+}
+
+}  // namespace
+
+extern "C" size_t hhs_split_cpu_order_workspace_size(int64_t n) {
+    return n <= 0 ? 0 : cpu_order_offset(n, 4);
+}
+
+extern "C" hhs_status hhs_split_cpu_order(const double* d_ts, int32_t n, double pivot,
+                                          int32_t* d_order, hhs_partition* d_counts,
+                                          void* d_workspace, size_t workspace_bytes,
+                                          void* stream) {
+    if (n < 0 || !d_counts || (n > 0 && (!d_ts || !d_order || !d_workspace)))
+        return HHS_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (n == 0) {
+        HHS_CUDA_TRY(cudaMemsetAsync(d_counts, 0, sizeof(hhs_partition), s));
+        return HHS_OK;
+    }
+    if (workspace_bytes < hhs_split_cpu_order_workspace_size(n)) return HHS_ERR_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(d_workspace) & 255u) != 0) return HHS_ERR_INVALID_ARG;
+    char* base = static_cast<char*>(d_workspace);
+    auto* flags = reinterpret_cast<int32_t*>(base + cpu_order_offset(n, 0));
+    auto* excl = reinterpret_cast<int32_t*>(base + cpu_order_offset(n, 1));
+    auto* pos_slow = reinterpret_cast<int32_t*>(base + cpu_order_offset(n, 2));
+    auto* pos_fast = reinterpret_cast<int32_t*>(base + cpu_order_offset(n, 3));
+    const int grid = (n + kOrderBlock - 1) / kOrderBlock;
+    k_cpu_order_flags<<<grid, kOrderBlock, 0, s>>>(d_ts, n, pivot, flags);
+    HHS_LAUNCH_CHECK();
+    hhs_status st = hhs_scan_exclusive_i32(flags, excl, n, d_workspace,
+                                           scan_workspace_bytes(n, kScanMinTile), stream);
+    if (st != HHS_OK) return st;
+    k_cpu_order_ranks<<<grid, kOrderBlock, 0, s>>>(flags, excl, n, d_order, pos_slow, pos_fast,
+                                                   d_counts);
+    HHS_LAUNCH_CHECK();
+    k_cpu_order_swap<<<grid, kOrderBlock, 0, s>>>(flags, excl, n, pos_slow, pos_fast, d_order);
+    HHS_LAUNCH_CHECK();
+    return HHS_OK;
+}

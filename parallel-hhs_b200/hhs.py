@@ -124,6 +124,9 @@ SIGNATURES = {
     "hhs_scan_workspace_size": (ctypes.c_size_t, [ctypes.c_int64]),
     "hhs_scan_exclusive_i32": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp, ctypes.c_size_t,
                                               _vp]),
+    "hhs_split_cpu_order_workspace_size": (ctypes.c_size_t, [ctypes.c_int64]),
+    "hhs_split_cpu_order": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_double, _vp, _vp, _vp,
+                                           ctypes.c_size_t, _vp]),
     "hhs_scan_workspace_status": (ctypes.c_int, [_vp, _vp]),
     "hhs_scan_selftest_stalled_predecessor": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp,
                                                               ctypes.c_size_t, ctypes.c_uint32,
@@ -550,6 +553,15 @@ def scan_selftest_stalled_predecessor(d_in, d_out, n, d_ws, ws_bytes, max_polls,
     """Status of a scan whose first tile never publishes (HHS_ERR_TIMEOUT expected)."""
     return lib().hhs_scan_selftest_stalled_predecessor(d_in, d_out, n, d_ws, ws_bytes,
                                                        max_polls, stream)
+
+
+def split_cpu_order(d_ts, n, pivot, d_order, d_counts, d_ws, ws_bytes, stream=None):
+    _check(lib().hhs_split_cpu_order(d_ts, n, pivot, d_order, d_counts, d_ws, ws_bytes, stream),
+           "hhs_split_cpu_order")
+
+
+def split_cpu_order_workspace_size(n):
+    return lib().hhs_split_cpu_order_workspace_size(n)
 
 
 def scan_workspace_status(d_ws, stream=None):

@@ -649,3 +649,27 @@ def test_hold_step_cluster_solver_mixed_close(cuda, hhs, oracle, cs, dist_n):
     dx = max(np.abs(out[k] - ref[k]).max() for k in ("x", "y", "z"))
     assert dx < 1e-7, dx
     assert abs((hhs.energy_host(out) - hhs.energy_host(ref)) / e0) < 1e-8
+
+
+# ------------------------------------------------------------------------------ CPU-order split
+@pytest.mark.parametrize("n", [1, 2, 3, 100, 4097, 65536, 1 << 22])
+def test_split_cpu_order_matches_oracle(cuda, hhs, oracle, n):
+    """hhs_split_cpu_order leaves the permutation of the HHS CPU integrators' in-place
+    partition (cpu_split), bit for bit, with ties at the pivot and all-fast / all-slow."""
+    torch = cuda
+    rng = np.random.default_rng(n)
+    ws_bytes = hhs.split_cpu_order_workspace_size(n)
+    ws = torch.empty(ws_bytes + 256, dtype=torch.uint8, device="cuda")
+    base = (ws.data_ptr() + 255) & ~255
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for kind, pivot in (("rand", 0.3), ("rand", 0.5), ("ties", 2.0), ("rand", -1.0), ("rand", 2.0)):
+        ts = rng.random(n) if kind == "rand" else rng.integers(0, 5, n).astype(np.float64)
+        d_ts = torch.from_numpy(ts).cuda()
+        order = torch.empty(n, dtype=torch.int32, device="cuda")
+        counts = torch.zeros(2, dtype=torch.int32, device="cuda")
+        hhs.split_cpu_order(_ptr(d_ts), n, pivot, _ptr(order), _ptr(counts),
+                            ctypes.c_void_p(base), ws_bytes, st)
+        ref, nf = oracle.split_cpu_order(ts, pivot)
+        c = counts.cpu().numpy()
+        assert c[1] == nf and c[0] == n - nf
+        assert np.array_equal(order.cpu().numpy(), ref), (kind, pivot)

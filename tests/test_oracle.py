@@ -66,6 +66,36 @@ def test_oracle_counts_match_reference_cpu_split_random():
                 if cnt != 1 else True
 
 
+def _ref_cpu_split_order(ts, pivot):
+    """The reference's own cpu_split run on the timesteps; distinct values map its output
+    back to particle indices."""
+    lib = ctypes.CDLL(REF_CPU)
+    lib.ref_cpu_split_f64.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                                      ctypes.c_double, ctypes.POINTER(ctypes.c_int),
+                                      ctypes.POINTER(ctypes.c_int)]
+    work = ts.copy()
+    ns, nf = ctypes.c_int(), ctypes.c_int()
+    lib.ref_cpu_split_f64(work.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(ts), pivot,
+                          ctypes.byref(ns), ctypes.byref(nf))
+    where = {v: i for i, v in enumerate(ts.tolist())}
+    return np.array([where[v] for v in work.tolist()], dtype=np.int32), nf.value
+
+
+@pytest.mark.skipif(not os.path.exists(REF_CPU), reason="reference CPU split not built")
+def test_cpu_order_split_matches_reference_cpu_split_permutation(oracle):
+    """oracle_split_cpu_order reproduces the permutation the reference's cpu_split leaves
+    behind (src/cpu_scan.h:20-50), not just its counts."""
+    rng = np.random.default_rng(11)
+    for n in (1, 2, 3, 17, 1000, 4097, 65536):
+        for p in (0.0, 0.01, 0.3, 0.5, 0.99, 1.0):
+            ts = rng.random(n)
+            pivot = float(np.quantile(ts, p)) if p > 0 else -1.0
+            ref_order, ref_nf = _ref_cpu_split_order(ts, pivot)
+            order, nf = oracle.split_cpu_order(ts, pivot)
+            assert nf == ref_nf == int((ts <= pivot).sum())
+            assert np.array_equal(order, ref_order), (n, p)
+
+
 def test_scan_exclusive_random(oracle):
     rng = np.random.default_rng(0)
     for n in (1, 2, 31, 4096, 4097, 100003):
