@@ -389,13 +389,13 @@ __device__ void ts_unit(const EParams& E, const int32_t* S, int n, int ib, int j
 // ---------------------------------------------------------------- symmetric timestep
 // The pair timestep is exactly symmetric under i <-> j (dr, dv negate exactly, squares,
 // products of two negated values and the mass sum are unchanged), so each unordered pair
-// is evaluated once, in the unit (row block of kEB list positions, column block of 64)
+// is evaluated once, in the unit (row block of kEB list positions, column block of kCB)
 // that holds it with i < j. Rows keep their running max rate in a register; the column
 // maxima of a warp's 32 rows come from a butterfly transpose-reduce (31 shuffles per 16
 // columns). Both are merged into rate_acc with an integer atomicMax on the FP32 bit
 // pattern (rates are >= 0, so integer order is float order). Max is exact and
 // order-independent: the result equals the all-pairs evaluation bit for bit.
-constexpr int kCB = 64;
+constexpr int kCB = 32;
 
 // Column maxima of a 32-row x 16-column block held one row per lane: after the first
 // exchange both half-warps hold the pairwise maxima of the same 16 columns, then a
@@ -415,57 +415,79 @@ __device__ __forceinline__ void butterfly_max16(float (&r)[16], int lane) {
     }
 }
 
-__device__ void ts_sym_unit(const EParams& E, const int32_t* S, int n, int rb, int cb,
-                            Smem& sm) {
+// Units [u0, u1) of the upper triangle of (256-row block, kCB-column block) tiles, in
+// row-major order: a contiguous range per CTA, so consecutive units mostly share their row
+// block, whose particles stay in registers (and whose row maximum is merged once).
+__device__ void ts_sym_range(const EParams& E, const int32_t* S, int n, int u0, int u1,
+                             Smem& sm) {
     const SoA& P = E.P;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int i = rb * kEB + threadIdx.x;
-    const int c0 = cb * kCB;
-    const int ncol = min(kCB, n - c0);
-    __syncthreads();
-    if ((int)threadIdx.x < ncol) {
-        const int gj = list_at(S, c0 + threadIdx.x);
-        const DS a = ds_split(P.x[gj]), b = ds_split(P.y[gj]), c = ds_split(P.z[gj]);
-        sm.u.tsm.A[threadIdx.x] = make_float4(a.hi, b.hi, c.hi, (float)P.m[gj]);
-        sm.u.tsm.B[threadIdx.x] = make_float4(a.lo, b.lo, c.lo, 0.0f);
-        sm.u.tsm.V[threadIdx.x] =
-            make_float4((float)P.vx[gj], (float)P.vy[gj], (float)P.vz[gj], 0.0f);
+    constexpr int kRowStep = kEB / kCB;
+    const int nrb = (n + kEB - 1) / kEB, ncb = (n + kCB - 1) / kCB;
+    int rb = 0, off = u0;  // unit u0 = (rb, rb * kRowStep + off)
+    while (rb < nrb && off >= ncb - rb * kRowStep) {
+        off -= ncb - rb * kRowStep;
+        rb++;
     }
-    const bool act = i < n;
+    int cur = -1, i = 0;
+    bool act = false;
     DS xi{0, 0}, yi{0, 0}, zi{0, 0};
-    float vxi = 0, vyi = 0, vzi = 0, mi = 0;
-    if (act) {
-        const int gi = list_at(S, i);
-        xi = ds_split(P.x[gi]); yi = ds_split(P.y[gi]); zi = ds_split(P.z[gi]);
-        vxi = (float)P.vx[gi]; vyi = (float)P.vy[gi]; vzi = (float)P.vz[gi];
-        mi = (float)P.m[gi];
-    }
-    __syncthreads();
-    float rowmax = 0.0f;
-#pragma unroll 1
-    for (int g = 0; g < kCB / 16; g++) {
-        float r[16];
-#pragma unroll
-        for (int c = 0; c < 16; c++) {
-            const int jl = g * 16 + c;
-            const float4 A = sm.u.tsm.A[jl], B = sm.u.tsm.B[jl], V = sm.u.tsm.V[jl];
-            const float rate = ts_pair_rate_mixed(
-                ds_diff(xi.hi, xi.lo, A.x, B.x), ds_diff(yi.hi, yi.lo, A.y, B.y),
-                ds_diff(zi.hi, zi.lo, A.z, B.z), vxi - V.x, vyi - V.y, vzi - V.z, mi + A.w,
-                E.inv_eta_s2, E.inv_eta);
-            const bool ok = act && (jl < ncol) && (c0 + jl > i);
-            r[c] = ok ? rate : 0.0f;
-            rowmax = fmaxf(rowmax, r[c]);
+    float vxi = 0, vyi = 0, vzi = 0, mi = 0, rowmax = 0.0f;
+    for (int u = u0; u < u1 && rb < nrb; u++) {
+        if (rb != cur) {
+            if (act && rowmax > 0.0f) atomicMax(&E.rate_acc[i], __float_as_uint(rowmax));
+            cur = rb;
+            rowmax = 0.0f;
+            i = rb * kEB + threadIdx.x;
+            act = i < n;
+            if (act) {
+                const int gi = list_at(S, i);
+                xi = ds_split(P.x[gi]); yi = ds_split(P.y[gi]); zi = ds_split(P.z[gi]);
+                vxi = (float)P.vx[gi]; vyi = (float)P.vy[gi]; vzi = (float)P.vz[gi];
+                mi = (float)P.m[gi];
+            }
         }
-        butterfly_max16(r, lane);
-        if (lane < 16) sm.colred[warp][g * 16 + lane] = r[0];
-    }
-    __syncthreads();
-    if ((int)threadIdx.x < ncol) {
-        float cm = 0.0f;
+        const int c0 = (rb * kRowStep + off) * kCB;
+        const int ncol = min(kCB, n - c0);
+        __syncthreads();
+        if ((int)threadIdx.x < ncol) {
+            const int gj = list_at(S, c0 + threadIdx.x);
+            const DS a = ds_split(P.x[gj]), b = ds_split(P.y[gj]), c = ds_split(P.z[gj]);
+            sm.u.tsm.A[threadIdx.x] = make_float4(a.hi, b.hi, c.hi, (float)P.m[gj]);
+            sm.u.tsm.B[threadIdx.x] = make_float4(a.lo, b.lo, c.lo, 0.0f);
+            sm.u.tsm.V[threadIdx.x] =
+                make_float4((float)P.vx[gj], (float)P.vy[gj], (float)P.vz[gj], 0.0f);
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int g = 0; g < kCB / 16; g++) {
+            float r[16];
 #pragma unroll
-        for (int w = 0; w < kEB / 32; w++) cm = fmaxf(cm, sm.colred[w][threadIdx.x]);
-        if (cm > 0.0f) atomicMax(&E.rate_acc[c0 + threadIdx.x], __float_as_uint(cm));
+            for (int c = 0; c < 16; c++) {
+                const int jl = g * 16 + c;
+                const float4 A = sm.u.tsm.A[jl], B = sm.u.tsm.B[jl], V = sm.u.tsm.V[jl];
+                const float rate = ts_pair_rate_mixed(
+                    ds_diff(xi.hi, xi.lo, A.x, B.x), ds_diff(yi.hi, yi.lo, A.y, B.y),
+                    ds_diff(zi.hi, zi.lo, A.z, B.z), vxi - V.x, vyi - V.y, vzi - V.z, mi + A.w,
+                    E.inv_eta_s2, E.inv_eta);
+                const bool ok = act && (jl < ncol) && (c0 + jl > i);
+                r[c] = ok ? rate : 0.0f;
+                rowmax = fmaxf(rowmax, r[c]);
+            }
+            butterfly_max16(r, lane);
+            if (lane < 16) sm.colred[warp][g * 16 + lane] = r[0];
+        }
+        __syncthreads();
+        if ((int)threadIdx.x < ncol) {
+            float cm = 0.0f;
+#pragma unroll
+            for (int w = 0; w < kEB / 32; w++) cm = fmaxf(cm, sm.colred[w][threadIdx.x]);
+            if (cm > 0.0f) atomicMax(&E.rate_acc[c0 + threadIdx.x], __float_as_uint(cm));
+        }
+        if (++off >= ncb - rb * kRowStep) {
+            off = 0;
+            rb++;
+        }
     }
     if (act && rowmax > 0.0f) atomicMax(&E.rate_acc[i], __float_as_uint(rowmax));
 }
@@ -1884,22 +1906,15 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                     }
                 } else {
                     // only units with a pair j > i: row block rb takes column blocks
-                    // cb >= rb * kEB / kCB; the workers stride through that triangle
+                    // cb >= rb * kEB / kCB; each worker takes a contiguous range of that
+                    // triangle in row-major order
                     const int nrb = (n + kEB - 1) / kEB, ncb = (n + kCB - 1) / kCB;
                     constexpr int kRowStep = kEB / kCB;
-                    int rb = 0, off = W.id;  // unit = (rb, rb * kRowStep + off)
-                    while (rb < nrb && off >= ncb - rb * kRowStep) {
-                        off -= ncb - rb * kRowStep;
-                        rb++;
-                    }
-                    while (rb < nrb) {
-                        ts_sym_unit(E, S, n, rb, rb * kRowStep + off, sm);
-                        off += W.count;
-                        while (rb < nrb && off >= ncb - rb * kRowStep) {
-                            off -= ncb - rb * kRowStep;
-                            rb++;
-                        }
-                    }
+                    long long units = 0;
+                    for (int r = 0; r < nrb; r++) units += max(0, ncb - r * kRowStep);
+                    const int u0 = (int)(units * W.id / W.count);
+                    const int u1 = (int)(units * (W.id + 1) / W.count);
+                    ts_sym_range(E, S, n, u0, u1, sm);
                 }
                 if (!phase_barrier(E, sm, W)) return false;
                 prof_mark(E, W, t_last, kProfTs, (double)n * (double)(n - 1), sm, lvl);
