@@ -804,22 +804,26 @@ __device__ void scatter_phase(const EParams& E, const int32_t* S, int n, double 
     }
 }
 
+// Sum of the per-chunk partial accelerations, v += a*dt, and for slow sinks both half
+// drifts. Mixed: one thread per (sink, component) adds its chunks with eight independent
+// loads in flight, so the reduction of a node spreads over the whole grid; FP64: one
+// thread per sink (slow then fast sources, the reference's order).
 template <int PREC>
 __device__ void kick_reduce_phase(const EParams& E, const int32_t* F, const int32_t* L, int nf,
                                   int ns, double dt, int nch, int C, const Workers& W,
                                   Smem& sm) {
     const int n = nf + ns;
     const double h = dt * 0.5;
-    const int ntiles = (n + kEB - 1) / kEB;
     const SoA& P = E.P;
-    for (int t = W.id; t < ntiles; t += W.count) {
-        const int s = t * kEB + threadIdx.x;
-        if (s >= n) continue;
-        const bool slow = s >= nf;
-        const int g = slow ? L[s - nf] : F[s];
-        const double v0[3] = {P.vx[g], P.vy[g], P.vz[g]};
-        double v1[3];
-        if (PREC == HHS_PREC_FP64) {
+    if (PREC == HHS_PREC_FP64) {
+        const int ntiles = (n + kEB - 1) / kEB;
+        for (int t = W.id; t < ntiles; t += W.count) {
+            const int s = t * kEB + threadIdx.x;
+            if (s >= n) continue;
+            const bool slow = s >= nf;
+            const int g = slow ? L[s - nf] : F[s];
+            const double v0[3] = {P.vx[g], P.vy[g], P.vz[g]};
+            double v1[3];
 #pragma unroll
             for (int k = 0; k < 3; k++) {
                 double v = f64_add(v0[k], f64_mul(E.k_part[(size_t)k * E.n_max + s], dt));
@@ -827,29 +831,58 @@ __device__ void kick_reduce_phase(const EParams& E, const int32_t* F, const int3
                     v = f64_add(v, f64_mul(E.k_part[(size_t)(3 + k) * E.n_max + s], dt));
                 v1[k] = v;
             }
-        } else {
-            const int last = slow ? nch : min(nch, (ns + C - 1) / C);
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                double a = 0.0;
-                for (int c = 0; c < last; c++) a += E.k_part[(size_t)(c * 3 + k) * E.n_max + s];
-                v1[k] = fma(a, dt, v0[k]);
-            }
-        }
-        P.vx[g] = v1[0]; P.vy[g] = v1[1]; P.vz[g] = v1[2];
-        if (slow) {
-            if (PREC == HHS_PREC_FP64) {
+            P.vx[g] = v1[0]; P.vy[g] = v1[1]; P.vz[g] = v1[2];
+            if (slow) {
                 P.x[g] = f64_add(f64_add(P.x[g], f64_mul(v0[0], h)), f64_mul(v1[0], h));
                 P.y[g] = f64_add(f64_add(P.y[g], f64_mul(v0[1], h)), f64_mul(v1[1], h));
                 P.z[g] = f64_add(f64_add(P.z[g], f64_mul(v0[2], h)), f64_mul(v1[2], h));
-            } else {
-                P.x[g] = fma(v1[0], h, fma(v0[0], h, P.x[g]));
-                P.y[g] = fma(v1[1], h, fma(v0[1], h, P.y[g]));
-                P.z[g] = fma(v1[2], h, fma(v0[2], h, P.z[g]));
+            }
+        }
+        return;
+    }
+    constexpr int kPer = kEB / 3;  // sinks per CTA iteration (3 components each)
+    const int ntiles = (n + kPer - 1) / kPer;
+    const int lastf = min(nch, (ns + C - 1) / C);  // chunks with sources for fast sinks
+    double* red = reinterpret_cast<double*>(&sm.u);
+    for (int t = W.id; t < ntiles; t += W.count) {
+        const int q = (int)threadIdx.x / 3, k = (int)threadIdx.x % 3;
+        const int s = t * kPer + q;
+        double a = 0.0;
+        if (q < kPer && s < n) {
+            const int last = s >= nf ? nch : lastf;
+            const double* part = E.k_part + (size_t)k * E.n_max + s;
+            const size_t stride = (size_t)3 * E.n_max;
+            int c = 0;
+            for (; c + 8 <= last; c += 8) {
+                double v[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) v[u] = part[(size_t)(c + u) * stride];
+#pragma unroll
+                for (int u = 0; u < 8; u++) a += v[u];
+            }
+            for (; c < last; c++) a += part[(size_t)c * stride];
+        }
+        __syncthreads();
+        red[threadIdx.x] = a;
+        __syncthreads();
+        if ((int)threadIdx.x < kPer) {
+            const int s2 = t * kPer + (int)threadIdx.x;
+            if (s2 < n) {
+                const bool slow = s2 >= nf;
+                const int g = slow ? L[s2 - nf] : F[s2];
+                const double v0[3] = {P.vx[g], P.vy[g], P.vz[g]};
+                double v1[3];
+#pragma unroll
+                for (int c = 0; c < 3; c++) v1[c] = fma(red[3 * threadIdx.x + c], dt, v0[c]);
+                P.vx[g] = v1[0]; P.vy[g] = v1[1]; P.vz[g] = v1[2];
+                if (slow) {
+                    P.x[g] = fma(v1[0], h, fma(v0[0], h, P.x[g]));
+                    P.y[g] = fma(v1[1], h, fma(v0[1], h, P.y[g]));
+                    P.z[g] = fma(v1[2], h, fma(v0[2], h, P.z[g]));
+                }
             }
         }
     }
-    (void)sm;
 }
 
 
