@@ -579,22 +579,32 @@ __device__ void kick_unit(const EParams& E, const int32_t* F, const int32_t* L, 
             if (act) {
                 const int je = min(tl, jend - t0);
                 // blocked compensated summation: 32-pair FP32 blocks, Kahan across blocks
-                for (int jb = 0; jb < je; jb += 32) {
-                    const int jn = min(32, je - jb);
+                // (full blocks unrolled so that consecutive pairs overlap)
+                auto pair = [&](int jl, float& bx, float& by, float& bz) {
+                    const float4 A = sm.u.km.A[jl], B = sm.u.km.B[jl];
+                    const float dx = ds_diff(A.x, B.x, xi.hi, xi.lo);
+                    const float dy = ds_diff(A.y, B.y, yi.hi, yi.lo);
+                    const float dz = ds_diff(A.z, B.z, zi.hi, zi.lo);
+                    const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, E.eps2f)));
+                    const float ri = rsqrt_nr(d2);
+                    const float ri2 = ri * ri;
+                    const float mr3 = (d2 > 0.0f) ? A.w * ri2 * ri : 0.0f;
+                    bx = fmaf(dx, mr3, bx);
+                    by = fmaf(dy, mr3, by);
+                    bz = fmaf(dz, mr3, bz);
+                };
+                int jb = 0;
+                for (; jb + 32 <= je; jb += 32) {
                     float bx = 0.0f, by = 0.0f, bz = 0.0f;
-                    for (int jl = jb; jl < jb + jn; jl++) {
-                        const float4 A = sm.u.km.A[jl], B = sm.u.km.B[jl];
-                        const float dx = ds_diff(A.x, B.x, xi.hi, xi.lo);
-                        const float dy = ds_diff(A.y, B.y, yi.hi, yi.lo);
-                        const float dz = ds_diff(A.z, B.z, zi.hi, zi.lo);
-                        const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, E.eps2f)));
-                        const float ri = rsqrt_nr(d2);
-                        const float ri2 = ri * ri;
-                        const float mr3 = (d2 > 0.0f) ? A.w * ri2 * ri : 0.0f;
-                        bx = fmaf(dx, mr3, bx);
-                        by = fmaf(dy, mr3, by);
-                        bz = fmaf(dz, mr3, bz);
-                    }
+#pragma unroll 8
+                    for (int jl = jb; jl < jb + 32; jl++) pair(jl, bx, by, bz);
+                    kahan_add(acc[0], cmp[0], bx);
+                    kahan_add(acc[1], cmp[1], by);
+                    kahan_add(acc[2], cmp[2], bz);
+                }
+                if (jb < je) {
+                    float bx = 0.0f, by = 0.0f, bz = 0.0f;
+                    for (int jl = jb; jl < je; jl++) pair(jl, bx, by, bz);
                     kahan_add(acc[0], cmp[0], bx);
                     kahan_add(acc[1], cmp[1], by);
                     kahan_add(acc[2], cmp[2], bz);
