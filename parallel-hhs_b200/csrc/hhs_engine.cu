@@ -52,7 +52,7 @@ enum ProfKind {
 };
 
 struct EngineState {
-    unsigned bar_count;
+    unsigned bar_count;   // grid-barrier arrivals of this launch (cleared before each launch)
     unsigned bar_gen;
     unsigned pad[2];
     unsigned long long prof_ns[8];
@@ -120,6 +120,7 @@ struct __align__(16) Smem {
     int red[kEB / 32];
     int ok;
     int bcast;
+    unsigned bar_k;               // grid barriers passed by this CTA in this launch
     // last, so that the persistent kernel's dynamic allocation can extend it to a MidState
     union {
         struct { float4 A[kEB], B[kEB], V[kEB]; } tsm;         // mixed timestep tiles
@@ -154,39 +155,32 @@ __device__ __forceinline__ int ld_volatile_i32(const int32_t* p) {
 }
 
 // ---------------------------------------------------------------- grid barrier
-// Sense-reversing barrier over all CTAs of the cooperative grid (also when the grid is
-// launched in thread-block clusters: a cluster-level first stage measured slower). The
-// last arrival resets the counter and advances the generation; the others poll the
-// generation, give up after kBarrierTimeoutNs (or as soon as another CTA recorded an
-// error) and report failure instead of hanging.
+// Counting barrier over all CTAs of the cooperative grid: the arrival counter is cleared
+// before each launch, the k-th barrier of the launch is passed when it reaches k times the
+// grid size. Arrivals are fire-and-forget release reductions (no CTA waits for its own
+// atomic to return); waiters poll with acquire loads, give up after kBarrierTimeoutNs (or
+// as soon as another CTA recorded an error) and report failure instead of hanging.
 __device__ bool grid_barrier(const EParams& E, Smem& sm) {
     __syncthreads();
     if (threadIdx.x == 0) {
         // The CTA barrier above orders every thread's writes before this thread's
-        // release; arrival is an acquire-release add (the last arrival acquires all the
-        // others' releases), the generation is advanced with a release add and polled
-        // with acquire loads, so no separate fences are needed.
+        // release; the acquire loads of the waiters make them visible, so no separate
+        // fences are needed.
         int ok = 1;
         EngineState* st = E.st;
-        const unsigned parties = gridDim.x;
-        const unsigned gen = ld_acquire_u32(&st->bar_gen);
-        const unsigned arrived = atom_add_acq_rel_u32(&st->bar_count, 1u);
-        if (arrived == parties - 1) {
-            *reinterpret_cast<volatile unsigned*>(&st->bar_count) = 0u;
-            red_add_release_u32(&st->bar_gen, 1u);
-        } else {
-            unsigned polls = 0;
-            unsigned long long t0 = 0;
-            while (ld_acquire_u32(&st->bar_gen) == gen) {
-                if (++polls < 256) continue;  // tight polling first
-                if (t0 == 0) t0 = gtimer();
-                if (*reinterpret_cast<volatile unsigned*>(E.err) != 0u) { ok = 0; break; }
-                __nanosleep(32);
-                if (gtimer() - t0 > kBarrierTimeoutNs) {
-                    atomicOr(E.err, HHS_ERRBIT_BARRIER_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
+        const unsigned target = (++sm.bar_k) * gridDim.x;
+        red_add_release_u32(&st->bar_count, 1u);
+        unsigned polls = 0;
+        unsigned long long t0 = 0;
+        while (ld_acquire_u32(&st->bar_count) < target) {
+            if (++polls < 256) continue;  // tight polling first
+            if (t0 == 0) t0 = gtimer();
+            if (*reinterpret_cast<volatile unsigned*>(E.err) != 0u) { ok = 0; break; }
+            __nanosleep(32);
+            if (gtimer() - t0 > kBarrierTimeoutNs) {
+                atomicOr(E.err, HHS_ERRBIT_BARRIER_TIMEOUT);
+                ok = 0;
+                break;
             }
         }
         sm.ok = ok;
@@ -2035,6 +2029,7 @@ __global__ void __launch_bounds__(kEB, 2) k_engine(EParams E) {
     extern __shared__ __align__(16) unsigned char engine_smem[];
     Smem& sm = *reinterpret_cast<Smem*>(engine_smem);
     const Workers W{(int)blockIdx.x, (int)gridDim.x, kModeGrid};
+    if (threadIdx.x == 0) sm.bar_k = 0u;  // published to thread 0 only; it alone uses it
     unsigned long long t_last = 0;
     prof_begin(E, sm);
     prof_mark(E, W, t_last, -1, 0.0, sm);
@@ -2363,6 +2358,8 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
         at[1].val.clusterDim.z = 1;
         cfg.numAttrs = 2;
     }
+    // the grid barrier counts this launch's arrivals from zero
+    HHS_CUDA_TRY(cudaMemsetAsync(&eh->st->bar_count, 0, sizeof(unsigned), stream));
     cudaError_t e = pi == 0 ? cudaLaunchKernelEx(&cfg, k_engine<HHS_PREC_FP64>, E)
                             : cudaLaunchKernelEx(&cfg, k_engine<HHS_PREC_MIXED>, E);
     hhs_count_launch();
