@@ -37,6 +37,7 @@
 #include "hhs_ctx.h"
 #include "hhs_kernels.h"
 #include "hhs_pairmath.cuh"
+#include "hhs_scan.cuh"
 
 using namespace hhs;
 
@@ -77,6 +78,7 @@ struct EParams {
     double* ts_part;   // [kMaxChunks][n_max] (float view for mixed)
     double* k_part;    // [kMaxChunks*3][n_max] (mixed) or [6][n_max] (FP64)
     int* tile_counts;  // [n_max/kEB + 1]
+    unsigned long long* tile_status;  // [n_max/kEB + 2] look-back words, cleared per launch
     unsigned* rate_acc;  // [n_max] max pair rate per list position (FP32 bits), kept at 0
     EngineState* st;
     unsigned* err;
@@ -121,6 +123,7 @@ struct __align__(16) Smem {
     int ok;
     int bcast;
     unsigned bar_k;               // grid barriers passed by this CTA in this launch
+    unsigned epoch;               // look-back epoch of the current split
     // last, so that the persistent kernel's dynamic allocation can extend it to a MidState
     union {
         struct { float4 A[kEB], B[kEB], V[kEB]; } tsm;         // mixed timestep tiles
@@ -805,6 +808,83 @@ __device__ void scatter_phase(const EParams& E, const int32_t* S, int n, double 
         atomicMax(&E.stats->max_level, level);
         atomicAdd(&E.stats->kick_pairs, ns * (ns - 1.0) + 2.0 * ns * nfd);
         if (calc) atomicAdd(&E.stats->ts_pairs, (double)n * (double)(n - 1));
+    }
+}
+
+// Predicate and stable scatter in one pass (grid mode): each 256-particle tile publishes
+// its fast count and finds its prefix by a decoupled look-back over the tiles before it
+// (hhs_scan.cuh), so no grid barrier separates counting from scattering. Tiles are taken
+// in increasing order by every CTA of the co-resident grid, so every look-back ends. The
+// N_fast == 1 fold costs nothing: the first fast particle is also written to L[n-1],
+// which is the lone particle's place after the fold and an unused slot otherwise (every
+// slow particle lands below n-1 once one fast particle exists). The tile that ends the
+// list writes the counts and the work counters.
+template <int PREC>
+__device__ void split_phase(const EParams& E, const int32_t* S, int n, double dt, int level,
+                            bool calc, int nch, const Workers& W, Smem& sm) {
+    const int ntiles = (n + kEB - 1) / kEB;
+    int32_t* F = E.fast_lists + (size_t)level * E.n_max;
+    int32_t* L = E.slow_lists + (size_t)level * E.n_max;
+    if (threadIdx.x == 0) sm.epoch = (sm.bar_k + 1u) & 0x3fffffffu;
+    __syncthreads();
+    const unsigned epoch = sm.epoch;
+    for (int t = W.id; t < ntiles; t += W.count) {
+        const int i = t * kEB + threadIdx.x;
+        int flag = 0, gi = 0;
+        if (i < n) {
+            gi = list_at(S, i);
+            double ts;
+            if (calc) {
+                if (PREC == HHS_PREC_FP64) {
+                    double mv = 1.e30;
+                    for (int c = 0; c < nch; c++) {
+                        const double v = E.ts_part[(size_t)c * E.n_max + i];
+                        if (v < mv) mv = v;
+                    }
+                    ts = mv;
+                } else {
+                    const float mr = __uint_as_float(E.rate_acc[i]);
+                    E.rate_acc[i] = 0u;
+                    const double tv = 1.0 / (double)mr;
+                    ts = tv < 1.e30 ? tv : 1.e30;
+                }
+                E.P.ts[gi] = ts;
+            } else {
+                ts = E.P.ts[gi];
+            }
+            flag = ts <= dt;
+        }
+        int tot;
+        const int ex = block_excl_flag(flag, sm, tot);
+        if (threadIdx.x < 32) {
+            const unsigned pre = scan_lookback_w<1>(E.tile_status, t, (unsigned)tot, epoch, E.err,
+                                                    HHS_SPIN_LIMIT);
+            if (threadIdx.x == 0) sm.bcast = (int)pre;
+        }
+        __syncthreads();
+        const int prefix = sm.bcast;
+        if (i < n) {
+            const int p = prefix + ex;
+            if (flag) {
+                F[p] = gi;
+                if (p == 0) L[n - 1] = gi;
+            } else {
+                L[i - p] = gi;
+            }
+        }
+        if (t == ntiles - 1 && threadIdx.x == 0) {
+            const int nf_raw = prefix + tot;
+            const int nf = nf_raw == 1 ? 0 : nf_raw;
+            E.counts[level].n_fast = nf;
+            E.counts[level].n_slow = n - nf;
+            if (nf == 0) *E.leaf_time += dt;
+            const double ns = (double)(n - nf), nfd = (double)nf;
+            atomicAdd(reinterpret_cast<unsigned long long*>(&E.stats->nodes), 1ull);
+            atomicMax(&E.stats->max_level, level);
+            atomicAdd(&E.stats->kick_pairs, ns * (ns - 1.0) + 2.0 * ns * nfd);
+            if (calc) atomicAdd(&E.stats->ts_pairs, (double)n * (double)(n - 1));
+        }
+        __syncthreads();
     }
 }
 
@@ -1929,8 +2009,8 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                 lvl--;
                 continue;
             }
+            int nch = 1;
             if (calc) {
-                int nch = 1;
                 if (PREC == HHS_PREC_FP64) {
                     nch = chunks_for(n, W, true, E.units_per_cta);
                     const int C = (n + nch - 1) / nch;
@@ -1955,12 +2035,14 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                 }
                 if (!phase_barrier(E, sm, W)) return false;
                 prof_mark(E, W, t_last, kProfTs, (double)n * (double)(n - 1), sm, lvl);
-                count_phase<PREC>(E, S, n, dt, true, nch, W, sm);
-            } else {
-                count_phase<PREC>(E, S, n, dt, false, 1, W, sm);
             }
-            if (!phase_barrier(E, sm, W)) return false;
-            scatter_phase(E, S, n, dt, lvl, calc, W, sm);
+            if constexpr (MODE == kModeGrid) {
+                split_phase<PREC>(E, S, n, dt, lvl, calc, nch, W, sm);
+            } else {
+                count_phase<PREC>(E, S, n, dt, calc, nch, W, sm);
+                if (!phase_barrier(E, sm, W)) return false;
+                scatter_phase(E, S, n, dt, lvl, calc, W, sm);
+            }
             if (!phase_barrier(E, sm, W)) return false;
             prof_mark(E, W, t_last, kProfSplit, 0.0, sm, lvl);
             after1 |= bit;
@@ -2139,6 +2221,7 @@ struct EngineHost {
     double* k_part = nullptr;
     int* tile_counts = nullptr;
     unsigned* rate_acc = nullptr;
+    unsigned long long* tile_status = nullptr;
     int n_max = 0;
 };
 
@@ -2152,7 +2235,7 @@ size_t engine_workspace_bytes(int n_max, int max_levels) {
     const size_t n = (size_t)n_max;
     return al(sizeof(EngineState)) + al(sizeof(double) * kMaxChunks * n) +
            al(sizeof(double) * kMaxChunks * 3 * n) + al(sizeof(int) * (n / kEB + 2)) +
-           al(sizeof(unsigned) * n);
+           al(sizeof(unsigned) * n) + al(sizeof(unsigned long long) * (n / kEB + 2));
 }
 
 hhs_status engine_init(hhs_ctx* c, void* base) {
@@ -2164,7 +2247,8 @@ hhs_status engine_init(hhs_ctx* c, void* base) {
     eh->ts_part = reinterpret_cast<double*>(p); p += al(sizeof(double) * kMaxChunks * n);
     eh->k_part = reinterpret_cast<double*>(p); p += al(sizeof(double) * kMaxChunks * 3 * n);
     eh->tile_counts = reinterpret_cast<int*>(p); p += al(sizeof(int) * (n / kEB + 2));
-    eh->rate_acc = reinterpret_cast<unsigned*>(p);
+    eh->rate_acc = reinterpret_cast<unsigned*>(p); p += al(sizeof(unsigned) * n);
+    eh->tile_status = reinterpret_cast<unsigned long long*>(p);
     eh->n_max = c->n_max;
     int dev = 0, sms = 0, coop = 0;
     cudaGetDevice(&dev);
@@ -2337,6 +2421,7 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
     E.ts_part = eh->ts_part;
     E.k_part = eh->k_part;
     E.tile_counts = eh->tile_counts;
+    E.tile_status = eh->tile_status;
     E.rate_acc = eh->rate_acc;
     E.st = eh->st;
     E.err = c->err;
@@ -2358,8 +2443,11 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
         at[1].val.clusterDim.z = 1;
         cfg.numAttrs = 2;
     }
-    // the grid barrier counts this launch's arrivals from zero
+    // the grid barrier counts this launch's arrivals from zero; look-back words of earlier
+    // launches must not look ready
     HHS_CUDA_TRY(cudaMemsetAsync(&eh->st->bar_count, 0, sizeof(unsigned), stream));
+    HHS_CUDA_TRY(cudaMemsetAsync(eh->tile_status, 0,
+                                 sizeof(unsigned long long) * (size_t)(eh->n_max / kEB + 2), stream));
     cudaError_t e = pi == 0 ? cudaLaunchKernelEx(&cfg, k_engine<HHS_PREC_FP64>, E)
                             : cudaLaunchKernelEx(&cfg, k_engine<HHS_PREC_MIXED>, E);
     hhs_count_launch();
@@ -2559,6 +2647,7 @@ extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, d
     E.stats = b->d_stats;
     E.ts_part = E.k_part = nullptr;
     E.tile_counts = nullptr;
+    E.tile_status = nullptr;
     E.rate_acc = nullptr;
     E.st = nullptr;
     E.err = b->d_err;
