@@ -430,6 +430,9 @@ __device__ void ts_sym_range(const EParams& E, const int32_t* S, int n, int u0, 
     bool act = false;
     DS xi{0, 0}, yi{0, 0}, zi{0, 0};
     float vxi = 0, vyi = 0, vzi = 0, mi = 0, rowmax = 0.0f;
+    // the next unit's columns are loaded into registers while this unit computes
+    double px = 0, py = 0, pz = 0, pvx = 0, pvy = 0, pvz = 0, pm = 0;
+    bool have = false;
     for (int u = u0; u < u1 && rb < nrb; u++) {
         if (rb != cur) {
             if (act && rowmax > 0.0f) atomicMax(&E.rate_acc[i], __float_as_uint(rowmax));
@@ -446,16 +449,33 @@ __device__ void ts_sym_range(const EParams& E, const int32_t* S, int n, int u0, 
         }
         const int c0 = (rb * kRowStep + off) * kCB;
         const int ncol = min(kCB, n - c0);
-        __syncthreads();
-        if ((int)threadIdx.x < ncol) {
+        if (!have && (int)threadIdx.x < ncol) {
             const int gj = list_at(S, c0 + threadIdx.x);
-            const DS a = ds_split(P.x[gj]), b = ds_split(P.y[gj]), c = ds_split(P.z[gj]);
-            sm.u.tsm.A[threadIdx.x] = make_float4(a.hi, b.hi, c.hi, (float)P.m[gj]);
-            sm.u.tsm.B[threadIdx.x] = make_float4(a.lo, b.lo, c.lo, 0.0f);
-            sm.u.tsm.V[threadIdx.x] =
-                make_float4((float)P.vx[gj], (float)P.vy[gj], (float)P.vz[gj], 0.0f);
+            px = P.x[gj]; py = P.y[gj]; pz = P.z[gj];
+            pvx = P.vx[gj]; pvy = P.vy[gj]; pvz = P.vz[gj]; pm = P.m[gj];
         }
         __syncthreads();
+        if ((int)threadIdx.x < ncol) {
+            const DS a = ds_split(px), b = ds_split(py), c = ds_split(pz);
+            sm.u.tsm.A[threadIdx.x] = make_float4(a.hi, b.hi, c.hi, (float)pm);
+            sm.u.tsm.B[threadIdx.x] = make_float4(a.lo, b.lo, c.lo, 0.0f);
+            sm.u.tsm.V[threadIdx.x] = make_float4((float)pvx, (float)pvy, (float)pvz, 0.0f);
+        }
+        __syncthreads();
+        {
+            int rb2 = rb, off2 = off + 1;
+            if (off2 >= ncb - rb * kRowStep) { off2 = 0; rb2++; }
+            have = false;
+            if (u + 1 < u1 && rb2 < nrb) {
+                have = true;
+                const int c0n = (rb2 * kRowStep + off2) * kCB;
+                if ((int)threadIdx.x < min(kCB, n - c0n)) {
+                    const int gj = list_at(S, c0n + threadIdx.x);
+                    px = P.x[gj]; py = P.y[gj]; pz = P.z[gj];
+                    pvx = P.vx[gj]; pvy = P.vy[gj]; pvz = P.vz[gj]; pm = P.m[gj];
+                }
+            }
+        }
 #pragma unroll 1
         for (int g = 0; g < kCB / 16; g++) {
             float r[16];
