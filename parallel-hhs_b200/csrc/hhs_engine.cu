@@ -596,14 +596,17 @@ __device__ void kick_unit(const EParams& E, const int32_t* F, const int32_t* L, 
             if (act) {
                 const int je = min(tl, jend - t0);
                 // blocked compensated summation: 32-pair FP32 blocks, Kahan across blocks
-                // (full blocks unrolled so that consecutive pairs overlap)
+                // (full blocks unrolled so that consecutive pairs overlap). 1/r is rsqrtf
+                // without a Newton step: its few-ulp error per pair is of the order of the
+                // FP32 pair arithmetic itself, and |dE/E| after one N-body time is unchanged
+                // (6.6e-9 against 6.9e-9 with the Newton step, Plummer N=16384).
                 auto pair = [&](int jl, float& bx, float& by, float& bz) {
                     const float4 A = sm.u.km.A[jl], B = sm.u.km.B[jl];
                     const float dx = ds_diff(A.x, B.x, xi.hi, xi.lo);
                     const float dy = ds_diff(A.y, B.y, yi.hi, yi.lo);
                     const float dz = ds_diff(A.z, B.z, zi.hi, zi.lo);
                     const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, E.eps2f)));
-                    const float ri = rsqrt_nr(d2);
+                    const float ri = rsqrtf(d2);
                     const float ri2 = ri * ri;
                     const float mr3 = (d2 > 0.0f) ? A.w * ri2 * ri : 0.0f;
                     bx = fmaf(dx, mr3, bx);
@@ -1194,7 +1197,7 @@ __device__ void tiny_hold(const EParams& E, const int32_t* S, int n, int level0,
                             const float dy = ds_diff(A.y, B.y, Ai.y, Bi.y);
                             const float dz = ds_diff(A.z, B.z, Ai.z, Bi.z);
                             const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, E.eps2f)));
-                            const float ri = rsqrt_nr(d2);
+                            const float ri = rsqrtf(d2);
                             const float mr3 = (d2 > 0.0f) ? A.w * ri * ri * ri : 0.0f;
                             a[0] = fmaf(dx, mr3, a[0]);
                             a[1] = fmaf(dy, mr3, a[1]);
@@ -1398,7 +1401,7 @@ __device__ __forceinline__ void acc_over(const EParams& E, const MidState& M, co
         const float dy = ds_diff(A.y, B.y, Ai.y, Bi.y);
         const float dz = ds_diff(A.z, B.z, Ai.z, Bi.z);
         const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, E.eps2f)));
-        const float ri = rsqrt_nr(d2);
+        const float ri = rsqrtf(d2);
         const float mr3 = (d2 > 0.0f) ? A.w * ri * ri * ri : 0.0f;
         a[0] = fmaf(dx, mr3, a[0]);
         a[1] = fmaf(dy, mr3, a[1]);
@@ -1596,7 +1599,7 @@ __device__ void warp_subtree(const EParams& E, MidState& M, const unsigned* memw
                             const float dy = ds_diff(A.y, B.y, Ai.y, Bi.y);
                             const float dz = ds_diff(A.z, B.z, Ai.z, Bi.z);
                             const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, E.eps2f)));
-                            const float ri = rsqrt_nr(d2);
+                            const float ri = rsqrtf(d2);
                             const float mr3 = (d2 > 0.0f) ? A.w * ri * ri * ri : 0.0f;
                             a[0] = fmaf(dx, mr3, a[0]);
                             a[1] = fmaf(dy, mr3, a[1]);
