@@ -63,6 +63,130 @@ __global__ void __launch_bounds__(kScanBlock, 6)
     if (SELF_RESET && scan_finish_is_last(hdr, num_tiles, &s_last)) scan_reset(hdr, epoch);
 }
 
+// Two-pass form for large inputs: the first kernel sums contiguous chunks of whole tiles
+// (one chunk per CTA, a few CTAs per SM), the second gives each CTA the sum of the chunks
+// before its own and scans its chunk tile by tile, carrying the running total. 12 bytes
+// of traffic per value instead of 8, but no look-back: the single-pass form is limited
+// by how fast the inclusive prefixes propagate through hundreds of resident tiles, and
+// loses to this beyond a few million values.
+constexpr int kChunkCtasPerSm = 4;
+constexpr long long kTwoPassMinN = 1LL << 22;
+
+template <bool VEC>
+__global__ void __launch_bounds__(kScanBlock)
+    k_chunk_reduce(const int32_t* __restrict__ in, long long n, long long chunk,
+                   unsigned* __restrict__ agg) {
+    __shared__ unsigned s_red[kScanBlock / 32];
+    const long long b = (long long)blockIdx.x * chunk;
+    const long long e = min(n, b + chunk);
+    unsigned a0 = 0u, a1 = 0u, a2 = 0u, a3 = 0u;
+    if (VEC) {
+        const long long nv = (e - b) / 4;  // b is a multiple of 4
+        const int4* v = reinterpret_cast<const int4*>(in + b);
+        for (long long k = threadIdx.x; k < nv; k += kScanBlock) {
+            const int4 q = __ldcs(v + k);
+            a0 += (unsigned)q.x; a1 += (unsigned)q.y; a2 += (unsigned)q.z; a3 += (unsigned)q.w;
+        }
+        for (long long k = b + nv * 4 + threadIdx.x; k < e; k += kScanBlock) a0 += (unsigned)in[k];
+    } else {
+        for (long long k = b + threadIdx.x; k < e; k += kScanBlock) a0 += (unsigned)in[k];
+    }
+    unsigned t = (unsigned)warp_sum((int)(a0 + a1 + a2 + a3));
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned sum = 0u;
+#pragma unroll
+        for (int w = 0; w < kScanBlock / 32; w++) sum += s_red[w];
+        agg[blockIdx.x] = sum;
+    }
+}
+
+template <bool VEC>
+__global__ void __launch_bounds__(kScanBlock)
+    k_chunk_scan(const int32_t* __restrict__ in, int32_t* __restrict__ out, long long n,
+                 long long chunk, const unsigned* __restrict__ agg) {
+    __shared__ unsigned s_warp[ScanT::WARPS], s_red[ScanT::WARPS];
+    __shared__ unsigned s_total;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // offset of this chunk: sum of the chunks before it
+    unsigned part = 0u;
+    for (int c = threadIdx.x; c < (int)blockIdx.x; c += kScanBlock) part += agg[c];
+    part = (unsigned)warp_sum((int)part);
+    if (lane == 0) s_red[warp] = part;
+    __syncthreads();
+    unsigned offset = 0u;
+#pragma unroll
+    for (int w = 0; w < ScanT::WARPS; w++) offset += s_red[w];
+    const long long b = (long long)blockIdx.x * chunk;
+    const long long e = min(n, b + chunk);
+    for (long long tbase = b; tbase < e; tbase += ScanT::TILE) {
+        unsigned v[kScanItems], cbase[ScanT::CHUNKS];
+#pragma unroll
+        for (int c = 0; c < ScanT::CHUNKS; c++) {
+            const long long el = tbase + ScanT::offset(warp, c, lane);
+            if (VEC && el + 4 <= e) {
+                const int4 q = __ldcs(reinterpret_cast<const int4*>(in + el));
+                v[4 * c] = q.x; v[4 * c + 1] = q.y; v[4 * c + 2] = q.z; v[4 * c + 3] = q.w;
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; k++) v[4 * c + k] = (el + k < e) ? (unsigned)in[el + k] : 0u;
+            }
+        }
+        unsigned run = 0u;
+#pragma unroll
+        for (int c = 0; c < ScanT::CHUNKS; c++) {
+            const unsigned sc = v[4 * c] + v[4 * c + 1] + v[4 * c + 2] + v[4 * c + 3];
+            const unsigned inc = (unsigned)warp_incl_scan((int)sc, lane);
+            cbase[c] = run + inc - sc;
+            run += (unsigned)__shfl_sync(HHS_FULL_MASK, (int)inc, 31);
+        }
+        if (lane == 0) s_warp[warp] = run;
+        __syncthreads();
+        if (warp == 0) {
+            const unsigned wt = lane < ScanT::WARPS ? s_warp[lane] : 0u;
+            const unsigned wi = (unsigned)warp_incl_scan((int)wt, lane);
+            if (lane < ScanT::WARPS) s_warp[lane] = wi - wt;
+            if (lane == 31) s_total = wi;
+        }
+        __syncthreads();
+        const unsigned base = offset + s_warp[warp];
+#pragma unroll
+        for (int c = 0; c < ScanT::CHUNKS; c++) {
+            const long long el = tbase + ScanT::offset(warp, c, lane);
+            const unsigned p0 = base + cbase[c], p1 = p0 + v[4 * c], p2 = p1 + v[4 * c + 1],
+                           p3 = p2 + v[4 * c + 2];
+            if (VEC && el + 4 <= e) {
+                __stcs(reinterpret_cast<int4*>(out + el),
+                       make_int4((int)p0, (int)p1, (int)p2, (int)p3));
+            } else {
+                const unsigned pp[4] = {p0, p1, p2, p3};
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (el + k < e) out[el + k] = (int)pp[k];
+            }
+        }
+        offset += s_total;
+        __syncthreads();
+    }
+}
+
+// chunks of whole tiles for the two-pass form; returns the chunk count
+int chunk_plan(long long n, long long* chunk) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 1;
+    }
+    const long long tiles = (n + ScanT::TILE - 1) / ScanT::TILE;
+    const long long want = (long long)sms * kChunkCtasPerSm;
+    const long long per = (tiles + want - 1) / want;
+    *chunk = per * ScanT::TILE;
+    return (int)((n + *chunk - 1) / *chunk);
+}
+
 // Launch-shape variants of the standalone scan (tile = BLOCK x ITEMS values, look-back
 // windows of 32 x LB tiles, at least MINB resident CTAs per SM), selected by
 // scan_variant(); the default shape is variant 0.
@@ -327,8 +451,24 @@ extern "C" hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out
         case 4: launch_scan_v<512, 16, 1, 1>(d_in, d_out, n, d_workspace, vec, s); break;
         case 5: launch_scan_v<256, 32, 1, 1>(d_in, d_out, n, d_workspace, vec, s); break;
         case 6: launch_scan_v<256, 8, 1, 8>(d_in, d_out, n, d_workspace, vec, s); break;
+        case 7: launch_scan_v<256, 16, 2, 6>(d_in, d_out, n, d_workspace, vec, s); break;
+        case 8: launch_scan_v<256, 16, 4, 6>(d_in, d_out, n, d_workspace, vec, s); break;
+        case 9: launch_scan_v<256, 16, 8, 6>(d_in, d_out, n, d_workspace, vec, s); break;
+        case 10: launch_scan_v<256, 32, 4, 3>(d_in, d_out, n, d_workspace, vec, s); break;
         default:
-            if (vec)
+            if (n >= kTwoPassMinN) {
+                // two passes; the chunk sums live where the look-back words would
+                long long chunk = 0;
+                const int nc = chunk_plan(n, &chunk);
+                auto* agg = reinterpret_cast<unsigned*>(status);
+                if (vec) {
+                    k_chunk_reduce<true><<<nc, kScanBlock, 0, s>>>(d_in, n, chunk, agg);
+                    k_chunk_scan<true><<<nc, kScanBlock, 0, s>>>(d_in, d_out, n, chunk, agg);
+                } else {
+                    k_chunk_reduce<false><<<nc, kScanBlock, 0, s>>>(d_in, n, chunk, agg);
+                    k_chunk_scan<false><<<nc, kScanBlock, 0, s>>>(d_in, d_out, n, chunk, agg);
+                }
+            } else if (vec)
                 k_scan_exclusive_i32<true, false><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n,
                                                                                hdr, status, tiles);
             else
