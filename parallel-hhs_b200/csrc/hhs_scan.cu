@@ -72,7 +72,8 @@ __global__ void __launch_bounds__(kScanBlock, 6)
 constexpr int kChunkCtasPerSm = 4;
 constexpr long long kTwoPassMinN = 1LL << 22;
 
-template <bool VEC>
+// FLAGS: the values are (in != 0) (stream compaction)
+template <bool VEC, bool FLAGS>
 __global__ void __launch_bounds__(kScanBlock)
     k_chunk_reduce(const int32_t* __restrict__ in, long long n, long long chunk,
                    unsigned* __restrict__ agg) {
@@ -85,11 +86,17 @@ __global__ void __launch_bounds__(kScanBlock)
         const int4* v = reinterpret_cast<const int4*>(in + b);
         for (long long k = threadIdx.x; k < nv; k += kScanBlock) {
             const int4 q = __ldcs(v + k);
-            a0 += (unsigned)q.x; a1 += (unsigned)q.y; a2 += (unsigned)q.z; a3 += (unsigned)q.w;
+            if (FLAGS) {
+                a0 += q.x != 0; a1 += q.y != 0; a2 += q.z != 0; a3 += q.w != 0;
+            } else {
+                a0 += (unsigned)q.x; a1 += (unsigned)q.y; a2 += (unsigned)q.z; a3 += (unsigned)q.w;
+            }
         }
-        for (long long k = b + nv * 4 + threadIdx.x; k < e; k += kScanBlock) a0 += (unsigned)in[k];
+        for (long long k = b + nv * 4 + threadIdx.x; k < e; k += kScanBlock)
+            a0 += FLAGS ? (unsigned)(in[k] != 0) : (unsigned)in[k];
     } else {
-        for (long long k = b + threadIdx.x; k < e; k += kScanBlock) a0 += (unsigned)in[k];
+        for (long long k = b + threadIdx.x; k < e; k += kScanBlock)
+            a0 += FLAGS ? (unsigned)(in[k] != 0) : (unsigned)in[k];
     }
     unsigned t = (unsigned)warp_sum((int)(a0 + a1 + a2 + a3));
     if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = t;
@@ -102,10 +109,13 @@ __global__ void __launch_bounds__(kScanBlock)
     }
 }
 
-template <bool VEC>
+// FLAGS: scan of (in != 0); the indices of the nonzero values go to idx_out[scan] and the
+// last chunk writes their number to *count (out, the scan itself, may then be null)
+template <bool VEC, bool FLAGS>
 __global__ void __launch_bounds__(kScanBlock)
     k_chunk_scan(const int32_t* __restrict__ in, int32_t* __restrict__ out, long long n,
-                 long long chunk, const unsigned* __restrict__ agg) {
+                 long long chunk, const unsigned* __restrict__ agg,
+                 int32_t* __restrict__ idx_out, int32_t* __restrict__ count) {
     __shared__ unsigned s_warp[ScanT::WARPS], s_red[ScanT::WARPS];
     __shared__ unsigned s_total;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -132,6 +142,10 @@ __global__ void __launch_bounds__(kScanBlock)
 #pragma unroll
                 for (int k = 0; k < 4; k++) v[4 * c + k] = (el + k < e) ? (unsigned)in[el + k] : 0u;
             }
+            if (FLAGS) {
+#pragma unroll
+                for (int k = 0; k < 4; k++) v[4 * c + k] = v[4 * c + k] != 0u;
+            }
         }
         unsigned run = 0u;
 #pragma unroll
@@ -156,19 +170,28 @@ __global__ void __launch_bounds__(kScanBlock)
             const long long el = tbase + ScanT::offset(warp, c, lane);
             const unsigned p0 = base + cbase[c], p1 = p0 + v[4 * c], p2 = p1 + v[4 * c + 1],
                            p3 = p2 + v[4 * c + 2];
-            if (VEC && el + 4 <= e) {
-                __stcs(reinterpret_cast<int4*>(out + el),
-                       make_int4((int)p0, (int)p1, (int)p2, (int)p3));
-            } else {
+            if (!FLAGS || out) {
+                if (VEC && el + 4 <= e) {
+                    __stcs(reinterpret_cast<int4*>(out + el),
+                           make_int4((int)p0, (int)p1, (int)p2, (int)p3));
+                } else {
+                    const unsigned pp[4] = {p0, p1, p2, p3};
+#pragma unroll
+                    for (int k = 0; k < 4; k++)
+                        if (el + k < e) out[el + k] = (int)pp[k];
+                }
+            }
+            if (FLAGS) {
                 const unsigned pp[4] = {p0, p1, p2, p3};
 #pragma unroll
                 for (int k = 0; k < 4; k++)
-                    if (el + k < e) out[el + k] = (int)pp[k];
+                    if (v[4 * c + k]) idx_out[pp[k]] = (int)(el + k);
             }
         }
         offset += s_total;
         __syncthreads();
     }
+    if (FLAGS && e == n && threadIdx.x == 0) *count = (int)offset;
 }
 
 // chunks of whole tiles for the two-pass form; returns the chunk count
@@ -462,11 +485,13 @@ extern "C" hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out
                 const int nc = chunk_plan(n, &chunk);
                 auto* agg = reinterpret_cast<unsigned*>(status);
                 if (vec) {
-                    k_chunk_reduce<true><<<nc, kScanBlock, 0, s>>>(d_in, n, chunk, agg);
-                    k_chunk_scan<true><<<nc, kScanBlock, 0, s>>>(d_in, d_out, n, chunk, agg);
+                    k_chunk_reduce<true, false><<<nc, kScanBlock, 0, s>>>(d_in, n, chunk, agg);
+                    k_chunk_scan<true, false><<<nc, kScanBlock, 0, s>>>(d_in, d_out, n, chunk,
+                                                                       agg, nullptr, nullptr);
                 } else {
-                    k_chunk_reduce<false><<<nc, kScanBlock, 0, s>>>(d_in, n, chunk, agg);
-                    k_chunk_scan<false><<<nc, kScanBlock, 0, s>>>(d_in, d_out, n, chunk, agg);
+                    k_chunk_reduce<false, false><<<nc, kScanBlock, 0, s>>>(d_in, n, chunk, agg);
+                    k_chunk_scan<false, false><<<nc, kScanBlock, 0, s>>>(d_in, d_out, n, chunk,
+                                                                        agg, nullptr, nullptr);
                 }
             } else if (vec)
                 k_scan_exclusive_i32<true, false><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n,
@@ -500,7 +525,20 @@ extern "C" hhs_status hhs_compact_flags_i32(const int32_t* d_flags, int32_t* d_s
                                                          sizeof(ScanHeader));
     const bool vec = ((reinterpret_cast<uintptr_t>(d_flags) |
                        reinterpret_cast<uintptr_t>(d_scan)) & 15u) == 0;
-    if (vec)
+    if (n >= kTwoPassMinN) {
+        long long chunk = 0;
+        const int nc = chunk_plan(n, &chunk);
+        auto* agg = reinterpret_cast<unsigned*>(status);
+        if (vec) {
+            k_chunk_reduce<true, true><<<nc, kScanBlock, 0, s>>>(d_flags, n, chunk, agg);
+            k_chunk_scan<true, true><<<nc, kScanBlock, 0, s>>>(d_flags, d_scan, n, chunk, agg,
+                                                               d_idx, d_count);
+        } else {
+            k_chunk_reduce<false, true><<<nc, kScanBlock, 0, s>>>(d_flags, n, chunk, agg);
+            k_chunk_scan<false, true><<<nc, kScanBlock, 0, s>>>(d_flags, d_scan, n, chunk, agg,
+                                                                d_idx, d_count);
+        }
+    } else if (vec)
         k_compact_flags<true, false><<<tiles, kScanBlock, 0, s>>>(d_flags, d_scan, d_idx,
                                                                   d_count, n, hdr, status, tiles);
     else
