@@ -45,7 +45,7 @@ def parse():
     p.add_argument("--small-n", type=int, default=64,
                    help="device schedule: nodes with n <= this are solved by one CTA")
     p.add_argument("--ctas-per-sm", type=int, default=2)
-    p.add_argument("--cluster-size", type=int, default=2,
+    p.add_argument("--cluster-size", type=int, default=4,
                    help="launch the HOLD kernel in thread-block clusters of this size")
     p.add_argument("--mid-n", type=int, default=640,
                    help="subtrees of at most this many particles run from shared memory on "

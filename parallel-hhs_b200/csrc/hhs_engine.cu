@@ -2235,7 +2235,7 @@ struct EngineHost {
     int small_n = 64;
     int units_per_cta = 16;
     int warp_n = 32;
-    int cluster_size = 2;
+    int cluster_size = 4;
     int mid_n = 640;
     int mid_dist_n = 96;
     int packed = 0;
