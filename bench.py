@@ -402,7 +402,7 @@ def run_ours(a, rank, world, torch, dist):
 
 # DRAM bytes of one k_engine launch of the default workload (dram__bytes_read.sum +
 # dram__bytes_write.sum of an ncu capture of one launch after three warm-up launches)
-ENGINE_16K_DRAM_BYTES = 1.419008e6 + 1.335808e6
+ENGINE_16K_DRAM_BYTES = 1.456128e6 + 1.422080e6
 
 
 def roofline(res, a, peaks_tflops):
