@@ -32,7 +32,8 @@ typedef enum {
     HHS_ERR_TIMEOUT = 4,             /* a bounded device wait gave up */
     HHS_ERR_DEVICE_FAULT_FLAG = 5,   /* a device-side check recorded an error word */
     HHS_ERR_DEPTH = 6,               /* hierarchy deeper than the context's level capacity */
-    HHS_ERR_CAPACITY = 7             /* n larger than the object was created for */
+    HHS_ERR_CAPACITY = 7,            /* n larger than the object was created for */
+    HHS_ERR_PEER = 8                 /* a peer rank failed or missed a barrier (multi-GPU) */
 } hhs_status;
 
 typedef enum { HHS_PREC_FP64 = 0, HHS_PREC_MIXED = 1 } hhs_precision;
@@ -200,8 +201,56 @@ hhs_status hhs_hold_integrate(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n,
 hhs_status hhs_hold_step_host(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n, double dt,
                               int32_t calc_timestep, hhs_precision prec, void* stream);
 
+/* ---- one system on several GPUs (sink-partitioned kick) --------------------------- */
+/* Every rank (one per GPU) holds a full replica of the system and runs the host-driven
+ * schedule of hhs_hold_step_host on it. Each timestep and kick launch of at least
+ * min_pairs pair terms is split by sink across the ranks: a rank computes its shard of
+ * the sinks and its kernel stores every result both locally and straight into each
+ * peer replica (P2P stores over NVLink), so the launch is the all-gather. A barrier
+ * before the launch (no peer still reads the old values) and one after it (every
+ * store has landed) bracket each shared launch. Everything else (splits, drifts, small
+ * levels) runs replicated and bit-identically on every rank, so all replicas stay
+ * equal, and equal to hhs_hold_step_host on one GPU: per sink, a shard computes the
+ * same operations in the same order as the whole launch.
+ *
+ * The barrier is the host's: hhs_barrier_fn(user, stream) must return 0 once the work
+ * enqueued on `stream` by every rank before the call is complete before any rank's
+ * later work starts (an NCCL all-reduce of one value on the stream, or a stream
+ * synchronise followed by a host barrier), or non-zero if a peer failed or did not
+ * arrive in time, which ends the step with HHS_ERR_PEER. Every rank takes the same
+ * barrier steps in the same order. */
+typedef int32_t (*hhs_barrier_fn)(void* user, void* stream);
+typedef struct hhs_dist hhs_dist;
+#define HHS_DIST_MAX_RANKS 8
+/* replicas[world]: each rank's system, as this process addresses it (a peer's arrays
+ * opened with hhs_ipc_open, or the systems themselves when the ranks share a process);
+ * replicas[rank] is not used. All replicas have the same capacity. */
+hhs_status hhs_dist_create(hhs_dist** out, int32_t rank, int32_t world,
+                           const hhs_particle_system* replicas, hhs_barrier_fn barrier,
+                           void* user, int64_t min_pairs);
+hhs_status hhs_dist_destroy(hhs_dist* d);
+/* Sink range [lo, hi) of `rank` for a launch whose first n_fast sinks cost n_slow pair
+ * terms each and whose other n_slow sinks cost n_slow + n_fast each (one kick of a split
+ * level; a timestep launch over n particles is n_fast = 0, n_slow = n): ranks get
+ * contiguous ranges of equal cost to within one sink. Host-only arithmetic. */
+hhs_status hhs_dist_shard(int32_t n_fast, int32_t n_slow, int32_t rank, int32_t world,
+                          int32_t* lo, int32_t* hi);
+/* One top-level step (hold_step, src/hold.cuh:51-181) of the rank's replica sys. */
+hhs_status hhs_hold_step_dist(hhs_ctx* ctx, hhs_dist* d, hhs_particle_system* sys, int32_t n,
+                              double dt, int32_t calc_timestep, hhs_precision prec,
+                              void* stream);
+/* Peer mappings of a system's device allocation (CUDA IPC): the handle is 64 bytes;
+ * hhs_ipc_open maps another process's system of capacity n into this one (peer access
+ * enabled) and fills a view whose arrays address it; close a view with hhs_ipc_close,
+ * never hhs_particle_system_free. */
+#define HHS_IPC_HANDLE_BYTES 64
+hhs_status hhs_ipc_handle(const hhs_particle_system* sys, void* handle_out);
+hhs_status hhs_ipc_open(const void* handle, int32_t n, hhs_particle_system* view_out);
+hhs_status hhs_ipc_close(hhs_particle_system* view);
+
 /* Exact exclusive prefix sum of int32 values (the contract of
- * scan_predicate_small/large, src/split.cuh:438-565) in one decoupled-lookback pass.
+ * scan_predicate_small/large, src/split.cuh:438-565): one decoupled-lookback pass below
+ * 2^22 values, two passes over chunks (chunk sums, then chunk scans) from there on.
  * d_workspace: hhs_scan_workspace_size(n) bytes of device memory (need not be zeroed;
  * the call clears what it uses). */
 size_t hhs_scan_workspace_size(int64_t n);
@@ -225,8 +274,8 @@ hhs_status hhs_scan_exclusive_i32_noalloc(const int32_t* d_in, int32_t* d_out, i
 
 /* Stream compaction (the split of a flag array, src/split.cuh:573-610 on int32 data):
  * d_idx[k] = index of the k-th nonzero flag, *d_count = number of nonzero flags, and
- * d_scan (optional, NULL = not written) = exclusive scan of (flag != 0). One pass;
- * workspace as for hhs_scan_exclusive_i32. */
+ * d_scan (optional, NULL = not written) = exclusive scan of (flag != 0). One pass below
+ * 2^22 flags, two from there on; workspace as for hhs_scan_exclusive_i32. */
 hhs_status hhs_compact_flags_i32(const int32_t* d_flags, int32_t* d_scan, int32_t* d_idx,
                                  int32_t* d_count, int64_t n, void* d_workspace,
                                  size_t workspace_bytes, void* stream);

@@ -110,21 +110,26 @@ extern "C" const char* hhs_status_string(hhs_status s) {
         case HHS_ERR_DEVICE_FAULT_FLAG: return "HHS_ERR_DEVICE_FAULT_FLAG";
         case HHS_ERR_DEPTH: return "HHS_ERR_DEPTH";
         case HHS_ERR_CAPACITY: return "HHS_ERR_CAPACITY";
+        case HHS_ERR_PEER: return "HHS_ERR_PEER";
     }
     return "HHS_ERR_UNKNOWN";
 }
 
 // ------------------------------------------------------------------ particle systems
-extern "C" hhs_status hhs_particle_system_alloc(hhs_particle_system* sys, int32_t n) {
-    if (!sys || n <= 0) return HHS_ERR_INVALID_ARG;
-    std::memset(sys, 0, sizeof(*sys));
+namespace {
+// One device allocation per system: x y z vx vy vz ts m, then ax ay az (3n contiguous
+// doubles), id, parent_id, each array 256-byte aligned. A peer mapping of the
+// allocation (hhs_ipc_open) is laid out by the same function.
+size_t system_bytes(int32_t n) {
     const size_t dbl = align_up(sizeof(double) * (size_t)n);
     const size_t acc3 = align_up(sizeof(double) * 3 * (size_t)n);
     const size_t i32 = align_up(sizeof(int32_t) * (size_t)n);
-    const size_t total = 8 * dbl + acc3 + 2 * i32;
-    void* base = nullptr;
-    cudaError_t e = cudaMalloc(&base, total);
-    if (e != cudaSuccess) return hhs_from_cuda(e);
+    return 8 * dbl + acc3 + 2 * i32;
+}
+void lay_out_system(hhs_particle_system* sys, void* base, int32_t n) {
+    const size_t dbl = align_up(sizeof(double) * (size_t)n);
+    const size_t acc3 = align_up(sizeof(double) * 3 * (size_t)n);
+    const size_t i32 = align_up(sizeof(int32_t) * (size_t)n);
     char* p = static_cast<char*>(base);
     double** f[8] = {&sys->x, &sys->y, &sys->z, &sys->vx, &sys->vy, &sys->vz, &sys->ts, &sys->m};
     for (int k = 0; k < 8; k++) { *f[k] = reinterpret_cast<double*>(p); p += dbl; }
@@ -136,6 +141,17 @@ extern "C" hhs_status hhs_particle_system_alloc(hhs_particle_system* sys, int32_
     sys->parent_id = reinterpret_cast<int32_t*>(p);
     sys->n = n;
     sys->_base = base;
+}
+}  // namespace
+
+extern "C" hhs_status hhs_particle_system_alloc(hhs_particle_system* sys, int32_t n) {
+    if (!sys || n <= 0) return HHS_ERR_INVALID_ARG;
+    std::memset(sys, 0, sizeof(*sys));
+    const size_t total = system_bytes(n);
+    void* base = nullptr;
+    cudaError_t e = cudaMalloc(&base, total);
+    if (e != cudaSuccess) return hhs_from_cuda(e);
+    lay_out_system(sys, base, n);
     e = cudaMemset(base, 0, total);
     if (e != cudaSuccess) { cudaFree(base); std::memset(sys, 0, sizeof(*sys)); return hhs_from_cuda(e); }
     return HHS_OK;
@@ -475,22 +491,88 @@ extern "C" hhs_status hhs_update_system(hhs_particle_system* prev,
                                 static_cast<cudaStream_t>(stream));
 }
 
+// ------------------------------------------------------------------ multi-GPU
+// One system on several GPUs: every rank holds a replica; the O(n^2) launches of the
+// host-driven schedule are split by sink and their kernels store each result into every
+// replica (PeerOut). No counterpart in the reference, which runs on one GPU.
+struct hhs_dist {
+    int rank = 0, world = 1;
+    int n_cap = 0;
+    SoA peer[kMaxPeers];  // the other ranks' replicas, in rank order
+    hhs_barrier_fn barrier = nullptr;
+    void* user = nullptr;
+    long long min_pairs = 0;
+};
+
+namespace {
+// First sink of rank r: the smallest s whose cumulative cost reaches r/world of the
+// total, sinks [0, nf) costing ns pair terms each and [nf, nf+ns) costing ns+nf.
+int shard_bound(long long nf, long long ns, int r, int world) {
+    const long long n = nf + ns;
+    if (r <= 0) return 0;
+    if (r >= world) return (int)n;
+    const __int128 cf = ns, cs = ns + nf;
+    const __int128 total = (__int128)nf * cf + (__int128)ns * cs;
+    if (total == 0) return (int)((__int128)n * r / world);
+    const __int128 target = total * r;  // cost(s) * world >= target
+    const __int128 fast_total = (__int128)nf * cf * world;
+    __int128 b;
+    if (cf > 0 && fast_total >= target) {
+        const __int128 q = cf * world;
+        b = (target + q - 1) / q;
+    } else {
+        const __int128 q = cs * world;
+        b = nf + (target - fast_total + q - 1) / q;
+    }
+    return (int)(b < n ? b : n);
+}
+
+// One sink-partitioned launch: barrier, this rank's shard (stores into every replica),
+// barrier. Every rank takes both barriers even with an empty shard.
+template <class Launch>
+hhs_status dist_launch(const hhs_dist* d, int n_fast, int n_slow, cudaStream_t s,
+                       Launch&& launch) {
+    PeerOut po = peer_out_local();
+    po.lo = shard_bound(n_fast, n_slow, d->rank, d->world);
+    po.hi = shard_bound(n_fast, n_slow, d->rank + 1, d->world);
+    po.n_peer = d->world - 1;
+    for (int r = 0; r < po.n_peer; r++) {
+        po.vx[r] = d->peer[r].vx; po.vy[r] = d->peer[r].vy; po.vz[r] = d->peer[r].vz;
+        po.ts[r] = d->peer[r].ts;
+    }
+    if (d->barrier(d->user, s) != 0) return HHS_ERR_PEER;
+    const hhs_status st = launch(po);
+    if (st != HHS_OK) return st;
+    if (d->barrier(d->user, s) != 0) return HHS_ERR_PEER;
+    return HHS_OK;
+}
+
+bool dist_shares(const hhs_dist* d, double pairs) {
+    return d && pairs >= (double)d->min_pairs;
+}
+
 // ------------------------------------------------------------------ host-driven HOLD
 // The schedule of src/hold.cuh:51-181 driven from the host: after each split the
 // partition counts are read back (the reference synchronises the device at the same
 // point, src/split.cuh:430) to decide the recursion. Level k's subsystem is the fast
-// list of level k-1 (the whole system at level 0).
-namespace {
+// list of level k-1 (the whole system at level 0). With d, the timestep and kick
+// launches of at least d->min_pairs pair terms are split across the ranks.
 hhs_status hold_host(hhs_ctx* c, const SoA& P, const int32_t* S, int n, int level, double dt,
-                     bool calc, hhs_precision prec, cudaStream_t s) {
+                     bool calc, hhs_precision prec, cudaStream_t s, const hhs_dist* d) {
     if (level >= c->max_levels) return HHS_ERR_DEPTH;
     auto* prof = static_cast<Profiler*>(c->prof);
     const bool timed = prof && prof->on;
     Profiler::Rec rec{};
     hhs_status st;
     if (calc) {
-        if (timed) prof->begin(rec, 0, (double)n * (double)(n - 1), s);
-        st = launch_timesteps(P, S, n, c->params.eta, prec, s);
+        const double pairs = (double)n * (double)(n - 1);
+        if (timed) prof->begin(rec, 0, pairs, s);
+        if (dist_shares(d, pairs))
+            st = dist_launch(d, 0, n, s, [&](const PeerOut& po) {
+                return launch_timesteps(P, S, n, c->params.eta, prec, s, po);
+            });
+        else
+            st = launch_timesteps(P, S, n, c->params.eta, prec, s);
         if (st != HHS_OK) return st;
         if (timed) prof->end(rec, s);
     }
@@ -508,7 +590,7 @@ hhs_status hold_host(hhs_ctx* c, const SoA& P, const int32_t* S, int n, int leve
     const int nf = c->host_counts[level].n_fast, ns = c->host_counts[level].n_slow;
     if (nf < 0 || ns < 0 || nf + ns != n) return HHS_ERR_DEVICE_FAULT_FLAG;
     if (nf > 0) {
-        st = hold_host(c, P, F, nf, level + 1, dt / 2, false, prec, s);
+        st = hold_host(c, P, F, nf, level + 1, dt / 2, false, prec, s, d);
         if (st != HHS_OK) return st;
     }
     if (ns > 0) {
@@ -516,14 +598,20 @@ hhs_status hold_host(hhs_ctx* c, const SoA& P, const int32_t* S, int n, int leve
         if (st != HHS_OK) return st;
         const double pairs = (double)ns * (ns - 1.0) + 2.0 * (double)ns * (double)nf;
         if (timed) prof->begin(rec, 1, pairs, s);
-        st = launch_kick_level(P, F, L, cnt, n, dt, c->params.eps * c->params.eps, prec, s);
+        const double eps2 = c->params.eps * c->params.eps;
+        if (dist_shares(d, pairs))
+            st = dist_launch(d, nf, ns, s, [&](const PeerOut& po) {
+                return launch_kick_level(P, F, L, cnt, n, dt, eps2, prec, s, po);
+            });
+        else
+            st = launch_kick_level(P, F, L, cnt, n, dt, eps2, prec, s);
         if (st != HHS_OK) return st;
         if (timed) prof->end(rec, s);
         st = launch_drift_slow(P, L, cnt, ns, dt * 0.5, s);
         if (st != HHS_OK) return st;
     }
     if (nf > 0) {
-        st = hold_host(c, P, F, nf, level + 1, dt / 2, true, prec, s);
+        st = hold_host(c, P, F, nf, level + 1, dt / 2, true, prec, s, d);
         if (st != HHS_OK) return st;
     }
     return HHS_OK;
@@ -536,9 +624,95 @@ extern "C" hhs_status hhs_hold_step_host(hhs_ctx* c, hhs_particle_system* sys, i
     if (!c || !sys_ok(sys) || n <= 0 || !(dt > 0.0)) return HHS_ERR_INVALID_ARG;
     if (n > sys->n || n > c->n_max) return HHS_ERR_CAPACITY;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    hhs_status st = hold_host(c, soa_of(sys), nullptr, n, 0, dt, calc_timestep != 0, prec, s);
+    hhs_status st = hold_host(c, soa_of(sys), nullptr, n, 0, dt, calc_timestep != 0, prec, s,
+                              nullptr);
     if (st != HHS_OK) return st;
     return hhs_ctx_check(c, stream);
+}
+
+extern "C" hhs_status hhs_dist_create(hhs_dist** out, int32_t rank, int32_t world,
+                                      const hhs_particle_system* replicas,
+                                      hhs_barrier_fn barrier, void* user, int64_t min_pairs) {
+    if (!out) return HHS_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (world < 1 || world > HHS_DIST_MAX_RANKS || world - 1 > kMaxPeers || rank < 0 ||
+        rank >= world || !barrier || min_pairs < 0 || (world > 1 && !replicas))
+        return HHS_ERR_INVALID_ARG;
+    int cap = 0;
+    for (int r = 0; r < world; r++) {
+        if (r == rank) continue;
+        const hhs_particle_system* p = &replicas[r];
+        if (!p->vx || !p->vy || !p->vz || !p->ts || p->n <= 0) return HHS_ERR_INVALID_ARG;
+        if (cap != 0 && p->n != cap) return HHS_ERR_INVALID_ARG;
+        cap = p->n;
+    }
+    auto* d = new (std::nothrow) hhs_dist;
+    if (!d) return HHS_ERR_OOM;
+    d->rank = rank;
+    d->world = world;
+    d->n_cap = cap;
+    int k = 0;
+    for (int r = 0; r < world; r++)
+        if (r != rank) d->peer[k++] = soa_of(&replicas[r]);
+    d->barrier = barrier;
+    d->user = user;
+    d->min_pairs = min_pairs;
+    *out = d;
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_dist_destroy(hhs_dist* d) {
+    delete d;
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_dist_shard(int32_t n_fast, int32_t n_slow, int32_t rank,
+                                     int32_t world, int32_t* lo, int32_t* hi) {
+    if (!lo || !hi || n_fast < 0 || n_slow < 0 || world < 1 || rank < 0 || rank >= world ||
+        (long long)n_fast + n_slow > 0x7fffffffLL)
+        return HHS_ERR_INVALID_ARG;
+    *lo = shard_bound(n_fast, n_slow, rank, world);
+    *hi = shard_bound(n_fast, n_slow, rank + 1, world);
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_hold_step_dist(hhs_ctx* c, hhs_dist* d, hhs_particle_system* sys,
+                                         int32_t n, double dt, int32_t calc_timestep,
+                                         hhs_precision prec, void* stream) {
+    if (!c || !d || !sys_ok(sys) || n <= 0 || !(dt > 0.0)) return HHS_ERR_INVALID_ARG;
+    if (n > sys->n || n > c->n_max || (d->world > 1 && n > d->n_cap)) return HHS_ERR_CAPACITY;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    hhs_status st = hold_host(c, soa_of(sys), nullptr, n, 0, dt, calc_timestep != 0, prec, s, d);
+    if (st != HHS_OK) return st;
+    return hhs_ctx_check(c, stream);
+}
+
+static_assert(sizeof(cudaIpcMemHandle_t) == HHS_IPC_HANDLE_BYTES, "IPC handle size");
+
+extern "C" hhs_status hhs_ipc_handle(const hhs_particle_system* sys, void* handle_out) {
+    if (!sys_ok(sys) || !handle_out) return HHS_ERR_INVALID_ARG;
+    cudaIpcMemHandle_t h;
+    HHS_CUDA_TRY(cudaIpcGetMemHandle(&h, sys->_base));
+    std::memcpy(handle_out, &h, sizeof(h));
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_ipc_open(const void* handle, int32_t n, hhs_particle_system* view_out) {
+    if (!handle || !view_out || n <= 0) return HHS_ERR_INVALID_ARG;
+    std::memset(view_out, 0, sizeof(*view_out));
+    cudaIpcMemHandle_t h;
+    std::memcpy(&h, handle, sizeof(h));
+    void* base = nullptr;
+    HHS_CUDA_TRY(cudaIpcOpenMemHandle(&base, h, cudaIpcMemLazyEnablePeerAccess));
+    lay_out_system(view_out, base, n);
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_ipc_close(hhs_particle_system* view) {
+    if (!view || !view->_base) return HHS_ERR_INVALID_ARG;
+    const cudaError_t e = cudaIpcCloseMemHandle(view->_base);
+    std::memset(view, 0, sizeof(*view));
+    return e == cudaSuccess ? HHS_OK : hhs_from_cuda(e);
 }
 
 extern "C" hhs_status hhs_hold_step(hhs_ctx* c, int32_t clevel, hhs_particle_system* sys,

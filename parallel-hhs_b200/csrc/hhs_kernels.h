@@ -17,15 +17,35 @@ hhs_status launch_split_list(const int32_t* list_in, int n, const double* ts, do
                              cudaStream_t stream);
 
 // ---- pair kernels, drift, gathers (hhs_pairs.cu)
+// Sink-partitioned launch of a pair kernel (the multi-GPU HOLD step): only sinks
+// [lo, hi) of the launch's sink index space are computed, and every result is stored
+// both in the local arrays and in each peer replica's arrays (P2P stores over NVLink,
+// or plain stores when the replicas share a device). hi < 0 selects every sink and
+// n_peer = 0 writes the local arrays only: the single-GPU launch.
+constexpr int kMaxPeers = 7;  // an 8-GPU NVSwitch node
+struct PeerOut {
+    int lo, hi, n_peer;
+    double* vx[kMaxPeers];
+    double* vy[kMaxPeers];
+    double* vz[kMaxPeers];
+    double* ts[kMaxPeers];
+};
+inline PeerOut peer_out_local() {
+    PeerOut p{};
+    p.lo = 0; p.hi = -1; p.n_peer = 0;
+    return p;
+}
 // Timesteps of the subsystem given by list (identity when nullptr), min over j != i.
 hhs_status launch_timesteps(const SoA& P, const int32_t* list, int n, double eta,
-                            hhs_precision prec, cudaStream_t stream);
+                            hhs_precision prec, cudaStream_t stream,
+                            const PeerOut& po = peer_out_local());
 // One HOLD kick of a split level: slow sinks get slow then fast sources, fast sinks get
-// slow sources; v += a*dt. Counts are read from the device (n_max bounds the grid).
+// slow sources; v += a*dt. Counts are read from the device (n_max bounds the grid). The
+// sink index space is the fast list, then the slow list.
 hhs_status launch_kick_level(const SoA& P, const int32_t* fast_list,
                              const int32_t* slow_list, const hhs_partition* counts,
                              int n_max, double dt, double eps2, hhs_precision prec,
-                             cudaStream_t stream);
+                             cudaStream_t stream, const PeerOut& po = peer_out_local());
 // Standalone kick: sinks = sink[0..n_sink), sources = src[0..n_src); acc written.
 hhs_status launch_kick_pair(const SoA& sink, double* ax, double* ay, double* az,
                             const SoA& src, int n_sink, int n_src, double dtfac,

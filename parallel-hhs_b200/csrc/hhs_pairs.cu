@@ -19,14 +19,30 @@ constexpr double kHuge = 1.e30;  // src/timestep.cuh:4
 
 __device__ __forceinline__ int list_at(const int32_t* list, int i) { return list ? list[i] : i; }
 
+// The stores of a sink-partitioned launch into the peer replicas, then a system-scope
+// fence so that the barrier which follows the launch orders them for every peer.
+__device__ __forceinline__ void peer_store_ts(const PeerOut& po, int g, double t) {
+    if (po.n_peer == 0) return;
+    for (int r = 0; r < po.n_peer; r++) po.ts[r][g] = t;
+    __threadfence_system();
+}
+__device__ __forceinline__ void peer_store_v(const PeerOut& po, int g, double vx, double vy,
+                                             double vz) {
+    if (po.n_peer == 0) return;
+    for (int r = 0; r < po.n_peer; r++) {
+        po.vx[r][g] = vx; po.vy[r][g] = vy; po.vz[r][g] = vz;
+    }
+    __threadfence_system();
+}
+
 // ---------------------------------------------------------------- timesteps, FP64
 __global__ void __launch_bounds__(kTsBlock)
     k_timesteps_fp64(SoA P, const int32_t* __restrict__ list, int n, double eta,
-                     double eta_s2) {
+                     double eta_s2, PeerOut po) {
     __shared__ double sx[kTsBlock], sy[kTsBlock], sz[kTsBlock];
     __shared__ double svx[kTsBlock], svy[kTsBlock], svz[kTsBlock], sm[kTsBlock];
-    const int i = blockIdx.x * kTsBlock + threadIdx.x;
-    const bool active = i < n;
+    const int i = po.lo + blockIdx.x * kTsBlock + threadIdx.x;
+    const bool active = i < (po.hi < 0 ? n : po.hi);
     const int gi = active ? list_at(list, i) : 0;
     double xi = 0, yi = 0, zi = 0, vxi = 0, vyi = 0, vzi = 0, mi = 0;
     if (active) {
@@ -55,18 +71,21 @@ __global__ void __launch_bounds__(kTsBlock)
         }
         __syncthreads();
     }
-    if (active) P.ts[gi] = minval;
+    if (active) {
+        P.ts[gi] = minval;
+        peer_store_ts(po, gi, minval);
+    }
 }
 
 // ---------------------------------------------------------------- timesteps, mixed
 __global__ void __launch_bounds__(kTsBlock)
     k_timesteps_mixed(SoA P, const int32_t* __restrict__ list, int n, float inv_eta_s2,
-                      float inv_eta) {
+                      float inv_eta, PeerOut po) {
     __shared__ float4 sA[kTsBlock];  // xh, yh, zh, m
     __shared__ float4 sB[kTsBlock];  // xl, yl, zl, -
     __shared__ float4 sV[kTsBlock];  // vx, vy, vz, -
-    const int i = blockIdx.x * kTsBlock + threadIdx.x;
-    const bool active = i < n;
+    const int i = po.lo + blockIdx.x * kTsBlock + threadIdx.x;
+    const bool active = i < (po.hi < 0 ? n : po.hi);
     const int gi = active ? list_at(list, i) : 0;
     DS xi{0, 0}, yi{0, 0}, zi{0, 0};
     float vxi = 0, vyi = 0, vzi = 0, mi = 0;
@@ -102,8 +121,10 @@ __global__ void __launch_bounds__(kTsBlock)
         __syncthreads();
     }
     if (active) {
-        const double t = 1.0 / (double)maxrate;
-        P.ts[gi] = (t < kHuge) ? t : kHuge;
+        double t = 1.0 / (double)maxrate;
+        t = (t < kHuge) ? t : kHuge;
+        P.ts[gi] = t;
+        peer_store_ts(po, gi, t);
     }
 }
 
@@ -114,13 +135,15 @@ __global__ void __launch_bounds__(kTsBlock)
 // src/hold.cuh:138,142); fast sinks apply v += aFL*dt (kick_sf(slow->fast), :143).
 __global__ void __launch_bounds__(kKickBlock)
     k_kick_level_fp64(SoA P, const int32_t* __restrict__ F, const int32_t* __restrict__ L,
-                      const hhs_partition* __restrict__ counts, double dt, double eps2) {
+                      const hhs_partition* __restrict__ counts, double dt, double eps2,
+                      PeerOut po) {
     __shared__ double sx[kKickBlock], sy[kKickBlock], sz[kKickBlock], sm[kKickBlock];
     const int nf = counts->n_fast, ns = counts->n_slow, n = nf + ns;
     if (ns == 0) return;
-    if ((int)(blockIdx.x * kKickBlock) >= n) return;
-    const int s = blockIdx.x * kKickBlock + threadIdx.x;
-    const bool active = s < n;
+    const int hi = po.hi < 0 ? n : min(po.hi, n);
+    if (po.lo + (int)(blockIdx.x * kKickBlock) >= hi) return;
+    const int s = po.lo + blockIdx.x * kKickBlock + threadIdx.x;
+    const bool active = s < hi;
     const bool slow_sink = s >= nf;
     const int g = active ? (slow_sink ? L[s - nf] : F[s]) : 0;
     const double xi = active ? P.x[g] : 0.0, yi = active ? P.y[g] : 0.0,
@@ -169,6 +192,7 @@ __global__ void __launch_bounds__(kKickBlock)
         vz = f64_add(vz, f64_mul(aFz, dt));
     }
     P.vx[g] = vx; P.vy[g] = vy; P.vz[g] = vz;
+    peer_store_v(po, g, vx, vy, vz);
 }
 
 // ---------------------------------------------------------------- kick, mixed
@@ -177,14 +201,16 @@ __global__ void __launch_bounds__(kKickBlock)
 // and fast source sums are kept apart so the update order matches the FP64 form.
 __global__ void __launch_bounds__(kKickBlock)
     k_kick_level_mixed(SoA P, const int32_t* __restrict__ F, const int32_t* __restrict__ L,
-                       const hhs_partition* __restrict__ counts, double dt, float eps2) {
+                       const hhs_partition* __restrict__ counts, double dt, float eps2,
+                       PeerOut po) {
     __shared__ float4 sA[kKickBlock];  // xh, yh, zh, m
     __shared__ float4 sB[kKickBlock];  // xl, yl, zl, -
     const int nf = counts->n_fast, ns = counts->n_slow, n = nf + ns;
     if (ns == 0) return;
-    if ((int)(blockIdx.x * kKickBlock) >= n) return;
-    const int s = blockIdx.x * kKickBlock + threadIdx.x;
-    const bool active = s < n;
+    const int hi = po.hi < 0 ? n : min(po.hi, n);
+    if (po.lo + (int)(blockIdx.x * kKickBlock) >= hi) return;
+    const int s = po.lo + blockIdx.x * kKickBlock + threadIdx.x;
+    const bool active = s < hi;
     const bool slow_sink = s >= nf;
     const int g = active ? (slow_sink ? L[s - nf] : F[s]) : 0;
     DS xi{0, 0}, yi{0, 0}, zi{0, 0};
@@ -231,6 +257,7 @@ __global__ void __launch_bounds__(kKickBlock)
         if (slow_sink && nf > 0) v[k] += ((double)acc[1][k] - (double)cmp[1][k]) * dt;
     }
     P.vx[g] = v[0]; P.vy[g] = v[1]; P.vz[g] = v[2];
+    peer_store_v(po, g, v[0], v[1], v[2]);
 }
 
 // ---------------------------------------------------------------- standalone kicks
@@ -372,15 +399,19 @@ inline int grid_stride(int n, int block) {
 }  // namespace
 
 hhs_status launch_timesteps(const SoA& P, const int32_t* list, int n, double eta,
-                            hhs_precision prec, cudaStream_t stream) {
+                            hhs_precision prec, cudaStream_t stream, const PeerOut& po) {
     if (n <= 0) return HHS_OK;
+    if (po.lo < 0 || po.n_peer < 0 || po.n_peer > kMaxPeers) return HHS_ERR_INVALID_ARG;
+    const int hi = po.hi < 0 ? n : po.hi;
+    if (hi > n || po.lo > hi) return HHS_ERR_INVALID_ARG;
+    if (hi == po.lo) return HHS_OK;  // an empty shard
     const double eta_s2 = eta / 1.41421356237309504880;  // eta / M_SQRT2
+    const int grid = grid_for(hi - po.lo, kTsBlock);
     if (prec == HHS_PREC_FP64)
-        k_timesteps_fp64<<<grid_for(n, kTsBlock), kTsBlock, 0, stream>>>(P, list, n, eta,
-                                                                          eta_s2);
+        k_timesteps_fp64<<<grid, kTsBlock, 0, stream>>>(P, list, n, eta, eta_s2, po);
     else
-        k_timesteps_mixed<<<grid_for(n, kTsBlock), kTsBlock, 0, stream>>>(
-            P, list, n, (float)(1.0 / eta_s2), (float)(1.0 / eta));
+        k_timesteps_mixed<<<grid, kTsBlock, 0, stream>>>(P, list, n, (float)(1.0 / eta_s2),
+                                                         (float)(1.0 / eta), po);
     HHS_LAUNCH_CHECK();
     return HHS_OK;
 }
@@ -388,14 +419,20 @@ hhs_status launch_timesteps(const SoA& P, const int32_t* list, int n, double eta
 hhs_status launch_kick_level(const SoA& P, const int32_t* fast_list,
                              const int32_t* slow_list, const hhs_partition* counts,
                              int n_max, double dt, double eps2, hhs_precision prec,
-                             cudaStream_t stream) {
+                             cudaStream_t stream, const PeerOut& po) {
     if (n_max <= 0) return HHS_OK;
+    if (po.lo < 0 || po.n_peer < 0 || po.n_peer > kMaxPeers) return HHS_ERR_INVALID_ARG;
+    // hi >= 0: a shard whose bounds the caller took from the host copy of the counts
+    const int hi = po.hi < 0 ? n_max : po.hi;
+    if (hi > n_max || po.lo > hi) return HHS_ERR_INVALID_ARG;
+    if (hi == po.lo) return HHS_OK;
+    const int grid = grid_for(hi - po.lo, kKickBlock);
     if (prec == HHS_PREC_FP64)
-        k_kick_level_fp64<<<grid_for(n_max, kKickBlock), kKickBlock, 0, stream>>>(
-            P, fast_list, slow_list, counts, dt, eps2);
+        k_kick_level_fp64<<<grid, kKickBlock, 0, stream>>>(P, fast_list, slow_list, counts, dt,
+                                                           eps2, po);
     else
-        k_kick_level_mixed<<<grid_for(n_max, kKickBlock), kKickBlock, 0, stream>>>(
-            P, fast_list, slow_list, counts, dt, (float)eps2);
+        k_kick_level_mixed<<<grid, kKickBlock, 0, stream>>>(P, fast_list, slow_list, counts, dt,
+                                                            (float)eps2, po);
     HHS_LAUNCH_CHECK();
     return HHS_OK;
 }

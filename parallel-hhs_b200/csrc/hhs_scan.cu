@@ -63,35 +63,48 @@ __global__ void __launch_bounds__(kScanBlock, 6)
     if (SELF_RESET && scan_finish_is_last(hdr, num_tiles, &s_last)) scan_reset(hdr, epoch);
 }
 
-// Two-pass form for large inputs: the first kernel sums contiguous chunks of whole tiles
-// (one chunk per CTA, a few CTAs per SM), the second gives each CTA the sum of the chunks
-// before its own and scans its chunk tile by tile, carrying the running total. 12 bytes
-// of traffic per value instead of 8, but no look-back: the single-pass form is limited
-// by how fast the inclusive prefixes propagate through hundreds of resident tiles, and
-// loses to this beyond a few million values.
+// Two-pass form for large inputs, over super-chunks of at most 2^24 values (64 MB, half
+// of L2): per super-chunk, the first kernel sums contiguous chunks of whole tiles (one
+// chunk per CTA, a few CTAs per SM), the second gives each CTA the sum of the chunks
+// before its own plus the running total of the earlier super-chunks and scans its chunk
+// tile by tile. The super-chunk is still in L2 when the second kernel reads it again, so
+// DRAM sees 8 bytes per value, and there is no look-back: the single-pass form is
+// limited by how fast the inclusive prefixes propagate through hundreds of resident
+// tiles, and loses to this beyond a few million values.
 constexpr int kChunkCtasPerSm = 4;
 constexpr long long kTwoPassMinN = 1LL << 22;
+constexpr long long kSuperChunk = 1LL << 24;
+constexpr int kCarryWord = 1024;  // carries live after the chunk sums (< 1024 chunks)
 
 // FLAGS: the values are (in != 0) (stream compaction)
 template <bool VEC, bool FLAGS>
 __global__ void __launch_bounds__(kScanBlock)
     k_chunk_reduce(const int32_t* __restrict__ in, long long n, long long chunk,
-                   unsigned* __restrict__ agg) {
+                   unsigned* __restrict__ agg, unsigned* __restrict__ clear_word) {
     __shared__ unsigned s_red[kScanBlock / 32];
+    if (clear_word && blockIdx.x == 0 && threadIdx.x == 0) *clear_word = 0u;
     const long long b = (long long)blockIdx.x * chunk;
     const long long e = min(n, b + chunk);
     unsigned a0 = 0u, a1 = 0u, a2 = 0u, a3 = 0u;
     if (VEC) {
+        // plain loads: the values stay in L2 for the scan pass; four 16-byte loads in
+        // flight per thread
         const long long nv = (e - b) / 4;  // b is a multiple of 4
         const int4* v = reinterpret_cast<const int4*>(in + b);
-        for (long long k = threadIdx.x; k < nv; k += kScanBlock) {
-            const int4 q = __ldcs(v + k);
+        auto add = [&](const int4 q) {
             if (FLAGS) {
                 a0 += q.x != 0; a1 += q.y != 0; a2 += q.z != 0; a3 += q.w != 0;
             } else {
                 a0 += (unsigned)q.x; a1 += (unsigned)q.y; a2 += (unsigned)q.z; a3 += (unsigned)q.w;
             }
+        };
+        long long k = threadIdx.x;
+        for (; k + 3 * kScanBlock < nv; k += 4 * kScanBlock) {
+            const int4 q0 = __ldg(v + k), q1 = __ldg(v + k + kScanBlock),
+                       q2 = __ldg(v + k + 2 * kScanBlock), q3 = __ldg(v + k + 3 * kScanBlock);
+            add(q0); add(q1); add(q2); add(q3);
         }
+        for (; k < nv; k += kScanBlock) add(__ldg(v + k));
         for (long long k = b + nv * 4 + threadIdx.x; k < e; k += kScanBlock)
             a0 += FLAGS ? (unsigned)(in[k] != 0) : (unsigned)in[k];
     } else {
@@ -109,18 +122,23 @@ __global__ void __launch_bounds__(kScanBlock)
     }
 }
 
-// FLAGS: scan of (in != 0); the indices of the nonzero values go to idx_out[scan] and the
-// last chunk writes their number to *count (out, the scan itself, may then be null)
+// One super-chunk [base, base + n) of the whole input: in and out point at its start.
+// carry_in (null: 0) is the total of the earlier super-chunks; the last chunk writes the
+// running total to carry_out and, for FLAGS, to *count.
+// FLAGS: scan of (in != 0); the indices of the nonzero values go to idx_out[scan] (out,
+// the scan itself, may then be null)
 template <bool VEC, bool FLAGS>
 __global__ void __launch_bounds__(kScanBlock)
     k_chunk_scan(const int32_t* __restrict__ in, int32_t* __restrict__ out, long long n,
                  long long chunk, const unsigned* __restrict__ agg,
-                 int32_t* __restrict__ idx_out, int32_t* __restrict__ count) {
+                 int32_t* __restrict__ idx_out, int32_t* __restrict__ count,
+                 const unsigned* __restrict__ carry_in, unsigned* __restrict__ carry_out,
+                 long long base) {
     __shared__ unsigned s_warp[ScanT::WARPS], s_red[ScanT::WARPS];
     __shared__ unsigned s_total;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // offset of this chunk: sum of the chunks before it
-    unsigned part = 0u;
+    // offset of this chunk: the earlier super-chunks, then the chunks before it
+    unsigned part = (carry_in && threadIdx.x == 0) ? *carry_in : 0u;
     for (int c = threadIdx.x; c < (int)blockIdx.x; c += kScanBlock) part += agg[c];
     part = (unsigned)warp_sum((int)part);
     if (lane == 0) s_red[warp] = part;
@@ -185,13 +203,16 @@ __global__ void __launch_bounds__(kScanBlock)
                 const unsigned pp[4] = {p0, p1, p2, p3};
 #pragma unroll
                 for (int k = 0; k < 4; k++)
-                    if (v[4 * c + k]) idx_out[pp[k]] = (int)(el + k);
+                    if (v[4 * c + k]) idx_out[pp[k]] = (int)(base + el + k);
             }
         }
         offset += s_total;
         __syncthreads();
     }
-    if (FLAGS && e == n && threadIdx.x == 0) *count = (int)offset;
+    if (e == n && threadIdx.x == 0) {
+        if (carry_out) *carry_out = offset;
+        if (FLAGS && count) *count = (int)offset;
+    }
 }
 
 // chunks of whole tiles for the two-pass form; returns the chunk count
@@ -208,6 +229,28 @@ int chunk_plan(long long n, long long* chunk) {
     const long long per = (tiles + want - 1) / want;
     *chunk = per * ScanT::TILE;
     return (int)((n + *chunk - 1) / *chunk);
+}
+
+// The two-pass form over the whole input (agg: the workspace's status words; the
+// header's error word is cleared by the first kernel).
+template <bool VEC, bool FLAGS>
+void launch_two_pass(const int32_t* in, int32_t* out, long long n, ScanHeader* hdr,
+                     unsigned* agg, int32_t* idx_out, int32_t* count, cudaStream_t s,
+                     long long super = kSuperChunk) {
+    unsigned* carry = agg + kCarryWord;
+    int k = 0;
+    for (long long base = 0; base < n; base += super, k++) {
+        const long long len = n - base < super ? n - base : super;
+        const bool last = base + len == n;
+        long long chunk = 0;
+        const int nc = chunk_plan(len, &chunk);
+        k_chunk_reduce<VEC, FLAGS><<<nc, kScanBlock, 0, s>>>(in + base, len, chunk, agg,
+                                                              k == 0 ? &hdr->error : nullptr);
+        k_chunk_scan<VEC, FLAGS><<<nc, kScanBlock, 0, s>>>(
+            in + base, out ? out + base : nullptr, len, chunk, agg, idx_out,
+            last ? count : nullptr, k > 0 ? carry + (k & 1) : nullptr,
+            last ? nullptr : carry + ((k + 1) & 1), base);
+    }
 }
 
 // Launch-shape variants of the standalone scan (tile = BLOCK x ITEMS values, look-back
@@ -461,13 +504,30 @@ extern "C" hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int tiles = (int)((n + ScanT::TILE - 1) / ScanT::TILE);
     const size_t used = scan_workspace_bytes(n, kScanMinTile);
-    HHS_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, used, s));
+    const int variant = scan_variant();
     auto* hdr = static_cast<ScanHeader*>(d_workspace);
     auto* status = reinterpret_cast<unsigned long long*>(static_cast<char*>(d_workspace) +
                                                          sizeof(ScanHeader));
     const bool vec = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) &
                       15u) == 0;
-    switch (scan_variant()) {
+    if ((variant == 0 || variant >= 11) && n >= kTwoPassMinN) {
+        // the chunk sums and carries are written before they are read: nothing to clear.
+        // Variants 11-14: super-chunks of 2^22, 2^23, 2^25 values, or one of n values.
+        const long long super = variant == 11   ? (1LL << 22)
+                                : variant == 12 ? (1LL << 23)
+                                : variant == 13 ? (1LL << 25)
+                                : variant == 14 ? n
+                                                : kSuperChunk;
+        auto* agg = reinterpret_cast<unsigned*>(status);
+        if (vec)
+            launch_two_pass<true, false>(d_in, d_out, n, hdr, agg, nullptr, nullptr, s, super);
+        else
+            launch_two_pass<false, false>(d_in, d_out, n, hdr, agg, nullptr, nullptr, s, super);
+        HHS_LAUNCH_CHECK();
+        return HHS_OK;
+    }
+    HHS_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, used, s));
+    switch (variant) {
         case 1: launch_scan_v<256, 8, 1, 1>(d_in, d_out, n, d_workspace, vec, s); break;
         case 2: launch_scan_v<128, 16, 1, 1>(d_in, d_out, n, d_workspace, vec, s); break;
         case 3: launch_scan_v<256, 16, 1, 6>(d_in, d_out, n, d_workspace, vec, s); break;
@@ -479,21 +539,7 @@ extern "C" hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out
         case 9: launch_scan_v<256, 16, 8, 6>(d_in, d_out, n, d_workspace, vec, s); break;
         case 10: launch_scan_v<256, 32, 4, 3>(d_in, d_out, n, d_workspace, vec, s); break;
         default:
-            if (n >= kTwoPassMinN) {
-                // two passes; the chunk sums live where the look-back words would
-                long long chunk = 0;
-                const int nc = chunk_plan(n, &chunk);
-                auto* agg = reinterpret_cast<unsigned*>(status);
-                if (vec) {
-                    k_chunk_reduce<true, false><<<nc, kScanBlock, 0, s>>>(d_in, n, chunk, agg);
-                    k_chunk_scan<true, false><<<nc, kScanBlock, 0, s>>>(d_in, d_out, n, chunk,
-                                                                       agg, nullptr, nullptr);
-                } else {
-                    k_chunk_reduce<false, false><<<nc, kScanBlock, 0, s>>>(d_in, n, chunk, agg);
-                    k_chunk_scan<false, false><<<nc, kScanBlock, 0, s>>>(d_in, d_out, n, chunk,
-                                                                        agg, nullptr, nullptr);
-                }
-            } else if (vec)
+            if (vec)
                 k_scan_exclusive_i32<true, false><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n,
                                                                                hdr, status, tiles);
             else
@@ -519,26 +565,22 @@ extern "C" hhs_status hhs_compact_flags_i32(const int32_t* d_flags, int32_t* d_s
     if (workspace_bytes < hhs_scan_workspace_size(n)) return HHS_ERR_INVALID_ARG;
     if ((reinterpret_cast<uintptr_t>(d_workspace) & 7u) != 0) return HHS_ERR_INVALID_ARG;
     const int tiles = (int)((n + ScanT::TILE - 1) / ScanT::TILE);
-    HHS_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, scan_workspace_bytes(n, ScanT::TILE), s));
     auto* hdr = static_cast<ScanHeader*>(d_workspace);
     auto* status = reinterpret_cast<unsigned long long*>(static_cast<char*>(d_workspace) +
                                                          sizeof(ScanHeader));
     const bool vec = ((reinterpret_cast<uintptr_t>(d_flags) |
                        reinterpret_cast<uintptr_t>(d_scan)) & 15u) == 0;
     if (n >= kTwoPassMinN) {
-        long long chunk = 0;
-        const int nc = chunk_plan(n, &chunk);
         auto* agg = reinterpret_cast<unsigned*>(status);
-        if (vec) {
-            k_chunk_reduce<true, true><<<nc, kScanBlock, 0, s>>>(d_flags, n, chunk, agg);
-            k_chunk_scan<true, true><<<nc, kScanBlock, 0, s>>>(d_flags, d_scan, n, chunk, agg,
-                                                               d_idx, d_count);
-        } else {
-            k_chunk_reduce<false, true><<<nc, kScanBlock, 0, s>>>(d_flags, n, chunk, agg);
-            k_chunk_scan<false, true><<<nc, kScanBlock, 0, s>>>(d_flags, d_scan, n, chunk, agg,
-                                                                d_idx, d_count);
-        }
-    } else if (vec)
+        if (vec)
+            launch_two_pass<true, true>(d_flags, d_scan, n, hdr, agg, d_idx, d_count, s);
+        else
+            launch_two_pass<false, true>(d_flags, d_scan, n, hdr, agg, d_idx, d_count, s);
+        HHS_LAUNCH_CHECK();
+        return HHS_OK;
+    }
+    HHS_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, scan_workspace_bytes(n, ScanT::TILE), s));
+    if (vec)
         k_compact_flags<true, false><<<tiles, kScanBlock, 0, s>>>(d_flags, d_scan, d_idx,
                                                                   d_count, n, hdr, status, tiles);
     else

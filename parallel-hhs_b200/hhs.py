@@ -22,7 +22,7 @@ MASS_EQUAL, MASS_SALPETER, MASS_TWO_COMPONENT = 0, 1, 2
 
 STATUS = {0: "HHS_OK", 1: "HHS_ERR_INVALID_ARG", 2: "HHS_ERR_CUDA", 3: "HHS_ERR_OOM",
           4: "HHS_ERR_TIMEOUT", 5: "HHS_ERR_DEVICE_FAULT_FLAG", 6: "HHS_ERR_DEPTH",
-          7: "HHS_ERR_CAPACITY"}
+          7: "HHS_ERR_CAPACITY", 8: "HHS_ERR_PEER"}
 
 
 class HHSError(RuntimeError):
@@ -78,6 +78,9 @@ class CParticleSystem(ctypes.Structure):
         [("id", _ip), ("parent_id", _ip), ("_base", _vp)]
 
 
+# hhs_barrier_fn: int32_t (*)(void* user, void* stream)
+BARRIER_FN = ctypes.CFUNCTYPE(ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p)
+
 # every symbol of include/hhs.h, with its ctypes signature (restype, argtypes)
 SIGNATURES = {
     "hhs_particle_system_alloc": (ctypes.c_int, [ctypes.POINTER(CParticleSystem), ctypes.c_int32]),
@@ -121,6 +124,17 @@ SIGNATURES = {
                                           ctypes.c_double, ctypes.c_int32, ctypes.c_int, _vp]),
     "hhs_hold_step_host": (ctypes.c_int, [_vp, ctypes.POINTER(CParticleSystem), ctypes.c_int32,
                                           ctypes.c_double, ctypes.c_int32, ctypes.c_int, _vp]),
+    "hhs_dist_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int32, ctypes.c_int32,
+                                       ctypes.POINTER(CParticleSystem), BARRIER_FN, _vp,
+                                       ctypes.c_int64]),
+    "hhs_dist_destroy": (ctypes.c_int, [_vp]),
+    "hhs_dist_shard": (ctypes.c_int, [ctypes.c_int32] * 4 + [_ip, _ip]),
+    "hhs_hold_step_dist": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(CParticleSystem),
+                                          ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
+                                          ctypes.c_int, _vp]),
+    "hhs_ipc_handle": (ctypes.c_int, [ctypes.POINTER(CParticleSystem), _vp]),
+    "hhs_ipc_open": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.POINTER(CParticleSystem)]),
+    "hhs_ipc_close": (ctypes.c_int, [ctypes.POINTER(CParticleSystem)]),
     "hhs_scan_workspace_size": (ctypes.c_size_t, [ctypes.c_int64]),
     "hhs_scan_exclusive_i32": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp, ctypes.c_size_t,
                                               _vp]),
@@ -566,3 +580,162 @@ def split_cpu_order_workspace_size(n):
 
 def scan_workspace_status(d_ws, stream=None):
     return lib().hhs_scan_workspace_status(d_ws, stream)
+
+
+# ---------------------------------------------------------------- one system, several GPUs
+IPC_HANDLE_BYTES = 64
+
+
+def dist_shard(n_fast, n_slow, rank, world):
+    """Sink range [lo, hi) of `rank` for a launch whose first n_fast sinks cost n_slow pair
+    terms and whose other n_slow sinks cost n_slow + n_fast (hhs_dist_shard)."""
+    lo, hi = ctypes.c_int32(), ctypes.c_int32()
+    _check(lib().hhs_dist_shard(n_fast, n_slow, rank, world, ctypes.byref(lo), ctypes.byref(hi)),
+           "hhs_dist_shard")
+    return lo.value, hi.value
+
+
+def ipc_handle(sys):
+    """64-byte CUDA IPC handle of a ParticleSystem's device allocation."""
+    buf = ctypes.create_string_buffer(IPC_HANDLE_BYTES)
+    _check(lib().hhs_ipc_handle(sys.ref, buf), "hhs_ipc_handle")
+    return buf.raw
+
+
+class PeerView:
+    """Another process's system of capacity n mapped into this one (hhs_ipc_open)."""
+
+    def __init__(self, handle, n):
+        self.c = CParticleSystem()
+        buf = ctypes.create_string_buffer(bytes(handle), IPC_HANDLE_BYTES)
+        _check(lib().hhs_ipc_open(buf, n, ctypes.byref(self.c)), "hhs_ipc_open")
+        self.n = n
+
+    def close(self):
+        if self.c._base:
+            _check(lib().hhs_ipc_close(ctypes.byref(self.c)), "hhs_ipc_close")
+
+
+class Dist:
+    """hhs_dist: this rank's side of one system replicated on `world` GPUs.
+
+    replicas[r] is rank r's system as this process addresses it (a ParticleSystem in the
+    same process, a PeerView of another process, or a CParticleSystem); replicas[rank] is
+    not used. barrier(stream) returns True once every rank's work enqueued on its stream
+    before the call is complete before any later work (False: a peer failed or did not
+    arrive). Launches of at least min_pairs pair terms are split across the ranks."""
+
+    def __init__(self, rank, world, replicas, barrier, min_pairs=1 << 24):
+        arr = (CParticleSystem * world)()
+        for r, p in enumerate(replicas):
+            if r != rank and p is not None:
+                arr[r] = p if isinstance(p, CParticleSystem) else p.c
+        self.barrier = barrier
+        self.failure = None
+
+        def _cb(_user, stream):
+            try:
+                return 0 if barrier(stream) else 1
+            except Exception as e:  # a callback must not raise into the library
+                self.failure = e
+                return 1
+        self._cb = BARRIER_FN(_cb)
+        self.h = _vp()
+        _check(lib().hhs_dist_create(ctypes.byref(self.h), rank, world, arr, self._cb, None,
+                                     int(min_pairs)), "hhs_dist_create")
+        self.rank, self.world = rank, world
+
+    def step(self, ctx, sys, n, dt, calc_timestep=True, prec=PREC_MIXED, stream=None):
+        """One top-level HOLD step of this rank's replica (hhs_hold_step_dist)."""
+        _check(lib().hhs_hold_step_dist(ctx.h, self.h, sys.ref, n, dt, int(bool(calc_timestep)),
+                                        prec, stream), "hhs_hold_step_dist")
+
+    def destroy(self):
+        if self.h:
+            lib().hhs_dist_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+class PeerBarrier:
+    """The barrier of a Dist over a torch.distributed process group.
+
+    NCCL group: a one-element all-reduce enqueued on the library's stream, so the host
+    does not wait; a rank that is gone ends that collective when the group's timeout
+    runs out. Other backends (gloo): synchronise the stream, then a monitored barrier,
+    which reports the rank that did not arrive within `timeout` seconds."""
+
+    def __init__(self, group=None, timeout=30.0):
+        import torch
+        import torch.distributed as tdist
+        self.group, self.timeout = group, timeout
+        self.nccl = tdist.get_backend(group) == "nccl"
+        self.token = torch.zeros(1, dtype=torch.int32, device="cuda") if self.nccl else None
+        self.failure = None
+
+    def __call__(self, stream):
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        try:
+            if self.nccl:
+                st = torch.cuda.ExternalStream(stream) if stream else torch.cuda.default_stream()
+                with torch.cuda.stream(st):
+                    tdist.all_reduce(self.token, group=self.group)
+            else:
+                if torch.cuda.is_available():
+                    if stream:
+                        torch.cuda.ExternalStream(stream).synchronize()
+                    else:
+                        torch.cuda.synchronize()
+                tdist.monitored_barrier(group=self.group,
+                                        timeout=datetime.timedelta(seconds=self.timeout))
+            return True
+        except Exception as e:
+            self.failure = e
+            return False
+
+
+class DistHold:
+    """One system integrated on every rank of a torch.distributed group, one GPU each.
+
+    Every rank uploads the same initial state into its own ParticleSystem; the handles
+    of all ranks' systems are exchanged over the group and mapped with CUDA IPC, and each
+    step() is hhs_hold_step_dist on this rank's replica: the O(n^2) timestep and kick
+    launches of at least min_pairs pair terms are split by sink and their kernels write
+    every result into all replicas over NVLink. The replicas stay bit-identical to
+    each other and to hhs_hold_step_host on one GPU."""
+
+    def __init__(self, ctx, sys, group=None, min_pairs=1 << 24, timeout=30.0, barrier=None):
+        import torch.distributed as tdist
+        self.rank = tdist.get_rank(group)
+        self.world = tdist.get_world_size(group)
+        handles = [None] * self.world
+        tdist.all_gather_object(handles, (ipc_handle(sys), sys.n), group=group)
+        self.views = {}
+        replicas = []
+        for r, (h, n) in enumerate(handles):
+            if r == self.rank:
+                replicas.append(None)
+                continue
+            self.views[r] = PeerView(h, n)
+            replicas.append(self.views[r])
+        self.barrier = barrier if barrier is not None else PeerBarrier(group, timeout)
+        self.dist = Dist(self.rank, self.world, replicas, self.barrier, min_pairs)
+        self.ctx, self.sys = ctx, sys
+
+    def step(self, n, dt, calc_timestep=True, prec=PREC_MIXED, stream=None):
+        self.dist.step(self.ctx, self.sys, n, dt, calc_timestep, prec, stream)
+
+    def close(self):
+        """Unmaps the peers. Call on every rank after the last step (whose closing
+        barrier has ordered every peer store)."""
+        self.dist.destroy()
+        for v in self.views.values():
+            v.close()
+        self.views = {}

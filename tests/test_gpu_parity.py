@@ -113,7 +113,8 @@ def test_scan_matches_golden_reference_test_inputs(cuda, hhs):
 
 
 @pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 127, 4095, 4096, 4097, 8191, 65536 + 3,
-                               (1 << 20) + 7, (1 << 22) + 5, (1 << 23) + 4099])
+                               (1 << 20) + 7, (1 << 22) + 5, (1 << 23) + 4099,
+                               (1 << 24), (1 << 25) + 4099])
 @pytest.mark.parametrize("offset", [0, 1])
 def test_scan_random_values_sizes_alignment(cuda, hhs, oracle, n, offset):
     torch = cuda
@@ -492,7 +493,8 @@ def test_autotune_restores_state_and_keeps_results(cuda, hhs, oracle):
 
 
 @pytest.mark.parametrize("n,p", [(1, 1.0), (5, 0.5), (4097, 0.01), (100003, 0.5),
-                                 ((1 << 20) + 5, 0.1), ((1 << 22) + 7, 0.3), (1 << 23, 0.01)])
+                                 ((1 << 20) + 5, 0.1), ((1 << 22) + 7, 0.3), (1 << 23, 0.01),
+                                 ((1 << 25) + 13, 0.2)])
 def test_compact_flags_matches_oracle(cuda, hhs, oracle, n, p):
     torch = cuda
     rng = np.random.default_rng(n)
