@@ -63,21 +63,22 @@ __global__ void __launch_bounds__(kScanBlock, 6)
     if (SELF_RESET && scan_finish_is_last(hdr, num_tiles, &s_last)) scan_reset(hdr, epoch);
 }
 
-// Two-pass form for large inputs, over super-chunks of at most 2^24 values (64 MB, half
-// of L2): per super-chunk, the first kernel sums contiguous chunks of whole tiles (one
-// chunk per CTA, a few CTAs per SM), the second gives each CTA the sum of the chunks
-// before its own plus the running total of the earlier super-chunks and scans its chunk
-// tile by tile. The super-chunk is still in L2 when the second kernel reads it again, so
-// DRAM sees 8 bytes per value, and there is no look-back: the single-pass form is
-// limited by how fast the inclusive prefixes propagate through hundreds of resident
-// tiles, and loses to this beyond a few million values.
+// Two-pass form for large inputs: the first kernel sums contiguous chunks of whole tiles
+// (one chunk per CTA, a few CTAs per SM), the second gives each CTA the sum of the chunks
+// before its own and scans its chunk tile by tile, carrying the running total. 12 bytes
+// of traffic per value instead of 8, but no look-back: the single-pass form is limited
+// by how fast the inclusive prefixes propagate through hundreds of resident tiles, and
+// loses to this beyond a few million values. The input can also be cut into super-chunks
+// run one after the other (a carry word passes the running total on), so that the second
+// kernel finds its super-chunk in L2; that measured slower at every size from 2^22 to
+// 2^28 (the extra launches cost more than the re-read), so the default is one
+// super-chunk of all n values and the L2-sized ones remain launch-shape variants.
 constexpr int kChunkCtasPerSm = 4;
 constexpr long long kTwoPassMinN = 1LL << 22;
-constexpr long long kSuperChunk = 1LL << 24;
 constexpr int kCarryWord = 1024;  // carries live after the chunk sums (< 1024 chunks)
 
-// FLAGS: the values are (in != 0) (stream compaction)
-template <bool VEC, bool FLAGS>
+// FLAGS: the values are (in != 0) (stream compaction). STREAM: evict-first loads
+template <bool VEC, bool FLAGS, bool STREAM>
 __global__ void __launch_bounds__(kScanBlock)
     k_chunk_reduce(const int32_t* __restrict__ in, long long n, long long chunk,
                    unsigned* __restrict__ agg, unsigned* __restrict__ clear_word) {
@@ -87,10 +88,10 @@ __global__ void __launch_bounds__(kScanBlock)
     const long long e = min(n, b + chunk);
     unsigned a0 = 0u, a1 = 0u, a2 = 0u, a3 = 0u;
     if (VEC) {
-        // plain loads: the values stay in L2 for the scan pass; four 16-byte loads in
-        // flight per thread
+        // four 16-byte loads in flight per thread
         const long long nv = (e - b) / 4;  // b is a multiple of 4
         const int4* v = reinterpret_cast<const int4*>(in + b);
+        auto ld = [&](const int4* p) { return STREAM ? __ldcs(p) : __ldg(p); };
         auto add = [&](const int4 q) {
             if (FLAGS) {
                 a0 += q.x != 0; a1 += q.y != 0; a2 += q.z != 0; a3 += q.w != 0;
@@ -100,11 +101,11 @@ __global__ void __launch_bounds__(kScanBlock)
         };
         long long k = threadIdx.x;
         for (; k + 3 * kScanBlock < nv; k += 4 * kScanBlock) {
-            const int4 q0 = __ldg(v + k), q1 = __ldg(v + k + kScanBlock),
-                       q2 = __ldg(v + k + 2 * kScanBlock), q3 = __ldg(v + k + 3 * kScanBlock);
+            const int4 q0 = ld(v + k), q1 = ld(v + k + kScanBlock),
+                       q2 = ld(v + k + 2 * kScanBlock), q3 = ld(v + k + 3 * kScanBlock);
             add(q0); add(q1); add(q2); add(q3);
         }
-        for (; k < nv; k += kScanBlock) add(__ldg(v + k));
+        for (; k < nv; k += kScanBlock) add(ld(v + k));
         for (long long k = b + nv * 4 + threadIdx.x; k < e; k += kScanBlock)
             a0 += FLAGS ? (unsigned)(in[k] != 0) : (unsigned)in[k];
     } else {
@@ -122,7 +123,7 @@ __global__ void __launch_bounds__(kScanBlock)
     }
 }
 
-// One super-chunk [base, base + n) of the whole input: in and out point at its start.
+// One super-chunk [gbase, gbase + n) of the whole input: in and out point at its start.
 // carry_in (null: 0) is the total of the earlier super-chunks; the last chunk writes the
 // running total to carry_out and, for FLAGS, to *count.
 // FLAGS: scan of (in != 0); the indices of the nonzero values go to idx_out[scan] (out,
@@ -133,7 +134,7 @@ __global__ void __launch_bounds__(kScanBlock)
                  long long chunk, const unsigned* __restrict__ agg,
                  int32_t* __restrict__ idx_out, int32_t* __restrict__ count,
                  const unsigned* __restrict__ carry_in, unsigned* __restrict__ carry_out,
-                 long long base) {
+                 long long gbase) {
     __shared__ unsigned s_warp[ScanT::WARPS], s_red[ScanT::WARPS];
     __shared__ unsigned s_total;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -182,11 +183,11 @@ __global__ void __launch_bounds__(kScanBlock)
             if (lane == 31) s_total = wi;
         }
         __syncthreads();
-        const unsigned base = offset + s_warp[warp];
+        const unsigned wbase = offset + s_warp[warp];
 #pragma unroll
         for (int c = 0; c < ScanT::CHUNKS; c++) {
             const long long el = tbase + ScanT::offset(warp, c, lane);
-            const unsigned p0 = base + cbase[c], p1 = p0 + v[4 * c], p2 = p1 + v[4 * c + 1],
+            const unsigned p0 = wbase + cbase[c], p1 = p0 + v[4 * c], p2 = p1 + v[4 * c + 1],
                            p3 = p2 + v[4 * c + 2];
             if (!FLAGS || out) {
                 if (VEC && el + 4 <= e) {
@@ -203,7 +204,7 @@ __global__ void __launch_bounds__(kScanBlock)
                 const unsigned pp[4] = {p0, p1, p2, p3};
 #pragma unroll
                 for (int k = 0; k < 4; k++)
-                    if (v[4 * c + k]) idx_out[pp[k]] = (int)(base + el + k);
+                    if (v[4 * c + k]) idx_out[pp[k]] = (int)(gbase + el + k);
             }
         }
         offset += s_total;
@@ -231,12 +232,16 @@ int chunk_plan(long long n, long long* chunk) {
     return (int)((n + *chunk - 1) / *chunk);
 }
 
-// The two-pass form over the whole input (agg: the workspace's status words; the
-// header's error word is cleared by the first kernel).
+// The two-pass form over the whole input in super-chunks of `super` values (0: one of
+// all n values). agg: the workspace's status words; the header's error word is cleared
+// by the first kernel.
+int scan_variant();
+
 template <bool VEC, bool FLAGS>
 void launch_two_pass(const int32_t* in, int32_t* out, long long n, ScanHeader* hdr,
                      unsigned* agg, int32_t* idx_out, int32_t* count, cudaStream_t s,
-                     long long super = kSuperChunk) {
+                     long long super = 0) {
+    if (super <= 0) super = n;
     unsigned* carry = agg + kCarryWord;
     int k = 0;
     for (long long base = 0; base < n; base += super, k++) {
@@ -244,8 +249,12 @@ void launch_two_pass(const int32_t* in, int32_t* out, long long n, ScanHeader* h
         const bool last = base + len == n;
         long long chunk = 0;
         const int nc = chunk_plan(len, &chunk);
-        k_chunk_reduce<VEC, FLAGS><<<nc, kScanBlock, 0, s>>>(in + base, len, chunk, agg,
-                                                              k == 0 ? &hdr->error : nullptr);
+        if (scan_variant() == 15)
+            k_chunk_reduce<VEC, FLAGS, true><<<nc, kScanBlock, 0, s>>>(
+                in + base, len, chunk, agg, k == 0 ? &hdr->error : nullptr);
+        else
+            k_chunk_reduce<VEC, FLAGS, false><<<nc, kScanBlock, 0, s>>>(
+                in + base, len, chunk, agg, k == 0 ? &hdr->error : nullptr);
         k_chunk_scan<VEC, FLAGS><<<nc, kScanBlock, 0, s>>>(
             in + base, out ? out + base : nullptr, len, chunk, agg, idx_out,
             last ? count : nullptr, k > 0 ? carry + (k & 1) : nullptr,
@@ -510,14 +519,14 @@ extern "C" hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out
                                                          sizeof(ScanHeader));
     const bool vec = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) &
                       15u) == 0;
-    if ((variant == 0 || variant >= 11) && n >= kTwoPassMinN) {
+    if ((variant == 0 || variant >= 11) && n >= kTwoPassMinN) {  // 15: evict-first sums
         // the chunk sums and carries are written before they are read: nothing to clear.
-        // Variants 11-14: super-chunks of 2^22, 2^23, 2^25 values, or one of n values.
+        // Variants 11-14: super-chunks of 2^22, 2^23, 2^24, 2^25 values.
         const long long super = variant == 11   ? (1LL << 22)
                                 : variant == 12 ? (1LL << 23)
-                                : variant == 13 ? (1LL << 25)
-                                : variant == 14 ? n
-                                                : kSuperChunk;
+                                : variant == 13 ? (1LL << 24)
+                                : variant == 14 ? (1LL << 25)
+                                                : 0;
         auto* agg = reinterpret_cast<unsigned*>(status);
         if (vec)
             launch_two_pass<true, false>(d_in, d_out, n, hdr, agg, nullptr, nullptr, s, super);

@@ -26,8 +26,8 @@ def _digest(out):
     return h.hexdigest()
 
 
-def _host_reference(hhs, s0, n, steps, prec, dt=1 / 64):
-    sy, ctx = hhs.ParticleSystem(n), hhs.Context(n)
+def _host_reference(hhs, s0, n, steps, prec, dt=1 / 64, eps=0.0):
+    sy, ctx = hhs.ParticleSystem(n), hhs.Context(n, eps=eps)
     sy.upload(s0)
     for _ in range(steps):
         hhs.hold_step_host(ctx, sy, n, dt, True, prec)
@@ -37,9 +37,9 @@ def _host_reference(hhs, s0, n, steps, prec, dt=1 / 64):
     return out
 
 
-def _run_threads(hhs, torch, s0, n, world, steps, prec, min_pairs, dt=1 / 64):
+def _run_threads(hhs, torch, s0, n, world, steps, prec, min_pairs, dt=1 / 64, eps=0.0):
     systems = [hhs.ParticleSystem(n) for _ in range(world)]
-    ctxs = [hhs.Context(n) for _ in range(world)]
+    ctxs = [hhs.Context(n, eps=eps) for _ in range(world)]
     streams = [torch.cuda.Stream() for _ in range(world)]
     for sy in systems:
         sy.upload(s0)
@@ -81,13 +81,16 @@ def _run_threads(hhs, torch, s0, n, world, steps, prec, min_pairs, dt=1 / 64):
     return outs, calls
 
 
-@pytest.mark.parametrize("world,prec,min_pairs", [(2, 0, 0), (3, 0, 0), (2, 1, 0),
-                                                  (4, 1, 0), (2, 0, 1 << 16), (3, 1, 1 << 14)])
-def test_sharded_step_replicas_equal_the_one_gpu_host_step(hhs, cuda, world, prec, min_pairs):
+@pytest.mark.parametrize("world,prec,min_pairs,eps", [(2, 0, 0, 0.0), (3, 0, 0, 0.0),
+                                                      (2, 1, 0, 0.0), (4, 1, 0, 0.0),
+                                                      (2, 0, 1 << 16, 0.0), (3, 1, 1 << 14, 0.0),
+                                                      (2, 0, 0, 0.02), (3, 1, 0, 0.02)])
+def test_sharded_step_replicas_equal_the_one_gpu_host_step(hhs, cuda, world, prec, min_pairs,
+                                                           eps):
     n, steps = 2048, 3
     s0 = hhs.plummer(n, 41)
-    ref = _host_reference(hhs, s0, n, steps, prec)
-    outs, calls = _run_threads(hhs, cuda, s0, n, world, steps, prec, min_pairs)
+    ref = _host_reference(hhs, s0, n, steps, prec, eps=eps)
+    outs, calls = _run_threads(hhs, cuda, s0, n, world, steps, prec, min_pairs, eps=eps)
     assert len(set(calls)) == 1 and calls[0] > 0  # every rank took the same barriers
     for out in outs:
         for k in FIELDS:

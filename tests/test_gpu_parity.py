@@ -125,6 +125,43 @@ def test_scan_random_values_sizes_alignment(cuda, hhs, oracle, n, offset):
     assert np.array_equal(out, oracle.scan_exclusive(a[offset:]))
 
 
+_SUPER_CHUNK_CHECK = r"""
+import ctypes, sys
+import numpy as np
+import torch
+sys.path.insert(0, sys.argv[1])
+import hhs
+n = 3 * (1 << 22) + 4099
+for offset in (0, 1):
+    a = np.random.default_rng(offset).integers(-1000, 1000, n + offset).astype(np.int32)
+    dev = torch.from_numpy(a).cuda()
+    out = torch.empty_like(dev)
+    wb = hhs.scan_workspace_size(n)
+    ws = torch.empty(wb, dtype=torch.uint8, device="cuda")
+    for _ in range(2):
+        hhs.scan_exclusive_i32(ctypes.c_void_p(dev[offset:].data_ptr()),
+                               ctypes.c_void_p(out[offset:].data_ptr()), n,
+                               ctypes.c_void_p(ws.data_ptr()), wb, None)
+        torch.cuda.synchronize()
+        ref = np.concatenate([[0], np.cumsum(a[offset:], dtype=np.int64)[:-1]]).astype(np.int32)
+        assert np.array_equal(out[offset:].cpu().numpy(), ref), offset
+print("ok")
+"""
+
+
+@pytest.mark.parametrize("variant", ["11", "12"])
+def test_scan_in_super_chunks_carries_the_running_total(cuda, variant):
+    """The two-pass scan cut into super-chunks of 2^22 or 2^23 values (launch-shape
+    variants), with a carry word between them: four or two super-chunks, the last one
+    ragged, aligned and unaligned, twice in a row on one workspace."""
+    import subprocess
+    import sys
+    from conftest import PKG
+    r = subprocess.run([sys.executable, "-c", _SUPER_CHUNK_CHECK, PKG], capture_output=True,
+                       text=True, timeout=600, env={**os.environ, "HHS_SCAN_VARIANT": variant})
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-2000:]
+
+
 def test_scan_lookback_wait_gives_up_and_reports_timeout(cuda, hhs, oracle):
     """Failure detection without a GPU fault: with the first tile left out, every look-back
     waits for a predecessor that never publishes; the bounded waits give up, the call
