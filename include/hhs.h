@@ -275,7 +275,8 @@ hhs_status hhs_scan_exclusive_i32_noalloc(const int32_t* d_in, int32_t* d_out, i
 /* Stream compaction (the split of a flag array, src/split.cuh:573-610 on int32 data):
  * d_idx[k] = index of the k-th nonzero flag, *d_count = number of nonzero flags, and
  * d_scan (optional, NULL = not written) = exclusive scan of (flag != 0). One pass below
- * 2^22 flags, two from there on; workspace as for hhs_scan_exclusive_i32. */
+ * 2^22 flags; from there on chunk sums then chunk scans (from 2^24 flags in one
+ * cooperative launch, in waves of 2^24 flags). Workspace as for hhs_scan_exclusive_i32. */
 hhs_status hhs_compact_flags_i32(const int32_t* d_flags, int32_t* d_scan, int32_t* d_idx,
                                  int32_t* d_count, int64_t n, void* d_workspace,
                                  size_t workspace_bytes, void* stream);

@@ -63,35 +63,37 @@ __global__ void __launch_bounds__(kScanBlock, 6)
     if (SELF_RESET && scan_finish_is_last(hdr, num_tiles, &s_last)) scan_reset(hdr, epoch);
 }
 
-// Two-pass form for large inputs: the first kernel sums contiguous chunks of whole tiles
-// (one chunk per CTA, a few CTAs per SM), the second gives each CTA the sum of the chunks
-// before its own and scans its chunk tile by tile, carrying the running total. 12 bytes
-// of traffic per value instead of 8, but no look-back: the single-pass form is limited
-// by how fast the inclusive prefixes propagate through hundreds of resident tiles, and
-// loses to this beyond a few million values. The input can also be cut into super-chunks
-// run one after the other (a carry word passes the running total on), so that the second
-// kernel finds its super-chunk in L2; that measured slower at every size from 2^22 to
-// 2^28 (the extra launches cost more than the re-read), so the default is one
-// super-chunk of all n values and the L2-sized ones remain launch-shape variants.
+// Large inputs (n >= 2^22). The single pass is held back by how fast the inclusive
+// prefixes propagate through hundreds of resident tiles, so large inputs are scanned in
+// two steps over contiguous chunks of whole tiles, one chunk per CTA: sum the chunk,
+// then scan it from the sum of the chunks before it.
+//  - Two-kernel form: a chunk-sum kernel and a chunk-scan kernel over the whole input,
+//    12 bytes of DRAM traffic per value. The default for the scan (4.25 TB/s at 2^28).
+//  - Wave form: one cooperative launch walks the input in waves of 2^24 values (64 MB,
+//    half of L2). Per wave every CTA sums its chunk, the grid meets at a counting
+//    barrier, and every CTA scans its chunk while most of it is still in L2. Each CTA
+//    adds up all of the wave's chunk sums itself, so the running total passes from wave
+//    to wave without another barrier. The default for stream compaction of n >= 2^24
+//    (3.27 against 2.88 TB/s at 2^28); for the scan it measured no faster (4.15 TB/s),
+//    and below 2^24 the cooperative launch and the header clear cost more than the
+//    re-read saves. Launch-shape variants 11-13 run the scan in waves of 2^22, 2^23 and
+//    2^24 values.
 constexpr int kChunkCtasPerSm = 4;
 constexpr long long kTwoPassMinN = 1LL << 22;
-constexpr int kCarryWord = 1024;  // carries live after the chunk sums (< 1024 chunks)
+constexpr long long kWaveValues = 1LL << 24;  // 64 MB of int32 per wave
+constexpr long long kWaveMinN = 1LL << 24;    // compaction: the wave form from here on
+constexpr unsigned long long kWaveBarrierTimeoutNs = 10ull * 1000000000ull;
 
-// FLAGS: the values are (in != 0) (stream compaction). STREAM: evict-first loads
-template <bool VEC, bool FLAGS, bool STREAM>
-__global__ void __launch_bounds__(kScanBlock)
-    k_chunk_reduce(const int32_t* __restrict__ in, long long n, long long chunk,
-                   unsigned* __restrict__ agg, unsigned* __restrict__ clear_word) {
-    __shared__ unsigned s_red[kScanBlock / 32];
-    if (clear_word && blockIdx.x == 0 && threadIdx.x == 0) *clear_word = 0u;
-    const long long b = (long long)blockIdx.x * chunk;
-    const long long e = min(n, b + chunk);
+// Block-wide sum of in[b, e) (FLAGS: the number of nonzero values), returned to every
+// thread. b is a multiple of 4.
+template <bool VEC, bool FLAGS>
+__device__ unsigned block_chunk_sum(const int32_t* __restrict__ in, long long b, long long e,
+                                    unsigned* s_red) {
     unsigned a0 = 0u, a1 = 0u, a2 = 0u, a3 = 0u;
     if (VEC) {
         // four 16-byte loads in flight per thread
-        const long long nv = (e - b) / 4;  // b is a multiple of 4
+        const long long nv = (e - b) / 4;
         const int4* v = reinterpret_cast<const int4*>(in + b);
-        auto ld = [&](const int4* p) { return STREAM ? __ldcs(p) : __ldg(p); };
         auto add = [&](const int4 q) {
             if (FLAGS) {
                 a0 += q.x != 0; a1 += q.y != 0; a2 += q.z != 0; a3 += q.w != 0;
@@ -101,54 +103,35 @@ __global__ void __launch_bounds__(kScanBlock)
         };
         long long k = threadIdx.x;
         for (; k + 3 * kScanBlock < nv; k += 4 * kScanBlock) {
-            const int4 q0 = ld(v + k), q1 = ld(v + k + kScanBlock),
-                       q2 = ld(v + k + 2 * kScanBlock), q3 = ld(v + k + 3 * kScanBlock);
+            const int4 q0 = __ldg(v + k), q1 = __ldg(v + k + kScanBlock),
+                       q2 = __ldg(v + k + 2 * kScanBlock), q3 = __ldg(v + k + 3 * kScanBlock);
             add(q0); add(q1); add(q2); add(q3);
         }
-        for (; k < nv; k += kScanBlock) add(ld(v + k));
-        for (long long k = b + nv * 4 + threadIdx.x; k < e; k += kScanBlock)
-            a0 += FLAGS ? (unsigned)(in[k] != 0) : (unsigned)in[k];
+        for (; k < nv; k += kScanBlock) add(__ldg(v + k));
+        for (long long t = b + nv * 4 + threadIdx.x; t < e; t += kScanBlock)
+            a0 += FLAGS ? (unsigned)(in[t] != 0) : (unsigned)in[t];
     } else {
-        for (long long k = b + threadIdx.x; k < e; k += kScanBlock)
-            a0 += FLAGS ? (unsigned)(in[k] != 0) : (unsigned)in[k];
+        for (long long t = b + threadIdx.x; t < e; t += kScanBlock)
+            a0 += FLAGS ? (unsigned)(in[t] != 0) : (unsigned)in[t];
     }
-    unsigned t = (unsigned)warp_sum((int)(a0 + a1 + a2 + a3));
+    const unsigned t = (unsigned)warp_sum((int)(a0 + a1 + a2 + a3));
     if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = t;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned sum = 0u;
+    unsigned sum = 0u;
 #pragma unroll
-        for (int w = 0; w < kScanBlock / 32; w++) sum += s_red[w];
-        agg[blockIdx.x] = sum;
-    }
+    for (int w = 0; w < kScanBlock / 32; w++) sum += s_red[w];
+    __syncthreads();  // s_red may be reused
+    return sum;
 }
 
-// One super-chunk [gbase, gbase + n) of the whole input: in and out point at its start.
-// carry_in (null: 0) is the total of the earlier super-chunks; the last chunk writes the
-// running total to carry_out and, for FLAGS, to *count.
-// FLAGS: scan of (in != 0); the indices of the nonzero values go to idx_out[scan] (out,
-// the scan itself, may then be null)
+// Scans in[b, e) tile by tile starting from `offset` and returns the running total at e.
+// out may be null with FLAGS; FLAGS: idx_out[scan] = index of each nonzero value.
 template <bool VEC, bool FLAGS>
-__global__ void __launch_bounds__(kScanBlock)
-    k_chunk_scan(const int32_t* __restrict__ in, int32_t* __restrict__ out, long long n,
-                 long long chunk, const unsigned* __restrict__ agg,
-                 int32_t* __restrict__ idx_out, int32_t* __restrict__ count,
-                 const unsigned* __restrict__ carry_in, unsigned* __restrict__ carry_out,
-                 long long gbase) {
-    __shared__ unsigned s_warp[ScanT::WARPS], s_red[ScanT::WARPS];
-    __shared__ unsigned s_total;
+__device__ unsigned block_chunk_scan(const int32_t* __restrict__ in, int32_t* __restrict__ out,
+                                     long long b, long long e, unsigned offset,
+                                     int32_t* __restrict__ idx_out, unsigned* s_warp,
+                                     unsigned* s_total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // offset of this chunk: the earlier super-chunks, then the chunks before it
-    unsigned part = (carry_in && threadIdx.x == 0) ? *carry_in : 0u;
-    for (int c = threadIdx.x; c < (int)blockIdx.x; c += kScanBlock) part += agg[c];
-    part = (unsigned)warp_sum((int)part);
-    if (lane == 0) s_red[warp] = part;
-    __syncthreads();
-    unsigned offset = 0u;
-#pragma unroll
-    for (int w = 0; w < ScanT::WARPS; w++) offset += s_red[w];
-    const long long b = (long long)blockIdx.x * chunk;
-    const long long e = min(n, b + chunk);
     for (long long tbase = b; tbase < e; tbase += ScanT::TILE) {
         unsigned v[kScanItems], cbase[ScanT::CHUNKS];
 #pragma unroll
@@ -180,7 +163,7 @@ __global__ void __launch_bounds__(kScanBlock)
             const unsigned wt = lane < ScanT::WARPS ? s_warp[lane] : 0u;
             const unsigned wi = (unsigned)warp_incl_scan((int)wt, lane);
             if (lane < ScanT::WARPS) s_warp[lane] = wi - wt;
-            if (lane == 31) s_total = wi;
+            if (lane == 31) *s_total = wi;
         }
         __syncthreads();
         const unsigned wbase = offset + s_warp[warp];
@@ -204,19 +187,130 @@ __global__ void __launch_bounds__(kScanBlock)
                 const unsigned pp[4] = {p0, p1, p2, p3};
 #pragma unroll
                 for (int k = 0; k < 4; k++)
-                    if (v[4 * c + k]) idx_out[pp[k]] = (int)(gbase + el + k);
+                    if (v[4 * c + k]) idx_out[pp[k]] = (int)(el + k);
             }
         }
-        offset += s_total;
+        offset += *s_total;
         __syncthreads();
     }
-    if (e == n && threadIdx.x == 0) {
-        if (carry_out) *carry_out = offset;
-        if (FLAGS && count) *count = (int)offset;
-    }
+    return offset;
 }
 
-// chunks of whole tiles for the two-pass form; returns the chunk count
+// ---- two-kernel form
+template <bool VEC, bool FLAGS>
+__global__ void __launch_bounds__(kScanBlock)
+    k_chunk_reduce(const int32_t* __restrict__ in, long long n, long long chunk,
+                   unsigned* __restrict__ agg, unsigned* __restrict__ clear_word) {
+    __shared__ unsigned s_red[kScanBlock / 32];
+    if (clear_word && blockIdx.x == 0 && threadIdx.x == 0) *clear_word = 0u;
+    const long long b = (long long)blockIdx.x * chunk;
+    const unsigned sum = block_chunk_sum<VEC, FLAGS>(in, b, min(n, b + chunk), s_red);
+    if (threadIdx.x == 0) agg[blockIdx.x] = sum;
+}
+
+// the last chunk writes the total to *count (FLAGS)
+template <bool VEC, bool FLAGS>
+__global__ void __launch_bounds__(kScanBlock)
+    k_chunk_scan(const int32_t* __restrict__ in, int32_t* __restrict__ out, long long n,
+                 long long chunk, const unsigned* __restrict__ agg,
+                 int32_t* __restrict__ idx_out, int32_t* __restrict__ count) {
+    __shared__ unsigned s_warp[ScanT::WARPS], s_red[ScanT::WARPS];
+    __shared__ unsigned s_total;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // offset of this chunk: the sum of the chunks before it
+    unsigned part = 0u;
+    for (int c = threadIdx.x; c < (int)blockIdx.x; c += kScanBlock) part += agg[c];
+    part = (unsigned)warp_sum((int)part);
+    if (lane == 0) s_red[warp] = part;
+    __syncthreads();
+    unsigned offset = 0u;
+#pragma unroll
+    for (int w = 0; w < ScanT::WARPS; w++) offset += s_red[w];
+    const long long b = (long long)blockIdx.x * chunk;
+    const long long e = min(n, b + chunk);
+    offset = block_chunk_scan<VEC, FLAGS>(in, out, b, e, offset, idx_out, s_warp, &s_total);
+    if (FLAGS && count && e == n && threadIdx.x == 0) *count = (int)offset;
+}
+
+// ---- wave form
+// Grid barrier of the wave kernel: arrivals are release reductions on a counter that
+// the host clears before the launch; the k-th barrier waits for k x grid arrivals.
+// Thread 0 polls with acquire loads and gives up after kWaveBarrierTimeoutNs, or as soon
+// as another CTA has recorded an error, recording HHS_ERRBIT_BARRIER_TIMEOUT.
+__device__ __forceinline__ bool wave_barrier(unsigned* count, unsigned target, unsigned* err,
+                                             unsigned* s_ok) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned ok = 1u;
+        red_add_release_u32(count, 1u);
+        unsigned polls = 0;
+        unsigned long long t0 = 0;
+        while (ld_acquire_u32(count) < target) {
+            if (++polls < 128) continue;
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            if (t0 == 0) t0 = t;
+            if (*reinterpret_cast<volatile unsigned*>(err) != 0u) { ok = 0u; break; }
+            if (t - t0 > kWaveBarrierTimeoutNs) {
+                atomicOr(err, HHS_ERRBIT_BARRIER_TIMEOUT);
+                ok = 0u;
+                break;
+            }
+            __nanosleep(64);
+        }
+        *s_ok = ok;
+    }
+    __syncthreads();
+    return *s_ok != 0u;
+}
+
+// Cooperative launch, every CTA resident. Wave k covers [k*wave, (k+1)*wave) with
+// wave = chunk x gridDim.x; CTA c owns [k*wave + c*chunk, ... + chunk) of it. agg holds
+// two sets of gridDim.x chunk sums, used by alternate waves (a CTA can be at most one
+// barrier ahead, so it never overwrites a set another CTA is still reading).
+template <bool VEC, bool FLAGS>
+__global__ void __launch_bounds__(kScanBlock)
+    k_wave_scan(const int32_t* __restrict__ in, int32_t* __restrict__ out, long long n,
+                long long chunk, unsigned* __restrict__ agg, ScanHeader* hdr,
+                int32_t* __restrict__ idx_out, int32_t* __restrict__ count) {
+    __shared__ unsigned s_warp[ScanT::WARPS], s_red[ScanT::WARPS], s_red2[ScanT::WARPS];
+    __shared__ unsigned s_total, s_ok;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long wave = chunk * gridDim.x;
+    unsigned carry = 0u;
+    int k = 0;
+    for (long long wb = 0; wb < n; wb += wave, k++) {
+        const long long b = wb + (long long)blockIdx.x * chunk;
+        const long long e = min(n, b + chunk);
+        unsigned* A = agg + (size_t)(k & 1) * gridDim.x;
+        const unsigned sum = b < e ? block_chunk_sum<VEC, FLAGS>(in, b, e, s_red) : 0u;
+        if (threadIdx.x == 0) A[blockIdx.x] = sum;
+        if (!wave_barrier(&hdr->wave_count, (unsigned)(k + 1) * gridDim.x, &hdr->error, &s_ok))
+            return;
+        // the chunks before this one, and the whole wave (loads that bypass L1: the sets
+        // are rewritten every other wave)
+        unsigned before = 0u, all = 0u;
+        for (int c = threadIdx.x; c < (int)gridDim.x; c += kScanBlock) {
+            const unsigned a = __ldcg(A + c);
+            all += a;
+            if (c < (int)blockIdx.x) before += a;
+        }
+        before = (unsigned)warp_sum((int)before);
+        all = (unsigned)warp_sum((int)all);
+        if (lane == 0) { s_red[warp] = before; s_red2[warp] = all; }
+        __syncthreads();
+        unsigned off = carry;
+        unsigned tot = 0u;
+#pragma unroll
+        for (int w = 0; w < ScanT::WARPS; w++) { off += s_red[w]; tot += s_red2[w]; }
+        __syncthreads();
+        if (b < e) block_chunk_scan<VEC, FLAGS>(in, out, b, e, off, idx_out, s_warp, &s_total);
+        carry += tot;
+    }
+    if (FLAGS && count && blockIdx.x == 0 && threadIdx.x == 0) *count = (int)carry;
+}
+
+// chunks of whole tiles for the two-kernel form; returns the chunk count
 int chunk_plan(long long n, long long* chunk) {
     static int sms = 0;
     if (sms == 0) {
@@ -232,34 +326,65 @@ int chunk_plan(long long n, long long* chunk) {
     return (int)((n + *chunk - 1) / *chunk);
 }
 
-// The two-pass form over the whole input in super-chunks of `super` values (0: one of
-// all n values). agg: the workspace's status words; the header's error word is cleared
-// by the first kernel.
-int scan_variant();
-
+// The two-kernel form over the whole input. agg: the workspace's status words; the
+// header's error word is cleared by the first kernel.
 template <bool VEC, bool FLAGS>
 void launch_two_pass(const int32_t* in, int32_t* out, long long n, ScanHeader* hdr,
-                     unsigned* agg, int32_t* idx_out, int32_t* count, cudaStream_t s,
-                     long long super = 0) {
-    if (super <= 0) super = n;
-    unsigned* carry = agg + kCarryWord;
-    int k = 0;
-    for (long long base = 0; base < n; base += super, k++) {
-        const long long len = n - base < super ? n - base : super;
-        const bool last = base + len == n;
-        long long chunk = 0;
-        const int nc = chunk_plan(len, &chunk);
-        if (scan_variant() == 15)
-            k_chunk_reduce<VEC, FLAGS, true><<<nc, kScanBlock, 0, s>>>(
-                in + base, len, chunk, agg, k == 0 ? &hdr->error : nullptr);
-        else
-            k_chunk_reduce<VEC, FLAGS, false><<<nc, kScanBlock, 0, s>>>(
-                in + base, len, chunk, agg, k == 0 ? &hdr->error : nullptr);
-        k_chunk_scan<VEC, FLAGS><<<nc, kScanBlock, 0, s>>>(
-            in + base, out ? out + base : nullptr, len, chunk, agg, idx_out,
-            last ? count : nullptr, k > 0 ? carry + (k & 1) : nullptr,
-            last ? nullptr : carry + ((k + 1) & 1), base);
+                     unsigned* agg, int32_t* idx_out, int32_t* count, cudaStream_t s) {
+    long long chunk = 0;
+    const int nc = chunk_plan(n, &chunk);
+    k_chunk_reduce<VEC, FLAGS><<<nc, kScanBlock, 0, s>>>(in, n, chunk, agg, &hdr->error);
+    k_chunk_scan<VEC, FLAGS><<<nc, kScanBlock, 0, s>>>(in, out, n, chunk, agg, idx_out, count);
+}
+
+// Resident CTAs of the wave kernel on the current device (0: cannot run).
+template <bool VEC, bool FLAGS>
+int wave_grid() {
+    static int grid[64] = {0};
+    static bool done[64] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    if (!done[dev]) {
+        int sms = 0, per = 0, coop = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_wave_scan<VEC, FLAGS>,
+                                                          kScanBlock, 0) != cudaSuccess)
+            per = 0;
+        per = per < kChunkCtasPerSm ? per : kChunkCtasPerSm;
+        grid[dev] = (coop && per > 0 && sms > 0) ? per * sms : 0;
+        done[dev] = true;
     }
+    return grid[dev];
+}
+
+// The large-input scan: the wave form with waves of `wave_values` values, or the
+// two-kernel form (wave_values = 0, or when the wave kernel cannot be launched with
+// every CTA resident).
+template <bool VEC, bool FLAGS>
+hhs_status launch_large(const int32_t* in, int32_t* out, long long n, ScanHeader* hdr,
+                        unsigned* agg, size_t agg_words, int32_t* idx_out, int32_t* count,
+                        cudaStream_t s, long long wave_values) {
+    const int grid = wave_grid<VEC, FLAGS>();
+    if (grid <= 0 || wave_values <= 0 || (size_t)2 * grid > agg_words) {
+        launch_two_pass<VEC, FLAGS>(in, out, n, hdr, agg, idx_out, count, s);
+        HHS_LAUNCH_CHECK();
+        return HHS_OK;
+    }
+    const long long tiles = (wave_values + ScanT::TILE - 1) / ScanT::TILE;
+    long long chunk = (tiles + grid - 1) / grid * ScanT::TILE;
+    // the header (error word, barrier counter) starts at zero
+    HHS_CUDA_TRY(cudaMemsetAsync(hdr, 0, sizeof(ScanHeader), s));
+    void* args[] = {(void*)&in, (void*)&out, (void*)&n, (void*)&chunk, (void*)&agg,
+                    (void*)&hdr, (void*)&idx_out, (void*)&count};
+    const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_wave_scan<VEC, FLAGS>,
+                                                      dim3(grid), dim3(kScanBlock), args, 0, s);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        launch_two_pass<VEC, FLAGS>(in, out, n, hdr, agg, idx_out, count, s);
+    }
+    HHS_LAUNCH_CHECK();
+    return HHS_OK;
 }
 
 // Launch-shape variants of the standalone scan (tile = BLOCK x ITEMS values, look-back
@@ -519,21 +644,19 @@ extern "C" hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out
                                                          sizeof(ScanHeader));
     const bool vec = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) &
                       15u) == 0;
-    if ((variant == 0 || variant >= 11) && n >= kTwoPassMinN) {  // 15: evict-first sums
-        // the chunk sums and carries are written before they are read: nothing to clear.
-        // Variants 11-14: super-chunks of 2^22, 2^23, 2^24, 2^25 values.
-        const long long super = variant == 11   ? (1LL << 22)
-                                : variant == 12 ? (1LL << 23)
-                                : variant == 13 ? (1LL << 24)
-                                : variant == 14 ? (1LL << 25)
-                                                : 0;
+    if ((variant == 0 || variant >= 11) && n >= kTwoPassMinN) {
+        // the chunk sums are written before they are read: only the header is cleared.
+        // Default: the two-kernel form; variants 11-13: waves of 2^22, 2^23, 2^24 values.
+        const long long wave = variant == 11   ? (1LL << 22)
+                               : variant == 12 ? (1LL << 23)
+                               : variant == 13 ? kWaveValues
+                                               : 0;
         auto* agg = reinterpret_cast<unsigned*>(status);
-        if (vec)
-            launch_two_pass<true, false>(d_in, d_out, n, hdr, agg, nullptr, nullptr, s, super);
-        else
-            launch_two_pass<false, false>(d_in, d_out, n, hdr, agg, nullptr, nullptr, s, super);
-        HHS_LAUNCH_CHECK();
-        return HHS_OK;
+        const size_t words = (used - sizeof(ScanHeader)) / sizeof(unsigned);
+        return vec ? launch_large<true, false>(d_in, d_out, n, hdr, agg, words, nullptr, nullptr,
+                                               s, wave)
+                   : launch_large<false, false>(d_in, d_out, n, hdr, agg, words, nullptr,
+                                                nullptr, s, wave);
     }
     HHS_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, used, s));
     switch (variant) {
@@ -581,12 +704,13 @@ extern "C" hhs_status hhs_compact_flags_i32(const int32_t* d_flags, int32_t* d_s
                        reinterpret_cast<uintptr_t>(d_scan)) & 15u) == 0;
     if (n >= kTwoPassMinN) {
         auto* agg = reinterpret_cast<unsigned*>(status);
-        if (vec)
-            launch_two_pass<true, true>(d_flags, d_scan, n, hdr, agg, d_idx, d_count, s);
-        else
-            launch_two_pass<false, true>(d_flags, d_scan, n, hdr, agg, d_idx, d_count, s);
-        HHS_LAUNCH_CHECK();
-        return HHS_OK;
+        const size_t words =
+            (scan_workspace_bytes(n, kScanMinTile) - sizeof(ScanHeader)) / sizeof(unsigned);
+        const long long wave = n >= kWaveMinN ? kWaveValues : 0;
+        return vec ? launch_large<true, true>(d_flags, d_scan, n, hdr, agg, words, d_idx,
+                                              d_count, s, wave)
+                   : launch_large<false, true>(d_flags, d_scan, n, hdr, agg, words, d_idx,
+                                               d_count, s, wave);
     }
     HHS_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, scan_workspace_bytes(n, ScanT::TILE), s));
     if (vec)
@@ -667,7 +791,7 @@ extern "C" hhs_status hhs_scan_workspace_status(const void* d_workspace, void* s
     unsigned err = 0;
     HHS_CUDA_TRY(cudaMemcpy(&err, &static_cast<const ScanHeader*>(d_workspace)->error,
                             sizeof(err), cudaMemcpyDeviceToHost));
-    if (err & HHS_ERRBIT_LOOKBACK_TIMEOUT) return HHS_ERR_TIMEOUT;
+    if (err & (HHS_ERRBIT_LOOKBACK_TIMEOUT | HHS_ERRBIT_BARRIER_TIMEOUT)) return HHS_ERR_TIMEOUT;
     return err ? HHS_ERR_DEVICE_FAULT_FLAG : HHS_OK;
 }
 

@@ -20,7 +20,8 @@ struct ScanHeader {
     unsigned epoch;         // status words of other epochs read as "not ready"
     unsigned error;         // HHS_ERRBIT_* set by timed-out waits
     unsigned spin_limit;    // look-back polls before giving up (0: HHS_SPIN_LIMIT)
-    unsigned pad[59];
+    unsigned wave_count;    // grid-barrier arrivals of the wave-form scan
+    unsigned pad[58];
 };
 static_assert(sizeof(ScanHeader) == 256, "scan header must stay 256 bytes");
 

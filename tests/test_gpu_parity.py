@@ -149,11 +149,11 @@ print("ok")
 """
 
 
-@pytest.mark.parametrize("variant", ["11", "12"])
-def test_scan_in_super_chunks_carries_the_running_total(cuda, variant):
-    """The two-pass scan cut into super-chunks of 2^22 or 2^23 values (launch-shape
-    variants), with a carry word between them: four or two super-chunks, the last one
-    ragged, aligned and unaligned, twice in a row on one workspace."""
+@pytest.mark.parametrize("variant", ["11", "12", "13"])
+def test_large_scan_forms_carry_the_running_total(cuda, variant):
+    """The large-input scan in the wave form (launch-shape variants): waves of 2^22, 2^23
+    or 2^24 values (three, two or one wave, the running total carried from wave to wave,
+    the last wave ragged); aligned and unaligned, twice in a row on one workspace."""
     import subprocess
     import sys
     from conftest import PKG
