@@ -300,6 +300,15 @@ hhs_status hhs_split_cpu_order(const double* d_ts, int32_t n, double pivot, int3
 hhs_status hhs_scan_selftest_stalled_predecessor(const int32_t* d_in, int32_t* d_out, int64_t n,
                                                  void* d_workspace, size_t workspace_bytes,
                                                  uint32_t max_polls, void* stream);
+/* Failure-detection self-test of the bounded grid barrier of the wave-form scan (the
+ * one-launch form that stream compaction uses from 2^24 values): runs it with every
+ * barrier waiting for one CTA more than the launch has; each wait gives up after
+ * timeout_us (1..10^7) microseconds, records the timeout in the workspace and returns.
+ * d_out is left unspecified. Synchronises the stream; returns HHS_ERR_TIMEOUT when the
+ * waits ran out as designed. n >= 2^22. */
+hhs_status hhs_scan_selftest_wave_barrier(const int32_t* d_in, int32_t* d_out, int64_t n,
+                                          void* d_workspace, size_t workspace_bytes,
+                                          uint32_t timeout_us, void* stream);
 
 /* ---- diagnostics ---------------------------------------------------------------- */
 /* Work recorded by the HOLD schedule since the last reset (device counters). */

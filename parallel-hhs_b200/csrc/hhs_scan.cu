@@ -235,10 +235,10 @@ __global__ void __launch_bounds__(kScanBlock)
 // ---- wave form
 // Grid barrier of the wave kernel: arrivals are release reductions on a counter that
 // the host clears before the launch; the k-th barrier waits for k x grid arrivals.
-// Thread 0 polls with acquire loads and gives up after kWaveBarrierTimeoutNs, or as soon
-// as another CTA has recorded an error, recording HHS_ERRBIT_BARRIER_TIMEOUT.
+// Thread 0 polls with acquire loads and gives up after timeout_ns, or as soon as another
+// CTA has recorded an error, recording HHS_ERRBIT_BARRIER_TIMEOUT.
 __device__ __forceinline__ bool wave_barrier(unsigned* count, unsigned target, unsigned* err,
-                                             unsigned* s_ok) {
+                                             unsigned* s_ok, unsigned long long timeout_ns) {
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned ok = 1u;
@@ -251,7 +251,7 @@ __device__ __forceinline__ bool wave_barrier(unsigned* count, unsigned target, u
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
             if (t0 == 0) t0 = t;
             if (*reinterpret_cast<volatile unsigned*>(err) != 0u) { ok = 0u; break; }
-            if (t - t0 > kWaveBarrierTimeoutNs) {
+            if (t - t0 > timeout_ns) {
                 atomicOr(err, HHS_ERRBIT_BARRIER_TIMEOUT);
                 ok = 0u;
                 break;
@@ -268,11 +268,14 @@ __device__ __forceinline__ bool wave_barrier(unsigned* count, unsigned target, u
 // wave = chunk x gridDim.x; CTA c owns [k*wave + c*chunk, ... + chunk) of it. agg holds
 // two sets of gridDim.x chunk sums, used by alternate waves (a CTA can be at most one
 // barrier ahead, so it never overwrites a set another CTA is still reading).
+// missing: arrivals each barrier waits for beyond the grid's own (0; 1 makes every
+// barrier wait for a CTA that does not exist: the failure-detection self-test).
 template <bool VEC, bool FLAGS>
 __global__ void __launch_bounds__(kScanBlock)
     k_wave_scan(const int32_t* __restrict__ in, int32_t* __restrict__ out, long long n,
                 long long chunk, unsigned* __restrict__ agg, ScanHeader* hdr,
-                int32_t* __restrict__ idx_out, int32_t* __restrict__ count) {
+                int32_t* __restrict__ idx_out, int32_t* __restrict__ count,
+                unsigned missing, unsigned long long timeout_ns) {
     __shared__ unsigned s_warp[ScanT::WARPS], s_red[ScanT::WARPS], s_red2[ScanT::WARPS];
     __shared__ unsigned s_total, s_ok;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -285,7 +288,8 @@ __global__ void __launch_bounds__(kScanBlock)
         unsigned* A = agg + (size_t)(k & 1) * gridDim.x;
         const unsigned sum = b < e ? block_chunk_sum<VEC, FLAGS>(in, b, e, s_red) : 0u;
         if (threadIdx.x == 0) A[blockIdx.x] = sum;
-        if (!wave_barrier(&hdr->wave_count, (unsigned)(k + 1) * gridDim.x, &hdr->error, &s_ok))
+        if (!wave_barrier(&hdr->wave_count, (unsigned)(k + 1) * (gridDim.x + missing),
+                          &hdr->error, &s_ok, timeout_ns))
             return;
         // the chunks before this one, and the whole wave (loads that bypass L1: the sets
         // are rewritten every other wave)
@@ -364,8 +368,10 @@ int wave_grid() {
 template <bool VEC, bool FLAGS>
 hhs_status launch_large(const int32_t* in, int32_t* out, long long n, ScanHeader* hdr,
                         unsigned* agg, size_t agg_words, int32_t* idx_out, int32_t* count,
-                        cudaStream_t s, long long wave_values) {
+                        cudaStream_t s, long long wave_values, unsigned missing = 0u,
+                        unsigned long long timeout_ns = kWaveBarrierTimeoutNs) {
     const int grid = wave_grid<VEC, FLAGS>();
+    if (missing && (grid <= 0 || (size_t)2 * grid > agg_words)) return HHS_ERR_INVALID_ARG;
     if (grid <= 0 || wave_values <= 0 || (size_t)2 * grid > agg_words) {
         launch_two_pass<VEC, FLAGS>(in, out, n, hdr, agg, idx_out, count, s);
         HHS_LAUNCH_CHECK();
@@ -375,12 +381,14 @@ hhs_status launch_large(const int32_t* in, int32_t* out, long long n, ScanHeader
     long long chunk = (tiles + grid - 1) / grid * ScanT::TILE;
     // the header (error word, barrier counter) starts at zero
     HHS_CUDA_TRY(cudaMemsetAsync(hdr, 0, sizeof(ScanHeader), s));
-    void* args[] = {(void*)&in, (void*)&out, (void*)&n, (void*)&chunk, (void*)&agg,
-                    (void*)&hdr, (void*)&idx_out, (void*)&count};
+    void* args[] = {(void*)&in,     (void*)&out,   (void*)&n,       (void*)&chunk,
+                    (void*)&agg,    (void*)&hdr,   (void*)&idx_out, (void*)&count,
+                    (void*)&missing, (void*)&timeout_ns};
     const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_wave_scan<VEC, FLAGS>,
                                                       dim3(grid), dim3(kScanBlock), args, 0, s);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
+        if (missing) return hhs_from_cuda(e);
         launch_two_pass<VEC, FLAGS>(in, out, n, hdr, agg, idx_out, count, s);
     }
     HHS_LAUNCH_CHECK();
@@ -824,6 +832,36 @@ extern "C" hhs_status hhs_scan_selftest_stalled_predecessor(const int32_t* d_in,
     k_scan_exclusive_i32<false, false><<<tiles - 1, kScanBlock, 0, s>>>(d_in, d_out, n, hdr,
                                                                        status, tiles);
     HHS_LAUNCH_CHECK();
+    return hhs_scan_workspace_status(d_workspace, stream);
+}
+
+// Runs the wave-form scan with every grid barrier waiting for one CTA more than the grid
+// has, so each wait runs out: every CTA gives up after timeout_us, records
+// HHS_ERRBIT_BARRIER_TIMEOUT in the workspace header and returns. d_out is left
+// unspecified. Synchronises the stream and returns the workspace status.
+extern "C" hhs_status hhs_scan_selftest_wave_barrier(const int32_t* d_in, int32_t* d_out,
+                                                     int64_t n, void* d_workspace,
+                                                     size_t workspace_bytes,
+                                                     uint32_t timeout_us, void* stream) {
+    if (!d_in || !d_out || !d_workspace || n < kTwoPassMinN || n > (int64_t)0x7fffffff ||
+        timeout_us == 0 || timeout_us > 10000000u)
+        return HHS_ERR_INVALID_ARG;
+    if (workspace_bytes < hhs_scan_workspace_size(n)) return HHS_ERR_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(d_workspace) & 7u) != 0) return HHS_ERR_INVALID_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    auto* hdr = static_cast<ScanHeader*>(d_workspace);
+    auto* agg = reinterpret_cast<unsigned*>(static_cast<char*>(d_workspace) + sizeof(ScanHeader));
+    const size_t words =
+        (scan_workspace_bytes(n, kScanMinTile) - sizeof(ScanHeader)) / sizeof(unsigned);
+    const bool vec = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) &
+                      15u) == 0;
+    const unsigned long long ns = (unsigned long long)timeout_us * 1000ull;
+    const hhs_status st =
+        vec ? launch_large<true, false>(d_in, d_out, n, hdr, agg, words, nullptr, nullptr, s,
+                                        kWaveValues, 1u, ns)
+            : launch_large<false, false>(d_in, d_out, n, hdr, agg, words, nullptr, nullptr, s,
+                                         kWaveValues, 1u, ns);
+    if (st != HHS_OK) return st;
     return hhs_scan_workspace_status(d_workspace, stream);
 }
 

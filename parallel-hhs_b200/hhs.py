@@ -145,6 +145,8 @@ SIGNATURES = {
     "hhs_scan_selftest_stalled_predecessor": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp,
                                                               ctypes.c_size_t, ctypes.c_uint32,
                                                               _vp]),
+    "hhs_scan_selftest_wave_barrier": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp,
+                                                       ctypes.c_size_t, ctypes.c_uint32, _vp]),
     "hhs_scan_exclusive_i32_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp]),
     "hhs_compact_flags_i32": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int64, _vp,
                                              ctypes.c_size_t, _vp]),
@@ -567,6 +569,13 @@ def scan_selftest_stalled_predecessor(d_in, d_out, n, d_ws, ws_bytes, max_polls,
     """Status of a scan whose first tile never publishes (HHS_ERR_TIMEOUT expected)."""
     return lib().hhs_scan_selftest_stalled_predecessor(d_in, d_out, n, d_ws, ws_bytes,
                                                        max_polls, stream)
+
+
+def scan_selftest_wave_barrier(d_in, d_out, n, d_ws, ws_bytes, timeout_us, stream=None):
+    """Makes every grid barrier of the wave-form scan wait for a CTA that does not exist;
+    returns the status (HHS_ERR_TIMEOUT = 4 when the bounded waits gave up)."""
+    return lib().hhs_scan_selftest_wave_barrier(d_in, d_out, n, d_ws, ws_bytes, timeout_us,
+                                                stream)
 
 
 def split_cpu_order(d_ts, n, pivot, d_order, d_counts, d_ws, ws_bytes, stream=None):

@@ -143,3 +143,53 @@ def test_peer_barrier_reports_a_rank_that_does_not_arrive(absent):
         assert out[0][2] is False and "1" in out[0][3]
     else:
         assert out[0][2] is True and out[1][2] is True
+
+
+def _fake_system(hhs, n, base):
+    """A particle-system struct whose arrays are never touched: hhs_dist_create only
+    records the peer addresses."""
+    import ctypes
+    c = hhs.CParticleSystem()
+    c.n = n
+    for k, name in enumerate(("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "ts", "m")):
+        setattr(c, name, ctypes.cast(ctypes.c_void_p(base + 8 * n * k), ctypes.POINTER(ctypes.c_double)))
+    c._base = ctypes.c_void_p(base)
+    return c
+
+
+def test_dist_create_validates_ranks_replicas_and_barrier(hhs):
+    ok = lambda _s: True
+    reps = [_fake_system(hhs, 1000, 1 << 40), _fake_system(hhs, 1000, 1 << 41),
+            _fake_system(hhs, 1000, 1 << 42)]
+    d = hhs.Dist(1, 3, reps, ok, 0)  # host-only: no device call
+    d.destroy()
+    d = hhs.Dist(0, 1, [None], ok)   # one rank needs no replicas
+    d.destroy()
+    bad = [
+        lambda: hhs.Dist(3, 3, reps, ok),                       # rank out of range
+        lambda: hhs.Dist(0, 9, reps * 3, ok),                   # more ranks than one node
+        lambda: hhs.Dist(0, 3, [reps[0], None, reps[2]], ok),   # a missing replica
+        lambda: hhs.Dist(0, 2, [reps[0], _fake_system(hhs, 0, 1 << 43)], ok),  # empty peer
+        lambda: hhs.Dist(0, 3, [reps[0], reps[1], _fake_system(hhs, 999, 1 << 43)], ok),
+        lambda: hhs.Dist(0, 2, reps[:2], ok, -1),               # negative threshold
+    ]
+    for make in bad:
+        with pytest.raises(hhs.HHSError) as e:
+            make()
+        assert e.value.status == 1
+
+
+def test_dist_callback_errors_become_a_failed_barrier(hhs):
+    """A barrier callable that raises is reported to the library as a failed barrier
+    (the callback never lets a Python exception cross into C), and the exception is kept."""
+    seen = []
+
+    def boom(stream):
+        seen.append(stream)
+        raise RuntimeError("peer lost")
+    d = hhs.Dist(0, 1, [None], boom, 0)
+    assert d._cb(None, None) == 1 and isinstance(d.failure, RuntimeError) and seen == [None]
+    good = hhs.Dist(0, 1, [None], lambda _s: True, 0)
+    assert good._cb(None, None) == 0
+    d.destroy()
+    good.destroy()

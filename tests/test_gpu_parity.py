@@ -162,6 +162,31 @@ def test_large_scan_forms_carry_the_running_total(cuda, variant):
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-2000:]
 
 
+def test_wave_barrier_wait_gives_up_and_reports_timeout(cuda, hhs, oracle):
+    """Failure detection without a GPU fault: every grid barrier of the wave-form scan
+    waits for one CTA more than the launch has; the bounded waits give up after 20 ms,
+    the call returns HHS_ERR_TIMEOUT, and the same workspace then serves a correct
+    compaction in the wave form."""
+    torch = cuda
+    n = (1 << 24) + 11
+    ws_bytes = hhs.scan_workspace_size(n)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    flags = np.random.default_rng(8).integers(0, 2, n).astype(np.int32)
+    dev = torch.from_numpy(flags).cuda()
+    out = torch.empty_like(dev)
+    assert hhs.scan_selftest_wave_barrier(_ptr(dev), _ptr(out), n, _ptr(ws), ws_bytes, 20000,
+                                          st) == 4
+    idx = torch.full_like(dev, -1)
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    hhs.compact_flags_i32(_ptr(dev), _ptr(out), _ptr(idx), _ptr(cnt), n, _ptr(ws), ws_bytes, st)
+    assert hhs.scan_workspace_status(_ptr(ws), st) == 0
+    k = int(cnt.item())
+    assert k == int(flags.sum())
+    assert np.array_equal(out.cpu().numpy(), oracle.scan_exclusive(flags))
+    assert np.array_equal(idx.cpu().numpy()[:k], np.flatnonzero(flags).astype(np.int32))
+
+
 def test_scan_lookback_wait_gives_up_and_reports_timeout(cuda, hhs, oracle):
     """Failure detection without a GPU fault: with the first tile left out, every look-back
     waits for a predecessor that never publishes; the bounded waits give up, the call
