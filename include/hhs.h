@@ -235,6 +235,12 @@ hhs_status hhs_dist_destroy(hhs_dist* d);
  * contiguous ranges of equal cost to within one sink. Host-only arithmetic. */
 hhs_status hhs_dist_shard(int32_t n_fast, int32_t n_slow, int32_t rank, int32_t world,
                           int32_t* lo, int32_t* hi);
+/* Subtrees in which no launch reaches min_pairs pair terms run, by default, as one
+ * launch of the device-resident engine (the kernel of hhs_hold_step) from their own
+ * level, identically on every rank. on = 0 keeps them on the host-driven schedule. With
+ * the engine, the FP64 replicas still equal hhs_hold_step_host bit for bit; the mixed
+ * ones equal a one-rank run with the same min_pairs. */
+hhs_status hhs_dist_set_subtree_engine(hhs_dist* d, int32_t on);
 /* One top-level step (hold_step, src/hold.cuh:51-181) of the rank's replica sys. */
 hhs_status hhs_hold_step_dist(hhs_ctx* ctx, hhs_dist* d, hhs_particle_system* sys, int32_t n,
                               double dt, int32_t calc_timestep, hhs_precision prec,

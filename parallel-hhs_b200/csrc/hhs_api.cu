@@ -2,6 +2,7 @@
 // points (timesteps / split / kick_slow / kick_sf / drift / update_system) and the
 // host-driven HOLD schedule.
 #include <atomic>
+#include <cmath>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -502,6 +503,7 @@ struct hhs_dist {
     hhs_barrier_fn barrier = nullptr;
     void* user = nullptr;
     long long min_pairs = 0;
+    bool engine_below = true;  // subtrees below min_pairs on the engine
 };
 
 namespace {
@@ -556,10 +558,16 @@ bool dist_shares(const hhs_dist* d, double pairs) {
 // partition counts are read back (the reference synchronises the device at the same
 // point, src/split.cuh:430) to decide the recursion. Level k's subsystem is the fast
 // list of level k-1 (the whole system at level 0). With d, the timestep and kick
-// launches of at least d->min_pairs pair terms are split across the ranks.
+// launches of at least d->min_pairs pair terms are split across the ranks, and a subtree
+// too small for that (no launch in it reaches min_pairs: a kick has at most n(n-1) pair
+// terms) runs as one launch of the device-resident engine from its own level,
+// identically on every rank.
 hhs_status hold_host(hhs_ctx* c, const SoA& P, const int32_t* S, int n, int level, double dt,
                      bool calc, hhs_precision prec, cudaStream_t s, const hhs_dist* d) {
     if (level >= c->max_levels) return HHS_ERR_DEPTH;
+    if (d && d->engine_below && c->engine_host && c->engine_bytes &&
+        (double)n * (double)(n - 1) < (double)d->min_pairs)
+        return engine_hold_step(c, P, n, std::ldexp(dt, level), calc, prec, false, s, level);
     auto* prof = static_cast<Profiler*>(c->prof);
     const bool timed = prof && prof->on;
     Profiler::Rec rec{};
@@ -658,6 +666,12 @@ extern "C" hhs_status hhs_dist_create(hhs_dist** out, int32_t rank, int32_t worl
     d->user = user;
     d->min_pairs = min_pairs;
     *out = d;
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_dist_set_subtree_engine(hhs_dist* d, int32_t on) {
+    if (!d) return HHS_ERR_INVALID_ARG;
+    d->engine_below = on != 0;
     return HHS_OK;
 }
 

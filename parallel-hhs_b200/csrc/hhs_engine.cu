@@ -68,6 +68,7 @@ struct EParams {
     int n_top, n_max, max_levels, small_n, calc_top, profile, units_per_cta, warp_n, mid_n;
     int mid_dist_n;  // cluster subtree solver: nodes above this size are spread over the cluster
     int packed;  // mixed kick: two sinks per thread in packed FP32x2 arithmetic
+    int top_level;  // level of the node the launch starts from (0: the whole system)
     double dt_top, eta, eta_s2, eps2;
     float inv_eta_s2, inv_eta, eps2f;
     int32_t* fast_lists;
@@ -2138,7 +2139,7 @@ __global__ void __launch_bounds__(kEB, 2) k_engine(EParams E) {
     unsigned long long t_last = 0;
     prof_begin(E, sm);
     prof_mark(E, W, t_last, -1, 0.0, sm);
-    run_hold<PREC, kModeGrid>(E, 0, E.calc_top != 0, W, sm, t_last);
+    run_hold<PREC, kModeGrid>(E, E.top_level, E.calc_top != 0, W, sm, t_last);
     prof_end(E, sm);
 }
 
@@ -2413,11 +2414,14 @@ hhs_status engine_reset_barrier(hhs_ctx* c, cudaStream_t stream) {
 }
 
 hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool calc_ts,
-                            hhs_precision prec, bool profile, cudaStream_t stream) {
+                            hhs_precision prec, bool profile, cudaStream_t stream,
+                            int top_level) {
     auto* eh = static_cast<EngineHost*>(c->engine_host);
     if (!eh) return HHS_ERR_INVALID_ARG;
+    if (top_level < 0 || top_level >= c->max_levels) return HHS_ERR_INVALID_ARG;
     EParams E;
     E.P = P;
+    E.top_level = top_level;
     E.n_top = n;
     E.n_max = c->n_max;
     E.max_levels = c->max_levels < kMaxLevels - 1 ? c->max_levels : kMaxLevels - 1;
@@ -2657,6 +2661,7 @@ extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, d
     E.mid_n = b->mid_n;
     E.mid_dist_n = b->mid_dist_n;
     E.packed = b->packed;
+    E.top_level = 0;
     E.dt_top = dt;
     E.eta = b->params.eta;
     E.eps2 = b->params.eps * b->params.eps;

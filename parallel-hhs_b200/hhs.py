@@ -128,6 +128,7 @@ SIGNATURES = {
                                        ctypes.POINTER(CParticleSystem), BARRIER_FN, _vp,
                                        ctypes.c_int64]),
     "hhs_dist_destroy": (ctypes.c_int, [_vp]),
+    "hhs_dist_set_subtree_engine": (ctypes.c_int, [_vp, ctypes.c_int32]),
     "hhs_dist_shard": (ctypes.c_int, [ctypes.c_int32] * 4 + [_ip, _ip]),
     "hhs_hold_step_dist": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(CParticleSystem),
                                           ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
@@ -632,9 +633,10 @@ class Dist:
     same process, a PeerView of another process, or a CParticleSystem); replicas[rank] is
     not used. barrier(stream) returns True once every rank's work enqueued on its stream
     before the call is complete before any later work (False: a peer failed or did not
-    arrive). Launches of at least min_pairs pair terms are split across the ranks."""
+    arrive). Launches of at least min_pairs pair terms are split across the ranks; with
+    subtree_engine, subtrees below that run as one engine launch on every rank."""
 
-    def __init__(self, rank, world, replicas, barrier, min_pairs=1 << 24):
+    def __init__(self, rank, world, replicas, barrier, min_pairs=1 << 24, subtree_engine=True):
         arr = (CParticleSystem * world)()
         for r, p in enumerate(replicas):
             if r != rank and p is not None:
@@ -652,6 +654,8 @@ class Dist:
         self.h = _vp()
         _check(lib().hhs_dist_create(ctypes.byref(self.h), rank, world, arr, self._cb, None,
                                      int(min_pairs)), "hhs_dist_create")
+        _check(lib().hhs_dist_set_subtree_engine(self.h, int(bool(subtree_engine))),
+               "hhs_dist_set_subtree_engine")
         self.rank, self.world = rank, world
 
     def step(self, ctx, sys, n, dt, calc_timestep=True, prec=PREC_MIXED, stream=None):
@@ -720,7 +724,8 @@ class DistHold:
     every result into all replicas over NVLink. The replicas stay bit-identical to
     each other and to hhs_hold_step_host on one GPU."""
 
-    def __init__(self, ctx, sys, group=None, min_pairs=1 << 24, timeout=30.0, barrier=None):
+    def __init__(self, ctx, sys, group=None, min_pairs=1 << 24, timeout=30.0, barrier=None,
+                 subtree_engine=True):
         import torch.distributed as tdist
         self.rank = tdist.get_rank(group)
         self.world = tdist.get_world_size(group)
@@ -735,7 +740,8 @@ class DistHold:
             self.views[r] = PeerView(h, n)
             replicas.append(self.views[r])
         self.barrier = barrier if barrier is not None else PeerBarrier(group, timeout)
-        self.dist = Dist(self.rank, self.world, replicas, self.barrier, min_pairs)
+        self.dist = Dist(self.rank, self.world, replicas, self.barrier, min_pairs,
+                         subtree_engine)
         self.ctx, self.sys = ctx, sys
 
     def step(self, n, dt, calc_timestep=True, prec=PREC_MIXED, stream=None):

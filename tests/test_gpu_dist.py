@@ -37,7 +37,8 @@ def _host_reference(hhs, s0, n, steps, prec, dt=1 / 64, eps=0.0):
     return out
 
 
-def _run_threads(hhs, torch, s0, n, world, steps, prec, min_pairs, dt=1 / 64, eps=0.0):
+def _run_threads(hhs, torch, s0, n, world, steps, prec, min_pairs, dt=1 / 64, eps=0.0,
+                 subtree_engine=False):
     systems = [hhs.ParticleSystem(n) for _ in range(world)]
     ctxs = [hhs.Context(n, eps=eps) for _ in range(world)]
     streams = [torch.cuda.Stream() for _ in range(world)]
@@ -55,7 +56,8 @@ def _run_threads(hhs, torch, s0, n, world, steps, prec, min_pairs, dt=1 / 64, ep
             return True
         return fn
 
-    dists = [hhs.Dist(r, world, systems, barrier_of(r), min_pairs) for r in range(world)]
+    dists = [hhs.Dist(r, world, systems, barrier_of(r), min_pairs, subtree_engine)
+             for r in range(world)]
     errors = [None] * world
 
     def work(r):
@@ -131,7 +133,7 @@ def test_a_failed_barrier_ends_the_step_with_a_peer_error(hhs, cuda):
     ctx.destroy()
 
 
-def _ipc_worker(rank, world, port, q, n, steps, prec):
+def _ipc_worker(rank, world, port, q, n, steps, prec, min_pairs=0, engine=False):
     import torch
     import torch.distributed as tdist
     import hhs
@@ -142,27 +144,42 @@ def _ipc_worker(rank, world, port, q, n, steps, prec):
     s0 = hhs.plummer(n, 44)
     sy, ctx = hhs.ParticleSystem(n), hhs.Context(n)
     sy.upload(s0)
-    dh = hhs.DistHold(ctx, sy, min_pairs=0, timeout=60.0)
+    dh = hhs.DistHold(ctx, sy, min_pairs=min_pairs, timeout=60.0, subtree_engine=engine)
     for _ in range(steps):
         dh.step(n, 1 / 64, True, prec)
     torch.cuda.synchronize()
-    got = _digest(sy.download(n))
+    mine = sy.download(n)
+    got = _digest(mine)
     dh.close()
     tdist.barrier()  # no rank frees its system while a peer still maps it
-    ref = _digest(_host_reference(hhs, s0, n, steps, prec)) if rank == 0 else None
-    q.put((rank, got, ref))
+    ref = one = None
+    dx = 0.0
+    if rank == 0:
+        host = _host_reference(hhs, s0, n, steps, prec)
+        ref = _digest(host)
+        dx = float(max(np.max(np.abs(mine[k] - host[k])) for k in ("x", "y", "z")))
+        if engine:  # the same schedule on one rank, in this process
+            one = _digest(_run_threads(hhs, torch, s0, n, 1, steps, prec, min_pairs,
+                                       subtree_engine=True)[0][0])
+    q.put((rank, got, ref, one, dx))
     tdist.barrier()
     tdist.destroy_process_group()
 
 
-@pytest.mark.parametrize("prec", [0, 1])
-def test_two_processes_share_one_system_through_cuda_ipc(cuda, prec):
+@pytest.mark.parametrize("prec,min_pairs,engine", [(0, 0, False), (1, 0, False),
+                                                    (0, 1 << 18, True), (1, 1 << 18, True)])
+def test_two_processes_share_one_system_through_cuda_ipc(cuda, prec, min_pairs, engine):
     """Two processes on one GPU, each mapping the other's system with CUDA IPC and a gloo
-    peer barrier between launches: both replicas end equal to the one-GPU host step."""
+    peer barrier between launches: both replicas end equal to the one-GPU host step.
+    With the subtree engine (subtrees below min_pairs as engine launches from their
+    level; the two processes' launches are time-sliced, never concurrent), FP64 still
+    equals the host step, and mixed equals a one-rank run of the same schedule and stays
+    within the mixed tolerance of the host step."""
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    port = 33500 + os.getpid() % 1000 + prec
-    procs = [ctx.Process(target=_ipc_worker, args=(r, 2, port, q, 1536, 2, prec))
+    port = 33500 + os.getpid() % 1000 + prec + (2 if engine else 0)
+    procs = [ctx.Process(target=_ipc_worker,
+                         args=(r, 2, port, q, 1536, 2, prec, min_pairs, engine))
              for r in range(2)]
     for p in procs:
         p.start()
@@ -170,7 +187,12 @@ def test_two_processes_share_one_system_through_cuda_ipc(cuda, prec):
     for p in procs:
         p.join(timeout=120)
         assert p.exitcode == 0
-    assert out[0][1] == out[1][1] == out[0][2]
+    assert out[0][1] == out[1][1]
+    if prec == 0 or not engine:
+        assert out[0][1] == out[0][2]
+    if engine:
+        assert out[0][1] == out[0][3]
+        assert out[0][4] < 1e-6
 
 
 def _nccl_worker(port, q, n, steps):
