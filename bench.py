@@ -26,7 +26,6 @@ sys.path.insert(0, os.path.join(ROOT, "parallel-hhs_b200"))
 
 METRIC = "pair interactions/s & HOLD steps/s at |dE/E|<=1e-6 vs plain FP64 GPU path"
 KICK_FLOPS_PER_PAIR = 20.0   # conventional direct-sum count (Nyland, Harris & Prins 2007)
-TS_FLOPS_PER_PAIR = 50.0     # FP operations of the reference pair-timestep expression
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -83,7 +82,7 @@ MASS_NAMES = {0: "equal-mass", 1: "Salpeter dN/dm ~ m^-2.35 on [0.1,100]",
 def workload_name(a):
     return (f"Plummer N={a.n} {MASS_NAMES[getattr(a, 'mass', 0)]}, Henon units, eta={a.eta}, "
             f"dt_top=2^{int(round(__import__('math').log2(a.dt)))}, "
-            f"{a.prec} precision, one top-level HOLD step per step")
+            f"one top-level HOLD step per step")
 
 
 # ------------------------------------------------------------------------ ranks
@@ -208,15 +207,35 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------ reference arm
-def run_reference(a, rank, world):
-    """CPU FP64 restatement of the reference HOLD step on the host cores (rank 0)."""
+def mapped_libraries():
+    """Shared objects mapped into this process (from /proc/self/maps)."""
+    out = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 6 and (parts[-1].endswith(".so") or ".so." in parts[-1]):
+                    out.add(parts[-1])
+    except OSError:
+        pass
+    return sorted(out)
+
+
+def run_reference(a, rank, world, isolated=True):
+    """CPU FP64 restatement of the reference HOLD step on the host cores (rank 0). The
+    initial conditions come from the oracle's own generator (the same arrays as the
+    product's), so with isolated=True (the --impl reference process) nothing of the
+    product library is loaded; that is checked before the timed loop."""
     if rank != 0:
         return None
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import hhs
     import oracle
     oracle.build()
-    s = hhs.plummer(a.n, a.seed)
+    s = oracle.plummer(a.n, a.seed, getattr(a, "mass", 0))
+    if isolated:
+        product = [m for m in mapped_libraries() if "libhhs_b200" in m]
+        if product:
+            raise RuntimeError(f"reference arm has the product library mapped: {product}")
     budget_s = 150.0
     t0 = time.perf_counter()
     oracle.hold_step(s, a.dt, True, a.eta)           # warm-up steps, as many as asked for
@@ -232,16 +251,20 @@ def run_reference(a, rank, world):
     el = time.perf_counter() - t0
     v = steps / el
     cores = oracle.threads()
-    return {"metric": METRIC, "value": v, "unit": "HOLD steps/s", "impl": "reference",
-            "n_gpus": world, "steps": steps, "warmup": warm, "ms_per_step": el / steps * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": workload_name(a).replace(a.prec, "fp64")},
-            "cpu_baseline": {"value": v, "unit": "HOLD steps/s", "cores": cores, "kind": "port",
-                             "sample": f"{steps} top-level HOLD step(s) of the same N={a.n} "
-                                       f"Plummer sphere, FP64 CPU restatement, OpenMP "
-                                       f"{cores} threads (the reference has no CPU HOLD)"},
-            "e2e": {"value": v, "unit": "HOLD steps/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+    out = {"metric": METRIC, "value": v, "unit": "HOLD steps/s", "impl": "reference",
+           "n_gpus": world, "steps": steps, "warmup": warm, "ms_per_step": el / steps * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic", "config": {"workload": workload_name(a), "n": a.n, "eta": a.eta,
+                                            "dt_top": a.dt, "precision": "fp64 (CPU oracle)"},
+           "cpu_baseline": {"value": v, "unit": "HOLD steps/s", "cores": cores, "kind": "port",
+                            "sample": f"{steps} top-level HOLD step(s) of the same N={a.n} "
+                                      f"Plummer sphere, FP64 CPU restatement, OpenMP "
+                                      f"{cores} threads (the reference has no CPU HOLD)"},
+           "e2e": {"value": v, "unit": "HOLD steps/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    if isolated:
+        out["libraries_mapped"] = [m for m in mapped_libraries() if ROOT in m]
+    return out
 
 
 # ------------------------------------------------------------------------ our arm
@@ -409,33 +432,60 @@ def run_ours(a, rank, world, torch, dist):
 ENGINE_16K_DRAM_BYTES = 1.456128e6 + 1.422080e6
 
 
-def roofline(res, a, peaks_tflops):
-    """Roofline of the dominant kernel, the persistent HOLD kernel (one launch per step):
-    algorithmic flops per launch (timestep pairs x 50 + kick pairs x 20, from the run's own
-    work counters) over the launch's CUDA-event duration, against the measured FMA-chain
-    peak; the timestep and kick phases are reported beside it from the phase profile."""
+def nominal_fp32_tflops(torch):
+    """Nominal FP32 FMA peak of the device: SMs x 128 FP32 lanes x 2 flops x max SM clock
+    (nvidia-smi clocks.max.sm; 1965 MHz on B200 when it cannot be read)."""
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = 1965.0
+    try:
+        q = subprocess.run(["nvidia-smi", "--query-gpu=clocks.max.sm", "--format=csv,noheader,nounits",
+                            "-i", str(torch.cuda.current_device())], capture_output=True,
+                           text=True, timeout=20)
+        mhz = float(q.stdout.strip().splitlines()[0])
+    except (OSError, ValueError, IndexError, subprocess.SubprocessError):
+        pass
+    return sms * 128 * 2 * mhz * 1e6 / 1e12
+
+
+def roofline(res, a, peaks_tflops, nominal_tflops):
+    """Roofline of the dominant kernel, the persistent HOLD kernel (one launch per step),
+    counted as the kick work alone: kick pairs (N_s(N_s-1) + 2 N_s N_f per node, from the
+    run's own work counters) x 20 flops over the launch's CUDA-event duration. Timestep
+    pair evaluations are reported beside it as a rate, with no flop credit. The peak is
+    the measured FP32 FMA-chain rate of this B200; the nominal FP32 peak is given too."""
     prof = res["prof"]
     st = res["stats"]
     launch_ms = res["t_ms"] / a.steps
-    flops = (st["ts_pairs"] * TS_FLOPS_PER_PAIR + st["kick_pairs"] * KICK_FLOPS_PER_PAIR) / a.steps
+    flops = st["kick_pairs"] * KICK_FLOPS_PER_PAIR / a.steps
     achieved = flops / (launch_ms * 1e-3) / 1e12
     peak = peaks_tflops[0] if a.prec == "mixed" else peaks_tflops[1]
     phases = {}
-    for kind, fpp in (("timesteps", TS_FLOPS_PER_PAIR), ("kick", KICK_FLOPS_PER_PAIR)):
+    for kind in ("timesteps", "kick", "split", "update", "cluster_node", "subtree"):
         p = (prof or {}).get(kind)
         if p and p["ms"] > 0:
-            tf = p["pairs"] * fpp / (p["ms"] * 1e-3) / 1e12
-            phases[kind] = {"achieved": tf, "frac": tf / peak, "flops_per_pair": fpp,
-                            "share_of_step": p["ms"] / res["t_ms"]}
+            phases[kind] = {"ms_per_step": p["ms"] / a.steps, "share_of_step": p["ms"] / res["t_ms"]}
+    kp = (prof or {}).get("kick")
+    if kp and kp["ms"] > 0:
+        tf = kp["pairs"] * KICK_FLOPS_PER_PAIR / (kp["ms"] * 1e-3) / 1e12
+        phases["kick"].update({"achieved": tf, "frac": tf / peak})
+    tp = (prof or {}).get("timesteps")
+    if tp and tp["ms"] > 0:
+        phases["timesteps"]["unordered_pair_evaluations_per_s"] = tp["pairs"] / 2 / (tp["ms"] * 1e-3)
     default = (a.n == 16384 and a.prec == "mixed" and a.workload == "plummer16k")
-    return {"bound": "fp32-fma" if a.prec == "mixed" else "fp64-fma", "kernel": "k_engine",
-            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "peak_source": "measured FMA-chain peak of this B200 (hhs_measure_fma_peaks); "
-                           "the pair kernels use neither tensor cores nor HBM bandwidth",
-            "flops_per_launch": flops, "launch_ms": launch_ms, "phases": phases,
-            "traffic": ENGINE_16K_DRAM_BYTES if default else None,
-            "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
-                            "of this workload" if default else None}
+    out = {"bound": "fp32-fma" if a.prec == "mixed" else "fp64-fma", "kernel": "k_engine",
+           "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+           "peak_source": "measured FMA-chain peak of this B200 (hhs_measure_fma_peaks); "
+                          "the pair kernels use neither tensor cores nor HBM bandwidth",
+           "flops_per_launch": flops, "flops_per_pair": KICK_FLOPS_PER_PAIR,
+           "work": "kick pairs x 20 flops (timestep work not counted)",
+           "launch_ms": launch_ms, "phases": phases,
+           "traffic": ENGINE_16K_DRAM_BYTES if default else None,
+           "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                           "of this workload" if default else None}
+    if a.prec == "mixed":
+        out["peak_nominal"] = nominal_tflops
+        out["frac_of_nominal"] = achieved / nominal_tflops
+    return out
 
 
 # ------------------------------------------------------------------------ other workloads
@@ -643,7 +693,7 @@ def run_plain1k(a, torch):
             "dE_over_E": (hhs.energy_host(gpu) - e0) / e0}
 
 
-def run_validate(a, torch):
+def run_validate(a, torch, tuning=None):
     """Integrates the workload to t_end in mixed precision and in FP64 (the FP64 device
     schedule reproduces the CPU oracle bit for bit) and reports both energy errors, the
     position deviation and the split agreement of the final state."""
@@ -656,6 +706,8 @@ def run_validate(a, torch):
     res = {}
     for name, prec in (("mixed", hhs.PREC_MIXED), ("fp64", hhs.PREC_FP64)):
         ctx = hhs.Context(a.n, 64, eta=a.eta)
+        if tuning:
+            ctx.set_tuning(**{k: v for k, v in tuning.items() if k != "ms_per_step"})
         d = hhs.ParticleSystem(a.n)
         d.upload(ics)
         ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -681,6 +733,53 @@ def run_validate(a, torch):
             "results": out, "max_abs_dx_mixed_vs_fp64": dx,
             "median_rel_ts_diff": float(np.median(rel_ts)),
             "speedup_mixed_vs_fp64_device": out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"]}
+
+
+def run_side_measurements(a, torch, res):
+    """Short measurements beside the headline, each well under a minute of GPU time:
+    - config 2's acceptance numbers: the same sphere integrated to t = 1 (64 top-level
+      steps) in mixed precision and on the FP64 device schedule (bit-exact with the CPU
+      oracle), |dE/E| of both and max |dx| between the final states;
+    - the scan of 2^28 Bernoulli(0.5) int32 flags (8 B per element) and stream
+      compaction, checked bit for bit against the reference's own scan on the same GPU;
+    - the batched workload (512 clusters, N log-uniform in [64, 4096]): cluster steps/s."""
+    out = {}
+    v = run_validate(argparse.Namespace(**{**vars(a), "t_end": 1.0}), torch, res.get("tuning"))
+    out["accuracy_t1"] = {
+        "t_end": 1.0, "steps": v["steps"],
+        "dE_over_E_t1": v["results"]["mixed"]["dE_over_E"],
+        "dE_over_E_t1_fp64": v["results"]["fp64"]["dE_over_E"],
+        "max_dx_vs_fp64": v["max_abs_dx_mixed_vs_fp64"],
+        "median_rel_ts_diff_vs_fp64": v["median_rel_ts_diff"],
+        "target": "|dE/E| <= 1e-6 after one N-body time"}
+    out["dE_over_E_t1"] = out["accuracy_t1"]["dE_over_E_t1"]
+    out["max_dx_vs_fp64"] = out["accuracy_t1"]["max_dx_vs_fp64"]
+    sc = run_scan(argparse.Namespace(**{**vars(a), "scan_log2n": 28, "steps": 5}), torch)
+    row = sc["sweep"][0]
+    hbm, src = hbm_peak()
+    out["scan_2p28"] = {"n": 1 << 28, "p": 0.5, "scan_GBps": row["scan_GBps"],
+                        "scan_frac_of_hbm": row["scan_GBps"] / hbm,
+                        "compact_GBps": row["compact_GBps"],
+                        "hbm_peak_GBps": hbm, "hbm_peak_source": src,
+                        "bytes_per_element": 8,
+                        "scan_properties_ok": row["scan_properties_ok"],
+                        "bit_exact_vs_reference": row.get("bit_exact_vs_reference"),
+                        "reference_scan_GBps": row.get("reference_scan_GBps")}
+    torch.cuda.empty_cache()
+    b = run_batched(argparse.Namespace(**{**vars(a), "steps": 5, "warmup": 3}), torch)
+    out["batched_512"] = {k: b[k] for k in ("value", "unit", "ms_per_step", "steps",
+                                            "pair_interactions_per_s", "dE_over_E_after_steps")}
+    out["batched_512"]["n_total"] = b["config"]["n_total"]
+    return out
+
+
+def hbm_peak():
+    """Measured HBM copy bandwidth of this pool's B200s (GB/s), else the fallback."""
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(peaks["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError, TypeError):
+        return 6650.0, "fallback"
 
 
 def main():
@@ -717,17 +816,10 @@ def main():
         if rank == 0:
             fn = {"scan": run_scan, "validate": run_validate, "plain1k": run_plain1k}[a.workload]
             out = fn(a, torch)
-            peaks = None
-            try:
-                peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-            except (OSError, ValueError):
-                pass
             if a.workload == "scan" and "roofline" in out:
-                # the measured copy bandwidth of this pool's B200s, else an earlier
-                # measurement on the same pool (6.65 TB/s)
-                hbm = peaks["hbm_gbs"] if peaks and "hbm_gbs" in peaks else 6650.0
+                hbm, src = hbm_peak()
                 out["roofline"]["peak"] = hbm
-                out["roofline"]["peak_source"] = "measured" if peaks else "fallback"
+                out["roofline"]["peak_source"] = src
                 out["roofline"]["frac"] = out["value"] / hbm
             print(json.dumps(out), flush=True)
         if dist is not None:
@@ -736,9 +828,12 @@ def main():
         return
     res = run_ours(a, rank, world, torch, dist)
     cpu = None
+    extra = {}
     if rank == 0 and world == 1 and not a.no_baselines:
-        ref = run_reference(argparse.Namespace(**{**vars(a), "steps": 1}), 0, 1)
+        ref = run_reference(argparse.Namespace(**{**vars(a), "steps": 1}), 0, 1, isolated=False)
         cpu = ref["cpu_baseline"]
+        if a.workload == "plummer16k":
+            extra = run_side_measurements(a, torch, res)
     if rank == 0:
         step_ms = res["t_ms"] / a.steps
         line = {
@@ -760,7 +855,7 @@ def main():
             "e2e": res["e2e"],
             "gpu_launches": res["launches"],
             "clocks": res["clocks"],
-            "roofline": roofline(res, a, res["fma_peaks"]),
+            "roofline": roofline(res, a, res["fma_peaks"], nominal_fp32_tflops(torch)),
             "kernel_profile": res["prof"],
             "fma_peaks_tflops": {"fp32": res["fma_peaks"][0], "fp64": res["fma_peaks"][1],
                                  "fp32x2_packed": res["fma2_peak"]},
@@ -774,6 +869,8 @@ def main():
         if "fp64_engine_steps_per_s" in res:
             line["fp64_device_schedule"] = {"value": res["fp64_engine_steps_per_s"],
                                             "unit": "HOLD steps/s"}
+            line["speedup_vs_fp64_device_schedule"] = res["value"] / res["fp64_engine_steps_per_s"]
+        line.update(extra)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -277,6 +277,19 @@ hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out, int64_t n
 #define HHS_SCAN_NOALLOC_MAX_N (1LL << 26)
 hhs_status hhs_scan_exclusive_i32_noalloc(const int32_t* d_in, int32_t* d_out, int64_t n,
                                           void* stream);
+/* Status of the last hhs_scan_exclusive_i32_noalloc on the current device (its bounded
+ * look-back waits record a timeout in the array instead of hanging): synchronises the
+ * stream; HHS_ERR_TIMEOUT if a wait gave up, in which case the output is not valid.
+ * The array's device address is looked up once per device and kept for the life of the
+ * process; it does not survive cudaDeviceReset (the library's module is reloaded), so
+ * do not call these functions after a device reset. */
+hhs_status hhs_scan_noalloc_status(void* stream);
+/* Bounded-wait self-test on the same static array: the scan with its first tile left
+ * out, every look-back giving up after max_polls (1..2^22) polls. Synchronises the
+ * stream; returns HHS_ERR_TIMEOUT when the waits ran out as designed. 8192 <= n <= 2^26. */
+hhs_status hhs_scan_noalloc_selftest_stalled_predecessor(const int32_t* d_in, int32_t* d_out,
+                                                         int64_t n, uint32_t max_polls,
+                                                         void* stream);
 
 /* Stream compaction (the split of a flag array, src/split.cuh:573-610 on int32 data):
  * d_idx[k] = index of the k-th nonzero flag, *d_count = number of nonzero flags, and
@@ -340,6 +353,16 @@ hhs_status hhs_ctx_get_profile(hhs_ctx* ctx, hhs_profile* out);
 /* The device schedule's phase times per kind and level since profiling was switched on:
  * ms[kind*64 + level] milliseconds and counts[kind*64 + level] phases (either may be NULL). */
 hhs_status hhs_ctx_get_level_profile(hhs_ctx* ctx, double* ms, uint64_t* counts);
+
+/* Node trace of the device-resident step (hhs_hold_step): while set, every node of the
+ * recursion -- each call of the reference's hold_step, src/hold.cuh:51-181 -- appends
+ * {level, n, n_fast, calc_timestep} (4 int32) to d_nodes in call order, and *d_count
+ * (device uint64, zeroed by the caller) counts the nodes, also past capacity. n_fast is
+ * the count after the N_fast == 1 fold. d_nodes is 16-byte aligned device memory; NULL
+ * (with d_count NULL) switches the trace off. The same record as the CPU restatement's
+ * trace, so a hierarchy can be compared node by node. */
+hhs_status hhs_ctx_set_trace(hhs_ctx* ctx, int32_t* d_nodes, int64_t capacity,
+                             uint64_t* d_count);
 
 /* Kernel launches issued by this library since it was loaded (all contexts). */
 uint64_t hhs_kernel_launch_count(void);

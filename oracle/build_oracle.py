@@ -29,8 +29,17 @@ def build_oracle():
     return oracle.build()
 
 
-def build_ref(reference_root="/root/reference", verbose=False):
+def reference_root_default():
+    """The reference tree: $HHS_REFERENCE_ROOT, else a checkout named `reference` beside
+    this repository's root."""
+    return os.environ.get("HHS_REFERENCE_ROOT",
+                          os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
+
+
+def build_ref(reference_root=None, verbose=False):
     """Compiles the reference shims if the reference tree exists; returns built paths."""
+    if reference_root is None:
+        reference_root = reference_root_default()
     src = os.path.join(reference_root, "src")
     if not os.path.isdir(src):
         return []

@@ -343,3 +343,90 @@ void oracle_energy(int n, const double* x, const double* y, const double* z,
     out[0] = ke.s + ke.c;
     out[1] = pot.s + pot.c;
 }
+
+/* ---- seeded initial conditions for the CPU-baseline leg ----------------------------
+ * The benchmark's reference arm builds its Plummer sphere here, so that the process
+ * timing the CPU path never maps the product library. The inputs of the two arms must
+ * be the same arrays, so this follows the same published methods with the same random
+ * stream and the same operation order as the product's generator (a CPU test compares
+ * the two bit for bit):
+ *  - SplitMix64 (Steele, Lea & Flood 2014), 53-bit uniforms on the open interval (0,1);
+ *  - masses first, independent of position: equal, Salpeter dN/dm ~ m^-2.35 on
+ *    [0.1,100] by inverse CDF, or 90/10 two-component (m = 1 or 10); normalised to 1;
+ *  - Plummer radius by the inverted cumulative mass (Aarseth, Henon & Wielen 1974),
+ *    radii beyond 10 rejected; speed by von Neumann rejection on q^2 (1-q^2)^(7/2);
+ *    isotropic directions;
+ *  - centre-of-mass frame, then Henon units: x *= beta, v /= sqrt(beta) with
+ *    beta = -4 E (E from oracle_energy); an unbound sample stays in structural units. */
+typedef struct { uint64_t s; } osm64;
+static uint64_t osm64_next(osm64* g) {
+    uint64_t z = (g->s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+static double osm64_uniform(osm64* g) {
+    return ((double)(osm64_next(g) >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+int oracle_plummer(int n, uint64_t seed, int mass_spectrum, double* x, double* y, double* z,
+                   double* vx, double* vy, double* vz, double* m) {
+    const double two_pi = 2.0 * 3.14159265358979323846;
+    osm64 g = {seed};
+    if (n < 2 || mass_spectrum < 0 || mass_spectrum > 2) return 1;
+    double mtot = 0.0;
+    for (int i = 0; i < n; i++) {
+        double mi = 1.0;
+        if (mass_spectrum == 1) {
+            const double p = 1.0 - 2.35, a = pow(0.1, p), b = pow(100.0, p);
+            mi = pow(a + osm64_uniform(&g) * (b - a), 1.0 / p);
+        } else if (mass_spectrum == 2) {
+            mi = osm64_uniform(&g) < 0.1 ? 10.0 : 1.0;
+        }
+        m[i] = mi;
+        mtot += mi;
+    }
+    for (int i = 0; i < n; i++) m[i] /= mtot;
+    for (int i = 0; i < n; i++) {
+        double r, q, w;
+        do {
+            r = 1.0 / sqrt(pow(osm64_uniform(&g), -2.0 / 3.0) - 1.0);
+        } while (!(r <= 10.0));
+        const double cth = 1.0 - 2.0 * osm64_uniform(&g);
+        const double phi = two_pi * osm64_uniform(&g);
+        const double sth = sqrt(1.0 - cth * cth);
+        x[i] = r * sth * cos(phi);
+        y[i] = r * sth * sin(phi);
+        z[i] = r * cth;
+        do {
+            q = osm64_uniform(&g);
+            w = osm64_uniform(&g);
+        } while (0.1 * w >= q * q * pow(1.0 - q * q, 3.5));
+        const double v = q * sqrt(2.0) * pow(1.0 + r * r, -0.25);
+        const double cv = 1.0 - 2.0 * osm64_uniform(&g);
+        const double pv = two_pi * osm64_uniform(&g);
+        const double sv = sqrt(1.0 - cv * cv);
+        vx[i] = v * sv * cos(pv);
+        vy[i] = v * sv * sin(pv);
+        vz[i] = v * cv;
+    }
+    double c[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < n; i++) {
+        c[0] += m[i] * x[i]; c[1] += m[i] * y[i]; c[2] += m[i] * z[i];
+        c[3] += m[i] * vx[i]; c[4] += m[i] * vy[i]; c[5] += m[i] * vz[i];
+    }
+    for (int i = 0; i < n; i++) {
+        x[i] -= c[0]; y[i] -= c[1]; z[i] -= c[2];
+        vx[i] -= c[3]; vy[i] -= c[4]; vz[i] -= c[5];
+    }
+    double e[2];
+    oracle_energy(n, x, y, z, vx, vy, vz, m, e);
+    const double etot = e[0] + e[1];
+    if (!(etot < 0.0)) return 0;
+    const double beta = -4.0 * etot, vs = 1.0 / sqrt(beta);
+    for (int i = 0; i < n; i++) {
+        x[i] *= beta; y[i] *= beta; z[i] *= beta;
+        vx[i] *= vs; vy[i] *= vs; vz[i] *= vs;
+    }
+    return 0;
+}

@@ -100,6 +100,13 @@ void oracle_energy(int n, const double* x, const double* y, const double* z,
                    const double* vx, const double* vy, const double* vz,
                    const double* m, double* out);
 
+/* Seeded Plummer sphere in Henon units (mass_spectrum 0 equal, 1 Salpeter on [0.1,100],
+ * 2 two-component 90/10): the inputs of the benchmark's CPU-baseline leg, identical bit
+ * for bit to the product generator's for the same seed. Returns 0, or 1 on bad
+ * arguments. */
+int oracle_plummer(int n, uint64_t seed, int mass_spectrum, double* x, double* y, double* z,
+                   double* vx, double* vy, double* vz, double* m);
+
 /* Single-threaded variants for the timed CPU baseline are the same functions with
  * OMP_NUM_THREADS=1; oracle_threads reports the OpenMP thread count in use. */
 int oracle_threads(void);

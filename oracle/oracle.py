@@ -68,6 +68,8 @@ def lib():
                                                                      ctypes.POINTER(Trace)]
         L.oracle_energy.argtypes = [ctypes.c_int] + [_dp] * 7 + [_dp]
         L.oracle_threads.restype = ctypes.c_int
+        L.oracle_plummer.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_int] + [_dp] * 7
+        L.oracle_plummer.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -150,6 +152,19 @@ def energy(s):
     lib().oracle_energy(len(s["x"]), _d(s["x"]), _d(s["y"]), _d(s["z"]), _d(s["vx"]),
                         _d(s["vy"]), _d(s["vz"]), _d(s["m"]), _d(out))
     return out[0] + out[1], out
+
+
+def plummer(n, seed, mass_spectrum=0):
+    """Seeded Plummer sphere in Henon units (dict of float64 arrays plus ts and id), the
+    same arrays as the product generator gives for the same seed."""
+    s = {k: np.empty(n) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    rc = lib().oracle_plummer(n, seed, mass_spectrum,
+                              *[_d(s[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")])
+    if rc != 0:
+        raise ValueError(f"oracle_plummer: bad arguments (n={n}, mass={mass_spectrum})")
+    s["ts"] = np.zeros(n)
+    s["id"] = np.arange(n, dtype=np.int32)
+    return s
 
 
 def threads():

@@ -379,6 +379,12 @@ extern "C" hhs_status hhs_ctx_get_tuning(hhs_ctx* c, hhs_tuning* t) {
     return engine_get_tuning(c, t);
 }
 
+extern "C" hhs_status hhs_ctx_set_trace(hhs_ctx* c, int32_t* d_nodes, int64_t capacity,
+                                        uint64_t* d_count) {
+    if (!c) return HHS_ERR_INVALID_ARG;
+    return engine_set_trace(c, d_nodes, capacity, reinterpret_cast<unsigned long long*>(d_count));
+}
+
 extern "C" hhs_status hhs_ctx_get_launch(hhs_ctx* c, int32_t* grid_ctas, int32_t* smem_bytes) {
     if (!c) return HHS_ERR_INVALID_ARG;
     return engine_get_launch(c, grid_ctas, smem_bytes);

@@ -83,6 +83,9 @@ struct EParams {
     unsigned* rate_acc;  // [n_max] max pair rate per list position (FP32 bits), kept at 0
     EngineState* st;
     unsigned* err;
+    int4* trace;                        // node record {level, n, n_fast, calc} in call order
+    unsigned long long* trace_count;    // nodes recorded (may exceed trace_cap)
+    long long trace_cap;
 };
 
 // Cluster subtree solver state (one replica per CTA of the cluster): a subsystem of at
@@ -152,6 +155,14 @@ __device__ __forceinline__ unsigned long long gtimer() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
+}
+
+// One node of the recursion, recorded in call order (the order of the reference's
+// hold_step calls) when the caller asked for a trace.
+__device__ __forceinline__ void trace_node(const EParams& E, int level, int n, int nf, bool calc) {
+    if (!E.trace) return;
+    const unsigned long long k = atomicAdd(E.trace_count, 1ull);
+    if ((long long)k < E.trace_cap) E.trace[k] = make_int4(level, n, nf, calc ? 1 : 0);
 }
 
 __device__ __forceinline__ int ld_volatile_i32(const int32_t* p) {
@@ -826,6 +837,7 @@ __device__ void scatter_phase(const EParams& E, const int32_t* S, int n, double 
         const int nf = fold ? 0 : nf_raw;
         E.counts[level].n_fast = nf;
         E.counts[level].n_slow = n - nf;
+        trace_node(E, level, n, nf, calc);
         if (nf == 0) *E.leaf_time += dt;
         const double ns = (double)(n - nf), nfd = (double)nf;
         atomicAdd(reinterpret_cast<unsigned long long*>(&E.stats->nodes), 1ull);
@@ -901,6 +913,7 @@ __device__ void split_phase(const EParams& E, const int32_t* S, int n, double dt
             const int nf = nf_raw == 1 ? 0 : nf_raw;
             E.counts[level].n_fast = nf;
             E.counts[level].n_slow = n - nf;
+            trace_node(E, level, n, nf, calc);
             if (nf == 0) *E.leaf_time += dt;
             const double ns = (double)(n - nf), nfd = (double)nf;
             atomicAdd(reinterpret_cast<unsigned long long*>(&E.stats->nodes), 1ull);
@@ -1098,6 +1111,7 @@ __device__ void tiny_hold(const EParams& E, const int32_t* S, int n, int level0,
                     sm.wfast[d] = F;
                     sm.wlone[d] = lone;
                     const int nf = __popc(F);
+                    trace_node(E, lvl, cnt, nf, (calcm & bit) != 0);
                     const double ns = (double)(cnt - nf), nfd = (double)nf;
                     if (nf == 0) *E.leaf_time += dt;
                     atomicAdd(reinterpret_cast<unsigned long long*>(&E.stats->nodes), 1ull);
@@ -1428,7 +1442,7 @@ template <int PREC>
 __device__ void warp_subtree(const EParams& E, MidState& M, const unsigned* memw, int nw,
                              int cnt, int level0, bool calc0, unsigned long long& nodes,
                              int& maxl, double& kpairs, double& tpairs, double& leaf,
-                             bool& ok) {
+                             bool& ok, bool rec) {
     const int lane = threadIdx.x & 31;
     // lane l takes the l-th member
     {
@@ -1519,6 +1533,7 @@ __device__ void warp_subtree(const EParams& E, MidState& M, const unsigned* memw
                 M.wf[dd] = F;
                 M.wl[dd] = lone;
                 const int nf = __popc(F);
+                if (rec) trace_node(E, lvl, n_here, nf, (calcm & bit) != 0);
                 const double ns = (double)(n_here - nf), nfd = (double)nf;
                 nodes++;
                 maxl = max(maxl, lvl);
@@ -1708,7 +1723,7 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
                 // at most 32 members: the whole subtree on warp 0 of every CTA
                 if (warp == 0)
                     warp_subtree<PREC>(E, M, memw, nw, M.nmem[d], lvl, (calcm & bit) != 0,
-                                       nodes, maxl, kpairs, tpairs, leaf, ok);
+                                       nodes, maxl, kpairs, tpairs, leaf, ok, rank == 0);
                 __syncthreads();
                 calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
                 d--;
@@ -1806,6 +1821,7 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
             if (tid == 0) {
                 M.lone[d] = lone;
                 if (nf > 0) M.nmem[d + 1] = nf;
+                if (rank == 0) trace_node(E, lvl, nm, nf, (calcm & bit) != 0);
                 const double ns = (double)(nm - nf), nfd = (double)nf;
                 nodes++;
                 maxl = max(maxl, lvl);
@@ -2247,6 +2263,9 @@ struct EngineHost {
     unsigned* rate_acc = nullptr;
     unsigned long long* tile_status = nullptr;
     int n_max = 0;
+    int32_t* trace = nullptr;                 // caller's node-record buffer (4 int32 each)
+    unsigned long long* trace_count = nullptr;
+    long long trace_cap = 0;
 };
 
 constexpr size_t kAl = 256;
@@ -2405,6 +2424,19 @@ hhs_status engine_get_profile(hhs_ctx* c, hhs_profile* out, bool reset) {
     return HHS_OK;
 }
 
+hhs_status engine_set_trace(hhs_ctx* c, int32_t* nodes, int64_t capacity,
+                            unsigned long long* count) {
+    auto* eh = static_cast<EngineHost*>(c->engine_host);
+    if (!eh) return HHS_ERR_INVALID_ARG;
+    if ((nodes == nullptr) != (count == nullptr) || capacity < 0 ||
+        (nodes && (reinterpret_cast<uintptr_t>(nodes) & 15u)))
+        return HHS_ERR_INVALID_ARG;
+    eh->trace = nodes;
+    eh->trace_count = count;
+    eh->trace_cap = nodes ? capacity : 0;
+    return HHS_OK;
+}
+
 hhs_status engine_reset_barrier(hhs_ctx* c, cudaStream_t stream) {
     auto* eh = static_cast<EngineHost*>(c->engine_host);
     if (!eh) return HHS_ERR_INVALID_ARG;
@@ -2452,6 +2484,9 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
     E.rate_acc = eh->rate_acc;
     E.st = eh->st;
     E.err = c->err;
+    E.trace = reinterpret_cast<int4*>(eh->trace);
+    E.trace_count = eh->trace_count;
+    E.trace_cap = eh->trace_cap;
     const int pi = prec == HHS_PREC_FP64 ? 0 : 1;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(eh->grid[pi], 1, 1);
@@ -2679,6 +2714,9 @@ extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, d
     E.rate_acc = nullptr;
     E.st = nullptr;
     E.err = b->d_err;
+    E.trace = nullptr;
+    E.trace_count = nullptr;
+    E.trace_cap = 0;
     B.offsets = b->d_offsets;
     B.order = b->d_order;
     B.n_sys = b->n_sys;

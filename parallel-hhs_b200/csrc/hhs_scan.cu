@@ -792,6 +792,33 @@ extern "C" hhs_status hhs_scan_exclusive_i32_noalloc(const int32_t* d_in, int32_
     return HHS_OK;
 }
 
+// Status of the last allocation-free scan on the current device: the error word of the
+// static array's header (set by a look-back wait that gave up), read after synchronising
+// the stream. Each hhs_scan_exclusive_i32_noalloc call clears the word before it runs.
+extern "C" hhs_status hhs_scan_noalloc_status(void* stream) {
+    void* ws = nullptr;
+    hhs_status st = static_scan_workspace(&ws);
+    if (st != HHS_OK) return st;
+    return hhs_scan_workspace_status(ws, stream);
+}
+
+// Bounded-wait self-test of the allocation-free scan: the same stalled-predecessor run
+// as hhs_scan_selftest_stalled_predecessor, on the static array. Its status comes back
+// through hhs_scan_noalloc_status (HHS_ERR_TIMEOUT when the waits ran out as designed).
+extern "C" hhs_status hhs_scan_noalloc_selftest_stalled_predecessor(const int32_t* d_in,
+                                                                    int32_t* d_out, int64_t n,
+                                                                    uint32_t max_polls,
+                                                                    void* stream) {
+    if (n < 2 * (int64_t)ScanT::TILE || n > kStaticScanMaxN || !d_in || !d_out ||
+        max_polls == 0 || max_polls > HHS_SPIN_LIMIT)
+        return HHS_ERR_INVALID_ARG;
+    void* ws = nullptr;
+    hhs_status st = static_scan_workspace(&ws);
+    if (st != HHS_OK) return st;
+    return hhs_scan_selftest_stalled_predecessor(d_in, d_out, n, ws, kStaticScanBytes, max_polls,
+                                                 stream);
+}
+
 extern "C" hhs_status hhs_scan_workspace_status(const void* d_workspace, void* stream) {
     if (!d_workspace) return HHS_ERR_INVALID_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);

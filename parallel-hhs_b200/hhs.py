@@ -149,6 +149,10 @@ SIGNATURES = {
     "hhs_scan_selftest_wave_barrier": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp,
                                                        ctypes.c_size_t, ctypes.c_uint32, _vp]),
     "hhs_scan_exclusive_i32_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp]),
+    "hhs_scan_noalloc_status": (ctypes.c_int, [_vp]),
+    "hhs_ctx_set_trace": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp]),
+    "hhs_scan_noalloc_selftest_stalled_predecessor": (ctypes.c_int, [_vp, _vp, ctypes.c_int64,
+                                                                     ctypes.c_uint32, _vp]),
     "hhs_compact_flags_i32": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int64, _vp,
                                              ctypes.c_size_t, _vp]),
     "hhs_ic_plummer": (ctypes.c_int, [ctypes.c_int32, ctypes.c_uint64, ctypes.c_int32]
@@ -316,6 +320,11 @@ class Context:
 
     def reset_stats(self, stream=None):
         _check(lib().hhs_ctx_reset_stats(self.h, stream), "reset_stats")
+
+    def set_trace(self, nodes_ptr, capacity, count_ptr):
+        """Records every node of hhs_hold_step into device buffers (4 int32 per node and a
+        uint64 count); set_trace(None, 0, None) switches it off."""
+        _check(lib().hhs_ctx_set_trace(self.h, nodes_ptr, capacity, count_ptr), "set_trace")
 
     def set_tuning(self, small_n=None, units_per_cta=None, ctas_per_sm=None, warp_n=None,
                    cluster_size=None, mid_n=None, packed=None, mid_dist_n=None):

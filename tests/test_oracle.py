@@ -228,3 +228,16 @@ def test_hold_step_leaf_dt_sum(oracle, hhs):
     tr, nodes = oracle.hold_step(s, 1.0 / 32, True, 0.03, capacity=100000)
     leaves = nodes[nodes[:, 2] == 0]
     assert tr.leaf_time == pytest.approx(np.sum((1.0 / 32) / 2.0 ** leaves[:, 0]), rel=1e-15)
+
+
+def test_oracle_plummer_equals_product_generator_bit_for_bit(oracle, hhs):
+    """The benchmark's CPU-baseline leg builds its inputs with the oracle's generator (so
+    that process never maps the product library); both arms must integrate the same
+    arrays."""
+    for n, seed, mass in ((2, 1, 0), (1024, 2024, 0), (16384, 2024, 0), (4096, 5, 1),
+                          (3000, 9, 2)):
+        a, b = oracle.plummer(n, seed, mass), hhs.plummer(n, seed, mass)
+        for k in ("x", "y", "z", "vx", "vy", "vz", "m", "ts", "id"):
+            assert np.array_equal(a[k], b[k]), (n, seed, mass, k)
+    with pytest.raises(ValueError):
+        oracle.plummer(1, 3)

@@ -66,3 +66,24 @@ def test_noalloc_scan_limits(cuda, hhs):
     assert int(out[0]) == 0
     assert torch.equal(out[1:] - out[:-1], flags[:-1])
     assert int(out[-1]) + int(flags[-1]) == int(flags.sum())
+
+
+def test_noalloc_scan_reports_a_lookback_timeout(cuda, hhs):
+    """The allocation-free scan's bounded look-back waits record a timeout in its fixed
+    array; hhs_scan_noalloc_status reads it back. A run with its first tile left out makes
+    every wait run out (no GPU fault: each wait gives up and its CTA returns); the status
+    is HHS_ERR_TIMEOUT, and the next ordinary call clears it and scans correctly."""
+    torch = cuda
+    lib = hhs.lib()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    n = 50_000
+    a = np.random.default_rng(5).integers(0, 2, n).astype(np.int32)
+    dev = torch.from_numpy(a).cuda()
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    assert lib.hhs_scan_noalloc_selftest_stalled_predecessor(_ptr(dev), _ptr(out), n, 2000,
+                                                             stream) == 4
+    assert lib.hhs_scan_noalloc_status(stream) == 4
+    assert lib.hhs_scan_exclusive_i32_noalloc(_ptr(dev), _ptr(out), n, stream) == 0
+    assert lib.hhs_scan_noalloc_status(stream) == 0
+    expect = np.concatenate([[0], np.cumsum(a)[:-1]]).astype(np.int32)
+    assert np.array_equal(out.cpu().numpy(), expect)
