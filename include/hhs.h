@@ -241,6 +241,25 @@ hhs_status hhs_dist_shard(int32_t n_fast, int32_t n_slow, int32_t rank, int32_t 
  * the engine, the FP64 replicas still equal hhs_hold_step_host bit for bit; the mixed
  * ones equal a one-rank run with the same min_pairs. */
 hhs_status hhs_dist_set_subtree_engine(hhs_dist* d, int32_t on);
+/* Configuration agreement. The order of the mixed-precision sums (and so the bits of
+ * every replica) depends on the engine's launch shape and tuning, which each rank sets
+ * on its own context. fn(user, value, out_min, out_max) returns in *out_min / *out_max
+ * the minimum and maximum of `value` over all ranks (for example two all-reduces on the
+ * ranks' communicator) and 0, or non-zero if a peer failed. With it set, every
+ * hhs_hold_step_dist first compares a hash of this rank's configuration
+ * (hhs_dist_config_hash) across the ranks and returns HHS_ERR_INVALID_ARG on every rank
+ * when they differ, before any kernel runs; HHS_ERR_PEER if fn fails. Host-only. */
+typedef int32_t (*hhs_minmax_fn)(void* user, uint64_t value, uint64_t* out_min,
+                                 uint64_t* out_max);
+hhs_status hhs_dist_set_agreement(hhs_dist* d, hhs_minmax_fn fn, void* user);
+/* The hash compared by the agreement check: precision, launch shape (grid CTAs of the
+ * persistent kernel for that precision), tuning, n, dt, eta and eps. Host-only. */
+hhs_status hhs_dist_config_hash(const hhs_tuning* t, int32_t grid_ctas, hhs_precision prec,
+                                int32_t n, double dt, hhs_params params, uint64_t* out);
+/* Runs the agreement check on a given hash: HHS_OK when every rank passed the same
+ * value (or no agreement function is set), HHS_ERR_INVALID_ARG when they differ,
+ * HHS_ERR_PEER if the function failed. Every rank must call it. Host-only. */
+hhs_status hhs_dist_check(hhs_dist* d, uint64_t config_hash);
 /* One top-level step (hold_step, src/hold.cuh:51-181) of the rank's replica sys. */
 hhs_status hhs_hold_step_dist(hhs_ctx* ctx, hhs_dist* d, hhs_particle_system* sys, int32_t n,
                               double dt, int32_t calc_timestep, hhs_precision prec,
@@ -363,6 +382,14 @@ hhs_status hhs_ctx_get_level_profile(hhs_ctx* ctx, double* ms, uint64_t* counts)
  * trace, so a hierarchy can be compared node by node. */
 hhs_status hhs_ctx_set_trace(hhs_ctx* ctx, int32_t* d_nodes, int64_t capacity,
                              uint64_t* d_count);
+
+/* Accelerations of the first n particles from one another (softened by the context's eps)
+ * computed by the mixed-precision kick phase of hhs_hold_step -- the same tiles, chunks,
+ * FP32 pair arithmetic and compensated sums -- written to sys->ax, ay, az. A diagnostic
+ * for checking that arithmetic against an FP64 direct sum; it uses the context's kick
+ * scratch, so do not run it concurrently with a step on the same context. */
+hhs_status hhs_engine_kick_accelerations(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n,
+                                         void* stream);
 
 /* Kernel launches issued by this library since it was loaded (all contexts). */
 uint64_t hhs_kernel_launch_count(void);

@@ -379,6 +379,13 @@ extern "C" hhs_status hhs_ctx_get_tuning(hhs_ctx* c, hhs_tuning* t) {
     return engine_get_tuning(c, t);
 }
 
+extern "C" hhs_status hhs_engine_kick_accelerations(hhs_ctx* c, hhs_particle_system* sys,
+                                                    int32_t n, void* stream) {
+    if (!c || !sys_ok(sys) || n < 1 || n > sys->n || n > c->n_max) return HHS_ERR_INVALID_ARG;
+    return engine_kick_accelerations(c, soa_of(sys), sys->ax, sys->ay, sys->az, n,
+                                     static_cast<cudaStream_t>(stream));
+}
+
 extern "C" hhs_status hhs_ctx_set_trace(hhs_ctx* c, int32_t* d_nodes, int64_t capacity,
                                         uint64_t* d_count) {
     if (!c) return HHS_ERR_INVALID_ARG;
@@ -510,6 +517,8 @@ struct hhs_dist {
     void* user = nullptr;
     long long min_pairs = 0;
     bool engine_below = true;  // subtrees below min_pairs on the engine
+    hhs_minmax_fn agree = nullptr;  // min/max of a value over the ranks (configuration check)
+    void* agree_user = nullptr;
 };
 
 namespace {
@@ -681,6 +690,57 @@ extern "C" hhs_status hhs_dist_set_subtree_engine(hhs_dist* d, int32_t on) {
     return HHS_OK;
 }
 
+extern "C" hhs_status hhs_dist_set_agreement(hhs_dist* d, hhs_minmax_fn fn, void* user) {
+    if (!d) return HHS_ERR_INVALID_ARG;
+    d->agree = fn;
+    d->agree_user = user;
+    return HHS_OK;
+}
+
+// FNV-1a over the fields that fix the operation order of a step: the precision, the
+// engine's launch shape and tuning, the system size, the step and the parameters.
+extern "C" hhs_status hhs_dist_config_hash(const hhs_tuning* t, int32_t grid_ctas,
+                                           hhs_precision prec, int32_t n, double dt,
+                                           hhs_params params, uint64_t* out) {
+    if (!t || !out) return HHS_ERR_INVALID_ARG;
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) {
+        for (int k = 0; k < 8; k++) {
+            h ^= (v >> (8 * k)) & 0xffu;
+            h *= 1099511628211ull;
+        }
+    };
+    auto bits = [](double v) {
+        uint64_t u;
+        std::memcpy(&u, &v, sizeof(u));
+        return u;
+    };
+    mix((uint64_t)prec);
+    mix((uint64_t)(uint32_t)grid_ctas);
+    mix((uint64_t)(uint32_t)t->small_n);
+    mix((uint64_t)(uint32_t)t->units_per_cta);
+    mix((uint64_t)(uint32_t)t->ctas_per_sm);
+    mix((uint64_t)(uint32_t)t->warp_n);
+    mix((uint64_t)(uint32_t)t->cluster_size);
+    mix((uint64_t)(uint32_t)t->mid_n);
+    mix((uint64_t)(uint32_t)t->packed);
+    mix((uint64_t)(uint32_t)t->mid_dist_n);
+    mix((uint64_t)(uint32_t)n);
+    mix(bits(dt));
+    mix(bits(params.eta));
+    mix(bits(params.eps));
+    *out = h;
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_dist_check(hhs_dist* d, uint64_t config_hash) {
+    if (!d) return HHS_ERR_INVALID_ARG;
+    if (!d->agree) return HHS_OK;
+    uint64_t lo = 0, hi = 0;
+    if (d->agree(d->agree_user, config_hash, &lo, &hi) != 0) return HHS_ERR_PEER;
+    return lo == hi ? HHS_OK : HHS_ERR_INVALID_ARG;
+}
+
 extern "C" hhs_status hhs_dist_destroy(hhs_dist* d) {
     delete d;
     return HHS_OK;
@@ -702,6 +762,19 @@ extern "C" hhs_status hhs_hold_step_dist(hhs_ctx* c, hhs_dist* d, hhs_particle_s
     if (!c || !d || !sys_ok(sys) || n <= 0 || !(dt > 0.0)) return HHS_ERR_INVALID_ARG;
     if (n > sys->n || n > c->n_max || (d->world > 1 && n > d->n_cap)) return HHS_ERR_CAPACITY;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (d->agree) {
+        // every rank must run the same operations in the same order, or replicas drift
+        hhs_tuning t{};
+        int32_t grid[2] = {0, 0};
+        hhs_status st = engine_get_tuning(c, &t);
+        if (st == HHS_OK) st = engine_get_launch(c, grid, nullptr);
+        uint64_t h = 0;
+        if (st == HHS_OK)
+            st = hhs_dist_config_hash(&t, grid[prec == HHS_PREC_FP64 ? 0 : 1], prec, n, dt,
+                                      c->params, &h);
+        if (st == HHS_OK) st = hhs_dist_check(d, h);
+        if (st != HHS_OK) return st;
+    }
     hhs_status st = hold_host(c, soa_of(sys), nullptr, n, 0, dt, calc_timestep != 0, prec, s, d);
     if (st != HHS_OK) return st;
     return hhs_ctx_check(c, stream);

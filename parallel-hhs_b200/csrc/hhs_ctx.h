@@ -49,6 +49,8 @@ hhs_status engine_get_level_profile(hhs_ctx* c, double* ms, uint64_t* counts);
 hhs_status engine_reset_barrier(hhs_ctx* c, cudaStream_t stream);
 hhs_status engine_set_trace(hhs_ctx* c, int32_t* nodes, int64_t capacity,
                             unsigned long long* count);
+hhs_status engine_kick_accelerations(hhs_ctx* c, const SoA& P, double* ax, double* ay,
+                                     double* az, int n, cudaStream_t stream);
 // top_level > 0: the launch walks the subtree of the level-top_level node, whose members
 // are the fast list of level top_level - 1 (written by the host-driven schedule); dt is
 // the top-level step and the node's own step is dt / 2^top_level.

@@ -38,12 +38,15 @@
 #include "hhs_kernels.h"
 #include "hhs_pairmath.cuh"
 #include "hhs_scan.cuh"
+#include "hhs_tma.cuh"
 
 using namespace hhs;
 
 namespace {
 
 constexpr int kEB = 256;          // engine block size (one sink per thread per unit)
+constexpr int kKB = 2 * kEB;      // sinks per block of the mixed grid kick (two per thread)
+constexpr int kTS = 1024;         // source records per shared-memory tile of that kick
 constexpr int kMaxChunks = 32;    // source chunks per node (partial-sum slots)
 constexpr int kMaxLevels = 64;    // per-level state is kept in 64-bit masks
 constexpr unsigned long long kBarrierTimeoutNs = 60ull * 1000000000ull;
@@ -83,6 +86,12 @@ struct EParams {
     unsigned* rate_acc;  // [n_max] max pair rate per list position (FP32 bits), kept at 0
     EngineState* st;
     unsigned* err;
+    // packed kick sources of each grid level (mixed precision): slow particle q of the
+    // level's slow list, drifted by half the level's step, as double-single position
+    // (pk_a = hi + mass, pk_b = lo), written by the split, read by bulk copies
+    float4* pk_a;   // [pk_levels][n_max]
+    float4* pk_b;   // [pk_levels][n_max]
+    int pk_levels;
     int4* trace;                        // node record {level, n, n_fast, calc} in call order
     unsigned long long* trace_count;    // nodes recorded (may exceed trace_cap)
     long long trace_cap;
@@ -128,11 +137,14 @@ struct __align__(16) Smem {
     int bcast;
     unsigned bar_k;               // grid barriers passed by this CTA in this launch
     unsigned epoch;               // look-back epoch of the current split
+    unsigned kphase;              // parity of the next phase of kbar
+    __align__(8) uint64_t kbar;   // completion barrier of the kick's source-tile copies
     // last, so that the persistent kernel's dynamic allocation can extend it to a MidState
     union {
         struct { float4 A[kEB], B[kEB], V[kEB]; } tsm;         // mixed timestep tiles
         struct { double x[kEB], y[kEB], z[kEB], vx[kEB], vy[kEB], vz[kEB], m[kEB]; } tsd;
         struct { float4 A[kEB], B[kEB]; } km;                   // mixed kick tiles
+        struct { float4 A[kTS], B[kTS]; } kt;                   // grid kick source tile
         struct { float4 P0[kEB], P1[kEB], P2[kEB]; float2 M[kEB]; } kx;  // packed kick tiles
         struct { double x[kEB], y[kEB], z[kEB], m[kEB]; } kd;   // FP64 kick tiles
         struct {                                                  // tiny-subtree state
@@ -400,29 +412,11 @@ __device__ void ts_unit(const EParams& E, const int32_t* S, int n, int ib, int j
 // products of two negated values and the mass sum are unchanged), so each unordered pair
 // is evaluated once, in the unit (row block of kEB list positions, column block of kCB)
 // that holds it with i < j. Rows keep their running max rate in a register; the column
-// maxima of a warp's 32 rows come from a butterfly transpose-reduce (31 shuffles per 16
-// columns). Both are merged into rate_acc with an integer atomicMax on the FP32 bit
-// pattern (rates are >= 0, so integer order is float order). Max is exact and
+// maxima of a warp's 32 rows come from one warp max-reduction (redux.sync) per column.
+// Both are merged into rate_acc with an integer atomicMax on the FP32 bit pattern (rates
+// are >= 0, so integer order is float order). Max is exact and
 // order-independent: the result equals the all-pairs evaluation bit for bit.
 constexpr int kCB = 32;
-
-// Column maxima of a 32-row x 16-column block held one row per lane: after the first
-// exchange both half-warps hold the pairwise maxima of the same 16 columns, then a
-// transpose-reduce over the 16 lanes of each half leaves column (lane & 15) in r[0].
-__device__ __forceinline__ void butterfly_max16(float (&r)[16], int lane) {
-#pragma unroll
-    for (int c = 0; c < 16; c++) r[c] = fmaxf(r[c], __shfl_xor_sync(HHS_FULL_MASK, r[c], 16));
-#pragma unroll
-    for (int k = 8; k >= 1; k >>= 1) {
-        const bool upper = (lane & k) != 0;
-#pragma unroll
-        for (int c = 0; c < k; c++) {
-            const float send = upper ? r[c] : r[c + k];
-            const float keep = upper ? r[c + k] : r[c];
-            r[c] = fmaxf(keep, __shfl_xor_sync(HHS_FULL_MASK, send, k));
-        }
-    }
-}
 
 // Units [u0, u1) of the upper triangle of (256-row block, kCB-column block) tiles, in
 // row-major order: a contiguous range per CTA, so consecutive units mostly share their row
@@ -488,24 +482,24 @@ __device__ void ts_sym_range(const EParams& E, const int32_t* S, int n, int u0, 
                 }
             }
         }
-#pragma unroll 1
-        for (int g = 0; g < kCB / 16; g++) {
-            float r[16];
-#pragma unroll
-            for (int c = 0; c < 16; c++) {
-                const int jl = g * 16 + c;
-                const float4 A = sm.u.tsm.A[jl], B = sm.u.tsm.B[jl], V = sm.u.tsm.V[jl];
-                const float rate = ts_pair_rate_mixed(
-                    ds_diff(xi.hi, xi.lo, A.x, B.x), ds_diff(yi.hi, yi.lo, A.y, B.y),
-                    ds_diff(zi.hi, zi.lo, A.z, B.z), vxi - V.x, vyi - V.y, vzi - V.z, mi + A.w,
-                    E.inv_eta_s2, E.inv_eta);
-                const bool ok = act && (jl < ncol) && (c0 + jl > i);
-                r[c] = ok ? rate : 0.0f;
-                rowmax = fmaxf(rowmax, r[c]);
-            }
-            butterfly_max16(r, lane);
-            if (lane < 16) sm.colred[warp][g * 16 + lane] = r[0];
+        // column maxima over the warp's 32 rows: one warp max-reduction per column on the
+        // rates' bit patterns (rates are >= 0 or +inf, so integer order is float order);
+        // lane c keeps column c's maximum
+        unsigned colmax = 0u;
+#pragma unroll 8
+        for (int jl = 0; jl < kCB; jl++) {
+            const float4 A = sm.u.tsm.A[jl], B = sm.u.tsm.B[jl], V = sm.u.tsm.V[jl];
+            const float rate = ts_pair_rate_mixed(
+                ds_diff(xi.hi, xi.lo, A.x, B.x), ds_diff(yi.hi, yi.lo, A.y, B.y),
+                ds_diff(zi.hi, zi.lo, A.z, B.z), vxi - V.x, vyi - V.y, vzi - V.z, mi + A.w,
+                E.inv_eta_s2, E.inv_eta);
+            const bool ok = act && (jl < ncol) && (c0 + jl > i);
+            const float r = ok ? rate : 0.0f;
+            rowmax = fmaxf(rowmax, r);
+            const unsigned cm = __reduce_max_sync(HHS_FULL_MASK, __float_as_uint(r));
+            colmax = lane == jl ? cm : colmax;
         }
+        sm.colred[warp][lane] = __uint_as_float(colmax);
         __syncthreads();
         if ((int)threadIdx.x < ncol) {
             float cm = 0.0f;
@@ -652,6 +646,187 @@ __device__ void kick_unit(const EParams& E, const int32_t* F, const int32_t* L, 
     }
 }
 
+
+// ---------------------------------------------------------------- grid kick (mixed)
+// The kick of a large node on the whole grid, mixed precision. Sources are staged in
+// shared memory tiles of up to kTS records: the slow ones (the majority of every node's
+// sources) arrive by bulk copy from the level's packed array, which the split wrote
+// once (position drifted by half the step, split to double-single, mass), and the fast
+// ones are gathered and split by the CTA. Work units are (block of 512 sinks, source
+// chunk) in chunk-major order, a contiguous range per CTA, so a CTA keeps its chunk
+// resident across consecutive units and stages it once. Each thread carries two sinks,
+// which share every shared-memory read. Pair terms are FP32: 1/d^3 from rsqrtf with one
+// Newton correction applied to its cube (y^3 (5/2 - 3/2 d2 y^2), the first-order Newton
+// step for d2^-3/2), summed per sink in 32-pair FP32 blocks that are added into Kahan-
+// compensated sums; the per-chunk sums go to k_part for the reduce phase as before.
+// Self pairs contribute exactly 0 (zero separation times a finite 1/d^3: d2 is floored
+// at 1e-20, which no separation in the state arrays ever reaches).
+struct SinkDS {
+    float nxh, nyh, nzh, nxl, nyl, nzl;  // negated double-single position
+};
+
+__device__ __forceinline__ void kick_pair_nr(const float4 A, const float4 B, const SinkDS& q,
+                                             float eps2, float& bx, float& by, float& bz) {
+    const float dx = __fadd_rn(__fadd_rn(A.x, q.nxh), __fadd_rn(B.x, q.nxl));
+    const float dy = __fadd_rn(__fadd_rn(A.y, q.nyh), __fadd_rn(B.y, q.nyl));
+    const float dz = __fadd_rn(__fadd_rn(A.z, q.nzh), __fadd_rn(B.z, q.nzl));
+    const float d2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2))), 1e-20f);
+    const float y = rsqrtf(d2);
+    const float y2 = __fmul_rn(y, y);
+    const float c = fmaf(-1.5f, __fmul_rn(d2, y2), 2.5f);
+    const float mr3 = __fmul_rn(__fmul_rn(A.w, __fmul_rn(y2, y)), c);
+    bx = fmaf(dx, mr3, bx);
+    by = fmaf(dy, mr3, by);
+    bz = fmaf(dz, mr3, bz);
+}
+
+// Sources [lo, hi) of the shared tile on one sink (32-pair blocks, Kahan across blocks).
+__device__ __forceinline__ void kick_span1(const Smem& sm, int lo, int hi, const SinkDS& q,
+                                           float eps2, float (&acc)[3], float (&cmp)[3]) {
+    int jb = lo;
+    for (; jb < hi; jb += 32) {
+        const int je = min(hi, jb + 32);
+        float b[3] = {0.f, 0.f, 0.f};
+#pragma unroll 4
+        for (int j = jb; j < je; j++) kick_pair_nr(sm.u.kt.A[j], sm.u.kt.B[j], q, eps2, b[0], b[1], b[2]);
+#pragma unroll
+        for (int c = 0; c < 3; c++) kahan_add(acc[c], cmp[c], b[c]);
+    }
+}
+
+// Sources [lo, hi) of the shared tile on two sinks at once (each record read once).
+__device__ __forceinline__ void kick_span2(const Smem& sm, int lo, int hi, const SinkDS& q0,
+                                           const SinkDS& q1, float eps2, float (&acc)[2][3],
+                                           float (&cmp)[2][3]) {
+    int jb = lo;
+    for (; jb + 32 <= hi; jb += 32) {
+        float b0[3] = {0.f, 0.f, 0.f}, b1[3] = {0.f, 0.f, 0.f};
+#pragma unroll 4
+        for (int j = jb; j < jb + 32; j++) {
+            const float4 A = sm.u.kt.A[j], B = sm.u.kt.B[j];
+            kick_pair_nr(A, B, q0, eps2, b0[0], b0[1], b0[2]);
+            kick_pair_nr(A, B, q1, eps2, b1[0], b1[1], b1[2]);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            kahan_add(acc[0][c], cmp[0][c], b0[c]);
+            kahan_add(acc[1][c], cmp[1][c], b1[c]);
+        }
+    }
+    if (jb < hi) {
+        float b0[3] = {0.f, 0.f, 0.f}, b1[3] = {0.f, 0.f, 0.f};
+        for (int j = jb; j < hi; j++) {
+            const float4 A = sm.u.kt.A[j], B = sm.u.kt.B[j];
+            kick_pair_nr(A, B, q0, eps2, b0[0], b0[1], b0[2]);
+            kick_pair_nr(A, B, q1, eps2, b1[0], b1[1], b1[2]);
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            kahan_add(acc[0][c], cmp[0][c], b0[c]);
+            kahan_add(acc[1][c], cmp[1][c], b1[c]);
+        }
+    }
+}
+
+// Stages source records [a, b) of the node (slow records [a, min(b, ns)) by bulk copy
+// from the packed arrays, fast ones gathered from the state arrays) into sm.u.kt.
+__device__ void kick_stage_tile(const EParams& E, const int32_t* F, const float4* PA,
+                                const float4* PB, int a, int b, int ns, Smem& sm) {
+    __syncthreads();  // every thread is done reading the previous tile
+    const int sb = min(b, ns);
+    const bool bulk = sb > a;
+    if (bulk && threadIdx.x == 0) {
+        const unsigned bytes = (unsigned)(sb - a) * (unsigned)sizeof(float4);
+        mbar_arrive_expect_tx(&sm.kbar, 2u * bytes);
+        bulk_load(sm.u.kt.A, PA + a, bytes, &sm.kbar);
+        bulk_load(sm.u.kt.B, PB + a, bytes, &sm.kbar);
+    }
+    const SoA& P = E.P;
+    for (int j = max(a, ns) + (int)threadIdx.x; j < b; j += kEB) {
+        const int g = F[j - ns];
+        const DS x = ds_split(P.x[g]), y = ds_split(P.y[g]), z = ds_split(P.z[g]);
+        sm.u.kt.A[j - a] = make_float4(x.hi, y.hi, z.hi, (float)P.m[g]);
+        sm.u.kt.B[j - a] = make_float4(x.lo, y.lo, z.lo, 0.0f);
+    }
+    if (bulk && !mbar_wait(&sm.kbar, sm.kphase, E.err)) {
+        // the copy did not complete in time: the error word ends the launch at the next
+        // grid barrier; let the copy land (bounded) before the buffer is reused
+        (void)mbar_wait(&sm.kbar, sm.kphase, nullptr);
+    }
+    __syncthreads();
+    if (bulk && threadIdx.x == 0) sm.kphase ^= 1u;
+}
+
+__device__ void kick_units_grid(const EParams& E, const int32_t* F, int nf, int ns, int lvl,
+                                int nch, int C, const Workers& W, Smem& sm) {
+    const int ntot = nf + ns;
+    const SoA& P = E.P;
+    const float4* PA = E.pk_a + (size_t)lvl * E.n_max;
+    const float4* PB = E.pk_b + (size_t)lvl * E.n_max;
+    const int nsb = (ntot + kKB - 1) / kKB;
+    const int nfb = nf / kKB;                        // blocks of fast sinks only
+    const int ncs = min(nch, (ns + C - 1) / C);      // chunks holding slow sources
+    const long long us = (long long)ncs * nsb;
+    const long long units = us + (long long)(nch - ncs) * (nsb - nfb);
+    const long long u0 = units * W.id / W.count, u1 = units * (W.id + 1) / W.count;
+    const float eps2 = E.eps2f;
+    int res_a = -1, res_b = -1;  // source records resident in sm.u.kt
+    for (long long u = u0; u < u1; u++) {
+        int jc, ib;
+        if (u < us) {
+            jc = (int)(u / nsb);
+            ib = (int)(u % nsb);
+        } else {
+            const long long v = u - us;
+            jc = ncs + (int)(v / (nsb - nfb));
+            ib = nfb + (int)(v % (nsb - nfb));
+        }
+        const int j0 = jc * C, j1 = min(ntot, j0 + C);
+        int sk[2], jend[2];
+        SinkDS q[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            sk[k] = ib * kKB + k * kEB + (int)threadIdx.x;
+            const bool act = sk[k] < ntot;
+            const bool slow = sk[k] >= nf;
+            q[k] = SinkDS{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            if (act) {
+                if (slow) {
+                    const float4 a = PA[sk[k] - nf], b = PB[sk[k] - nf];
+                    q[k] = SinkDS{-a.x, -a.y, -a.z, -b.x, -b.y, -b.z};
+                } else {
+                    const int g = F[sk[k]];
+                    const DS x = ds_split(P.x[g]), y = ds_split(P.y[g]), z = ds_split(P.z[g]);
+                    q[k] = SinkDS{-x.hi, -y.hi, -z.hi, -x.lo, -y.lo, -z.lo};
+                }
+            }
+            jend[k] = act ? (slow ? j1 : min(j1, ns)) : j0;
+        }
+        float acc[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+        float cmp[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+        for (int a = j0; a < j1; a += kTS) {
+            const int b = min(j1, a + kTS);
+            if (a != res_a || b != res_b) {
+                kick_stage_tile(E, F, PA, PB, a, b, ns, sm);
+                res_a = a;
+                res_b = b;
+            }
+            const int e0 = max(0, min(b, jend[0]) - a), e1 = max(0, min(b, jend[1]) - a);
+            const int m = min(e0, e1);
+            kick_span2(sm, 0, m, q[0], q[1], eps2, acc, cmp);
+            if (e0 > m) kick_span1(sm, m, e0, q[0], eps2, acc[0], cmp[0]);
+            if (e1 > m) kick_span1(sm, m, e1, q[1], eps2, acc[1], cmp[1]);
+        }
+        double* part = E.k_part;
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+            if (sk[k] < ntot)
+#pragma unroll
+                for (int c = 0; c < 3; c++)
+                    part[(size_t)(jc * 3 + c) * E.n_max + sk[k]] =
+                        (double)acc[k][c] - (double)cmp[k][c];
+    }
+}
 
 // ---------------------------------------------------------------- packed kick units
 // The mixed kick with two sinks per thread (s and s + kEB) evaluated together in packed
@@ -901,11 +1076,26 @@ __device__ void split_phase(const EParams& E, const int32_t* S, int n, double dt
         const int prefix = sm.bcast;
         if (i < n) {
             const int p = prefix + ex;
+            int q = -1;  // slow-list position (the first fast particle: the fold's slot)
             if (flag) {
                 F[p] = gi;
-                if (p == 0) L[n - 1] = gi;
+                if (p == 0) {
+                    L[n - 1] = gi;
+                    q = n - 1;
+                }
             } else {
                 L[i - p] = gi;
+                q = i - p;
+            }
+            if (PREC != HHS_PREC_FP64 && q >= 0 && E.pk_a && level < E.pk_levels) {
+                // packed kick source: the slow particle at its drifted kick position
+                const double h = dt * 0.5;
+                const DS x = ds_split(fma(E.P.vx[gi], h, E.P.x[gi]));
+                const DS y = ds_split(fma(E.P.vy[gi], h, E.P.y[gi]));
+                const DS z = ds_split(fma(E.P.vz[gi], h, E.P.z[gi]));
+                const size_t o = (size_t)level * E.n_max + q;
+                E.pk_a[o] = make_float4(x.hi, y.hi, z.hi, (float)E.P.m[gi]);
+                E.pk_b[o] = make_float4(x.lo, y.lo, z.lo, 0.0f);
             }
         }
         if (t == ntiles - 1 && threadIdx.x == 0) {
@@ -2099,8 +2289,10 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
             const int ns = ld_volatile_i32(&E.counts[lvl].n_slow);
             if (ns > 0) {
                 const int ntot = nf + ns;
+                const bool grid_tma = MODE == kModeGrid && PREC != HHS_PREC_FP64 && !E.packed &&
+                                      E.pk_a && lvl < E.pk_levels;
                 const bool x2 = PREC != HHS_PREC_FP64 && E.packed;
-                const int blk = x2 ? 2 * kEB : kEB;
+                const int blk = (x2 || grid_tma) ? 2 * kEB : kEB;
                 const int nch = chunks_for(ntot, W, PREC != HHS_PREC_FP64, E.units_per_cta, blk);
                 const int C = (ntot + nch - 1) / nch;
                 const int nsb = (ntot + blk - 1) / blk;
@@ -2110,7 +2302,8 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                 const int nfb = nf / blk;
                 const int jcs = min(nch, (ns + C - 1) / C);
                 const int uf = nfb * jcs;
-                const int units = uf + (nsb - nfb) * nch;
+                const int units = grid_tma ? 0 : uf + (nsb - nfb) * nch;
+                if (grid_tma) kick_units_grid(E, F, nf, ns, lvl, nch, C, W, sm);
                 for (int u = W.id; u < units; u += W.count) {
                     int ib, jc;
                     if (u < uf) {
@@ -2151,12 +2344,55 @@ __global__ void __launch_bounds__(kEB, 2) k_engine(EParams E) {
     extern __shared__ __align__(16) unsigned char engine_smem[];
     Smem& sm = *reinterpret_cast<Smem*>(engine_smem);
     const Workers W{(int)blockIdx.x, (int)gridDim.x, kModeGrid};
-    if (threadIdx.x == 0) sm.bar_k = 0u;  // published to thread 0 only; it alone uses it
+    if (threadIdx.x == 0) {
+        sm.bar_k = 0u;  // thread 0 alone uses it
+        sm.kphase = 0u;
+        mbar_init(&sm.kbar, 1u);
+        fence_barrier_init();
+    }
+    __syncthreads();
     unsigned long long t_last = 0;
     prof_begin(E, sm);
     prof_mark(E, W, t_last, -1, 0.0, sm);
     run_hold<PREC, kModeGrid>(E, E.top_level, E.calc_top != 0, W, sm, t_last);
     prof_end(E, sm);
+}
+
+// Probe of the mixed grid kick: the whole system as one node of slow particles (no
+// drift), packed, kicked by kick_units_grid and reduced per sink in the kick-reduce
+// phase's order; accelerations go to E.ts_part / rate_acc / tile_counts reinterpreted
+// as FP64 ax / ay / az (see engine_kick_accelerations).
+__global__ void __launch_bounds__(kEB, 2) k_engine_accel(EParams E) {
+    extern __shared__ __align__(16) unsigned char engine_smem[];
+    Smem& sm = *reinterpret_cast<Smem*>(engine_smem);
+    const Workers W{(int)blockIdx.x, (int)gridDim.x, kModeGrid};
+    if (threadIdx.x == 0) {
+        sm.bar_k = 0u;
+        sm.kphase = 0u;
+        mbar_init(&sm.kbar, 1u);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    const int n = E.n_top;
+    for (int i = W.id * kEB + (int)threadIdx.x; i < n; i += W.count * kEB) {
+        const DS x = ds_split(E.P.x[i]), y = ds_split(E.P.y[i]), z = ds_split(E.P.z[i]);
+        E.pk_a[i] = make_float4(x.hi, y.hi, z.hi, (float)E.P.m[i]);
+        E.pk_b[i] = make_float4(x.lo, y.lo, z.lo, 0.0f);
+    }
+    if (!grid_barrier(E, sm)) return;
+    const int nch = chunks_for(n, W, true, E.units_per_cta, kKB);
+    const int C = (n + nch - 1) / nch;
+    kick_units_grid(E, nullptr, 0, n, 0, nch, C, W, sm);
+    if (!grid_barrier(E, sm)) return;
+    double* out[3] = {E.ts_part, reinterpret_cast<double*>(E.rate_acc),
+                      reinterpret_cast<double*>(E.tile_counts)};
+    for (int s = W.id * kEB + (int)threadIdx.x; s < n; s += W.count * kEB)
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            double a = 0.0;
+            for (int c = 0; c < nch; c++) a += E.k_part[(size_t)(c * 3 + k) * E.n_max + s];
+            out[k][s] = a;
+        }
 }
 
 // ---------------------------------------------------------------- batched systems
@@ -2263,6 +2499,9 @@ struct EngineHost {
     unsigned* rate_acc = nullptr;
     unsigned long long* tile_status = nullptr;
     int n_max = 0;
+    float4* pk_a = nullptr;
+    float4* pk_b = nullptr;
+    int pk_levels = 0;
     int32_t* trace = nullptr;                 // caller's node-record buffer (4 int32 each)
     unsigned long long* trace_count = nullptr;
     long long trace_cap = 0;
@@ -2273,12 +2512,16 @@ inline size_t al(size_t v) { return (v + kAl - 1) & ~(kAl - 1); }
 
 }  // namespace
 
+// levels with packed kick sources (deeper levels, if they run grid phases at all, gather)
+constexpr int kPkLevels = 24;
+inline int pk_levels_for(int max_levels) { return max_levels < kPkLevels ? max_levels : kPkLevels; }
+
 size_t engine_workspace_bytes(int n_max, int max_levels) {
-    (void)max_levels;
     const size_t n = (size_t)n_max;
     return al(sizeof(EngineState)) + al(sizeof(double) * kMaxChunks * n) +
            al(sizeof(double) * kMaxChunks * 3 * n) + al(sizeof(int) * (n / kEB + 2)) +
-           al(sizeof(unsigned) * n) + al(sizeof(unsigned long long) * (n / kEB + 2));
+           al(sizeof(unsigned) * n) + al(sizeof(unsigned long long) * (n / kEB + 2)) +
+           2 * al(sizeof(float4) * n * (size_t)pk_levels_for(max_levels));
 }
 
 hhs_status engine_init(hhs_ctx* c, void* base) {
@@ -2292,6 +2535,10 @@ hhs_status engine_init(hhs_ctx* c, void* base) {
     eh->tile_counts = reinterpret_cast<int*>(p); p += al(sizeof(int) * (n / kEB + 2));
     eh->rate_acc = reinterpret_cast<unsigned*>(p); p += al(sizeof(unsigned) * n);
     eh->tile_status = reinterpret_cast<unsigned long long*>(p);
+    p += al(sizeof(unsigned long long) * (n / kEB + 2));
+    eh->pk_levels = pk_levels_for(c->max_levels);
+    eh->pk_a = reinterpret_cast<float4*>(p); p += al(sizeof(float4) * n * (size_t)eh->pk_levels);
+    eh->pk_b = reinterpret_cast<float4*>(p);
     eh->n_max = c->n_max;
     int dev = 0, sms = 0, coop = 0;
     cudaGetDevice(&dev);
@@ -2303,6 +2550,8 @@ hhs_status engine_init(hhs_ctx* c, void* base) {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEngineSmem));
     HHS_CUDA_TRY(cudaFuncSetAttribute(k_engine<HHS_PREC_MIXED>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEngineSmem));
+    HHS_CUDA_TRY(cudaFuncSetAttribute(k_engine_accel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kEngineSmem));
     HHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_engine<HHS_PREC_FP64>, kEB,
                                                                kEngineSmem));
     HHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_engine<HHS_PREC_MIXED>, kEB,
@@ -2445,12 +2694,9 @@ hhs_status engine_reset_barrier(hhs_ctx* c, cudaStream_t stream) {
     return HHS_OK;
 }
 
-hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool calc_ts,
-                            hhs_precision prec, bool profile, cudaStream_t stream,
-                            int top_level) {
-    auto* eh = static_cast<EngineHost*>(c->engine_host);
-    if (!eh) return HHS_ERR_INVALID_ARG;
-    if (top_level < 0 || top_level >= c->max_levels) return HHS_ERR_INVALID_ARG;
+namespace {
+EParams engine_params(hhs_ctx* c, EngineHost* eh, const SoA& P, int n, double dt, bool calc_ts,
+                      bool profile, int top_level) {
     EParams E;
     E.P = P;
     E.top_level = top_level;
@@ -2484,10 +2730,18 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
     E.rate_acc = eh->rate_acc;
     E.st = eh->st;
     E.err = c->err;
+    E.pk_a = eh->pk_a;
+    E.pk_b = eh->pk_b;
+    E.pk_levels = eh->pk_levels;
     E.trace = reinterpret_cast<int4*>(eh->trace);
     E.trace_count = eh->trace_count;
     E.trace_cap = eh->trace_cap;
-    const int pi = prec == HHS_PREC_FP64 ? 0 : 1;
+    return E;
+}
+
+// Cooperative launch of a persistent engine kernel in the context's launch shape.
+template <class K>
+cudaError_t engine_launch(EngineHost* eh, int pi, K kernel, const EParams& E, cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(eh->grid[pi], 1, 1);
     cfg.blockDim = dim3(kEB, 1, 1);
@@ -2507,11 +2761,42 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
     }
     // the grid barrier counts this launch's arrivals from zero; look-back words of earlier
     // launches must not look ready
-    HHS_CUDA_TRY(cudaMemsetAsync(&eh->st->bar_count, 0, sizeof(unsigned), stream));
-    HHS_CUDA_TRY(cudaMemsetAsync(eh->tile_status, 0,
-                                 sizeof(unsigned long long) * (size_t)(eh->n_max / kEB + 2), stream));
-    cudaError_t e = pi == 0 ? cudaLaunchKernelEx(&cfg, k_engine<HHS_PREC_FP64>, E)
-                            : cudaLaunchKernelEx(&cfg, k_engine<HHS_PREC_MIXED>, E);
+    cudaError_t e = cudaMemsetAsync(&eh->st->bar_count, 0, sizeof(unsigned), stream);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(eh->tile_status, 0,
+                            sizeof(unsigned long long) * (size_t)(eh->n_max / kEB + 2), stream);
+    if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, kernel, E);
+    return e;
+}
+}  // namespace
+
+hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool calc_ts,
+                            hhs_precision prec, bool profile, cudaStream_t stream,
+                            int top_level) {
+    auto* eh = static_cast<EngineHost*>(c->engine_host);
+    if (!eh) return HHS_ERR_INVALID_ARG;
+    if (top_level < 0 || top_level >= c->max_levels) return HHS_ERR_INVALID_ARG;
+    const EParams E = engine_params(c, eh, P, n, dt, calc_ts, profile, top_level);
+    const int pi = prec == HHS_PREC_FP64 ? 0 : 1;
+    const cudaError_t e = pi == 0 ? engine_launch(eh, 0, k_engine<HHS_PREC_FP64>, E, stream)
+                                  : engine_launch(eh, 1, k_engine<HHS_PREC_MIXED>, E, stream);
+    hhs_count_launch();
+    if (e != cudaSuccess) return hhs_from_cuda(e);
+    return HHS_OK;
+}
+
+// Accelerations of all n particles from one another with the engine's mixed grid kick
+// (the arithmetic of the kick phase of hhs_hold_step), into P's acceleration arrays.
+hhs_status engine_kick_accelerations(hhs_ctx* c, const SoA& P, double* ax, double* ay,
+                                     double* az, int n, cudaStream_t stream) {
+    auto* eh = static_cast<EngineHost*>(c->engine_host);
+    if (!eh || n < 1 || n > c->n_max || !ax || !ay || !az || eh->pk_levels < 1)
+        return HHS_ERR_INVALID_ARG;
+    EParams E = engine_params(c, eh, P, n, 1.0, false, false, 0);
+    E.ts_part = ax;  // outputs (the probe needs no timestep partials)
+    E.rate_acc = reinterpret_cast<unsigned*>(ay);
+    E.tile_counts = reinterpret_cast<int*>(az);
+    const cudaError_t e = engine_launch(eh, 1, k_engine_accel, E, stream);
     hhs_count_launch();
     if (e != cudaSuccess) return hhs_from_cuda(e);
     return HHS_OK;
@@ -2714,6 +2999,8 @@ extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, d
     E.rate_acc = nullptr;
     E.st = nullptr;
     E.err = b->d_err;
+    E.pk_a = E.pk_b = nullptr;
+    E.pk_levels = 0;
     E.trace = nullptr;
     E.trace_count = nullptr;
     E.trace_cap = 0;

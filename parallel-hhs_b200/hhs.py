@@ -80,6 +80,9 @@ class CParticleSystem(ctypes.Structure):
 
 # hhs_barrier_fn: int32_t (*)(void* user, void* stream)
 BARRIER_FN = ctypes.CFUNCTYPE(ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p)
+# hhs_minmax_fn: int32_t (*)(void* user, uint64_t value, uint64_t* out_min, uint64_t* out_max)
+MINMAX_FN = ctypes.CFUNCTYPE(ctypes.c_int32, ctypes.c_void_p, ctypes.c_uint64,
+                             ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64))
 
 # every symbol of include/hhs.h, with its ctypes signature (restype, argtypes)
 SIGNATURES = {
@@ -129,6 +132,11 @@ SIGNATURES = {
                                        ctypes.c_int64]),
     "hhs_dist_destroy": (ctypes.c_int, [_vp]),
     "hhs_dist_set_subtree_engine": (ctypes.c_int, [_vp, ctypes.c_int32]),
+    "hhs_dist_set_agreement": (ctypes.c_int, [_vp, MINMAX_FN, _vp]),
+    "hhs_dist_config_hash": (ctypes.c_int, [ctypes.POINTER(Tuning), ctypes.c_int32, ctypes.c_int,
+                                            ctypes.c_int32, ctypes.c_double, Params,
+                                            ctypes.POINTER(ctypes.c_uint64)]),
+    "hhs_dist_check": (ctypes.c_int, [_vp, ctypes.c_uint64]),
     "hhs_dist_shard": (ctypes.c_int, [ctypes.c_int32] * 4 + [_ip, _ip]),
     "hhs_hold_step_dist": (ctypes.c_int, [_vp, _vp, ctypes.POINTER(CParticleSystem),
                                           ctypes.c_int32, ctypes.c_double, ctypes.c_int32,
@@ -151,6 +159,7 @@ SIGNATURES = {
     "hhs_scan_exclusive_i32_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp]),
     "hhs_scan_noalloc_status": (ctypes.c_int, [_vp]),
     "hhs_ctx_set_trace": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp]),
+    "hhs_engine_kick_accelerations": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp]),
     "hhs_scan_noalloc_selftest_stalled_predecessor": (ctypes.c_int, [_vp, _vp, ctypes.c_int64,
                                                                      ctypes.c_uint32, _vp]),
     "hhs_compact_flags_i32": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int64, _vp,
@@ -666,6 +675,25 @@ class Dist:
         _check(lib().hhs_dist_set_subtree_engine(self.h, int(bool(subtree_engine))),
                "hhs_dist_set_subtree_engine")
         self.rank, self.world = rank, world
+        self._agree = None
+
+    def set_agreement(self, minmax):
+        """minmax(value) -> (min, max) of an unsigned 64-bit value over all ranks; with it
+        every step first checks that all ranks run the same configuration."""
+        def _cb(_user, value, out_min, out_max):
+            try:
+                lo, hi = minmax(int(value))
+                out_min[0], out_max[0] = lo, hi
+                return 0
+            except Exception as e:
+                self.failure = e
+                return 1
+        self._agree = MINMAX_FN(_cb)
+        _check(lib().hhs_dist_set_agreement(self.h, self._agree, None), "hhs_dist_set_agreement")
+
+    def check(self, config_hash):
+        """hhs_dist_check: the status code (0 when every rank passed the same hash)."""
+        return lib().hhs_dist_check(self.h, ctypes.c_uint64(config_hash))
 
     def step(self, ctx, sys, n, dt, calc_timestep=True, prec=PREC_MIXED, stream=None):
         """One top-level HOLD step of this rank's replica (hhs_hold_step_dist)."""
@@ -682,6 +710,35 @@ class Dist:
             self.destroy()
         except Exception:
             pass
+
+
+def config_hash(tuning, grid_ctas, prec, n, dt, eta, eps=0.0):
+    """hhs_dist_config_hash of a tuning dict (as Context.tuning() returns)."""
+    t = Tuning()
+    for k, v in tuning.items():
+        if hasattr(t, k):
+            setattr(t, k, v)
+    out = ctypes.c_uint64()
+    _check(lib().hhs_dist_config_hash(ctypes.byref(t), grid_ctas, prec, n, dt, Params(eta, eps),
+                                      ctypes.byref(out)), "hhs_dist_config_hash")
+    return out.value
+
+
+def group_minmax(group=None):
+    """A minmax callback over a torch.distributed group (two all-reduces of the value's
+    two 32-bit halves, packed so min/max order is the 64-bit order)."""
+    def minmax(value):
+        import torch
+        import torch.distributed as tdist
+        dev = "cuda" if tdist.get_backend(group) == "nccl" else "cpu"
+        out = []
+        for op in (tdist.ReduceOp.MIN, tdist.ReduceOp.MAX):
+            # int64 holds values below 2^63; shift the unsigned range into it
+            t = torch.tensor([value - (1 << 63)], dtype=torch.int64, device=dev)
+            tdist.all_reduce(t, op=op, group=group)
+            out.append(int(t.item()) + (1 << 63))
+        return out[0], out[1]
+    return minmax
 
 
 class PeerBarrier:
@@ -751,6 +808,7 @@ class DistHold:
         self.barrier = barrier if barrier is not None else PeerBarrier(group, timeout)
         self.dist = Dist(self.rank, self.world, replicas, self.barrier, min_pairs,
                          subtree_engine)
+        self.dist.set_agreement(group_minmax(group))
         self.ctx, self.sys = ctx, sys
 
     def step(self, n, dt, calc_timestep=True, prec=PREC_MIXED, stream=None):

@@ -193,3 +193,58 @@ def test_dist_callback_errors_become_a_failed_barrier(hhs):
     assert good._cb(None, None) == 0
     d.destroy()
     good.destroy()
+
+
+def _agree_worker(rank, world, port, q, differ):
+    import torch.distributed as dist
+    import hhs
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    reps = [_fake_system(hhs, 4096, 1 << (40 + r)) for r in range(world)]
+    d = hhs.Dist(rank, world, reps, lambda _s: True, 0)
+    d.set_agreement(hhs.group_minmax())
+    tuning = {"small_n": 64, "units_per_cta": 16, "ctas_per_sm": 2, "warp_n": 32,
+              "cluster_size": 4, "mid_n": 640, "packed": 0, "mid_dist_n": 96}
+    if differ and rank == 1:
+        tuning["cluster_size"] = 8  # this rank's engine would sum in another order
+    h = hhs.config_hash(tuning, 284, hhs.PREC_MIXED, 4096, 1 / 64, 0.03)
+    q.put((rank, d.check(h)))
+    d.destroy()
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("differ", [False, True])
+def test_ranks_with_different_engine_tuning_are_rejected(hhs, differ):
+    """The mixed-precision sums' order follows each rank's engine launch shape and tuning;
+    two gloo ranks compare their configuration hashes before a step, and a mismatch ends
+    the step on every rank with HHS_ERR_INVALID_ARG instead of letting replicas drift."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 33500 + os.getpid() % 1000 + (7 if differ else 0)
+    procs = [ctx.Process(target=_agree_worker, args=(r, 2, port, q, differ)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = sorted((q.get(timeout=300) for _ in range(2)), key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert [s for _, s in out] == ([1, 1] if differ else [0, 0])
+
+
+def test_config_hash_covers_every_field(hhs):
+    base = {"small_n": 64, "units_per_cta": 16, "ctas_per_sm": 2, "warp_n": 32,
+            "cluster_size": 4, "mid_n": 640, "packed": 0, "mid_dist_n": 96}
+    h0 = hhs.config_hash(base, 284, hhs.PREC_MIXED, 4096, 1 / 64, 0.03)
+    assert h0 == hhs.config_hash(dict(base), 284, hhs.PREC_MIXED, 4096, 1 / 64, 0.03)
+    seen = {h0}
+    for k in base:
+        t = dict(base)
+        t[k] += 1
+        seen.add(hhs.config_hash(t, 284, hhs.PREC_MIXED, 4096, 1 / 64, 0.03))
+    for args in ((296, hhs.PREC_MIXED, 4096, 1 / 64, 0.03), (284, hhs.PREC_FP64, 4096, 1 / 64, 0.03),
+                 (284, hhs.PREC_MIXED, 4097, 1 / 64, 0.03), (284, hhs.PREC_MIXED, 4096, 1 / 32, 0.03),
+                 (284, hhs.PREC_MIXED, 4096, 1 / 64, 0.02)):
+        seen.add(hhs.config_hash(base, *args))
+    seen.add(hhs.config_hash(base, 284, hhs.PREC_MIXED, 4096, 1 / 64, 0.03, eps=1e-3))
+    assert len(seen) == 1 + len(base) + 6

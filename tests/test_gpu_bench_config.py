@@ -10,6 +10,8 @@ pair work spread over the cluster above 96 members).
   workload): one mixed step against one FP64 step of the device schedule (which equals
   the oracle bit for bit), with the split agreement counted per level.
 """
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -125,3 +127,34 @@ def test_deep_hierarchy_mixed_step_against_fp64_schedule(cuda, hhs):
     _assert_close_hierarchy(lm, lf)
     assert dx <= 1e-6, dx
     assert abs(de) <= 1e-8, de
+
+
+class _DevArray:
+    """A device pointer seen as an FP64 array (CUDA array interface), for torch.as_tensor."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False),
+                                         "version": 3}
+
+
+@pytest.mark.parametrize("n,eps", [(4096, 0.0), (16384, 0.0), (3000, 0.01)])
+def test_engine_mixed_kick_accelerations_against_oracle(cuda, hhs, oracle, n, eps):
+    """The kick phase of the device step in mixed precision (bulk-copied source tiles,
+    FP32 pair terms with a Newton-corrected 1/d^3, blocked compensated sums) against the
+    FP64 direct sum of the oracle: every particle's acceleration within 1e-6 of |a|."""
+    torch = cuda
+    s = hhs.plummer(n, 77 + n)
+    ctx = hhs.Context(n, 64, eta=0.03, eps=eps)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    assert hhs.lib().hhs_engine_kick_accelerations(ctx.h, d.ref, n, None) == 0
+    ctx.check()
+    a = np.stack([torch.as_tensor(_DevArray(ctypes.cast(getattr(d.c, k), ctypes.c_void_p).value,
+                                            n), device="cuda").cpu().numpy()
+                  for k in ("ax", "ay", "az")])
+    ref = {k: v.copy() for k, v in s.items()}
+    acc = oracle.kick(ref, s, 1.0, eps=eps)
+    amag = np.sqrt((acc ** 2).sum(0))
+    err = np.sqrt(((a - acc) ** 2).sum(0)) / amag
+    print(f"\nengine kick n={n} eps={eps}: max rel err {err.max():.3e}, median {np.median(err):.3e}")
+    assert err.max() < 1e-6, err.max()
