@@ -53,8 +53,8 @@ def parse():
                    help="inside such a subtree, nodes above this size spread over the cluster")
     p.add_argument("--packed", type=int, default=0)
     p.add_argument("--units-per-cta", type=int, default=16)
-    p.add_argument("--autotune", action="store_true",
-                   help="pick the device-schedule tuning with the library's autotuner")
+    p.add_argument("--no-autotune", dest="autotune", action="store_false",
+                   help="keep the given tuning instead of the library's autotuner's pick")
     p.add_argument("--profile-out", default=None,
                    help="write the per-level phase profile (JSON) to this path")
     p.add_argument("--workload", default="plummer16k",
@@ -286,7 +286,8 @@ def run_ours(a, rank, world, torch, dist):
     sys_.upload(ics, stream=sh)
     tuned = None
     if a.autotune and a.schedule == "auto":
-        tuned = ctx.autotune(sys_, a.n, a.dt, prec, stream=sh)
+        tuned = {"chosen": ctx.autotune(sys_, a.n, a.dt, prec, stream=sh),
+                 "candidates": ctx.autotune_results()}
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
     def step(p=prec):
@@ -509,6 +510,10 @@ def run_batched(a, torch, rank=0, world=1, dist=None):
     d = hhs.ParticleSystem(n)
     d.upload(packed, stream=sh)
     b = hhs.Batch(off, 64, eta=a.eta)
+    tuned = None
+    if getattr(a, "autotune", True):
+        best, table = b.autotune(d, a.dt, prec, stream=sh)
+        tuned = {"chosen": best, "candidates": table}
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     with torch.cuda.stream(stream):
         for _ in range(a.warmup):
@@ -557,6 +562,7 @@ def run_batched(a, torch, rank=0, world=1, dist=None):
                                    f"(total {n_total}), eta={a.eta}, dt_top={a.dt}, one launch "
                                    f"per top step per rank",
                        "n_total": n_total, "l2": "flushed between timed steps",
+                       "autotuned": tuned is not None, "autotune": tuned,
                        "parallelism": f"clusters sharded x{world} (balanced sum N^2)"},
             "pair_interactions_per_s": pairs / (t_ms * 1e-3),
             "dE_over_E_after_steps": {"steps": steps_all, "median": float(np.median(de)),
@@ -770,6 +776,8 @@ def run_side_measurements(a, torch, res):
     out["batched_512"] = {k: b[k] for k in ("value", "unit", "ms_per_step", "steps",
                                             "pair_interactions_per_s", "dE_over_E_after_steps")}
     out["batched_512"]["n_total"] = b["config"]["n_total"]
+    out["batched_512"]["autotuned"] = b["config"]["autotuned"]
+    out["batched_512"]["tuning"] = (b["config"]["autotune"] or {}).get("chosen")
     return out
 
 
@@ -845,6 +853,7 @@ def main():
             "config": {"workload": workload_name(a), "n": a.n, "eta": a.eta, "dt_top": a.dt,
                        "precision": a.prec, "schedule": a.schedule,
                        "tuning": res["tuning"], "autotuned": res["autotune"] is not None,
+                       "autotune": res["autotune"],
                        "l2": "flushed between timed steps (256 MiB memset)",
                        "parallelism": f"replicas x{world}"},
             "pair_interactions_per_s": res["pairs_per_step"] * res["value"],

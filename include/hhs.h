@@ -146,6 +146,11 @@ hhs_status hhs_ctx_get_launch(hhs_ctx* ctx, int32_t* grid_ctas, int32_t* smem_by
  * Allocates a snapshot of the system (call it outside any timed or captured region). */
 hhs_status hhs_ctx_autotune(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n, double dt,
                             hhs_precision prec, hhs_tuning* out, void* stream);
+/* The candidates the last hhs_ctx_autotune timed, in trial order, each with its
+ * ms_per_step (the mean of three steps after one warm-up step): *count receives their
+ * number, out the first `capacity` of them. Host-only. */
+hhs_status hhs_ctx_autotune_results(hhs_ctx* ctx, hhs_tuning* out, int32_t capacity,
+                                    int32_t* count);
 
 /* timesteps<T,BS>(sys, globals, N): src/timestep.cuh:103-118 (kernel :65-99) */
 hhs_status hhs_timesteps(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n,
@@ -419,6 +424,21 @@ hhs_status hhs_batch_set_tuning(hhs_batch* b, int32_t big_n, int32_t small_n,
  * cluster for large systems (nodes above mid_dist_n spread over its CTAs), on one CTA for
  * the others (default 640 and 96; mid_n = 0 turns it off). */
 hhs_status hhs_batch_set_mid(hhs_batch* b, int32_t mid_n, int32_t mid_dist_n);
+/* Tuning of the batched launch, as hhs_batch_set_tuning / hhs_batch_set_mid set it. */
+typedef struct {
+    int32_t big_n, small_n, units_per_cta, mid_n, mid_dist_n;
+    double ms_per_step;      /* filled by hhs_batch_autotune */
+} hhs_batch_tuning;
+/* Batched autotuner: times hhs_hold_batched on the caller's systems for a grid of
+ * (big_n, units_per_cta, mid_dist_n) candidates -- the state, per-system leaf times and
+ * work counters restored before every trial and at the end -- and keeps the fastest.
+ * out (optional) receives it; table (optional, capacity entries) every candidate timed,
+ * *count (optional) their number. Allocates a snapshot of the state: call it outside
+ * any timed or captured region. */
+hhs_status hhs_batch_autotune(hhs_batch* b, hhs_particle_system* sys, double dt,
+                              hhs_precision prec, hhs_batch_tuning* out,
+                              hhs_batch_tuning* table, int32_t capacity, int32_t* count,
+                              void* stream);
 hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, double dt,
                             int32_t calc_timestep, hhs_precision prec, void* stream);
 hhs_status hhs_batch_get_simtime(hhs_batch* b, double* per_system, void* stream);

@@ -513,6 +513,8 @@ struct hhs_dist {
     int rank = 0, world = 1;
     int n_cap = 0;
     SoA peer[kMaxPeers];  // the other ranks' replicas, in rank order
+    double* peer_ax[kMaxPeers];  // their acceleration arrays: pair-rate words of the timestep
+    unsigned* rate_words = nullptr;  // this rank's (its system's ax), set per step
     hhs_barrier_fn barrier = nullptr;
     void* user = nullptr;
     long long min_pairs = 0;
@@ -556,6 +558,7 @@ hhs_status dist_launch(const hhs_dist* d, int n_fast, int n_slow, cudaStream_t s
     for (int r = 0; r < po.n_peer; r++) {
         po.vx[r] = d->peer[r].vx; po.vy[r] = d->peer[r].vy; po.vz[r] = d->peer[r].vz;
         po.ts[r] = d->peer[r].ts;
+        po.rate[r] = reinterpret_cast<unsigned*>(d->peer_ax[r]);
     }
     if (d->barrier(d->user, s) != 0) return HHS_ERR_PEER;
     const hhs_status st = launch(po);
@@ -566,6 +569,20 @@ hhs_status dist_launch(const hhs_dist* d, int n_fast, int n_slow, cudaStream_t s
 
 bool dist_shares(const hhs_dist* d, double pairs) {
     return d && pairs >= (double)d->min_pairs;
+}
+
+// Sink-block share [b_lo, b_hi) of this rank for a kick of a split level: the sink shards
+// of equal pair cost, rounded to whole blocks of `blk` sinks (the same on every rank).
+void kick_blocks(const hhs_dist* d, int nf, int ns, int blk, int* b_lo, int* b_hi) {
+    const int nsb = (nf + ns + blk - 1) / blk;
+    auto bound = [&](int r) {
+        if (r <= 0) return 0;
+        if (r >= d->world) return nsb;
+        const int b = (shard_bound(nf, ns, r, d->world) + blk / 2) / blk;
+        return b < nsb ? b : nsb;
+    };
+    *b_lo = bound(d->rank);
+    *b_hi = bound(d->rank + 1);
 }
 
 // ------------------------------------------------------------------ host-driven HOLD
@@ -590,12 +607,24 @@ hhs_status hold_host(hhs_ctx* c, const SoA& P, const int32_t* S, int n, int leve
     if (calc) {
         const double pairs = (double)n * (double)(n - 1);
         if (timed) prof->begin(rec, 0, pairs, s);
-        if (dist_shares(d, pairs))
+        if (dist_shares(d, pairs) && c->engine_host && d->rate_words) {
+            // the engine's tiled timestep over this rank's share; mixed: the symmetric
+            // pair-rate maxima go to every replica's rate words, converted after the barrier
+            if (prec != HHS_PREC_FP64)
+                HHS_CUDA_TRY(cudaMemsetAsync(d->rate_words, 0, sizeof(unsigned) * (size_t)n, s));
+            st = dist_launch(d, 0, n, s, [&](const PeerOut& po) {
+                return engine_shard_timesteps(c, P, d->rate_words, S, n, prec, d->rank, d->world,
+                                              po, s);
+            });
+            if (st == HHS_OK && prec != HHS_PREC_FP64)
+                st = engine_rates_to_ts(c, P, d->rate_words, S, n, s);
+        } else if (dist_shares(d, pairs)) {
             st = dist_launch(d, 0, n, s, [&](const PeerOut& po) {
                 return launch_timesteps(P, S, n, c->params.eta, prec, s, po);
             });
-        else
+        } else {
             st = launch_timesteps(P, S, n, c->params.eta, prec, s);
+        }
         if (st != HHS_OK) return st;
         if (timed) prof->end(rec, s);
     }
@@ -622,12 +651,28 @@ hhs_status hold_host(hhs_ctx* c, const SoA& P, const int32_t* S, int n, int leve
         const double pairs = (double)ns * (ns - 1.0) + 2.0 * (double)ns * (double)nf;
         if (timed) prof->begin(rec, 1, pairs, s);
         const double eps2 = c->params.eps * c->params.eps;
-        if (dist_shares(d, pairs))
-            st = dist_launch(d, nf, ns, s, [&](const PeerOut& po) {
-                return launch_kick_level(P, F, L, cnt, n, dt, eps2, prec, s, po);
-            });
-        else
-            st = launch_kick_level(P, F, L, cnt, n, dt, eps2, prec, s);
+        bool done = false;
+        if (dist_shares(d, pairs) && c->engine_host) {
+            // the engine's tiled kick over this rank's sink blocks
+            int b_lo = 0, b_hi = 0;
+            kick_blocks(d, nf, ns, engine_shard_kick_block(prec), &b_lo, &b_hi);
+            // mixed precision needs the level's packed-source array (every rank decides
+            // alike: the contexts have the same level capacity)
+            if (prec == HHS_PREC_FP64 || level < engine_pk_levels(c)) {
+                st = dist_launch(d, nf, ns, s, [&](const PeerOut& po) {
+                    return engine_shard_kick(c, P, F, L, nf, ns, level, dt, prec, b_lo, b_hi, po, s);
+                });
+                done = true;
+            }
+        }
+        if (!done) {
+            if (dist_shares(d, pairs))
+                st = dist_launch(d, nf, ns, s, [&](const PeerOut& po) {
+                    return launch_kick_level(P, F, L, cnt, n, dt, eps2, prec, s, po);
+                });
+            else
+                st = launch_kick_level(P, F, L, cnt, n, dt, eps2, prec, s);
+        }
         if (st != HHS_OK) return st;
         if (timed) prof->end(rec, s);
         st = launch_drift_slow(P, L, cnt, ns, dt * 0.5, s);
@@ -665,7 +710,7 @@ extern "C" hhs_status hhs_dist_create(hhs_dist** out, int32_t rank, int32_t worl
     for (int r = 0; r < world; r++) {
         if (r == rank) continue;
         const hhs_particle_system* p = &replicas[r];
-        if (!p->vx || !p->vy || !p->vz || !p->ts || p->n <= 0) return HHS_ERR_INVALID_ARG;
+        if (!p->vx || !p->vy || !p->vz || !p->ts || !p->ax || p->n <= 0) return HHS_ERR_INVALID_ARG;
         if (cap != 0 && p->n != cap) return HHS_ERR_INVALID_ARG;
         cap = p->n;
     }
@@ -676,7 +721,10 @@ extern "C" hhs_status hhs_dist_create(hhs_dist** out, int32_t rank, int32_t worl
     d->n_cap = cap;
     int k = 0;
     for (int r = 0; r < world; r++)
-        if (r != rank) d->peer[k++] = soa_of(&replicas[r]);
+        if (r != rank) {
+            d->peer_ax[k] = replicas[r].ax;
+            d->peer[k++] = soa_of(&replicas[r]);
+        }
     d->barrier = barrier;
     d->user = user;
     d->min_pairs = min_pairs;
@@ -775,7 +823,9 @@ extern "C" hhs_status hhs_hold_step_dist(hhs_ctx* c, hhs_dist* d, hhs_particle_s
         if (st == HHS_OK) st = hhs_dist_check(d, h);
         if (st != HHS_OK) return st;
     }
+    d->rate_words = reinterpret_cast<unsigned*>(sys->ax);
     hhs_status st = hold_host(c, soa_of(sys), nullptr, n, 0, dt, calc_timestep != 0, prec, s, d);
+    d->rate_words = nullptr;
     if (st != HHS_OK) return st;
     return hhs_ctx_check(c, stream);
 }
@@ -868,6 +918,8 @@ extern "C" hhs_status hhs_ctx_autotune(hhs_ctx* c, hhs_particle_system* sys, int
     const Tier tiers[] = {{64, 0, 1},   {128, 0, 1},  {64, 0, 2},   {64, 640, 1},
                           {64, 640, 2}, {64, 256, 2}, {64, 640, 4}, {64, 640, 8}};
     const int upc_cands[] = {8, 16};
+    constexpr int kTimed = 3;
+    c->tune_table.clear();
     for (int cps = 1; cps <= 2; cps++)
     for (const Tier& tr : tiers) {
         for (int upc : upc_cands) {
@@ -879,14 +931,15 @@ extern "C" hhs_status hhs_ctx_autotune(hhs_ctx* c, hhs_particle_system* sys, int
             if (st == HHS_OK) st = copy_all(false);
             if (st != HHS_OK) break;
             cudaEventRecord(e0, s);
-            for (int r = 0; r < 2 && st == HHS_OK; r++)
+            for (int r = 0; r < kTimed && st == HHS_OK; r++)
                 st = engine_hold_step(c, soa_of(sys), n, dt, true, prec, false, s);
             cudaEventRecord(e1, s);
             if (st == HHS_OK) st = hhs_ctx_check(c, stream);
             if (st != HHS_OK) break;
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);
-            t.ms_per_step = ms / 2.0;
+            t.ms_per_step = ms / kTimed;
+            c->tune_table.push_back(t);
             if (t.ms_per_step < best.ms_per_step) best = t;
         }
     }
@@ -904,6 +957,14 @@ extern "C" hhs_status hhs_ctx_autotune(hhs_ctx* c, hhs_particle_system* sys, int
     }
     engine_set_tuning(c, best);
     if (out) *out = best;
+    return HHS_OK;
+}
+
+extern "C" hhs_status hhs_ctx_autotune_results(hhs_ctx* c, hhs_tuning* out, int32_t capacity,
+                                               int32_t* count) {
+    if (!c || !count || capacity < 0 || (capacity > 0 && !out)) return HHS_ERR_INVALID_ARG;
+    *count = (int32_t)c->tune_table.size();
+    for (int32_t k = 0; k < capacity && k < *count; k++) out[k] = c->tune_table[k];
     return HHS_OK;
 }
 

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "hhs_common.cuh"
 
 // nbodysystem_globals<T> (src/particle_system.cuh:65-104) plus a preallocated
@@ -32,6 +34,8 @@ struct hhs_ctx {
     // CUDA graph of a captured multi-step integration (hhs_hold_integrate)
     cudaGraphExec_t graph_exec = nullptr;
     unsigned long long graph_key[6] = {0, 0, 0, 0, 0, 0};
+    // candidates timed by the last hhs_ctx_autotune (ms_per_step filled)
+    std::vector<hhs_tuning> tune_table;
 
     int32_t* fast(int level) const { return fast_lists + (size_t)level * n_max; }
     int32_t* slow(int level) const { return slow_lists + (size_t)level * n_max; }
@@ -51,6 +55,24 @@ hhs_status engine_set_trace(hhs_ctx* c, int32_t* nodes, int64_t capacity,
                             unsigned long long* count);
 hhs_status engine_kick_accelerations(hhs_ctx* c, const SoA& P, double* ax, double* ay,
                                      double* az, int n, cudaStream_t stream);
+// Sharded phases of the multi-GPU step (one rank's share; results into every replica).
+// Mixed timesteps leave pair-rate maxima in rate_words (local) and the peers' words;
+// engine_rates_to_ts turns them into timesteps on every rank after the barrier.
+struct PeerOut;
+hhs_status engine_shard_timesteps(hhs_ctx* c, const SoA& P, unsigned* rate_words,
+                                  const int32_t* S, int n, hhs_precision prec, int rank,
+                                  int world, const PeerOut& po, cudaStream_t s);
+hhs_status engine_rates_to_ts(hhs_ctx* c, const SoA& P, unsigned* rate_words, const int32_t* S,
+                              int n, cudaStream_t s);
+// levels with packed kick sources (the mixed sharded kick runs below this level)
+int engine_pk_levels(hhs_ctx* c);
+// sinks per block of the sharded kick (rank shares are whole blocks)
+int engine_shard_kick_block(hhs_precision prec);
+// Kick of a split level (positions already drifted), sink blocks [b_lo, b_hi); mixed
+// precision returns HHS_ERR_CAPACITY for levels without packed sources (no work done).
+hhs_status engine_shard_kick(hhs_ctx* c, const SoA& P, const int32_t* F, const int32_t* L,
+                             int nf, int ns, int level, double dt, hhs_precision prec, int b_lo,
+                             int b_hi, const PeerOut& po, cudaStream_t s);
 // top_level > 0: the launch walks the subtree of the level-top_level node, whose members
 // are the fast list of level top_level - 1 (written by the host-driven schedule); dt is
 // the top-level step and the node's own step is dt / 2^top_level.

@@ -109,6 +109,7 @@ struct __align__(16) MidState {
     int lone[kMaxLevels];                 // slot folded into the slow set, or -1
     int nmem[kMaxLevels];                 // member count of the node at each depth
     short mem[kMid];                      // member slots of the current node, increasing
+    unsigned rmax[kMid];                  // mixed: maximum pair rate of each slot (FP32 bits)
     short kl[kMid];                       // kick order: slow slots (lone last), then fast
     union {
         double pmin[8][32];               // partial timesteps (FP64)
@@ -421,8 +422,16 @@ constexpr int kCB = 32;
 // Units [u0, u1) of the upper triangle of (256-row block, kCB-column block) tiles, in
 // row-major order: a contiguous range per CTA, so consecutive units mostly share their row
 // block, whose particles stay in registers (and whose row maximum is merged once).
+// Every max also goes to the peer replicas' rate words when po is given (the sharded
+// timestep of the multi-GPU step).
+__device__ __forceinline__ void rate_max(const EParams& E, const PeerOut* po, int i, float v) {
+    atomicMax(&E.rate_acc[i], __float_as_uint(v));
+    if (po)
+        for (int r = 0; r < po->n_peer; r++) atomicMax(&po->rate[r][i], __float_as_uint(v));
+}
+
 __device__ void ts_sym_range(const EParams& E, const int32_t* S, int n, int u0, int u1,
-                             Smem& sm) {
+                             Smem& sm, const PeerOut* po = nullptr) {
     const SoA& P = E.P;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int kRowStep = kEB / kCB;
@@ -441,7 +450,7 @@ __device__ void ts_sym_range(const EParams& E, const int32_t* S, int n, int u0, 
     bool have = false;
     for (int u = u0; u < u1 && rb < nrb; u++) {
         if (rb != cur) {
-            if (act && rowmax > 0.0f) atomicMax(&E.rate_acc[i], __float_as_uint(rowmax));
+            if (act && rowmax > 0.0f) rate_max(E, po, i, rowmax);
             cur = rb;
             rowmax = 0.0f;
             i = rb * kEB + threadIdx.x;
@@ -505,14 +514,14 @@ __device__ void ts_sym_range(const EParams& E, const int32_t* S, int n, int u0, 
             float cm = 0.0f;
 #pragma unroll
             for (int w = 0; w < kEB / 32; w++) cm = fmaxf(cm, sm.colred[w][threadIdx.x]);
-            if (cm > 0.0f) atomicMax(&E.rate_acc[c0 + threadIdx.x], __float_as_uint(cm));
+            if (cm > 0.0f) rate_max(E, po, c0 + (int)threadIdx.x, cm);
         }
         if (++off >= ncb - rb * kRowStep) {
             off = 0;
             rb++;
         }
     }
-    if (act && rowmax > 0.0f) atomicMax(&E.rate_acc[i], __float_as_uint(rowmax));
+    if (act && rowmax > 0.0f) rate_max(E, po, i, rowmax);
 }
 
 
@@ -757,14 +766,20 @@ __device__ void kick_stage_tile(const EParams& E, const int32_t* F, const float4
     if (bulk && threadIdx.x == 0) sm.kphase ^= 1u;
 }
 
+// Sink blocks [ib_lo, ib_hi) of the node (all of them by default; a rank's share in the
+// sharded kick of the multi-GPU step).
 __device__ void kick_units_grid(const EParams& E, const int32_t* F, int nf, int ns, int lvl,
-                                int nch, int C, const Workers& W, Smem& sm) {
+                                int nch, int C, const Workers& W, Smem& sm, int ib_lo = 0,
+                                int ib_hi = -1) {
     const int ntot = nf + ns;
     const SoA& P = E.P;
     const float4* PA = E.pk_a + (size_t)lvl * E.n_max;
     const float4* PB = E.pk_b + (size_t)lvl * E.n_max;
-    const int nsb = (ntot + kKB - 1) / kKB;
-    const int nfb = nf / kKB;                        // blocks of fast sinks only
+    if (ib_hi < 0) ib_hi = (ntot + kKB - 1) / kKB;
+    const int nsb = ib_hi - ib_lo;
+    if (nsb <= 0) return;
+    // blocks of fast sinks only (the first nf / kKB blocks of the node) within the range
+    const int nfb = min(nsb, max(0, nf / kKB - ib_lo));
     const int ncs = min(nch, (ns + C - 1) / C);      // chunks holding slow sources
     const long long us = (long long)ncs * nsb;
     const long long units = us + (long long)(nch - ncs) * (nsb - nfb);
@@ -775,11 +790,11 @@ __device__ void kick_units_grid(const EParams& E, const int32_t* F, int nf, int 
         int jc, ib;
         if (u < us) {
             jc = (int)(u / nsb);
-            ib = (int)(u % nsb);
+            ib = ib_lo + (int)(u % nsb);
         } else {
             const long long v = u - us;
             jc = ncs + (int)(v / (nsb - nfb));
-            ib = nfb + (int)(v % (nsb - nfb));
+            ib = ib_lo + nfb + (int)(v % (nsb - nfb));
         }
         const int j0 = jc * C, j1 = min(ntot, j0 + C);
         int sk[2], jend[2];
@@ -1555,6 +1570,76 @@ __device__ __forceinline__ void put(T* p, T v, bool dist, int cs) {
     for (int r = 0; r < cs; r++) *cl.map_shared_rank(p, (unsigned)r) = v;
 }
 
+// atomic maximum of a slot's rate word in this replica only, or in every replica
+__device__ __forceinline__ void put_max(unsigned* p, unsigned v, bool dist, int cs) {
+    if (!dist) {
+        atomicMax(p, v);
+        return;
+    }
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    for (int r = 0; r < cs; r++) atomicMax(cl.map_shared_rank(p, (unsigned)r), v);
+}
+
+// Mixed timesteps of the node's members (M.mem[0..nm)), each unordered pair evaluated
+// once (the pair rate is exactly symmetric): 32 x 32 tiles of the upper triangle over
+// the warps of the CTA, or of the whole cluster when dist; row maxima in registers,
+// column maxima by one warp max-reduction per column; both merged into every replica's
+// per-slot maxima, then every CTA turns them into timesteps. The result equals the
+// maximum over all ordered pairs bit for bit.
+__device__ void mid_timesteps_sym(const EParams& E, MidState& M, int nm, bool dist, int cs,
+                                  int rank) {
+    namespace cg = cooperative_groups;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int k = tid; k < nm; k += kEB) M.rmax[M.mem[k]] = 0u;
+    if (dist) cg::this_cluster().sync();
+    else __syncthreads();
+    const int nb = (nm + 31) >> 5;
+    const int tiles = nb * (nb + 1) / 2;
+    const int gw = (dist ? rank : 0) * (kEB / 32) + warp;
+    const int nwarps = (dist ? cs : 1) * (kEB / 32);
+    for (int t = gw; t < tiles; t += nwarps) {
+        int rb = 0, rem = t;
+        while (rem >= nb - rb) {
+            rem -= nb - rb;
+            rb++;
+        }
+        const int cb = rb + rem;
+        const int p = rb * 32 + lane;
+        const bool act = p < nm;
+        const int i = act ? M.mem[p] : 0;
+        const float4 Ai = M.A[i], Bi = M.B[i], Vi = M.V[i];
+        float rowmax = 0.0f;
+        unsigned colmax = 0u;
+        const int ncol = min(32, nm - cb * 32);
+#pragma unroll 4
+        for (int c = 0; c < ncol; c++) {
+            const int q = cb * 32 + c;
+            const int j = M.mem[q];
+            const float4 A = M.A[j], B = M.B[j], V = M.V[j];
+            const float r = ts_pair_rate_mixed(ds_diff(Ai.x, Bi.x, A.x, B.x),
+                                               ds_diff(Ai.y, Bi.y, A.y, B.y),
+                                               ds_diff(Ai.z, Bi.z, A.z, B.z), Vi.x - V.x,
+                                               Vi.y - V.y, Vi.z - V.z, Ai.w + A.w,
+                                               E.inv_eta_s2, E.inv_eta);
+            const float rr = (act && q > p) ? r : 0.0f;
+            rowmax = fmaxf(rowmax, rr);
+            const unsigned cm = __reduce_max_sync(HHS_FULL_MASK, __float_as_uint(rr));
+            colmax = lane == c ? cm : colmax;
+        }
+        if (act && rowmax > 0.0f) put_max(&M.rmax[i], __float_as_uint(rowmax), dist, cs);
+        if (lane < ncol && colmax > 0u) put_max(&M.rmax[M.mem[cb * 32 + lane]], colmax, dist, cs);
+    }
+    if (dist) cg::this_cluster().sync();
+    else __syncthreads();
+    for (int k = tid; k < nm; k += kEB) {
+        const int slot = M.mem[k];
+        const double tv = 1.0 / (double)__uint_as_float(M.rmax[slot]);
+        M.ts[slot] = tv < 1.e30 ? tv : 1.e30;
+    }
+    __syncthreads();
+}
+
 // the CTA's share [s0, s1) of n sinks and the (sink group, source part) work layout
 struct Share {
     int s0, s1, ng, wpg;
@@ -1923,6 +2008,10 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
                 // ---- timesteps of the members (min over all other members)
                 const int nm = mid::compact(memw, nw, M.mem, M);
                 const bool dist = cs > 1 && nm > dist_n;
+                if (PREC != HHS_PREC_FP64) {
+                    mid::mid_timesteps_sym(E, M, nm, dist, cs, rank);
+                    if (tid == 0) tpairs += (double)nm * (double)(nm - 1);
+                } else {
                 if (dist) cl.sync();
                 const mid::Share sh = mid::share_of(nm, dist, cs, rank);
                 const int items = sh.ng * sh.wpg;
@@ -1982,6 +2071,7 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
                 if (dist) cl.sync();
                 else __syncthreads();
                 if (tid == 0) tpairs += (double)nm * (double)(nm - 1);
+                }
             }
             // ---- split: fast = members with ts <= dt, N_fast == 1 folded into the slow set
             int cnt = 0, mcnt = 0;
@@ -2395,6 +2485,146 @@ __global__ void __launch_bounds__(kEB, 2) k_engine_accel(EParams E) {
         }
 }
 
+// ---------------------------------------------------------------- sharded phases
+// The engine's tiled timestep and kick phases over one rank's share of a level, for the
+// multi-GPU step (hhs_hold_step_dist): ordinary launches whose CTAs split the rank's
+// share; every result also goes into each peer replica (atomic maxima of pair rates,
+// stored velocities and timesteps over NVLink). No kernel waits on another rank: the
+// host's barrier brackets each launch.
+__device__ __forceinline__ void kick_smem_init(Smem& sm) {
+    if (threadIdx.x == 0) {
+        sm.kphase = 0u;
+        mbar_init(&sm.kbar, 1u);
+        fence_barrier_init();
+    }
+    __syncthreads();
+}
+
+// Mixed timestep: units [u_lo, u_hi) of the level's symmetric triangle, row and column
+// maxima into the local rate words (E.rate_acc) and each peer's.
+__global__ void __launch_bounds__(kEB, 2)
+    k_shard_ts_mixed(EParams E, const int32_t* S, int n, long long u_lo, long long u_hi,
+                     PeerOut po) {
+    extern __shared__ __align__(16) unsigned char engine_smem[];
+    Smem& sm = *reinterpret_cast<Smem*>(engine_smem);
+    const long long span = u_hi - u_lo;
+    const int u0 = (int)(u_lo + span * blockIdx.x / gridDim.x);
+    const int u1 = (int)(u_lo + span * (blockIdx.x + 1) / gridDim.x);
+    ts_sym_range(E, S, n, u0, u1, sm, &po);
+    if (po.n_peer > 0) __threadfence_system();
+}
+
+// Rate words -> timesteps of the level's members (every rank, after the barrier), the
+// conversion of the engine's split phase.
+__global__ void k_rates_to_ts(EParams E, const int32_t* S, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float mr = __uint_as_float(E.rate_acc[i]);
+        const double tv = 1.0 / (double)mr;
+        E.P.ts[list_at(S, i)] = tv < 1.e30 ? tv : 1.e30;
+    }
+}
+
+// FP64 timestep: sink blocks [ib_lo, ib_hi) x nch source chunks, partial minima per chunk
+// in ts_part; then the minimum of each sink of [s_lo, s_hi) to every replica.
+__global__ void __launch_bounds__(kEB, 2)
+    k_shard_ts_fp64(EParams E, const int32_t* S, int n, int ib_lo, int ib_hi, int nch) {
+    extern __shared__ __align__(16) unsigned char engine_smem[];
+    Smem& sm = *reinterpret_cast<Smem*>(engine_smem);
+    const int C = (n + nch - 1) / nch;
+    const int units = (ib_hi - ib_lo) * nch;
+    for (int u = blockIdx.x; u < units; u += gridDim.x) {
+        const int ib = ib_lo + u / nch, jc = u % nch;
+        const int j0 = jc * C, j1 = min(n, j0 + C);
+        ts_unit<HHS_PREC_FP64>(E, S, n, ib, j0, j1, E.ts_part + (size_t)jc * E.n_max, nullptr, sm);
+    }
+}
+
+__global__ void k_shard_ts_fp64_reduce(EParams E, const int32_t* S, int s_lo, int s_hi, int nch,
+                                       PeerOut po) {
+    for (int i = s_lo + blockIdx.x * blockDim.x + threadIdx.x; i < s_hi;
+         i += gridDim.x * blockDim.x) {
+        double mv = 1.e30;
+        for (int c = 0; c < nch; c++) {
+            const double v = E.ts_part[(size_t)c * E.n_max + i];
+            if (v < mv) mv = v;
+        }
+        const int g = list_at(S, i);
+        E.P.ts[g] = mv;
+        for (int r = 0; r < po.n_peer; r++) po.ts[r][g] = mv;
+    }
+    if (po.n_peer > 0) __threadfence_system();
+}
+
+// Slow sources of a level at their current (already drifted) positions, packed for the
+// mixed kick's bulk copies (every rank).
+__global__ void k_pack_slow(EParams E, const int32_t* L, int ns, int lvl) {
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < ns; q += gridDim.x * blockDim.x) {
+        const int g = L[q];
+        const DS x = ds_split(E.P.x[g]), y = ds_split(E.P.y[g]), z = ds_split(E.P.z[g]);
+        const size_t o = (size_t)lvl * E.n_max + q;
+        E.pk_a[o] = make_float4(x.hi, y.hi, z.hi, (float)E.P.m[g]);
+        E.pk_b[o] = make_float4(x.lo, y.lo, z.lo, 0.0f);
+    }
+}
+
+// Mixed kick units of sink blocks [ib_lo, ib_hi) (kKB sinks each), partials in k_part.
+__global__ void __launch_bounds__(kEB, 2)
+    k_shard_kick_mixed(EParams E, const int32_t* F, int nf, int ns, int lvl, int nch, int C,
+                       int ib_lo, int ib_hi) {
+    extern __shared__ __align__(16) unsigned char engine_smem[];
+    Smem& sm = *reinterpret_cast<Smem*>(engine_smem);
+    kick_smem_init(sm);
+    const Workers W{(int)blockIdx.x, (int)gridDim.x, kModeGrid};
+    kick_units_grid(E, F, nf, ns, lvl, nch, C, W, sm, ib_lo, ib_hi);
+}
+
+// FP64 kick units of sink blocks [ib_lo, ib_hi) (kEB sinks each), one chunk: slow then
+// fast sources in list order, the reference's order.
+__global__ void __launch_bounds__(kEB, 2)
+    k_shard_kick_fp64(EParams E, const int32_t* F, const int32_t* L, int nf, int ns, int ib_lo,
+                      int ib_hi) {
+    extern __shared__ __align__(16) unsigned char engine_smem[];
+    Smem& sm = *reinterpret_cast<Smem*>(engine_smem);
+    for (int ib = ib_lo + (int)blockIdx.x; ib < ib_hi; ib += gridDim.x)
+        kick_unit<HHS_PREC_FP64>(E, F, L, nf, ns, 0.0, ib, 0, 0, nf + ns, sm);
+}
+
+// v += a*dt for sinks [s_lo, s_hi) from the per-chunk partials (the kick-reduce phase's
+// sums, without its drifts), stored locally and into every peer replica.
+template <int PREC>
+__global__ void k_shard_kick_reduce(EParams E, const int32_t* F, const int32_t* L, int nf,
+                                    int ns, double dt, int nch, int C, int s_lo, int s_hi,
+                                    PeerOut po) {
+    const SoA& P = E.P;
+    const int lastf = min(nch, (ns + C - 1) / C);
+    for (int s = s_lo + blockIdx.x * blockDim.x + threadIdx.x; s < s_hi;
+         s += gridDim.x * blockDim.x) {
+        const bool slow = s >= nf;
+        const int g = slow ? L[s - nf] : F[s];
+        const double v0[3] = {P.vx[g], P.vy[g], P.vz[g]};
+        double v1[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            if (PREC == HHS_PREC_FP64) {
+                double v = f64_add(v0[k], f64_mul(E.k_part[(size_t)k * E.n_max + s], dt));
+                if (slow && nf > 0)
+                    v = f64_add(v, f64_mul(E.k_part[(size_t)(3 + k) * E.n_max + s], dt));
+                v1[k] = v;
+            } else {
+                const int last = slow ? nch : lastf;
+                double a = 0.0;
+                for (int c = 0; c < last; c++) a += E.k_part[(size_t)(c * 3 + k) * E.n_max + s];
+                v1[k] = fma(a, dt, v0[k]);
+            }
+        }
+        P.vx[g] = v1[0]; P.vy[g] = v1[1]; P.vz[g] = v1[2];
+        for (int r = 0; r < po.n_peer; r++) {
+            po.vx[r][g] = v1[0]; po.vy[r][g] = v1[1]; po.vz[r][g] = v1[2];
+        }
+    }
+    if (po.n_peer > 0) __threadfence_system();
+}
+
 // ---------------------------------------------------------------- batched systems
 // Many independent systems packed back to back: the hardware clusters of the launch
 // first take the large systems from a queue ordered by decreasing size (each cluster
@@ -2552,6 +2782,14 @@ hhs_status engine_init(hhs_ctx* c, void* base) {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEngineSmem));
     HHS_CUDA_TRY(cudaFuncSetAttribute(k_engine_accel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kEngineSmem));
+    HHS_CUDA_TRY(cudaFuncSetAttribute(k_shard_ts_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kEngineSmem));
+    HHS_CUDA_TRY(cudaFuncSetAttribute(k_shard_ts_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kEngineSmem));
+    HHS_CUDA_TRY(cudaFuncSetAttribute(k_shard_kick_mixed,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEngineSmem));
+    HHS_CUDA_TRY(cudaFuncSetAttribute(k_shard_kick_fp64,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEngineSmem));
     HHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_engine<HHS_PREC_FP64>, kEB,
                                                                kEngineSmem));
     HHS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_engine<HHS_PREC_MIXED>, kEB,
@@ -2802,6 +3040,103 @@ hhs_status engine_kick_accelerations(hhs_ctx* c, const SoA& P, double* ax, doubl
     return HHS_OK;
 }
 
+// ------------------------------------------------------------------ sharded phases (host)
+namespace {
+// source chunks of the grid kick for a node of n sinks, as chunks_for computes them on
+// the device for a grid of `workers` CTAs (so every rank cuts the node the same way)
+int chunks_host(int n, int workers, int upc, int block) {
+    const int nsb = (n + block - 1) / block;
+    int c = (upc * workers + nsb - 1) / nsb;
+    c = c < 1 ? 1 : (c > kMaxChunks ? kMaxChunks : c);
+    const int maxc = (n + 63) / 64;
+    return c < maxc ? c : (maxc < 1 ? 1 : maxc);
+}
+}  // namespace
+
+hhs_status engine_shard_timesteps(hhs_ctx* c, const SoA& P, unsigned* rate_words,
+                                  const int32_t* S, int n, hhs_precision prec, int rank,
+                                  int world, const PeerOut& po, cudaStream_t s) {
+    auto* eh = static_cast<EngineHost*>(c->engine_host);
+    if (!eh || n < 1 || world < 1 || rank < 0 || rank >= world) return HHS_ERR_INVALID_ARG;
+    EParams E = engine_params(c, eh, P, n, 1.0, true, false, 0);
+    const int pi = prec == HHS_PREC_FP64 ? 0 : 1;
+    const int grid = eh->grid[pi];
+    if (pi == 1) {
+        E.rate_acc = rate_words;
+        const long long nrb = (n + kEB - 1) / kEB, ncb = (n + kCB - 1) / kCB;
+        long long units = 0;
+        for (long long r = 0; r < nrb; r++) units += ncb - r * (kEB / kCB) > 0 ? ncb - r * (kEB / kCB) : 0;
+        const long long u_lo = units * rank / world, u_hi = units * (rank + 1) / world;
+        k_shard_ts_mixed<<<grid, kEB, kEngineSmem, s>>>(E, S, n, u_lo, u_hi, po);
+        HHS_LAUNCH_CHECK();
+        return HHS_OK;
+    }
+    const int nsb = (n + kEB - 1) / kEB;
+    const int b_lo = (int)((long long)nsb * rank / world), b_hi = (int)((long long)nsb * (rank + 1) / world);
+    const int nch = chunks_host(n, grid, eh->units_per_cta, kEB);
+    if (b_hi > b_lo) {
+        k_shard_ts_fp64<<<grid, kEB, kEngineSmem, s>>>(E, S, n, b_lo, b_hi, nch);
+        HHS_LAUNCH_CHECK();
+        const int s_lo = b_lo * kEB, s_hi = b_hi * kEB < n ? b_hi * kEB : n;
+        k_shard_ts_fp64_reduce<<<(s_hi - s_lo + kEB - 1) / kEB, kEB, 0, s>>>(E, S, s_lo, s_hi, nch, po);
+        HHS_LAUNCH_CHECK();
+    }
+    return HHS_OK;
+}
+
+hhs_status engine_rates_to_ts(hhs_ctx* c, const SoA& P, unsigned* rate_words, const int32_t* S,
+                              int n, cudaStream_t s) {
+    auto* eh = static_cast<EngineHost*>(c->engine_host);
+    if (!eh || n < 1) return HHS_ERR_INVALID_ARG;
+    EParams E = engine_params(c, eh, P, n, 1.0, true, false, 0);
+    E.rate_acc = rate_words;
+    k_rates_to_ts<<<(n + kEB - 1) / kEB, kEB, 0, s>>>(E, S, n);
+    HHS_LAUNCH_CHECK();
+    return HHS_OK;
+}
+
+int engine_shard_kick_block(hhs_precision prec) { return prec == HHS_PREC_FP64 ? kEB : kKB; }
+
+int engine_pk_levels(hhs_ctx* c) {
+    auto* eh = static_cast<EngineHost*>(c->engine_host);
+    return eh ? eh->pk_levels : 0;
+}
+
+hhs_status engine_shard_kick(hhs_ctx* c, const SoA& P, const int32_t* F, const int32_t* L,
+                             int nf, int ns, int level, double dt, hhs_precision prec, int b_lo,
+                             int b_hi, const PeerOut& po, cudaStream_t s) {
+    auto* eh = static_cast<EngineHost*>(c->engine_host);
+    if (!eh || ns < 1 || nf < 0) return HHS_ERR_INVALID_ARG;
+    const int pi = prec == HHS_PREC_FP64 ? 0 : 1;
+    if (pi == 1 && level >= eh->pk_levels) return HHS_ERR_CAPACITY;  // caller falls back
+    const int ntot = nf + ns;
+    EParams E = engine_params(c, eh, P, ntot, dt, false, false, level);
+    const int grid = eh->grid[pi];
+    if (pi == 1) {
+        k_pack_slow<<<(ns + kEB - 1) / kEB, kEB, 0, s>>>(E, L, ns, level);
+        HHS_LAUNCH_CHECK();
+    }
+    if (b_hi <= b_lo) return HHS_OK;
+    const int blk = engine_shard_kick_block(prec);
+    const int nch = pi == 1 ? chunks_host(ntot, eh->grid[1], eh->units_per_cta, kKB) : 1;
+    const int C = (ntot + nch - 1) / nch;
+    if (pi == 1)
+        k_shard_kick_mixed<<<grid, kEB, kEngineSmem, s>>>(E, F, nf, ns, level, nch, C, b_lo, b_hi);
+    else
+        k_shard_kick_fp64<<<grid, kEB, kEngineSmem, s>>>(E, F, L, nf, ns, b_lo, b_hi);
+    HHS_LAUNCH_CHECK();
+    const int s_lo = b_lo * blk, s_hi = b_hi * blk < ntot ? b_hi * blk : ntot;
+    const int g2 = (s_hi - s_lo + kEB - 1) / kEB;
+    if (pi == 1)
+        k_shard_kick_reduce<HHS_PREC_MIXED><<<g2, kEB, 0, s>>>(E, F, L, nf, ns, dt, nch, C, s_lo,
+                                                               s_hi, po);
+    else
+        k_shard_kick_reduce<HHS_PREC_FP64><<<g2, kEB, 0, s>>>(E, F, L, nf, ns, dt, nch, C, s_lo,
+                                                              s_hi, po);
+    HHS_LAUNCH_CHECK();
+    return HHS_OK;
+}
+
 // ------------------------------------------------------------------ batched host side
 struct hhs_batch {
     int n_sys = 0, n_total = 0, n_max_sys = 0, max_levels = 0;
@@ -3032,6 +3367,92 @@ extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, d
                             : cudaLaunchKernelEx(&cfg, k_batched<HHS_PREC_MIXED>, B);
     hhs_count_launch();
     return hhs_from_cuda(e);
+}
+
+// Batched autotuner: times hhs_hold_batched on the caller's systems for a grid of
+// (big_n, units_per_cta, mid_dist_n) candidates, restoring the particle state, the
+// per-system leaf times and the work counters before every trial and at the end, and
+// keeps the fastest. Allocates a snapshot of the state (outside any timed region).
+extern "C" hhs_status hhs_batch_autotune(hhs_batch* b, hhs_particle_system* sys, double dt,
+                                         hhs_precision prec, hhs_batch_tuning* out,
+                                         hhs_batch_tuning* table, int32_t capacity,
+                                         int32_t* count, void* stream) {
+    if (!b || !sys || !sys->_base || !(dt > 0.0) || capacity < 0 || (capacity > 0 && !table))
+        return HHS_ERR_INVALID_ARG;
+    if (b->n_total > sys->n) return HHS_ERR_CAPACITY;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int n = b->n_total;
+    hhs_particle_system snap;
+    hhs_status st = hhs_particle_system_alloc(&snap, n);
+    if (st != HHS_OK) return st;
+    double* leaf = nullptr;
+    if (cudaMalloc(&leaf, sizeof(double) * (size_t)b->n_sys) != cudaSuccess) {
+        hhs_particle_system_free(&snap);
+        return HHS_ERR_OOM;
+    }
+    const size_t bytes = sizeof(double) * (size_t)n;
+    double* src[7] = {sys->x, sys->y, sys->z, sys->vx, sys->vy, sys->vz, sys->ts};
+    double* dst[7] = {snap.x, snap.y, snap.z, snap.vx, snap.vy, snap.vz, snap.ts};
+    auto copy_all = [&](bool save) -> hhs_status {
+        for (int k = 0; k < 7; k++)
+            HHS_CUDA_TRY(cudaMemcpyAsync(save ? dst[k] : src[k], save ? src[k] : dst[k], bytes,
+                                         cudaMemcpyDeviceToDevice, s));
+        HHS_CUDA_TRY(cudaMemcpyAsync(save ? leaf : b->d_leaf, save ? b->d_leaf : leaf,
+                                     sizeof(double) * (size_t)b->n_sys, cudaMemcpyDeviceToDevice, s));
+        return HHS_OK;
+    };
+    hhs_stats stats_saved{};
+    cudaMemcpyAsync(&stats_saved, b->d_stats, sizeof(hhs_stats), cudaMemcpyDeviceToHost, s);
+    const hhs_batch_tuning cur{b->big_n, b->small_n, b->units_per_cta, b->mid_n, b->mid_dist_n, 0.0};
+    hhs_batch_tuning best = cur;
+    best.ms_per_step = 1e300;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    st = copy_all(true);
+    const int big_c[] = {512, 1024, 2048};
+    const int upc_c[] = {8, 16};
+    const int dist_c[] = {64, 96};
+    constexpr int kTimed = 3;
+    int k = 0;
+    for (int big : big_c)
+        for (int upc : upc_c)
+            for (int dn : dist_c) {
+                if (st != HHS_OK) break;
+                hhs_batch_tuning t{big, cur.small_n, upc, cur.mid_n, dn, 0.0};
+                if ((st = hhs_batch_set_tuning(b, t.big_n, t.small_n, t.units_per_cta)) != HHS_OK) break;
+                if ((st = hhs_batch_set_mid(b, t.mid_n, t.mid_dist_n)) != HHS_OK) break;
+                st = copy_all(false);
+                if (st == HHS_OK) st = hhs_hold_batched(b, sys, dt, 1, prec, stream);
+                if (st == HHS_OK) st = copy_all(false);
+                if (st != HHS_OK) break;
+                cudaEventRecord(e0, s);
+                for (int r = 0; r < kTimed && st == HHS_OK; r++)
+                    st = hhs_hold_batched(b, sys, dt, 1, prec, stream);
+                cudaEventRecord(e1, s);
+                if (st == HHS_OK) st = hhs_batch_check(b, stream);
+                if (st != HHS_OK) break;
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                t.ms_per_step = ms / kTimed;
+                if (k < capacity) table[k] = t;
+                k++;
+                if (t.ms_per_step < best.ms_per_step) best = t;
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const hhs_status st2 = copy_all(false);
+    cudaMemcpyAsync(b->d_stats, &stats_saved, sizeof(hhs_stats), cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
+    cudaFree(leaf);
+    hhs_particle_system_free(&snap);
+    if (count) *count = k;
+    const hhs_batch_tuning pick = (st == HHS_OK && st2 == HHS_OK) ? best : cur;
+    hhs_batch_set_tuning(b, pick.big_n, pick.small_n, pick.units_per_cta);
+    hhs_batch_set_mid(b, pick.mid_n, pick.mid_dist_n);
+    if (st == HHS_OK) st = st2;
+    if (st == HHS_OK && out) *out = best;
+    return st;
 }
 
 extern "C" hhs_status hhs_batch_get_simtime(hhs_batch* b, double* out, void* stream) {

@@ -29,6 +29,7 @@ struct PeerOut {
     double* vy[kMaxPeers];
     double* vz[kMaxPeers];
     double* ts[kMaxPeers];
+    unsigned* rate[kMaxPeers];  // peers' pair-rate words (their ax arrays, reinterpreted)
 };
 inline PeerOut peer_out_local() {
     PeerOut p{};

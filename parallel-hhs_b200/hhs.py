@@ -59,6 +59,12 @@ PROFILE_KINDS = ("timesteps", "kick", "split", "update", "engine", "subtree", "c
                  "k7")
 
 
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("big_n", ctypes.c_int32), ("small_n", ctypes.c_int32),
+                ("units_per_cta", ctypes.c_int32), ("mid_n", ctypes.c_int32),
+                ("mid_dist_n", ctypes.c_int32), ("ms_per_step", ctypes.c_double)]
+
+
 class Tuning(ctypes.Structure):
     _fields_ = [("small_n", ctypes.c_int32), ("units_per_cta", ctypes.c_int32),
                 ("ctas_per_sm", ctypes.c_int32), ("warp_n", ctypes.c_int32),
@@ -159,6 +165,11 @@ SIGNATURES = {
     "hhs_scan_exclusive_i32_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp]),
     "hhs_scan_noalloc_status": (ctypes.c_int, [_vp]),
     "hhs_ctx_set_trace": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, _vp]),
+    "hhs_ctx_autotune_results": (ctypes.c_int, [_vp, _vp, ctypes.c_int32,
+                                                ctypes.POINTER(ctypes.c_int32)]),
+    "hhs_batch_autotune": (ctypes.c_int, [_vp, ctypes.POINTER(CParticleSystem), ctypes.c_double,
+                                          ctypes.c_int, ctypes.POINTER(BatchTuning), _vp,
+                                          ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), _vp]),
     "hhs_engine_kick_accelerations": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp]),
     "hhs_scan_noalloc_selftest_stalled_predecessor": (ctypes.c_int, [_vp, _vp, ctypes.c_int64,
                                                                      ctypes.c_uint32, _vp]),
@@ -381,6 +392,15 @@ class Context:
                 "cluster_size": t.cluster_size, "mid_n": t.mid_n, "packed": t.packed,
                 "mid_dist_n": t.mid_dist_n, "ms_per_step": t.ms_per_step}
 
+    def autotune_results(self):
+        """Every candidate the last autotune timed, as tuning dicts with ms_per_step."""
+        cnt = ctypes.c_int32()
+        _check(lib().hhs_ctx_autotune_results(self.h, None, 0, ctypes.byref(cnt)), "results")
+        arr = (Tuning * max(1, cnt.value))()
+        _check(lib().hhs_ctx_autotune_results(self.h, arr, cnt.value, ctypes.byref(cnt)),
+               "results")
+        return [{k: getattr(t, k) for k, _ in Tuning._fields_} for t in arr[:cnt.value]]
+
     def set_profiling(self, on):
         _check(lib().hhs_ctx_set_profiling(self.h, int(on)), "set_profiling")
 
@@ -447,6 +467,16 @@ class Batch:
     def step(self, sys, dt, calc_timestep=True, prec=PREC_MIXED, stream=None):
         _check(lib().hhs_hold_batched(self.h, sys.ref, dt, int(calc_timestep), prec, stream),
                "hhs_hold_batched")
+
+    def autotune(self, sys, dt, prec=PREC_MIXED, stream=None):
+        """hhs_batch_autotune: (best tuning dict, [every candidate timed])."""
+        best = BatchTuning()
+        table = (BatchTuning * 64)()
+        cnt = ctypes.c_int32()
+        _check(lib().hhs_batch_autotune(self.h, sys.ref, dt, prec, ctypes.byref(best), table, 64,
+                                        ctypes.byref(cnt), stream), "hhs_batch_autotune")
+        as_dict = lambda t: {k: getattr(t, k) for k, _ in BatchTuning._fields_}
+        return as_dict(best), [as_dict(t) for t in table[:cnt.value]]
 
     def check(self, stream=None):
         _check(lib().hhs_batch_check(self.h, stream), "hhs_batch_check")

@@ -546,12 +546,40 @@ def test_autotune_restores_state_and_keeps_results(cuda, hhs, oracle):
     for k in FIELDS:
         assert np.array_equal(after[k], s[k]), k
     assert ctx.simtime() == 0.0 and ctx.stats()["nodes"] == 0
+    table = ctx.autotune_results()
+    assert len(table) >= 8 and all(r["ms_per_step"] > 0 for r in table)
+    assert t["ms_per_step"] == min(r["ms_per_step"] for r in table)
     hhs.hold_step(ctx, d, n, 0.0, 1.0 / 64, True, hhs.PREC_FP64)
     ctx.check()
     oracle.hold_step(ref, 1.0 / 64, True, 0.03)
     out = d.download()
     for k in FIELDS:
         assert np.array_equal(out[k], ref[k]), k
+
+
+def test_batch_autotune_restores_state_and_keeps_results(cuda, hhs, oracle):
+    """The batched autotuner leaves the systems, leaf times and counters as it found
+    them, keeps the fastest candidate, and the next step still equals the oracle."""
+    sizes = [64, 100, 33, 500, 1500, 2100, 7, 260]
+    parts, packed, offsets = _packed(hhs, sizes, 310)
+    n = int(offsets[-1])
+    d = hhs.ParticleSystem(n)
+    d.upload(packed)
+    b = hhs.Batch(offsets, 64, eta=0.03)
+    best, table = b.autotune(d, 1.0 / 64, hhs.PREC_FP64)
+    assert len(table) == 12 and best["ms_per_step"] == min(t["ms_per_step"] for t in table)
+    after = d.download()
+    for f in FIELDS:
+        assert np.array_equal(after[f], packed[f]), f
+    assert np.all(b.simtime() == 0.0)
+    b.step(d, 1.0 / 64, True, hhs.PREC_FP64)
+    b.check()
+    out = d.download()
+    for k, p in enumerate(parts):
+        oracle.hold_step(p, 1.0 / 64, True, 0.03)
+        sl = slice(offsets[k], offsets[k + 1])
+        for f in FIELDS:
+            assert np.array_equal(out[f][sl], p[f]), (k, f)
 
 
 @pytest.mark.parametrize("n,p", [(1, 1.0), (5, 0.5), (4097, 0.01), (100003, 0.5),
