@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--mid-dist-n", type=int, default=96,
                    help="inside such a subtree, nodes above this size spread over the cluster")
     p.add_argument("--packed", type=int, default=0)
+    p.add_argument("--overlap", type=int, default=1,
+                   help="slow-only kick units beside a subtree's first pass (1) or not (0)")
     p.add_argument("--units-per-cta", type=int, default=16)
     p.add_argument("--no-autotune", dest="autotune", action="store_false",
                    help="keep the given tuning instead of the library's autotuner's pick")
@@ -281,7 +283,7 @@ def run_ours(a, rank, world, torch, dist):
     e0 = hhs.energy_host(ics)
     ctx = hhs.Context(a.n, 64, eta=a.eta)
     ctx.set_tuning(a.small_n, a.units_per_cta, a.ctas_per_sm, cluster_size=a.cluster_size,
-                   mid_n=a.mid_n, packed=a.packed, mid_dist_n=a.mid_dist_n)
+                   mid_n=a.mid_n, packed=a.packed, mid_dist_n=a.mid_dist_n, overlap=a.overlap)
     sys_ = hhs.ParticleSystem(a.n)
     sys_.upload(ics, stream=sh)
     tuned = None
@@ -748,7 +750,10 @@ def run_side_measurements(a, torch, res):
       oracle), |dE/E| of both and max |dx| between the final states;
     - the scan of 2^28 Bernoulli(0.5) int32 flags (8 B per element) and stream
       compaction, checked bit for bit against the reference's own scan on the same GPU;
-    - the batched workload (512 clusters, N log-uniform in [64, 4096]): cluster steps/s."""
+    - config 1 (N=1024 FP64 to t=1, bit for bit against the CPU oracle), config 3
+      (N=65536 Salpeter) and config 5 (N=262144 90/10 masses) step rates;
+    - the batched workload (512 clusters, N log-uniform in [64, 4096]): cluster steps/s,
+      and the per-cluster energy errors at t=0.5 in mixed precision and FP64."""
     out = {}
     v = run_validate(argparse.Namespace(**{**vars(a), "t_end": 1.0}), torch, res.get("tuning"))
     out["accuracy_t1"] = {
@@ -772,6 +777,18 @@ def run_side_measurements(a, torch, res):
                         "bit_exact_vs_reference": row.get("bit_exact_vs_reference"),
                         "reference_scan_GBps": row.get("reference_scan_GBps")}
     torch.cuda.empty_cache()
+    p1 = run_plain1k(a, torch)
+    out["plain1k"] = {k: p1[k] for k in ("value", "unit", "steps", "gpu_steps_per_s",
+                                         "cpu_oracle_steps_per_s", "cpu_threads",
+                                         "bit_exact_gpu_vs_oracle", "dE_over_E")}
+    out["plain1k"]["workload"] = "Plummer N=1024 FP64, eta=0.03, to t=1 (config 1)"
+    out["deep_65536"] = time_engine(torch, 65536, 0.02, 1, a.dt, 3, 1)
+    out["deep_65536"]["workload"] = ("Plummer N=65536 Salpeter masses, eta=0.02, mixed "
+                                     "(config 3)")
+    out["large_262144"] = time_engine(torch, 262144, 0.02, 2, a.dt, 2, 1)
+    out["large_262144"]["workload"] = ("Plummer N=262144 90/10 masses, eta=0.02, mixed "
+                                       "(config 5)")
+    out["batched_accuracy_t05"] = run_batched_accuracy(a, torch)
     b = run_batched(argparse.Namespace(**{**vars(a), "steps": 5, "warmup": 3}), torch)
     out["batched_512"] = {k: b[k] for k in ("value", "unit", "ms_per_step", "steps",
                                             "pair_interactions_per_s", "dE_over_E_after_steps")}
@@ -779,6 +796,74 @@ def run_side_measurements(a, torch, res):
     out["batched_512"]["autotuned"] = b["config"]["autotuned"]
     out["batched_512"]["tuning"] = (b["config"]["autotune"] or {}).get("chosen")
     return out
+
+
+def time_engine(torch, n, eta, mass, dt, steps, warmup, seed=2024):
+    """Mixed-precision device steps of one seeded sphere (default tuning): steps/s, pair
+    interactions/s and the hierarchy, timed with CUDA events on the launching stream."""
+    import hhs
+    s = hhs.plummer(n, seed, mass)
+    ctx = hhs.Context(n, 64, eta=eta)
+    d = hhs.ParticleSystem(n)
+    stream = torch.cuda.Stream()
+    sh = ctypes.c_void_p(stream.cuda_stream)
+    d.upload(s, stream=sh)
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            hhs.hold_step(ctx, d, n, 0.0, dt, True, hhs.PREC_MIXED, stream=sh)
+        ctx.check(sh)
+        ctx.reset_stats(sh)
+        ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for _ in range(steps):
+            hhs.hold_step(ctx, d, n, 0.0, dt, True, hhs.PREC_MIXED, stream=sh)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        ctx.check(sh)
+    sec = ev[0].elapsed_time(ev[1]) * 1e-3
+    st = ctx.stats(sh)
+    ctx.destroy()
+    d.free()
+    return {"steps_per_s": steps / sec, "s_per_step": sec / steps, "steps": steps,
+            "warmup": warmup, "pair_interactions_per_s": (st["kick_pairs"] + st["ts_pairs"]) / sec,
+            "kick_pairs_per_step": st["kick_pairs"] / steps, "nodes_per_step": st["nodes"] / steps,
+            "max_level": st["max_level"]}
+
+
+def run_batched_accuracy(a, torch, t_end=0.5):
+    """The batched workload integrated to t_end in mixed precision and in FP64 from the same
+    initial conditions: the per-cluster |dE/E| of both, and of their difference."""
+    import numpy as np
+    import hhs
+    sizes = cluster_sizes(a.seed)
+    parts = [hhs.plummer(int(sizes[k]), a.seed * 1000 + int(k)) for k in range(len(sizes))]
+    e0 = np.array([hhs.energy_host(p) for p in parts])
+    packed = {f: np.concatenate([p[f] for p in parts]) for f in hhs.FIELDS}
+    n = int(sizes.sum())
+    packed["id"] = np.arange(n, dtype=np.int32)
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    steps = int(round(t_end / a.dt))
+    de = {}
+    for name, prec in (("mixed", hhs.PREC_MIXED), ("fp64", hhs.PREC_FP64)):
+        d = hhs.ParticleSystem(n)
+        d.upload(packed)
+        b = hhs.Batch(off, 64, eta=a.eta)
+        for _ in range(steps):
+            b.step(d, a.dt, True, prec)
+        b.check()
+        out = d.download()
+        e1 = np.array([hhs.energy_host({f: np.ascontiguousarray(out[f][off[k]:off[k + 1]])
+                                        for f in ("x", "y", "z", "vx", "vy", "vz", "m")})
+                       for k in range(len(sizes))])
+        de[name] = (e1 - e0) / e0
+        d.free()
+    diff = np.abs(de["mixed"] - de["fp64"])
+    q = lambda v: {"median": float(np.median(v)), "p90": float(np.percentile(v, 90)),
+                   "max": float(np.max(v))}
+    return {"t_end": t_end, "steps": steps, "clusters": len(sizes), "n_total": n,
+            "abs_dE_over_E_mixed": q(np.abs(de["mixed"])), "abs_dE_over_E_fp64": q(np.abs(de["fp64"])),
+            "abs_dE_over_E_mixed_minus_fp64": q(diff)}
 
 
 def hbm_peak():

@@ -126,13 +126,17 @@ typedef struct {
     int32_t units_per_cta;
     int32_t ctas_per_sm;     /* CTAs of the persistent kernel per SM (1 or 2) */
     int32_t warp_n;          /* nodes with at most warp_n (<= 32) particles run on one warp */
-    int32_t cluster_size;    /* launch the persistent kernel in thread-block clusters (1,2,4,8) */
+    int32_t cluster_size;    /* launch the persistent kernel in thread-block clusters (1,2,4,8,
+                                or 16 where the device allows clusters beyond 8) */
     int32_t mid_n;           /* nodes with n <= mid_n (at most 640) run, with their whole subtree,
                                 from shared memory on the first cluster (on CTA 0 when
                                 cluster_size is 1); 0 = never */
     int32_t packed;          /* mixed kick: two sinks per thread in packed FP32x2 arithmetic */
     int32_t mid_dist_n;      /* in such a subtree, nodes with more than mid_dist_n particles spread
                                 their pair work over the cluster's CTAs */
+    int32_t overlap;         /* mixed: while such a subtree's first pass runs on the first
+                                cluster, the other CTAs compute its parent's kick terms between
+                                slow particles (1, the default) or wait (0) */
     double ms_per_step;      /* filled by hhs_ctx_autotune: time of the chosen setting */
 } hhs_tuning;
 hhs_status hhs_ctx_set_tuning(hhs_ctx* ctx, const hhs_tuning* t);
@@ -388,11 +392,14 @@ hhs_status hhs_ctx_get_level_profile(hhs_ctx* ctx, double* ms, uint64_t* counts)
 hhs_status hhs_ctx_set_trace(hhs_ctx* ctx, int32_t* d_nodes, int64_t capacity,
                              uint64_t* d_count);
 
-/* Accelerations of the first n particles from one another (softened by the context's eps)
- * computed by the mixed-precision kick phase of hhs_hold_step -- the same tiles, chunks,
- * FP32 pair arithmetic and compensated sums -- written to sys->ax, ay, az. A diagnostic
- * for checking that arithmetic against an FP64 direct sum; it uses the context's kick
- * scratch, so do not run it concurrently with a step on the same context. */
+/* Accelerations computed by the mixed-precision kick phase of hhs_hold_step -- the same
+ * packed tiles, work units, FP32 pair arithmetic, column sums and compensated sums --
+ * for the first n >= 2 particles taken as one split node whose fast set is every third
+ * particle (index % 3 == 0) and whose slow set is the rest, positions as they are:
+ * fast particles get the pull of the slow set, slow particles that of all others, as
+ * in the kick of src/hold.cuh:135-143. Written to sys->ax, ay, az. A diagnostic for
+ * checking that arithmetic against an FP64 direct sum; it uses the context's level
+ * lists and kick scratch, so do not run it concurrently with a step on the context. */
 hhs_status hhs_engine_kick_accelerations(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n,
                                          void* stream);
 

@@ -381,7 +381,7 @@ extern "C" hhs_status hhs_ctx_get_tuning(hhs_ctx* c, hhs_tuning* t) {
 
 extern "C" hhs_status hhs_engine_kick_accelerations(hhs_ctx* c, hhs_particle_system* sys,
                                                     int32_t n, void* stream) {
-    if (!c || !sys_ok(sys) || n < 1 || n > sys->n || n > c->n_max) return HHS_ERR_INVALID_ARG;
+    if (!c || !sys_ok(sys) || n < 2 || n > sys->n || n > c->n_max) return HHS_ERR_INVALID_ARG;
     return engine_kick_accelerations(c, soa_of(sys), sys->ax, sys->ay, sys->az, n,
                                      static_cast<cudaStream_t>(stream));
 }
@@ -773,6 +773,7 @@ extern "C" hhs_status hhs_dist_config_hash(const hhs_tuning* t, int32_t grid_cta
     mix((uint64_t)(uint32_t)t->mid_n);
     mix((uint64_t)(uint32_t)t->packed);
     mix((uint64_t)(uint32_t)t->mid_dist_n);
+    mix((uint64_t)(uint32_t)t->overlap);
     mix((uint64_t)(uint32_t)n);
     mix(bits(dt));
     mix(bits(params.eta));
@@ -916,7 +917,8 @@ extern "C" hhs_status hhs_ctx_autotune(hhs_ctx* c, hhs_particle_system* sys, int
     // (small_n, mid_n, cluster_size) tiers, then units per CTA and CTAs per SM
     struct Tier { int sn, mid, cs; };
     const Tier tiers[] = {{64, 0, 1},   {128, 0, 1},  {64, 0, 2},   {64, 640, 1},
-                          {64, 640, 2}, {64, 256, 2}, {64, 640, 4}, {64, 640, 8}};
+                          {64, 640, 2}, {64, 256, 2}, {64, 640, 4}, {64, 640, 8},
+                          {64, 640, 16}};
     const int upc_cands[] = {8, 16};
     constexpr int kTimed = 3;
     c->tune_table.clear();
@@ -924,7 +926,8 @@ extern "C" hhs_status hhs_ctx_autotune(hhs_ctx* c, hhs_particle_system* sys, int
     for (const Tier& tr : tiers) {
         for (int upc : upc_cands) {
             if (st != HHS_OK) break;
-            hhs_tuning t{tr.sn, upc, cps, cur.warp_n, tr.cs, tr.mid, cur.packed, cur.mid_dist_n, 0.0};
+            hhs_tuning t{tr.sn, upc, cps, cur.warp_n, tr.cs, tr.mid, cur.packed, cur.mid_dist_n,
+                         cur.overlap, 0.0};
             if (engine_set_tuning(c, t) != HHS_OK) continue;  // e.g. no cluster occupancy
             st = copy_all(false);
             if (st == HHS_OK) st = engine_hold_step(c, soa_of(sys), n, dt, true, prec, false, s);
@@ -989,7 +992,8 @@ extern "C" hhs_status hhs_hold_integrate(hhs_ctx* c, hhs_particle_system* sys, i
             (unsigned long long)prec,
         ((unsigned long long)t.small_n << 32) | (unsigned)t.mid_n,
         ((unsigned long long)t.units_per_cta << 32) |
-            (unsigned)(t.ctas_per_sm | (t.warp_n << 8) | (t.cluster_size << 16) | (t.packed << 24))};
+            (unsigned)(t.ctas_per_sm | (t.warp_n << 8) | (t.cluster_size << 16) | (t.packed << 24) |
+                       (t.overlap << 25))};
     const bool hit = c->graph_exec && std::memcmp(key, c->graph_key, sizeof(key)) == 0;
     if (!hit) {
         if (c->graph_exec) { cudaGraphExecDestroy(c->graph_exec); c->graph_exec = nullptr; }

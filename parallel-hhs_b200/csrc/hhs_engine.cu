@@ -47,6 +47,8 @@ namespace {
 constexpr int kEB = 256;          // engine block size (one sink per thread per unit)
 constexpr int kKB = 2 * kEB;      // sinks per block of the mixed grid kick (two per thread)
 constexpr int kTS = 1024;         // source records per shared-memory tile of that kick
+constexpr int kTX = 256;          // slow records per tile of the symmetric grid kick
+constexpr int kMaxFsb = 64;       // fast super-blocks of that kick (column-partial slots)
 constexpr int kMaxChunks = 32;    // source chunks per node (partial-sum slots)
 constexpr int kMaxLevels = 64;    // per-level state is kept in 64-bit masks
 constexpr unsigned long long kBarrierTimeoutNs = 60ull * 1000000000ull;
@@ -59,6 +61,7 @@ struct EngineState {
     unsigned bar_count;   // grid-barrier arrivals of this launch (cleared before each launch)
     unsigned bar_gen;
     unsigned pad[2];
+    unsigned kick_ctr[2][kMaxLevels];  // dynamic work counters of each level's kick units
     unsigned long long prof_ns[8];
     unsigned long long prof_cnt[8];
     double prof_pairs[8];
@@ -81,6 +84,7 @@ struct EParams {
     hhs_stats* stats;
     double* ts_part;   // [kMaxChunks][n_max] (float view for mixed)
     double* k_part;    // [kMaxChunks*3][n_max] (mixed) or [6][n_max] (FP64)
+    double* c_part;    // [kMaxFsb*3][n_max]: column sums of the symmetric kick (slow sinks)
     int* tile_counts;  // [n_max/kEB + 1]
     unsigned long long* tile_status;  // [n_max/kEB + 2] look-back words, cleared per launch
     unsigned* rate_acc;  // [n_max] max pair rate per list position (FP32 bits), kept at 0
@@ -92,6 +96,8 @@ struct EParams {
     float4* pk_a;   // [pk_levels][n_max]
     float4* pk_b;   // [pk_levels][n_max]
     int pk_levels;
+    int prec_mixed;  // this launch runs the mixed-precision kernels
+    int overlap;     // slow-only kick units beside a subtree's first pass (tuning)
     int4* trace;                        // node record {level, n, n_fast, calc} in call order
     unsigned long long* trace_count;    // nodes recorded (may exceed trace_cap)
     long long trace_cap;
@@ -146,6 +152,7 @@ struct __align__(16) Smem {
         struct { double x[kEB], y[kEB], z[kEB], vx[kEB], vy[kEB], vz[kEB], m[kEB]; } tsd;
         struct { float4 A[kEB], B[kEB]; } km;                   // mixed kick tiles
         struct { float4 A[kTS], B[kTS]; } kt;                   // grid kick source tile
+        struct { float4 A[kTX], B[kTX]; float colw[kEB / 32][kTX][3]; } kc;  // symmetric kick
         struct { float4 P0[kEB], P1[kEB], P2[kEB]; float2 M[kEB]; } kx;  // packed kick tiles
         struct { double x[kEB], y[kEB], z[kEB], m[kEB]; } kd;   // FP64 kick tiles
         struct {                                                  // tiny-subtree state
@@ -766,35 +773,81 @@ __device__ void kick_stage_tile(const EParams& E, const int32_t* F, const float4
     if (bulk && threadIdx.x == 0) sm.kphase ^= 1u;
 }
 
+// Work units (sink block ib, source chunk jc) of a node, as up to three rectangles
+// {chunks [jc0, jc1) x blocks [ib0, ib1)}, enumerated chunk-major.
+struct UnitGroups {
+    int n;
+    int jc0[3], jc1[3], ib0[3], ib1[3];
+    __device__ long long count(int k) const {
+        const int a = jc1[k] - jc0[k], b = ib1[k] - ib0[k];
+        return (a > 0 && b > 0) ? (long long)a * b : 0;
+    }
+    __device__ void add(int j0, int j1, int i0, int i1) {
+        jc0[n] = j0; jc1[n] = j1; ib0[n] = i0; ib1[n] = i1; n++;
+    }
+};
+
+// Which units of a node's kick: every one, only those independent of the fast set
+// (blocks of slow sinks x chunks of slow sources; they can run while the fast set is
+// still being advanced), or the others.
+enum { kUnitsAll = 0, kUnitsSlowOnly = 1, kUnitsRest = 2 };
+
+__device__ UnitGroups kick_unit_groups(int nf, int ns, int nch, int C, int part, int ib_lo,
+                                       int ib_hi) {
+    const int ntot = nf + ns;
+    const int nsb = (ntot + kKB - 1) / kKB;
+    const int nfb = nf / kKB;                        // blocks of fast sinks only
+    const int ibs = (nf + kKB - 1) / kKB;            // first block of slow sinks only
+    const int ncs = min(nch, (ns + C - 1) / C);      // chunks holding slow sources
+    const int ncss = min(nch, ns / C);               // chunks of slow sources only
+    UnitGroups g;
+    g.n = 0;
+    if (part == kUnitsAll) {
+        g.add(0, ncs, 0, nsb);
+        g.add(ncs, nch, nfb, nsb);
+    } else if (part == kUnitsSlowOnly) {
+        g.add(0, ncss, ibs, nsb);
+    } else {
+        g.add(0, ncss, 0, ibs);
+        g.add(ncss, ncs, 0, nsb);
+        g.add(ncs, nch, nfb, nsb);
+    }
+    for (int k = 0; k < g.n; k++) {
+        g.ib0[k] = max(g.ib0[k], ib_lo);
+        g.ib1[k] = min(g.ib1[k], ib_hi);
+    }
+    return g;
+}
+
 // Sink blocks [ib_lo, ib_hi) of the node (all of them by default; a rank's share in the
-// sharded kick of the multi-GPU step).
+// sharded kick of the multi-GPU step); `part` selects the units (kUnits*).
 __device__ void kick_units_grid(const EParams& E, const int32_t* F, int nf, int ns, int lvl,
                                 int nch, int C, const Workers& W, Smem& sm, int ib_lo = 0,
-                                int ib_hi = -1) {
+                                int ib_hi = -1, int part = kUnitsAll) {
     const int ntot = nf + ns;
     const SoA& P = E.P;
     const float4* PA = E.pk_a + (size_t)lvl * E.n_max;
     const float4* PB = E.pk_b + (size_t)lvl * E.n_max;
     if (ib_hi < 0) ib_hi = (ntot + kKB - 1) / kKB;
-    const int nsb = ib_hi - ib_lo;
-    if (nsb <= 0) return;
-    // blocks of fast sinks only (the first nf / kKB blocks of the node) within the range
-    const int nfb = min(nsb, max(0, nf / kKB - ib_lo));
-    const int ncs = min(nch, (ns + C - 1) / C);      // chunks holding slow sources
-    const long long us = (long long)ncs * nsb;
-    const long long units = us + (long long)(nch - ncs) * (nsb - nfb);
+    if (ib_hi <= ib_lo || W.count <= 0) return;
+    const UnitGroups grp = kick_unit_groups(nf, ns, nch, C, part, ib_lo, ib_hi);
+    long long units = 0;
+    for (int k = 0; k < grp.n; k++) units += grp.count(k);
     const long long u0 = units * W.id / W.count, u1 = units * (W.id + 1) / W.count;
     const float eps2 = E.eps2f;
     int res_a = -1, res_b = -1;  // source records resident in sm.u.kt
     for (long long u = u0; u < u1; u++) {
-        int jc, ib;
-        if (u < us) {
-            jc = (int)(u / nsb);
-            ib = ib_lo + (int)(u % nsb);
-        } else {
-            const long long v = u - us;
-            jc = ncs + (int)(v / (nsb - nfb));
-            ib = ib_lo + nfb + (int)(v % (nsb - nfb));
+        int jc = 0, ib = 0;
+        long long v = u;
+        for (int k = 0; k < grp.n; k++) {
+            const long long c = grp.count(k);
+            if (v < c) {
+                const int nb = grp.ib1[k] - grp.ib0[k];
+                jc = grp.jc0[k] + (int)(v / nb);
+                ib = grp.ib0[k] + (int)(v % nb);
+                break;
+            }
+            v -= c;
         }
         const int j0 = jc * C, j1 = min(ntot, j0 + C);
         int sk[2], jend[2];
@@ -840,6 +893,262 @@ __device__ void kick_units_grid(const EParams& E, const int32_t* F, int nf, int 
                 for (int c = 0; c < 3; c++)
                     part[(size_t)(jc * 3 + c) * E.n_max + sk[k]] =
                         (double)acc[k][c] - (double)cmp[k][c];
+    }
+}
+
+// ---------------------------------------------------------------- symmetric grid kick
+// The kick of a large grid node in mixed precision, with each (fast, slow) pair
+// evaluated once. The pair vector w = (x_j - x_i) / |x_j - x_i|^3 (fast i, slow j, slow
+// position drifted by half the step) gives the fast sink m_j w and the slow sink -m_i w
+// (Newton's third law); the reference evaluates the two kicks of the pair separately
+// (src/kick.cuh:111-155 and :59-106). Work units, taken dynamically from a counter:
+//  - cross units (fast super-block, slow chunk): rows are the super-block's fast sinks,
+//    kEB at a time, one per thread; columns are the chunk's slow particles, bulk-copied
+//    into shared memory in tiles of kTX. Rows sum their pair terms in 32-pair FP32 blocks
+//    into Kahan-compensated sums (one partial per chunk); each column's terms are summed
+//    over the warp by a transposed butterfly, over the CTA's warps in order and over the
+//    super-block's rows in order, into one FP64 partial per (super-block, slow sink);
+//  - slow units (block of kEB slow sinks, slow chunk): the slow-slow pairs, per sink.
+// The reduce phase adds, per sink, its chunk partials in order and (slow sinks) its
+// super-block partials in order: every sum has a fixed order, so a step is deterministic.
+struct KickPlan {
+    int ncs, Cs;         // slow chunks: ncs chunks of Cs slow particles
+    int nsub, FB, nfsb;  // fast sub-blocks of kEB sinks; FB of them per super-block
+    int nsb;             // blocks of kEB slow sinks
+    int nx, nsl;         // cross units (nfsb x ncs) and slow units (nsb x ncs)
+};
+
+__device__ __forceinline__ KickPlan kick_plan(int nf, int ns, int workers) {
+    KickPlan p;
+    p.nsub = (nf + kEB - 1) / kEB;
+    const int f = p.nsub < kMaxFsb ? p.nsub : kMaxFsb;
+    p.FB = f > 0 ? (p.nsub + f - 1) / f : 1;
+    p.nfsb = (p.nsub + p.FB - 1) / p.FB;
+    p.nsb = (ns + kEB - 1) / kEB;
+    const int per = p.nfsb + p.nsb;  // units per chunk
+    int c = (3 * workers + per - 1) / per;  // about three units per CTA
+    const int cmax = min(kMaxChunks, (ns + 31) / 32);  // at least 32 slow particles a chunk
+    c = c < 1 ? 1 : (c > cmax ? cmax : c);
+    p.Cs = (ns + c - 1) / c;
+    p.ncs = (ns + p.Cs - 1) / p.Cs;
+    p.nx = p.nfsb * p.ncs;
+    p.nsl = p.nsb * p.ncs;
+    return p;
+}
+
+// Column sums over the warp of eight columns (three components each): lane l ends with
+// the sums of column ((l >> 2) & 7) in r (every lane of a group of four holds them).
+__device__ __forceinline__ void warp_colsum8(const float (&v)[8][3], float (&r)[3], int lane) {
+    float a[4][3], b[2][3];
+    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const float keep = b4 ? v[c + 4][k] : v[c][k], send = b4 ? v[c][k] : v[c + 4][k];
+            a[c][k] = keep + __shfl_xor_sync(HHS_FULL_MASK, send, 16);
+        }
+#pragma unroll
+    for (int c = 0; c < 2; c++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const float keep = b3 ? a[c + 2][k] : a[c][k], send = b3 ? a[c][k] : a[c + 2][k];
+            b[c][k] = keep + __shfl_xor_sync(HHS_FULL_MASK, send, 8);
+        }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float keep = b2 ? b[1][k] : b[0][k], send = b2 ? b[0][k] : b[1][k];
+        float t = keep + __shfl_xor_sync(HHS_FULL_MASK, send, 4);
+        t += __shfl_xor_sync(HHS_FULL_MASK, t, 2);
+        t += __shfl_xor_sync(HHS_FULL_MASK, t, 1);
+        r[k] = t;
+    }
+}
+
+// Slow records [a, b) of the level's packed array into sm.u.kc (bulk copy), the rest of
+// the last group of eight zeroed (massless records far from nothing: their terms vanish).
+__device__ void kick_stage_slow(const EParams& E, const float4* PA, const float4* PB, int a,
+                                int b, Smem& sm) {
+    __syncthreads();  // every thread is done with the previous tile
+    const int len = b - a;
+    if (threadIdx.x == 0) {
+        const unsigned bytes = (unsigned)len * (unsigned)sizeof(float4);
+        mbar_arrive_expect_tx(&sm.kbar, 2u * bytes);
+        bulk_load(sm.u.kc.A, PA + a, bytes, &sm.kbar);
+        bulk_load(sm.u.kc.B, PB + a, bytes, &sm.kbar);
+    }
+    const int len8 = (len + 7) & ~7;
+    if ((int)threadIdx.x < len8 - len) {
+        sm.u.kc.A[len + threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
+        sm.u.kc.B[len + threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (!mbar_wait(&sm.kbar, sm.kphase, E.err)) (void)mbar_wait(&sm.kbar, sm.kphase, nullptr);
+    __syncthreads();
+    if (threadIdx.x == 0) sm.kphase ^= 1u;
+}
+
+// pair vector w = d * r3 (d = source - sink, r3 = 1/|d|^3 with one Newton correction)
+__device__ __forceinline__ void pair_w(const float4 A, const float4 B, const SinkDS& q, float eps2,
+                                       float& wx, float& wy, float& wz) {
+    const float dx = __fadd_rn(__fadd_rn(A.x, q.nxh), __fadd_rn(B.x, q.nxl));
+    const float dy = __fadd_rn(__fadd_rn(A.y, q.nyh), __fadd_rn(B.y, q.nyl));
+    const float dz = __fadd_rn(__fadd_rn(A.z, q.nzh), __fadd_rn(B.z, q.nzl));
+    const float d2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2))), 1e-20f);
+    const float y = rsqrtf(d2);
+    const float y2 = __fmul_rn(y, y);
+    const float c = fmaf(-1.5f, __fmul_rn(d2, y2), 2.5f);
+    const float r3 = __fmul_rn(__fmul_rn(y2, y), c);
+    wx = __fmul_rn(dx, r3);
+    wy = __fmul_rn(dy, r3);
+    wz = __fmul_rn(dz, r3);
+}
+
+__device__ void kick_cross_unit(const EParams& E, const int32_t* F, int nf, int lvl,
+                                const KickPlan& p, int fsb, int jc, int ns, Smem& sm,
+                                int& res_a, int& res_b) {
+    const SoA& P = E.P;
+    const size_t nmx = E.n_max;
+    const float4* PA = E.pk_a + (size_t)lvl * nmx;
+    const float4* PB = E.pk_b + (size_t)lvl * nmx;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int j0 = jc * p.Cs, j1 = min(ns, j0 + p.Cs);
+    double* cp = E.c_part + (size_t)fsb * 3 * nmx + nf;  // slow sink q at cp[k * nmx + q]
+    const float eps2 = E.eps2f;
+    const int sb0 = fsb * p.FB, sb1 = min(p.nsub, sb0 + p.FB);
+    for (int sb = sb0; sb < sb1; sb++) {
+        const int s = sb * kEB + (int)threadIdx.x;
+        const bool act = s < nf;
+        SinkDS q{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float nmi = 0.0f;  // -m_i: the column terms
+        if (act) {
+            const int g = F[s];
+            const DS x = ds_split(P.x[g]), y = ds_split(P.y[g]), z = ds_split(P.z[g]);
+            q = SinkDS{-x.hi, -y.hi, -z.hi, -x.lo, -y.lo, -z.lo};
+            nmi = -(float)P.m[g];
+        }
+        float acc[3] = {0.f, 0.f, 0.f}, cmp[3] = {0.f, 0.f, 0.f};
+        for (int a = j0; a < j1; a += kTX) {
+            const int b = min(j1, a + kTX), len = b - a;
+            if (a != res_a || b != res_b) {
+                kick_stage_slow(E, PA, PB, a, b, sm);
+                res_a = a;
+                res_b = b;
+            }
+            float bl[3] = {0.f, 0.f, 0.f};
+            int nb = 0;
+            for (int g8 = 0; g8 < len; g8 += 8) {
+                float v[8][3];
+#pragma unroll
+                for (int c = 0; c < 8; c++) {
+                    const float4 A = sm.u.kc.A[g8 + c], B = sm.u.kc.B[g8 + c];
+                    float wx, wy, wz;
+                    pair_w(A, B, q, eps2, wx, wy, wz);
+                    bl[0] = fmaf(wx, A.w, bl[0]);
+                    bl[1] = fmaf(wy, A.w, bl[1]);
+                    bl[2] = fmaf(wz, A.w, bl[2]);
+                    v[c][0] = __fmul_rn(wx, nmi);
+                    v[c][1] = __fmul_rn(wy, nmi);
+                    v[c][2] = __fmul_rn(wz, nmi);
+                }
+                float r[3];
+                warp_colsum8(v, r, lane);
+                const int col = ((lane >> 2) & 7);
+                if ((lane & 3) == 0 && g8 + col < len) {
+                    sm.u.kc.colw[warp][g8 + col][0] = r[0];
+                    sm.u.kc.colw[warp][g8 + col][1] = r[1];
+                    sm.u.kc.colw[warp][g8 + col][2] = r[2];
+                }
+                if (++nb == 4) {  // 32 pairs: into the compensated row sums
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        kahan_add(acc[k], cmp[k], bl[k]);
+                        bl[k] = 0.0f;
+                    }
+                    nb = 0;
+                }
+            }
+            if (nb) {
+#pragma unroll
+                for (int k = 0; k < 3; k++) kahan_add(acc[k], cmp[k], bl[k]);
+            }
+            __syncthreads();
+            // the tile's column sums: the CTA's warps in order, then the super-block's rows
+            // in order (first sub-block stores, later ones add)
+            for (int t = threadIdx.x; t < 3 * len; t += kEB) {
+                const int jl = t / 3, k = t - 3 * jl;
+                double sum = 0.0;
+#pragma unroll
+                for (int w = 0; w < kEB / 32; w++) sum += (double)sm.u.kc.colw[w][jl][k];
+                double* o = cp + (size_t)k * nmx + a + jl;
+                *o = sb == sb0 ? sum : *o + sum;
+            }
+            __syncthreads();  // colw is rewritten by the next pass
+        }
+        if (act)
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                E.k_part[(size_t)(jc * 3 + k) * nmx + s] = (double)acc[k] - (double)cmp[k];
+    }
+}
+
+__device__ void kick_slow_unit(const EParams& E, int nf, int lvl, const KickPlan& p, int sb,
+                               int jc, int ns, Smem& sm, int& res_a, int& res_b) {
+    const size_t nmx = E.n_max;
+    const float4* PA = E.pk_a + (size_t)lvl * nmx;
+    const float4* PB = E.pk_b + (size_t)lvl * nmx;
+    const int j0 = jc * p.Cs, j1 = min(ns, j0 + p.Cs);
+    const int qs = sb * kEB + (int)threadIdx.x;  // slow sink position
+    const bool act = qs < ns;
+    SinkDS q{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (act) {
+        const float4 a = PA[qs], b = PB[qs];
+        q = SinkDS{-a.x, -a.y, -a.z, -b.x, -b.y, -b.z};
+    }
+    const float eps2 = E.eps2f;
+    float acc[3] = {0.f, 0.f, 0.f}, cmp[3] = {0.f, 0.f, 0.f};
+    for (int a = j0; a < j1; a += kTX) {
+        const int b = min(j1, a + kTX), len = b - a;
+        if (a != res_a || b != res_b) {
+            kick_stage_slow(E, PA, PB, a, b, sm);
+            res_a = a;
+            res_b = b;
+        }
+        for (int jb = 0; jb < len; jb += 32) {
+            const int je = min(len, jb + 32);
+            float bl[3] = {0.f, 0.f, 0.f};
+#pragma unroll 4
+            for (int j = jb; j < je; j++)
+                kick_pair_nr(sm.u.kc.A[j], sm.u.kc.B[j], q, eps2, bl[0], bl[1], bl[2]);
+#pragma unroll
+            for (int k = 0; k < 3; k++) kahan_add(acc[k], cmp[k], bl[k]);
+        }
+    }
+    if (act)
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            E.k_part[(size_t)(jc * 3 + k) * nmx + nf + qs] = (double)acc[k] - (double)cmp[k];
+}
+
+// Units of one kind set, taken from the level's counter `set` until none is left:
+// kinds 0 = cross units then slow units, 1 = slow units only, 2 = cross units only.
+__device__ void kick_sym_units(const EParams& E, const int32_t* F, int nf, int ns, int lvl,
+                               const KickPlan& p, int set, int kinds, Smem& sm) {
+    const int nx = kinds == 1 ? 0 : p.nx;
+    const int total = nx + (kinds == 2 ? 0 : p.nsl);
+    int res_a = -1, res_b = -1;
+    unsigned* ctr = &E.st->kick_ctr[set][lvl];
+    while (true) {
+        __syncthreads();  // every thread has read the previous unit index
+        if (threadIdx.x == 0) sm.bcast = (int)atomicAdd(ctr, 1u);
+        __syncthreads();
+        const int u = sm.bcast;
+        if (u >= total) break;
+        if (u < nx) {
+            kick_cross_unit(E, F, nf, lvl, p, u % p.nfsb, u / p.nfsb, ns, sm, res_a, res_b);
+        } else {
+            const int v = u - nx;
+            kick_slow_unit(E, nf, lvl, p, v % p.nsb, v / p.nsb, ns, sm, res_a, res_b);
+        }
     }
 }
 
@@ -1118,6 +1427,10 @@ __device__ void split_phase(const EParams& E, const int32_t* S, int n, double dt
             const int nf = nf_raw == 1 ? 0 : nf_raw;
             E.counts[level].n_fast = nf;
             E.counts[level].n_slow = n - nf;
+            if (E.st && level < kMaxLevels) {  // the level's kick takes its units afresh
+                E.st->kick_ctr[0][level] = 0u;
+                E.st->kick_ctr[1][level] = 0u;
+            }
             trace_node(E, level, n, nf, calc);
             if (nf == 0) *E.leaf_time += dt;
             const double ns = (double)(n - nf), nfd = (double)nf;
@@ -1134,10 +1447,12 @@ __device__ void split_phase(const EParams& E, const int32_t* S, int n, double dt
 // drifts. Mixed: one thread per (sink, component) adds its chunks with eight independent
 // loads in flight, so the reduction of a node spreads over the whole grid; FP64: one
 // thread per sink (slow then fast sources, the reference's order).
+// nfsb >= 0: the symmetric kick's partials (nch = its chunk count: fast sinks add their
+// nch chunk partials, slow sinks those and then their nfsb super-block partials).
 template <int PREC>
 __device__ void kick_reduce_phase(const EParams& E, const int32_t* F, const int32_t* L, int nf,
                                   int ns, double dt, int nch, int C, const Workers& W,
-                                  Smem& sm) {
+                                  Smem& sm, int nfsb = -1) {
     const int n = nf + ns;
     const double h = dt * 0.5;
     const SoA& P = E.P;
@@ -1168,7 +1483,7 @@ __device__ void kick_reduce_phase(const EParams& E, const int32_t* F, const int3
     }
     constexpr int kPer = kEB / 3;  // sinks per CTA iteration (3 components each)
     const int ntiles = (n + kPer - 1) / kPer;
-    const int lastf = min(nch, (ns + C - 1) / C);  // chunks with sources for fast sinks
+    const int lastf = nfsb >= 0 ? nch : min(nch, (ns + C - 1) / C);  // chunks for fast sinks
     double* red = reinterpret_cast<double*>(&sm.u);
     for (int t = W.id; t < ntiles; t += W.count) {
         const int q = (int)threadIdx.x / 3, k = (int)threadIdx.x % 3;
@@ -1187,6 +1502,10 @@ __device__ void kick_reduce_phase(const EParams& E, const int32_t* F, const int3
                 for (int u = 0; u < 8; u++) a += v[u];
             }
             for (; c < last; c++) a += part[(size_t)c * stride];
+            if (nfsb > 0 && s >= nf) {
+                const double* cpart = E.c_part + (size_t)k * E.n_max + s;
+                for (int f = 0; f < nfsb; f++) a += cpart[(size_t)f * stride];
+            }
         }
         __syncthreads();
         red[threadIdx.x] = a;
@@ -2268,6 +2587,16 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
     else __syncthreads();
 }
 
+// True when the kick of level lvl (a grid node with a fast set of at most mid_n) runs its
+// slow-only units beside the fast set's first pass on the first cluster: mixed precision,
+// packed sources at that level, and CTAs outside the first cluster.
+__device__ __forceinline__ bool kick_overlaps(const EParams& E, int lvl, const Workers& W) {
+    namespace cg = cooperative_groups;
+    return W.mode == kModeGrid && E.overlap && E.pk_a && lvl < E.pk_levels && !E.packed &&
+           E.prec_mixed && (int)cg::this_cluster().num_blocks() < W.count &&
+           ld_volatile_i32(&E.counts[lvl].n_slow) > 0;
+}
+
 // ---------------------------------------------------------------- the recursion
 // Walks the HOLD recursion from `top` (whose subsystem is already defined by the
 // counts/lists above it). Grid and cluster modes delegate nodes with n <= small_n,
@@ -2297,9 +2626,18 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                 if constexpr (MODE == kModeGrid) {
                     namespace cg = cooperative_groups;
                     const int cs = (int)cg::this_cluster().num_blocks();
-                    if ((int)blockIdx.x < cs)
+                    if ((int)blockIdx.x < cs) {
                         mid_hold<PREC>(E, S, n, lvl, calc, E.mid_dist_n, cs,
                                        (int)cg::this_cluster().block_rank(), sm);
+                    } else if (!calc && lvl > top && kick_overlaps(E, lvl - 1, W)) {
+                        // meanwhile the other CTAs run the parent's kick units that do not
+                        // involve the fast set (this node), which mid_hold is advancing
+                        const int pl = lvl - 1;
+                        const int pnf = n, pns = ld_volatile_i32(&E.counts[pl].n_slow);
+                        const KickPlan kp = kick_plan(pnf, pns, W.count);
+                        kick_sym_units(E, E.fast_lists + (size_t)pl * E.n_max, pnf, pns, pl, kp, 1,
+                                       1, sm);
+                    }
                 } else {
                     mid_hold<PREC>(E, S, n, lvl, calc, E.mid_dist_n, W.count, W.id, sm);
                 }
@@ -2393,7 +2731,15 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                 const int jcs = min(nch, (ns + C - 1) / C);
                 const int uf = nfb * jcs;
                 const int units = grid_tma ? 0 : uf + (nsb - nfb) * nch;
-                if (grid_tma) kick_units_grid(E, F, nf, ns, lvl, nch, C, W, sm);
+                KickPlan kp{};
+                if (grid_tma) {
+                    // the slow units already ran beside the fast set's first pass when that
+                    // pass was a subtree on the first cluster
+                    const bool overlapped = nf > 0 && nf <= E.mid_n && nf <= kMid &&
+                                            kick_overlaps(E, lvl, W);
+                    kp = kick_plan(nf, ns, W.count);
+                    kick_sym_units(E, F, nf, ns, lvl, kp, 0, overlapped ? 2 : 0, sm);
+                }
                 for (int u = W.id; u < units; u += W.count) {
                     int ib, jc;
                     if (u < uf) {
@@ -2410,7 +2756,8 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                 if (!phase_barrier(E, sm, W)) return false;
                 const double ns_d = ns, nf_d = nf;
                 prof_mark(E, W, t_last, kProfKick, ns_d * (ns_d - 1.0) + 2.0 * ns_d * nf_d, sm, lvl);
-                kick_reduce_phase<PREC>(E, F, L, nf, ns, dt, nch, C, W, sm);
+                if (grid_tma) kick_reduce_phase<PREC>(E, F, L, nf, ns, dt, kp.ncs, 0, W, sm, kp.nfsb);
+                else kick_reduce_phase<PREC>(E, F, L, nf, ns, dt, nch, C, W, sm);
                 if (!phase_barrier(E, sm, W)) return false;
                 prof_mark(E, W, t_last, kProfUpdate, 0.0, sm, lvl);
             }
@@ -2448,10 +2795,12 @@ __global__ void __launch_bounds__(kEB, 2) k_engine(EParams E) {
     prof_end(E, sm);
 }
 
-// Probe of the mixed grid kick: the whole system as one node of slow particles (no
-// drift), packed, kicked by kick_units_grid and reduced per sink in the kick-reduce
-// phase's order; accelerations go to E.ts_part / rate_acc / tile_counts reinterpreted
-// as FP64 ax / ay / az (see engine_kick_accelerations).
+// Probe of the mixed grid kick: the system as one split node whose fast set is every
+// third particle (index % 3 == 0) and whose slow set is the rest, with no drift. The
+// level's slow records are packed, the symmetric kick runs its units, and the reduce
+// phase's sums give each particle's acceleration (fast: from the slow set; slow: from
+// all others), written to E.ts_part / rate_acc / tile_counts reinterpreted as FP64
+// ax / ay / az (see engine_kick_accelerations).
 __global__ void __launch_bounds__(kEB, 2) k_engine_accel(EParams E) {
     extern __shared__ __align__(16) unsigned char engine_smem[];
     Smem& sm = *reinterpret_cast<Smem*>(engine_smem);
@@ -2464,15 +2813,24 @@ __global__ void __launch_bounds__(kEB, 2) k_engine_accel(EParams E) {
     }
     __syncthreads();
     const int n = E.n_top;
+    const int nf = (n + 2) / 3, ns = n - nf;
+    int32_t* F = E.fast_lists;
+    int32_t* L = E.slow_lists;
     for (int i = W.id * kEB + (int)threadIdx.x; i < n; i += W.count * kEB) {
-        const DS x = ds_split(E.P.x[i]), y = ds_split(E.P.y[i]), z = ds_split(E.P.z[i]);
-        E.pk_a[i] = make_float4(x.hi, y.hi, z.hi, (float)E.P.m[i]);
-        E.pk_b[i] = make_float4(x.lo, y.lo, z.lo, 0.0f);
+        if (i % 3 == 0) {
+            F[i / 3] = i;
+        } else {
+            const int q = (i / 3) * 2 + (i % 3) - 1;
+            L[q] = i;
+            const DS x = ds_split(E.P.x[i]), y = ds_split(E.P.y[i]), z = ds_split(E.P.z[i]);
+            E.pk_a[q] = make_float4(x.hi, y.hi, z.hi, (float)E.P.m[i]);
+            E.pk_b[q] = make_float4(x.lo, y.lo, z.lo, 0.0f);
+        }
     }
+    if (W.id == 0 && threadIdx.x == 0) E.st->kick_ctr[0][0] = 0u;
     if (!grid_barrier(E, sm)) return;
-    const int nch = chunks_for(n, W, true, E.units_per_cta, kKB);
-    const int C = (n + nch - 1) / nch;
-    kick_units_grid(E, nullptr, 0, n, 0, nch, C, W, sm);
+    const KickPlan kp = kick_plan(nf, ns, W.count);
+    kick_sym_units(E, F, nf, ns, 0, kp, 0, 0, sm);
     if (!grid_barrier(E, sm)) return;
     double* out[3] = {E.ts_part, reinterpret_cast<double*>(E.rate_acc),
                       reinterpret_cast<double*>(E.tile_counts)};
@@ -2480,8 +2838,11 @@ __global__ void __launch_bounds__(kEB, 2) k_engine_accel(EParams E) {
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             double a = 0.0;
-            for (int c = 0; c < nch; c++) a += E.k_part[(size_t)(c * 3 + k) * E.n_max + s];
-            out[k][s] = a;
+            for (int c = 0; c < kp.ncs; c++) a += E.k_part[(size_t)(c * 3 + k) * E.n_max + s];
+            if (s >= nf)
+                for (int f = 0; f < kp.nfsb; f++)
+                    a += E.c_part[(size_t)(f * 3 + k) * E.n_max + s];
+            out[k][s >= nf ? L[s - nf] : F[s]] = a;
         }
 }
 
@@ -2722,6 +3083,7 @@ struct EngineHost {
     int mid_n = 640;
     int mid_dist_n = 96;
     int packed = 0;
+    int overlap = 1;
     EngineState* st = nullptr;
     double* ts_part = nullptr;
     double* k_part = nullptr;
@@ -2732,6 +3094,7 @@ struct EngineHost {
     float4* pk_a = nullptr;
     float4* pk_b = nullptr;
     int pk_levels = 0;
+    double* c_part = nullptr;
     int32_t* trace = nullptr;                 // caller's node-record buffer (4 int32 each)
     unsigned long long* trace_count = nullptr;
     long long trace_cap = 0;
@@ -2751,7 +3114,8 @@ size_t engine_workspace_bytes(int n_max, int max_levels) {
     return al(sizeof(EngineState)) + al(sizeof(double) * kMaxChunks * n) +
            al(sizeof(double) * kMaxChunks * 3 * n) + al(sizeof(int) * (n / kEB + 2)) +
            al(sizeof(unsigned) * n) + al(sizeof(unsigned long long) * (n / kEB + 2)) +
-           2 * al(sizeof(float4) * n * (size_t)pk_levels_for(max_levels));
+           2 * al(sizeof(float4) * n * (size_t)pk_levels_for(max_levels)) +
+           al(sizeof(double) * kMaxFsb * 3 * n);
 }
 
 hhs_status engine_init(hhs_ctx* c, void* base) {
@@ -2768,7 +3132,8 @@ hhs_status engine_init(hhs_ctx* c, void* base) {
     p += al(sizeof(unsigned long long) * (n / kEB + 2));
     eh->pk_levels = pk_levels_for(c->max_levels);
     eh->pk_a = reinterpret_cast<float4*>(p); p += al(sizeof(float4) * n * (size_t)eh->pk_levels);
-    eh->pk_b = reinterpret_cast<float4*>(p);
+    eh->pk_b = reinterpret_cast<float4*>(p); p += al(sizeof(float4) * n * (size_t)eh->pk_levels);
+    eh->c_part = reinterpret_cast<double*>(p);
     eh->n_max = c->n_max;
     int dev = 0, sms = 0, coop = 0;
     cudaGetDevice(&dev);
@@ -2782,6 +3147,14 @@ hhs_status engine_init(hhs_ctx* c, void* base) {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEngineSmem));
     HHS_CUDA_TRY(cudaFuncSetAttribute(k_engine_accel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kEngineSmem));
+    // clusters of 16 CTAs (beyond the portable 8) for the subtree solver, where allowed
+    if (cudaFuncSetAttribute(k_engine<HHS_PREC_FP64>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_engine<HHS_PREC_MIXED>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_engine_accel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess)
+        (void)cudaGetLastError();  // cluster size 16 then fails its occupancy check
     HHS_CUDA_TRY(cudaFuncSetAttribute(k_shard_ts_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kEngineSmem));
     HHS_CUDA_TRY(cudaFuncSetAttribute(k_shard_ts_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2822,13 +3195,14 @@ hhs_status engine_set_tuning(hhs_ctx* c, const hhs_tuning& t) {
     if (!eh || t.small_n < 0 || t.units_per_cta < 1 || t.units_per_cta > 64 ||
         t.ctas_per_sm < 1 || t.ctas_per_sm > 2 || t.warp_n < 0 || t.warp_n > 32 ||
         !(t.cluster_size == 1 || t.cluster_size == 2 || t.cluster_size == 4 ||
-          t.cluster_size == 8) || t.mid_n < 0 || t.mid_dist_n < 0)
+          t.cluster_size == 8 || t.cluster_size == 16) || t.mid_n < 0 || t.mid_dist_n < 0)
         return HHS_ERR_INVALID_ARG;
     eh->warp_n = t.warp_n;
     eh->cluster_size = t.cluster_size;
     eh->mid_n = t.mid_n;
     eh->mid_dist_n = t.mid_dist_n;
     eh->packed = t.packed != 0;
+    eh->overlap = t.overlap != 0;
     eh->small_n = t.small_n;
     eh->units_per_cta = t.units_per_cta;
     eh->ctas_per_sm = t.ctas_per_sm;
@@ -2878,6 +3252,7 @@ hhs_status engine_get_tuning(hhs_ctx* c, hhs_tuning* t) {
     t->mid_n = eh->mid_n;
     t->mid_dist_n = eh->mid_dist_n;
     t->packed = eh->packed;
+    t->overlap = eh->overlap;
     return HHS_OK;
 }
 
@@ -2963,6 +3338,7 @@ EParams engine_params(hhs_ctx* c, EngineHost* eh, const SoA& P, int n, double dt
     E.stats = c->stats;
     E.ts_part = eh->ts_part;
     E.k_part = eh->k_part;
+    E.c_part = eh->c_part;
     E.tile_counts = eh->tile_counts;
     E.tile_status = eh->tile_status;
     E.rate_acc = eh->rate_acc;
@@ -2971,6 +3347,8 @@ EParams engine_params(hhs_ctx* c, EngineHost* eh, const SoA& P, int n, double dt
     E.pk_a = eh->pk_a;
     E.pk_b = eh->pk_b;
     E.pk_levels = eh->pk_levels;
+    E.prec_mixed = 0;
+    E.overlap = eh->overlap;
     E.trace = reinterpret_cast<int4*>(eh->trace);
     E.trace_count = eh->trace_count;
     E.trace_cap = eh->trace_cap;
@@ -3014,8 +3392,9 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
     auto* eh = static_cast<EngineHost*>(c->engine_host);
     if (!eh) return HHS_ERR_INVALID_ARG;
     if (top_level < 0 || top_level >= c->max_levels) return HHS_ERR_INVALID_ARG;
-    const EParams E = engine_params(c, eh, P, n, dt, calc_ts, profile, top_level);
+    EParams E = engine_params(c, eh, P, n, dt, calc_ts, profile, top_level);
     const int pi = prec == HHS_PREC_FP64 ? 0 : 1;
+    E.prec_mixed = pi;
     const cudaError_t e = pi == 0 ? engine_launch(eh, 0, k_engine<HHS_PREC_FP64>, E, stream)
                                   : engine_launch(eh, 1, k_engine<HHS_PREC_MIXED>, E, stream);
     hhs_count_launch();
@@ -3028,7 +3407,7 @@ hhs_status engine_hold_step(hhs_ctx* c, const SoA& P, int n, double dt, bool cal
 hhs_status engine_kick_accelerations(hhs_ctx* c, const SoA& P, double* ax, double* ay,
                                      double* az, int n, cudaStream_t stream) {
     auto* eh = static_cast<EngineHost*>(c->engine_host);
-    if (!eh || n < 1 || n > c->n_max || !ax || !ay || !az || eh->pk_levels < 1)
+    if (!eh || n < 2 || n > c->n_max || !ax || !ay || !az || eh->pk_levels < 1)
         return HHS_ERR_INVALID_ARG;
     EParams E = engine_params(c, eh, P, n, 1.0, false, false, 0);
     E.ts_part = ax;  // outputs (the probe needs no timestep partials)
@@ -3328,7 +3707,7 @@ extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, d
     E.counts = nullptr;
     E.leaf_time = nullptr;
     E.stats = b->d_stats;
-    E.ts_part = E.k_part = nullptr;
+    E.ts_part = E.k_part = E.c_part = nullptr;
     E.tile_counts = nullptr;
     E.tile_status = nullptr;
     E.rate_acc = nullptr;
@@ -3336,6 +3715,8 @@ extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, d
     E.err = b->d_err;
     E.pk_a = E.pk_b = nullptr;
     E.pk_levels = 0;
+    E.prec_mixed = pi;
+    E.overlap = 0;
     E.trace = nullptr;
     E.trace_count = nullptr;
     E.trace_cap = 0;

@@ -5,7 +5,6 @@
 
 #include "hhs_scan.cuh"
 #include "hhs_kernels.h"
-#include "hhs_tma.cuh"
 
 namespace {
 
@@ -396,176 +395,6 @@ hhs_status launch_large(const int32_t* in, int32_t* out, long long n, ScanHeader
     return HHS_OK;
 }
 
-// ---- pipelined single pass
-// Persistent CTAs each keep STAGES tiles in flight: the tile's values arrive in shared
-// memory by one bulk copy (cp.async.bulk, completing on an mbarrier), so while a CTA
-// waits in the look-back of its current tile the next tiles' loads are already under
-// way, and the input is read from DRAM exactly once (8 bytes of traffic per value for
-// the scan). Tiles are taken in increasing order by every CTA (one atomic counter), and
-// each tile publishes its aggregate before it waits for its predecessors, so every
-// look-back ends: the lowest unfinished tile is always either current in its CTA (all
-// of its predecessors have published) or queued behind a tile of its own CTA that is.
-// The last, partial tile is read with plain loads; n % 4 != 0 or unaligned pointers use
-// the plain kernels. FLAGS: the values are (flag != 0) and idx_out receives the index
-// of every nonzero flag at its scan position (stream compaction); out may then be null.
-constexpr int kPipeBlock = 256;
-
-template <int STAGES, int ITEMS>
-constexpr size_t pipe_smem_bytes() {
-    return (size_t)STAGES * kPipeBlock * ITEMS * sizeof(int32_t);
-}
-
-template <int STAGES, int ITEMS, int LB, int MINB, bool FLAGS>
-__global__ void __launch_bounds__(kPipeBlock, MINB)
-    k_scan_pipe(const int32_t* __restrict__ in, int32_t* __restrict__ out, long long n,
-                ScanHeader* hdr, unsigned long long* status, int num_tiles, int num_full,
-                int32_t* __restrict__ idx_out, int32_t* __restrict__ count) {
-    using T = TileScan<kPipeBlock, ITEMS, LB>;
-    constexpr int TILE = T::TILE;
-    constexpr unsigned TILE_BYTES = TILE * sizeof(int32_t);
-    extern __shared__ __align__(128) unsigned char pipe_smem[];
-    int4* buf = reinterpret_cast<int4*>(pipe_smem);
-    __shared__ __align__(8) uint64_t bar[STAGES];
-    __shared__ int s_tile[STAGES];
-    __shared__ unsigned s_epoch, s_prefix, s_limit, s_warp[T::WARPS];
-    __shared__ int s_ok;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) {
-        s_epoch = scan_next_epoch(hdr);
-        const unsigned lim = *reinterpret_cast<volatile const unsigned*>(&hdr->spin_limit);
-        s_limit = lim ? lim : HHS_SPIN_LIMIT;
-        s_ok = 1;
-        for (int k = 0; k < STAGES; k++) mbar_init(&bar[k], 1u);
-        fence_barrier_init();
-        for (int k = 0; k < STAGES; k++) {
-            const int t = (int)atomicAdd(&hdr->tile_counter, 1u);
-            s_tile[k] = t;
-            if (t < num_full) {
-                mbar_arrive_expect_tx(&bar[k], TILE_BYTES);
-                bulk_load(buf + (size_t)k * (TILE / 4), in + (long long)t * TILE, TILE_BYTES,
-                          &bar[k]);
-            }
-        }
-    }
-    __syncthreads();
-    const unsigned epoch = s_epoch;
-    unsigned phase = 0u;  // parity bit of each stage's barrier
-    for (int k = 0;; k++) {
-        const int st = k % STAGES;
-        const int tile = s_tile[st];
-        if (tile >= num_tiles || !s_ok) break;
-        const long long tbase = (long long)tile * TILE;
-        unsigned v[ITEMS], cb[T::CHUNKS];
-        if (tile < num_full) {
-            if (!mbar_wait(&bar[st], (phase >> st) & 1u, &hdr->error)) s_ok = 0;
-            phase ^= 1u << st;
-            const int4* b = buf + (size_t)st * (TILE / 4);
-#pragma unroll
-            for (int c = 0; c < T::CHUNKS; c++) {
-                const int4 q = b[T::offset(warp, c, lane) / 4];
-                v[4 * c] = q.x; v[4 * c + 1] = q.y; v[4 * c + 2] = q.z; v[4 * c + 3] = q.w;
-            }
-        } else {
-#pragma unroll
-            for (int c = 0; c < T::CHUNKS; c++) {
-                const long long e = tbase + T::offset(warp, c, lane);
-#pragma unroll
-                for (int q = 0; q < 4; q++) v[4 * c + q] = (e + q < n) ? (unsigned)in[e + q] : 0u;
-            }
-        }
-        if (FLAGS) {
-#pragma unroll
-            for (int q = 0; q < ITEMS; q++) v[q] = v[q] != 0u;
-        }
-        T::scan(v, cb, status, tile, epoch, &hdr->error, s_warp, &s_prefix, s_limit);
-#pragma unroll
-        for (int c = 0; c < T::CHUNKS; c++) {
-            const long long e = tbase + T::offset(warp, c, lane);
-            const unsigned p0 = cb[c], p1 = p0 + v[4 * c], p2 = p1 + v[4 * c + 1],
-                           p3 = p2 + v[4 * c + 2];
-            if (out) {
-                if (e + 4 <= n) {
-                    __stcs(reinterpret_cast<int4*>(out + e),
-                           make_int4((int)p0, (int)p1, (int)p2, (int)p3));
-                } else {
-                    const unsigned pp[4] = {p0, p1, p2, p3};
-#pragma unroll
-                    for (int q = 0; q < 4; q++)
-                        if (e + q < n) out[e + q] = (int)pp[q];
-                }
-            }
-            if (FLAGS) {
-                const unsigned pp[4] = {p0, p1, p2, p3};
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-                    if (v[4 * c + q]) idx_out[pp[q]] = (int)(e + q);
-            }
-        }
-        if (FLAGS && count && tile == num_tiles - 1 && threadIdx.x == kPipeBlock - 1)
-            *count = (int)(cb[T::CHUNKS - 1] + v[ITEMS - 4] + v[ITEMS - 3] + v[ITEMS - 2] +
-                           v[ITEMS - 1]);
-        __syncthreads();  // every thread is done with this stage's buffer and tile index
-        if (threadIdx.x == 0) {
-            const int t = s_ok ? (int)atomicAdd(&hdr->tile_counter, 1u) : num_tiles;
-            s_tile[st] = t;
-            if (t < num_full) {
-                mbar_arrive_expect_tx(&bar[st], TILE_BYTES);
-                bulk_load(buf + (size_t)st * (TILE / 4), in + (long long)t * TILE, TILE_BYTES,
-                          &bar[st]);
-            }
-        }
-        __syncthreads();
-    }
-    // after a failed wait, let the copies this CTA started land before it exits
-    if (threadIdx.x == 0 && !s_ok) {
-        for (int k = 0; k < STAGES; k++) {
-            const int t = s_tile[k];
-            if (t < num_full) (void)mbar_wait(&bar[k], (phase >> k) & 1u, nullptr);
-        }
-    }
-}
-
-// Resident CTAs per SM of a pipelined launch shape (0 when it cannot run).
-template <int STAGES, int ITEMS, int LB, int MINB, bool FLAGS>
-int pipe_grid() {
-    static int g = -1;
-    if (g >= 0) return g;
-    const int smem = (int)pipe_smem_bytes<STAGES, ITEMS>();
-    int dev = 0, sms = 0, per = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaFuncSetAttribute(k_scan_pipe<STAGES, ITEMS, LB, MINB, FLAGS>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &per, k_scan_pipe<STAGES, ITEMS, LB, MINB, FLAGS>, kPipeBlock, smem) != cudaSuccess) {
-        (void)cudaGetLastError();
-        per = 0;
-    }
-    g = sms * per;
-    return g;
-}
-
-// Launches the pipelined pass; the caller has checked 16-byte alignment of in and out and
-// cleared the workspace (header and status words). Returns false when the shape cannot
-// run on this device (the caller then uses another form).
-template <int STAGES, int ITEMS, int LB, int MINB, bool FLAGS>
-bool launch_pipe(const int32_t* in, int32_t* out, long long n, void* ws, int32_t* idx_out,
-                 int32_t* count, cudaStream_t s) {
-    constexpr int TILE = kPipeBlock * ITEMS;
-    const int grid_max = pipe_grid<STAGES, ITEMS, LB, MINB, FLAGS>();
-    if (grid_max <= 0) return false;
-    const int tiles = (int)((n + TILE - 1) / TILE);
-    const int full = (int)(n / TILE);
-    const int grid = tiles < grid_max ? tiles : grid_max;
-    auto* hdr = static_cast<ScanHeader*>(ws);
-    auto* status = reinterpret_cast<unsigned long long*>(static_cast<char*>(ws) +
-                                                         sizeof(ScanHeader));
-    k_scan_pipe<STAGES, ITEMS, LB, MINB, FLAGS>
-        <<<grid, kPipeBlock, pipe_smem_bytes<STAGES, ITEMS>(), s>>>(in, out, n, hdr, status,
-                                                                   tiles, full, idx_out, count);
-    return true;
-}
-
 // Launch-shape variants of the standalone scan (tile = BLOCK x ITEMS values, look-back
 // windows of 32 x LB tiles, at least MINB resident CTAs per SM), selected by
 // scan_variant(); the default shape is variant 0.
@@ -823,7 +652,7 @@ extern "C" hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out
                                                          sizeof(ScanHeader));
     const bool vec = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) &
                       15u) == 0;
-    if ((variant == 0 || (variant >= 11 && variant < 20)) && n >= kTwoPassMinN) {
+    if ((variant == 0 || variant >= 11) && n >= kTwoPassMinN) {
         // the chunk sums are written before they are read: only the header is cleared.
         // Default: the two-kernel form; variants 11-13: waves of 2^22, 2^23, 2^24 values.
         const long long wave = variant == 11   ? (1LL << 22)
@@ -838,23 +667,6 @@ extern "C" hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out
                                                 nullptr, s, wave);
     }
     HHS_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, used, s));
-    if (variant >= 20 && vec) {
-        bool ok = false;
-        switch (variant) {
-            case 20: ok = launch_pipe<3, 32, 8, 2, false>(d_in, d_out, n, d_workspace, nullptr, nullptr, s); break;
-            case 21: ok = launch_pipe<4, 16, 8, 3, false>(d_in, d_out, n, d_workspace, nullptr, nullptr, s); break;
-            case 22: ok = launch_pipe<2, 32, 8, 3, false>(d_in, d_out, n, d_workspace, nullptr, nullptr, s); break;
-            case 23: ok = launch_pipe<3, 32, 4, 2, false>(d_in, d_out, n, d_workspace, nullptr, nullptr, s); break;
-            case 24: ok = launch_pipe<6, 16, 8, 2, false>(d_in, d_out, n, d_workspace, nullptr, nullptr, s); break;
-            case 25: ok = launch_pipe<4, 32, 8, 1, false>(d_in, d_out, n, d_workspace, nullptr, nullptr, s); break;
-            case 26: ok = launch_pipe<3, 16, 4, 4, false>(d_in, d_out, n, d_workspace, nullptr, nullptr, s); break;
-            default: break;
-        }
-        if (ok) {
-            HHS_LAUNCH_CHECK();
-            return HHS_OK;
-        }
-    }
     switch (variant) {
         case 1: launch_scan_v<256, 8, 1, 1>(d_in, d_out, n, d_workspace, vec, s); break;
         case 2: launch_scan_v<128, 16, 1, 1>(d_in, d_out, n, d_workspace, vec, s); break;

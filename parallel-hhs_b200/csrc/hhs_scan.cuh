@@ -56,7 +56,6 @@ __device__ __forceinline__ unsigned scan_lookback_w(unsigned long long* status, 
     while (true) {
         unsigned val[PER_LANE], flag[PER_LANE];
         while (true) {
-            bool ready = true;
 #pragma unroll
             for (int k = 0; k < PER_LANE; k++) {
                 const int idx = pred - (lane * PER_LANE + k);
@@ -68,9 +67,23 @@ __device__ __forceinline__ unsigned scan_lookback_w(unsigned long long* status, 
                     flag[k] = 2u;  // virtual tile -1: inclusive prefix 0
                     val[k] = 0u;
                 }
-                ready = ready && flag[k] != 0u;
             }
-            if (__all_sync(HHS_FULL_MASK, ready)) break;
+            // only the predecessors up to the nearest inclusive prefix matter: they must
+            // all have published (aggregate or inclusive); those beyond it need not have
+            int lane_p = PER_LANE;  // this lane's first inclusive entry
+            bool gap_before_p = false, gap_any = false;
+#pragma unroll
+            for (int k = PER_LANE - 1; k >= 0; k--)
+                if (flag[k] == 2u) lane_p = k;
+#pragma unroll
+            for (int k = 0; k < PER_LANE; k++) {
+                gap_any = gap_any || flag[k] == 0u;
+                gap_before_p = gap_before_p || (flag[k] == 0u && k < lane_p);
+            }
+            const unsigned with_p = __ballot_sync(HHS_FULL_MASK, lane_p < PER_LANE);
+            const int first_p = with_p ? __ffs(with_p) - 1 : 32;
+            const bool gap = lane < first_p ? gap_any : (lane == first_p ? gap_before_p : false);
+            if (!__any_sync(HHS_FULL_MASK, gap)) break;
             if (++spins > limit) {
                 if (lane == 0) atomicOr(err, HHS_ERRBIT_LOOKBACK_TIMEOUT);
 #pragma unroll

@@ -70,7 +70,7 @@ class Tuning(ctypes.Structure):
                 ("ctas_per_sm", ctypes.c_int32), ("warp_n", ctypes.c_int32),
                 ("cluster_size", ctypes.c_int32), ("mid_n", ctypes.c_int32),
                 ("packed", ctypes.c_int32), ("mid_dist_n", ctypes.c_int32),
-                ("ms_per_step", ctypes.c_double)]
+                ("overlap", ctypes.c_int32), ("ms_per_step", ctypes.c_double)]
 
 
 class RunLog(ctypes.Structure):
@@ -347,7 +347,7 @@ class Context:
         _check(lib().hhs_ctx_set_trace(self.h, nodes_ptr, capacity, count_ptr), "set_trace")
 
     def set_tuning(self, small_n=None, units_per_cta=None, ctas_per_sm=None, warp_n=None,
-                   cluster_size=None, mid_n=None, packed=None, mid_dist_n=None):
+                   cluster_size=None, mid_n=None, packed=None, mid_dist_n=None, overlap=None):
         t = Tuning()
         _check(lib().hhs_ctx_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
         if small_n is not None:
@@ -366,6 +366,8 @@ class Context:
             t.packed = int(packed)
         if mid_dist_n is not None:
             t.mid_dist_n = mid_dist_n
+        if overlap is not None:
+            t.overlap = int(overlap)
         _check(lib().hhs_ctx_set_tuning(self.h, ctypes.byref(t)), "set_tuning")
 
     def tuning(self):
@@ -374,7 +376,7 @@ class Context:
         return {"small_n": t.small_n, "units_per_cta": t.units_per_cta,
                 "ctas_per_sm": t.ctas_per_sm, "warp_n": t.warp_n,
                 "cluster_size": t.cluster_size, "mid_n": t.mid_n, "packed": t.packed,
-                "mid_dist_n": t.mid_dist_n}
+                "mid_dist_n": t.mid_dist_n, "overlap": t.overlap}
 
     def launch(self):
         """(grid CTAs for FP64, grid CTAs for mixed, dynamic shared memory bytes per CTA)."""
@@ -390,7 +392,7 @@ class Context:
         return {"small_n": t.small_n, "units_per_cta": t.units_per_cta,
                 "ctas_per_sm": t.ctas_per_sm, "warp_n": t.warp_n,
                 "cluster_size": t.cluster_size, "mid_n": t.mid_n, "packed": t.packed,
-                "mid_dist_n": t.mid_dist_n, "ms_per_step": t.ms_per_step}
+                "mid_dist_n": t.mid_dist_n, "overlap": t.overlap, "ms_per_step": t.ms_per_step}
 
     def autotune_results(self):
         """Every candidate the last autotune timed, as tuning dicts with ms_per_step."""

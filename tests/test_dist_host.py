@@ -204,7 +204,8 @@ def _agree_worker(rank, world, port, q, differ):
     d = hhs.Dist(rank, world, reps, lambda _s: True, 0)
     d.set_agreement(hhs.group_minmax())
     tuning = {"small_n": 64, "units_per_cta": 16, "ctas_per_sm": 2, "warp_n": 32,
-              "cluster_size": 4, "mid_n": 640, "packed": 0, "mid_dist_n": 96}
+              "cluster_size": 4, "mid_n": 640, "packed": 0, "mid_dist_n": 96,
+              "overlap": 1}
     if differ and rank == 1:
         tuning["cluster_size"] = 8  # this rank's engine would sum in another order
     h = hhs.config_hash(tuning, 284, hhs.PREC_MIXED, 4096, 1 / 64, 0.03)
@@ -234,7 +235,8 @@ def test_ranks_with_different_engine_tuning_are_rejected(hhs, differ):
 
 def test_config_hash_covers_every_field(hhs):
     base = {"small_n": 64, "units_per_cta": 16, "ctas_per_sm": 2, "warp_n": 32,
-            "cluster_size": 4, "mid_n": 640, "packed": 0, "mid_dist_n": 96}
+            "cluster_size": 4, "mid_n": 640, "packed": 0, "mid_dist_n": 96,
+              "overlap": 1}
     h0 = hhs.config_hash(base, 284, hhs.PREC_MIXED, 4096, 1 / 64, 0.03)
     assert h0 == hhs.config_hash(dict(base), 284, hhs.PREC_MIXED, 4096, 1 / 64, 0.03)
     seen = {h0}
