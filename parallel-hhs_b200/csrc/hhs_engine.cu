@@ -425,6 +425,8 @@ __device__ void ts_unit(const EParams& E, const int32_t* S, int n, int ib, int j
 // are >= 0, so integer order is float order). Max is exact and
 // order-independent: the result equals the all-pairs evaluation bit for bit.
 constexpr int kCB = 32;
+constexpr int kTsRows = 1;                // rows per thread in the symmetric timestep
+constexpr int kTsBlock = kTsRows * kEB;   // rows per unit
 
 // Units [u0, u1) of the upper triangle of (256-row block, kCB-column block) tiles, in
 // row-major order: a contiguous range per CTA, so consecutive units mostly share their row
@@ -441,33 +443,44 @@ __device__ void ts_sym_range(const EParams& E, const int32_t* S, int n, int u0, 
                              Smem& sm, const PeerOut* po = nullptr) {
     const SoA& P = E.P;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int kRowStep = kEB / kCB;
-    const int nrb = (n + kEB - 1) / kEB, ncb = (n + kCB - 1) / kCB;
+    constexpr int R = kTsRows;
+    constexpr int kRowStep = kTsBlock / kCB;
+    const int nrb = (n + kTsBlock - 1) / kTsBlock, ncb = (n + kCB - 1) / kCB;
     int rb = 0, off = u0;  // unit u0 = (rb, rb * kRowStep + off)
     while (rb < nrb && off >= ncb - rb * kRowStep) {
         off -= ncb - rb * kRowStep;
         rb++;
     }
-    int cur = -1, i = 0;
-    bool act = false;
-    DS xi{0, 0}, yi{0, 0}, zi{0, 0};
-    float vxi = 0, vyi = 0, vzi = 0, mi = 0, rowmax = 0.0f;
+    int cur = -1;
+    int i[R];
+    bool act[R];
+    DS xi[R], yi[R], zi[R];
+    float vxi[R], vyi[R], vzi[R], mi[R], rowmax[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        i[r] = 0; act[r] = false; rowmax[r] = 0.0f;
+        xi[r] = yi[r] = zi[r] = DS{0.f, 0.f};
+        vxi[r] = vyi[r] = vzi[r] = mi[r] = 0.0f;
+    }
     // the next unit's columns are loaded into registers while this unit computes
     double px = 0, py = 0, pz = 0, pvx = 0, pvy = 0, pvz = 0, pm = 0;
     bool have = false;
     for (int u = u0; u < u1 && rb < nrb; u++) {
         if (rb != cur) {
-            if (act && rowmax > 0.0f) rate_max(E, po, i, rowmax);
-            cur = rb;
-            rowmax = 0.0f;
-            i = rb * kEB + threadIdx.x;
-            act = i < n;
-            if (act) {
-                const int gi = list_at(S, i);
-                xi = ds_split(P.x[gi]); yi = ds_split(P.y[gi]); zi = ds_split(P.z[gi]);
-                vxi = (float)P.vx[gi]; vyi = (float)P.vy[gi]; vzi = (float)P.vz[gi];
-                mi = (float)P.m[gi];
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                if (act[r] && rowmax[r] > 0.0f) rate_max(E, po, i[r], rowmax[r]);
+                rowmax[r] = 0.0f;
+                i[r] = rb * kTsBlock + r * kEB + (int)threadIdx.x;
+                act[r] = i[r] < n;
+                if (act[r]) {
+                    const int gi = list_at(S, i[r]);
+                    xi[r] = ds_split(P.x[gi]); yi[r] = ds_split(P.y[gi]); zi[r] = ds_split(P.z[gi]);
+                    vxi[r] = (float)P.vx[gi]; vyi[r] = (float)P.vy[gi]; vzi[r] = (float)P.vz[gi];
+                    mi[r] = (float)P.m[gi];
+                }
             }
+            cur = rb;
         }
         const int c0 = (rb * kRowStep + off) * kCB;
         const int ncol = min(kCB, n - c0);
@@ -498,21 +511,26 @@ __device__ void ts_sym_range(const EParams& E, const int32_t* S, int n, int u0, 
                 }
             }
         }
-        // column maxima over the warp's 32 rows: one warp max-reduction per column on the
+        // column maxima over the warp's rows: one warp max-reduction per column on the
         // rates' bit patterns (rates are >= 0 or +inf, so integer order is float order);
         // lane c keeps column c's maximum
         unsigned colmax = 0u;
 #pragma unroll 8
         for (int jl = 0; jl < kCB; jl++) {
             const float4 A = sm.u.tsm.A[jl], B = sm.u.tsm.B[jl], V = sm.u.tsm.V[jl];
-            const float rate = ts_pair_rate_mixed(
-                ds_diff(xi.hi, xi.lo, A.x, B.x), ds_diff(yi.hi, yi.lo, A.y, B.y),
-                ds_diff(zi.hi, zi.lo, A.z, B.z), vxi - V.x, vyi - V.y, vzi - V.z, mi + A.w,
-                E.inv_eta_s2, E.inv_eta);
-            const bool ok = act && (jl < ncol) && (c0 + jl > i);
-            const float r = ok ? rate : 0.0f;
-            rowmax = fmaxf(rowmax, r);
-            const unsigned cm = __reduce_max_sync(HHS_FULL_MASK, __float_as_uint(r));
+            float cmax = 0.0f;
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const float rate = ts_pair_rate_mixed(
+                    ds_diff(xi[r].hi, xi[r].lo, A.x, B.x), ds_diff(yi[r].hi, yi[r].lo, A.y, B.y),
+                    ds_diff(zi[r].hi, zi[r].lo, A.z, B.z), vxi[r] - V.x, vyi[r] - V.y,
+                    vzi[r] - V.z, mi[r] + A.w, E.inv_eta_s2, E.inv_eta);
+                const bool ok = act[r] && (jl < ncol) && (c0 + jl > i[r]);
+                const float rr = ok ? rate : 0.0f;
+                rowmax[r] = fmaxf(rowmax[r], rr);
+                cmax = fmaxf(cmax, rr);
+            }
+            const unsigned cm = __reduce_max_sync(HHS_FULL_MASK, __float_as_uint(cmax));
             colmax = lane == jl ? cm : colmax;
         }
         sm.colred[warp][lane] = __uint_as_float(colmax);
@@ -528,7 +546,18 @@ __device__ void ts_sym_range(const EParams& E, const int32_t* S, int n, int u0, 
             rb++;
         }
     }
-    if (act && rowmax > 0.0f) rate_max(E, po, i, rowmax);
+#pragma unroll
+    for (int r = 0; r < R; r++)
+        if (act[r] && rowmax[r] > 0.0f) rate_max(E, po, i[r], rowmax[r]);
+}
+
+// Units of the upper triangle of (kTsBlock-row block, kCB-column block) tiles of a node
+__host__ __device__ __forceinline__ long long ts_sym_units(int n) {
+    constexpr int kRowStep = kTsBlock / kCB;
+    const long long nrb = (n + kTsBlock - 1) / kTsBlock, ncb = (n + kCB - 1) / kCB;
+    long long units = 0;
+    for (long long r = 0; r < nrb; r++) units += ncb - r * kRowStep > 0 ? ncb - r * kRowStep : 0;
+    return units;
 }
 
 
@@ -2683,10 +2712,7 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                     // only units with a pair j > i: row block rb takes column blocks
                     // cb >= rb * kEB / kCB; each worker takes a contiguous range of that
                     // triangle in row-major order
-                    const int nrb = (n + kEB - 1) / kEB, ncb = (n + kCB - 1) / kCB;
-                    constexpr int kRowStep = kEB / kCB;
-                    long long units = 0;
-                    for (int r = 0; r < nrb; r++) units += max(0, ncb - r * kRowStep);
+                    const long long units = ts_sym_units(n);
                     const int u0 = (int)(units * W.id / W.count);
                     const int u1 = (int)(units * (W.id + 1) / W.count);
                     ts_sym_range(E, S, n, u0, u1, sm);
@@ -3442,9 +3468,7 @@ hhs_status engine_shard_timesteps(hhs_ctx* c, const SoA& P, unsigned* rate_words
     const int grid = eh->grid[pi];
     if (pi == 1) {
         E.rate_acc = rate_words;
-        const long long nrb = (n + kEB - 1) / kEB, ncb = (n + kCB - 1) / kCB;
-        long long units = 0;
-        for (long long r = 0; r < nrb; r++) units += ncb - r * (kEB / kCB) > 0 ? ncb - r * (kEB / kCB) : 0;
+        const long long units = ts_sym_units(n);
         const long long u_lo = units * rank / world, u_hi = units * (rank + 1) / world;
         k_shard_ts_mixed<<<grid, kEB, kEngineSmem, s>>>(E, S, n, u_lo, u_hi, po);
         HHS_LAUNCH_CHECK();
