@@ -61,7 +61,7 @@ def parse():
                    help="write the per-level phase profile (JSON) to this path")
     p.add_argument("--workload", default="plummer16k",
                    choices=["plummer16k", "batched", "scan", "large", "deep", "validate",
-                            "plain1k"],
+                            "plain1k", "kickprobe"],
                    help="plummer16k (default headline), batched (512 clusters), scan (flag "
                         "compaction sweep), large (N=262144, 90/10 masses), deep (N=65536 "
                         "Salpeter), validate (integrate --n/--eta/--mass to --t-end in mixed "
@@ -663,6 +663,37 @@ def run_scan(a, torch):
                          "unit": "GB/s", "traffic": None}, "sweep": rows}
 
 
+def run_kickprobe(a, torch):
+    """The engine's mixed kick phase alone (hhs_engine_kick_accelerations: a split node
+    with every third particle fast) on a seeded sphere of --n particles: pair
+    evaluations per second, each fast-slow pair counted once, slow-slow pairs as the
+    ordered pairs the slow units evaluate."""
+    import hhs
+    n = a.n
+    s = hhs.plummer(n, a.seed)
+    ctx = hhs.Context(n, 64, eta=a.eta)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    L = hhs.lib()
+    for _ in range(a.warmup):
+        assert L.hhs_engine_kick_accelerations(ctx.h, d.ref, n, None) == 0
+    ctx.check()
+    ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    torch.cuda.synchronize()
+    ev[0].record()
+    for _ in range(a.steps):
+        assert L.hhs_engine_kick_accelerations(ctx.h, d.ref, n, None) == 0
+    ev[1].record()
+    ctx.check()
+    ms = ev[0].elapsed_time(ev[1]) / a.steps
+    nf = (n + 2) // 3
+    ns = n - nf
+    evals = nf * ns + ns * ns
+    return {"metric": "engine kick pair evaluations/s", "value": evals / (ms * 1e-3),
+            "unit": "pair evaluations/s", "n": n, "n_fast": nf, "n_slow": ns, "ms": ms,
+            "kick_pairs_equivalent_per_s": (2 * nf * ns + ns * (ns - 1)) / (ms * 1e-3)}
+
+
 def run_plain1k(a, torch):
     """Plain FP64 HOLD of a Plummer N=1024 sphere to t=1 on the GPU (device schedule) and on
     the CPU oracle (OpenMP, host cores): the final states must agree bit for bit."""
@@ -905,9 +936,10 @@ def main():
         if dist is not None:
             dist.destroy_process_group()
         return
-    if a.workload in ("scan", "validate", "plain1k"):
+    if a.workload in ("scan", "validate", "plain1k", "kickprobe"):
         if rank == 0:
-            fn = {"scan": run_scan, "validate": run_validate, "plain1k": run_plain1k}[a.workload]
+            fn = {"scan": run_scan, "validate": run_validate, "plain1k": run_plain1k,
+                  "kickprobe": run_kickprobe}[a.workload]
             out = fn(a, torch)
             if a.workload == "scan" and "roofline" in out:
                 hbm, src = hbm_peak()

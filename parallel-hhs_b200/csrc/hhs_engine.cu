@@ -48,6 +48,7 @@ constexpr int kEB = 256;          // engine block size (one sink per thread per 
 constexpr int kKB = 2 * kEB;      // sinks per block of the mixed grid kick (two per thread)
 constexpr int kTS = 1024;         // source records per shared-memory tile of that kick
 constexpr int kTX = 256;          // slow records per tile of the symmetric grid kick
+constexpr int kTW = 256;          // widest column tile of the packed grid timestep
 constexpr int kMaxFsb = 64;       // fast super-blocks of that kick (column-partial slots)
 constexpr int kMaxChunks = 32;    // source chunks per node (partial-sum slots)
 constexpr int kMaxLevels = 64;    // per-level state is kept in 64-bit masks
@@ -96,6 +97,11 @@ struct EParams {
     float4* pk_a;   // [pk_levels][n_max]
     float4* pk_b;   // [pk_levels][n_max]
     int pk_levels;
+    // the members of the current grid node packed for the mixed timestep, in list order:
+    // double-single position (tr_a = hi + mass, tr_b = lo) and FP32 velocity
+    float4* tr_a;
+    float4* tr_b;
+    float4* tr_v;
     int prec_mixed;  // this launch runs the mixed-precision kernels
     int overlap;     // slow-only kick units beside a subtree's first pass (tuning)
     int4* trace;                        // node record {level, n, n_fast, calc} in call order
@@ -145,7 +151,9 @@ struct __align__(16) Smem {
     unsigned bar_k;               // grid barriers passed by this CTA in this launch
     unsigned epoch;               // look-back epoch of the current split
     unsigned kphase;              // parity of the next phase of kbar
+    unsigned tphase;              // parities of the next phases of tbar[0], tbar[1]
     __align__(8) uint64_t kbar;   // completion barrier of the kick's source-tile copies
+    __align__(8) uint64_t tbar[2];  // completion barriers of the timestep's column tiles
     // last, so that the persistent kernel's dynamic allocation can extend it to a MidState
     union {
         struct { float4 A[kEB], B[kEB], V[kEB]; } tsm;         // mixed timestep tiles
@@ -153,6 +161,10 @@ struct __align__(16) Smem {
         struct { float4 A[kEB], B[kEB]; } km;                   // mixed kick tiles
         struct { float4 A[kTS], B[kTS]; } kt;                   // grid kick source tile
         struct { float4 A[kTX], B[kTX]; float colw[kEB / 32][kTX][3]; } kc;  // symmetric kick
+        struct {                                                  // packed timestep tiles
+            float4 A[2][kTW], B[2][kTW], V[2][kTW];
+            float colred[2][kEB / 32][kTW];
+        } ts2;
         struct { float4 P0[kEB], P1[kEB], P2[kEB]; float2 M[kEB]; } kx;  // packed kick tiles
         struct { double x[kEB], y[kEB], z[kEB], m[kEB]; } kd;   // FP64 kick tiles
         struct {                                                  // tiny-subtree state
@@ -560,6 +572,143 @@ __host__ __device__ __forceinline__ long long ts_sym_units(int n) {
     return units;
 }
 
+
+// ---------------------------------------------------------------- packed grid timestep
+// The same symmetric evaluation on the whole grid from the node's packed members (list
+// order, written by the kick-reduce phase that last changed them, or by pack_ts): units
+// are (kEB-row block, CW-column block) tiles of the upper triangle, CW chosen per node
+// (the widest of 256/128/64/32 that still gives every CTA two units). A CTA takes a
+// contiguous range of units in row-major order; each unit's columns arrive by bulk copy
+// into one of two shared buffers while the previous unit computes.
+__device__ __forceinline__ long long ts_tile_units(int n, int cw) {
+    const long long nrb = (n + kEB - 1) / kEB, ncb = (n + cw - 1) / cw, step = kEB / cw;
+    long long units = 0;
+    for (long long r = 0; r < nrb; r++) units += ncb - r * step > 0 ? ncb - r * step : 0;
+    return units;
+}
+
+__device__ __forceinline__ int ts_tile_width(int n, int workers) {
+    int cw = kTW;
+    while (cw > 32 && ts_tile_units(n, cw) < 2LL * workers) cw >>= 1;
+    return cw;
+}
+
+// The node's members (list S, n of them) into the packed timestep arrays.
+__device__ void pack_ts(const EParams& E, const int32_t* S, int n, const Workers& W) {
+    const SoA& P = E.P;
+    for (int i = W.id * kEB + (int)threadIdx.x; i < n; i += W.count * kEB) {
+        const int g = list_at(S, i);
+        const DS x = ds_split(P.x[g]), y = ds_split(P.y[g]), z = ds_split(P.z[g]);
+        E.tr_a[i] = make_float4(x.hi, y.hi, z.hi, (float)P.m[g]);
+        E.tr_b[i] = make_float4(x.lo, y.lo, z.lo, 0.0f);
+        E.tr_v[i] = make_float4((float)P.vx[g], (float)P.vy[g], (float)P.vz[g], 0.0f);
+    }
+}
+
+// unit u of the triangle -> (row block, column block)
+__device__ __forceinline__ void ts_tile_of(long long u, int nrb, int ncb, int step, int& rb,
+                                           int& cb) {
+    rb = 0;
+    while (rb < nrb && u >= ncb - (long long)rb * step) {
+        u -= ncb - (long long)rb * step;
+        rb++;
+    }
+    cb = rb * step + (int)u;
+}
+
+__device__ __forceinline__ void ts_tile_stage(const EParams& E, int buf, int c0, int ncol,
+                                              Smem& sm) {
+    const unsigned bytes = (unsigned)ncol * (unsigned)sizeof(float4);
+    mbar_arrive_expect_tx(&sm.tbar[buf], 3u * bytes);
+    bulk_load(sm.u.ts2.A[buf], E.tr_a + c0, bytes, &sm.tbar[buf]);
+    bulk_load(sm.u.ts2.B[buf], E.tr_b + c0, bytes, &sm.tbar[buf]);
+    bulk_load(sm.u.ts2.V[buf], E.tr_v + c0, bytes, &sm.tbar[buf]);
+}
+
+__device__ void ts_sym_tiles(const EParams& E, int n, int cw, long long u0, long long u1,
+                             Smem& sm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int step = kEB / cw;
+    const int nrb = (n + kEB - 1) / kEB, ncb = (n + cw - 1) / cw;
+    if (u0 >= u1) return;
+    int rb = 0, cb = 0;
+    ts_tile_of(u0, nrb, ncb, step, rb, cb);
+    // prologue: the first two units' columns
+    if (threadIdx.x == 0) {
+        int r2 = rb, c2 = cb;
+        for (int k = 0; k < 2 && u0 + k < u1; k++) {
+            const int c0 = c2 * cw;
+            ts_tile_stage(E, k, c0, min(cw, n - c0), sm);
+            if (++c2 >= ncb) { r2++; c2 = r2 * step; }
+        }
+    }
+    int cur = -1, i = 0;
+    bool act = false;
+    DS xi{0, 0}, yi{0, 0}, zi{0, 0};
+    float vxi = 0, vyi = 0, vzi = 0, mi = 0, rowmax = 0.0f;
+    unsigned phase = sm.tphase;
+    int nrb_n = rb, ncb_n = cb;  // the unit two ahead, for the refill
+    for (int k = 0; k < 2; k++)
+        if (++ncb_n >= ncb) { nrb_n++; ncb_n = nrb_n * step; }
+    for (long long u = u0; u < u1; u++) {
+        const int buf = (int)((u - u0) & 1);
+        if (rb != cur) {
+            if (act && rowmax > 0.0f) rate_max(E, nullptr, i, rowmax);
+            cur = rb;
+            rowmax = 0.0f;
+            i = rb * kEB + threadIdx.x;
+            act = i < n;
+            if (act) {
+                const float4 a = E.tr_a[i], b = E.tr_b[i], v = E.tr_v[i];
+                xi = DS{a.x, b.x}; yi = DS{a.y, b.y}; zi = DS{a.z, b.z};
+                vxi = v.x; vyi = v.y; vzi = v.z; mi = a.w;
+            }
+        }
+        const int c0 = cb * cw;
+        const int ncol = min(cw, n - c0);
+        if (!mbar_wait(&sm.tbar[buf], (phase >> buf) & 1u, E.err))
+            (void)mbar_wait(&sm.tbar[buf], (phase >> buf) & 1u, nullptr);
+        phase ^= 1u << buf;
+        const float4* TA = sm.u.ts2.A[buf];
+        const float4* TB = sm.u.ts2.B[buf];
+        const float4* TV = sm.u.ts2.V[buf];
+        for (int g = 0; g < ncol; g += 32) {
+            const int nc = min(32, ncol - g);
+            unsigned colmax = 0u;
+#pragma unroll 8
+            for (int c = 0; c < nc; c++) {
+                const int jl = g + c;
+                const float4 A = TA[jl], B = TB[jl], V = TV[jl];
+                const float rate = ts_pair_rate_mixed(
+                    ds_diff(xi.hi, xi.lo, A.x, B.x), ds_diff(yi.hi, yi.lo, A.y, B.y),
+                    ds_diff(zi.hi, zi.lo, A.z, B.z), vxi - V.x, vyi - V.y, vzi - V.z, mi + A.w,
+                    E.inv_eta_s2, E.inv_eta);
+                const float r = (act && c0 + jl > i) ? rate : 0.0f;
+                rowmax = fmaxf(rowmax, r);
+                const unsigned cm = __reduce_max_sync(HHS_FULL_MASK, __float_as_uint(r));
+                colmax = lane == c ? cm : colmax;
+            }
+            sm.u.ts2.colred[buf][warp][g + lane] = __uint_as_float(colmax);
+        }
+        __syncthreads();  // this buffer's columns are read, colred[buf] is complete
+        if ((int)threadIdx.x < ncol) {
+            float cm = 0.0f;
+#pragma unroll
+            for (int w = 0; w < kEB / 32; w++) cm = fmaxf(cm, sm.u.ts2.colred[buf][w][threadIdx.x]);
+            if (cm > 0.0f) rate_max(E, nullptr, c0 + (int)threadIdx.x, cm);
+        }
+        if (threadIdx.x == 0 && u + 2 < u1) {
+            const int cn = ncb_n * cw;
+            ts_tile_stage(E, buf, cn, min(cw, n - cn), sm);
+        }
+        if (++ncb_n >= ncb) { nrb_n++; ncb_n = nrb_n * step; }
+        if (++cb >= ncb) { rb++; cb = rb * step; }
+    }
+    if (act && rowmax > 0.0f) rate_max(E, nullptr, i, rowmax);
+    __syncthreads();  // colred and the buffers are free; every wait of this range is done
+    if (threadIdx.x == 0) sm.tphase = phase;
+    __syncthreads();
+}
 
 // ---------------------------------------------------------------- kick units
 // Sinks s in [0, nf + ns): s < nf -> F[s] (fast), else L[s - nf] (slow). Sources j in
@@ -1549,6 +1698,13 @@ __device__ void kick_reduce_phase(const EParams& E, const int32_t* F, const int3
 #pragma unroll
                 for (int c = 0; c < 3; c++) v1[c] = fma(red[3 * threadIdx.x + c], dt, v0[c]);
                 P.vx[g] = v1[0]; P.vy[g] = v1[1]; P.vz[g] = v1[2];
+                if (!slow && E.tr_a && W.mode == kModeGrid) {
+                    // the fast set's next pass recomputes its timesteps from these records
+                    const DS x = ds_split(P.x[g]), y = ds_split(P.y[g]), z = ds_split(P.z[g]);
+                    E.tr_a[s2] = make_float4(x.hi, y.hi, z.hi, (float)P.m[g]);
+                    E.tr_b[s2] = make_float4(x.lo, y.lo, z.lo, 0.0f);
+                    E.tr_v[s2] = make_float4((float)v1[0], (float)v1[1], (float)v1[2], 0.0f);
+                }
                 if (slow) {
                     P.x[g] = fma(v1[0], h, fma(v0[0], h, P.x[g]));
                     P.y[g] = fma(v1[1], h, fma(v0[1], h, P.y[g]));
@@ -2708,6 +2864,17 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                         ts_unit<PREC>(E, S, n, ib, j0, j1, E.ts_part + (size_t)jc * E.n_max,
                                       nullptr, sm);
                     }
+                } else if (MODE == kModeGrid && E.tr_a) {
+                    // packed members: written by the parent's kick-reduce phase when it
+                    // ran (the second pass of a fast set), else packed here
+                    if (lvl == top || ld_volatile_i32(&E.counts[lvl - 1].n_slow) == 0) {
+                        pack_ts(E, S, n, W);
+                        if (!phase_barrier(E, sm, W)) return false;
+                    }
+                    const int cw = ts_tile_width(n, W.count);
+                    const long long units = ts_tile_units(n, cw);
+                    ts_sym_tiles(E, n, cw, units * W.id / W.count, units * (W.id + 1) / W.count,
+                                 sm);
                 } else {
                     // only units with a pair j > i: row block rb takes column blocks
                     // cb >= rb * kEB / kCB; each worker takes a contiguous range of that
@@ -2810,7 +2977,10 @@ __global__ void __launch_bounds__(kEB, 2) k_engine(EParams E) {
     if (threadIdx.x == 0) {
         sm.bar_k = 0u;  // thread 0 alone uses it
         sm.kphase = 0u;
+        sm.tphase = 0u;
         mbar_init(&sm.kbar, 1u);
+        mbar_init(&sm.tbar[0], 1u);
+        mbar_init(&sm.tbar[1], 1u);
         fence_barrier_init();
     }
     __syncthreads();
@@ -3121,6 +3291,9 @@ struct EngineHost {
     float4* pk_b = nullptr;
     int pk_levels = 0;
     double* c_part = nullptr;
+    float4* tr_a = nullptr;
+    float4* tr_b = nullptr;
+    float4* tr_v = nullptr;
     int32_t* trace = nullptr;                 // caller's node-record buffer (4 int32 each)
     unsigned long long* trace_count = nullptr;
     long long trace_cap = 0;
@@ -3141,7 +3314,7 @@ size_t engine_workspace_bytes(int n_max, int max_levels) {
            al(sizeof(double) * kMaxChunks * 3 * n) + al(sizeof(int) * (n / kEB + 2)) +
            al(sizeof(unsigned) * n) + al(sizeof(unsigned long long) * (n / kEB + 2)) +
            2 * al(sizeof(float4) * n * (size_t)pk_levels_for(max_levels)) +
-           al(sizeof(double) * kMaxFsb * 3 * n);
+           al(sizeof(double) * kMaxFsb * 3 * n) + 3 * al(sizeof(float4) * n);
 }
 
 hhs_status engine_init(hhs_ctx* c, void* base) {
@@ -3159,7 +3332,10 @@ hhs_status engine_init(hhs_ctx* c, void* base) {
     eh->pk_levels = pk_levels_for(c->max_levels);
     eh->pk_a = reinterpret_cast<float4*>(p); p += al(sizeof(float4) * n * (size_t)eh->pk_levels);
     eh->pk_b = reinterpret_cast<float4*>(p); p += al(sizeof(float4) * n * (size_t)eh->pk_levels);
-    eh->c_part = reinterpret_cast<double*>(p);
+    eh->c_part = reinterpret_cast<double*>(p); p += al(sizeof(double) * kMaxFsb * 3 * n);
+    eh->tr_a = reinterpret_cast<float4*>(p); p += al(sizeof(float4) * n);
+    eh->tr_b = reinterpret_cast<float4*>(p); p += al(sizeof(float4) * n);
+    eh->tr_v = reinterpret_cast<float4*>(p);
     eh->n_max = c->n_max;
     int dev = 0, sms = 0, coop = 0;
     cudaGetDevice(&dev);
@@ -3365,6 +3541,9 @@ EParams engine_params(hhs_ctx* c, EngineHost* eh, const SoA& P, int n, double dt
     E.ts_part = eh->ts_part;
     E.k_part = eh->k_part;
     E.c_part = eh->c_part;
+    E.tr_a = eh->tr_a;
+    E.tr_b = eh->tr_b;
+    E.tr_v = eh->tr_v;
     E.tile_counts = eh->tile_counts;
     E.tile_status = eh->tile_status;
     E.rate_acc = eh->rate_acc;
@@ -3732,6 +3911,7 @@ extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, d
     E.leaf_time = nullptr;
     E.stats = b->d_stats;
     E.ts_part = E.k_part = E.c_part = nullptr;
+    E.tr_a = E.tr_b = E.tr_v = nullptr;
     E.tile_counts = nullptr;
     E.tile_status = nullptr;
     E.rate_acc = nullptr;
