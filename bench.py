@@ -331,7 +331,8 @@ def run_ours(a, rank, world, torch, dist):
         prof = ctx.profile()
         if a.profile_out and a.schedule == "auto":
             lms, lcnt = ctx.level_profile()
-            kinds = ["timesteps", "kick", "split", "update", "engine", "subtree", "cluster_node", "k7"]
+            kinds = ["timesteps", "kick", "split", "update", "engine", "subtree", "cluster_node",
+                     "subtree_stages"]
             lp = {kinds[k]: {str(l): [round(float(lms[k, l]) / a.steps, 4), int(lcnt[k, l]) // a.steps]
                              for l in range(64) if lcnt[k, l]} for k in range(8)}
             with open(a.profile_out, "w") as f:

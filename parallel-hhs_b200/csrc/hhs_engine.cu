@@ -160,7 +160,10 @@ struct __align__(16) Smem {
         struct { double x[kEB], y[kEB], z[kEB], vx[kEB], vy[kEB], vz[kEB], m[kEB]; } tsd;
         struct { float4 A[kEB], B[kEB]; } km;                   // mixed kick tiles
         struct { float4 A[kTS], B[kTS]; } kt;                   // grid kick source tile
-        struct { float4 A[kTX], B[kTX]; float colw[kEB / 32][kTX][3]; } kc;  // symmetric kick
+        struct {                                                  // symmetric kick
+            float4 A[2][kTX], B[2][kTX];
+            float colw[kEB / 32][kTX][3];
+        } kc;
         struct {                                                  // packed timestep tiles
             float4 A[2][kTW], B[2][kTW], V[2][kTW];
             float colred[2][kEB / 32][kTW];
@@ -1143,26 +1146,47 @@ __device__ __forceinline__ void warp_colsum8(const float (&v)[8][3], float (&r)[
     }
 }
 
-// Slow records [a, b) of the level's packed array into sm.u.kc (bulk copy), the rest of
-// the last group of eight zeroed (massless records far from nothing: their terms vanish).
-__device__ void kick_stage_slow(const EParams& E, const float4* PA, const float4* PB, int a,
-                                int b, Smem& sm) {
-    __syncthreads();  // every thread is done with the previous tile
-    const int len = b - a;
-    if (threadIdx.x == 0) {
-        const unsigned bytes = (unsigned)len * (unsigned)sizeof(float4);
-        mbar_arrive_expect_tx(&sm.kbar, 2u * bytes);
-        bulk_load(sm.u.kc.A, PA + a, bytes, &sm.kbar);
-        bulk_load(sm.u.kc.B, PB + a, bytes, &sm.kbar);
+// Two shared buffers of slow records: the tile a unit computes on, and the first tile of
+// the next unit, copied in while this one computes. State is uniform across the CTA.
+struct TileCache {
+    int a[2], b[2];      // records [a, b) of the level's packed array held (or on their way)
+    bool pending[2];     // a copy into the buffer was issued and not yet waited for
+    unsigned phase;      // parities of the buffers' barriers (sm.tbar)
+};
+
+// thread 0: copy records [a, b) into buffer c
+__device__ __forceinline__ void tc_issue(const float4* PA, const float4* PB, int a, int b, int c,
+                                         Smem& sm) {
+    const unsigned bytes = (unsigned)(b - a) * (unsigned)sizeof(float4);
+    mbar_arrive_expect_tx(&sm.tbar[c], 2u * bytes);
+    bulk_load(sm.u.kc.A[c], PA + a, bytes, &sm.tbar[c]);
+    bulk_load(sm.u.kc.B[c], PB + a, bytes, &sm.tbar[c]);
+}
+
+// Makes records [a, b) available in buffer c (every thread calls it): copies them unless
+// they are held or on their way, waits for an outstanding copy, and zeroes the records
+// after b up to the next multiple of eight (massless: their pair terms vanish).
+__device__ void tc_use(const EParams& E, const float4* PA, const float4* PB, int a, int b, int c,
+                       TileCache& tc, Smem& sm) {
+    if (tc.a[c] != a || tc.b[c] != b) {
+        __syncthreads();  // every thread is done with the buffer's previous records
+        if (threadIdx.x == 0) tc_issue(PA, PB, a, b, c, sm);
+        tc.a[c] = a;
+        tc.b[c] = b;
+        tc.pending[c] = true;
     }
-    const int len8 = (len + 7) & ~7;
-    if ((int)threadIdx.x < len8 - len) {
-        sm.u.kc.A[len + threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
-        sm.u.kc.B[len + threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (tc.pending[c]) {
+        if (!mbar_wait(&sm.tbar[c], (tc.phase >> c) & 1u, E.err))
+            (void)mbar_wait(&sm.tbar[c], (tc.phase >> c) & 1u, nullptr);
+        tc.phase ^= 1u << c;
+        tc.pending[c] = false;
+        const int len = b - a, len8 = (len + 7) & ~7;
+        if ((int)threadIdx.x < len8 - len) {
+            sm.u.kc.A[c][len + threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
+            sm.u.kc.B[c][len + threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncthreads();
     }
-    if (!mbar_wait(&sm.kbar, sm.kphase, E.err)) (void)mbar_wait(&sm.kbar, sm.kphase, nullptr);
-    __syncthreads();
-    if (threadIdx.x == 0) sm.kphase ^= 1u;
 }
 
 // pair vector w = d * r3 (d = source - sink, r3 = 1/|d|^3 with one Newton correction)
@@ -1183,7 +1207,7 @@ __device__ __forceinline__ void pair_w(const float4 A, const float4 B, const Sin
 
 __device__ void kick_cross_unit(const EParams& E, const int32_t* F, int nf, int lvl,
                                 const KickPlan& p, int fsb, int jc, int ns, Smem& sm,
-                                int& res_a, int& res_b) {
+                                TileCache& tc, int cb) {
     const SoA& P = E.P;
     const size_t nmx = E.n_max;
     const float4* PA = E.pk_a + (size_t)lvl * nmx;
@@ -1207,18 +1231,16 @@ __device__ void kick_cross_unit(const EParams& E, const int32_t* F, int nf, int 
         float acc[3] = {0.f, 0.f, 0.f}, cmp[3] = {0.f, 0.f, 0.f};
         for (int a = j0; a < j1; a += kTX) {
             const int b = min(j1, a + kTX), len = b - a;
-            if (a != res_a || b != res_b) {
-                kick_stage_slow(E, PA, PB, a, b, sm);
-                res_a = a;
-                res_b = b;
-            }
+            tc_use(E, PA, PB, a, b, cb, tc, sm);
+            const float4* TA = sm.u.kc.A[cb];
+            const float4* TB = sm.u.kc.B[cb];
             float bl[3] = {0.f, 0.f, 0.f};
             int nb = 0;
             for (int g8 = 0; g8 < len; g8 += 8) {
                 float v[8][3];
 #pragma unroll
                 for (int c = 0; c < 8; c++) {
-                    const float4 A = sm.u.kc.A[g8 + c], B = sm.u.kc.B[g8 + c];
+                    const float4 A = TA[g8 + c], B = TB[g8 + c];
                     float wx, wy, wz;
                     pair_w(A, B, q, eps2, wx, wy, wz);
                     bl[0] = fmaf(wx, A.w, bl[0]);
@@ -1270,7 +1292,7 @@ __device__ void kick_cross_unit(const EParams& E, const int32_t* F, int nf, int 
 }
 
 __device__ void kick_slow_unit(const EParams& E, int nf, int lvl, const KickPlan& p, int sb,
-                               int jc, int ns, Smem& sm, int& res_a, int& res_b) {
+                               int jc, int ns, Smem& sm, TileCache& tc, int cb) {
     const size_t nmx = E.n_max;
     const float4* PA = E.pk_a + (size_t)lvl * nmx;
     const float4* PB = E.pk_b + (size_t)lvl * nmx;
@@ -1286,17 +1308,15 @@ __device__ void kick_slow_unit(const EParams& E, int nf, int lvl, const KickPlan
     float acc[3] = {0.f, 0.f, 0.f}, cmp[3] = {0.f, 0.f, 0.f};
     for (int a = j0; a < j1; a += kTX) {
         const int b = min(j1, a + kTX), len = b - a;
-        if (a != res_a || b != res_b) {
-            kick_stage_slow(E, PA, PB, a, b, sm);
-            res_a = a;
-            res_b = b;
-        }
+        tc_use(E, PA, PB, a, b, cb, tc, sm);
+        const float4* TA = sm.u.kc.A[cb];
+        const float4* TB = sm.u.kc.B[cb];
         for (int jb = 0; jb < len; jb += 32) {
             const int je = min(len, jb + 32);
             float bl[3] = {0.f, 0.f, 0.f};
 #pragma unroll 4
             for (int j = jb; j < je; j++)
-                kick_pair_nr(sm.u.kc.A[j], sm.u.kc.B[j], q, eps2, bl[0], bl[1], bl[2]);
+                kick_pair_nr(TA[j], TB[j], q, eps2, bl[0], bl[1], bl[2]);
 #pragma unroll
             for (int k = 0; k < 3; k++) kahan_add(acc[k], cmp[k], bl[k]);
         }
@@ -1309,25 +1329,71 @@ __device__ void kick_slow_unit(const EParams& E, int nf, int lvl, const KickPlan
 
 // Units of one kind set, taken from the level's counter `set` until none is left:
 // kinds 0 = cross units then slow units, 1 = slow units only, 2 = cross units only.
+// While a unit computes, thread 0 already takes the next unit and starts the copy of its
+// first tile into the other buffer.
+__device__ __forceinline__ void unit_first_tile(const KickPlan& p, int nx, int u, int& a, int& b) {
+    const int jc = u < nx ? u / p.nfsb : (u - nx) / p.nsb;
+    a = jc * p.Cs;
+    b = a + min(p.Cs, kTX);
+}
+
 __device__ void kick_sym_units(const EParams& E, const int32_t* F, int nf, int ns, int lvl,
                                const KickPlan& p, int set, int kinds, Smem& sm) {
     const int nx = kinds == 1 ? 0 : p.nx;
     const int total = nx + (kinds == 2 ? 0 : p.nsl);
-    int res_a = -1, res_b = -1;
+    const float4* PA = E.pk_a + (size_t)lvl * E.n_max;
+    const float4* PB = E.pk_b + (size_t)lvl * E.n_max;
     unsigned* ctr = &E.st->kick_ctr[set][lvl];
-    while (true) {
-        __syncthreads();  // every thread has read the previous unit index
-        if (threadIdx.x == 0) sm.bcast = (int)atomicAdd(ctr, 1u);
-        __syncthreads();
-        const int u = sm.bcast;
-        if (u >= total) break;
+    TileCache tc;
+    tc.a[0] = tc.a[1] = tc.b[0] = tc.b[1] = -1;
+    tc.pending[0] = tc.pending[1] = false;
+    tc.phase = sm.tphase;
+    __syncthreads();  // every thread has read sm.tphase and the previous phase's sm.bcast
+    if (threadIdx.x == 0) sm.bcast = (int)atomicAdd(ctr, 1u);
+    __syncthreads();
+    int u = sm.bcast, c = 0;
+    auto clip = [&](int& a, int& b) { b = min(b, ns); };
+    if (u < total) {
+        int a, b;
+        unit_first_tile(p, nx, u, a, b);
+        clip(a, b);
+        if (threadIdx.x == 0) tc_issue(PA, PB, a, b, c, sm);
+        tc.a[c] = a; tc.b[c] = b; tc.pending[c] = true;
+    }
+    while (u < total) {
+        __syncthreads();  // every thread has read sm.bcast
+        if (threadIdx.x == 0) {
+            const int un = (int)atomicAdd(ctr, 1u);
+            sm.bcast = un;
+            if (un < total) {
+                int a, b;
+                unit_first_tile(p, nx, un, a, b);
+                clip(a, b);
+                if (tc.a[c ^ 1] != a || tc.b[c ^ 1] != b) tc_issue(PA, PB, a, b, c ^ 1, sm);
+            }
+        }
         if (u < nx) {
-            kick_cross_unit(E, F, nf, lvl, p, u % p.nfsb, u / p.nfsb, ns, sm, res_a, res_b);
+            kick_cross_unit(E, F, nf, lvl, p, u % p.nfsb, u / p.nfsb, ns, sm, tc, c);
         } else {
             const int v = u - nx;
-            kick_slow_unit(E, nf, lvl, p, v % p.nsb, v / p.nsb, ns, sm, res_a, res_b);
+            kick_slow_unit(E, nf, lvl, p, v % p.nsb, v / p.nsb, ns, sm, tc, c);
         }
+        __syncthreads();  // the unit is done; sm.bcast holds the next one
+        const int un = sm.bcast;
+        if (un < total) {
+            int a, b;
+            unit_first_tile(p, nx, un, a, b);
+            clip(a, b);
+            if (tc.a[c ^ 1] != a || tc.b[c ^ 1] != b) {
+                tc.a[c ^ 1] = a; tc.b[c ^ 1] = b; tc.pending[c ^ 1] = true;
+            }
+        }
+        u = un;
+        c ^= 1;
     }
+    __syncthreads();
+    if (threadIdx.x == 0) sm.tphase = tc.phase;
+    __syncthreads();
 }
 
 // ---------------------------------------------------------------- packed kick units
@@ -2459,6 +2525,20 @@ __device__ void warp_subtree(const EParams& E, MidState& M, const unsigned* memw
 
 // cs, rank: the hardware cluster that runs the subtree (every CTA of it calls mid_hold),
 // or cs = 1 for one CTA alone whatever cluster it belongs to.
+// Fine-grained timing inside the cluster subtree solver (profiling only; CTA 0, thread 0):
+// kind 7 of the level table, slots 56 load, 57 timesteps, 58 split, 59 kick, 60 warp
+// subtrees, 61 write-back.
+__device__ __forceinline__ void mid_mark(const EParams& E, Smem& sm, unsigned long long& t,
+                                         int slot) {
+    if (!E.profile || blockIdx.x != 0 || threadIdx.x != 0) return;
+    const unsigned long long now = gtimer();
+    if (slot >= 0) {
+        sm.prof_ns[7][slot] += now - t;
+        sm.prof_cnt[7][slot] += 1;
+    }
+    t = now;
+}
+
 template <int PREC>
 __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, bool calc0,
                          int dist_n, int cs, int rank, Smem& sm) {
@@ -2468,6 +2548,8 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const SoA& P = E.P;
     const int nw = (n + 31) >> 5;
+    unsigned long long tm = 0;
+    mid_mark(E, sm, tm, -1);
     for (int k = tid; k < n; k += kEB) {
         const int g = list_at(S, k);
         M.g[k] = g;
@@ -2480,6 +2562,7 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
         M.allw[tid] = tid < nw ? (tid == nw - 1 && (n & 31) ? (1u << (n & 31)) - 1u : ~0u) : 0u;
     if (tid == 0) M.nmem[0] = n;
     __syncthreads();
+    mid_mark(E, sm, tm, 56);
     // work counters of this subtree (thread 0; added to the context once, by CTA 0)
     unsigned long long nodes = 0;
     int maxl = 0;
@@ -2500,14 +2583,17 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
             }
             if (M.nmem[d] <= 32) {
                 // at most 32 members: the whole subtree on warp 0 of every CTA
+                mid_mark(E, sm, tm, -1);
                 if (warp == 0)
                     warp_subtree<PREC>(E, M, memw, nw, M.nmem[d], lvl, (calcm & bit) != 0,
                                        nodes, maxl, kpairs, tpairs, leaf, ok, rank == 0);
                 __syncthreads();
+                mid_mark(E, sm, tm, 60);
                 calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
                 d--;
                 continue;
             }
+            mid_mark(E, sm, tm, -1);
             if (calcm & bit) {
                 // ---- timesteps of the members (min over all other members)
                 const int nm = mid::compact(memw, nw, M.mem, M);
@@ -2577,6 +2663,7 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
                 if (tid == 0) tpairs += (double)nm * (double)(nm - 1);
                 }
             }
+            mid_mark(E, sm, tm, 57);
             // ---- split: fast = members with ts <= dt, N_fast == 1 folded into the slow set
             int cnt = 0, mcnt = 0;
             for (int w = warp; w < nw; w += kEB / 32) {
@@ -2614,6 +2701,7 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
             }
             __syncthreads();  // everyone has read fmask[d] before the fold clears it
             if (lone >= 0 && tid == 0) M.fmask[d][lone >> 5] = 0u;
+            mid_mark(E, sm, tm, 58);
             after1 |= bit;
             if (nf > 0) {
                 d++;
@@ -2624,6 +2712,7 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
             __syncthreads();
         }
         if (!(after2 & bit)) {
+            mid_mark(E, sm, tm, -1);
             // ---- kick order: slow slots (stable, lone last), then fast slots
             int nf = 0;
             const int ns = mid::kick_order(memw, M.fmask[d], M.lone[d], nw, M.kl, M, &nf);
@@ -2742,6 +2831,7 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
                 }
                 __syncthreads();
             }
+            mid_mark(E, sm, tm, 59);
             after2 |= bit;
             if (nf > 0) {
                 d++;
@@ -2754,6 +2844,7 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
         calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;
         d--;
     }
+    mid_mark(E, sm, tm, -1);
     // write back this CTA's share of the slots; work counters once per subtree
     for (int k = rank + cs * tid; k < n; k += cs * kEB) {
         const int g = M.g[k];
@@ -2770,6 +2861,7 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
     }
     if (cs > 1) cl.sync();
     else __syncthreads();
+    mid_mark(E, sm, tm, 61);
 }
 
 // True when the kick of level lvl (a grid node with a fast set of at most mid_n) runs its
@@ -3004,7 +3096,10 @@ __global__ void __launch_bounds__(kEB, 2) k_engine_accel(EParams E) {
     if (threadIdx.x == 0) {
         sm.bar_k = 0u;
         sm.kphase = 0u;
+        sm.tphase = 0u;
         mbar_init(&sm.kbar, 1u);
+        mbar_init(&sm.tbar[0], 1u);
+        mbar_init(&sm.tbar[1], 1u);
         fence_barrier_init();
     }
     __syncthreads();

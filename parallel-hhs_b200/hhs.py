@@ -55,8 +55,10 @@ class Profile(ctypes.Structure):
                 ("pairs", ctypes.c_double * 8)]
 
 
+# kind 7: stages inside the cluster subtree solver, by slot (56 load, 57 timesteps, 58 split,
+# 59 kick, 60 warp subtrees, 61 write-back) in the per-level table
 PROFILE_KINDS = ("timesteps", "kick", "split", "update", "engine", "subtree", "cluster_node",
-                 "k7")
+                 "subtree_stages")
 
 
 class BatchTuning(ctypes.Structure):
