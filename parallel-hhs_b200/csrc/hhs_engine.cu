@@ -50,6 +50,7 @@ constexpr int kTS = 1024;         // source records per shared-memory tile of th
 constexpr int kTX = 256;          // slow records per tile of the symmetric grid kick
 constexpr int kTW = 256;          // widest column tile of the packed grid timestep
 constexpr int kMaxFsb = 64;       // fast super-blocks of that kick (column-partial slots)
+constexpr int kXRows = 2;         // fast sinks per thread in that kick's cross units
 constexpr int kMaxChunks = 32;    // source chunks per node (partial-sum slots)
 constexpr int kMaxLevels = 64;    // per-level state is kept in 64-bit masks
 constexpr unsigned long long kBarrierTimeoutNs = 60ull * 1000000000ull;
@@ -1094,14 +1095,14 @@ __device__ void kick_units_grid(const EParams& E, const int32_t* F, int nf, int 
 // super-block partials in order: every sum has a fixed order, so a step is deterministic.
 struct KickPlan {
     int ncs, Cs;         // slow chunks: ncs chunks of Cs slow particles
-    int nsub, FB, nfsb;  // fast sub-blocks of kEB sinks; FB of them per super-block
+    int nsub, FB, nfsb;  // fast sub-blocks of kXRows*kEB sinks; FB of them per super-block
     int nsb;             // blocks of kEB slow sinks
     int nx, nsl;         // cross units (nfsb x ncs) and slow units (nsb x ncs)
 };
 
 __device__ __forceinline__ KickPlan kick_plan(int nf, int ns, int workers) {
     KickPlan p;
-    p.nsub = (nf + kEB - 1) / kEB;
+    p.nsub = (nf + kXRows * kEB - 1) / (kXRows * kEB);
     const int f = p.nsub < kMaxFsb ? p.nsub : kMaxFsb;
     p.FB = f > 0 ? (p.nsub + f - 1) / f : 1;
     p.nfsb = (p.nsub + p.FB - 1) / p.FB;
@@ -1205,9 +1206,11 @@ __device__ __forceinline__ void pair_w(const float4 A, const float4 B, const Sin
     wz = __fmul_rn(dz, r3);
 }
 
+// kXRows fast sinks per thread: the column sums' butterfly then serves kXRows rows at once
 __device__ void kick_cross_unit(const EParams& E, const int32_t* F, int nf, int lvl,
                                 const KickPlan& p, int fsb, int jc, int ns, Smem& sm,
                                 TileCache& tc, int cb) {
+    constexpr int R = kXRows;
     const SoA& P = E.P;
     const size_t nmx = E.n_max;
     const float4* PA = E.pk_a + (size_t)lvl * nmx;
@@ -1218,58 +1221,82 @@ __device__ void kick_cross_unit(const EParams& E, const int32_t* F, int nf, int 
     const float eps2 = E.eps2f;
     const int sb0 = fsb * p.FB, sb1 = min(p.nsub, sb0 + p.FB);
     for (int sb = sb0; sb < sb1; sb++) {
-        const int s = sb * kEB + (int)threadIdx.x;
-        const bool act = s < nf;
-        SinkDS q{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        float nmi = 0.0f;  // -m_i: the column terms
-        if (act) {
-            const int g = F[s];
-            const DS x = ds_split(P.x[g]), y = ds_split(P.y[g]), z = ds_split(P.z[g]);
-            q = SinkDS{-x.hi, -y.hi, -z.hi, -x.lo, -y.lo, -z.lo};
-            nmi = -(float)P.m[g];
+        int s[R];
+        SinkDS q[R];
+        float nmi[R];  // -m_i: the column terms
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            s[r] = sb * (R * kEB) + r * kEB + (int)threadIdx.x;
+            q[r] = SinkDS{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            nmi[r] = 0.0f;
+            if (s[r] < nf) {
+                const int g = F[s[r]];
+                const DS x = ds_split(P.x[g]), y = ds_split(P.y[g]), z = ds_split(P.z[g]);
+                q[r] = SinkDS{-x.hi, -y.hi, -z.hi, -x.lo, -y.lo, -z.lo};
+                nmi[r] = -(float)P.m[g];
+            }
         }
-        float acc[3] = {0.f, 0.f, 0.f}, cmp[3] = {0.f, 0.f, 0.f};
+        float acc[R][3], cmp[R][3];
+#pragma unroll
+        for (int r = 0; r < R; r++)
+#pragma unroll
+            for (int k = 0; k < 3; k++) acc[r][k] = cmp[r][k] = 0.0f;
         for (int a = j0; a < j1; a += kTX) {
             const int b = min(j1, a + kTX), len = b - a;
             tc_use(E, PA, PB, a, b, cb, tc, sm);
             const float4* TA = sm.u.kc.A[cb];
             const float4* TB = sm.u.kc.B[cb];
-            float bl[3] = {0.f, 0.f, 0.f};
+            float bl[R][3];
+#pragma unroll
+            for (int r = 0; r < R; r++) bl[r][0] = bl[r][1] = bl[r][2] = 0.0f;
             int nb = 0;
             for (int g8 = 0; g8 < len; g8 += 8) {
                 float v[8][3];
 #pragma unroll
                 for (int c = 0; c < 8; c++) {
                     const float4 A = TA[g8 + c], B = TB[g8 + c];
-                    float wx, wy, wz;
-                    pair_w(A, B, q, eps2, wx, wy, wz);
-                    bl[0] = fmaf(wx, A.w, bl[0]);
-                    bl[1] = fmaf(wy, A.w, bl[1]);
-                    bl[2] = fmaf(wz, A.w, bl[2]);
-                    v[c][0] = __fmul_rn(wx, nmi);
-                    v[c][1] = __fmul_rn(wy, nmi);
-                    v[c][2] = __fmul_rn(wz, nmi);
+#pragma unroll
+                    for (int r = 0; r < R; r++) {
+                        float wx, wy, wz;
+                        pair_w(A, B, q[r], eps2, wx, wy, wz);
+                        bl[r][0] = fmaf(wx, A.w, bl[r][0]);
+                        bl[r][1] = fmaf(wy, A.w, bl[r][1]);
+                        bl[r][2] = fmaf(wz, A.w, bl[r][2]);
+                        if (r == 0) {
+                            v[c][0] = __fmul_rn(wx, nmi[r]);
+                            v[c][1] = __fmul_rn(wy, nmi[r]);
+                            v[c][2] = __fmul_rn(wz, nmi[r]);
+                        } else {
+                            v[c][0] = fmaf(wx, nmi[r], v[c][0]);
+                            v[c][1] = fmaf(wy, nmi[r], v[c][1]);
+                            v[c][2] = fmaf(wz, nmi[r], v[c][2]);
+                        }
+                    }
                 }
-                float r[3];
-                warp_colsum8(v, r, lane);
+                float rs[3];
+                warp_colsum8(v, rs, lane);
                 const int col = ((lane >> 2) & 7);
                 if ((lane & 3) == 0 && g8 + col < len) {
-                    sm.u.kc.colw[warp][g8 + col][0] = r[0];
-                    sm.u.kc.colw[warp][g8 + col][1] = r[1];
-                    sm.u.kc.colw[warp][g8 + col][2] = r[2];
+                    sm.u.kc.colw[warp][g8 + col][0] = rs[0];
+                    sm.u.kc.colw[warp][g8 + col][1] = rs[1];
+                    sm.u.kc.colw[warp][g8 + col][2] = rs[2];
                 }
                 if (++nb == 4) {  // 32 pairs: into the compensated row sums
 #pragma unroll
-                    for (int k = 0; k < 3; k++) {
-                        kahan_add(acc[k], cmp[k], bl[k]);
-                        bl[k] = 0.0f;
-                    }
+                    for (int r = 0; r < R; r++)
+#pragma unroll
+                        for (int k = 0; k < 3; k++) {
+                            kahan_add(acc[r][k], cmp[r][k], bl[r][k]);
+                            bl[r][k] = 0.0f;
+                        }
                     nb = 0;
                 }
             }
             if (nb) {
 #pragma unroll
-                for (int k = 0; k < 3; k++) kahan_add(acc[k], cmp[k], bl[k]);
+                for (int r = 0; r < R; r++)
+#pragma unroll
+                    for (int k = 0; k < 3; k++) kahan_add(acc[r][k], cmp[r][k], bl[r][k]);
             }
             __syncthreads();
             // the tile's column sums: the CTA's warps in order, then the super-block's rows
@@ -1284,10 +1311,13 @@ __device__ void kick_cross_unit(const EParams& E, const int32_t* F, int nf, int 
             }
             __syncthreads();  // colw is rewritten by the next pass
         }
-        if (act)
 #pragma unroll
-            for (int k = 0; k < 3; k++)
-                E.k_part[(size_t)(jc * 3 + k) * nmx + s] = (double)acc[k] - (double)cmp[k];
+        for (int r = 0; r < R; r++)
+            if (s[r] < nf)
+#pragma unroll
+                for (int k = 0; k < 3; k++)
+                    E.k_part[(size_t)(jc * 3 + k) * nmx + s[r]] =
+                        (double)acc[r][k] - (double)cmp[r][k];
     }
 }
 
