@@ -307,7 +307,6 @@ def run_ours(a, rank, world, torch, dist):
             step()
         ctx.check(sh)
         ctx.reset_stats(sh)
-        ctx.set_profiling(True)
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                for _ in range(a.steps)]
         clocks = ClockSampler(dev)
@@ -328,20 +327,33 @@ def run_ours(a, rank, world, torch, dist):
         clk = clocks.stop()
         ctx.check(sh)
         t_ms = sum(e0_.elapsed_time(e1_) for e0_, e1_ in evs)
-        prof = ctx.profile()
+        stats = ctx.stats(sh)
+        out = sys_.download(stream=sh)
+        torch.cuda.synchronize()
+        # the phase profile (timer reads at every phase boundary) from separate steps after
+        # the timed ones, so that it does not weigh on the timed region
+        ctx.reset_stats(sh)
+        ctx.set_profiling(True)
+        prof_steps = min(a.steps, 5)
+        for _ in range(prof_steps):
+            step()
+        torch.cuda.synchronize()
+        ctx.check(sh)
+        prof = {k: dict(v, launches=v["launches"] * a.steps // prof_steps,
+                        ms=v["ms"] * a.steps / prof_steps,
+                        pairs=v["pairs"] * a.steps / prof_steps)
+                for k, v in ctx.profile().items()}
         if a.profile_out and a.schedule == "auto":
             lms, lcnt = ctx.level_profile()
             kinds = ["timesteps", "kick", "split", "update", "engine", "subtree", "cluster_node",
                      "subtree_stages"]
-            lp = {kinds[k]: {str(l): [round(float(lms[k, l]) / a.steps, 4), int(lcnt[k, l]) // a.steps]
+            lp = {kinds[k]: {str(l): [round(float(lms[k, l]) / prof_steps, 4),
+                                      int(lcnt[k, l]) // prof_steps]
                              for l in range(64) if lcnt[k, l]} for k in range(8)}
             with open(a.profile_out, "w") as f:
                 json.dump({"per_step_ms_and_phases_by_level": lp, "tuning": ctx.tuning()}, f,
                           indent=1)
         ctx.set_profiling(False)
-        stats = ctx.stats(sh)
-        out = sys_.download(stream=sh)
-        torch.cuda.synchronize()
     e1 = hhs.energy_host(out)
 
     t_max = max_over_ranks(t_ms, dist, torch)
@@ -784,6 +796,7 @@ def run_side_measurements(a, torch, res):
       compaction, checked bit for bit against the reference's own scan on the same GPU;
     - config 1 (N=1024 FP64 to t=1, bit for bit against the CPU oracle), config 3
       (N=65536 Salpeter) and config 5 (N=262144 90/10 masses) step rates;
+    - config 3 through the multi-GPU step (hhs.DistHold) on a one-rank NCCL group;
     - the batched workload (512 clusters, N log-uniform in [64, 4096]): cluster steps/s,
       and the per-cluster energy errors at t=0.5 in mixed precision and FP64."""
     out = {}
@@ -817,6 +830,12 @@ def run_side_measurements(a, torch, res):
     out["deep_65536"] = time_engine(torch, 65536, 0.02, 1, a.dt, 3, 1)
     out["deep_65536"]["workload"] = ("Plummer N=65536 Salpeter masses, eta=0.02, mixed "
                                      "(config 3)")
+    dist = time_dist(torch, 65536, 0.02, 1, a.dt, 3, 1)
+    if dist is not None:
+        dist["vs_device_step"] = dist["s_per_step"] / out["deep_65536"]["s_per_step"]
+        dist["workload"] = ("config 3 through hhs.DistHold on a one-rank NCCL group, against "
+                            "deep_65536 (the device-resident step)")
+        out["dist_65536"] = dist
     out["large_262144"] = time_engine(torch, 262144, 0.02, 2, a.dt, 2, 1)
     out["large_262144"]["workload"] = ("Plummer N=262144 90/10 masses, eta=0.02, mixed "
                                        "(config 5)")
@@ -861,6 +880,51 @@ def time_engine(torch, n, eta, mass, dt, steps, warmup, seed=2024):
             "warmup": warmup, "pair_interactions_per_s": (st["kick_pairs"] + st["ts_pairs"]) / sec,
             "kick_pairs_per_step": st["kick_pairs"] / steps, "nodes_per_step": st["nodes"] / steps,
             "max_level": st["max_level"]}
+
+
+def time_dist(torch, n, eta, mass, dt, steps, warmup, seed=2024):
+    """The multi-GPU step (hhs.DistHold: timestep and kick launches split by sink, every
+    result stored into each replica by the kernels, host barriers between launches) on a
+    one-rank NCCL group, timed with CUDA events on the library's stream like the device
+    step. With one rank every launch is a whole level, so the gap to the device step is the
+    cost of the host-driven schedule and its barriers."""
+    import datetime
+    import socket
+    import torch.distributed as tdist
+    import hhs
+    if tdist.is_available() and tdist.is_initialized():
+        return None
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    tdist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0,
+                             world_size=1, timeout=datetime.timedelta(seconds=120))
+    try:
+        s = hhs.plummer(n, seed, mass)
+        ctx = hhs.Context(n, 64, eta=eta)
+        d = hhs.ParticleSystem(n)
+        d.upload(s)
+        dh = hhs.DistHold(ctx, d)
+        st = torch.cuda.default_stream()
+        for _ in range(warmup):
+            dh.step(n, dt, True, hhs.PREC_MIXED)
+        torch.cuda.synchronize()
+        ctx.check()
+        ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        ev[0].record(st)
+        for _ in range(steps):
+            dh.step(n, dt, True, hhs.PREC_MIXED)
+        ev[1].record(st)
+        torch.cuda.synchronize()
+        ctx.check()
+        sec = ev[0].elapsed_time(ev[1]) * 1e-3
+        dh.close()
+        ctx.destroy()
+        d.free()
+    finally:
+        tdist.destroy_process_group()
+    return {"s_per_step": sec / steps, "steps": steps, "warmup": warmup, "ranks": 1,
+            "backend": "nccl", "min_pairs": 1 << 24}
 
 
 def run_batched_accuracy(a, torch, t_end=0.5):

@@ -50,7 +50,6 @@ constexpr int kTS = 1024;         // source records per shared-memory tile of th
 constexpr int kTX = 256;          // slow records per tile of the symmetric grid kick
 constexpr int kTW = 256;          // widest column tile of the packed grid timestep
 constexpr int kMaxFsb = 64;       // fast super-blocks of that kick (column-partial slots)
-constexpr int kXRows = 2;         // fast sinks per thread in that kick's cross units
 constexpr int kMaxChunks = 32;    // source chunks per node (partial-sum slots)
 constexpr int kMaxLevels = 64;    // per-level state is kept in 64-bit masks
 constexpr unsigned long long kBarrierTimeoutNs = 60ull * 1000000000ull;
@@ -138,6 +137,23 @@ struct __align__(16) MidState {
     int total, total2;
 };
 
+// fast sets of at least kX2Min sinks take two sinks per thread in the cross units; slow
+// sets of at least kSymMin evaluate each slow-slow pair once for both particles (below
+// that, the units would be too few and the column sums of one-row passes cost more than
+// the halved pair count saves)
+constexpr int kX2Min = 8192;
+constexpr int kSymMin = 12288;
+static_assert(kSymMin > kMaxChunks * kEB, "symmetric slow chunks are whole two-row passes");
+
+struct KickPlan {
+    int R;               // fast sinks per thread in the cross units (1 or 2)
+    int ncs, Cs;         // slow chunks: ncs chunks of Cs slow particles (the partial-sum slots)
+    int nsub, FB, nfsb;  // fast sub-blocks of R*kEB sinks; FB of them per super-block
+    int nsb;             // blocks of kEB slow sinks
+    int sym, Rs, noff;   // symmetric slow-slow units: Rs sinks per thread, noff chunk pairs
+    int nx, nsl;         // cross units (nfsb x ncs) and slow units
+};
+
 struct __align__(16) Smem {
     float colred[kEB / 32][64];
     unsigned long long prof_ns[8][kMaxLevels];  // phase times of this launch (CTA 0)
@@ -155,6 +171,8 @@ struct __align__(16) Smem {
     unsigned tphase;              // parities of the next phases of tbar[0], tbar[1]
     __align__(8) uint64_t kbar;   // completion barrier of the kick's source-tile copies
     __align__(8) uint64_t tbar[2];  // completion barriers of the timestep's column tiles
+    KickPlan kp;                  // unit layout of the running kick (read from shared memory
+                                  // after every unit, so it holds no registers meanwhile)
     // last, so that the persistent kernel's dynamic allocation can extend it to a MidState
     union {
         struct { float4 A[kEB], B[kEB], V[kEB]; } tsm;         // mixed timestep tiles
@@ -1093,29 +1111,53 @@ __device__ void kick_units_grid(const EParams& E, const int32_t* F, int nf, int 
 //  - slow units (block of kEB slow sinks, slow chunk): the slow-slow pairs, per sink.
 // The reduce phase adds, per sink, its chunk partials in order and (slow sinks) its
 // super-block partials in order: every sum has a fixed order, so a step is deterministic.
-struct KickPlan {
-    int ncs, Cs;         // slow chunks: ncs chunks of Cs slow particles
-    int nsub, FB, nfsb;  // fast sub-blocks of kXRows*kEB sinks; FB of them per super-block
-    int nsb;             // blocks of kEB slow sinks
-    int nx, nsl;         // cross units (nfsb x ncs) and slow units (nsb x ncs)
-};
-
+// Unit layout of the mixed grid kick of a node with nf fast and ns slow particles.
+// Cross units (fast super-block, slow chunk) evaluate each fast-slow pair once for both
+// particles. Slow units are either (sym) the chunk pairs a < b, each evaluating the pairs
+// of chunk a x chunk b once for both particles, followed by one unit per block of kEB
+// slow sinks against its own chunk; or (small slow sets, where those units would be too
+// coarse to spread over the grid) blocks of kEB slow sinks x chunks, one direction only.
+// Either way every slow particle receives exactly one partial per chunk slot.
 __device__ __forceinline__ KickPlan kick_plan(int nf, int ns, int workers) {
     KickPlan p;
-    p.nsub = (nf + kXRows * kEB - 1) / (kXRows * kEB);
+    p.R = nf >= kX2Min ? 2 : 1;
+    p.nsub = (nf + p.R * kEB - 1) / (p.R * kEB);
     const int f = p.nsub < kMaxFsb ? p.nsub : kMaxFsb;
     p.FB = f > 0 ? (p.nsub + f - 1) / f : 1;
     p.nfsb = (p.nsub + p.FB - 1) / p.FB;
     p.nsb = (ns + kEB - 1) / kEB;
-    const int per = p.nfsb + p.nsb;  // units per chunk
-    int c = (3 * workers + per - 1) / per;  // about three units per CTA
-    const int cmax = min(kMaxChunks, (ns + 31) / 32);  // at least 32 slow particles a chunk
-    c = c < 1 ? 1 : (c > cmax ? cmax : c);
-    p.Cs = (ns + c - 1) / c;
-    p.ncs = (ns + p.Cs - 1) / p.Cs;
+    p.sym = ns >= kSymMin;
+    if (p.sym) {
+        // chunks of whole two-row passes, at most kMaxChunks of them
+        p.Rs = 2;
+        const int rb = p.Rs * kEB, span = kMaxChunks * rb;
+        p.Cs = rb * ((ns + span - 1) / span);
+        p.ncs = (ns + p.Cs - 1) / p.Cs;
+        p.noff = p.ncs * (p.ncs - 1) / 2;
+        p.nsl = p.noff + p.nsb;
+    } else {
+        const int per = p.nfsb + p.nsb;  // units per chunk
+        int c = (3 * workers + per - 1) / per;  // about three units per CTA
+        const int cmax = min(kMaxChunks, (ns + 31) / 32);  // at least 32 slow particles a chunk
+        c = c < 1 ? 1 : (c > cmax ? cmax : c);
+        p.Cs = (ns + c - 1) / c;
+        p.ncs = (ns + p.Cs - 1) / p.Cs;
+        p.Rs = 1;
+        p.noff = 0;
+        p.nsl = p.nsb * p.ncs;
+    }
     p.nx = p.nfsb * p.ncs;
-    p.nsl = p.nsb * p.ncs;
     return p;
+}
+
+// chunk pair (a, b), a < b, of symmetric slow unit v (row-major over the upper triangle)
+__device__ __forceinline__ void sym_pair_of(int v, int G, int& a, int& b) {
+    a = 0;
+    while (v >= G - 1 - a) {
+        v -= G - 1 - a;
+        a++;
+    }
+    b = a + 1 + v;
 }
 
 // Column sums over the warp of eight columns (three components each): lane l ends with
@@ -1206,34 +1248,42 @@ __device__ __forceinline__ void pair_w(const float4 A, const float4 B, const Sin
     wz = __fmul_rn(dz, r3);
 }
 
-// kXRows fast sinks per thread: the column sums' butterfly then serves kXRows rows at once
-__device__ void kick_cross_unit(const EParams& E, const int32_t* F, int nf, int lvl,
-                                const KickPlan& p, int fsb, int jc, int ns, Smem& sm,
-                                TileCache& tc, int cb) {
-    constexpr int R = kXRows;
+// Pair terms of rows [r0, r1) (sinks: the fast list, or the level's packed slow records)
+// against the packed slow records [j0, j1) (columns), each pair evaluated once for both
+// particles. R sinks per thread, so one column butterfly serves R rows. Row partials (the
+// rows' accelerations from these columns) go to rout[k * nmx + row]; column partials (the
+// columns' accelerations from these rows) to cout[k * nmx + j], summed over the row passes
+// in order (the first pass stores).
+template <int R>
+__device__ void kick_pair_block(const EParams& E, const int32_t* F, bool rows_fast, int r0,
+                                int r1, int j0, int j1, int lvl, double* rout, double* cout,
+                                Smem& sm, TileCache& tc, int cb) {
     const SoA& P = E.P;
     const size_t nmx = E.n_max;
     const float4* PA = E.pk_a + (size_t)lvl * nmx;
     const float4* PB = E.pk_b + (size_t)lvl * nmx;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int j0 = jc * p.Cs, j1 = min(ns, j0 + p.Cs);
-    double* cp = E.c_part + (size_t)fsb * 3 * nmx + nf;  // slow sink q at cp[k * nmx + q]
     const float eps2 = E.eps2f;
-    const int sb0 = fsb * p.FB, sb1 = min(p.nsub, sb0 + p.FB);
-    for (int sb = sb0; sb < sb1; sb++) {
+    for (int rp = r0; rp < r1; rp += R * kEB) {
         int s[R];
         SinkDS q[R];
         float nmi[R];  // -m_i: the column terms
 #pragma unroll
         for (int r = 0; r < R; r++) {
-            s[r] = sb * (R * kEB) + r * kEB + (int)threadIdx.x;
+            s[r] = rp + r * kEB + (int)threadIdx.x;
             q[r] = SinkDS{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             nmi[r] = 0.0f;
-            if (s[r] < nf) {
-                const int g = F[s[r]];
-                const DS x = ds_split(P.x[g]), y = ds_split(P.y[g]), z = ds_split(P.z[g]);
-                q[r] = SinkDS{-x.hi, -y.hi, -z.hi, -x.lo, -y.lo, -z.lo};
-                nmi[r] = -(float)P.m[g];
+            if (s[r] < r1) {
+                if (rows_fast) {
+                    const int g = F[s[r]];
+                    const DS x = ds_split(P.x[g]), y = ds_split(P.y[g]), z = ds_split(P.z[g]);
+                    q[r] = SinkDS{-x.hi, -y.hi, -z.hi, -x.lo, -y.lo, -z.lo};
+                    nmi[r] = -(float)P.m[g];
+                } else {
+                    const float4 a = PA[s[r]], b = PB[s[r]];
+                    q[r] = SinkDS{-a.x, -a.y, -a.z, -b.x, -b.y, -b.z};
+                    nmi[r] = -a.w;
+                }
             }
         }
         float acc[R][3], cmp[R][3];
@@ -1281,7 +1331,7 @@ __device__ void kick_cross_unit(const EParams& E, const int32_t* F, int nf, int 
                     sm.u.kc.colw[warp][g8 + col][1] = rs[1];
                     sm.u.kc.colw[warp][g8 + col][2] = rs[2];
                 }
-                if (++nb == 4) {  // 32 pairs: into the compensated row sums
+                if (++nb == 4) {  // 32 pairs a row: into the compensated sums
 #pragma unroll
                     for (int r = 0; r < R; r++)
 #pragma unroll
@@ -1299,25 +1349,23 @@ __device__ void kick_cross_unit(const EParams& E, const int32_t* F, int nf, int 
                     for (int k = 0; k < 3; k++) kahan_add(acc[r][k], cmp[r][k], bl[r][k]);
             }
             __syncthreads();
-            // the tile's column sums: the CTA's warps in order, then the super-block's rows
-            // in order (first sub-block stores, later ones add)
+            // the tile's column sums: the CTA's warps in order, then the row passes in order
             for (int t = threadIdx.x; t < 3 * len; t += kEB) {
                 const int jl = t / 3, k = t - 3 * jl;
                 double sum = 0.0;
 #pragma unroll
                 for (int w = 0; w < kEB / 32; w++) sum += (double)sm.u.kc.colw[w][jl][k];
-                double* o = cp + (size_t)k * nmx + a + jl;
-                *o = sb == sb0 ? sum : *o + sum;
+                double* o = cout + (size_t)k * nmx + a + jl;
+                *o = rp == r0 ? sum : *o + sum;
             }
             __syncthreads();  // colw is rewritten by the next pass
         }
 #pragma unroll
         for (int r = 0; r < R; r++)
-            if (s[r] < nf)
+            if (s[r] < r1)
 #pragma unroll
                 for (int k = 0; k < 3; k++)
-                    E.k_part[(size_t)(jc * 3 + k) * nmx + s[r]] =
-                        (double)acc[r][k] - (double)cmp[r][k];
+                    rout[(size_t)k * nmx + s[r]] = (double)acc[r][k] - (double)cmp[r][k];
     }
 }
 
@@ -1361,16 +1409,27 @@ __device__ void kick_slow_unit(const EParams& E, int nf, int lvl, const KickPlan
 // kinds 0 = cross units then slow units, 1 = slow units only, 2 = cross units only.
 // While a unit computes, thread 0 already takes the next unit and starts the copy of its
 // first tile into the other buffer.
+__device__ __forceinline__ int unit_chunk(const KickPlan& p, int nx, int u) {
+    if (u < nx) return u / p.nfsb;
+    const int v = u - nx;
+    if (!p.sym) return v / p.nsb;
+    if (v >= p.noff) return (v - p.noff) * kEB / p.Cs;  // a block of slow sinks: its own chunk
+    int a, b;
+    sym_pair_of(v, p.ncs, a, b);
+    return b;
+}
+
 __device__ __forceinline__ void unit_first_tile(const KickPlan& p, int nx, int u, int& a, int& b) {
-    const int jc = u < nx ? u / p.nfsb : (u - nx) / p.nsb;
-    a = jc * p.Cs;
+    a = unit_chunk(p, nx, u) * p.Cs;
     b = a + min(p.Cs, kTX);
 }
 
 __device__ void kick_sym_units(const EParams& E, const int32_t* F, int nf, int ns, int lvl,
-                               const KickPlan& p, int set, int kinds, Smem& sm) {
-    const int nx = kinds == 1 ? 0 : p.nx;
-    const int total = nx + (kinds == 2 ? 0 : p.nsl);
+                               const KickPlan& plan, int set, int kinds, Smem& sm) {
+    const int nx = kinds == 1 ? 0 : plan.nx;
+    const int total = nx + (kinds == 2 ? 0 : plan.nsl);
+    if (threadIdx.x == 0) sm.kp = plan;  // read back after each barrier below
+    const KickPlan& p = sm.kp;
     const float4* PA = E.pk_a + (size_t)lvl * E.n_max;
     const float4* PB = E.pk_b + (size_t)lvl * E.n_max;
     unsigned* ctr = &E.st->kick_ctr[set][lvl];
@@ -1402,11 +1461,44 @@ __device__ void kick_sym_units(const EParams& E, const int32_t* F, int nf, int n
                 if (tc.a[c ^ 1] != a || tc.b[c ^ 1] != b) tc_issue(PA, PB, a, b, c ^ 1, sm);
             }
         }
-        if (u < nx) {
-            kick_cross_unit(E, F, nf, lvl, p, u % p.nfsb, u / p.nfsb, ns, sm, tc, c);
-        } else {
+        // one call site per kind of block keeps the inlined pair loops to three copies
+        {
+            const size_t nmx = E.n_max;
+            int kind = 0, r0 = 0, r1 = 0, j0 = 0, j1 = 0, sb = 0, jc = 0;
+            double *rout = nullptr, *cout = nullptr;
             const int v = u - nx;
-            kick_slow_unit(E, nf, lvl, p, v % p.nsb, v / p.nsb, ns, sm, tc, c);
+            if (u < nx) {  // cross unit: fast super-block fsb x slow chunk jc
+                const int fsb = u % p.nfsb, rb = p.R * kEB;
+                jc = u / p.nfsb;
+                kind = p.R == 2 ? 2 : 1;
+                r0 = fsb * p.FB * rb;
+                r1 = min(nf, r0 + p.FB * rb);
+                rout = E.k_part + (size_t)jc * 3 * nmx;
+                cout = E.c_part + (size_t)fsb * 3 * nmx + nf;
+            } else if (p.sym && v < p.noff) {  // slow chunk a x slow chunk b > a
+                int a, b;
+                sym_pair_of(v, p.ncs, a, b);
+                kind = 3;
+                r0 = a * p.Cs;
+                r1 = min(ns, r0 + p.Cs);
+                jc = b;
+                rout = E.k_part + (size_t)b * 3 * nmx + nf;
+                cout = E.k_part + (size_t)a * 3 * nmx + nf;
+            } else if (p.sym) {  // a block of slow sinks against its own chunk
+                sb = v - p.noff;
+                jc = sb * kEB / p.Cs;
+            } else {
+                sb = v % p.nsb;
+                jc = v / p.nsb;
+            }
+            j0 = jc * p.Cs;
+            j1 = min(ns, j0 + p.Cs);
+            if (kind >= 2)
+                kick_pair_block<2>(E, F, kind == 2, r0, r1, j0, j1, lvl, rout, cout, sm, tc, c);
+            else if (kind == 1)
+                kick_pair_block<1>(E, F, true, r0, r1, j0, j1, lvl, rout, cout, sm, tc, c);
+            else
+                kick_slow_unit(E, nf, lvl, p, sb, jc, ns, sm, tc, c);
         }
         __syncthreads();  // the unit is done; sm.bcast holds the next one
         const int un = sm.bcast;
@@ -2309,6 +2401,20 @@ __device__ __forceinline__ void acc_over(const EParams& E, const MidState& M, co
 
 }  // namespace mid
 
+// Fine-grained timing inside the cluster subtree solver (profiling only; CTA 0, thread 0):
+// kind 7 of the level table, slots 56 load, 57 timesteps, 58 split, 59 kick, 60 warp
+// subtrees (of which 62 their timesteps, 63 their kicks and drifts), 61 write-back.
+__device__ __forceinline__ void mid_mark(const EParams& E, Smem& sm, unsigned long long& t,
+                                         int slot) {
+    if (!E.profile || blockIdx.x != 0 || threadIdx.x != 0) return;
+    const unsigned long long now = gtimer();
+    if (slot >= 0) {
+        sm.prof_ns[7][slot] += now - t;
+        sm.prof_cnt[7][slot] += 1;
+    }
+    t = now;
+}
+
 // Warp solver for a node of at most 32 members with its whole subtree (every node below
 // it is smaller): warp 0 of the CTA, one member per lane, warp barriers only. Lanes are
 // members in increasing slot order (the stable order); the state stays in the MidState
@@ -2317,8 +2423,9 @@ template <int PREC>
 __device__ void warp_subtree(const EParams& E, MidState& M, const unsigned* memw, int nw,
                              int cnt, int level0, bool calc0, unsigned long long& nodes,
                              int& maxl, double& kpairs, double& tpairs, double& leaf,
-                             bool& ok, bool rec) {
+                             bool& ok, bool rec, Smem& sm) {
     const int lane = threadIdx.x & 31;
+    unsigned long long tw = 0;
     // lane l takes the l-th member
     {
         const int c = lane < nw ? __popc(memw[lane]) : 0;
@@ -2349,6 +2456,7 @@ __device__ void warp_subtree(const EParams& E, MidState& M, const unsigned* memw
             }
             const int n_here = __popc(mk);
             if (calcm & bit) {
+                mid_mark(E, sm, tw, -1);
                 if (in) {
                     const unsigned srcs = mk & ~(1u << lane);
                     if (PREC == HHS_PREC_FP64) {
@@ -2397,6 +2505,7 @@ __device__ void warp_subtree(const EParams& E, MidState& M, const unsigned* memw
                 }
                 __syncwarp();
                 if (lane == 0) tpairs += (double)n_here * (double)(n_here - 1);
+                mid_mark(E, sm, tw, 62);
             }
             unsigned F = __ballot_sync(HHS_FULL_MASK, in && M.ts[me] <= dt);
             int lone = -1;
@@ -2431,6 +2540,7 @@ __device__ void warp_subtree(const EParams& E, MidState& M, const unsigned* memw
             const bool is_slow = (L >> lane) & 1u, is_fast = (F >> lane) & 1u;
             const double h = dt * 0.5;
             if (L) {
+                mid_mark(E, sm, tw, -1);
                 // first half drift of the slow lanes (src/hold.cuh:123-124)
                 if (is_slow) {
                     if (PREC == HHS_PREC_FP64) {
@@ -2538,6 +2648,7 @@ __device__ void warp_subtree(const EParams& E, MidState& M, const unsigned* memw
                     }
                 }
                 __syncwarp();
+                mid_mark(E, sm, tw, 63);
             }
             after2 |= bit;
             if (F) {
@@ -2555,20 +2666,6 @@ __device__ void warp_subtree(const EParams& E, MidState& M, const unsigned* memw
 
 // cs, rank: the hardware cluster that runs the subtree (every CTA of it calls mid_hold),
 // or cs = 1 for one CTA alone whatever cluster it belongs to.
-// Fine-grained timing inside the cluster subtree solver (profiling only; CTA 0, thread 0):
-// kind 7 of the level table, slots 56 load, 57 timesteps, 58 split, 59 kick, 60 warp
-// subtrees, 61 write-back.
-__device__ __forceinline__ void mid_mark(const EParams& E, Smem& sm, unsigned long long& t,
-                                         int slot) {
-    if (!E.profile || blockIdx.x != 0 || threadIdx.x != 0) return;
-    const unsigned long long now = gtimer();
-    if (slot >= 0) {
-        sm.prof_ns[7][slot] += now - t;
-        sm.prof_cnt[7][slot] += 1;
-    }
-    t = now;
-}
-
 template <int PREC>
 __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, bool calc0,
                          int dist_n, int cs, int rank, Smem& sm) {
@@ -2616,7 +2713,7 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
                 mid_mark(E, sm, tm, -1);
                 if (warp == 0)
                     warp_subtree<PREC>(E, M, memw, nw, M.nmem[d], lvl, (calcm & bit) != 0,
-                                       nodes, maxl, kpairs, tpairs, leaf, ok, rank == 0);
+                                       nodes, maxl, kpairs, tpairs, leaf, ok, rank == 0, sm);
                 __syncthreads();
                 mid_mark(E, sm, tm, 60);
                 calcm &= ~bit; after1 &= ~bit; after2 &= ~bit;

@@ -156,13 +156,15 @@ def _sum_of_magnitudes(s, eps, src=None, rows=None, block=512):
     return out
 
 
-@pytest.mark.parametrize("n,eps", [(4096, 0.0), (16384, 0.0), (3000, 0.01)])
+@pytest.mark.parametrize("n,eps", [(4096, 0.0), (16384, 0.0), (24576, 0.0), (3000, 0.01)])
 def test_engine_mixed_kick_accelerations_against_oracle(cuda, hhs, oracle, n, eps):
     """The kick phase of the device step in mixed precision (bulk-copied slow tiles, each
-    fast-slow pair evaluated once for both particles, FP32 pair terms with a
-    Newton-corrected 1/d^3, compensated row sums and tree-ordered column sums) on a split
-    node -- fast set every third particle -- against the FP64 direct sums of the oracle
-    over the same sets."""
+    fast-slow pair -- and, for slow sets of 2048 or more, each slow-slow pair -- evaluated
+    once for both particles, FP32 pair terms with a Newton-corrected 1/d^3, compensated row
+    sums and tree-ordered column sums) on a split node -- fast set every third particle --
+    against the FP64 direct sums of the oracle over the same sets. The sizes cover one and
+    two fast sinks per thread (fast sets below / from 8192), slow chunks of one and two
+    row passes, and (n=3000) the one-directional slow units of small slow sets."""
     torch = cuda
     s = hhs.plummer(n, 77 + n)
     ctx = hhs.Context(n, 64, eta=0.03, eps=eps)
