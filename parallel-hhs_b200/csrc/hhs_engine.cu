@@ -26,6 +26,7 @@
 // (src/split.cuh:341-356, src/update_system.cuh:14-23): particle data stays in the
 // caller's SoA arrays and every level works on global indices.
 #include <cooperative_groups.h>
+#include <type_traits>
 
 #include <algorithm>
 #include <cstddef>
@@ -217,6 +218,12 @@ __device__ __forceinline__ void trace_node(const EParams& E, int level, int n, i
     if (!E.trace) return;
     const unsigned long long k = atomicAdd(E.trace_count, 1ull);
     if ((long long)k < E.trace_cap) E.trace[k] = make_int4(level, n, nf, calc ? 1 : 0);
+}
+
+// E.dt_top * 2^-lvl, exact (the same double as ldexp(E.dt_top, -lvl) for the levels
+// kept, which stay far from the subnormal range)
+__device__ __forceinline__ double dt_at(const EParams& E, int lvl) {
+    return __dmul_rn(E.dt_top, __longlong_as_double((long long)(1023 - lvl) << 52));
 }
 
 __device__ __forceinline__ int ld_volatile_i32(const int32_t* p) {
@@ -694,24 +701,35 @@ __device__ void ts_sym_tiles(const EParams& E, int n, int cw, long long u0, long
         const float4* TA = sm.u.ts2.A[buf];
         const float4* TB = sm.u.ts2.B[buf];
         const float4* TV = sm.u.ts2.V[buf];
-        for (int g = 0; g < ncol; g += 32) {
-            const int nc = min(32, ncol - g);
-            unsigned colmax = 0u;
+        // pairs need a mask only in the tiles that cross the diagonal (j > i) or hold rows
+        // past the end
+        const int diag_end = (rb + 1) * kEB;  // columns from here see every row as j > i
+        const int mask = c0 < diag_end ? 2 : (diag_end > n ? 1 : 0);
+        auto cols = [&](auto MASK) {
+            constexpr int M = decltype(MASK)::value;
+            for (int g = 0; g < ncol; g += 32) {
+                const int nc = min(32, ncol - g);
+                unsigned colmax = 0u;
 #pragma unroll 8
-            for (int c = 0; c < nc; c++) {
-                const int jl = g + c;
-                const float4 A = TA[jl], B = TB[jl], V = TV[jl];
-                const float rate = ts_pair_rate_mixed(
-                    ds_diff(xi.hi, xi.lo, A.x, B.x), ds_diff(yi.hi, yi.lo, A.y, B.y),
-                    ds_diff(zi.hi, zi.lo, A.z, B.z), vxi - V.x, vyi - V.y, vzi - V.z, mi + A.w,
-                    E.inv_eta_s2, E.inv_eta);
-                const float r = (act && c0 + jl > i) ? rate : 0.0f;
-                rowmax = fmaxf(rowmax, r);
-                const unsigned cm = __reduce_max_sync(HHS_FULL_MASK, __float_as_uint(r));
-                colmax = lane == c ? cm : colmax;
+                for (int c = 0; c < nc; c++) {
+                    const int jl = g + c;
+                    const float4 A = TA[jl], B = TB[jl], V = TV[jl];
+                    const float rate = ts_pair_rate_mixed(
+                        ds_diff(xi.hi, xi.lo, A.x, B.x), ds_diff(yi.hi, yi.lo, A.y, B.y),
+                        ds_diff(zi.hi, zi.lo, A.z, B.z), vxi - V.x, vyi - V.y, vzi - V.z,
+                        mi + A.w, E.inv_eta_s2, E.inv_eta);
+                    const float r = M == 2 ? ((act && c0 + jl > i) ? rate : 0.0f)
+                                           : (M == 1 ? (act ? rate : 0.0f) : rate);
+                    rowmax = fmaxf(rowmax, r);
+                    const unsigned cm = __reduce_max_sync(HHS_FULL_MASK, __float_as_uint(r));
+                    colmax = lane == c ? cm : colmax;
+                }
+                sm.u.ts2.colred[buf][warp][g + lane] = __uint_as_float(colmax);
             }
-            sm.u.ts2.colred[buf][warp][g + lane] = __uint_as_float(colmax);
-        }
+        };
+        if (mask == 0) cols(std::integral_constant<int, 0>{});
+        else if (mask == 1) cols(std::integral_constant<int, 1>{});
+        else cols(std::integral_constant<int, 2>{});
         __syncthreads();  // this buffer's columns are read, colred[buf] is complete
         if ((int)threadIdx.x < ncol) {
             float cm = 0.0f;
@@ -1937,7 +1955,7 @@ __device__ void tiny_hold(const EParams& E, const int32_t* S, int n, int level0,
         const unsigned long long bit = 1ull << d;
         const unsigned mask = d == 0 ? top_mask : sm.wfast[d - 1];
         const bool in = (mask >> lane) & 1u;
-        const double dt = ldexp(E.dt_top, -lvl);
+        const double dt = dt_at(E, lvl);
         if (!(after1 & bit)) {
             if (lvl >= E.max_levels || lvl >= kMaxLevels - 1) {
                 if (threadIdx.x == 0) atomicOr(E.err, HHS_ERRBIT_DEPTH);
@@ -2428,13 +2446,16 @@ __device__ void warp_subtree(const EParams& E, MidState& M, const unsigned* memw
     unsigned long long tw = 0;
     // lane l takes the l-th member
     {
+        // member slot w * 32 + l (bit l of word w) is the k-th member, k = the members in
+        // the words before w plus the set bits below l
         const int c = lane < nw ? __popc(memw[lane]) : 0;
         const int base = warp_incl_scan(c, lane) - c;
         for (int w = 0; w < nw; w++) {
+            const unsigned mw = memw[w];
+            if (!mw) continue;
             const int bw = __shfl_sync(HHS_FULL_MASK, base, w);
-            const int cw = __shfl_sync(HHS_FULL_MASK, c, w);
-            if (lane >= bw && lane < bw + cw)
-                M.wslot[lane] = (short)(w * 32 + (int)__fns(memw[w], 0, lane - bw + 1));
+            if ((mw >> lane) & 1u)
+                M.wslot[bw + __popc(mw & ((1u << lane) - 1u))] = (short)(w * 32 + lane);
         }
         __syncwarp();
     }
@@ -2445,7 +2466,7 @@ __device__ void warp_subtree(const EParams& E, MidState& M, const unsigned* memw
     while (dd >= 0) {
         const int lvl = level0 + dd;
         const unsigned long long bit = 1ull << dd;
-        const double dt = ldexp(E.dt_top, -lvl);
+        const double dt = dt_at(E, lvl);
         const unsigned mk = dd == 0 ? top : M.wf[dd - 1];
         const bool in = (mk >> lane) & 1u;
         if (!(after1 & bit)) {
@@ -2700,7 +2721,7 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
     while (d >= 0) {
         const int lvl = level0 + d;
         const unsigned long long bit = 1ull << d;
-        const double dt = ldexp(E.dt_top, -lvl);
+        const double dt = dt_at(E, lvl);
         const unsigned* memw = d == 0 ? M.allw : M.fmask[d - 1];
         if (!(after1 & bit)) {
             if (lvl >= E.max_levels || lvl >= kMaxLevels - 1) {
@@ -3015,7 +3036,7 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
         const unsigned long long bit = 1ull << lvl;
         const int n = (lvl == 0) ? E.n_top : ld_volatile_i32(&E.counts[lvl - 1].n_fast);
         const int32_t* S = (lvl == 0) ? nullptr : E.fast_lists + (size_t)(lvl - 1) * E.n_max;
-        const double dt = ldexp(E.dt_top, -lvl);
+        const double dt = dt_at(E, lvl);
         const bool calc = (calcm & bit) != 0;
         int32_t* F = E.fast_lists + (size_t)lvl * E.n_max;
         int32_t* L = E.slow_lists + (size_t)lvl * E.n_max;

@@ -111,13 +111,14 @@ __device__ __forceinline__ float ts_pair_rate_mixed(float drx, float dry, float 
     const float rinv = rsqrtf(dr2);
     const float rinv2 = rinv * rinv;
     const float vdr = rdv * rinv2;
-    const float u = msum * rinv2 * rinv;
+    const float mr1 = msum * rinv;
+    const float u = mr1 * rinv2;
     const float r0 = u * rsqrtf(u) * inv_eta_s2;
     const float b0 = 1.5f * vdr;
     const float rate_ff = (b0 < r0) ? fmaf(-0.5f, b0, r0) : 0.5f * r0;
     const float q = rsqrtf(dv2);
     const float r1 = dv2 * q * rinv * inv_eta;
-    const float b1 = vdr * fmaf(msum * rinv, q * q, 1.0f);
+    const float b1 = vdr * fmaf(mr1, q * q, 1.0f);
     const float rate_fb = (b1 < r1) ? fmaf(-0.5f, b1, r1) : 0.5f * r1;
     const float rate = fmaxf(rate_ff, rate_fb);
     return dr2 == 0.0f ? __int_as_float(0x7f800000) : rate;
