@@ -61,7 +61,7 @@ def parse():
                    help="write the per-level phase profile (JSON) to this path")
     p.add_argument("--workload", default="plummer16k",
                    choices=["plummer16k", "batched", "scan", "large", "deep", "validate",
-                            "plain1k", "kickprobe"],
+                            "plain1k", "kickprobe", "tsprobe"],
                    help="plummer16k (default headline), batched (512 clusters), scan (flag "
                         "compaction sweep), large (N=262144, 90/10 masses), deep (N=65536 "
                         "Salpeter), validate (integrate --n/--eta/--mass to --t-end in mixed "
@@ -678,9 +678,9 @@ def run_scan(a, torch):
 
 def run_kickprobe(a, torch):
     """The engine's mixed kick phase alone (hhs_engine_kick_accelerations: a split node
-    with every third particle fast) on a seeded sphere of --n particles: pair
-    evaluations per second, each fast-slow pair counted once, slow-slow pairs as the
-    ordered pairs the slow units evaluate."""
+    with every third particle fast) on a seeded sphere of --n particles: kick pairs per
+    second (2 N_f N_s + N_s (N_s - 1) ordered sink-source pairs per call, the count of
+    the reference's kick_sf + kick_slow), and the same as FP32 FLOP/s at 20 flops a pair."""
     import hhs
     n = a.n
     s = hhs.plummer(n, a.seed)
@@ -701,10 +701,37 @@ def run_kickprobe(a, torch):
     ms = ev[0].elapsed_time(ev[1]) / a.steps
     nf = (n + 2) // 3
     ns = n - nf
-    evals = nf * ns + ns * ns
-    return {"metric": "engine kick pair evaluations/s", "value": evals / (ms * 1e-3),
-            "unit": "pair evaluations/s", "n": n, "n_fast": nf, "n_slow": ns, "ms": ms,
-            "kick_pairs_equivalent_per_s": (2 * nf * ns + ns * (ns - 1)) / (ms * 1e-3)}
+    pairs = 2 * nf * ns + ns * (ns - 1)
+    return {"metric": "engine kick pairs/s", "value": pairs / (ms * 1e-3),
+            "unit": "kick pairs/s", "n": n, "n_fast": nf, "n_slow": ns, "ms": ms,
+            "tflops_at_20_per_pair": 20.0 * pairs / (ms * 1e-3) * 1e-12}
+
+
+def run_tsprobe(a, torch):
+    """The engine's mixed timestep phase alone (hhs_engine_timestep_rates: one node of --n
+    particles, packed symmetric tiles) on a seeded sphere: unordered pair evaluations per
+    second (n (n - 1) / 2 per call; each gives the pair's rate to both particles)."""
+    import hhs
+    n = a.n
+    s = hhs.plummer(n, a.seed)
+    ctx = hhs.Context(n, 64, eta=a.eta)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    L = hhs.lib()
+    for _ in range(a.warmup):
+        assert L.hhs_engine_timestep_rates(ctx.h, d.ref, n, None) == 0
+    ctx.check()
+    ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    torch.cuda.synchronize()
+    ev[0].record()
+    for _ in range(a.steps):
+        assert L.hhs_engine_timestep_rates(ctx.h, d.ref, n, None) == 0
+    ev[1].record()
+    ctx.check()
+    ms = ev[0].elapsed_time(ev[1]) / a.steps
+    pairs = n * (n - 1) // 2
+    return {"metric": "engine timestep unordered pairs/s", "value": pairs / (ms * 1e-3),
+            "unit": "pair evaluations/s", "n": n, "ms": ms}
 
 
 def run_plain1k(a, torch):
@@ -1001,10 +1028,10 @@ def main():
         if dist is not None:
             dist.destroy_process_group()
         return
-    if a.workload in ("scan", "validate", "plain1k", "kickprobe"):
+    if a.workload in ("scan", "validate", "plain1k", "kickprobe", "tsprobe"):
         if rank == 0:
             fn = {"scan": run_scan, "validate": run_validate, "plain1k": run_plain1k,
-                  "kickprobe": run_kickprobe}[a.workload]
+                  "kickprobe": run_kickprobe, "tsprobe": run_tsprobe}[a.workload]
             out = fn(a, torch)
             if a.workload == "scan" and "roofline" in out:
                 hbm, src = hbm_peak()

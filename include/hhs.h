@@ -403,6 +403,18 @@ hhs_status hhs_ctx_set_trace(hhs_ctx* ctx, int32_t* d_nodes, int64_t capacity,
 hhs_status hhs_engine_kick_accelerations(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n,
                                          void* stream);
 
+/* Timesteps computed by the mixed-precision timestep phase of hhs_hold_step -- the same
+ * packed members, bulk-copied column tiles, symmetric FP32 pair rates (one evaluation per
+ * unordered pair) and row/column maxima -- for the first n >= 2 particles taken as one
+ * node (every other particle of the n is a source), converted to timesteps as the split
+ * does (1 / max rate, capped at 1e30) and written to sys->ts. The counterpart of
+ * _timesteps / timesteps (src/timestep.cuh:65-118) in mixed precision; a diagnostic for
+ * checking that arithmetic against the FP64 expression. It uses the context's packed
+ * member arrays and rate words, so do not run it concurrently with a step on the
+ * context. */
+hhs_status hhs_engine_timestep_rates(hhs_ctx* ctx, hhs_particle_system* sys, int32_t n,
+                                     void* stream);
+
 /* Kernel launches issued by this library since it was loaded (all contexts). */
 uint64_t hhs_kernel_launch_count(void);
 

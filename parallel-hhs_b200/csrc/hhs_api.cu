@@ -386,6 +386,12 @@ extern "C" hhs_status hhs_engine_kick_accelerations(hhs_ctx* c, hhs_particle_sys
                                      static_cast<cudaStream_t>(stream));
 }
 
+extern "C" hhs_status hhs_engine_timestep_rates(hhs_ctx* c, hhs_particle_system* sys, int32_t n,
+                                                void* stream) {
+    if (!c || !sys_ok(sys) || n < 2 || n > sys->n || n > c->n_max) return HHS_ERR_INVALID_ARG;
+    return engine_timestep_rates(c, soa_of(sys), n, static_cast<cudaStream_t>(stream));
+}
+
 extern "C" hhs_status hhs_ctx_set_trace(hhs_ctx* c, int32_t* d_nodes, int64_t capacity,
                                         uint64_t* d_count) {
     if (!c) return HHS_ERR_INVALID_ARG;

@@ -55,6 +55,7 @@ hhs_status engine_set_trace(hhs_ctx* c, int32_t* nodes, int64_t capacity,
                             unsigned long long* count);
 hhs_status engine_kick_accelerations(hhs_ctx* c, const SoA& P, double* ax, double* ay,
                                      double* az, int n, cudaStream_t stream);
+hhs_status engine_timestep_rates(hhs_ctx* c, const SoA& P, int n, cudaStream_t stream);
 // Sharded phases of the multi-GPU step (one rank's share; results into every replica).
 // Mixed timesteps leave pair-rate maxima in rate_words (local) and the peers' words;
 // engine_rates_to_ts turns them into timesteps on every rank after the barrier.

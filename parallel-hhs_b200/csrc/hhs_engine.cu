@@ -836,19 +836,15 @@ __device__ void kick_unit(const EParams& E, const int32_t* F, const int32_t* L, 
             if (act) {
                 const int je = min(tl, jend - t0);
                 // blocked compensated summation: 32-pair FP32 blocks, Kahan across blocks
-                // (full blocks unrolled so that consecutive pairs overlap). 1/r is rsqrtf
-                // without a Newton step: its few-ulp error per pair is of the order of the
-                // FP32 pair arithmetic itself, and |dE/E| after one N-body time is unchanged
-                // (6.6e-9 against 6.9e-9 with the Newton step, Plummer N=16384).
+                // (full blocks unrolled so that consecutive pairs overlap); 1/r^3 from
+                // rsqrtf with one Newton correction
                 auto pair = [&](int jl, float& bx, float& by, float& bz) {
                     const float4 A = sm.u.km.A[jl], B = sm.u.km.B[jl];
                     const float dx = ds_diff(A.x, B.x, xi.hi, xi.lo);
                     const float dy = ds_diff(A.y, B.y, yi.hi, yi.lo);
                     const float dz = ds_diff(A.z, B.z, zi.hi, zi.lo);
                     const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, E.eps2f)));
-                    const float ri = rsqrtf(d2);
-                    const float ri2 = ri * ri;
-                    const float mr3 = (d2 > 0.0f) ? A.w * ri2 * ri : 0.0f;
+                    const float mr3 = mr3_nr(A.w, d2);
                     bx = fmaf(dx, mr3, bx);
                     by = fmaf(dy, mr3, by);
                     bz = fmaf(dz, mr3, bz);
@@ -2127,8 +2123,7 @@ __device__ void tiny_hold(const EParams& E, const int32_t* S, int n, int level0,
                             const float dy = ds_diff(A.y, B.y, Ai.y, Bi.y);
                             const float dz = ds_diff(A.z, B.z, Ai.z, Bi.z);
                             const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, E.eps2f)));
-                            const float ri = rsqrtf(d2);
-                            const float mr3 = (d2 > 0.0f) ? A.w * ri * ri * ri : 0.0f;
+                            const float mr3 = mr3_nr(A.w, d2);
                             a[0] = fmaf(dx, mr3, a[0]);
                             a[1] = fmaf(dy, mr3, a[1]);
                             a[2] = fmaf(dz, mr3, a[2]);
@@ -2401,8 +2396,7 @@ __device__ __forceinline__ void acc_over(const EParams& E, const MidState& M, co
         const float dy = ds_diff(A.y, B.y, Ai.y, Bi.y);
         const float dz = ds_diff(A.z, B.z, Ai.z, Bi.z);
         const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, E.eps2f)));
-        const float ri = rsqrtf(d2);
-        const float mr3 = (d2 > 0.0f) ? A.w * ri * ri * ri : 0.0f;
+        const float mr3 = mr3_nr(A.w, d2);
         a[0] = fmaf(dx, mr3, a[0]);
         a[1] = fmaf(dy, mr3, a[1]);
         a[2] = fmaf(dz, mr3, a[2]);
@@ -2621,8 +2615,7 @@ __device__ void warp_subtree(const EParams& E, MidState& M, const unsigned* memw
                             const float dy = ds_diff(A.y, B.y, Ai.y, Bi.y);
                             const float dz = ds_diff(A.z, B.z, Ai.z, Bi.z);
                             const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, E.eps2f)));
-                            const float ri = rsqrtf(d2);
-                            const float mr3 = (d2 > 0.0f) ? A.w * ri * ri * ri : 0.0f;
+                            const float mr3 = mr3_nr(A.w, d2);
                             a[0] = fmaf(dx, mr3, a[0]);
                             a[1] = fmaf(dy, mr3, a[1]);
                             a[2] = fmaf(dz, mr3, a[2]);
@@ -3285,6 +3278,39 @@ __global__ void __launch_bounds__(kEB, 2) k_engine_accel(EParams E) {
         }
 }
 
+// Probe of the mixed grid timestep: the first n particles as one node whose timesteps
+// are computed by the packed symmetric tile phase of k_engine (members packed, column
+// tiles bulk-copied, one rate per unordered pair, row and column maxima), then converted
+// to timesteps as the split phase does, into P.ts (see engine_timestep_rates).
+__global__ void __launch_bounds__(kEB, 2) k_engine_ts(EParams E) {
+    extern __shared__ __align__(16) unsigned char engine_smem[];
+    Smem& sm = *reinterpret_cast<Smem*>(engine_smem);
+    const Workers W{(int)blockIdx.x, (int)gridDim.x, kModeGrid};
+    if (threadIdx.x == 0) {
+        sm.bar_k = 0u;
+        sm.kphase = 0u;
+        sm.tphase = 0u;
+        mbar_init(&sm.kbar, 1u);
+        mbar_init(&sm.tbar[0], 1u);
+        mbar_init(&sm.tbar[1], 1u);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    const int n = E.n_top;
+    pack_ts(E, nullptr, n, W);
+    if (!grid_barrier(E, sm)) return;
+    const int cw = ts_tile_width(n, W.count);
+    const long long units = ts_tile_units(n, cw);
+    ts_sym_tiles(E, n, cw, units * W.id / W.count, units * (W.id + 1) / W.count, sm);
+    if (!grid_barrier(E, sm)) return;
+    for (int i = W.id * kEB + (int)threadIdx.x; i < n; i += W.count * kEB) {
+        const float mr = __uint_as_float(E.rate_acc[i]);
+        E.rate_acc[i] = 0u;
+        const double tv = 1.0 / (double)mr;
+        E.P.ts[i] = tv < 1.e30 ? tv : 1.e30;
+    }
+}
+
 // ---------------------------------------------------------------- sharded phases
 // The engine's tiled timestep and kick phases over one rank's share of a level, for the
 // multi-GPU step (hhs_hold_step_dist): ordinary launches whose CTAs split the rank's
@@ -3862,6 +3888,17 @@ hhs_status engine_kick_accelerations(hhs_ctx* c, const SoA& P, double* ax, doubl
     E.rate_acc = reinterpret_cast<unsigned*>(ay);
     E.tile_counts = reinterpret_cast<int*>(az);
     const cudaError_t e = engine_launch(eh, 1, k_engine_accel, E, stream);
+    hhs_count_launch();
+    if (e != cudaSuccess) return hhs_from_cuda(e);
+    return HHS_OK;
+}
+
+hhs_status engine_timestep_rates(hhs_ctx* c, const SoA& P, int n, cudaStream_t stream) {
+    auto* eh = static_cast<EngineHost*>(c->engine_host);
+    if (!eh || n < 2 || n > c->n_max) return HHS_ERR_INVALID_ARG;
+    EParams E = engine_params(c, eh, P, n, 1.0, true, false, 0);
+    if (!E.tr_a) return HHS_ERR_INVALID_ARG;
+    const cudaError_t e = engine_launch(eh, 1, k_engine_ts, E, stream);
     hhs_count_launch();
     if (e != cudaSuccess) return hhs_from_cuda(e);
     return HHS_OK;

@@ -84,6 +84,16 @@ __device__ __forceinline__ float rsqrt_nr(float x) {
     return y * fmaf(-0.5f * x, y * y, 1.5f);
 }
 
+// m / d^3 from rsqrtf(d2) with one Newton-Raphson correction folded into the cube:
+// y^3 (2.5 - 1.5 d2 y^2), whose relative error is second order in rsqrtf's; 0 when d2 == 0
+// (a particle and itself).
+__device__ __forceinline__ float mr3_nr(float m, float d2) {
+    const float y = rsqrtf(d2);
+    const float y2 = y * y;
+    const float c = fmaf(-1.5f, d2 * y2, 2.5f);
+    return d2 > 0.0f ? m * (y2 * y) * c : 0.0f;
+}
+
 // Kahan-compensated accumulation s += t (c holds the running compensation).
 __device__ __forceinline__ void kahan_add(float& s, float& c, float t) {
     const float y = __fsub_rn(t, c);

@@ -173,6 +173,7 @@ SIGNATURES = {
                                           ctypes.c_int, ctypes.POINTER(BatchTuning), _vp,
                                           ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), _vp]),
     "hhs_engine_kick_accelerations": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp]),
+    "hhs_engine_timestep_rates": (ctypes.c_int, [_vp, _vp, ctypes.c_int32, _vp]),
     "hhs_scan_noalloc_selftest_stalled_predecessor": (ctypes.c_int, [_vp, _vp, ctypes.c_int64,
                                                                      ctypes.c_uint32, _vp]),
     "hhs_compact_flags_i32": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_int64, _vp,

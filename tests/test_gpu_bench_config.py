@@ -191,3 +191,28 @@ def test_engine_mixed_kick_accelerations_against_oracle(cuda, hhs, oracle, n, ep
     # particle whose pulls nearly cancel has a small |a| but the same absolute error)
     assert err_s.max() < 5e-7, err_s.max()
     assert err.max() < 2e-6 and np.median(err) < 1e-7, (err.max(), np.median(err))
+
+
+@pytest.mark.parametrize("n,eta", [(3000, 0.03), (16384, 0.03), (20000, 0.02)])
+def test_engine_mixed_timesteps_against_oracle(cuda, hhs, oracle, n, eta):
+    """The timestep phase of the device step in mixed precision (members packed, column
+    tiles bulk-copied, one FP32 rate per unordered pair feeding both particles' maxima,
+    tiles unmasked away from the diagonal) over a whole node, against the FP64 timesteps
+    of the oracle: the largest relative difference stays at the FP32 rounding of the pair
+    expression (rsqrtf without a Newton step), far inside the width of a timestep level."""
+    s = hhs.plummer(n, 900 + n)
+    ref = oracle.timesteps(s, eta)
+    ctx = hhs.Context(n, 64, eta=eta)
+    d = hhs.ParticleSystem(n)
+    d.upload(s)
+    assert hhs.lib().hhs_engine_timestep_rates(ctx.h, d.ref, n, None) == 0
+    ctx.check()
+    ts = d.download()["ts"]
+    rel = np.abs(ts - ref) / ref
+    print(f"\nengine timesteps n={n}: max rel {rel.max():.3e} median {np.median(rel):.3e}")
+    assert rel.max() < 2e-6, rel.max()
+    # a second call on the same context: the rate words were left at zero
+    d.upload(s)
+    assert hhs.lib().hhs_engine_timestep_rates(ctx.h, d.ref, n, None) == 0
+    ctx.check()
+    assert np.array_equal(d.download()["ts"], ts)
