@@ -267,12 +267,13 @@ __device__ bool grid_barrier(const EParams& E, Smem& sm) {
                     break;
                 }
             }
-            sm.ok = ok;
+            // the verdict into every CTA of the cluster while all of them wait at the
+            // barrier below (no CTA reads another's shared memory after it, when that
+            // CTA may already have exited)
+            for (unsigned r = 0; r < cs; r++) *cl.map_shared_rank(&sm.ok, (int)r) = ok;
         }
         cl.sync();
-        // rank 0 rewrites its verdict only after every CTA of the cluster has reached the
-        // next barrier's first stage
-        return *cl.map_shared_rank(&sm.ok, 0) != 0;
+        return sm.ok != 0;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -3655,12 +3656,16 @@ hhs_status engine_init(hhs_ctx* c, void* base) {
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEngineSmem));
     HHS_CUDA_TRY(cudaFuncSetAttribute(k_engine_accel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kEngineSmem));
+    HHS_CUDA_TRY(cudaFuncSetAttribute(k_engine_ts, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kEngineSmem));
     // clusters of 16 CTAs (beyond the portable 8) for the subtree solver, where allowed
     if (cudaFuncSetAttribute(k_engine<HHS_PREC_FP64>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
             cudaSuccess ||
         cudaFuncSetAttribute(k_engine<HHS_PREC_MIXED>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
             cudaSuccess ||
         cudaFuncSetAttribute(k_engine_accel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_engine_ts, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
             cudaSuccess)
         (void)cudaGetLastError();  // cluster size 16 then fails its occupancy check
     HHS_CUDA_TRY(cudaFuncSetAttribute(k_shard_ts_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
