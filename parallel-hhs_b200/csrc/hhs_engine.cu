@@ -236,45 +236,7 @@ __device__ __forceinline__ int ld_volatile_i32(const int32_t* p) {
 // grid size. Arrivals are fire-and-forget release reductions (no CTA waits for its own
 // atomic to return); waiters poll with acquire loads, give up after kBarrierTimeoutNs (or
 // as soon as another CTA recorded an error) and report failure instead of hanging.
-// Grid barrier in two stages when true: the CTAs of each hardware cluster meet at a
-// cluster barrier, one CTA per cluster counts in and waits on the global counter, and a
-// second cluster barrier releases the rest (a quarter of the global atomics and pollers
-// with clusters of 4).
-constexpr bool kClusterBarrier = false;
-
 __device__ bool grid_barrier(const EParams& E, Smem& sm) {
-    if constexpr (kClusterBarrier) {
-        namespace cg = cooperative_groups;
-        cg::cluster_group cl = cg::this_cluster();
-        const unsigned cs = cl.num_blocks();
-        cl.sync();  // every CTA of the cluster is done with the phase
-        if (cl.block_rank() == 0 && threadIdx.x == 0) {
-            // the cluster barrier ordered the other CTAs' writes before this release
-            int ok = 1;
-            EngineState* st = E.st;
-            const unsigned target = (++sm.bar_k) * (gridDim.x / cs);
-            red_add_release_u32(&st->bar_count, 1u);
-            unsigned polls = 0;
-            unsigned long long t0 = 0;
-            while (ld_acquire_u32(&st->bar_count) < target) {
-                if (++polls < 256) continue;
-                if (t0 == 0) t0 = gtimer();
-                if (*reinterpret_cast<volatile unsigned*>(E.err) != 0u) { ok = 0; break; }
-                __nanosleep(32);
-                if (gtimer() - t0 > kBarrierTimeoutNs) {
-                    atomicOr(E.err, HHS_ERRBIT_BARRIER_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
-            }
-            // the verdict into every CTA of the cluster while all of them wait at the
-            // barrier below (no CTA reads another's shared memory after it, when that
-            // CTA may already have exited)
-            for (unsigned r = 0; r < cs; r++) *cl.map_shared_rank(&sm.ok, (int)r) = ok;
-        }
-        cl.sync();
-        return sm.ok != 0;
-    }
     __syncthreads();
     if (threadIdx.x == 0) {
         // The CTA barrier above orders every thread's writes before this thread's
