@@ -98,11 +98,11 @@ struct EParams {
     float4* pk_a;   // [pk_levels][n_max]
     float4* pk_b;   // [pk_levels][n_max]
     int pk_levels;
-    // the members of the current grid node packed for the mixed timestep, in list order:
-    // double-single position (tr_a = hi + mass, tr_b = lo) and FP32 velocity
-    float4* tr_a;
-    float4* tr_b;
-    float4* tr_v;
+    // the members of the current grid node packed for the mixed timestep, in list order,
+    // in pairs: five arrays of tq_stride float4, member 2p + h at component h (and 2 + h)
+    // of entry p: (x hi, y hi), (z hi, mass), (x lo, y lo), (z lo, vx), (vy, vz)
+    float4* tq;
+    long long tq_stride;
     int prec_mixed;  // this launch runs the mixed-precision kernels
     int overlap;     // slow-only kick units beside a subtree's first pass (tuning)
     int4* trace;                        // node record {level, n, n_fast, calc} in call order
@@ -185,7 +185,7 @@ struct __align__(16) Smem {
             float colw[kEB / 32][kTX][3];
         } kc;
         struct {                                                  // packed timestep tiles
-            float4 A[2][kTW], B[2][kTW], V[2][kTW];
+            float4 Q[2][5][kTW / 2];                              // column pairs
             float colred[2][kEB / 32][kTW];
         } ts2;
         struct { float4 P0[kEB], P1[kEB], P2[kEB]; float2 M[kEB]; } kx;  // packed kick tiles
@@ -622,15 +622,40 @@ __device__ __forceinline__ int ts_tile_width(int n, int workers) {
     return cw;
 }
 
+// Member i of the packed timestep arrays: pair entry i / 2, component i % 2 (and 2 + i % 2)
+// of each of the five arrays.
+__device__ __forceinline__ void tq_put(const EParams& E, int i, double x, double y, double z,
+                                       double m, double vx, double vy, double vz) {
+    const DS X = ds_split(x), Y = ds_split(y), Z = ds_split(z);
+    float* q = reinterpret_cast<float*>(E.tq) + 4 * (size_t)(i >> 1) + (i & 1);
+    const size_t a = 4 * (size_t)E.tq_stride;  // floats per array
+    q[0] = X.hi;
+    q[2] = Y.hi;
+    q[a] = Z.hi;
+    q[a + 2] = (float)m;
+    q[2 * a] = X.lo;
+    q[2 * a + 2] = Y.lo;
+    q[3 * a] = Z.lo;
+    q[3 * a + 2] = (float)vx;
+    q[4 * a] = (float)vy;
+    q[4 * a + 2] = (float)vz;
+}
+
+// Member i as a sink of the packed timestep: negated, each value in both lanes.
+__device__ __forceinline__ TsSink2 tq_sink(const EParams& E, int i) {
+    const float* q = reinterpret_cast<const float*>(E.tq) + 4 * (size_t)(i >> 1) + (i & 1);
+    const size_t a = 4 * (size_t)E.tq_stride;
+    return TsSink2{f2dup(-q[0]), f2dup(-q[2]), f2dup(-q[a]), f2dup(-q[2 * a]),
+                   f2dup(-q[2 * a + 2]), f2dup(-q[3 * a]), f2dup(-q[3 * a + 2]),
+                   f2dup(-q[4 * a]), f2dup(-q[4 * a + 2]), f2dup(q[a + 2])};
+}
+
 // The node's members (list S, n of them) into the packed timestep arrays.
 __device__ void pack_ts(const EParams& E, const int32_t* S, int n, const Workers& W) {
     const SoA& P = E.P;
     for (int i = W.id * kEB + (int)threadIdx.x; i < n; i += W.count * kEB) {
         const int g = list_at(S, i);
-        const DS x = ds_split(P.x[g]), y = ds_split(P.y[g]), z = ds_split(P.z[g]);
-        E.tr_a[i] = make_float4(x.hi, y.hi, z.hi, (float)P.m[g]);
-        E.tr_b[i] = make_float4(x.lo, y.lo, z.lo, 0.0f);
-        E.tr_v[i] = make_float4((float)P.vx[g], (float)P.vy[g], (float)P.vz[g], 0.0f);
+        tq_put(E, i, P.x[g], P.y[g], P.z[g], P.m[g], P.vx[g], P.vy[g], P.vz[g]);
     }
 }
 
@@ -645,13 +670,15 @@ __device__ __forceinline__ void ts_tile_of(long long u, int nrb, int ncb, int st
     cb = rb * step + (int)u;
 }
 
+// columns [c0, c0 + ncol), c0 even: their (ncol + 1) / 2 pair entries of the five arrays
 __device__ __forceinline__ void ts_tile_stage(const EParams& E, int buf, int c0, int ncol,
                                               Smem& sm) {
-    const unsigned bytes = (unsigned)ncol * (unsigned)sizeof(float4);
-    mbar_arrive_expect_tx(&sm.tbar[buf], 3u * bytes);
-    bulk_load(sm.u.ts2.A[buf], E.tr_a + c0, bytes, &sm.tbar[buf]);
-    bulk_load(sm.u.ts2.B[buf], E.tr_b + c0, bytes, &sm.tbar[buf]);
-    bulk_load(sm.u.ts2.V[buf], E.tr_v + c0, bytes, &sm.tbar[buf]);
+    const unsigned bytes = (unsigned)((ncol + 1) >> 1) * (unsigned)sizeof(float4);
+    mbar_arrive_expect_tx(&sm.tbar[buf], 5u * bytes);
+#pragma unroll
+    for (int k = 0; k < 5; k++)
+        bulk_load(sm.u.ts2.Q[buf][k], E.tq + (size_t)k * E.tq_stride + (c0 >> 1), bytes,
+                  &sm.tbar[buf]);
 }
 
 __device__ void ts_sym_tiles(const EParams& E, int n, int cw, long long u0, long long u1,
@@ -673,8 +700,8 @@ __device__ void ts_sym_tiles(const EParams& E, int n, int cw, long long u0, long
     }
     int cur = -1, i = 0;
     bool act = false;
-    DS xi{0, 0}, yi{0, 0}, zi{0, 0};
-    float vxi = 0, vyi = 0, vzi = 0, mi = 0, rowmax = 0.0f;
+    TsSink2 si{};
+    float rowmax = 0.0f;
     unsigned phase = sm.tphase;
     int nrb_n = rb, ncb_n = cb;  // the unit two ahead, for the refill
     for (int k = 0; k < 2; k++)
@@ -687,42 +714,49 @@ __device__ void ts_sym_tiles(const EParams& E, int n, int cw, long long u0, long
             rowmax = 0.0f;
             i = rb * kEB + threadIdx.x;
             act = i < n;
-            if (act) {
-                const float4 a = E.tr_a[i], b = E.tr_b[i], v = E.tr_v[i];
-                xi = DS{a.x, b.x}; yi = DS{a.y, b.y}; zi = DS{a.z, b.z};
-                vxi = v.x; vyi = v.y; vzi = v.z; mi = a.w;
-            }
+            if (act) si = tq_sink(E, i);
         }
         const int c0 = cb * cw;
         const int ncol = min(cw, n - c0);
         if (!mbar_wait(&sm.tbar[buf], (phase >> buf) & 1u, E.err))
             (void)mbar_wait(&sm.tbar[buf], (phase >> buf) & 1u, nullptr);
         phase ^= 1u << buf;
-        const float4* TA = sm.u.ts2.A[buf];
-        const float4* TB = sm.u.ts2.B[buf];
-        const float4* TV = sm.u.ts2.V[buf];
-        // pairs need a mask only in the tiles that cross the diagonal (j > i) or hold rows
-        // past the end
+        const float4* Q0 = sm.u.ts2.Q[buf][0];
+        const float4* Q1 = sm.u.ts2.Q[buf][1];
+        const float4* Q2 = sm.u.ts2.Q[buf][2];
+        const float4* Q3 = sm.u.ts2.Q[buf][3];
+        const float4* Q4 = sm.u.ts2.Q[buf][4];
+        // pairs need a mask only in the tiles that cross the diagonal (j > i), hold rows
+        // past the end or end in half a column pair
         const int diag_end = (rb + 1) * kEB;  // columns from here see every row as j > i
-        const int mask = c0 < diag_end ? 2 : (diag_end > n ? 1 : 0);
+        const int mask = c0 < diag_end ? 2 : ((diag_end > n || (ncol & 1)) ? 1 : 0);
         auto cols = [&](auto MASK) {
             constexpr int M = decltype(MASK)::value;
             for (int g = 0; g < ncol; g += 32) {
-                const int nc = min(32, ncol - g);
+                const int np = (min(32, ncol - g) + 1) >> 1;  // column pairs of this group
                 unsigned colmax = 0u;
-#pragma unroll 8
-                for (int c = 0; c < nc; c++) {
-                    const int jl = g + c;
-                    const float4 A = TA[jl], B = TB[jl], V = TV[jl];
-                    const float rate = ts_pair_rate_mixed(
-                        ds_diff(xi.hi, xi.lo, A.x, B.x), ds_diff(yi.hi, yi.lo, A.y, B.y),
-                        ds_diff(zi.hi, zi.lo, A.z, B.z), vxi - V.x, vyi - V.y, vzi - V.z,
-                        mi + A.w, E.inv_eta_s2, E.inv_eta);
-                    const float r = M == 2 ? ((act && c0 + jl > i) ? rate : 0.0f)
-                                           : (M == 1 ? (act ? rate : 0.0f) : rate);
-                    rowmax = fmaxf(rowmax, r);
-                    const unsigned cm = __reduce_max_sync(HHS_FULL_MASK, __float_as_uint(r));
-                    colmax = lane == c ? cm : colmax;
+#pragma unroll 4
+                for (int q = 0; q < np; q++) {
+                    const int e = (g >> 1) + q;  // pair entry: columns c0 + 2e, c0 + 2e + 1
+                    const float4 a0 = Q0[e], a1 = Q1[e], a2 = Q2[e], a3 = Q3[e], a4 = Q4[e];
+                    const float2 rate = ts_pair_rate_mixed2(
+                        make_float2(a0.x, a0.y), make_float2(a0.z, a0.w), make_float2(a1.x, a1.y),
+                        make_float2(a2.x, a2.y), make_float2(a2.z, a2.w), make_float2(a3.x, a3.y),
+                        make_float2(a3.z, a3.w), make_float2(a4.x, a4.y), make_float2(a4.z, a4.w),
+                        make_float2(a1.z, a1.w), si, E.inv_eta_s2, E.inv_eta);
+                    float r0 = rate.x, r1 = rate.y;
+                    if (M != 0) {
+                        const int c = c0 + 2 * e;
+                        const bool ok0 = act && c < n && (M == 1 || c > i);
+                        const bool ok1 = act && c + 1 < n && (M == 1 || c + 1 > i);
+                        r0 = ok0 ? r0 : 0.0f;
+                        r1 = ok1 ? r1 : 0.0f;
+                    }
+                    rowmax = fmaxf(rowmax, fmaxf(r0, r1));
+                    const unsigned m0 = __reduce_max_sync(HHS_FULL_MASK, __float_as_uint(r0));
+                    const unsigned m1 = __reduce_max_sync(HHS_FULL_MASK, __float_as_uint(r1));
+                    colmax = lane == 2 * q ? m0 : colmax;
+                    colmax = lane == 2 * q + 1 ? m1 : colmax;
                 }
                 sm.u.ts2.colred[buf][warp][g + lane] = __uint_as_float(colmax);
             }
@@ -1900,12 +1934,9 @@ __device__ void kick_reduce_phase(const EParams& E, const int32_t* F, const int3
 #pragma unroll
                 for (int c = 0; c < 3; c++) v1[c] = fma(red[3 * threadIdx.x + c], dt, v0[c]);
                 P.vx[g] = v1[0]; P.vy[g] = v1[1]; P.vz[g] = v1[2];
-                if (!slow && E.tr_a && W.mode == kModeGrid) {
+                if (!slow && E.tq && W.mode == kModeGrid) {
                     // the fast set's next pass recomputes its timesteps from these records
-                    const DS x = ds_split(P.x[g]), y = ds_split(P.y[g]), z = ds_split(P.z[g]);
-                    E.tr_a[s2] = make_float4(x.hi, y.hi, z.hi, (float)P.m[g]);
-                    E.tr_b[s2] = make_float4(x.lo, y.lo, z.lo, 0.0f);
-                    E.tr_v[s2] = make_float4((float)v1[0], (float)v1[1], (float)v1[2], 0.0f);
+                    tq_put(E, s2, P.x[g], P.y[g], P.z[g], P.m[g], v1[0], v1[1], v1[2]);
                 }
                 if (slow) {
                     P.x[g] = fma(v1[0], h, fma(v0[0], h, P.x[g]));
@@ -3097,7 +3128,7 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
                         ts_unit<PREC>(E, S, n, ib, j0, j1, E.ts_part + (size_t)jc * E.n_max,
                                       nullptr, sm);
                     }
-                } else if (MODE == kModeGrid && E.tr_a) {
+                } else if (MODE == kModeGrid && E.tq) {
                     // packed members: written by the parent's kick-reduce phase when it
                     // ran (the second pass of a fast set), else packed here
                     if (lvl == top || ld_volatile_i32(&E.counts[lvl - 1].n_slow) == 0) {
@@ -3560,9 +3591,8 @@ struct EngineHost {
     float4* pk_b = nullptr;
     int pk_levels = 0;
     double* c_part = nullptr;
-    float4* tr_a = nullptr;
-    float4* tr_b = nullptr;
-    float4* tr_v = nullptr;
+    float4* tq = nullptr;
+    long long tq_stride = 0;
     int32_t* trace = nullptr;                 // caller's node-record buffer (4 int32 each)
     unsigned long long* trace_count = nullptr;
     long long trace_cap = 0;
@@ -3583,7 +3613,7 @@ size_t engine_workspace_bytes(int n_max, int max_levels) {
            al(sizeof(double) * kMaxChunks * 3 * n) + al(sizeof(int) * (n / kEB + 2)) +
            al(sizeof(unsigned) * n) + al(sizeof(unsigned long long) * (n / kEB + 2)) +
            2 * al(sizeof(float4) * n * (size_t)pk_levels_for(max_levels)) +
-           al(sizeof(double) * kMaxFsb * 3 * n) + 3 * al(sizeof(float4) * n);
+           al(sizeof(double) * kMaxFsb * 3 * n) + al(sizeof(float4) * 5 * (n / 2 + 1));
 }
 
 hhs_status engine_init(hhs_ctx* c, void* base) {
@@ -3602,9 +3632,8 @@ hhs_status engine_init(hhs_ctx* c, void* base) {
     eh->pk_a = reinterpret_cast<float4*>(p); p += al(sizeof(float4) * n * (size_t)eh->pk_levels);
     eh->pk_b = reinterpret_cast<float4*>(p); p += al(sizeof(float4) * n * (size_t)eh->pk_levels);
     eh->c_part = reinterpret_cast<double*>(p); p += al(sizeof(double) * kMaxFsb * 3 * n);
-    eh->tr_a = reinterpret_cast<float4*>(p); p += al(sizeof(float4) * n);
-    eh->tr_b = reinterpret_cast<float4*>(p); p += al(sizeof(float4) * n);
-    eh->tr_v = reinterpret_cast<float4*>(p);
+    eh->tq = reinterpret_cast<float4*>(p);
+    eh->tq_stride = (long long)(n / 2 + 1);
     eh->n_max = c->n_max;
     int dev = 0, sms = 0, coop = 0;
     cudaGetDevice(&dev);
@@ -3814,9 +3843,8 @@ EParams engine_params(hhs_ctx* c, EngineHost* eh, const SoA& P, int n, double dt
     E.ts_part = eh->ts_part;
     E.k_part = eh->k_part;
     E.c_part = eh->c_part;
-    E.tr_a = eh->tr_a;
-    E.tr_b = eh->tr_b;
-    E.tr_v = eh->tr_v;
+    E.tq = eh->tq;
+    E.tq_stride = eh->tq_stride;
     E.tile_counts = eh->tile_counts;
     E.tile_status = eh->tile_status;
     E.rate_acc = eh->rate_acc;
@@ -3901,7 +3929,7 @@ hhs_status engine_timestep_rates(hhs_ctx* c, const SoA& P, int n, cudaStream_t s
     auto* eh = static_cast<EngineHost*>(c->engine_host);
     if (!eh || n < 2 || n > c->n_max) return HHS_ERR_INVALID_ARG;
     EParams E = engine_params(c, eh, P, n, 1.0, true, false, 0);
-    if (!E.tr_a) return HHS_ERR_INVALID_ARG;
+    if (!E.tq) return HHS_ERR_INVALID_ARG;
     const cudaError_t e = engine_launch(eh, 1, k_engine_ts, E, stream);
     hhs_count_launch();
     if (e != cudaSuccess) return hhs_from_cuda(e);
@@ -4195,7 +4223,8 @@ extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, d
     E.leaf_time = nullptr;
     E.stats = b->d_stats;
     E.ts_part = E.k_part = E.c_part = nullptr;
-    E.tr_a = E.tr_b = E.tr_v = nullptr;
+    E.tq = nullptr;
+    E.tq_stride = 0;
     E.tile_counts = nullptr;
     E.tile_status = nullptr;
     E.rate_acc = nullptr;

@@ -125,16 +125,61 @@ __device__ __forceinline__ float ts_pair_rate_mixed(float drx, float dry, float 
     const float u = mr1 * rinv2;
     const float r0 = u * rsqrtf(u) * inv_eta_s2;
     const float b0 = 1.5f * vdr;
-    const float rate_ff = (b0 < r0) ? fmaf(-0.5f, b0, r0) : 0.5f * r0;
+    // (b0 < r0) ? r0 - b0/2 : r0/2, as r0 - min(b0, r0)/2 (the same value: r0 - r0/2 is
+    // exact, and fminf keeps r0 when b0 is NaN, as the comparison does)
+    const float rate_ff = fmaf(-0.5f, fminf(b0, r0), r0);
     const float q = rsqrtf(dv2);
     const float r1 = dv2 * q * rinv * inv_eta;
     const float b1 = vdr * fmaf(mr1, q * q, 1.0f);
-    const float rate_fb = (b1 < r1) ? fmaf(-0.5f, b1, r1) : 0.5f * r1;
+    const float rate_fb = fmaf(-0.5f, fminf(b1, r1), r1);
     const float rate = fmaxf(rate_ff, rate_fb);
     return dr2 == 0.0f ? __int_as_float(0x7f800000) : rate;
 }
 
 // ---- packed FP32 pairs (sm_100 f32x2) ----------------------------------------------
+// A sink against two sources at once in f32x2 arithmetic: the sink's values come negated
+// and duplicated, the sources' as pairs. Every lane runs the operations of
+// ts_pair_rate_mixed in the same order on the negated offsets (source minus sink), whose
+// squares and products are those of the scalar form, so each lane's rate equals it bit
+// for bit.
+struct TsSink2 {
+    float2 nxh, nyh, nzh, nxl, nyl, nzl, nvx, nvy, nvz, m;
+};
+
+__device__ __forceinline__ float2 f2dup(float v) { return make_float2(v, v); }
+
+__device__ __forceinline__ float2 ts_pair_rate_mixed2(float2 xh, float2 yh, float2 zh, float2 xl,
+                                                      float2 yl, float2 zl, float2 vx, float2 vy,
+                                                      float2 vz, float2 m, const TsSink2& s,
+                                                      float inv_eta_s2, float inv_eta) {
+    const float2 drx = __fadd2_rn(__fadd2_rn(xh, s.nxh), __fadd2_rn(xl, s.nxl));
+    const float2 dry = __fadd2_rn(__fadd2_rn(yh, s.nyh), __fadd2_rn(yl, s.nyl));
+    const float2 drz = __fadd2_rn(__fadd2_rn(zh, s.nzh), __fadd2_rn(zl, s.nzl));
+    const float2 dvx = __fadd2_rn(vx, s.nvx), dvy = __fadd2_rn(vy, s.nvy),
+                 dvz = __fadd2_rn(vz, s.nvz);
+    const float2 dr2 = __ffma2_rn(drx, drx, __ffma2_rn(dry, dry, __fmul2_rn(drz, drz)));
+    const float2 dv2 = __ffma2_rn(dvx, dvx, __ffma2_rn(dvy, dvy, __fmul2_rn(dvz, dvz)));
+    const float2 rdv = __ffma2_rn(drx, dvx, __ffma2_rn(dry, dvy, __fmul2_rn(drz, dvz)));
+    const float2 rinv = make_float2(rsqrtf(dr2.x), rsqrtf(dr2.y));
+    const float2 rinv2 = __fmul2_rn(rinv, rinv);
+    const float2 vdr = __fmul2_rn(rdv, rinv2);
+    const float2 mr1 = __fmul2_rn(__fadd2_rn(s.m, m), rinv);
+    const float2 u = __fmul2_rn(mr1, rinv2);
+    const float2 ru = make_float2(rsqrtf(u.x), rsqrtf(u.y));
+    const float2 r0 = __fmul2_rn(__fmul2_rn(u, ru), f2dup(inv_eta_s2));
+    const float2 b0 = __fmul2_rn(f2dup(1.5f), vdr);
+    const float2 rff =
+        __ffma2_rn(f2dup(-0.5f), make_float2(fminf(b0.x, r0.x), fminf(b0.y, r0.y)), r0);
+    const float2 q = make_float2(rsqrtf(dv2.x), rsqrtf(dv2.y));
+    const float2 r1 = __fmul2_rn(__fmul2_rn(__fmul2_rn(dv2, q), rinv), f2dup(inv_eta));
+    const float2 b1 = __fmul2_rn(vdr, __ffma2_rn(mr1, __fmul2_rn(q, q), f2dup(1.0f)));
+    const float2 rfb =
+        __ffma2_rn(f2dup(-0.5f), make_float2(fminf(b1.x, r1.x), fminf(b1.y, r1.y)), r1);
+    const float inf = __int_as_float(0x7f800000);
+    return make_float2(dr2.x == 0.0f ? inf : fmaxf(rff.x, rfb.x),
+                       dr2.y == 0.0f ? inf : fmaxf(rff.y, rfb.y));
+}
+
 __device__ __forceinline__ float2 rsqrt_nr2(float2 x) {
     const float2 y = make_float2(rsqrtf(x.x), rsqrtf(x.y));
     return __fmul2_rn(y, __ffma2_rn(__fmul2_rn(x, make_float2(-0.5f, -0.5f)), __fmul2_rn(y, y),

@@ -195,11 +195,15 @@ def test_engine_mixed_kick_accelerations_against_oracle(cuda, hhs, oracle, n, ep
 
 @pytest.mark.parametrize("n,eta", [(3000, 0.03), (16384, 0.03), (20000, 0.02)])
 def test_engine_mixed_timesteps_against_oracle(cuda, hhs, oracle, n, eta):
-    """The timestep phase of the device step in mixed precision (members packed, column
-    tiles bulk-copied, one FP32 rate per unordered pair feeding both particles' maxima,
-    tiles unmasked away from the diagonal) over a whole node, against the FP64 timesteps
-    of the oracle: the largest relative difference stays at the FP32 rounding of the pair
-    expression (rsqrtf without a Newton step), far inside the width of a timestep level."""
+    """The timestep phase of the device step in mixed precision (members packed in column
+    pairs, column tiles bulk-copied, one rate per unordered pair in f32x2 arithmetic
+    feeding both particles' maxima, tiles unmasked away from the diagonal) over a whole
+    node, against the FP64 timesteps of the oracle: the largest relative difference stays
+    at the FP32 rounding of the pair expression (rsqrtf without a Newton step), far inside
+    the width of a timestep level. Each lane of the packed arithmetic runs the scalar
+    expression's operations in its order, and a maximum does not depend on the order of
+    its terms, so the result also equals the plain one-thread-per-sink mixed kernel
+    (hhs_timesteps) bit for bit."""
     s = hhs.plummer(n, 900 + n)
     ref = oracle.timesteps(s, eta)
     ctx = hhs.Context(n, 64, eta=eta)
@@ -211,6 +215,10 @@ def test_engine_mixed_timesteps_against_oracle(cuda, hhs, oracle, n, eta):
     rel = np.abs(ts - ref) / ref
     print(f"\nengine timesteps n={n}: max rel {rel.max():.3e} median {np.median(rel):.3e}")
     assert rel.max() < 2e-6, rel.max()
+    plain = hhs.ParticleSystem(n)
+    plain.upload(s)
+    hhs.timesteps(ctx, plain, n, hhs.PREC_MIXED)
+    assert np.array_equal(plain.download()["ts"], ts)
     # a second call on the same context: the rate words were left at zero
     d.upload(s)
     assert hhs.lib().hhs_engine_timestep_rates(ctx.h, d.ref, n, None) == 0
