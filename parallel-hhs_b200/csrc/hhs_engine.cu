@@ -94,9 +94,11 @@ struct EParams {
     unsigned* err;
     // packed kick sources of each grid level (mixed precision): slow particle q of the
     // level's slow list, drifted by half the level's step, as double-single position
-    // (pk_a = hi + mass, pk_b = lo), written by the split, read by bulk copies
-    float4* pk_a;   // [pk_levels][n_max]
-    float4* pk_b;   // [pk_levels][n_max]
+    // in pairs: entry e of a level holds records 2e and 2e + 1 as four float4
+    // (x hi, y hi), (z hi, mass), (x lo, y lo), (z lo, 0), written by the split, read by
+    // bulk copies and unpacked into f32x2 operands
+    float4* pk;             // [pk_levels][pk_stride][4]
+    long long pk_stride;    // pair entries per level
     int pk_levels;
     // the members of the current grid node packed for the mixed timestep, in list order,
     // in pairs: five arrays of tq_stride float4, member 2p + h at component h (and 2 + h)
@@ -181,7 +183,7 @@ struct __align__(16) Smem {
         struct { float4 A[kEB], B[kEB]; } km;                   // mixed kick tiles
         struct { float4 A[kTS], B[kTS]; } kt;                   // grid kick source tile
         struct {                                                  // symmetric kick
-            float4 A[2][kTX], B[2][kTX];
+            float4 T[2][kTX / 2][4];                              // source pairs
             float colw[kEB / 32][kTX][3];
         } kc;
         struct {                                                  // packed timestep tiles
@@ -929,6 +931,29 @@ struct SinkDS {
     float nxh, nyh, nzh, nxl, nyl, nzl;  // negated double-single position
 };
 
+// The packed kick sources of a level, and record q of them.
+__device__ __forceinline__ float4* pk_level(const EParams& E, int lvl) {
+    return E.pk + (size_t)lvl * (size_t)E.pk_stride * 4;
+}
+__device__ __forceinline__ void pk_put(float4* L, int q, const DS& x, const DS& y, const DS& z,
+                                       float m) {
+    float* p = reinterpret_cast<float*>(L + 4 * (size_t)(q >> 1)) + (q & 1);
+    p[0] = x.hi;
+    p[2] = y.hi;
+    p[4] = z.hi;
+    p[6] = m;
+    p[8] = x.lo;
+    p[10] = y.lo;
+    p[12] = z.lo;
+    p[14] = 0.0f;
+}
+// record q as (hi x, y, z, m) and (lo x, y, z, 0)
+__device__ __forceinline__ void pk_get(const float4* L, int q, float4& a, float4& b) {
+    const float* p = reinterpret_cast<const float*>(L + 4 * (size_t)(q >> 1)) + (q & 1);
+    a = make_float4(p[0], p[2], p[4], p[6]);
+    b = make_float4(p[8], p[10], p[12], 0.0f);
+}
+
 __device__ __forceinline__ void kick_pair_nr(const float4 A, const float4 B, const SinkDS& q,
                                              float eps2, float& bx, float& by, float& bz) {
     const float dx = __fadd_rn(__fadd_rn(A.x, q.nxh), __fadd_rn(B.x, q.nxl));
@@ -992,19 +1017,14 @@ __device__ __forceinline__ void kick_span2(const Smem& sm, int lo, int hi, const
     }
 }
 
-// Stages source records [a, b) of the node (slow records [a, min(b, ns)) by bulk copy
-// from the packed arrays, fast ones gathered from the state arrays) into sm.u.kt.
-__device__ void kick_stage_tile(const EParams& E, const int32_t* F, const float4* PA,
-                                const float4* PB, int a, int b, int ns, Smem& sm) {
+// Stages source records [a, b) of the node into sm.u.kt: slow records [a, min(b, ns))
+// from the level's packed pairs, fast ones gathered from the state arrays.
+__device__ void kick_stage_tile(const EParams& E, const int32_t* F, const float4* PK, int a,
+                                int b, int ns, Smem& sm) {
     __syncthreads();  // every thread is done reading the previous tile
     const int sb = min(b, ns);
-    const bool bulk = sb > a;
-    if (bulk && threadIdx.x == 0) {
-        const unsigned bytes = (unsigned)(sb - a) * (unsigned)sizeof(float4);
-        mbar_arrive_expect_tx(&sm.kbar, 2u * bytes);
-        bulk_load(sm.u.kt.A, PA + a, bytes, &sm.kbar);
-        bulk_load(sm.u.kt.B, PB + a, bytes, &sm.kbar);
-    }
+    for (int j = a + (int)threadIdx.x; j < sb; j += kEB)
+        pk_get(PK, j, sm.u.kt.A[j - a], sm.u.kt.B[j - a]);
     const SoA& P = E.P;
     for (int j = max(a, ns) + (int)threadIdx.x; j < b; j += kEB) {
         const int g = F[j - ns];
@@ -1012,13 +1032,7 @@ __device__ void kick_stage_tile(const EParams& E, const int32_t* F, const float4
         sm.u.kt.A[j - a] = make_float4(x.hi, y.hi, z.hi, (float)P.m[g]);
         sm.u.kt.B[j - a] = make_float4(x.lo, y.lo, z.lo, 0.0f);
     }
-    if (bulk && !mbar_wait(&sm.kbar, sm.kphase, E.err)) {
-        // the copy did not complete in time: the error word ends the launch at the next
-        // grid barrier; let the copy land (bounded) before the buffer is reused
-        (void)mbar_wait(&sm.kbar, sm.kphase, nullptr);
-    }
     __syncthreads();
-    if (bulk && threadIdx.x == 0) sm.kphase ^= 1u;
 }
 
 // Work units (sink block ib, source chunk jc) of a node, as up to three rectangles
@@ -1074,8 +1088,7 @@ __device__ void kick_units_grid(const EParams& E, const int32_t* F, int nf, int 
                                 int ib_hi = -1, int part = kUnitsAll) {
     const int ntot = nf + ns;
     const SoA& P = E.P;
-    const float4* PA = E.pk_a + (size_t)lvl * E.n_max;
-    const float4* PB = E.pk_b + (size_t)lvl * E.n_max;
+    const float4* PK = pk_level(E, lvl);
     if (ib_hi < 0) ib_hi = (ntot + kKB - 1) / kKB;
     if (ib_hi <= ib_lo || W.count <= 0) return;
     const UnitGroups grp = kick_unit_groups(nf, ns, nch, C, part, ib_lo, ib_hi);
@@ -1108,7 +1121,8 @@ __device__ void kick_units_grid(const EParams& E, const int32_t* F, int nf, int 
             q[k] = SinkDS{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             if (act) {
                 if (slow) {
-                    const float4 a = PA[sk[k] - nf], b = PB[sk[k] - nf];
+                    float4 a, b;
+                    pk_get(PK, sk[k] - nf, a, b);
                     q[k] = SinkDS{-a.x, -a.y, -a.z, -b.x, -b.y, -b.z};
                 } else {
                     const int g = F[sk[k]];
@@ -1123,7 +1137,7 @@ __device__ void kick_units_grid(const EParams& E, const int32_t* F, int nf, int 
         for (int a = j0; a < j1; a += kTS) {
             const int b = min(j1, a + kTS);
             if (a != res_a || b != res_b) {
-                kick_stage_tile(E, F, PA, PB, a, b, ns, sm);
+                kick_stage_tile(E, F, PK, a, b, ns, sm);
                 res_a = a;
                 res_b = b;
             }
@@ -1188,7 +1202,7 @@ __device__ __forceinline__ KickPlan kick_plan(int nf, int ns, int workers) {
         int c = (3 * workers + per - 1) / per;  // about three units per CTA
         const int cmax = min(kMaxChunks, (ns + 31) / 32);  // at least 32 slow particles a chunk
         c = c < 1 ? 1 : (c > cmax ? cmax : c);
-        p.Cs = (ns + c - 1) / c;
+        p.Cs = ((ns + c - 1) / c + 1) & ~1;  // even: chunks start on whole source pairs
         p.ncs = (ns + p.Cs - 1) / p.Cs;
         p.Rs = 1;
         p.noff = 0;
@@ -1245,23 +1259,22 @@ struct TileCache {
     unsigned phase;      // parities of the buffers' barriers (sm.tbar)
 };
 
-// thread 0: copy records [a, b) into buffer c
-__device__ __forceinline__ void tc_issue(const float4* PA, const float4* PB, int a, int b, int c,
-                                         Smem& sm) {
-    const unsigned bytes = (unsigned)(b - a) * (unsigned)sizeof(float4);
-    mbar_arrive_expect_tx(&sm.tbar[c], 2u * bytes);
-    bulk_load(sm.u.kc.A[c], PA + a, bytes, &sm.tbar[c]);
-    bulk_load(sm.u.kc.B[c], PB + a, bytes, &sm.tbar[c]);
+// thread 0: copy records [a, b) (a even: whole pair entries) into buffer c
+__device__ __forceinline__ void tc_issue(const float4* PK, int a, int b, int c, Smem& sm) {
+    const unsigned bytes = (unsigned)((b - a + 1) >> 1) * (unsigned)(4 * sizeof(float4));
+    mbar_arrive_expect_tx(&sm.tbar[c], bytes);
+    bulk_load(sm.u.kc.T[c], PK + 4 * (size_t)(a >> 1), bytes, &sm.tbar[c]);
 }
 
 // Makes records [a, b) available in buffer c (every thread calls it): copies them unless
 // they are held or on their way, waits for an outstanding copy, and zeroes the records
-// after b up to the next multiple of eight (massless: their pair terms vanish).
-__device__ void tc_use(const EParams& E, const float4* PA, const float4* PB, int a, int b, int c,
-                       TileCache& tc, Smem& sm) {
+// after b up to the next multiple of eight (massless at the origin: their pair terms
+// vanish).
+__device__ void tc_use(const EParams& E, const float4* PK, int a, int b, int c, TileCache& tc,
+                       Smem& sm) {
     if (tc.a[c] != a || tc.b[c] != b) {
         __syncthreads();  // every thread is done with the buffer's previous records
-        if (threadIdx.x == 0) tc_issue(PA, PB, a, b, c, sm);
+        if (threadIdx.x == 0) tc_issue(PK, a, b, c, sm);
         tc.a[c] = a;
         tc.b[c] = b;
         tc.pending[c] = true;
@@ -1273,27 +1286,45 @@ __device__ void tc_use(const EParams& E, const float4* PA, const float4* PB, int
         tc.pending[c] = false;
         const int len = b - a, len8 = (len + 7) & ~7;
         if ((int)threadIdx.x < len8 - len) {
-            sm.u.kc.A[c][len + threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
-            sm.u.kc.B[c][len + threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
+            const int r = len + (int)threadIdx.x;
+            float* q = reinterpret_cast<float*>(sm.u.kc.T[c][r >> 1]) + (r & 1);
+#pragma unroll
+            for (int k = 0; k < 8; k++) q[2 * k] = 0.0f;
         }
         __syncthreads();
     }
 }
 
-// pair vector w = d * r3 (d = source - sink, r3 = 1/|d|^3 with one Newton correction)
-__device__ __forceinline__ void pair_w(const float4 A, const float4 B, const SinkDS& q, float eps2,
-                                       float& wx, float& wy, float& wz) {
-    const float dx = __fadd_rn(__fadd_rn(A.x, q.nxh), __fadd_rn(B.x, q.nxl));
-    const float dy = __fadd_rn(__fadd_rn(A.y, q.nyh), __fadd_rn(B.y, q.nyl));
-    const float dz = __fadd_rn(__fadd_rn(A.z, q.nzh), __fadd_rn(B.z, q.nzl));
-    const float d2 = fmaxf(fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2))), 1e-20f);
-    const float y = rsqrtf(d2);
-    const float y2 = __fmul_rn(y, y);
-    const float c = fmaf(-1.5f, __fmul_rn(d2, y2), 2.5f);
-    const float r3 = __fmul_rn(__fmul_rn(y2, y), c);
-    wx = __fmul_rn(dx, r3);
-    wy = __fmul_rn(dy, r3);
-    wz = __fmul_rn(dz, r3);
+// A sink against a pair entry of sources in f32x2 arithmetic (the sink negated, each
+// value in both lanes); each lane runs the scalar pair operations in their order.
+struct SinkDS2 {
+    float2 nxh, nyh, nzh, nxl, nyl, nzl;
+};
+__device__ __forceinline__ SinkDS2 sink2(const SinkDS& q) {
+    return SinkDS2{f2dup(q.nxh), f2dup(q.nyh), f2dup(q.nzh),
+                   f2dup(q.nxl), f2dup(q.nyl), f2dup(q.nzl)};
+}
+
+// offsets d = source - sink of the entry's two sources, and d2 = |d|^2 + eps^2 (floored)
+__device__ __forceinline__ void pair_d2(const float4& Q0, const float4& Q1, const float4& Q2,
+                                        const float4& Q3, const SinkDS2& q, float eps2,
+                                        float2& dx, float2& dy, float2& dz, float2& d2) {
+    dx = __fadd2_rn(__fadd2_rn(make_float2(Q0.x, Q0.y), q.nxh),
+                    __fadd2_rn(make_float2(Q2.x, Q2.y), q.nxl));
+    dy = __fadd2_rn(__fadd2_rn(make_float2(Q0.z, Q0.w), q.nyh),
+                    __fadd2_rn(make_float2(Q2.z, Q2.w), q.nyl));
+    dz = __fadd2_rn(__fadd2_rn(make_float2(Q1.x, Q1.y), q.nzh),
+                    __fadd2_rn(make_float2(Q3.x, Q3.y), q.nzl));
+    const float2 t = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, f2dup(eps2))));
+    d2 = make_float2(fmaxf(t.x, 1e-20f), fmaxf(t.y, 1e-20f));
+}
+
+// 1/|d|^3 with one Newton correction, per lane
+__device__ __forceinline__ float2 r3_nr2(float2 d2) {
+    const float2 y = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+    const float2 y2 = __fmul2_rn(y, y);
+    const float2 c = __ffma2_rn(f2dup(-1.5f), __fmul2_rn(d2, y2), f2dup(2.5f));
+    return __fmul2_rn(__fmul2_rn(y2, y), c);
 }
 
 // Pair terms of rows [r0, r1) (sinks: the fast list, or the level's packed slow records)
@@ -1308,31 +1339,32 @@ __device__ void kick_pair_block(const EParams& E, const int32_t* F, bool rows_fa
                                 Smem& sm, TileCache& tc, int cb) {
     const SoA& P = E.P;
     const size_t nmx = E.n_max;
-    const float4* PA = E.pk_a + (size_t)lvl * nmx;
-    const float4* PB = E.pk_b + (size_t)lvl * nmx;
+    const float4* PK = pk_level(E, lvl);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const float eps2 = E.eps2f;
     for (int rp = r0; rp < r1; rp += R * kEB) {
         int s[R];
-        SinkDS q[R];
+        SinkDS2 q[R];
         float nmi[R];  // -m_i: the column terms
 #pragma unroll
         for (int r = 0; r < R; r++) {
             s[r] = rp + r * kEB + (int)threadIdx.x;
-            q[r] = SinkDS{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            SinkDS q1{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             nmi[r] = 0.0f;
             if (s[r] < r1) {
                 if (rows_fast) {
                     const int g = F[s[r]];
                     const DS x = ds_split(P.x[g]), y = ds_split(P.y[g]), z = ds_split(P.z[g]);
-                    q[r] = SinkDS{-x.hi, -y.hi, -z.hi, -x.lo, -y.lo, -z.lo};
+                    q1 = SinkDS{-x.hi, -y.hi, -z.hi, -x.lo, -y.lo, -z.lo};
                     nmi[r] = -(float)P.m[g];
                 } else {
-                    const float4 a = PA[s[r]], b = PB[s[r]];
-                    q[r] = SinkDS{-a.x, -a.y, -a.z, -b.x, -b.y, -b.z};
+                    float4 a, b;
+                    pk_get(PK, s[r], a, b);
+                    q1 = SinkDS{-a.x, -a.y, -a.z, -b.x, -b.y, -b.z};
                     nmi[r] = -a.w;
                 }
             }
+            q[r] = sink2(q1);
         }
         float acc[R][3], cmp[R][3];
 #pragma unroll
@@ -1341,36 +1373,50 @@ __device__ void kick_pair_block(const EParams& E, const int32_t* F, bool rows_fa
             for (int k = 0; k < 3; k++) acc[r][k] = cmp[r][k] = 0.0f;
         for (int a = j0; a < j1; a += kTX) {
             const int b = min(j1, a + kTX), len = b - a;
-            tc_use(E, PA, PB, a, b, cb, tc, sm);
-            const float4* TA = sm.u.kc.A[cb];
-            const float4* TB = sm.u.kc.B[cb];
-            float bl[R][3];
+            tc_use(E, PK, a, b, cb, tc, sm);
+            const float4(*T)[4] = sm.u.kc.T[cb];
+            // rows' sums of the even and odd columns in the two lanes
+            float2 bl[R][3];
 #pragma unroll
-            for (int r = 0; r < R; r++) bl[r][0] = bl[r][1] = bl[r][2] = 0.0f;
+            for (int r = 0; r < R; r++) bl[r][0] = bl[r][1] = bl[r][2] = make_float2(0.f, 0.f);
             int nb = 0;
             for (int g8 = 0; g8 < len; g8 += 8) {
-                float v[8][3];
+                float2 v2[4][3];  // column terms of the four entries (eight columns)
 #pragma unroll
-                for (int c = 0; c < 8; c++) {
-                    const float4 A = TA[g8 + c], B = TB[g8 + c];
+                for (int c2 = 0; c2 < 4; c2++) {
+                    const int e = (g8 >> 1) + c2;
+                    const float4 Q0 = T[e][0], Q1 = T[e][1], Q2 = T[e][2], Q3 = T[e][3];
+                    const float2 m = make_float2(Q1.z, Q1.w);
 #pragma unroll
                     for (int r = 0; r < R; r++) {
-                        float wx, wy, wz;
-                        pair_w(A, B, q[r], eps2, wx, wy, wz);
-                        bl[r][0] = fmaf(wx, A.w, bl[r][0]);
-                        bl[r][1] = fmaf(wy, A.w, bl[r][1]);
-                        bl[r][2] = fmaf(wz, A.w, bl[r][2]);
+                        float2 dx, dy, dz, d2;
+                        pair_d2(Q0, Q1, Q2, Q3, q[r], eps2, dx, dy, dz, d2);
+                        const float2 r3 = r3_nr2(d2);
+                        const float2 wx = __fmul2_rn(dx, r3), wy = __fmul2_rn(dy, r3),
+                                     wz = __fmul2_rn(dz, r3);
+                        bl[r][0] = __ffma2_rn(wx, m, bl[r][0]);
+                        bl[r][1] = __ffma2_rn(wy, m, bl[r][1]);
+                        bl[r][2] = __ffma2_rn(wz, m, bl[r][2]);
+                        const float2 nm = f2dup(nmi[r]);
                         if (r == 0) {
-                            v[c][0] = __fmul_rn(wx, nmi[r]);
-                            v[c][1] = __fmul_rn(wy, nmi[r]);
-                            v[c][2] = __fmul_rn(wz, nmi[r]);
+                            v2[c2][0] = __fmul2_rn(wx, nm);
+                            v2[c2][1] = __fmul2_rn(wy, nm);
+                            v2[c2][2] = __fmul2_rn(wz, nm);
                         } else {
-                            v[c][0] = fmaf(wx, nmi[r], v[c][0]);
-                            v[c][1] = fmaf(wy, nmi[r], v[c][1]);
-                            v[c][2] = fmaf(wz, nmi[r], v[c][2]);
+                            v2[c2][0] = __ffma2_rn(wx, nm, v2[c2][0]);
+                            v2[c2][1] = __ffma2_rn(wy, nm, v2[c2][1]);
+                            v2[c2][2] = __ffma2_rn(wz, nm, v2[c2][2]);
                         }
                     }
                 }
+                float v[8][3];
+#pragma unroll
+                for (int c2 = 0; c2 < 4; c2++)
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        v[2 * c2][k] = v2[c2][k].x;
+                        v[2 * c2 + 1][k] = v2[c2][k].y;
+                    }
                 float rs[3];
                 warp_colsum8(v, rs, lane);
                 const int col = ((lane >> 2) & 7);
@@ -1384,8 +1430,8 @@ __device__ void kick_pair_block(const EParams& E, const int32_t* F, bool rows_fa
                     for (int r = 0; r < R; r++)
 #pragma unroll
                         for (int k = 0; k < 3; k++) {
-                            kahan_add(acc[r][k], cmp[r][k], bl[r][k]);
-                            bl[r][k] = 0.0f;
+                            kahan_add(acc[r][k], cmp[r][k], bl[r][k].x + bl[r][k].y);
+                            bl[r][k] = make_float2(0.f, 0.f);
                         }
                     nb = 0;
                 }
@@ -1394,7 +1440,8 @@ __device__ void kick_pair_block(const EParams& E, const int32_t* F, bool rows_fa
 #pragma unroll
                 for (int r = 0; r < R; r++)
 #pragma unroll
-                    for (int k = 0; k < 3; k++) kahan_add(acc[r][k], cmp[r][k], bl[r][k]);
+                    for (int k = 0; k < 3; k++)
+                        kahan_add(acc[r][k], cmp[r][k], bl[r][k].x + bl[r][k].y);
             }
             __syncthreads();
             // the tile's column sums: the CTA's warps in order, then the row passes in order
@@ -1417,34 +1464,45 @@ __device__ void kick_pair_block(const EParams& E, const int32_t* F, bool rows_fa
     }
 }
 
+// One-directional slow unit: the block sb of kEB slow sinks against slow chunk jc, in
+// f32x2 arithmetic over the chunk's source pairs (the even and odd sources' sums in the
+// two lanes, 32 sources a block into the compensated sums).
 __device__ void kick_slow_unit(const EParams& E, int nf, int lvl, const KickPlan& p, int sb,
                                int jc, int ns, Smem& sm, TileCache& tc, int cb) {
     const size_t nmx = E.n_max;
-    const float4* PA = E.pk_a + (size_t)lvl * nmx;
-    const float4* PB = E.pk_b + (size_t)lvl * nmx;
+    const float4* PK = pk_level(E, lvl);
     const int j0 = jc * p.Cs, j1 = min(ns, j0 + p.Cs);
     const int qs = sb * kEB + (int)threadIdx.x;  // slow sink position
     const bool act = qs < ns;
-    SinkDS q{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    SinkDS q1{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (act) {
-        const float4 a = PA[qs], b = PB[qs];
-        q = SinkDS{-a.x, -a.y, -a.z, -b.x, -b.y, -b.z};
+        float4 a, b;
+        pk_get(PK, qs, a, b);
+        q1 = SinkDS{-a.x, -a.y, -a.z, -b.x, -b.y, -b.z};
     }
+    const SinkDS2 q = sink2(q1);
     const float eps2 = E.eps2f;
     float acc[3] = {0.f, 0.f, 0.f}, cmp[3] = {0.f, 0.f, 0.f};
     for (int a = j0; a < j1; a += kTX) {
         const int b = min(j1, a + kTX), len = b - a;
-        tc_use(E, PA, PB, a, b, cb, tc, sm);
-        const float4* TA = sm.u.kc.A[cb];
-        const float4* TB = sm.u.kc.B[cb];
+        tc_use(E, PK, a, b, cb, tc, sm);
+        const float4(*T)[4] = sm.u.kc.T[cb];
         for (int jb = 0; jb < len; jb += 32) {
-            const int je = min(len, jb + 32);
-            float bl[3] = {0.f, 0.f, 0.f};
+            const int ne = (min(len, jb + 32) - jb + 1) >> 1;  // entries of this block
+            float2 bl[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
 #pragma unroll 4
-            for (int j = jb; j < je; j++)
-                kick_pair_nr(TA[j], TB[j], q, eps2, bl[0], bl[1], bl[2]);
+            for (int i = 0; i < ne; i++) {
+                const int e = (jb >> 1) + i;
+                const float4 Q0 = T[e][0], Q1 = T[e][1], Q2 = T[e][2], Q3 = T[e][3];
+                float2 dx, dy, dz, d2;
+                pair_d2(Q0, Q1, Q2, Q3, q, eps2, dx, dy, dz, d2);
+                const float2 mr3 = __fmul2_rn(make_float2(Q1.z, Q1.w), r3_nr2(d2));
+                bl[0] = __ffma2_rn(dx, mr3, bl[0]);
+                bl[1] = __ffma2_rn(dy, mr3, bl[1]);
+                bl[2] = __ffma2_rn(dz, mr3, bl[2]);
+            }
 #pragma unroll
-            for (int k = 0; k < 3; k++) kahan_add(acc[k], cmp[k], bl[k]);
+            for (int k = 0; k < 3; k++) kahan_add(acc[k], cmp[k], bl[k].x + bl[k].y);
         }
     }
     if (act)
@@ -1478,8 +1536,7 @@ __device__ void kick_sym_units(const EParams& E, const int32_t* F, int nf, int n
     const int total = nx + (kinds == 2 ? 0 : plan.nsl);
     if (threadIdx.x == 0) sm.kp = plan;  // read back after each barrier below
     const KickPlan& p = sm.kp;
-    const float4* PA = E.pk_a + (size_t)lvl * E.n_max;
-    const float4* PB = E.pk_b + (size_t)lvl * E.n_max;
+    const float4* PK = pk_level(E, lvl);
     unsigned* ctr = &E.st->kick_ctr[set][lvl];
     TileCache tc;
     tc.a[0] = tc.a[1] = tc.b[0] = tc.b[1] = -1;
@@ -1494,7 +1551,7 @@ __device__ void kick_sym_units(const EParams& E, const int32_t* F, int nf, int n
         int a, b;
         unit_first_tile(p, nx, u, a, b);
         clip(a, b);
-        if (threadIdx.x == 0) tc_issue(PA, PB, a, b, c, sm);
+        if (threadIdx.x == 0) tc_issue(PK, a, b, c, sm);
         tc.a[c] = a; tc.b[c] = b; tc.pending[c] = true;
     }
     while (u < total) {
@@ -1506,7 +1563,7 @@ __device__ void kick_sym_units(const EParams& E, const int32_t* F, int nf, int n
                 int a, b;
                 unit_first_tile(p, nx, un, a, b);
                 clip(a, b);
-                if (tc.a[c ^ 1] != a || tc.b[c ^ 1] != b) tc_issue(PA, PB, a, b, c ^ 1, sm);
+                if (tc.a[c ^ 1] != a || tc.b[c ^ 1] != b) tc_issue(PK, a, b, c ^ 1, sm);
             }
         }
         // one call site per kind of block keeps the inlined pair loops to three copies
@@ -1825,15 +1882,13 @@ __device__ void split_phase(const EParams& E, const int32_t* S, int n, double dt
                 L[i - p] = gi;
                 q = i - p;
             }
-            if (PREC != HHS_PREC_FP64 && q >= 0 && E.pk_a && level < E.pk_levels) {
+            if (PREC != HHS_PREC_FP64 && q >= 0 && E.pk && level < E.pk_levels) {
                 // packed kick source: the slow particle at its drifted kick position
                 const double h = dt * 0.5;
                 const DS x = ds_split(fma(E.P.vx[gi], h, E.P.x[gi]));
                 const DS y = ds_split(fma(E.P.vy[gi], h, E.P.y[gi]));
                 const DS z = ds_split(fma(E.P.vz[gi], h, E.P.z[gi]));
-                const size_t o = (size_t)level * E.n_max + q;
-                E.pk_a[o] = make_float4(x.hi, y.hi, z.hi, (float)E.P.m[gi]);
-                E.pk_b[o] = make_float4(x.lo, y.lo, z.lo, 0.0f);
+                pk_put(pk_level(E, level), q, x, y, z, (float)E.P.m[gi]);
             }
         }
         if (t == ntiles - 1 && threadIdx.x == 0) {
@@ -3041,7 +3096,7 @@ __device__ void mid_hold(const EParams& E, const int32_t* S, int n, int level0, 
 // packed sources at that level, and CTAs outside the first cluster.
 __device__ __forceinline__ bool kick_overlaps(const EParams& E, int lvl, const Workers& W) {
     namespace cg = cooperative_groups;
-    return W.mode == kModeGrid && E.overlap && E.pk_a && lvl < E.pk_levels && !E.packed &&
+    return W.mode == kModeGrid && E.overlap && E.pk && lvl < E.pk_levels && !E.packed &&
            E.prec_mixed && (int)cg::this_cluster().num_blocks() < W.count &&
            ld_volatile_i32(&E.counts[lvl].n_slow) > 0;
 }
@@ -3175,7 +3230,7 @@ __device__ bool run_hold(const EParams& E, int top, bool top_calc, const Workers
             if (ns > 0) {
                 const int ntot = nf + ns;
                 const bool grid_tma = MODE == kModeGrid && PREC != HHS_PREC_FP64 && !E.packed &&
-                                      E.pk_a && lvl < E.pk_levels;
+                                      E.pk && lvl < E.pk_levels;
                 const bool x2 = PREC != HHS_PREC_FP64 && E.packed;
                 const int blk = (x2 || grid_tma) ? 2 * kEB : kEB;
                 const int nch = chunks_for(ntot, W, PREC != HHS_PREC_FP64, E.units_per_cta, blk);
@@ -3286,8 +3341,7 @@ __global__ void __launch_bounds__(kEB, 2) k_engine_accel(EParams E) {
             const int q = (i / 3) * 2 + (i % 3) - 1;
             L[q] = i;
             const DS x = ds_split(E.P.x[i]), y = ds_split(E.P.y[i]), z = ds_split(E.P.z[i]);
-            E.pk_a[q] = make_float4(x.hi, y.hi, z.hi, (float)E.P.m[i]);
-            E.pk_b[q] = make_float4(x.lo, y.lo, z.lo, 0.0f);
+            pk_put(E.pk, q, x, y, z, (float)E.P.m[i]);
         }
     }
     if (W.id == 0 && threadIdx.x == 0) E.st->kick_ctr[0][0] = 0u;
@@ -3418,9 +3472,7 @@ __global__ void k_pack_slow(EParams E, const int32_t* L, int ns, int lvl) {
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < ns; q += gridDim.x * blockDim.x) {
         const int g = L[q];
         const DS x = ds_split(E.P.x[g]), y = ds_split(E.P.y[g]), z = ds_split(E.P.z[g]);
-        const size_t o = (size_t)lvl * E.n_max + q;
-        E.pk_a[o] = make_float4(x.hi, y.hi, z.hi, (float)E.P.m[g]);
-        E.pk_b[o] = make_float4(x.lo, y.lo, z.lo, 0.0f);
+        pk_put(pk_level(E, lvl), q, x, y, z, (float)E.P.m[g]);
     }
 }
 
@@ -3587,8 +3639,8 @@ struct EngineHost {
     unsigned* rate_acc = nullptr;
     unsigned long long* tile_status = nullptr;
     int n_max = 0;
-    float4* pk_a = nullptr;
-    float4* pk_b = nullptr;
+    float4* pk = nullptr;
+    long long pk_stride = 0;
     int pk_levels = 0;
     double* c_part = nullptr;
     float4* tq = nullptr;
@@ -3612,7 +3664,7 @@ size_t engine_workspace_bytes(int n_max, int max_levels) {
     return al(sizeof(EngineState)) + al(sizeof(double) * kMaxChunks * n) +
            al(sizeof(double) * kMaxChunks * 3 * n) + al(sizeof(int) * (n / kEB + 2)) +
            al(sizeof(unsigned) * n) + al(sizeof(unsigned long long) * (n / kEB + 2)) +
-           2 * al(sizeof(float4) * n * (size_t)pk_levels_for(max_levels)) +
+           al(sizeof(float4) * 4 * (n / 2 + 1) * (size_t)pk_levels_for(max_levels)) +
            al(sizeof(double) * kMaxFsb * 3 * n) + al(sizeof(float4) * 5 * (n / 2 + 1));
 }
 
@@ -3629,8 +3681,9 @@ hhs_status engine_init(hhs_ctx* c, void* base) {
     eh->tile_status = reinterpret_cast<unsigned long long*>(p);
     p += al(sizeof(unsigned long long) * (n / kEB + 2));
     eh->pk_levels = pk_levels_for(c->max_levels);
-    eh->pk_a = reinterpret_cast<float4*>(p); p += al(sizeof(float4) * n * (size_t)eh->pk_levels);
-    eh->pk_b = reinterpret_cast<float4*>(p); p += al(sizeof(float4) * n * (size_t)eh->pk_levels);
+    eh->pk_stride = (long long)(n / 2 + 1);
+    eh->pk = reinterpret_cast<float4*>(p);
+    p += al(sizeof(float4) * 4 * (size_t)eh->pk_stride * (size_t)eh->pk_levels);
     eh->c_part = reinterpret_cast<double*>(p); p += al(sizeof(double) * kMaxFsb * 3 * n);
     eh->tq = reinterpret_cast<float4*>(p);
     eh->tq_stride = (long long)(n / 2 + 1);
@@ -3850,8 +3903,8 @@ EParams engine_params(hhs_ctx* c, EngineHost* eh, const SoA& P, int n, double dt
     E.rate_acc = eh->rate_acc;
     E.st = eh->st;
     E.err = c->err;
-    E.pk_a = eh->pk_a;
-    E.pk_b = eh->pk_b;
+    E.pk = eh->pk;
+    E.pk_stride = eh->pk_stride;
     E.pk_levels = eh->pk_levels;
     E.prec_mixed = 0;
     E.overlap = eh->overlap;
@@ -4230,7 +4283,8 @@ extern "C" hhs_status hhs_hold_batched(hhs_batch* b, hhs_particle_system* sys, d
     E.rate_acc = nullptr;
     E.st = nullptr;
     E.err = b->d_err;
-    E.pk_a = E.pk_b = nullptr;
+    E.pk = nullptr;
+    E.pk_stride = 0;
     E.pk_levels = 0;
     E.prec_mixed = pi;
     E.overlap = 0;
