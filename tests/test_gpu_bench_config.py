@@ -190,7 +190,10 @@ def test_engine_mixed_kick_accelerations_against_oracle(cuda, hhs, oracle, n, ep
     # the summation error bound: relative to the sum of the pair terms' magnitudes (a
     # particle whose pulls nearly cancel has a small |a| but the same absolute error)
     assert err_s.max() < 5e-7, err_s.max()
-    assert err.max() < 2e-6 and np.median(err) < 1e-7, (err.max(), np.median(err))
+    # relative to |a| itself where the pulls do not cancel much (|a| at least a quarter of
+    # the sum of magnitudes)
+    weak = amag >= 0.25 * smag
+    assert err[weak].max() < 1e-6 and np.median(err) < 1e-7, (err[weak].max(), np.median(err))
 
 
 @pytest.mark.parametrize("n,eta", [(3000, 0.03), (16384, 0.03), (20000, 0.02)])
