@@ -284,7 +284,10 @@ hhs_status hhs_ipc_close(hhs_particle_system* view);
 
 /* Exact exclusive prefix sum of int32 values (the contract of
  * scan_predicate_small/large, src/split.cuh:438-565): one decoupled-lookback pass below
- * 2^22 values, two passes over chunks (chunk sums, then chunk scans) from there on.
+ * 2^22 values, two passes over chunks (chunk sums, then chunk scans) up to 2^25, and from
+ * 2^25 values (16-byte aligned input and output) one streamed pass: a cooperative launch
+ * of resident CTAs that bulk-copy chunks into shared memory and exchange chunk
+ * aggregates two rounds ahead (unaligned pointers keep the two-pass form).
  * d_workspace: hhs_scan_workspace_size(n) bytes of device memory (need not be zeroed;
  * the call clears what it uses). */
 size_t hhs_scan_workspace_size(int64_t n);
@@ -294,7 +297,8 @@ hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out, int64_t n
  * callers that must not allocate device memory -- an application that has handed the
  * device to its own memory pool, or a step loop that must run under a fixed device-memory
  * budget -- and so cannot provide the workspace hhs_scan_exclusive_i32 needs. The same
- * kernel runs with its workspace in a fixed 128.3 KiB array inside the library's own
+ * kernels (the single pass below 2^22 values, the two-pass form up to 2^25, the streamed
+ * pass above) run with their workspace in a fixed 128.3 KiB array inside the library's own
  * device memory, present on every device that loads the library until the process
  * exits. Limit: n <= HHS_SCAN_NOALLOC_MAX_N (2^26 values); larger n returns
  * HHS_ERR_CAPACITY. The call allocates nothing; it clears the part of the array it uses

@@ -5,6 +5,7 @@
 
 #include "hhs_scan.cuh"
 #include "hhs_kernels.h"
+#include "hhs_tma.cuh"
 
 namespace {
 
@@ -68,7 +69,9 @@ __global__ void __launch_bounds__(kScanBlock, 6)
 // two steps over contiguous chunks of whole tiles, one chunk per CTA: sum the chunk,
 // then scan it from the sum of the chunks before it.
 //  - Two-kernel form: a chunk-sum kernel and a chunk-scan kernel over the whole input,
-//    12 bytes of DRAM traffic per value. The default for the scan (4.25 TB/s at 2^28).
+//    12 bytes of DRAM traffic per value. The default for the scan from 2^22 values up to
+//    the streamed pass below (4.25 TB/s at 2^28, where the streamed pass reaches 5.0), and
+//    for unaligned inputs.
 //  - Wave form: one cooperative launch walks the input in waves of 2^24 values (64 MB,
 //    half of L2). Per wave every CTA sums its chunk, the grid meets at a counting
 //    barrier, and every CTA scans its chunk while most of it is still in L2. Each CTA
@@ -460,6 +463,359 @@ int scan_variant() {
     return v;
 }
 
+// ---- streamed single pass
+// One cooperative launch of persistent CTAs (every CTA resident). CTA b owns chunks
+// b, b + G, b + 2G, ... (G CTAs, chunks of BLOCK x VPT values), so round r is the chunks
+// [rG, rG + G). A chunk's exclusive prefix is the running total of the rounds before it
+// plus the aggregates of the chunks before it in its round. Every CTA publishes the
+// aggregate of its chunk two rounds ahead, as soon as that chunk is in shared memory, and
+// warp 0 reads all aggregates of the next round while the other warps store the current
+// one: their sum over the chunks before its own is its prefix within the round, and their
+// sum over the round carries the running total, which every CTA keeps itself. No chain
+// of inclusive prefixes runs through the grid (with a decoupled look-back over chunks of
+// this size, that chain of L2 round trips held the same data path to 1.9 TB/s), and a CTA
+// waits only when another is more than a round behind.
+// Data: a CTA keeps STAGES chunks in flight. When its threads have read a chunk out of
+// shared memory, thread 0 bulk-copies (cp.async.bulk, completing on an mbarrier) the
+// chunk STAGES rounds ahead into the freed buffer. Values are scanned in registers and
+// stored from registers with 16-byte streaming stores; input and output must be 16-byte
+// aligned. The bulk copy of the last chunk stops at a multiple of 4 values; the last
+// n mod 4 values are read with plain loads. Status words (one per chunk) carry the
+// call's epoch and the chunk's aggregate.
+
+// Internal status of launch_stream: the device cannot take the cooperative launch.
+constexpr hhs_status kStreamUnavailable = static_cast<hhs_status>(-1);
+
+template <int BLOCK, int VPT, int STAGES>
+struct StreamShape {
+    static constexpr int CHUNK = BLOCK * VPT;  // values per chunk
+    static constexpr size_t SMEM = (size_t)STAGES * CHUNK * sizeof(int32_t);
+    static_assert(CHUNK % 4 == 0 && CHUNK * 4 < (1 << 20), "chunk bytes within one phase");
+    static_assert(BLOCK % 32 == 0 && BLOCK + 32 <= 1024 && VPT % 4 == 0, "launch shape");
+    static_assert(STAGES >= 3, "aggregates are published two rounds ahead");
+};
+
+// values of the chunk starting at `base` that its bulk copy delivers (a multiple of 4)
+__device__ __forceinline__ long long stream_bulk_values(long long base, long long n,
+                                                        int chunk) {
+    const long long r = n - base;
+    return (r < chunk ? r : (long long)chunk) & ~3LL;
+}
+
+// FLAGS: scan (flag != 0), store the scan to `out` when it is not null, the index of every
+// nonzero flag to idx_out[scan], and the number of them to *count (by the CTA that holds
+// the last chunk). Requires gridDim.x <= num_chunks.
+template <int BLOCK, int VPT, int STAGES, int MINB, bool FLAGS>
+__global__ void __launch_bounds__(BLOCK + 32, MINB)
+    k_scan_stream(const int32_t* __restrict__ in, int32_t* __restrict__ out, long long n,
+                  ScanHeader* hdr, unsigned long long* status, int num_chunks,
+                  int32_t* __restrict__ idx_out, int32_t* __restrict__ count) {
+    constexpr int CHUNK = StreamShape<BLOCK, VPT, STAGES>::CHUNK;
+    constexpr int WARPS = BLOCK / 32, GROUPS = VPT / 4;
+    extern __shared__ __align__(128) int4 s_buf[];  // STAGES x CHUNK/4
+    __shared__ __align__(8) uint64_t s_bar[STAGES];
+    // parity-indexed by round: a warp can be one round ahead of the slowest
+    __shared__ unsigned s_warp[2][WARPS], s_red[2][WARPS], s_prefix[2];
+    __shared__ unsigned s_epoch, s_limit;
+    __shared__ int s_issued;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int G = (int)gridDim.x, b = (int)blockIdx.x;
+    const int rounds = (num_chunks - b + G - 1) / G;  // chunks of this CTA
+    auto chunk_of = [&](int r) { return (long long)b + (long long)r * G; };
+
+    const bool coord = warp == WARPS;  // the coordinator warp (holds no values)
+    // coordinator lane 0: start the copy of round r's chunk into its buffer
+    auto issue = [&](int r) {
+        if (r >= rounds) return;
+        const int slot = r % STAGES;
+        const long long base = chunk_of(r) * CHUNK;
+        const unsigned bytes = (unsigned)(stream_bulk_values(base, n, CHUNK) * 4);
+        mbar_arrive_expect_tx(&s_bar[slot], bytes);
+        if (bytes) bulk_load(s_buf + (size_t)slot * (CHUNK / 4), in + base, bytes, &s_bar[slot]);
+        s_issued = r + 1;
+    };
+    // every thread: round r's copy has landed (false: it did not within the poll limit)
+    auto wait_round = [&](int r) {
+        return mbar_wait(&s_bar[r % STAGES], (unsigned)(r / STAGES) & 1u, &hdr->error);
+    };
+    // this thread's group g (4 consecutive values) of round r's chunk; 0 past n
+    auto group = [&](int r, int g, unsigned (&q)[4]) {
+        const long long base = chunk_of(r) * CHUNK;
+        const long long bulk_end = base + stream_bulk_values(base, n, CHUNK);
+        const int o = warp * (32 * VPT) + g * 128 + lane * 4;
+        const long long e = base + o;
+        const int4 w = s_buf[(size_t)(r % STAGES) * (CHUNK / 4) + (o >> 2)];
+        q[0] = (unsigned)w.x; q[1] = (unsigned)w.y; q[2] = (unsigned)w.z; q[3] = (unsigned)w.w;
+        if (e + 4 > bulk_end) {  // the last chunk's tail
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (e + k >= bulk_end) q[k] = e + k < n ? (unsigned)__ldg(in + e + k) : 0u;
+        }
+        if (FLAGS) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) q[k] = q[k] != 0u;
+        }
+    };
+    // this thread's share of the aggregate of round r's chunk, summed over the warp
+    auto warp_aggregate = [&](int r) {
+        unsigned t = 0u;
+#pragma unroll
+        for (int g = 0; g < GROUPS; g++) {
+            unsigned q[4];
+            group(r, g, q);
+            t += q[0] + q[1] + q[2] + q[3];
+        }
+        return (unsigned)warp_sum((int)t);
+    };
+
+    // coordinator: the aggregates of round r's chunks, summed over those before this CTA's
+    // chunk and over all of them (batches of 8 words per lane, loads of a batch in flight
+    // together; a word that stays unpublished past the poll limit records a timeout)
+    auto poll_round = [&](int r, unsigned epoch, unsigned limit, unsigned& before,
+                          unsigned& all) {
+        const long long r0 = (long long)r * G;
+        const int cnt = (int)min((long long)G, (long long)num_chunks - r0);
+        before = 0u;
+        all = 0u;
+        for (int k0 = 0; k0 < cnt; k0 += 8 * 32) {
+            unsigned long long sw[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int k = k0 + i * 32 + lane;
+                sw[i] = k < cnt ? ld_relaxed_u64(&status[r0 + k]) : 0ull;
+            }
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int k = k0 + i * 32 + lane;
+                if (k >= cnt) continue;
+                for (unsigned spins = 0;
+                     (unsigned)(sw[i] >> 34) != epoch || ((sw[i] >> 32) & 3u) == 0u; spins++) {
+                    if (spins >= limit) {
+                        atomicOr(&hdr->error, HHS_ERRBIT_LOOKBACK_TIMEOUT);
+                        sw[i] = 0ull;
+                        break;
+                    }
+                    if (spins > 64) __nanosleep(64);
+                    sw[i] = ld_relaxed_u64(&status[r0 + k]);
+                }
+                all += (unsigned)sw[i];
+                before += k < b ? (unsigned)sw[i] : 0u;
+            }
+        }
+        before = (unsigned)warp_sum((int)before);
+        all = (unsigned)warp_sum((int)all);
+    };
+    // coordinator: publish the aggregate of round r's chunk from the data warps' shares
+    auto publish = [&](int r, const unsigned* red, unsigned epoch) {
+        const unsigned a = (unsigned)warp_sum((int)(lane < WARPS ? red[lane] : 0u));
+        if (lane == 0) st_relaxed_u64(&status[chunk_of(r)], scan_pack(epoch, 1u, a));
+    };
+
+    if (coord && lane == 0) {
+        s_epoch = scan_next_epoch(hdr);
+        const unsigned lim = *reinterpret_cast<volatile const unsigned*>(&hdr->spin_limit);
+        s_limit = lim ? lim : HHS_SPIN_LIMIT;
+        s_issued = 0;
+#pragma unroll
+        for (int k = 0; k < STAGES; k++) mbar_init(&s_bar[k], 1u);
+        fence_barrier_init();
+#pragma unroll 1
+        for (int r = 0; r < STAGES; r++) issue(r);
+    }
+    __syncthreads();
+    const unsigned epoch = s_epoch, limit = s_limit;
+    // Aggregates are published two rounds ahead, and the coordinator reads round r + 1's
+    // while the data warps store round r and read round r + 1: the prefix of a round is
+    // known when the round starts, and the L2 round trips of the coordinator overlap the
+    // data warps' work.
+    int waited = 0;       // rounds whose copies every data thread has seen land
+    unsigned carry = 0u;  // coordinator: the total of the rounds read so far
+    {
+        bool ok = true;
+        if (!coord) {
+            ok = wait_round(0);
+            unsigned t = warp_aggregate(0);
+            if (lane == 0) s_red[0][warp] = t;
+            if (rounds > 1) {
+                ok = wait_round(1) && ok;
+                t = warp_aggregate(1);
+                if (lane == 0) s_red[1][warp] = t;
+            }
+        }
+        if (__syncthreads_and(ok)) {
+            waited = rounds > 1 ? 2 : 1;
+            if (coord) {
+                publish(0, s_red[0], epoch);
+                if (rounds > 1) publish(1, s_red[1], epoch);
+                unsigned before, all;
+                poll_round(0, epoch, limit, before, all);
+                if (lane == 0) s_prefix[0] = before;
+                if (FLAGS && count && lane == 0 && chunk_of(0) == num_chunks - 1)
+                    *count = (int)all;
+                carry = all;
+            }
+        }
+        __syncthreads();
+    }
+    for (int r = 0; r < rounds && waited > r; r++) {
+        const int p = r & 1;  // also the parity of round r + 2
+        const bool has2 = r + 2 < rounds;
+        bool ok = true;
+        unsigned v[VPT], cb[GROUPS];
+        if (!coord) {
+            // the aggregate of the chunk two rounds ahead
+            if (has2) {
+                ok = wait_round(r + 2);
+                const unsigned t = warp_aggregate(r + 2);
+                if (lane == 0) s_red[p][warp] = t;
+            }
+            // this chunk: values, scans within each 128-value group and over the warp
+            unsigned run = 0u;
+#pragma unroll
+            for (int g = 0; g < GROUPS; g++) {
+                unsigned q[4];
+                group(r, g, q);
+                v[4 * g] = q[0]; v[4 * g + 1] = q[1]; v[4 * g + 2] = q[2]; v[4 * g + 3] = q[3];
+                const unsigned sg = q[0] + q[1] + q[2] + q[3];
+                const unsigned inc = (unsigned)warp_incl_scan((int)sg, lane);
+                cb[g] = run + inc - sg;
+                run += (unsigned)__shfl_sync(HHS_FULL_MASK, (int)inc, 31);
+            }
+            if (lane == 0) s_warp[p][warp] = run;
+        }
+        // every data thread has read this chunk's buffer and agrees whether the copy landed
+        if (!__syncthreads_and(ok)) break;
+        if (has2) waited = r + 3;
+        if (coord) {
+            if (lane == 0) issue(r + STAGES);
+            if (has2) publish(r + 2, s_red[p], epoch);
+            const unsigned wt = lane < WARPS ? s_warp[p][lane] : 0u;
+            const unsigned wi = (unsigned)warp_incl_scan((int)wt, lane);
+            if (lane < WARPS) s_warp[p][lane] = wi - wt;
+        }
+        __syncthreads();
+        if (coord) {
+            if (r + 1 < rounds) {
+                unsigned before, all;
+                poll_round(r + 1, epoch, limit, before, all);
+                if (lane == 0) s_prefix[p ^ 1] = carry + before;
+                if (FLAGS && count && lane == 0 && chunk_of(r + 1) == num_chunks - 1)
+                    *count = (int)(carry + all);
+                carry += all;
+            }
+            continue;
+        }
+        const unsigned wbase = s_prefix[p] + s_warp[p][warp];
+        const long long base = chunk_of(r) * CHUNK;
+#pragma unroll
+        for (int g = 0; g < GROUPS; g++) {
+            const long long e = base + warp * (32 * VPT) + g * 128 + lane * 4;
+            const unsigned p0 = wbase + cb[g], p1 = p0 + v[4 * g], p2 = p1 + v[4 * g + 1],
+                           p3 = p2 + v[4 * g + 2];
+            if (!FLAGS || out) {
+                if (e + 4 <= n) {
+                    __stcs(reinterpret_cast<int4*>(out + e),
+                           make_int4((int)p0, (int)p1, (int)p2, (int)p3));
+                } else {
+                    if (e < n) out[e] = (int)p0;
+                    if (e + 1 < n) out[e + 1] = (int)p1;
+                    if (e + 2 < n) out[e + 2] = (int)p2;
+                }
+            }
+            if (FLAGS) {
+                if (v[4 * g]) idx_out[p0] = (int)e;
+                if (v[4 * g + 1]) idx_out[p1] = (int)(e + 1);
+                if (v[4 * g + 2]) idx_out[p2] = (int)(e + 2);
+                if (v[4 * g + 3]) idx_out[p3] = (int)(e + 3);
+            }
+        }
+    }
+    // A copy that did not land in time ended the loop early: wait once more (bounded) for
+    // the copies this CTA still has in flight before its shared memory goes away. On the
+    // normal exit every issued copy has been waited for.
+    __syncthreads();
+    if (coord && lane == 0) {
+        for (int j = waited; j < s_issued; j++)
+            if (!wait_round(j)) break;
+    }
+}
+
+// One streamed scan: clears the header and the status words it uses, then launches as
+// many persistent CTAs as are resident on the device at once (at most one per chunk) as
+// one cooperative launch. Returns kStreamUnavailable, with nothing queued after the
+// header clear, when the device cannot take the cooperative launch; the caller then uses
+// the tiled scan.
+template <int BLOCK, int VPT, int STAGES, int MINB, bool FLAGS>
+hhs_status launch_stream(const int32_t* in, int32_t* out, long long n, void* ws,
+                         size_t ws_bytes, int32_t* idx_out, int32_t* count, cudaStream_t s) {
+    using Shape = StreamShape<BLOCK, VPT, STAGES>;
+    auto* kern = k_scan_stream<BLOCK, VPT, STAGES, MINB, FLAGS>;
+    const long long chunks = (n + Shape::CHUNK - 1) / Shape::CHUNK;
+    const size_t used = sizeof(ScanHeader) + (size_t)chunks * sizeof(unsigned long long);
+    if (used > ws_bytes || chunks > 0x7fffffffLL) return HHS_ERR_INVALID_ARG;
+    static int resident[64] = {0};  // per device: CTAs resident at once (-1: none)
+    int dev = 0;
+    HHS_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return kStreamUnavailable;
+    if (resident[dev] == 0) {
+        int sms = 0, per = 0, coop = 0;
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)Shape::SMEM) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, BLOCK + 32, Shape::SMEM) !=
+                cudaSuccess) {
+            (void)cudaGetLastError();
+            per = 0;
+        }
+        resident[dev] = (coop && per > 0 && sms > 0) ? sms * per : -1;
+    }
+    if (resident[dev] < 0) return kStreamUnavailable;
+    const int grid = (int)(chunks < resident[dev] ? chunks : resident[dev]);
+    HHS_CUDA_TRY(cudaMemsetAsync(ws, 0, used, s));
+    auto* hdr = static_cast<ScanHeader*>(ws);
+    auto* status = reinterpret_cast<unsigned long long*>(static_cast<char*>(ws) +
+                                                         sizeof(ScanHeader));
+    int nch = (int)chunks;
+    void* args[] = {(void*)&in,  (void*)&out,    (void*)&n,       (void*)&hdr,
+                    (void*)&status, (void*)&nch, (void*)&idx_out, (void*)&count};
+    const cudaError_t e = cudaLaunchCooperativeKernel((const void*)kern, dim3(grid),
+                                                      dim3(BLOCK + 32), args, Shape::SMEM, s);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        return kStreamUnavailable;
+    }
+    HHS_LAUNCH_CHECK();
+    return HHS_OK;
+}
+
+// Launch shapes of the streamed scan (threads, values per thread, stages, CTAs per SM).
+// Shape 0 is the default; HHS_SCAN_VARIANT 20 + k selects shape k at every size.
+constexpr int kStreamShapes = 5;
+// The streamed form is the default scan of aligned inputs of at least kStreamMinN values
+// (below that the pipeline's fill and drain cost more than the look-back form saves), in
+// shape kStreamDefaultShape: at 2^28 values 5.0 TB/s against 4.25 for the two-kernel
+// form, at 2^26 4.35 against 3.87; at 2^24 2.8 against 3.3.
+constexpr long long kStreamMinN = 1LL << 25;
+constexpr int kStreamDefaultShape = 3;
+template <bool FLAGS>
+hhs_status launch_stream_shape(int shape, const int32_t* in, int32_t* out, long long n,
+                               void* ws, size_t ws_bytes, int32_t* idx_out, int32_t* count,
+                               cudaStream_t s) {
+    switch (shape) {
+        case 1:  // 72 KiB chunks, 3 stages
+            return launch_stream<512, 36, 3, 1, FLAGS>(in, out, n, ws, ws_bytes, idx_out, count, s);
+        case 2:  // 50 KiB chunks, 4 stages, 640 data threads
+            return launch_stream<640, 20, 4, 1, FLAGS>(in, out, n, ws, ws_bytes, idx_out, count, s);
+        case 3:  // 48 KiB chunks, 4 stages, 768 data threads
+            return launch_stream<768, 16, 4, 1, FLAGS>(in, out, n, ws, ws_bytes, idx_out, count, s);
+        case 4:  // 48 KiB chunks, 4 stages
+            return launch_stream<512, 24, 4, 1, FLAGS>(in, out, n, ws, ws_bytes, idx_out, count, s);
+        default:  // 64 KiB chunks, 3 stages, 512 data threads and a coordinator warp
+            return launch_stream<512, 32, 3, 1, FLAGS>(in, out, n, ws, ws_bytes, idx_out, count, s);
+    }
+}
+
 // Stream compaction of int32 flags: the indices of the nonzero flags, in order, go to
 // idx_out[scan]; the exclusive scan of (flag != 0) optionally goes to scan_out; the last
 // CTA writes the number of selected elements to *count.
@@ -652,7 +1008,14 @@ extern "C" hhs_status hhs_scan_exclusive_i32(const int32_t* d_in, int32_t* d_out
                                                          sizeof(ScanHeader));
     const bool vec = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) &
                       15u) == 0;
-    if ((variant == 0 || variant >= 11) && n >= kTwoPassMinN) {
+    const bool stream_variant = variant >= 20 && variant < 20 + kStreamShapes;
+    if (vec && (stream_variant || (variant == 0 && n >= kStreamMinN))) {
+        const int shape = stream_variant ? variant - 20 : kStreamDefaultShape;
+        const hhs_status st = launch_stream_shape<false>(shape, d_in, d_out, n, d_workspace,
+                                                         workspace_bytes, nullptr, nullptr, s);
+        if (st != kStreamUnavailable) return st;
+    }
+    if ((variant == 0 || (variant >= 11 && variant <= 13)) && n >= kTwoPassMinN) {
         // the chunk sums are written before they are read: only the header is cleared.
         // Default: the two-kernel form; variants 11-13: waves of 2^22, 2^23, 2^24 values.
         const long long wave = variant == 11   ? (1LL << 22)
@@ -710,6 +1073,13 @@ extern "C" hhs_status hhs_compact_flags_i32(const int32_t* d_flags, int32_t* d_s
                                                          sizeof(ScanHeader));
     const bool vec = ((reinterpret_cast<uintptr_t>(d_flags) |
                        reinterpret_cast<uintptr_t>(d_scan)) & 15u) == 0;
+    const int variant = scan_variant();
+    if (vec && variant >= 20 && variant < 20 + kStreamShapes) {
+        const hhs_status st = launch_stream_shape<true>(variant - 20, d_flags, d_scan, n,
+                                                        d_workspace, workspace_bytes, d_idx,
+                                                        d_count, s);
+        if (st != kStreamUnavailable) return st;
+    }
     if (n >= kTwoPassMinN) {
         auto* agg = reinterpret_cast<unsigned*>(status);
         const size_t words =
@@ -774,14 +1144,30 @@ extern "C" hhs_status hhs_scan_exclusive_i32_noalloc(const int32_t* d_in, int32_
     if (st != HHS_OK) return st;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int tiles = (int)((n + ScanT::TILE - 1) / ScanT::TILE);
-    // the array keeps the previous call's contents: clear the header and the status words
-    // this call uses
-    HHS_CUDA_TRY(cudaMemsetAsync(ws, 0, scan_workspace_bytes(n, ScanT::TILE), s));
     auto* hdr = static_cast<ScanHeader*>(ws);
     auto* status = reinterpret_cast<unsigned long long*>(static_cast<char*>(ws) +
                                                          sizeof(ScanHeader));
     const bool vec = ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) &
                       15u) == 0;
+    // The forms of the allocating scan, each within the array: the streamed form (status
+    // words of its chunks), the two-kernel form (chunk sums), the single pass (a status
+    // word per tile). Each clears the part of the array it uses, which still holds the
+    // previous call's contents.
+    if (vec && n >= kStreamMinN) {
+        st = launch_stream_shape<false>(kStreamDefaultShape, d_in, d_out, n, ws, kStaticScanBytes,
+                                        nullptr, nullptr, s);
+        if (st != kStreamUnavailable) return st;
+    }
+    if (n >= kTwoPassMinN) {
+        HHS_CUDA_TRY(cudaMemsetAsync(ws, 0, sizeof(ScanHeader), s));
+        auto* agg = reinterpret_cast<unsigned*>(status);
+        const size_t words = (kStaticScanBytes - sizeof(ScanHeader)) / sizeof(unsigned);
+        return vec ? launch_large<true, false>(d_in, d_out, n, hdr, agg, words, nullptr, nullptr,
+                                               s, 0)
+                   : launch_large<false, false>(d_in, d_out, n, hdr, agg, words, nullptr,
+                                                nullptr, s, 0);
+    }
+    HHS_CUDA_TRY(cudaMemsetAsync(ws, 0, scan_workspace_bytes(n, ScanT::TILE), s));
     if (vec)
         k_scan_exclusive_i32<true, false><<<tiles, kScanBlock, 0, s>>>(d_in, d_out, n, hdr,
                                                                        status, tiles);

@@ -114,7 +114,7 @@ def test_scan_matches_golden_reference_test_inputs(cuda, hhs):
 
 @pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 127, 4095, 4096, 4097, 8191, 65536 + 3,
                                (1 << 20) + 7, (1 << 22) + 5, (1 << 23) + 4099,
-                               (1 << 24), (1 << 25) + 4099])
+                               (1 << 24), (1 << 25) + 4099, (1 << 26) + 3])
 @pytest.mark.parametrize("offset", [0, 1])
 def test_scan_random_values_sizes_alignment(cuda, hhs, oracle, n, offset):
     torch = cuda
@@ -158,6 +158,66 @@ def test_large_scan_forms_carry_the_running_total(cuda, variant):
     import sys
     from conftest import PKG
     r = subprocess.run([sys.executable, "-c", _SUPER_CHUNK_CHECK, PKG], capture_output=True,
+                       text=True, timeout=600, env={**os.environ, "HHS_SCAN_VARIANT": variant})
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-2000:]
+
+
+_STREAM_CHECK = r"""
+import ctypes, sys
+import numpy as np
+import torch
+sys.path.insert(0, sys.argv[1])
+import hhs
+def P(t):
+    return ctypes.c_void_p(t.data_ptr())
+rng = np.random.default_rng(23)
+# ragged tails (n mod 4 != 0), fewer values than one chunk, more chunks than resident CTAs
+sizes = [1, 3, 4, 5, 4099, 16384, 65536 + 6, (1 << 22) + 7, 148 * 3 * 16384 + 4097,
+         (1 << 24) + 2]
+wb = hhs.scan_workspace_size(max(sizes))
+ws = torch.empty(wb, dtype=torch.uint8, device="cuda")
+for n in sizes:
+    a = rng.integers(-1000, 1000, n).astype(np.int32)
+    ref = np.zeros(n, np.int64)
+    ref[1:] = np.cumsum(a, dtype=np.int64)[:-1]
+    ref = ref.astype(np.int32)
+    dev = torch.from_numpy(a).cuda()
+    out = torch.full_like(dev, -7)
+    for _ in range(2):
+        hhs.scan_exclusive_i32(P(dev), P(out), n, P(ws), wb, None)
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), ref), ("scan", n)
+    flags = np.where(rng.random(n) < 0.3, rng.integers(1, 9, n), 0).astype(np.int32)
+    sel = np.flatnonzero(flags).astype(np.int32)
+    fs = np.zeros(n, np.int64)
+    fs[1:] = np.cumsum(flags != 0)[:-1]
+    fdev = torch.from_numpy(flags).cuda()
+    for scan_out in (True, False):
+        idx = torch.full_like(fdev, -1)
+        cnt = torch.full((1,), -1, dtype=torch.int32, device="cuda")
+        sc = torch.full_like(fdev, -7)
+        hhs.compact_flags_i32(P(fdev), P(sc) if scan_out else None, P(idx), P(cnt), n, P(ws),
+                              wb, None)
+        torch.cuda.synchronize()
+        k = int(cnt.item())
+        assert k == len(sel), ("count", n, k)
+        assert np.array_equal(idx.cpu().numpy()[:k], sel), ("indices", n)
+        if scan_out:
+            assert np.array_equal(sc.cpu().numpy(), fs.astype(np.int32)), ("flag scan", n)
+print("ok")
+"""
+
+
+@pytest.mark.parametrize("variant", ["20", "21", "22", "23", "24"])
+def test_streamed_scan_shapes_match_numpy(cuda, variant):
+    """The streamed single-pass scan (persistent CTAs, bulk-copied chunks) in each launch
+    shape: exclusive scan and stream compaction (with and without the scan output) at ragged
+    sizes from 1 to 2^24 + 2, including inputs shorter than one chunk and inputs with more
+    chunks than resident CTAs; twice in a row on one workspace, against numpy."""
+    import subprocess
+    import sys
+    from conftest import PKG
+    r = subprocess.run([sys.executable, "-c", _STREAM_CHECK, PKG], capture_output=True,
                        text=True, timeout=600, env={**os.environ, "HHS_SCAN_VARIANT": variant})
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-2000:]
 
