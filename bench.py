@@ -445,7 +445,7 @@ def run_ours(a, rank, world, torch, dist):
 
 # DRAM bytes of one k_engine launch of the default workload (dram__bytes_read.sum +
 # dram__bytes_write.sum of an ncu capture of one launch after three warm-up launches)
-ENGINE_16K_DRAM_BYTES = 1.456128e6 + 1.422080e6
+ENGINE_16K_DRAM_BYTES = 1.582336e6 + 2.816000e6
 
 
 def nominal_fp32_tflops(torch):
